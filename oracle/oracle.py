@@ -1,0 +1,258 @@
+"""ctypes bindings for the CPU oracle: TEST INFRASTRUCTURE ONLY.
+
+`Oracle` wraps liboracle.so, the plain-C restatement of the reference hot path
+(oracle/gail_oracle.c). `Reference` wraps _ref/libgailref.so, the reference's own CPU
+sources compiled by oracle/Makefile (present where the reference tree was available at
+build time; the built file travels with the repository tree).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module;
+the product (libgail_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libgailref.so")
+
+MAX_PASSES = 64
+
+
+class T1Result(C.Structure):
+    _fields_ = [("nbps", C.c_int32), ("num_passes", C.c_int32), ("data_len", C.c_uint32),
+                ("num_symbols", C.c_uint32), ("pass_len", C.c_uint32 * 64), ("pass_dist", C.c_int32 * 64)]
+
+
+class OrBand(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("comp", "res", "level", "orient", "px0", "py0", "w", "h", "ncbx", "ncby",
+                                         "cblk_base", "eps", "mu", "mb")] + [("delta", C.c_float), ("weight", C.c_double)]
+
+
+class OrCblk(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("band", "x0", "y0", "w", "h")]
+
+
+class Planar(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("width", "height", "active_w", "active_h", "ox", "oy", "sx", "sy", "rgb",
+                                         "bits", "full_range", "chroma")] + [("kr", C.c_double), ("kb", C.c_double)]
+
+
+def _p(a, t=C.c_void_p):
+    return a.ctypes.data_as(t)
+
+
+def build(ref: bool = True) -> None:
+    """Compile liboracle.so (and the reference library when its sources are present)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", HERE, "all" if ref else "liboracle.so"], check=True)
+
+
+class T1Block:
+    """The result of coding one block: the fields of the reference's T1Result."""
+
+    def __init__(self, r: T1Result, data: bytes):
+        self.nbps = r.nbps
+        self.num_passes = r.num_passes
+        self.data = data
+        self.pass_len = list(r.pass_len[: r.num_passes])
+        self.pass_dist = list(r.pass_dist[: r.num_passes])
+        self.num_symbols = r.num_symbols
+
+    def key(self):
+        return (self.nbps, self.num_passes, self.data, tuple(self.pass_len), tuple(self.pass_dist))
+
+
+class _Common:
+    lib: C.CDLL
+
+    def _t1(self, fn, coeffs, w, h, orient, max_passes=64, slope=0.0, dist_scale=1.0) -> T1Block:
+        c = np.ascontiguousarray(coeffs, dtype=np.uint32).reshape(-1)
+        assert c.size == 1024
+        buf = np.zeros(4096 * 24 + 64, np.uint8)
+        r = T1Result()
+        rc = fn(_p(c), w, h, orient, max_passes, C.c_float(slope), C.c_float(dist_scale), _p(buf), buf.size, C.byref(r))
+        if rc != 0:
+            raise RuntimeError(f"Tier-1 encode failed ({rc})")
+        return T1Block(r, bytes(buf[: r.data_len]))
+
+
+class Oracle(_Common):
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build(ref=False)
+        L = self.lib = C.CDLL(path)
+        L.or_t1_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p,
+                                   C.c_size_t, C.c_void_p]
+        L.or_quantize.restype = C.c_uint32
+        L.or_quantize.argtypes = [C.c_float, C.c_float, C.c_uint32]
+        L.or_fdwt97_2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.or_idwt97_2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.or_synthesis_norm.restype = C.c_double
+        L.or_synthesis_norm.argtypes = [C.c_int, C.c_int]
+        L.or_geometry_counts.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.or_make_layout.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        L.or_color_init.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double]
+        L.or_color_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.or_planar_to_rgb48.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.or_t1_decode.argtypes = [C.c_void_p, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.or_ict_inverse_pack.argtypes = [C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]
+
+    def t1_encode(self, coeffs, w, h, orient, max_passes=64, slope=0.0, dist_scale=1.0) -> T1Block:
+        return self._t1(self.lib.or_t1_encode, coeffs, w, h, orient, max_passes, slope, dist_scale)
+
+    def quantize(self, v, inv_delta, max_mag):
+        return self.lib.or_quantize(C.c_float(v), C.c_float(inv_delta), max_mag)
+
+    def fdwt(self, plane: np.ndarray, levels: int) -> np.ndarray:
+        p = np.ascontiguousarray(plane, dtype=np.float32).copy()
+        h, w = p.shape
+        self.lib.or_fdwt97_2d(_p(p), w, w, h, levels)
+        return p
+
+    def idwt(self, plane: np.ndarray, levels: int, skip: int = 0) -> np.ndarray:
+        p = np.ascontiguousarray(plane, dtype=np.float32).copy()
+        h, w = p.shape
+        self.lib.or_idwt97_2d(_p(p), w, w, h, levels, skip)
+        return p
+
+    def layout(self, width, height, fourk, base_step=1.0):
+        nb, nc = C.c_int(), C.c_int()
+        self.lib.or_geometry_counts(width, height, 6 if fourk else 5, C.byref(nb), C.byref(nc))
+        bands = (OrBand * nb.value)()
+        cblks = (OrCblk * nc.value)()
+        if self.lib.or_make_layout(width, height, int(fourk), C.c_double(base_step), bands, cblks) != 0:
+            raise RuntimeError("layout: step size out of range")
+        return list(bands), list(cblks)
+
+    def color_frame(self, rgb48: np.ndarray, transfer: int, primaries: int, sdr_white: float = 48.0):
+        """Interleaved R'G'B' 16-bit (H, W, 3) -> (planes (3, H, W) float32, xyz12 (H, W, 3))."""
+        buf = C.create_string_buffer(65536 * 4 + 9 * 4 + 64)
+        self.lib.or_color_init(buf, transfer, primaries, C.c_double(sdr_white))
+        rgb = np.ascontiguousarray(rgb48, dtype=np.uint16)
+        h, w = rgb.shape[:2]
+        planes = np.zeros((3, h, w), np.float32)
+        xyz = np.zeros((h, w, 3), np.uint16)
+        self.lib.or_color_frame(buf, _p(rgb), h * w, _p(planes[0]), _p(planes[1]), _p(planes[2]), _p(xyz))
+        return planes, xyz
+
+    def planar_to_rgb48(self, fmt: Planar, src: np.ndarray) -> np.ndarray:
+        out = np.zeros((fmt.height, fmt.width, 3), np.uint16)
+        s = np.ascontiguousarray(src)
+        self.lib.or_planar_to_rgb48(C.byref(fmt), _p(s), _p(out))
+        return out
+
+    def t1_decode(self, data: bytes, w, h, orient, nbps, passes, length=None) -> np.ndarray:
+        out = np.zeros(1024, np.uint32)
+        d = np.frombuffer(bytes(data) + b"\0", np.uint8)
+        n = len(data) if length is None else length
+        self.lib.or_t1_decode(_p(d), n, w, h, orient, nbps, passes, _p(out))
+        return out
+
+
+class Reference(_Common):
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = self.lib = C.CDLL(path)
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_t1_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p,
+                                    C.c_size_t, C.c_void_p]
+        L.ref_quantize.restype = C.c_uint32
+        L.ref_quantize.argtypes = [C.c_float, C.c_float, C.c_uint32]
+        L.ref_t1_decode.argtypes = [C.c_void_p, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.ref_fdwt97_2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.ref_idwt97_2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.ref_layout_counts.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.ref_make_layout.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        L.ref_synthesis_norm.restype = C.c_double
+        L.ref_synthesis_norm.argtypes = [C.c_int, C.c_int]
+        L.ref_color_frame.argtypes = [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]
+        L.ref_color_tables.argtypes = [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        L.ref_planar_to_rgb48.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_suite_blocks.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.ref_plugin_layout_hash.restype = C.c_uint64
+        L.ref_plugin_sizes.argtypes = [C.c_void_p]
+        L.ref_usable_cpus.restype = C.c_int
+
+    def error(self) -> str:
+        return self.lib.ref_last_error().decode()
+
+    def t1_encode(self, coeffs, w, h, orient, max_passes=64, slope=0.0, dist_scale=1.0) -> T1Block:
+        return self._t1(self.lib.ref_t1_encode, coeffs, w, h, orient, max_passes, slope, dist_scale)
+
+    def quantize(self, v, inv_delta, max_mag):
+        return self.lib.ref_quantize(C.c_float(v), C.c_float(inv_delta), max_mag)
+
+    def t1_decode(self, data: bytes, w, h, orient, nbps, passes, length=None) -> np.ndarray:
+        out = np.zeros(1024, np.uint32)
+        d = np.frombuffer(bytes(data) + b"\0", np.uint8)
+        n = len(data) if length is None else length
+        self.lib.ref_t1_decode(_p(d), n, w, h, orient, nbps, passes, _p(out))
+        return out
+
+    def fdwt(self, plane: np.ndarray, levels: int) -> np.ndarray:
+        p = np.ascontiguousarray(plane, dtype=np.float32).copy()
+        h, w = p.shape
+        self.lib.ref_fdwt97_2d(_p(p), w, h, levels)
+        return p
+
+    def idwt(self, plane: np.ndarray, levels: int, skip: int = 0) -> np.ndarray:
+        p = np.ascontiguousarray(plane, dtype=np.float32).copy()
+        h, w = p.shape
+        self.lib.ref_idwt97_2d(_p(p), w, h, levels, skip)
+        return p
+
+    def layout(self, width, height, fourk, base_step=1.0):
+        nb, nc = C.c_int(), C.c_int()
+        if self.lib.ref_layout_counts(width, height, int(fourk), C.byref(nb), C.byref(nc)) != 0:
+            raise RuntimeError(self.error())
+        bands = (OrBand * nb.value)()
+        cblks = np.zeros((nc.value, 5), np.int32)
+        if self.lib.ref_make_layout(width, height, int(fourk), C.c_double(base_step), bands, _p(cblks)) != 0:
+            raise RuntimeError(self.error())
+        return list(bands), cblks
+
+    def color_frame(self, rgb48: np.ndarray, transfer: int, primaries: int, sdr_white: float = 48.0):
+        rgb = np.ascontiguousarray(rgb48, dtype=np.uint16)
+        h, w = rgb.shape[:2]
+        planes = np.zeros((3, h, w), np.float32)
+        xyz = np.zeros((h, w, 3), np.uint16)
+        self.lib.ref_color_frame(transfer, primaries, C.c_double(sdr_white), _p(rgb), h * w, _p(planes[0]),
+                                 _p(planes[1]), _p(planes[2]), _p(xyz))
+        return planes, xyz
+
+    def color_tables(self, transfer: int, primaries: int, sdr_white: float = 48.0):
+        eotf = np.zeros(65536, np.float32)
+        params = np.zeros(48, np.float32)
+        self.lib.ref_color_tables(transfer, primaries, C.c_double(sdr_white), _p(eotf), _p(params))
+        return eotf, params
+
+    def planar_to_rgb48(self, fmt: Planar, src: np.ndarray) -> np.ndarray:
+        out = np.zeros((fmt.height, fmt.width, 3), np.uint16)
+        s = np.ascontiguousarray(src)
+        self.lib.ref_planar_to_rgb48(C.byref(fmt), _p(s), _p(out))
+        return out
+
+    def suite(self, which: int, ntrials: int):
+        coeffs = np.zeros((ntrials, 1024), np.uint32)
+        meta = np.zeros((ntrials, 4), np.int32)
+        if self.lib.ref_suite_blocks(which, ntrials, _p(coeffs), _p(meta)) != 0:
+            raise ValueError("unknown suite")
+        return coeffs, meta
+
+    def plugin_layout_hash(self) -> int:
+        return self.lib.ref_plugin_layout_hash()
+
+    def plugin_sizes(self):
+        out = np.zeros(12, np.uint64)
+        self.lib.ref_plugin_sizes(_p(out))
+        return [int(x) for x in out]
+
+
+def have_reference() -> bool:
+    return os.path.exists(REF_SO)
