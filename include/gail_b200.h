@@ -1,0 +1,58 @@
+/* gail_b200: B200-native (sm_100a) JPEG 2000 encode/decode hot path behind GAIL's
+ * CUDA plugin ABI.
+ *
+ * The library libgail_cuda13.so exports exactly two kinds of entry point:
+ *
+ *  1. gail_cuda_plugin_get(), the one symbol a GAIL CUDA plugin exports, returning the
+ *     GailCudaPlugin function table (declared in gail_cuda_plugin_abi.h). It replaces the
+ *     reference plugin's entry point, Josephur/libgail src/cuda/cuda_plugin.h:195 and
+ *     src/cuda/cuda_plugin.cpp:249, so that libgail loads this library as its
+ *     gail_cuda13 backend.
+ *
+ *  2. The gb_* functions below: the stages of that path over plain buffers, for callers
+ *     that hold code-blocks, codestreams or Tier-1 frames rather than whole pictures.
+ *     Each names the reference interface it replaces.
+ *
+ * Every function that can fail returns a GailCudaStatus value (0 = OK) and leaves its
+ * message for the calling thread in gb_last_error(). Host pointers everywhere; no
+ * function keeps a pointer it was given after it returns.
+ */
+#ifndef GAIL_B200_H
+#define GAIL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define GB_API __declspec(dllexport)
+#else
+#define GB_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Message of the calling thread's most recent failed call (never NULL). Replaces the
+ * plugin table's last_error, src/cuda/cuda_plugin.h:151. */
+GB_API const char* gb_last_error(void);
+
+/* Tier-1 encode of n quantised code-blocks on the current CUDA device. Replaces
+ * t1EncodeRef (src/core/t1_ref.h:39-40) applied to each block.
+ *   coeffs     n x 1024 sign-magnitude words (bit 31 sign, 6 fractional magnitude bits),
+ *              32 x 32 row-major per block, zero outside the block's w x h
+ *   geom4      n x {w (1..32), h (1..32), orient (0 LL, 1 HL, 2 LH, 3 HH), maxPasses (0..64)}
+ *   slope      early-termination threshold (0: code every pass)
+ *   distScale  per-block distortion scale of that rule (NULL: 1)
+ *   info4      out: n x {nbps, passes, MQ decisions, codeword bytes}
+ *   passLen    out: n x 64 truncation lengths; passDist: n x 64 distortion reductions
+ *   data       out: codeword of block i at data + i * dataStride */
+GB_API int gb_t1_encode_blocks(const uint32_t* coeffs, const int32_t* geom4, uint32_t n, float slope,
+                               const float* distScale, uint32_t* info4, uint32_t* passLen, int32_t* passDist,
+                               uint8_t* data, uint32_t dataStride);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,644 @@
+// EBCOT Tier-1 encoder for sm_100a.
+//
+// Stage 1, context modelling (t1CmKernel): one warp per code-block. Lane x owns column x
+// of the block and keeps its state as 32-bit row masks (bit r = row r): significance,
+// sign, refined-before, coded-in-this-plane. A stripe (4 rows) of one pass is done by all
+// lanes at once. The only sequential dependency of the scan order (columns left to right,
+// rows top down) that matters is significance propagation, where a sample that becomes
+// significant makes later samples eligible; it is solved as a least fixpoint over the
+// warp (shuffle the left column's new significance, recompute, until no lane changes),
+// which is the causal result because the dependency graph runs strictly left to right
+// and top down. Each lane then emits its column's decisions in scan order and a warp
+// prefix sum places them; a plane's decisions are staged in shared memory and copied out
+// with coalesced stores. Per-pass symbol counts and distortion reductions are written.
+//
+// Stage 2, ordering (t1OrderKernel): counting sort of the blocks by decision count, most
+// first, so the longest serial MQ chains start first.
+//
+// Stage 3, MQ coding (t1MqKernel): one lane per code-block. Lanes pull blocks from a
+// device queue one at a time, so a lane that finishes early takes the next block
+// instead of idling while its warp-mates finish. The coder is in branch-free
+// select form (both MPS and LPS take the same instruction path until renormalisation),
+// its contexts live in shared memory, and its input is prefetched 16 decisions ahead.
+// After the flush, each pass's truncation length is computed from the MQ state recorded
+// at its end and the final codeword bytes.
+//
+// Semantics restated from ISO/IEC 15444-1 Annexes C and D as the reference coder applies
+// them (Josephur/libgail core/t1_ref.cpp:52-292, kernels/mq_encoder.h:48-169,
+// kernels/t1_common.h:20-53); bit-exact with it for every block.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+
+#include "common.cuh"
+#include "t1_encode.cuh"
+#include "t1_tables.h"
+
+namespace gb {
+
+namespace {
+
+constexpr int CM_WARPS = 4;          // warps (code-blocks in flight) per CTA
+constexpr int CM_THREADS = CM_WARPS * 32;
+constexpr int STAGE = 2560 + 64;     // staging bytes per warp: one plane's decisions
+constexpr int MQ_THREADS = 128;
+constexpr int ORDER_BUCKETS = 128;
+
+__constant__ uint8_t c_zc[4 * 45];   // zero-coding context by orient, h + 3 v + 9 d
+__constant__ uint8_t c_sc[9];        // sign context | xor bit << 5, by (hc+1) * 3 + (vc+1)
+__constant__ uint32_t c_mq[47];      // Qe | switch << 17 | NMPS << 18 | NLPS << 24
+
+__device__ __forceinline__ uint32_t bit(uint32_t m, int r) { return (m >> r) & 1u; }
+__device__ __forceinline__ int chi(uint32_t sig, uint32_t sgn, int r) {
+    return bit(sig, r) ? (bit(sgn, r) ? -1 : 1) : 0;
+}
+__device__ __forceinline__ int clamp1(int v) { return v < -1 ? -1 : (v > 1 ? 1 : v); }
+__device__ __forceinline__ int32_t distSig(uint32_t w) { return 192 * (int32_t)w - 9216; }
+__device__ __forceinline__ int32_t distRef(uint32_t w) { return w >= 64u ? 64 * (int32_t)w - 5120 : 3072 - 64 * (int32_t)w; }
+
+// Neighbourhood of one column for one stripe, all as row masks.
+struct Nbr {
+    uint32_t L;    // left column, current (includes its new significance in this stripe)
+    uint32_t R;    // right column, as before this stripe (it is visited later)
+    uint32_t S;    // own column as before this stripe
+    uint32_t Gl, Gr, G;  // signs of left, right, own column
+};
+
+// Per-lane decision buffer for one stripe (at most 10 decisions of 6 bits).
+struct Emit {
+    unsigned long long acc;
+    uint32_t n;
+    __device__ __forceinline__ void put(uint32_t cx, uint32_t d) {
+        acc |= (unsigned long long)((cx << 1) | d) << (6 * n);
+        ++n;
+    }
+};
+
+// Zero-coding decision of row r; SN = own column with the rows above r already updated.
+__device__ __forceinline__ uint32_t zcContext(const uint8_t* zc, const Nbr& q, uint32_t SN, int r) {
+    const uint32_t h = bit(q.L, r) + bit(q.R, r);
+    const uint32_t v = bit(SN << 1, r) + bit(q.S >> 1, r);
+    const uint32_t d = bit(q.L << 1, r) + bit(q.L >> 1, r) + bit(q.R << 1, r) + bit(q.R >> 1, r);
+    return zc[h + 3 * v + 9 * d];
+}
+
+// Sign decision of row r (its neighbours as the scan order sees them).
+__device__ __forceinline__ void codeSign(Emit& e, const uint8_t* sc, const Nbr& q, uint32_t SN, int r) {
+    const int hc = clamp1(chi(q.L, q.Gl, r) + chi(q.R, q.Gr, r));
+    const int vc = clamp1(chi(SN << 1, q.G << 1, r) + chi(q.S >> 1, q.G >> 1, r));
+    const uint32_t t = sc[(hc + 1) * 3 + (vc + 1)];
+    e.put(t & 31u, bit(q.G, r) ^ (t >> 5));
+}
+
+// Warp-inclusive prefix sum.
+__device__ __forceinline__ uint32_t warpScan(uint32_t v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__device__ __forceinline__ int32_t warpSum(int32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ uint32_t shUp(uint32_t v, int lane) {
+    const uint32_t t = __shfl_up_sync(kFull, v, 1);
+    return lane == 0 ? 0u : t;
+}
+__device__ __forceinline__ uint32_t shDown(uint32_t v, int lane) {
+    const uint32_t t = __shfl_down_sync(kFull, v, 1);
+    return lane == 31 ? 0u : t;
+}
+
+// Places the stripe's decisions of every lane after `count` in the staging buffer.
+__device__ __forceinline__ uint32_t stage(Emit& e, uint8_t* buf, uint32_t count, int lane, uint32_t* status) {
+    const uint32_t incl = warpScan(e.n, lane);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t at = count + incl - e.n;
+    if (count + total <= (uint32_t)STAGE) {
+        for (uint32_t i = 0; i < e.n; ++i) buf[at + i] = (uint8_t)((e.acc >> (6 * i)) & 63u);
+    } else if (lane == 0) {
+        atomicOr(status, kErrSymbolSpace);
+    }
+    e.acc = 0;
+    e.n = 0;
+    return count + total;
+}
+
+__global__ void __launch_bounds__(CM_THREADS) t1CmKernel(T1Launch P) {
+    __shared__ uint32_t s_mag[CM_WARPS][32][32];
+    __shared__ __align__(16) uint8_t s_stage[CM_WARPS][STAGE];
+    __shared__ uint8_t s_zc[4 * 45];
+    __shared__ uint8_t s_sc[16];
+    __shared__ uint32_t s_hist[CM_WARPS][19];
+    for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) s_zc[i] = c_zc[i];
+    if (threadIdx.x < 9) s_sc[threadIdx.x] = c_sc[threadIdx.x];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t (*mag)[32] = s_mag[wid];
+    uint8_t* buf = s_stage[wid];
+    uint32_t* status = P.ctl + 1;
+
+    for (uint32_t job = blockIdx.x * CM_WARPS + wid; job < P.n; job += gridDim.x * CM_WARPS) {
+        const T1Job J = P.jobs[job];
+        const int w = (J.geom & 31u) + 1, h = ((J.geom >> 5) & 31u) + 1, orient = (J.geom >> 10) & 3u;
+        const int maxPasses = (J.geom >> 12) & 127u;
+        const float slope = P.slope ? P.slope[J.geom >> 19] : 0.f;
+        const uint8_t* zc = s_zc + 45 * orient;
+
+        // Load: lane x reads column x, one 128-byte row per step.
+        const uint32_t* src = P.coeffs + (size_t)J.coeff * kCblkArea;
+        uint32_t sgn = 0, colMax = 0;
+        for (int r = 0; r < 32; ++r) {
+            const uint32_t v = (lane < w && r < h) ? src[r * 32 + lane] : 0u;
+            mag[r][lane] = v & 0x7FFFFFFFu;
+            sgn |= (v >> 31) << r;
+            colMax = max(colMax, v & 0x7FFFFFFFu);
+        }
+        uint32_t mx = colMax;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+        const uint32_t top = mx >> kFracBits;
+        const int nbps = top ? 32 - __clz(top) : 0;
+        uint32_t* info = P.info + 4 * (size_t)job;
+        if (nbps == 0 || 3 * nbps - 2 > kMaxPasses) {
+            if (lane == 0) {
+                info[0] = nbps > 0 ? (uint32_t)nbps : 0u;
+                info[1] = 0;
+                info[2] = 0;
+                info[3] = 0;
+                if (nbps) atomicOr(status, kErrTooManyPlanes);
+            }
+            __syncwarp();
+            continue;
+        }
+        if (lane < 19) s_hist[wid][lane] = 0;
+        __syncwarp();
+
+        const uint32_t valid = lane < w ? (h >= 32 ? kFull : ((1u << h) - 1u)) : 0u;
+        const uint32_t sgnL = shUp(sgn, lane), sgnR = shDown(sgn, lane);
+        uint32_t sig = 0, refined = 0, symTotal = 0;
+        int np = 0;
+        const int nstripes = (h + 3) >> 2;
+        uint8_t* gsym = P.sym + J.region;
+
+        for (int p = nbps - 1; p >= 0 && np < maxPasses; --p) {
+            uint32_t Bp = 0;
+            for (int r = 0; r < h; ++r) Bp |= ((mag[r][lane] >> (p + kFracBits)) & 1u) << r;
+            const uint32_t sig0 = sig;
+            uint32_t vis = 0, count = 0;
+            int32_t planeDist = 0;
+            for (int type = (p == nbps - 1 ? 2 : 0); type < 3 && np < maxPasses; ++type) {
+                int32_t dist = 0;
+                Emit e{0ull, 0u};
+                for (int s = 0; s < nstripes; ++s) {
+                    const int r0 = 4 * s;
+                    const uint32_t sm = (0xFu << r0) & valid;
+                    Nbr q;
+                    q.S = sig;
+                    q.R = shDown(sig, lane);
+                    q.G = sgn;
+                    q.Gl = sgnL;
+                    q.Gr = sgnR;
+                    const uint32_t SL = shUp(sig, lane);
+                    if (type == 0) {
+                        // significance propagation: eligible = insignificant with a
+                        // significant neighbour, in scan order
+                        const uint32_t cand = sm & ~q.S;
+                        const uint32_t spreadLR = SL | (SL << 1) | (SL >> 1) | q.R | (q.R << 1) | (q.R >> 1);
+                        if (!__any_sync(kFull, cand & (spreadLR | (q.S << 1) | (q.S >> 1)))) continue;
+                        uint32_t NEW = 0, E = 0;
+                        for (int it = 0; it < 34; ++it) {
+                            const uint32_t L = SL | shUp(NEW, lane);
+                            const uint32_t side = L | (L << 1) | (L >> 1) | q.R | (q.R << 1) | (q.R >> 1) | (q.S >> 1);
+                            uint32_t nn = 0, ee = 0;
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+                                const uint32_t b = 1u << (r0 + k);
+                                if (!(cand & b)) continue;
+                                const uint32_t above = ((q.S | nn) << 1) & b;
+                                if ((side & b) | above) {
+                                    ee |= b;
+                                    nn |= Bp & b;
+                                }
+                            }
+                            const bool changed = nn != NEW;
+                            NEW = nn;
+                            E = ee;
+                            if (!__any_sync(kFull, changed)) break;
+                        }
+                        q.L = SL | shUp(NEW, lane);
+                        const uint32_t SN = q.S | NEW;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int r = r0 + k;
+                            if (!bit(E, r)) continue;
+                            // above: rows < r are final; below: as before the stripe
+                            const uint32_t upto = SN & ((1u << r) - 1u);
+                            e.put(zcContext(zc, q, q.S | upto, r), bit(Bp, r));
+                            if (bit(NEW, r)) {
+                                codeSign(e, s_sc, q, q.S | upto, r);
+                                dist += distSig((mag[r][lane] >> p) & 0x7Fu);
+                            }
+                        }
+                        sig = SN;
+                        vis |= E;
+                    } else if (type == 1) {
+                        // magnitude refinement of what was significant before this plane
+                        const uint32_t coded = sig0 & sm;
+                        if (!__any_sync(kFull, coded)) continue;
+                        const uint32_t nAny = (q.S << 1) | (q.S >> 1) | SL | (SL << 1) | (SL >> 1) | q.R | (q.R << 1) |
+                                              (q.R >> 1);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int r = r0 + k;
+                            if (!bit(coded, r)) continue;
+                            const uint32_t cx = bit(refined, r) ? 16u : (bit(nAny, r) ? 15u : 14u);
+                            e.put(cx, bit(Bp, r));
+                            dist += distRef((mag[r][lane] >> p) & 0x7Fu);
+                        }
+                    } else {
+                        // cleanup: everything not yet significant and not coded this plane
+                        const uint32_t C = sm & ~q.S & ~vis;
+                        if (!__any_sync(kFull, C)) continue;
+                        const uint32_t NEW = C & Bp;
+                        q.L = SL | shUp(NEW, lane);
+                        const uint32_t SN = q.S | NEW;
+                        const uint32_t four = 0xFu << r0;
+                        int rs = r0;
+                        bool run = r0 + 3 < h && (C & four) == four;
+                        if (run) {
+                            const uint32_t win = r0 == 0 ? 0x1Fu : (0x3Fu << (r0 - 1));
+                            run = !(q.L & win) && !(q.R & win) && !(q.S & win);
+                        }
+                        if (run) {
+                            const uint32_t nb = (NEW >> r0) & 0xFu;
+                            if (nb == 0) {
+                                e.put(17u, 0u);
+                                rs = r0 + 4;
+                            } else {
+                                const int first = __ffs(nb) - 1;
+                                e.put(17u, 1u);
+                                e.put(18u, (uint32_t)first >> 1);
+                                e.put(18u, (uint32_t)first & 1u);
+                                const int r = r0 + first;
+                                codeSign(e, s_sc, q, q.S | (SN & ((1u << r) - 1u)), r);
+                                dist += distSig((mag[r][lane] >> p) & 0x7Fu);
+                                rs = r + 1;
+                            }
+                        }
+                        for (int r = rs; r < r0 + 4; ++r) {
+                            if (!bit(C, r)) continue;
+                            const uint32_t upto = q.S | (SN & ((1u << r) - 1u));
+                            e.put(zcContext(zc, q, upto, r), bit(Bp, r));
+                            if (bit(NEW, r)) {
+                                codeSign(e, s_sc, q, upto, r);
+                                dist += distSig((mag[r][lane] >> p) & 0x7Fu);
+                            }
+                        }
+                        sig = SN;
+                    }
+                    count = stage(e, buf, count, lane, status);
+                }
+                if (type == 1) refined |= sig0;
+                const int32_t total = warpSum(dist);
+                if (lane == 0) {
+                    P.passEnd[(size_t)job * kMaxPasses + np] = symTotal + min(count, (uint32_t)STAGE);
+                    P.passDist[(size_t)job * kMaxPasses + np] = total;
+                }
+                ++np;
+                planeDist += total;
+            }
+            // the plane's decisions to the block's region
+            count = min(count, (uint32_t)STAGE);
+            __syncwarp();
+            if (symTotal + count <= J.cap) {
+                for (uint32_t i = lane; i < count; i += 32) gsym[symTotal + i] = buf[i];
+            } else if (lane == 0) {
+                atomicOr(status, kErrSymbolSpace);
+            }
+            bool stop = false;
+            if (slope > 0.f) {
+                // early termination (the reference's stopAfterPlane, core/t1_ref.cpp:115-162),
+                // with every float operation in the CPU's order
+                for (uint32_t i = lane; i < count; i += 32) {
+                    const uint32_t s = buf[i];
+                    atomicAdd(&s_hist[wid][s >> 1], (s & 1u) ? 0x10000u : 1u);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    float bits = 0.f;
+                    for (int cx = 0; cx < 19; ++cx) {
+                        const uint32_t hv = s_hist[wid][cx];
+                        const float n0 = (float)(hv & 0xFFFFu), n1 = (float)(hv >> 16), n = __fadd_rn(n0, n1);
+                        if (n > 0.f) {
+                            const float l0 = log2f(__fdiv_rn(fmaxf(n0, 0.5f), n));
+                            const float l1 = log2f(__fdiv_rn(fmaxf(n1, 0.5f), n));
+                            const float t = __fadd_rn(__fmul_rn(n0, l0), __fmul_rn(n1, l1));
+                            bits = __fadd_rn(bits, __fadd_rn(-t, 2.f));
+                        }
+                    }
+                    const float bytes = __fadd_rn(__fmul_rn(bits, 0.125f), 1.f);
+                    if (p > 0) {
+                        const float lim = __fmul_rn(slope, bytes);
+                        const float dabs =
+                            __fmul_rn(__fmul_rn(__fmul_rn((float)planeDist, exp2f((float)(2 * p))), 1.f / 4096.f), J.dscale);
+                        if (dabs < lim) {
+                            float e = 0.f;
+                            const float step = exp2f((float)p);
+                            for (int y = 0; y < h; ++y)
+                                for (int x = 0; x < w; ++x) {
+                                    const uint32_t m = mag[y][x];
+                                    const float v = __fmul_rn((float)m, 1.f / 64.f);
+                                    const uint32_t qq = m >> (p + kFracBits);
+                                    const float rec = qq == 0 ? 0.f : __fmul_rn(__fadd_rn((float)qq, 0.5f), step);
+                                    const float d = __fsub_rn(v, rec);
+                                    e = __fadd_rn(e, __fmul_rn(d, d));
+                                }
+                            stop = __fmul_rn(e, J.dscale) < lim;
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane < 19) s_hist[wid][lane] = 0;
+                stop = __shfl_sync(kFull, stop, 0);
+            }
+            symTotal += count;
+            __syncwarp();
+            if (stop) break;
+        }
+        if (lane == 0) {
+            info[0] = (uint32_t)nbps;
+            info[1] = (uint32_t)np;
+            info[2] = symTotal;
+            info[3] = 0;
+            atomicAdd(P.ctl + 2, symTotal);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------- ordering
+__device__ __forceinline__ uint32_t orderBucket(uint32_t s) {
+    // log-spaced classes, four per octave; the most decisions first
+    if (s < 4) return ORDER_BUCKETS - 1;
+    const uint32_t l = 31 - __clz(s);
+    const uint32_t cls = min(4 * l + ((s >> (l - 2)) & 3u), (uint32_t)ORDER_BUCKETS - 1);
+    return ORDER_BUCKETS - 1 - cls;
+}
+
+__global__ void __launch_bounds__(1024) t1OrderKernel(T1Launch P) {
+    __shared__ uint32_t hist[ORDER_BUCKETS];
+    for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < P.n; i += blockDim.x) atomicAdd(&hist[orderBucket(P.info[4 * (size_t)i + 2])], 1u);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        // exclusive scan of 128 counters by one warp, four per lane
+        const int lane = threadIdx.x;
+        uint32_t v[4], s = 0;
+        for (int k = 0; k < 4; ++k) {
+            v[k] = hist[4 * lane + k];
+            s += v[k];
+        }
+        const uint32_t incl = warpScan(s, lane);
+        uint32_t run = incl - s;
+        for (int k = 0; k < 4; ++k) {
+            hist[4 * lane + k] = run;
+            run += v[k];
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < P.n; i += blockDim.x)
+        P.perm[atomicAdd(&hist[orderBucket(P.info[4 * (size_t)i + 2])], 1u)] = i;
+}
+
+// ---------------------------------------------------------------------------- MQ coding
+struct Coder {
+    uint32_t A, C, B;
+    int CT, bp;
+    uint8_t* out;
+    uint32_t cap;
+    bool overflow;
+
+    __device__ __forceinline__ void byteout() {
+        bool stuff = B == 0xFFu;
+        if (!stuff && C >= 0x8000000u) {
+            B += 1u;  // carry into the pending byte
+            if (B == 0xFFu) {
+                C &= 0x7FFFFFFu;
+                stuff = true;
+            }
+        }
+        if (bp >= 0) {
+            if ((uint32_t)bp < cap) out[bp] = (uint8_t)B;
+            else overflow = true;
+        }
+        ++bp;
+        if (stuff) {
+            B = C >> 20;
+            C &= 0xFFFFFu;
+            CT = 7;
+        } else {
+            B = (C >> 19) & 0xFFu;
+            C &= 0x7FFFFu;
+            CT = 8;
+        }
+    }
+    __device__ __forceinline__ void renorm() {
+        int n = __clz(A) - 16;
+        do {
+            const int s = min(n, CT);
+            A <<= s;
+            C <<= s;
+            CT -= s;
+            n -= s;
+            if (CT == 0) byteout();
+        } while (n > 0);
+    }
+    // One decision in context state t (table entry | mps << 16); returns the new state.
+    __device__ __forceinline__ uint32_t encode(uint32_t t, uint32_t d, const uint32_t* tab) {
+        const uint32_t qe = t & 0xFFFFu, mps = (t >> 16) & 1u;
+        const uint32_t a = A - qe;
+        const bool lps = d != mps;
+        const bool upper = (a >= qe) != lps;  // which sub-interval the decision takes
+        C += upper ? qe : 0u;
+        A = upper ? a : qe;
+        if (lps || !(a & 0x8000u)) {
+            const uint32_t nidx = lps ? (t >> 24) & 63u : (t >> 18) & 63u;
+            const uint32_t nm = mps ^ (lps ? (t >> 17) & 1u : 0u);
+            t = tab[nidx] | (nm << 16);
+            renorm();
+        }
+        return t;
+    }
+    __device__ __forceinline__ uint32_t flush() {
+        const uint32_t tempc = C + A;
+        C |= 0xFFFFu;
+        if (C >= tempc) C -= 0x8000u;
+        C <<= CT;
+        byteout();
+        C <<= CT;
+        byteout();
+        if (B != 0xFFu) {
+            if ((uint32_t)bp < cap) out[bp] = (uint8_t)B;
+            else overflow = true;
+            return (uint32_t)(bp + 1);
+        }
+        return (uint32_t)bp;
+    }
+};
+
+// Shortest prefix >= minLen that a decoder reading 1-bits past the end decodes exactly
+// up to the snapshot, never ending on 0xFF. Same arithmetic as the oracle's mq_trunc.
+__device__ uint32_t truncLen(uint4 s, const uint8_t* buf, uint32_t len, uint32_t minLen) {
+    const int bp = (int)s.x;
+    const uint32_t C = s.y, A = s.z & 0xFFFFu, B = s.w;
+    const int CT = (int)(s.z >> 16);
+    const int base = 43 - CT;
+    const unsigned long long low = ((unsigned long long)B << base) + ((unsigned long long)C << 16);
+    const unsigned long long high = low + ((unsigned long long)A << 16);
+    unsigned long long acc = 0;
+    int used = 0;
+    for (int i = bp; i < (int)len; ++i) {
+        const uint32_t byte = i >= 0 ? buf[i] : 0u;
+        const int sh = base - used;
+        if (sh < 0) break;
+        acc += (unsigned long long)byte << sh;
+        const unsigned long long tail = 1ull << sh;
+        const uint32_t l = (uint32_t)(i + 1);
+        if (l >= minLen && byte != 0xFFu && acc + tail <= high && acc + tail > low) return l;
+        used += byte == 0xFFu ? 7 : 8;
+    }
+    return len;
+}
+
+__device__ __forceinline__ uint32_t byteOf(const uint4& v, uint32_t i) {
+    const uint32_t w = i < 8 ? (i < 4 ? v.x : v.y) : (i < 12 ? v.z : v.w);
+    return (w >> (8 * (i & 3u))) & 0xFFu;
+}
+
+__global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
+    __shared__ uint32_t s_tab[48];
+    __shared__ uint32_t s_ctx[19 * MQ_THREADS];
+    for (int i = threadIdx.x; i < 47; i += blockDim.x) s_tab[i] = c_mq[i];
+    __syncthreads();
+    uint32_t* ctx = s_ctx + threadIdx.x;
+    uint32_t* status = P.ctl + 1;
+
+    // Per-lane state of the block in hand.
+    uint32_t job = 0, pos = 0, nsym = 0, np = 0, k = 0, nextEnd = 0;
+    const uint8_t* sym = nullptr;
+    uint4 cur = make_uint4(0, 0, 0, 0), nxt = cur;
+    Coder e;
+    e.cap = 0;
+    bool have = false;
+
+    for (;;) {
+        if (!have || pos == nsym) {
+            if (have) {
+                // end of block: remaining pass ends, flush, truncation points
+                while (k < np) {
+                    P.snaps[(size_t)job * kMaxPasses + k] =
+                        make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
+                    ++k;
+                }
+                const uint32_t len = e.flush();
+                if (e.overflow) atomicOr(status, kErrCodewordSpace);
+                uint32_t prev = 1;
+                for (uint32_t q = 0; q < np; ++q) {
+                    const uint32_t L =
+                        q == np - 1 ? len : truncLen(P.snaps[(size_t)job * kMaxPasses + q], e.out, min(len, e.cap), prev);
+                    P.passLen[(size_t)job * kMaxPasses + q] = L;
+                    prev = max(prev, L);
+                }
+                P.info[4 * (size_t)job + 3] = e.overflow ? 0u : len;
+                have = false;
+            }
+            // next block
+            uint32_t qi;
+            for (;;) {
+                qi = atomicAdd(P.ctl, 1u);
+                if (qi >= P.n) break;
+                job = P.perm[qi];
+                np = P.info[4 * (size_t)job + 1];
+                nsym = P.info[4 * (size_t)job + 2];
+                if (np == 0) {
+                    P.info[4 * (size_t)job + 3] = 0;
+                    continue;
+                }
+                break;
+            }
+            if (qi >= P.n) break;
+            const T1Job J = P.jobs[job];
+            sym = P.sym + J.region;
+            e.out = P.cw + J.region;
+            e.cap = J.cap;
+            e.A = 0x8000u;
+            e.C = 0;
+            e.CT = 12;
+            e.bp = -1;
+            e.B = 0;
+            e.overflow = false;
+            // initial states, Table D.7: ZC context 0 state 4, run-length 3, uniform 46
+#pragma unroll
+            for (int c = 0; c < 19; ++c) ctx[c * MQ_THREADS] = s_tab[0];
+            ctx[0] = s_tab[4];
+            ctx[17 * MQ_THREADS] = s_tab[3];
+            ctx[18 * MQ_THREADS] = s_tab[46];
+            pos = 0;
+            k = 0;
+            nextEnd = P.passEnd[(size_t)job * kMaxPasses];
+            cur = nsym ? *reinterpret_cast<const uint4*>(sym) : make_uint4(0, 0, 0, 0);
+            nxt = nsym > 16 ? *reinterpret_cast<const uint4*>(sym + 16) : make_uint4(0, 0, 0, 0);
+            have = true;
+            if (nsym == 0) continue;
+        }
+        while (pos == nextEnd && k < np) {
+            P.snaps[(size_t)job * kMaxPasses + k] = make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
+            ++k;
+            nextEnd = k < np ? P.passEnd[(size_t)job * kMaxPasses + k] : 0xFFFFFFFFu;
+        }
+        const uint32_t s = byteOf(cur, pos & 15u);
+        const uint32_t cx = s >> 1;
+        ctx[cx * MQ_THREADS] = e.encode(ctx[cx * MQ_THREADS], s & 1u, s_tab);
+        ++pos;
+        if ((pos & 15u) == 0) {
+            cur = nxt;
+            if (pos + 16 < nsym) nxt = *reinterpret_cast<const uint4*>(sym + pos + 16);
+        }
+    }
+}
+
+}  // namespace
+
+void t1Init() {
+    uint8_t zc[4 * 45], sc[9];
+    uint32_t mq[47];
+    t1BuildTables(zc, sc, mq);
+    GB_CHECK(cudaMemcpyToSymbol(c_zc, zc, sizeof zc));
+    GB_CHECK(cudaMemcpyToSymbol(c_sc, sc, sizeof sc));
+    GB_CHECK(cudaMemcpyToSymbol(c_mq, mq, sizeof mq));
+}
+
+void t1Encode(const T1Launch& L, cudaStream_t st) {
+    if (L.n == 0) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t cmBlocks = min(divUp(L.n, CM_WARPS), (uint32_t)sms * 16u);
+    t1CmKernel<<<cmBlocks, CM_THREADS, 0, st>>>(L);
+    t1OrderKernel<<<1, 1024, 0, st>>>(L);
+    const uint32_t mqBlocks = min(divUp(L.n, MQ_THREADS), (uint32_t)sms * 16u);
+    t1MqKernel<<<mqBlocks, MQ_THREADS, 0, st>>>(L);
+    GB_CHECK(cudaGetLastError());
+}
+
+}  // namespace gb

@@ -1,0 +1,58 @@
+// EBCOT Tier-1 encoder on sm_100a: context modelling, MQ coding, exact truncation
+// lengths and per-pass distortions, bit-exact with the reference CPU coder
+// (Josephur/libgail core/t1_ref.cpp). Host-side view of the device work.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace gb {
+
+// One code-block to code. 32 bytes, read once per block by each kernel.
+struct T1Job {
+    uint32_t coeff;   // index of the block's 1024 sign-magnitude words in the coefficient buffer
+    uint32_t region;  // byte offset of its symbol region, and of its codeword region (16-aligned)
+    uint32_t cap;     // bytes in either region
+    uint32_t geom;    // (w-1) | (h-1) << 5 | orient << 10 | maxPasses << 12 | frame << 19
+    float dscale;     // band delta^2 * weight: distortion units of the early-termination rule
+    uint32_t pad[3];
+};
+
+inline uint32_t t1Geom(int w, int h, int orient, int maxPasses, int frame) {
+    return (uint32_t)(w - 1) | ((uint32_t)(h - 1) << 5) | ((uint32_t)orient << 10) | ((uint32_t)maxPasses << 12) |
+           ((uint32_t)frame << 19);
+}
+
+// Worst-case MQ decisions of a block: each sample is coded once per bit-plane with at most
+// a significance and a sign decision, plus run-length decisions (3 per stripe column of 4
+// samples, which then skip one significance decision): 2.5 per sample and plane.
+inline uint32_t t1SymbolBound(int w, int h, int planes) {
+    const uint32_t perPlane = (uint32_t)((5 * w * h + 1) / 2);
+    return ((perPlane * (uint32_t)planes + 64u) + 15u) & ~15u;
+}
+
+// Device pointers of one Tier-1 launch (any number of frames: the jobs say where).
+struct T1Launch {
+    const uint32_t* coeffs;
+    const T1Job* jobs;
+    uint32_t n;
+    uint8_t* sym;        // symbol arena
+    uint8_t* cw;         // codeword arena, same offsets as the symbol arena
+    uint32_t* info;      // 4 words per job: nbps, passes, symbols, codeword bytes
+    uint32_t* passEnd;   // 64 per job: decisions coded by the end of each pass
+    uint32_t* passLen;   // 64 per job: truncation length after each pass
+    int32_t* passDist;   // 64 per job: distortion reduction of each pass (x4096, plane units)
+    uint4* snaps;        // 64 per job: MQ state at the end of each pass
+    uint32_t* perm;      // n: jobs in MQ order (most decisions first)
+    uint32_t* ctl;       // [0] MQ queue head, [1] status bits, [2] total decisions
+    const float* slope;  // per-frame early-termination threshold (NULL: code every pass)
+};
+
+// Enqueues the whole Tier-1 stage on st: context modelling, ordering, MQ coding.
+// ctl must be zeroed by the caller (it is part of the launch so that graphs can hold it).
+void t1Encode(const T1Launch& L, cudaStream_t st);
+
+// Uploads the context tables (once per device, before the first launch).
+void t1Init();
+
+}  // namespace gb
