@@ -23,6 +23,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "gail_cuda_plugin_abi.h"
+
 #if defined(_WIN32)
 #define GB_API __declspec(dllexport)
 #else
@@ -50,6 +52,21 @@ GB_API const char* gb_last_error(void);
 GB_API int gb_t1_encode_blocks(const uint32_t* coeffs, const int32_t* geom4, uint32_t n, float slope,
                                const float* distScale, uint32_t* info4, uint32_t* passLen, int32_t* passDist,
                                uint8_t* data, uint32_t dataStride);
+
+/* The DCI frame layout: subbands (with their quantisation steps) in the plugin ABI's
+ * form, for callers that build GailCudaLayout themselves. Replaces makeLayout
+ * (src/core/layout.h:87 with Profile::Cinema2K / Cinema4K). maxBands >= 3 * 19 + 3. */
+GB_API int gb_make_layout(int width, int height, int fourk, double baseStep, GbSubband* bands, int maxBands,
+                          int* numBands, int* numCblks);
+
+/* The colour tables the encoder uploads for a colour setting: the 65536-entry EOTF, the
+ * RGB->XYZ matrix and the 4096 thresholds of the 12-bit DCI encoding. Replaces
+ * ColorConverter's lut()/params() (src/core/color.h:105-108). Any pointer may be NULL. */
+GB_API int gb_color_tables(const GailCudaColor* color, float* eotf65536, float* matrix9, float* thresholds4096);
+
+/* FNV hash of the ABI structure sizes, as the plugin table's `layout` field carries it
+ * (cudaPluginLayout, src/cuda/cuda_plugin.h:208-217). */
+GB_API uint64_t gb_plugin_layout_hash(void);
 
 #ifdef __cplusplus
 }

@@ -38,6 +38,8 @@ def lib() -> C.CDLL:
         L.gb_last_error.restype = C.c_char_p
         L.gb_t1_encode_blocks.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+        L.gb_plugin_layout_hash.restype = C.c_uint64
+        L.gb_plugin_layout_hash.argtypes = []
         _lib = L
     return _lib
 

@@ -7,6 +7,8 @@
 #include <mutex>
 #include <set>
 
+#include "decoder.h"
+#include "frontend.cuh"
 #include "t1_encode.cuh"
 
 namespace gb {
@@ -26,6 +28,8 @@ void ensureDevice() {
     std::lock_guard<std::mutex> lock(g_initMutex);
     if (g_ready.count(dev)) return;
     t1Init();
+    frontendInit();
+    decoderInit();
     g_ready.insert(dev);
 }
 

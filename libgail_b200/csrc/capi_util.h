@@ -42,5 +42,7 @@ int gbGuard(F&& fn) noexcept {
 
 // Makes sure the calling thread has a current device with this library's tables loaded.
 void ensureDevice();
+// Whether this library's kernels load on the current device (cudaSuccess when they do).
+cudaError_t kernelsLoadable();
 
 }  // namespace gb

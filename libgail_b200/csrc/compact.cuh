@@ -1,0 +1,27 @@
+// Packing of Tier-1 results into the Tier1Frame layout.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "t1_encode.cuh"
+
+namespace gb {
+
+struct CompactArgs {
+    uint32_t n;
+    const uint32_t* info;      // 4 words per block (nbps, passes, decisions, bytes)
+    const uint32_t* passLen;   // 64 per block
+    const int32_t* passDist;   // 64 per block
+    const uint8_t* cw;         // codeword arena
+    const T1Job* jobs;         // each block's codeword region
+    uint32_t* outInfo;         // 5 words per block: CblkInfo
+    uint32_t* outPassLen;
+    int32_t* outPassDist;
+    uint8_t* outData;
+    uint32_t* tot;             // [0] data bytes, [1] passes
+};
+
+void compactTier1(const CompactArgs& a, cudaStream_t st);
+
+}  // namespace gb

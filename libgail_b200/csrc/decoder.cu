@@ -1,0 +1,677 @@
+// Decoder on sm_100a: Tier-1 decoding with dequantisation, inverse 9/7 wavelet, inverse
+// ICT and 12-bit packing.
+//
+// Tier-1 (decodeKernel): one lane per code-block. The MQ decoder is serial per block, so
+// lanes pull blocks from a device queue ordered longest codeword first (orderKernel) and
+// take the next as soon as theirs is done. A block's state is kept as row masks in
+// shared memory (significance and sign for rows -1..32, coded-this-plane and refined),
+// the scan visits only columns that have something to code (bit scans over candidate
+// masks), and the decoded words (sign, twice the magnitude plus the mid-point of the
+// planes not decoded) are built in place in the wavelet plane and turned into floats
+// (word * step / 2) when the block is done. Untrusted input: bytes past the codeword read
+// as 0xFF, a block whose bytes lie outside the codestream decodes as zero, and nothing
+// outside the block's own samples is written.
+//
+// Inverse wavelet (invLevelKernel): per level, 64 x 64 output tiles with a 4-sample halo
+// in the interleaved domain, rows then columns (the reference's order), whole-sample
+// symmetric mirror at the edges. The last level carries the inverse ICT, the rounding
+// and clamping to 12 bits and the interleaved 16-bit store.
+//
+// Semantics restated from Josephur/libgail core/t1_dec.cpp:45-179,
+// kernels/mq_decoder.h:46-114, core/cpu_decode_backend.cpp:36-99 and
+// core/dwt_cpu.cpp:96-133, 213-240; bit-identical to the CPU decoder.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "common.cuh"
+#include "decoder.h"
+#include "t1_tables.h"
+
+namespace gb {
+
+namespace {
+
+constexpr int DEC_THREADS = 64;
+constexpr int ORDER_BUCKETS = 128;
+
+__constant__ uint8_t c_zc[4 * 45];
+__constant__ uint8_t c_sc[9];
+__constant__ uint32_t c_mq[47];
+
+struct DecArgs {
+    const uint8_t* bytes;
+    uint64_t size;
+    const GbCblkCode* codes;
+    const DecBlock* blocks;
+    uint32_t n;
+    const float* half;  // per band: step / 2
+    uint32_t* planes;   // float planes seen as words while decoding
+    uint32_t W;
+    uint32_t* perm;
+    uint32_t* ctl;      // [0] queue head, [1] status, [2] wanted blocks
+};
+
+__device__ __forceinline__ uint32_t lenBucket(uint32_t len) {
+    if (len < 4) return ORDER_BUCKETS - 1;
+    const uint32_t l = 31 - __clz(len);
+    return ORDER_BUCKETS - 1 - min(4 * l + ((len >> (l - 2)) & 3u), (uint32_t)ORDER_BUCKETS - 1);
+}
+
+__global__ void __launch_bounds__(1024) orderKernel(DecArgs a) {
+    __shared__ uint32_t hist[ORDER_BUCKETS];
+    __shared__ uint32_t total;
+    for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
+    if (threadIdx.x == 0) total = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < a.n; i += blockDim.x)
+        if (a.blocks[i].wanted) {
+            atomicAdd(&hist[lenBucket(a.codes[i].len)], 1u);
+            atomicAdd(&total, 1u);
+        }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int b = 0; b < ORDER_BUCKETS; ++b) {
+            const uint32_t c = hist[b];
+            hist[b] = run;
+            run += c;
+        }
+        a.ctl[2] = total;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < a.n; i += blockDim.x)
+        if (a.blocks[i].wanted) a.perm[atomicAdd(&hist[lenBucket(a.codes[i].len)], 1u)] = i;
+}
+
+// MQ decoder (ISO/IEC 15444-1 C.3) over one codeword; bytes past its end read as 0xFF.
+struct MqDecoder {
+    uint32_t A, C, bp, end;
+    int CT;
+    const uint8_t* in;
+
+    __device__ __forceinline__ uint32_t at(uint32_t i) const { return i < end ? (uint32_t)in[i] : 0xFFu; }
+    __device__ __forceinline__ void bytein() {
+        const uint32_t b = at(bp), b1 = at(bp + 1);
+        if (b == 0xFFu) {
+            if (b1 > 0x8Fu) {  // a marker: not consumed, ones from here on
+                C += 0xFF00u;
+                CT = 8;
+            } else {
+                ++bp;
+                C += b1 << 9;
+                CT = 7;
+            }
+        } else {
+            ++bp;
+            C += b1 << 8;
+            CT = 8;
+        }
+    }
+    __device__ __forceinline__ void init(const uint8_t* data, uint32_t len) {
+        in = data;
+        end = len;
+        bp = 0;
+        C = at(0) << 16;
+        bytein();
+        C <<= 7;
+        CT -= 7;
+        A = 0x8000u;
+    }
+    __device__ __forceinline__ void renorm() {
+        int n = __clz(A) - 16;
+        do {
+            if (CT == 0) bytein();
+            const int s = min(n, CT);
+            A <<= s;
+            C <<= s;
+            CT -= s;
+            n -= s;
+        } while (n > 0);
+    }
+    // One decision in context cx (state word: table entry | mps << 16).
+    __device__ __forceinline__ uint32_t decode(uint32_t* ctx, int cx, const uint32_t* tab) {
+        uint32_t t = ctx[cx * DEC_THREADS];
+        const uint32_t qe = t & 0xFFFFu, mps = (t >> 16) & 1u;
+        A -= qe;
+        bool lps;
+        if ((C >> 16) < qe) {
+            lps = A >= qe;  // conditional exchange in the lower sub-interval
+            A = qe;
+        } else {
+            C -= qe << 16;
+            if (A & 0x8000u) return mps;
+            lps = A < qe;
+        }
+        const uint32_t nidx = lps ? (t >> 24) & 63u : (t >> 18) & 63u;
+        const uint32_t nm = mps ^ (lps ? (t >> 17) & 1u : 0u);
+        ctx[cx * DEC_THREADS] = tab[nidx] | (nm << 16);
+        renorm();
+        return lps ? mps ^ 1u : mps;
+    }
+};
+
+__device__ __forceinline__ uint32_t bt(uint32_t m, int x) { return (m >> x) & 1u; }
+__device__ __forceinline__ int chiAt(uint32_t s, uint32_t g, int x) {
+    return (x < 0 || x > 31) ? 0 : (bt(s, x) ? (bt(g, x) ? -1 : 1) : 0);
+}
+
+struct BlockState {
+    uint32_t* sig;  // rows -1..32 at index (y + 1) * DEC_THREADS
+    uint32_t* sgn;
+    uint32_t* vis;  // rows 0..31
+    uint32_t* ref;
+    uint32_t* out;  // the block's top-left word in the plane
+    uint32_t W;
+    const uint8_t* zc;
+    const uint8_t* sc;
+    const uint32_t* tab;
+    uint32_t* ctx;
+    MqDecoder mq;
+
+    __device__ __forceinline__ uint32_t S(int y) const { return sig[(y + 1) * DEC_THREADS]; }
+    __device__ __forceinline__ uint32_t G(int y) const { return sgn[(y + 1) * DEC_THREADS]; }
+
+    __device__ __forceinline__ uint32_t zcAt(int x, int y) const {
+        const uint32_t U = S(y - 1), M = S(y), D = S(y + 1);
+        const uint32_t h = bt(M << 1, x) + bt(M >> 1, x);
+        const uint32_t v = bt(U, x) + bt(D, x);
+        const uint32_t d = bt(U << 1, x) + bt(U >> 1, x) + bt(D << 1, x) + bt(D >> 1, x);
+        return zc[h + 3 * v + 9 * d];
+    }
+    __device__ __forceinline__ bool anyNbr(int x, int y) const {
+        const uint32_t U = S(y - 1), M = S(y), D = S(y + 1);
+        const uint32_t all = U | (U << 1) | (U >> 1) | (M << 1) | (M >> 1) | D | (D << 1) | (D >> 1);
+        return bt(all, x);
+    }
+    // The sample's first 1-bit is in plane p: decode its sign and set bit plus mid-point.
+    __device__ __forceinline__ void becomeSig(int x, int y, int p) {
+        const uint32_t U = S(y - 1), M = S(y), D = S(y + 1);
+        const int hc = max(-1, min(1, chiAt(M, G(y), x - 1) + chiAt(M, G(y), x + 1)));
+        const int vc = max(-1, min(1, chiAt(U, G(y - 1), x) + chiAt(D, G(y + 1), x)));
+        const uint32_t t = sc[(hc + 1) * 3 + (vc + 1)];
+        const uint32_t neg = mq.decode(ctx, t & 31u, tab) ^ (t >> 5);
+        sig[(y + 1) * DEC_THREADS] |= 1u << x;
+        if (neg) sgn[(y + 1) * DEC_THREADS] |= 1u << x;
+        out[(size_t)y * W + x] = (neg << 31) | (3u << p);
+    }
+};
+
+__global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
+    __shared__ uint32_t s_sig[34 * DEC_THREADS], s_sgn[34 * DEC_THREADS], s_vis[32 * DEC_THREADS], s_ref[32 * DEC_THREADS];
+    __shared__ uint32_t s_ctx[19 * DEC_THREADS];
+    __shared__ uint32_t s_tab[48];
+    __shared__ uint8_t s_zc[4 * 45], s_sc[16];
+    for (int i = threadIdx.x; i < 47; i += blockDim.x) s_tab[i] = c_mq[i];
+    for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) s_zc[i] = c_zc[i];
+    if (threadIdx.x < 9) s_sc[threadIdx.x] = c_sc[threadIdx.x];
+    __syncthreads();
+    const int tid = threadIdx.x;
+    BlockState b;
+    b.sig = s_sig + tid;
+    b.sgn = s_sgn + tid;
+    b.vis = s_vis + tid;
+    b.ref = s_ref + tid;
+    b.ctx = s_ctx + tid;
+    b.sc = s_sc;
+    b.tab = s_tab;
+    b.W = a.W;
+    const uint32_t count = a.ctl[2];
+    for (;;) {
+        const uint32_t q = atomicAdd(a.ctl, 1u);
+        if (q >= count) break;
+        const uint32_t j = a.perm[q];
+        const DecBlock blk = a.blocks[j];
+        const GbCblkCode code = a.codes[j];
+        const int w = blk.w, h = blk.h;
+        uint32_t* out = a.planes + blk.dst;
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x) out[(size_t)y * a.W + x] = 0u;
+        const int nbps = code.nbps;
+        const bool valid = code.passes > 0 && nbps >= 1 && nbps <= 30 && (uint64_t)code.offset + code.len <= a.size;
+        if (valid) {
+            b.out = out;
+            b.zc = s_zc + 45 * blk.orient;
+            for (int i = 0; i < 34; ++i) {
+                b.sig[i * DEC_THREADS] = 0;
+                b.sgn[i * DEC_THREADS] = 0;
+            }
+            for (int i = 0; i < 32; ++i) {
+                b.vis[i * DEC_THREADS] = 0;
+                b.ref[i * DEC_THREADS] = 0;
+            }
+            for (int c = 0; c < 19; ++c) b.ctx[c * DEC_THREADS] = s_tab[0];
+            b.ctx[0] = s_tab[4];
+            b.ctx[17 * DEC_THREADS] = s_tab[3];
+            b.ctx[18 * DEC_THREADS] = s_tab[46];
+            b.mq.init(a.bytes + code.offset, code.len);
+            const uint32_t wmask = w >= 32 ? 0xFFFFFFFFu : (1u << w) - 1u;
+            int done = 0;
+            const int passes = code.passes;
+            for (int p = nbps - 1; p >= 0 && done < passes; --p) {
+                for (int type = (p == nbps - 1 ? 2 : 0); type < 3 && done < passes; ++type, ++done) {
+                    for (int y0 = 0; y0 < h; y0 += 4) {
+                        const int n = min(4, h - y0);
+                        if (type == 0) {
+                            uint32_t cm = 0;
+                            for (int k = 0; k < n; ++k) {
+                                const uint32_t U = b.S(y0 + k - 1), M = b.S(y0 + k), D = b.S(y0 + k + 1);
+                                const uint32_t nb = U | (U << 1) | (U >> 1) | (M << 1) | (M >> 1) | D | (D << 1) | (D >> 1);
+                                cm |= nb & ~M & wmask;
+                            }
+                            while (cm) {
+                                const int x = __ffs(cm) - 1;
+                                cm &= cm - 1;
+                                for (int k = 0; k < n; ++k) {
+                                    const int y = y0 + k;
+                                    if (bt(b.S(y), x) || !b.anyNbr(x, y)) continue;
+                                    const uint32_t bit = b.mq.decode(b.ctx, b.zcAt(x, y), b.tab);
+                                    b.vis[y * DEC_THREADS] |= 1u << x;
+                                    if (bit) {
+                                        b.becomeSig(x, y, p);
+                                        cm |= (2u << x) & wmask;  // the next column may now be eligible
+                                    }
+                                }
+                            }
+                        } else if (type == 1) {
+                            uint32_t cm = 0;
+                            for (int k = 0; k < n; ++k) cm |= b.S(y0 + k) & ~b.vis[(y0 + k) * DEC_THREADS];
+                            while (cm) {
+                                const int x = __ffs(cm) - 1;
+                                cm &= cm - 1;
+                                for (int k = 0; k < n; ++k) {
+                                    const int y = y0 + k;
+                                    if (!bt(b.S(y), x) || bt(b.vis[y * DEC_THREADS], x)) continue;
+                                    const int cx = bt(b.ref[y * DEC_THREADS], x) ? 16 : (b.anyNbr(x, y) ? 15 : 14);
+                                    const uint32_t bit = b.mq.decode(b.ctx, cx, b.tab);
+                                    uint32_t& word = out[(size_t)y * a.W + x];
+                                    word = bit ? word + (1u << p) : word - (1u << p);
+                                    b.ref[y * DEC_THREADS] |= 1u << x;
+                                }
+                            }
+                        } else {
+                            uint32_t cm = 0;
+                            for (int k = 0; k < n; ++k) cm |= ~b.S(y0 + k) & ~b.vis[(y0 + k) * DEC_THREADS] & wmask;
+                            while (cm) {
+                                const int x = __ffs(cm) - 1;
+                                cm &= cm - 1;
+                                int r = 0;
+                                if (n == 4) {
+                                    bool quiet = true;
+                                    for (int k = 0; k < 4 && quiet; ++k) {
+                                        const int y = y0 + k;
+                                        if (bt(b.S(y) | b.vis[y * DEC_THREADS], x) || b.anyNbr(x, y)) quiet = false;
+                                    }
+                                    if (quiet) {
+                                        if (!b.mq.decode(b.ctx, 17, b.tab)) continue;
+                                        int first = (int)b.mq.decode(b.ctx, 18, b.tab) << 1;
+                                        first |= (int)b.mq.decode(b.ctx, 18, b.tab);
+                                        b.becomeSig(x, y0 + first, p);
+                                        r = first + 1;
+                                    }
+                                }
+                                for (int k = r; k < n; ++k) {
+                                    const int y = y0 + k;
+                                    if (bt(b.S(y) | b.vis[y * DEC_THREADS], x)) continue;
+                                    if (b.mq.decode(b.ctx, b.zcAt(x, y), b.tab)) b.becomeSig(x, y, p);
+                                }
+                            }
+                        }
+                    }
+                }
+                for (int i = 0; i < 32; ++i) b.vis[i * DEC_THREADS] = 0;
+            }
+        }
+        // dequantise in place: word * step / 2, sign from bit 31
+        const float half = a.half[blk.band];
+        float* f = reinterpret_cast<float*>(out);
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x) {
+                const uint32_t v = out[(size_t)y * a.W + x];
+                const float m = (float)(v & 0x7FFFFFFFu) * half;
+                f[(size_t)y * a.W + x] = (v & 0x80000000u) ? -m : m;
+            }
+    }
+}
+
+// ---------------------------------------------------------------------------- inverse DWT
+constexpr int TS = 64, HALO = 4, TW = TS + 2 * HALO, TP = TW + 1;
+constexpr int IV_THREADS = 256;
+__constant__ float kUnlift[4] = {-(float)0.443506852043971, -(float)0.882911075530934, -(float)-0.052980118572961,
+                              -(float)-1.586134342059924};  // -delta, -gamma, -beta, -alpha
+constexpr float kK = (float)1.230174104914001;
+constexpr float kInvK = (float)(1.0 / 1.230174104914001);
+
+__device__ __forceinline__ int mirror(int i, int n) {
+    if (n == 1) return 0;
+    const int period = 2 * (n - 1);
+    i %= period;
+    if (i < 0) i += period;
+    return i < n ? i : period - i;
+}
+
+struct InvArgs {
+    int w, h;            // this level's output (interleaved) size
+    int snx, sny;        // low-band sizes
+    const float* A;      // Mallat planes (high bands of this level; LL too at the top level)
+    uint64_t aComp;
+    int aStride;
+    const float* ll;     // LL of this level (the previous inverse output), or NULL: take it from A
+    uint64_t llComp;
+    int llStride;
+    float* out;          // LL of the level below (interleaved), or NULL at the last level
+    uint64_t outComp;
+    int outStride;
+    uint16_t* pix;       // last level: interleaved 12-bit X'Y'Z' output
+    int shift;
+};
+
+__device__ __forceinline__ float coeffAt(const InvArgs& a, int comp, int gy, int gx) {
+    const bool ly = !(gy & 1), lx = !(gx & 1);
+    if (ly && lx) {
+        if (a.ll) return a.ll[comp * a.llComp + (size_t)(gy >> 1) * a.llStride + (gx >> 1)];
+        return a.A[comp * a.aComp + (size_t)(gy >> 1) * a.aStride + (gx >> 1)];
+    }
+    const int row = ly ? (gy >> 1) : a.sny + (gy >> 1), col = lx ? (gx >> 1) : a.snx + (gx >> 1);
+    return a.A[comp * a.aComp + (size_t)row * a.aStride + col];
+}
+
+template <bool LAST>
+__global__ void __launch_bounds__(IV_THREADS) invLevelKernel(InvArgs a) {
+    extern __shared__ float smem[];
+    constexpr int NC = LAST ? 3 : 1;
+    const int tid = threadIdx.x, tx = blockIdx.x, ty = blockIdx.y;
+    const int x0 = tx * TS - HALO, y0 = ty * TS - HALO;
+    const int w = a.w, h = a.h;
+    for (int k = 0; k < NC; ++k) {
+        const int comp = LAST ? k : (int)blockIdx.z;
+        float* t = smem + k * TW * TP;
+        for (int idx = tid; idx < TW * TW; idx += IV_THREADS) {
+            const int ly = idx / TW, lx = idx % TW;
+            t[ly * TP + lx] = coeffAt(a, comp, mirror(y0 + ly, h), mirror(x0 + lx, w));
+        }
+    }
+    __syncthreads();
+    for (int k = 0; k < NC; ++k) {
+        float* t = smem + k * TW * TP;
+        if (w >= 2) {  // rows: scale, then the lifting steps undone in reverse
+            for (int idx = tid; idx < TW * TW; idx += IV_THREADS) {
+                const int r = idx % TW, col = idx / TW;
+                t[r * TP + col] *= (col & 1) ? kInvK : kK;
+            }
+            __syncthreads();
+#pragma unroll 1
+            for (int s = 0; s < 4; ++s) {
+                const int first = (s & 1) ? 1 : 2;  // -delta, -beta: even; -gamma, -alpha: odd
+                const float c = kUnlift[s];
+                for (int idx = tid; idx < TW * 35; idx += IV_THREADS) {
+                    const int r = idx % TW, i = first + 2 * (idx / TW);
+                    float* x = t + r * TP + i;
+                    x[0] += c * (x[-1] + x[1]);
+                }
+                __syncthreads();
+            }
+        }
+        if (h >= 2) {  // then columns
+            for (int idx = tid; idx < TW * TS; idx += IV_THREADS) {
+                const int col = HALO + idx % TS, r = idx / TS;
+                t[r * TP + col] *= (r & 1) ? kInvK : kK;
+            }
+            __syncthreads();
+#pragma unroll 1
+            for (int s = 0; s < 4; ++s) {
+                const int first = (s & 1) ? 1 : 2;
+                const float c = kUnlift[s];
+                for (int idx = tid; idx < TS * 35; idx += IV_THREADS) {
+                    const int col = HALO + idx % TS, i = first + 2 * (idx / TS);
+                    float* x = t + i * TP + col;
+                    x[0] += c * (x[-TP] + x[TP]);
+                }
+                __syncthreads();
+            }
+        }
+    }
+    for (int idx = tid; idx < TS * TS; idx += IV_THREADS) {
+        const int ly = HALO + idx / TS, lx = HALO + idx % TS;
+        const int gy = y0 + ly, gx = x0 + lx;
+        if (gy >= h || gx >= w) continue;
+        if (LAST) {
+            const float y0v = smem[ly * TP + lx], y1v = smem[TW * TP + ly * TP + lx], y2v = smem[2 * TW * TP + ly * TP + lx];
+            const float v[3] = {y0v + (float)1.402 * y2v, y0v + (float)(-0.34413) * y1v + (float)(-0.71414) * y2v,
+                                y0v + (float)1.772 * y1v};
+            uint16_t* o = a.pix + ((size_t)gy * w + gx) * 3;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int code = (int)floorf(v[c] + 2048.5f);
+                o[c] = (uint16_t)(min(max(code, 0), 4095) << a.shift);
+            }
+        } else {
+            a.out[blockIdx.z * a.outComp + (size_t)gy * a.outStride + gx] = smem[ly * TP + lx];
+        }
+    }
+}
+
+// reduce == levels: the picture is the LL band as it is.
+__global__ void colorOutKernel(const float* A, uint64_t comp, int stride, int w, int h, uint16_t* pix, int shift) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t i = (size_t)y * stride + x;
+    const float y0 = A[i], y1 = A[comp + i], y2 = A[2 * comp + i];
+    const float v[3] = {y0 + (float)1.402 * y2, y0 + (float)(-0.34413) * y1 + (float)(-0.71414) * y2, y0 + (float)1.772 * y1};
+    uint16_t* o = pix + ((size_t)y * w + x) * 3;
+    for (int c = 0; c < 3; ++c) {
+        const int code = (int)floorf(v[c] + 2048.5f);
+        o[c] = (uint16_t)(min(max(code, 0), 4095) << shift);
+    }
+}
+
+constexpr size_t kInvSmemLast = (size_t)3 * TW * TP * 4;
+constexpr size_t kInvSmem = (size_t)TW * TP * 4;
+
+
+}  // namespace
+
+void decoderInit() {
+    uint8_t zc[4 * 45], sc[9];
+    uint32_t mq[47];
+    t1BuildTables(zc, sc, mq);
+    GB_CHECK(cudaMemcpyToSymbol(c_zc, zc, sizeof zc));
+    GB_CHECK(cudaMemcpyToSymbol(c_sc, sc, sizeof sc));
+    GB_CHECK(cudaMemcpyToSymbol(c_mq, mq, sizeof mq));
+    GB_CHECK(cudaFuncSetAttribute(invLevelKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmemLast));
+}
+
+uint64_t decoderSlotBytes(const Layout& L, const GailCudaDecodeSettings& s) {
+    const uint64_t npix = (uint64_t)L.width * L.height, ll = (uint64_t)L.levelW(1) * L.levelH(1);
+    const uint64_t out = (uint64_t)L.levelW(s.reduce) * L.levelH(s.reduce) * 6;
+    return npix * 12 + 2 * ll * 12 + out + (uint64_t)L.numCblks() * (12 + 12 + 4) + (4ull << 20);
+}
+
+DecoderSlot::DecoderSlot(int device, const Layout& L, const GailCudaDecodeSettings& s) : dev_(device), L_(L), s_(s) {
+    if (s.reduce < 0 || s.reduce > L.levels) throw std::runtime_error("more resolution levels left out than the stream has");
+    outW_ = L.levelW(s.reduce);
+    outH_ = L.levelH(s.reduce);
+    try {
+        GB_CHECK(cudaSetDevice(dev_));
+        GB_CHECK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+        for (auto& e : ev_) GB_CHECK(cudaEventCreate(&e));
+        const uint64_t npix = (uint64_t)L.width * L.height, ll = (uint64_t)L.levelW(1) * L.levelH(1);
+        const uint64_t n = (uint64_t)L.numCblks();
+        auto alloc = [&](auto*& p, uint64_t bytes) {
+            void* q = nullptr;
+            check(cudaMalloc(&q, std::max<uint64_t>(bytes, 16)), "device memory for a decoder slot");
+            allocs_.push_back(q);
+            p = static_cast<std::remove_reference_t<decltype(p)>>(q);
+        };
+        alloc(dPlanes_, npix * 12);
+        alloc(dLL_[0], ll * 12);
+        alloc(dLL_[1], ll * 12);
+        alloc(dHalf_, L.bands.size() * 4);
+        alloc(dCodes_, n * sizeof(GbCblkCode));
+        alloc(dBlocks_, n * sizeof(DecBlock));
+        alloc(dPerm_, n * 4);
+        alloc(dCtl_, 64);
+        alloc(dOut_, (uint64_t)outW_ * outH_ * 6);
+        check(cudaHostAlloc((void**)&hOut_, std::max<uint64_t>(16, (uint64_t)outW_ * outH_ * 6), cudaHostAllocDefault),
+              "pinned host memory");
+        check(cudaHostAlloc((void**)&hCodes_, std::max<uint64_t>(16, n * sizeof(GbCblkCode)), cudaHostAllocDefault),
+              "pinned host memory");
+        check(cudaHostAlloc((void**)&hHalf_, L.bands.size() * 4 + 16, cudaHostAllocDefault), "pinned host memory");
+        check(cudaHostAlloc((void**)&hCtl_, 64, cudaHostAllocDefault), "pinned host memory");
+        capBytes_ = 1500000;
+        alloc(dBytes_, capBytes_);
+        check(cudaHostAlloc((void**)&hBytes_, capBytes_, cudaHostAllocDefault), "pinned host memory");
+        std::vector<DecBlock> blocks(n);
+        const int maxRes = L.levels - s.reduce;
+        for (uint64_t i = 0; i < n; ++i) {
+            const CodeBlock& cb = L.cblks[i];
+            const GbSubband& b = L.bands[cb.band];
+            blocks[i] = {(uint32_t)((uint64_t)b.comp * npix + (uint64_t)(b.py0 + cb.y0) * L.width + b.px0 + cb.x0),
+                         (uint16_t)cb.w, (uint16_t)cb.h, (uint8_t)b.orient, (uint8_t)cb.band,
+                         (uint8_t)(b.res <= maxRes ? 1 : 0), 0};
+        }
+        GB_CHECK(cudaMemcpy(dBlocks_, blocks.data(), n * sizeof(DecBlock), cudaMemcpyHostToDevice));
+    } catch (...) {
+        release();
+        throw;
+    }
+}
+
+DecoderSlot::~DecoderSlot() { release(); }
+
+void DecoderSlot::release() {
+    cudaSetDevice(dev_);
+    if (st_) cudaStreamSynchronize(st_);
+    for (void* p : allocs_) cudaFree(p);
+    allocs_.clear();
+    for (void* p : {(void*)hOut_, (void*)hCodes_, (void*)hHalf_, (void*)hCtl_, (void*)hBytes_})
+        if (p) cudaFreeHost(p);
+    hOut_ = nullptr;
+    hCodes_ = nullptr;
+    hHalf_ = nullptr;
+    hCtl_ = nullptr;
+    hBytes_ = nullptr;
+    for (auto& e : ev_)
+        if (e) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
+    if (st_) cudaStreamDestroy(st_);
+    st_ = nullptr;
+    cudaGetLastError();
+}
+
+void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, const GbCblkCode* blocks, size_t numBlocks,
+                         void* dst, ptrdiff_t strideBytes, GailCudaDecodeTimings* tm) {
+    const auto t0 = std::chrono::steady_clock::now();
+    if (frame.width != L_.width || frame.height != L_.height || frame.levels != L_.levels ||
+        frame.bands.size() != L_.bands.size() || (int)numBlocks != L_.numCblks())
+        throw std::logic_error("frame does not match the layout the slot was made for");
+    if (size > 0xFFFFFFFFull) throw std::runtime_error("codestream too large");
+    GB_CHECK(cudaSetDevice(dev_));
+    const cudaStream_t st = st_;
+    const uint64_t npix = (uint64_t)L_.width * L_.height, n = numBlocks;
+    if (size > capBytes_) {
+        cudaStreamSynchronize(st);
+        cudaFree(dBytes_);
+        allocs_.erase(std::find(allocs_.begin(), allocs_.end(), (void*)dBytes_));
+        cudaFreeHost(hBytes_);
+        dBytes_ = nullptr;
+        hBytes_ = nullptr;
+        capBytes_ = size + size / 2;
+        void* q = nullptr;
+        check(cudaMalloc(&q, capBytes_), "device memory for a decoder slot");
+        dBytes_ = (uint8_t*)q;
+        allocs_.push_back(q);
+        check(cudaHostAlloc((void**)&hBytes_, capBytes_, cudaHostAllocDefault), "pinned host memory");
+    }
+    std::memcpy(hBytes_, data, size);
+    std::memcpy(hCodes_, blocks, n * sizeof(GbCblkCode));
+    for (size_t i = 0; i < frame.bands.size(); ++i) hHalf_[i] = 0.5f * frame.bands[i].delta;
+    const bool wantWavelet = tm && tm->wantWavelet;
+
+    GB_CHECK(cudaEventRecord(ev_[0], st));
+    GB_CHECK(cudaMemcpyAsync(dBytes_, hBytes_, size, cudaMemcpyHostToDevice, st));
+    GB_CHECK(cudaMemcpyAsync(dCodes_, hCodes_, n * sizeof(GbCblkCode), cudaMemcpyHostToDevice, st));
+    GB_CHECK(cudaMemcpyAsync(dHalf_, hHalf_, frame.bands.size() * 4, cudaMemcpyHostToDevice, st));
+    GB_CHECK(cudaMemsetAsync(dCtl_, 0, 64, st));
+    if (wantWavelet) GB_CHECK(cudaMemsetAsync(dPlanes_, 0, npix * 12, st));
+    DecArgs da{dBytes_, size, dCodes_, dBlocks_, (uint32_t)n, dHalf_, (uint32_t*)dPlanes_, (uint32_t)L_.width, dPerm_, dCtl_};
+    orderKernel<<<1, 1024, 0, st>>>(da);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_);
+    decodeKernel<<<std::min<uint32_t>(divUp((uint32_t)n, DEC_THREADS), (uint32_t)sms * 16), DEC_THREADS, 0, st>>>(da);
+    GB_CHECK(cudaGetLastError());
+    GB_CHECK(cudaEventRecord(ev_[1], st));
+    if (wantWavelet) {
+        GB_CHECK(cudaStreamSynchronize(st));
+        for (int c = 0; c < 3; ++c) {
+            wavelet_[c].resize(npix);
+            GB_CHECK(cudaMemcpy(wavelet_[c].data(), dPlanes_ + c * npix, npix * 4, cudaMemcpyDeviceToHost));
+        }
+    }
+    // inverse wavelet, levels top down; the last one writes the picture
+    const int stop = s_.reduce;
+    const int llStride = L_.levelW(1);
+    const uint64_t llComp = (uint64_t)L_.levelW(1) * L_.levelH(1);
+    const int shift = s_.highBits ? 4 : 0;
+    if (stop == L_.levels) {
+        colorOutKernel<<<dim3(divUp(outW_, 256), outH_), 256, 0, st>>>(dPlanes_, npix, L_.width, outW_, outH_, dOut_, shift);
+    }
+    for (int l = L_.levels; l > stop; --l) {
+        InvArgs a{};
+        a.w = L_.levelW(l - 1);
+        a.h = L_.levelH(l - 1);
+        a.snx = L_.levelW(l);
+        a.sny = L_.levelH(l);
+        a.A = dPlanes_;
+        a.aComp = npix;
+        a.aStride = L_.width;
+        a.ll = l == L_.levels ? nullptr : dLL_[l & 1];
+        a.llComp = llComp;
+        a.llStride = llStride;
+        const bool last = l - 1 == stop;
+        a.out = last ? nullptr : dLL_[(l - 1) & 1];
+        a.outComp = llComp;
+        a.outStride = llStride;
+        a.pix = dOut_;
+        a.shift = shift;
+        if (last)
+            invLevelKernel<true><<<dim3(divUp(a.w, TS), divUp(a.h, TS), 1), IV_THREADS, kInvSmemLast, st>>>(a);
+        else
+            invLevelKernel<false><<<dim3(divUp(a.w, TS), divUp(a.h, TS), 3), IV_THREADS, kInvSmem, st>>>(a);
+    }
+    GB_CHECK(cudaGetLastError());
+    GB_CHECK(cudaEventRecord(ev_[2], st));
+    const uint64_t outBytes = (uint64_t)outW_ * outH_ * 6;
+    GB_CHECK(cudaMemcpyAsync(hOut_, dOut_, outBytes, cudaMemcpyDeviceToHost, st));
+    GB_CHECK(cudaMemcpyAsync(hCtl_, dCtl_, 64, cudaMemcpyDeviceToHost, st));
+    GB_CHECK(cudaEventRecord(ev_[3], st));
+    GB_CHECK(cudaStreamSynchronize(st));
+    GB_CHECK(cudaGetLastError());
+    const uint64_t rowBytes = (uint64_t)outW_ * 6;
+    if (strideBytes == (ptrdiff_t)rowBytes) {
+        std::memcpy(dst, hOut_, outBytes);
+    } else {
+        for (int y = 0; y < outH_; ++y)
+            std::memcpy((uint8_t*)dst + (ptrdiff_t)y * strideBytes, (const uint8_t*)hOut_ + (uint64_t)y * rowBytes, rowBytes);
+    }
+    if (tm) {
+        float a = 0, b = 0, c = 0;
+        cudaEventElapsedTime(&a, ev_[0], ev_[1]);
+        cudaEventElapsedTime(&b, ev_[1], ev_[2]);
+        cudaEventElapsedTime(&c, ev_[2], ev_[3]);
+        tm->t1 = a;
+        tm->dwt = b;
+        tm->color = c;
+        tm->total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        tm->numWavelet = wantWavelet ? npix : 0;
+        for (int k = 0; k < 3; ++k) tm->wavelet[k] = wantWavelet ? wavelet_[k].data() : nullptr;
+    }
+}
+
+}  // namespace gb

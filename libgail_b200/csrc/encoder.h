@@ -1,0 +1,83 @@
+// One frame in flight on the device: the plain per-frame encode path behind the
+// plugin's encoder_* entry points (the role of the reference's CudaSlot,
+// Josephur/libgail src/cuda/cuda_backend.cu:778-1008): upload, front end, Tier-1,
+// compaction, download.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "color.h"
+#include "compact.cuh"
+#include "gail_cuda_plugin_abi.h"
+#include "layout.h"
+#include "t1_encode.cuh"
+
+namespace gb {
+
+// Device memory of one slot, in allocation order (also what encoder_bytes reports).
+struct SlotSizes {
+    uint64_t npix = 0, n = 0, inBytes = 0, arena = 0, llFloats = 0;
+    uint64_t deviceBytes() const;
+};
+SlotSizes slotSizes(const Layout& L, const GbFrameFormat& in);
+
+// The Tier-1 job table of a layout: per block its coefficient block, its symbol/codeword
+// region (sized for Mb bit-planes) and geometry; returns the arena size.
+uint64_t buildJobs(const Layout& L, int frame, uint32_t coeffBase, uint64_t regionBase, std::vector<T1Job>& jobs);
+
+class EncoderSlot {
+public:
+    EncoderSlot(int device, const Layout& L, const GailCudaEncodeSettings& s);
+    ~EncoderSlot();
+    EncoderSlot(const EncoderSlot&) = delete;
+    EncoderSlot& operator=(const EncoderSlot&) = delete;
+
+    void* inputBuffer() { return hIn_; }
+    void setSlope(double t) { slope_ = (float)t; }
+    // The plain path: frame (host memory) in, Tier-1 frame (this slot's pinned memory) out.
+    void encode(const void* frame, GailCudaTier1* out, GbFrameTimings* tm, GailCudaDebug* dbg);
+
+    const Layout& layout() const { return L_; }
+
+private:
+    void release();
+    void uploadStatic();
+
+    int dev_;
+    Layout L_;
+    GailCudaEncodeSettings s_;
+    SlotSizes z_;
+    float slope_ = 0.f;
+    cudaStream_t st_ = nullptr;
+    cudaEvent_t ev_[5] = {};
+    std::vector<void*> dev_allocs_;
+    std::vector<T1Job> jobs_;
+
+    // device
+    void* dIn_ = nullptr;
+    float *dEotf_ = nullptr, *dThr_ = nullptr, *dLL_[2] = {nullptr, nullptr}, *dSlope_ = nullptr, *dTap_ = nullptr;
+    uint32_t *dCoeffs_ = nullptr, *dInfo_ = nullptr, *dEnd_ = nullptr, *dLen_ = nullptr, *dPerm_ = nullptr,
+             *dCtl_ = nullptr, *dOutInfo_ = nullptr, *dOutLen_ = nullptr;
+    int32_t *dDist_ = nullptr, *dOutDist_ = nullptr;
+    uint4* dSnaps_ = nullptr;
+    uint8_t *dSym_ = nullptr, *dCw_ = nullptr, *dOutData_ = nullptr;
+    uint16_t* dXyz_ = nullptr;
+    T1Job* dJobs_ = nullptr;
+    ColorTables color_;
+    float m_[9];
+    // host (pinned)
+    void* hIn_ = nullptr;
+    uint32_t *hInfo_ = nullptr, *hLen_ = nullptr, *hSmall_ = nullptr;
+    int32_t* hDist_ = nullptr;
+    uint8_t* hData_ = nullptr;
+    uint64_t hDataCap_ = 0;
+    float* hSlope_ = nullptr;
+    // debug taps
+    std::vector<uint16_t> xyz_;
+    std::vector<uint32_t> coeffs_;
+    std::vector<float> wavelet_;
+};
+
+}  // namespace gb

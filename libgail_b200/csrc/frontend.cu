@@ -1,0 +1,275 @@
+// Encoder front end: colour -> 9/7 DWT -> dead-zone quantisation, one kernel per level.
+//
+// Each CTA owns a 64 x 64 tile of the level's input and loads it with a 4-sample halo
+// (72 x 72, whole-sample symmetric mirror at the image edges) into shared memory, lifts
+// the columns, then the rows (the order of the reference, Annex F.4.2), and writes the
+// four 32 x 32 subband pieces it produced. Because tiles are 64-aligned, each piece is
+// exactly one code-block of its band, so the high bands (and the LL band at the last
+// level) are quantised in registers and stored straight into the code-block-major
+// layout Tier-1 reads: 32 consecutive words per row, zero outside the band. The LL piece
+// of an intermediate level goes to a float plane for the next level.
+//
+// Level 1 also does the colour conversion in its tile loads (the frame is read once,
+// never written back as planes): R'G'B' from interleaved 16-bit or planar Y'CbCr,
+// EOTF lookup, 3x3 to XYZ, the 12-bit DCI encoding by binary search over 4096 host-built
+// thresholds in shared memory (no pow on the device), DC shift and forward ICT.
+//
+// Float arithmetic is compiled without contraction and written in the reference's
+// operation order (Josephur/libgail core/dwt_cpu.cpp:24-93, core/color.cpp:142-189,
+// kernels/color_math.h:109-179, core/quant.h:20-25), so coefficients are bit-identical
+// to the CPU path's.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "frontend.cuh"
+
+namespace gb {
+
+namespace {
+
+constexpr int TS = 64, HALO = 4, TW = TS + 2 * HALO, TP = TW + 1;
+constexpr int FE_THREADS = 256;
+__constant__ float kLiftF[4] = {(float)-1.586134342059924, (float)-0.052980118572961, (float)0.882911075530934,
+                             (float)0.443506852043971};
+constexpr float kLowScale = (float)(1.0 / 1.230174104914001);
+constexpr float kHighScale = (float)1.230174104914001;
+
+__device__ __forceinline__ int mirror(int i, int n) {
+    if (n == 1) return 0;
+    const int period = 2 * (n - 1);
+    i %= period;
+    if (i < 0) i += period;
+    return i < n ? i : period - i;
+}
+
+__device__ __forceinline__ uint32_t quantize(float v, float inv, uint32_t maxMag) {
+    const float a = fabsf(v);
+    const float q = a * inv * 64.0f;
+    const uint32_t m = q >= (float)maxMag ? maxMag : (uint32_t)q;
+    return m | ((v < 0.f && m >= 64u) ? 0x80000000u : 0u);
+}
+
+__device__ __forceinline__ float sampleAt(const void* src, int bits, size_t i) {
+    return bits > 8 ? (float)((const uint16_t*)src)[i] : (float)((const uint8_t*)src)[i];
+}
+
+__device__ __forceinline__ uint32_t round16(float v) {
+    const int r = (int)v;
+    return (uint32_t)(r + ((v - (float)r) >= 0.5f ? 1 : 0));
+}
+
+__device__ __forceinline__ float clamp01(float v) { return fminf(fmaxf(v, 0.f), 1.f); }
+
+// R'G'B' 16-bit codes of container pixel (x, y) of a planar frame (black outside the
+// active picture).
+__device__ void planarRgb(const void* src, const PlanarParams& p, int x, int y, uint32_t rgb[3]) {
+    const int ax = x - p.ox, ay = y - p.oy;
+    if (ax < 0 || ay < 0 || ax >= p.aw || ay >= p.ah) {
+        rgb[0] = rgb[1] = rgb[2] = 0;
+        return;
+    }
+    float cyp = !p.sy ? (float)ay : p.chroma == 2 ? ay * 0.5f : (ay - 0.5f) * 0.5f;
+    cyp = fminf(fmaxf(cyp, 0.f), (float)(p.ch - 1));
+    const int y0 = (int)cyp, y1 = min(y0 + 1, p.ch - 1);
+    const float fy = cyp - y0;
+    float cxp = !p.sx ? (float)ax : p.chroma == 1 ? (ax - 0.5f) * 0.5f : ax * 0.5f;
+    cxp = fminf(fmaxf(cxp, 0.f), (float)(p.cw - 1));
+    const int x0 = (int)cxp, x1 = min(x0 + 1, p.cw - 1);
+    const float fx = cxp - x0;
+    const size_t uOff = (size_t)p.aw * p.ah, vOff = uOff + (size_t)p.cw * p.ch;
+    float uv[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const size_t off = k ? vOff : uOff;
+        const float a = sampleAt(src, p.bits, off + (size_t)y0 * p.cw + x0);
+        const float b = sampleAt(src, p.bits, off + (size_t)y0 * p.cw + x1);
+        const float c = sampleAt(src, p.bits, off + (size_t)y1 * p.cw + x0);
+        const float d = sampleAt(src, p.bits, off + (size_t)y1 * p.cw + x1);
+        uv[k] = (a * (1 - fx) + b * fx) * (1 - fy) + (c * (1 - fx) + d * fx) * fy;
+    }
+    float Y = sampleAt(src, p.bits, (size_t)ay * p.aw + ax), U = uv[0], V = uv[1];
+    float v[3];
+    if (p.rgb) {  // planes G', B', R'
+        v[0] = V / p.maxv;
+        v[1] = Y / p.maxv;
+        v[2] = U / p.maxv;
+    } else {
+        if (p.fullRange) {
+            Y /= p.maxv;
+            U = (U - 128.f * p.scale) / p.maxv;
+            V = (V - 128.f * p.scale) / p.maxv;
+        } else {
+            Y = (Y - 16.f * p.scale) / (219.f * p.scale);
+            U = (U - 128.f * p.scale) / (224.f * p.scale);
+            V = (V - 128.f * p.scale) / (224.f * p.scale);
+        }
+        v[0] = Y + p.crR * V;
+        v[1] = Y - p.cbG * U - p.crG * V;
+        v[2] = Y + p.cbB * U;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) rgb[c] = round16(clamp01(v[c]) * 65535.f);
+}
+
+// 12-bit code: the number of thresholds at or below n (thr[0] = 0).
+__device__ __forceinline__ int dciCode(const float* thr, float n) {
+    int k = 0;
+#pragma unroll
+    for (int step = 2048; step > 0; step >>= 1)
+        if (k + step <= 4095 && thr[k + step] <= n) k += step;
+    return k;
+}
+
+__device__ __forceinline__ int eotfIndex(uint32_t code16) {
+    const float v = code16 / 65535.f;
+    return (int)floorf(clamp01(v) * 65535.0f + 0.5f);
+}
+
+// Lifting steps along columns (rows of the tile) of one component, then the scaling.
+__device__ void liftColumns(float* t, int tid) {
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+        const int first = (s & 1) ? 2 : 1;  // alpha, gamma: odd samples; beta, delta: even
+        const float c = kLiftF[s];
+        for (int idx = tid; idx < TW * 35; idx += FE_THREADS) {
+            const int col = idx % TW, i = first + 2 * (idx / TW);
+            float* x = t + i * TP + col;
+            x[0] += c * (x[-TP] + x[TP]);
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < TS * TW; idx += FE_THREADS) {
+        const int col = idx % TW, r = HALO + idx / TW;
+        t[r * TP + col] *= (r & 1) ? kHighScale : kLowScale;
+    }
+    __syncthreads();
+}
+
+// Lifting along rows for the rows that produce output, then the scaling.
+__device__ void liftRows(float* t, int tid) {
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+        const int first = (s & 1) ? 2 : 1;
+        const float c = kLiftF[s];
+        for (int idx = tid; idx < TS * 35; idx += FE_THREADS) {
+            const int r = HALO + idx % TS, i = first + 2 * (idx / TS);
+            float* x = t + r * TP + i;
+            x[0] += c * (x[-1] + x[1]);
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < TS * TS; idx += FE_THREADS) {
+        const int r = HALO + idx % TS, col = HALO + idx / TS;
+        t[r * TP + col] *= (col & 1) ? kHighScale : kLowScale;
+    }
+    __syncthreads();
+}
+
+// The tile's outputs for component comp: its code-block of each band (and LL floats).
+__device__ void writeOutputs(const LevelArgs& a, const float* t, int comp, int tx, int ty, int tid) {
+    const int x0 = tx * TS - HALO, y0 = ty * TS - HALO;
+    for (int o = 0; o < 4; ++o) {
+        const BandOut& b = a.band[comp][o];
+        const bool quant = o != 0 || a.last;
+        if (tx >= b.ncbx || ty >= b.ncby) continue;
+        uint32_t* blk = a.coeffs + ((size_t)b.cblkBase + (size_t)ty * b.ncbx + tx) * kCblkArea;
+        for (int idx = tid; idx < kCblkArea; idx += FE_THREADS) {
+            const int i = idx & 31, j = idx >> 5;
+            const int bx = tx * 32 + i, by = ty * 32 + j;
+            const bool in = bx < b.w && by < b.h;
+            float v = 0.f;
+            if (in) {
+                const int gx = 2 * bx + (o & 1), gy = 2 * by + (o >> 1);
+                v = t[(gy - y0) * TP + (gx - x0)];
+            }
+            if (quant) {
+                blk[idx] = in ? quantize(v, b.invDelta, b.maxMag) : 0u;
+                if (in && a.tap) a.tap[comp * a.tapComp + (size_t)(b.py0 + by) * a.tapStride + b.px0 + bx] = v;
+            } else if (in) {
+                a.ll[comp * a.llComp + (size_t)by * a.llStride + bx] = v;
+            }
+        }
+    }
+}
+
+template <bool COLOR>
+__global__ void __launch_bounds__(FE_THREADS) levelKernel(ColorArgs c, LevelArgs a) {
+    extern __shared__ float smem[];
+    constexpr int NC = COLOR ? 3 : 1;
+    float* thr = smem + NC * TW * TP;
+    const int tid = threadIdx.x, tx = blockIdx.x, ty = blockIdx.y;
+    const int x0 = tx * TS - HALO, y0 = ty * TS - HALO;
+    const int w = a.w, h = a.h;
+    if (COLOR) {
+        for (int i = tid; i < 4096; i += FE_THREADS) thr[i] = c.thr[i];
+        __syncthreads();
+        for (int idx = tid; idx < TW * TW; idx += FE_THREADS) {
+            const int ly = idx / TW, lx = idx % TW;
+            const int gy = mirror(y0 + ly, h), gx = mirror(x0 + lx, w);
+            uint32_t rgb[3];
+            if (c.kind == 0) {
+                const uint16_t* p = (const uint16_t*)c.src + ((size_t)gy * w + gx) * 3;
+                rgb[0] = p[0];
+                rgb[1] = p[1];
+                rgb[2] = p[2];
+            } else {
+                planarRgb(c.src, c.pp, gx, gy, rgb);
+            }
+            const float R = c.eotf[eotfIndex(rgb[0])], G = c.eotf[eotfIndex(rgb[1])], B = c.eotf[eotfIndex(rgb[2])];
+            const float X = c.m[0] * R + c.m[1] * G + c.m[2] * B;
+            const float Yv = c.m[3] * R + c.m[4] * G + c.m[5] * B;
+            const float Z = c.m[6] * R + c.m[7] * G + c.m[8] * B;
+            const int cx = dciCode(thr, clamp01(X / 52.37f));
+            const int cy = dciCode(thr, clamp01(Yv / 52.37f));
+            const int cz = dciCode(thr, clamp01(Z / 52.37f));
+            if (c.xyz && lx >= HALO && lx < HALO + TS && ly >= HALO && ly < HALO + TS && x0 + lx < w && y0 + ly < h) {
+                uint16_t* o = c.xyz + ((size_t)(y0 + ly) * w + (x0 + lx)) * 3;
+                o[0] = (uint16_t)cx;
+                o[1] = (uint16_t)cy;
+                o[2] = (uint16_t)cz;
+            }
+            const float fx = (float)(cx - 2048), fy = (float)(cy - 2048), fz = (float)(cz - 2048);
+            smem[0 * TW * TP + ly * TP + lx] = (float)0.299 * fx + (float)0.587 * fy + (float)0.114 * fz;
+            smem[1 * TW * TP + ly * TP + lx] = (float)(-0.16875) * fx + (float)(-0.33126) * fy + (float)0.5 * fz;
+            smem[2 * TW * TP + ly * TP + lx] = (float)0.5 * fx + (float)(-0.41869) * fy + (float)(-0.08131) * fz;
+        }
+    } else {
+        const int comp = blockIdx.z;
+        const float* src = a.src + comp * a.srcComp;
+        for (int idx = tid; idx < TW * TW; idx += FE_THREADS) {
+            const int ly = idx / TW, lx = idx % TW;
+            smem[ly * TP + lx] = src[(size_t)mirror(y0 + ly, h) * a.srcStride + mirror(x0 + lx, w)];
+        }
+    }
+    __syncthreads();
+    for (int k = 0; k < NC; ++k) {
+        float* t = smem + k * TW * TP;
+        if (h >= 2) liftColumns(t, tid);
+        if (w >= 2) liftRows(t, tid);
+        writeOutputs(a, t, COLOR ? k : (int)blockIdx.z, tx, ty, tid);
+    }
+}
+
+constexpr size_t kSmemColor = (size_t)3 * TW * TP * 4 + 4096 * 4;
+constexpr size_t kSmemPlain = (size_t)TW * TP * 4;
+
+}  // namespace
+
+void frontendInit() {
+    GB_CHECK(cudaFuncSetAttribute(levelKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemColor));
+    GB_CHECK(cudaFuncSetAttribute(levelKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemPlain));
+}
+
+void launchLevel1(const ColorArgs& c, const LevelArgs& a, cudaStream_t st) {
+    const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 1);
+    levelKernel<true><<<grid, FE_THREADS, kSmemColor, st>>>(c, a);
+    GB_CHECK(cudaGetLastError());
+}
+
+void launchLevel(const LevelArgs& a, cudaStream_t st) {
+    const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 3);
+    levelKernel<false><<<grid, FE_THREADS, kSmemPlain, st>>>(ColorArgs{}, a);
+    GB_CHECK(cudaGetLastError());
+}
+
+}  // namespace gb

@@ -33,6 +33,7 @@
 
 #include "common.cuh"
 #include "t1_encode.cuh"
+#include "capi_util.h"
 #include "t1_tables.h"
 
 namespace gb {
@@ -618,6 +619,11 @@ __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
 }
 
 }  // namespace
+
+cudaError_t kernelsLoadable() {
+    cudaFuncAttributes attr;
+    return cudaFuncGetAttributes(&attr, t1OrderKernel);
+}
 
 void t1Init() {
     uint8_t zc[4 * 45], sc[9];

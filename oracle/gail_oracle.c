@@ -1089,3 +1089,49 @@ void or_ict_inverse_pack(float y0, float y1, float y2, int shift, uint16_t out[3
         out[k] = (uint16_t)(code << shift);
     }
 }
+
+/* ==================================================================================
+ * Batch helpers for the tests (loops over the functions above).
+ * ================================================================================== */
+int or_t1_encode_many(const uint32_t* coeffs, const int32_t* geom4, uint32_t n, float slope, const float* dscale,
+                      uint32_t* info4, uint32_t* pass_len, int32_t* pass_dist, uint8_t* data, uint32_t stride) {
+    static uint8_t buf[OR_CBLK_AREA * 4 * 24 + 64];
+    for (uint32_t i = 0; i < n; ++i) {
+        or_t1_result r;
+        const int32_t* g = geom4 + 4 * i;
+        if (or_t1_encode(coeffs + (size_t)i * OR_CBLK_AREA, g[0], g[1], g[2], g[3], slope, dscale ? dscale[i] : 1.f, buf,
+                         sizeof buf, &r) != 0)
+            return -1;
+        if (r.data_len > stride) return -2;
+        info4[4 * i] = (uint32_t)r.nbps;
+        info4[4 * i + 1] = (uint32_t)r.num_passes;
+        info4[4 * i + 2] = r.num_symbols;
+        info4[4 * i + 3] = r.data_len;
+        memcpy(pass_len + (size_t)i * 64, r.pass_len, sizeof r.pass_len);
+        memcpy(pass_dist + (size_t)i * 64, r.pass_dist, sizeof r.pass_dist);
+        memcpy(data + (size_t)i * stride, buf, r.data_len);
+    }
+    return 0;
+}
+
+/* Dead-zone quantisation of Mallat planes into code-block-major words
+ * (quantizeCodeBlock, core/quant.cpp:8-20). */
+void or_quantize_frame(const float* planes, int width, int height, const or_band* bands, const or_cblk* cblks, int nc,
+                       uint32_t* out) {
+    const size_t npix = (size_t)width * height;
+    for (int i = 0; i < nc; ++i) {
+        const or_cblk* k = &cblks[i];
+        const or_band* b = &bands[k->band];
+        const float* plane = planes + (size_t)b->comp * npix;
+        const float inv = 1.0f / b->delta;
+        const uint32_t max_mag = ((1u << b->mb) << OR_FRAC_BITS) - 1u;
+        uint32_t* o = out + (size_t)i * OR_CBLK_AREA;
+        memset(o, 0, OR_CBLK_AREA * 4);
+        for (int y = 0; y < k->h; ++y)
+            for (int x = 0; x < k->w; ++x)
+                o[y * OR_CBLK + x] = or_quantize(plane[(size_t)(b->py0 + k->y0 + y) * width + b->px0 + k->x0 + x], inv, max_mag);
+    }
+}
+
+/* The 12-bit code of X / 52.37 = n (cm_encode's arithmetic, color_math.h:109-112). */
+int or_dci_code(float n) { return (int)floorf(4095.0f * powf(n, 1.0f / 2.6f) + 0.5f); }

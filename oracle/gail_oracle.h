@@ -107,6 +107,15 @@ void or_t1_decode(const uint8_t* data, uint32_t len, int w, int h, int orient, i
 /* Inverse ICT + level shift + 12-bit clamp of one sample triple (cpu_decode_backend.cpp:77-91). */
 void or_ict_inverse_pack(float y0, float y1, float y2, int shift, uint16_t out[3]);
 
+/* Batch forms for the tests: or_t1_encode over n blocks (same arguments as the
+ * library's gb_t1_encode_blocks), quantisation of whole Mallat planes into
+ * code-block-major words, and the 12-bit encoding of one normalised value. */
+int or_t1_encode_many(const uint32_t* coeffs, const int32_t* geom4, uint32_t n, float slope, const float* dscale,
+                      uint32_t* info4, uint32_t* pass_len, int32_t* pass_dist, uint8_t* data, uint32_t stride);
+void or_quantize_frame(const float* planes, int width, int height, const or_band* bands, const or_cblk* cblks, int nc,
+                       uint32_t* out);
+int or_dci_code(float n);
+
 /* 12-bit code -> 16-bit signal as the public API fills X'Y'Z' frames (gail_api.cpp:389-394). */
 uint16_t or_xyz12_to_16(uint32_t v);
 

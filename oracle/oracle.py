@@ -100,12 +100,45 @@ class Oracle(_Common):
         L.or_planar_to_rgb48.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.or_t1_decode.argtypes = [C.c_void_p, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.or_ict_inverse_pack.argtypes = [C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]
+        L.or_t1_encode_many.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+        L.or_quantize_frame.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        L.or_dci_code.argtypes = [C.c_float]
+        L.or_dci_code.restype = C.c_int
 
     def t1_encode(self, coeffs, w, h, orient, max_passes=64, slope=0.0, dist_scale=1.0) -> T1Block:
         return self._t1(self.lib.or_t1_encode, coeffs, w, h, orient, max_passes, slope, dist_scale)
 
     def quantize(self, v, inv_delta, max_mag):
         return self.lib.or_quantize(C.c_float(v), C.c_float(inv_delta), max_mag)
+
+    def t1_encode_many(self, coeffs, geom4, slope=0.0, dist_scale=None, stride=65536):
+        """or_t1_encode over n blocks: (info4, pass_len, pass_dist, codewords)."""
+        c = np.ascontiguousarray(coeffs, np.uint32).reshape(-1, 1024)
+        g = np.ascontiguousarray(geom4, np.int32).reshape(-1, 4)
+        n = c.shape[0]
+        ds = None if dist_scale is None else np.ascontiguousarray(dist_scale, np.float32)
+        info = np.zeros((n, 4), np.uint32)
+        plen = np.zeros((n, 64), np.uint32)
+        pdist = np.zeros((n, 64), np.int32)
+        data = np.zeros((n, stride), np.uint8)
+        rc = self.lib.or_t1_encode_many(_p(c), _p(g), n, C.c_float(slope), None if ds is None else _p(ds), _p(info),
+                                        _p(plen), _p(pdist), _p(data), stride)
+        if rc != 0:
+            raise RuntimeError(f"oracle Tier-1 failed ({rc})")
+        return info, plen, pdist, [bytes(data[i, : info[i, 3]]) for i in range(n)]
+
+    def quantize_frame(self, planes: np.ndarray, bands, cblks) -> np.ndarray:
+        p = np.ascontiguousarray(planes, np.float32)
+        _, h, w = p.shape
+        b = (OrBand * len(bands))(*bands)
+        k = (OrCblk * len(cblks))(*cblks)
+        out = np.zeros((len(cblks), 1024), np.uint32)
+        self.lib.or_quantize_frame(_p(p), w, h, b, k, len(cblks), _p(out))
+        return out
+
+    def dci_code(self, n: float) -> int:
+        return self.lib.or_dci_code(C.c_float(n))
 
     def fdwt(self, plane: np.ndarray, levels: int) -> np.ndarray:
         p = np.ascontiguousarray(plane, dtype=np.float32).copy()
@@ -256,3 +289,134 @@ class Reference(_Common):
 
 def have_reference() -> bool:
     return os.path.exists(REF_SO)
+
+
+class RefEncOut(C.Structure):
+    _fields_ = [("info", C.POINTER(C.c_uint32)), ("passLen", C.POINTER(C.c_uint32)), ("passDist", C.POINTER(C.c_int32)),
+                ("data", C.POINTER(C.c_uint8)), ("numInfo", C.c_uint64), ("numPasses", C.c_uint64),
+                ("numData", C.c_uint64), ("xyz12", C.POINTER(C.c_uint16)), ("coeffs", C.POINTER(C.c_uint32)),
+                ("ms", C.c_double)]
+
+
+class RefTier1:
+    """A copy of the reference CPU encoder's Tier1Frame."""
+
+    def __init__(self, o: RefEncOut):
+        n, npass, nd = o.numInfo, o.numPasses, o.numData
+        self.info = np.ctypeslib.as_array(o.info, (n * 5,)).reshape(n, 5).copy()
+        self.pass_len = np.ctypeslib.as_array(o.passLen, (npass,)).copy() if npass else np.zeros(0, np.uint32)
+        self.pass_dist = np.ctypeslib.as_array(o.passDist, (npass,)).copy() if npass else np.zeros(0, np.int32)
+        self.data = np.ctypeslib.as_array(o.data, (nd,)).copy() if nd else np.zeros(0, np.uint8)
+        self.ms = o.ms
+
+
+def _ref_bind(L):
+    L.ref_encoder_create.restype = C.c_void_p
+    L.ref_encoder_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, C.c_void_p,
+                                     C.c_int]
+    L.ref_encoder_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.POINTER(RefEncOut)]
+    L.ref_encoder_destroy.argtypes = [C.c_void_p]
+    L.ref_rate_and_build.restype = C.c_longlong
+    L.ref_rate_and_build.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_uint64, C.c_void_p,
+                                     C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_double, C.c_double,
+                                     C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double)]
+    L.ref_build.restype = C.c_longlong
+    L.ref_build.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                            C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64]
+    L.ref_check_dci.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_char_p, C.c_uint64]
+    L.ref_parse.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_int),
+                            C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.ref_decode.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_longlong, C.c_void_p,
+                             C.POINTER(C.c_double)]
+    L.ref_empty_codestream_bytes.restype = C.c_longlong
+    L.ref_empty_codestream_bytes.argtypes = [C.c_int, C.c_int, C.c_int]
+    L.ref_dci_limits.argtypes = [C.c_double, C.c_double, C.c_double, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+
+
+CBLK_CODE = np.dtype({"names": ["offset", "len", "passes", "nbps"], "formats": [np.uint32, np.uint32, np.uint8, np.uint8],
+                      "offsets": [0, 4, 8, 9], "itemsize": 12})
+
+
+class RefEncoder:
+    """The reference CPU encoder (CpuSlot through createCpuDevice) on one frame format."""
+
+    def __init__(self, ref: "Reference", width, height, fourk, transfer=5, primaries=4, sdr_white=48.0,
+                 planar: Planar = None, threads=0, base_step=1.0):
+        self.ref = ref
+        _ref_bind(ref.lib)
+        self.h = ref.lib.ref_encoder_create(width, height, int(fourk), C.c_double(base_step), transfer, primaries,
+                                            C.c_double(sdr_white), C.byref(planar) if planar is not None else None,
+                                            threads)
+        if not self.h:
+            raise RuntimeError(ref.error())
+        self.width, self.height, self.fourk = width, height, fourk
+
+    def encode(self, frame: np.ndarray, slope=0.0, debug=False) -> RefTier1:
+        o = RefEncOut()
+        f = np.ascontiguousarray(frame)
+        if self.ref.lib.ref_encoder_encode(self.h, _p(f), C.c_double(slope), int(debug), C.byref(o)) != 0:
+            raise RuntimeError(self.ref.error())
+        t = RefTier1(o)
+        if debug:
+            t.xyz12 = np.ctypeslib.as_array(o.xyz12, (self.width * self.height * 3,)).copy()
+            t.coeffs = np.ctypeslib.as_array(o.coeffs, (t.info.shape[0] * 1024,)).copy()
+        return t
+
+    def close(self):
+        if self.h:
+            self.ref.lib.ref_encoder_destroy(self.h)
+            self.h = None
+
+
+def ref_codestream(ref: "Reference", width, height, fourk, t1, fps=24.0, mbps=230.0, tag=b"", base_step=1.0):
+    """allocateRate + buildCodestream on a Tier-1 frame (info (n, 5), pass arrays, data)."""
+    _ref_bind(ref.lib)
+    info = np.ascontiguousarray(t1.info, np.uint32)
+    n = info.shape[0]
+    pl = np.ascontiguousarray(t1.pass_len, np.uint32)
+    pd = np.ascontiguousarray(t1.pass_dist, np.int32)
+    data = np.ascontiguousarray(t1.data, np.uint8)
+    passes = np.zeros(n, np.uint8)
+    cs = np.zeros(4 << 20, np.uint8)
+    lam, ms = C.c_double(), C.c_double()
+    size = ref.lib.ref_rate_and_build(width, height, int(fourk), C.c_double(base_step), _p(info), n, _p(pl), _p(pd),
+                                      pl.size, _p(data), data.size, C.c_double(fps), C.c_double(mbps), tag, _p(passes),
+                                      _p(cs), cs.size, C.byref(lam), C.byref(ms))
+    if size < 0:
+        raise RuntimeError(ref.error())
+    return bytes(cs[:size]), passes, lam.value, ms.value
+
+
+def ref_parse(ref: "Reference", cs: bytes, reduce=0):
+    _ref_bind(ref.lib)
+    d = np.frombuffer(cs, np.uint8)
+    blocks = np.zeros(40000, CBLK_CODE)
+    nb, w, h, lv = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    if ref.lib.ref_parse(_p(d), d.size, reduce, _p(blocks), len(blocks), C.byref(nb), C.byref(w), C.byref(h),
+                         C.byref(lv)) != 0:
+        raise RuntimeError(ref.error())
+    return blocks[: nb.value].copy(), w.value, h.value, lv.value
+
+
+def ref_decode(ref: "Reference", cs: bytes, width, height, reduce=0, high_bits=False, threads=0, wavelet=False):
+    _ref_bind(ref.lib)
+    d = np.frombuffer(cs, np.uint8)
+    ow, oh = width, height
+    for _ in range(reduce):
+        ow, oh = (ow + 1) // 2, (oh + 1) // 2
+    out = np.zeros((oh, ow, 3), np.uint16)
+    wl = np.zeros((3, height, width), np.float32) if wavelet else None
+    ms = C.c_double()
+    if ref.lib.ref_decode(_p(d), d.size, reduce, int(high_bits), threads, _p(out), ow * 6,
+                          _p(wl) if wavelet else None, C.byref(ms)) != 0:
+        raise RuntimeError(ref.error())
+    return out, wl, ms.value
+
+
+def ref_check(ref: "Reference", cs: bytes, fps=24.0):
+    _ref_bind(ref.lib)
+    d = np.frombuffer(cs, np.uint8)
+    msg = C.create_string_buffer(512)
+    ok = ref.lib.ref_check_dci(_p(d), d.size, C.c_double(fps), msg, 512)
+    return bool(ok), msg.value.decode(errors="replace")

@@ -1,0 +1,81 @@
+"""Decoding through the plugin table against the reference CPU decoder: codestreams made by
+the reference CPU encoder (rate-controlled to the DCI budget, DCI-checked), parsed by the
+reference's packet parser; the dequantised coefficients must be bit-identical to the CPU
+decoder's and the picture within one code value of it (as the reference's testGpuDecode,
+tests/test_main.cpp:2420-2499), at full and half size."""
+import numpy as np
+import pytest
+
+from libgail_b200 import plugin as P
+from libgail_b200 import synth
+from oracle.oracle import Reference, RefEncoder, have_reference, ref_check, ref_codestream, ref_decode, ref_parse
+
+pytestmark = pytest.mark.skipif(not have_reference(), reason="reference build not present")
+
+
+@pytest.fixture(scope="module")
+def dev():
+    d = P.Plugin().device(0)
+    yield d
+    d.close()
+
+
+def _codestream(W, H, fourk, seed):
+    ref = Reference()
+    planes = synth.xyz12_planes(W, H, seed=seed)
+    enc = RefEncoder(ref, W, H, fourk)
+    t1 = enc.encode(synth.xyz12_to_rgb48(planes))
+    enc.close()
+    cs, _, _, _ = ref_codestream(ref, W, H, fourk, t1, mbps=250.0)
+    ok, msg = ref_check(ref, cs)
+    assert ok, msg
+    return ref, cs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("W,H,fourk,reduce", [(1998, 1080, 0, 0), (1998, 1080, 0, 1), (3996, 2160, 1, 0),
+                                              (3996, 2160, 1, 1), (333, 200, 1, 0)])
+def test_decode_matches_cpu(dev, W, H, fourk, reduce):
+    ref, cs = _codestream(W, H, fourk, seed=7 + W)
+    blocks, w, h, lv = ref_parse(ref, cs, reduce)
+    lay = P.LayoutHolder(W, H, fourk)
+    dec = dev.decoder(lay, reduce=reduce, high_bits=False)
+    try:
+        pic, tm, wl = dec.decode(cs, blocks.view(P.CBLK_CODE_DTYPE), wavelet=True)
+    finally:
+        dec.close()
+    want, wref, _ = ref_decode(ref, cs, W, H, reduce, wavelet=True)
+    # coefficients of the decoded resolutions: bit-identical
+    wl = wl.reshape(3, H, W)
+    mask = np.zeros((H, W), bool)
+    bands, _ = Reference().layout(W, H, fourk)
+    for b in bands:
+        if b.res <= lv - reduce:
+            mask[b.py0:b.py0 + b.h, b.px0:b.px0 + b.w] = True
+    diff = np.count_nonzero((wl.view(np.uint32) != wref.view(np.uint32)) & mask[None])
+    assert diff == 0, f"{diff} dequantised coefficients differ"
+    d = np.abs(pic.astype(np.int32) - want.astype(np.int32))
+    assert d.max() <= 1, f"picture differs by up to {d.max()} codes"
+    assert np.count_nonzero(d) <= 0.02 * d.size
+
+
+@pytest.mark.gpu
+def test_decode_damaged_input_stays_in_bounds(dev):
+    """Blocks pointing past the codestream decode as zero; junk bytes decode to
+    something without error."""
+    W, H = 333, 200
+    ref, cs = _codestream(W, H, 1, seed=1)
+    blocks, _, _, _ = ref_parse(ref, cs, 0)
+    b = blocks.copy()
+    b["offset"][::3] = len(cs) + 100
+    b["len"][1::5] = 0xFFFFFF
+    lay = P.LayoutHolder(W, H, 1)
+    dec = dev.decoder(lay)
+    try:
+        junk = bytes(np.random.default_rng(0).integers(0, 256, len(cs), dtype=np.uint8))
+        pic, _, _ = dec.decode(junk, b.view(P.CBLK_CODE_DTYPE))
+        pic2, _, _ = dec.decode(cs, blocks.view(P.CBLK_CODE_DTYPE))
+    finally:
+        dec.close()
+    want, _, _ = ref_decode(ref, cs, W, H, 0)
+    assert np.abs(pic2.astype(np.int32) - want.astype(np.int32)).max() <= 1
