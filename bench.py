@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark: 4K DCI JPEG 2000 encode on one B200 (and N replicas under torchrun).
+
+Workload (the 4K configuration): 48 preloaded 3996x2160 frames of 10-bit Y'CbCr 4:2:2
+BT.2020 PQ from the seeded generator (libgail_b200/synth.py), colour-converted on the GPU
+to 12-bit X'Y'Z', 9/7 wavelet with 6 levels, 32x32 code-blocks, Tier-1 with every coding
+pass (bit-exact with the CPU reference). One step = encoding all 48 frames; the 48 frames
+(1.66 GB) are larger than L2, so no flush is needed between steps.
+
+  value  frames/s with the frames resident in HBM: the device stages only, timed with CUDA
+         events on the encoder's stream, max over ranks.
+  e2e    frames/s through the plugin table's encoder_encode from host memory: each frame's
+         upload from pinned memory, the device stages and the download of its Tier-1
+         output (CblkInfo, pass tables, codewords) are inside the timed region.
+
+--impl reference times the reference's own CPU encoder (the CpuSlot path, built from the
+reference sources into oracle/_ref) on the same frames with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W4K, H4K, FRAMES = 3996, 2160, 48
+METRIC = "4K encode fps & p99 frame latency, served vs plain, 1 B200, Tier-1 bit-exact"
+WORKLOAD = ("4K 3996x2160 Y'CbCr 4:2:2 10-bit BT.2020 PQ -> 12-bit X'Y'Z', 9/7 6 levels, 32x32 code-blocks, "
+            "Tier-1 all passes, 48 preloaded frames")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=FRAMES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gen_frames(count):
+    from libgail_b200 import synth
+    return synth.many(synth.yuv422p10, count, W4K, H4K, seed=1000)
+
+
+def cpu_baseline(frames, sample=2):
+    """The reference CPU encoder (or, without its build, the oracle port) on a bounded sample."""
+    from oracle.oracle import Planar, Reference, RefEncoder, have_reference
+    pl = Planar(width=W4K, height=H4K, active_w=W4K, active_h=H4K, ox=0, oy=0, sx=1, sy=0, rgb=0, bits=10,
+                full_range=0, chroma=0, kr=0.2627, kb=0.0593)
+    if have_reference():
+        ref = Reference()
+        cores = ref.lib.ref_usable_cpus()
+        enc = RefEncoder(ref, W4K, H4K, 1, transfer=2, primaries=1, planar=pl, threads=0)
+        enc.encode(frames[0])  # warm-up
+        t0 = time.perf_counter()
+        for i in range(sample):
+            enc.encode(frames[1 + i % (len(frames) - 1)])
+        dt = time.perf_counter() - t0
+        enc.close()
+        return {"value": sample / dt, "unit": "frames/s", "cores": cores, "kind": "reference",
+                "sample": f"{sample} 4K frames (after 1 warm-up) through the reference CpuSlot encoder, all passes"}
+    from oracle.oracle import Oracle
+    o = Oracle()
+    t0 = time.perf_counter()
+    rgb = o.planar_to_rgb48(pl, frames[0])
+    planes, _ = o.color_frame(rgb, 2, 1)
+    wav = np.stack([o.fdwt(planes[c], 6) for c in range(3)])
+    bands, cblks = o.layout(W4K, H4K, 1)
+    q = o.quantize_frame(wav, bands, cblks)
+    geom = np.array([[k.w, k.h, bands[k.band].orient, 64] for k in cblks], np.int32)
+    o.t1_encode_many(q, geom)
+    dt = time.perf_counter() - t0
+    return {"value": 1 / dt, "unit": "frames/s", "cores": 1, "kind": "port",
+            "sample": "1 4K frame through the single-threaded C oracle"}
+
+
+def run_reference(args):
+    rank, local, world = rank_info()
+    if rank != 0:
+        return
+    from oracle.oracle import Planar, Reference, RefEncoder, have_reference
+    if not have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not present"}))
+        return
+    frames = gen_frames(min(args.frames, args.steps + args.warmup + 1))
+    ref = Reference()
+    cores = ref.lib.ref_usable_cpus()
+    pl = Planar(width=W4K, height=H4K, active_w=W4K, active_h=H4K, ox=0, oy=0, sx=1, sy=0, rgb=0, bits=10,
+                full_range=0, chroma=0, kr=0.2627, kb=0.0593)
+    enc = RefEncoder(ref, W4K, H4K, 1, transfer=2, primaries=1, planar=pl, threads=0)
+    for i in range(args.warmup):
+        enc.encode(frames[i % len(frames)])
+    lat = []
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        t = time.perf_counter()
+        enc.encode(frames[(args.warmup + i) % len(frames)])
+        lat.append((time.perf_counter() - t) * 1e3)
+    dt = time.perf_counter() - t0
+    enc.close()
+    fps = args.steps / dt
+    out = {"impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32 (integer Tier-1), f32 (colour, wavelet)",
+           "data": "synthetic (seeded generator)",
+           "config": {"workload": WORKLOAD, "step": "one frame (bounded sample of the 48-frame workload)",
+                      "path": "reference CpuSlot (colour, wavelet, quantisation, Tier-1), all host threads"},
+           "latency_ms": {"p50": statistics.median(lat), "p99": float(np.percentile(lat, 99))},
+           "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "reference",
+                            "sample": f"{args.steps} 4K frames after {args.warmup} warm-up"},
+           "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, local, world = rank_info()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    import libgail_b200 as gb
+    from libgail_b200 import plugin as P
+
+    L = gb.lib()
+    L.gb_encoder_stream.restype = C.c_void_p
+    L.gb_encoder_stream.argtypes = [C.c_void_p]
+    L.gb_encoder_enqueue_device.argtypes = [C.c_void_p, C.c_void_p]
+    L.gb_encoder_finish.argtypes = [C.c_void_p]
+    L.gb_encoder_stage_timing.argtypes = [C.c_void_p, C.c_int]
+    L.gb_encoder_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+
+    frames = gen_frames(args.frames)
+    plugin = P.Plugin()
+    dev = plugin.device(local)
+    lay = P.LayoutHolder(W4K, H4K, 1)
+    enc = dev.encoder(lay, P.planar_format(W4K, H4K, bits=10, sx=1, sy=0), P.color("pq", "bt2020"))
+    h = enc.h
+    dframes = [torch.from_numpy(f.view(np.int16)).to(f"cuda:{local}") for f in frames]
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(L.gb_encoder_stream(h), device=f"cuda:{local}")
+
+    def step():
+        for f in dframes:
+            gb.check(L.gb_encoder_enqueue_device(h, C.c_void_p(f.data_ptr())))
+
+    for _ in range(args.warmup):
+        step()
+    gb.check(L.gb_encoder_finish(h))
+    ms5 = np.zeros(5)
+    cnt = C.c_int()
+    gb.check(L.gb_encoder_stage_timing(h, 1))
+    gb.check(L.gb_encoder_stage_times(h, ms5.ctypes.data, C.byref(cnt)))  # reset
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    gb.check(L.gb_encoder_finish(h))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_ms = e0.elapsed_time(e1)
+    gb.check(L.gb_encoder_stage_times(h, ms5.ctypes.data, C.byref(cnt)))
+    gb.check(L.gb_encoder_stage_timing(h, 0))
+    if world > 1:
+        t = torch.tensor([t_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+        dist.barrier()
+    nframes = args.steps * len(dframes)
+    value = nframes * world / (t_ms / 1e3)
+    stage = ms5 / max(cnt.value, 1)  # ms per frame: front, cm, order, mq, pack
+
+    # e2e: host frames through encoder_encode, uploads from the pinned input buffer
+    inbuf = enc.input_buffer()
+    nbytes = frames[0].nbytes
+    d2h = 0
+    lat = []
+    for i in range(2):  # warm-up
+        C.memmove(inbuf, frames[i].ctypes.data, nbytes)
+        enc.encode(np.ctypeslib.as_array(C.cast(inbuf, C.POINTER(C.c_uint16)), (nbytes // 2,)))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for f in frames:
+        t = time.perf_counter()
+        C.memmove(inbuf, f.ctypes.data, nbytes)
+        t1, _, _ = enc.encode(np.ctypeslib.as_array(C.cast(inbuf, C.POINTER(C.c_uint16)), (nbytes // 2,)))
+        d2h += t1.info.nbytes + t1.pass_len.nbytes + t1.pass_dist.nbytes + t1.data.nbytes
+        lat.append((time.perf_counter() - t) * 1e3)
+    e2e_s = time.perf_counter() - t0
+    e2e_fps = len(frames) / e2e_s
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_fps = len(frames) * world / float(t.item())
+
+    out = None
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        npix = W4K * H4K
+        # dominant kernel: the largest stage
+        names = ["front end (colour+DWT+quantise)", "Tier-1 context modelling", "Tier-1 ordering", "Tier-1 MQ coding",
+                 "Tier-1 packing"]
+        k = int(np.argmax(stage))
+        # algorithmic bytes per launch (one frame): front end reads the frame and writes the
+        # coefficient words + LL floats of the deeper levels; context modelling reads the
+        # coefficient words and writes one byte per decision; MQ reads the decisions and
+        # writes the codewords
+        syms_per_frame = None
+        alg = {0: nbytes + npix * 3 * 4 + npix * 3 * 4 // 3 * 2, 1: npix * 3 * 4, 3: 0}
+        roofline = {"bound": "hbm", "kernel": names[k], "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
+                    "traffic": None, "peak_source": "measured" if peaks else "fallback"}
+        if k in alg and alg[k]:
+            ach = alg[k] / (stage[k] * 1e-3) / 1e9
+            roofline.update(achieved=ach, frac=ach / hbm)
+        out = {
+            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8/int32 (integer Tier-1), f32 (colour, wavelet)",
+            "data": "synthetic (seeded generator, 48 frames)",
+            "config": {"workload": WORKLOAD, "frames_per_step": len(dframes), "path": "plain per-frame",
+                       "parallelism": f"replicas x{world}",
+                       "l2": f"inputs larger than L2 ({len(dframes)} frames, {len(dframes) * nbytes / 1e9:.2f} GB)"},
+            "stage_ms_per_frame": dict(zip(["front", "t1_cm", "t1_order", "t1_mq", "pack"], [round(x, 4) for x in stage])),
+            "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": nbytes * len(frames),
+                    "d2h_bytes_per_step": int(d2h), "path": "plugin encoder_encode, host frames",
+                    "latency_ms": {"p50": statistics.median(lat), "p99": float(np.percentile(lat, 99))}},
+            "gpu_launches": nframes * (6 + 3 + 2),
+            "roofline": roofline,
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                out["cpu_baseline"] = cpu_baseline(frames)
+            except Exception as e:  # a missing baseline must not hide the measurement
+                out["cpu_baseline"] = {"unavailable": str(e)}
+    enc.close()
+    dev.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

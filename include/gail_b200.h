@@ -64,6 +64,28 @@ GB_API int gb_make_layout(int width, int height, int fourk, double baseStep, GbS
  * ColorConverter's lut()/params() (src/core/color.h:105-108). Any pointer may be NULL. */
 GB_API int gb_color_tables(const GailCudaColor* color, float* eotf65536, float* matrix9, float* thresholds4096);
 
+/* Frames already in device memory (a serving layer that keeps them resident). The
+ * encoder is one made by the plugin table's encoder_create; these replace the upload half
+ * of encoder_encode (the reference's CudaSlot::encodeView, src/cuda/cuda_backend.cu:870-977).
+ *   gb_encoder_stream          the encoder's CUDA stream (cudaStream_t), for ordering and
+ *                              timing the caller's own work against it
+ *   gb_encoder_enqueue_device  enqueue front end, Tier-1 and packing of the frame at dFrame
+ *                              (device memory, the encoder's input format) on that stream;
+ *                              returns at once; dFrame must stay valid until it is done
+ *   gb_encoder_finish          wait for the enqueued work and check the kernels' status */
+GB_API void* gb_encoder_stream(GailCudaEncoder* e);
+GB_API int gb_encoder_enqueue_device(GailCudaEncoder* e, const void* dFrame);
+GB_API int gb_encoder_finish(GailCudaEncoder* e);
+
+/* Per-stage device time of gb_encoder_enqueue_device (the reference's FrameTimings stage
+ * split, src/core/backend.h:33-37): gb_encoder_stage_timing(e, 1) makes every enqueue
+ * record CUDA events between its stages; gb_encoder_stage_times waits for the stream and
+ * returns in ms5 the summed durations of {front end (colour, wavelet, quantisation),
+ * Tier-1 context modelling, Tier-1 ordering, MQ coding, packing} over the enqueues since
+ * the last call (at most 512), and their number in count. */
+GB_API int gb_encoder_stage_timing(GailCudaEncoder* e, int on);
+GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
+
 /* FNV hash of the ABI structure sizes, as the plugin table's `layout` field carries it
  * (cudaPluginLayout, src/cuda/cuda_plugin.h:208-217). */
 GB_API uint64_t gb_plugin_layout_hash(void);

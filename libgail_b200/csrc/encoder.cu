@@ -157,6 +157,9 @@ void EncoderSlot::release() {
             cudaEventDestroy(e);
             e = nullptr;
         }
+    for (auto& e : ring_)
+        if (e) cudaEventDestroy(e);
+    ring_.clear();
     if (st_) cudaStreamDestroy(st_);
     st_ = nullptr;
     cudaGetLastError();
@@ -168,32 +171,33 @@ void EncoderSlot::uploadStatic() {
     GB_CHECK(cudaMemcpy(dJobs_, jobs_.data(), jobs_.size() * sizeof(T1Job), cudaMemcpyHostToDevice));
 }
 
-void EncoderSlot::encode(const void* frame, GailCudaTier1* out, GbFrameTimings* tm, GailCudaDebug* dbg) {
-    const auto t0 = std::chrono::steady_clock::now();
-    GB_CHECK(cudaSetDevice(dev_));
-    if (!frame) throw std::logic_error("no frame");
-    const bool full = dbg && dbg->full;
-    const uint64_t npix = z_.npix, n = z_.n;
-    if (dbg && !dXyz_) check(cudaMalloc(&dXyz_, npix * 6), "device memory for the debug taps");
-    if (full && !dTap_) check(cudaMalloc(&dTap_, npix * 12), "device memory for the debug taps");
-    if (frame != hIn_) std::memcpy(hIn_, frame, z_.inBytes);
-    *hSlope_ = slope_;
+void EncoderSlot::enqueueStages(const void* dFrame, bool taps, bool full) {
     const cudaStream_t st = st_;
-    GB_CHECK(cudaEventRecord(ev_[0], st));
-    GB_CHECK(cudaMemcpyAsync(dIn_, hIn_, z_.inBytes, cudaMemcpyHostToDevice, st));
-    GB_CHECK(cudaMemcpyAsync(dSlope_, hSlope_, 4, cudaMemcpyHostToDevice, st));
-    GB_CHECK(cudaMemsetAsync(dCtl_, 0, 64, st));
-    GB_CHECK(cudaEventRecord(ev_[1], st));
-
+    const uint64_t npix = z_.npix;
+    // control words: all but the status word (ctl[1]), which collects every frame's
+    // status until finish() or encode() reads it
+    GB_CHECK(cudaMemsetAsync(dCtl_, 0, 4, st));
+    GB_CHECK(cudaMemsetAsync(dCtl_ + 2, 0, 56, st));
+    cudaEvent_t* mark = nullptr;
+    if (timing_) {
+        if (ring_.empty()) {
+            ring_.resize((size_t)kTimingRing * 6);
+            for (auto& e : ring_) GB_CHECK(cudaEventCreate(&e));
+        }
+        mark = &ring_[(size_t)ringNext_ * 6];
+        ringNext_ = (ringNext_ + 1) % kTimingRing;
+        ringCount_ = std::min(ringCount_ + 1, kTimingRing);
+        GB_CHECK(cudaEventRecord(mark[0], st));
+    }
     // front end: colour + level 1, then one kernel per level
     ColorArgs c{};
     c.kind = s_.input.kind == GB_FRAME_PLANAR ? 1 : 0;
-    c.src = dIn_;
+    c.src = dFrame;
     c.pp = planarParams(s_.input);
     c.eotf = dEotf_;
     c.thr = dThr_;
     std::memcpy(c.m, m_, sizeof m_);
-    c.xyz = dbg ? dXyz_ : nullptr;
+    c.xyz = taps ? dXyz_ : nullptr;
     const int NL = L_.levels;
     for (int l = 1; l <= NL; ++l) {
         LevelArgs a{};
@@ -228,13 +232,67 @@ void EncoderSlot::encode(const void* frame, GailCudaTier1* out, GbFrameTimings* 
         else launchLevel(a, st);
     }
     GB_CHECK(cudaEventRecord(ev_[2], st));
-
+    if (mark) GB_CHECK(cudaEventRecord(mark[1], st));
+    const uint64_t n = z_.n;
     T1Launch t{dCoeffs_, dJobs_, (uint32_t)n, dSym_, dCw_, dInfo_, dEnd_, dLen_, dDist_, dSnaps_, dPerm_, dCtl_, dSlope_};
-    t1Encode(t, st);
+    t1Encode(t, st, mark ? mark + 2 : nullptr);
     GB_CHECK(cudaEventRecord(ev_[3], st));
-
+    if (mark) GB_CHECK(cudaEventRecord(mark[4], st));
     CompactArgs ca{(uint32_t)n, dInfo_, dLen_, dDist_, dCw_, dJobs_, dOutInfo_, dOutLen_, dOutDist_, dOutData_, dCtl_ + 8};
     compactTier1(ca, st);
+    if (mark) GB_CHECK(cudaEventRecord(mark[5], st));
+}
+
+void EncoderSlot::enqueue(const void* dFrame) {
+    GB_CHECK(cudaSetDevice(dev_));
+    *hSlope_ = slope_;
+    GB_CHECK(cudaMemcpyAsync(dSlope_, hSlope_, 4, cudaMemcpyHostToDevice, st_));
+    enqueueStages(dFrame ? dFrame : dIn_, false, false);
+}
+
+void EncoderSlot::finish() {
+    GB_CHECK(cudaSetDevice(dev_));
+    GB_CHECK(cudaMemcpyAsync(hSmall_, dCtl_, 64, cudaMemcpyDeviceToHost, st_));
+    GB_CHECK(cudaStreamSynchronize(st_));
+    GB_CHECK(cudaGetLastError());
+    const uint32_t status = hSmall_[1];
+    GB_CHECK(cudaMemsetAsync(dCtl_ + 1, 0, 4, st_));
+    if (status) throw std::runtime_error("Tier-1 kernels reported status " + std::to_string(status));
+}
+
+int EncoderSlot::stageTimes(double ms[5]) {
+    for (int k = 0; k < 5; ++k) ms[k] = 0;
+    GB_CHECK(cudaStreamSynchronize(st_));
+    const int count = ringCount_;
+    for (int i = 0; i < count; ++i) {
+        cudaEvent_t* e = &ring_[(size_t)((ringNext_ - 1 - i + kTimingRing) % kTimingRing) * 6];
+        for (int k = 0; k < 5; ++k) {
+            float t = 0;
+            GB_CHECK(cudaEventElapsedTime(&t, e[k], e[k + 1]));
+            ms[k] += t;
+        }
+    }
+    ringCount_ = 0;
+    return count;
+}
+
+void EncoderSlot::encode(const void* frame, GailCudaTier1* out, GbFrameTimings* tm, GailCudaDebug* dbg) {
+    const auto t0 = std::chrono::steady_clock::now();
+    GB_CHECK(cudaSetDevice(dev_));
+    if (!frame) throw std::logic_error("no frame");
+    const bool full = dbg && dbg->full;
+    const uint64_t npix = z_.npix, n = z_.n;
+    if (dbg && !dXyz_) check(cudaMalloc(&dXyz_, npix * 6), "device memory for the debug taps");
+    if (full && !dTap_) check(cudaMalloc(&dTap_, npix * 12), "device memory for the debug taps");
+    if (frame != hIn_) std::memcpy(hIn_, frame, z_.inBytes);
+    *hSlope_ = slope_;
+    const cudaStream_t st = st_;
+    GB_CHECK(cudaEventRecord(ev_[0], st));
+    GB_CHECK(cudaMemcpyAsync(dIn_, hIn_, z_.inBytes, cudaMemcpyHostToDevice, st));
+    GB_CHECK(cudaMemcpyAsync(dSlope_, hSlope_, 4, cudaMemcpyHostToDevice, st));
+    GB_CHECK(cudaMemsetAsync(dCtl_ + 1, 0, 4, st));
+    GB_CHECK(cudaEventRecord(ev_[1], st));
+    enqueueStages(dIn_, dbg != nullptr, full);
     GB_CHECK(cudaMemcpyAsync(hSmall_, dCtl_, 64, cudaMemcpyDeviceToHost, st));
     GB_CHECK(cudaStreamSynchronize(st));
     const uint32_t status = hSmall_[1], totData = hSmall_[8], totPasses = hSmall_[9];

@@ -39,11 +39,30 @@ public:
     // The plain path: frame (host memory) in, Tier-1 frame (this slot's pinned memory) out.
     void encode(const void* frame, GailCudaTier1* out, GbFrameTimings* tm, GailCudaDebug* dbg);
 
+    // The same work split up for callers whose frames are already in device memory:
+    // enqueue() puts the front end, Tier-1 and compaction of the frame at dFrame (device
+    // memory of frameBytes(); NULL: this slot's own input buffer) on the slot's stream and
+    // returns without waiting; the packed results stay on the device. finish() waits for
+    // them and checks the kernels' status.
+    void enqueue(const void* dFrame);
+    void finish();
+    cudaStream_t stream() const { return st_; }
+    uint64_t inputBytes() const { return z_.inBytes; }
+
+    // Stage timing of enqueue(): when on, every enqueue records CUDA events between its
+    // stages (front end, context modelling, ordering, MQ, packing) on the slot's stream.
+    // stageTimes() (after finish()) sums their durations in ms over the enqueues since the
+    // last call, at most kTimingRing of them, and returns how many it summed.
+    static constexpr int kTimingRing = 512;
+    void setTiming(bool on) { timing_ = on; }
+    int stageTimes(double ms[5]);
+
     const Layout& layout() const { return L_; }
 
 private:
     void release();
     void uploadStatic();
+    void enqueueStages(const void* dFrame, bool taps, bool fullTaps);
 
     int dev_;
     Layout L_;
@@ -52,6 +71,9 @@ private:
     float slope_ = 0.f;
     cudaStream_t st_ = nullptr;
     cudaEvent_t ev_[5] = {};
+    bool timing_ = false;
+    std::vector<cudaEvent_t> ring_;  // kTimingRing x 6 events
+    int ringNext_ = 0, ringCount_ = 0;
     std::vector<void*> dev_allocs_;
     std::vector<T1Job> jobs_;
 

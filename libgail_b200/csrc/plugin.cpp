@@ -252,3 +252,34 @@ const GailCudaPlugin kPlugin = {
 extern "C" const GailCudaPlugin* gail_cuda_plugin_get(uint32_t abi) { return abi == GAIL_CUDA_PLUGIN_ABI ? &kPlugin : nullptr; }
 
 extern "C" GB_API uint64_t gb_plugin_layout_hash(void) { return layoutHash(); }
+
+// ---- device-resident frames (gail_b200.h) -------------------------------------------
+extern "C" GB_API void* gb_encoder_stream(GailCudaEncoder* e) { return e ? (void*)e->slot->stream() : nullptr; }
+
+extern "C" GB_API int gb_encoder_enqueue_device(GailCudaEncoder* e, const void* dFrame) {
+    return gbGuard([&] {
+        if (!e) throw std::logic_error("no encoder");
+        e->slot->enqueue(dFrame);
+    });
+}
+
+extern "C" GB_API int gb_encoder_finish(GailCudaEncoder* e) {
+    return gbGuard([&] {
+        if (!e) throw std::logic_error("no encoder");
+        e->slot->finish();
+    });
+}
+
+extern "C" GB_API int gb_encoder_stage_timing(GailCudaEncoder* e, int on) {
+    return gbGuard([&] {
+        if (!e) throw std::logic_error("no encoder");
+        e->slot->setTiming(on != 0);
+    });
+}
+
+extern "C" GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count) {
+    return gbGuard([&] {
+        if (!e || !ms5 || !count) throw std::logic_error("null argument");
+        *count = e->slot->stageTimes(ms5);
+    });
+}

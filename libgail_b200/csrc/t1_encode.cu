@@ -634,14 +634,16 @@ void t1Init() {
     GB_CHECK(cudaMemcpyToSymbol(c_mq, mq, sizeof mq));
 }
 
-void t1Encode(const T1Launch& L, cudaStream_t st) {
+void t1Encode(const T1Launch& L, cudaStream_t st, cudaEvent_t* marks) {
     if (L.n == 0) return;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t cmBlocks = min(divUp(L.n, CM_WARPS), (uint32_t)sms * 16u);
     t1CmKernel<<<cmBlocks, CM_THREADS, 0, st>>>(L);
+    if (marks) GB_CHECK(cudaEventRecord(marks[0], st));
     t1OrderKernel<<<1, 1024, 0, st>>>(L);
+    if (marks) GB_CHECK(cudaEventRecord(marks[1], st));
     const uint32_t mqBlocks = min(divUp(L.n, MQ_THREADS), (uint32_t)sms * 16u);
     t1MqKernel<<<mqBlocks, MQ_THREADS, 0, st>>>(L);
     GB_CHECK(cudaGetLastError());

@@ -50,7 +50,8 @@ struct T1Launch {
 
 // Enqueues the whole Tier-1 stage on st: context modelling, ordering, MQ coding.
 // ctl must be zeroed by the caller (it is part of the launch so that graphs can hold it).
-void t1Encode(const T1Launch& L, cudaStream_t st);
+// marks (optional): two events recorded after context modelling and after ordering.
+void t1Encode(const T1Launch& L, cudaStream_t st, cudaEvent_t* marks = nullptr);
 
 // Uploads the context tables (once per device, before the first launch).
 void t1Init();

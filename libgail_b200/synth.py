@@ -16,15 +16,21 @@ def plane(width: int, height: int, rng: np.random.Generator, drift: float = 0.0)
     phi = rng.uniform(0, 2 * np.pi) + drift
     x = np.arange(width, dtype=np.float64)
     y = np.arange(height, dtype=np.float64)
-    v = 2048.0 + 900.0 * np.sin(2 * np.pi * f1 * x / width + phi)[None, :] * np.cos(2 * np.pi * f2 * y / height)[:, None]
+    sx = (900.0 * np.sin(2 * np.pi * f1 * x / width + phi)).astype(np.float32)
+    cy = np.cos(2 * np.pi * f2 * y / height).astype(np.float32)
+    v = rng.standard_normal((height, width), dtype=np.float32)
+    v *= np.float32(30.0)
+    v += np.float32(2048.0)
+    v += cy[:, None] * sx[None, :]
     for _ in range(25):
         rw = int(rng.uniform(width / 40, width / 4))
         rh = int(rng.uniform(height / 40, height / 4))
         x0 = int(rng.uniform(0, width - rw))
         y0 = int(rng.uniform(0, height - rh))
-        v[y0:y0 + rh, x0:x0 + rw] += rng.uniform(-600, 600)
-    v += rng.normal(0.0, 30.0, (height, width))
-    return np.clip(np.rint(v), 0, 4095).astype(np.uint16)
+        v[y0:y0 + rh, x0:x0 + rw] += np.float32(rng.uniform(-600, 600))
+    np.rint(v, out=v)
+    np.clip(v, 0, 4095, out=v)
+    return v.astype(np.uint16)
 
 
 def xyz12_planes(width: int, height: int, seed: int, index: int = 0) -> np.ndarray:
@@ -45,10 +51,25 @@ def yuv422p10(width: int, height: int, seed: int, index: int = 0) -> np.ndarray:
     generator, as one flat uint16 array Y | Cb | Cr (the layout the encoder takes)."""
     rng = np.random.default_rng(seed + index)
     cw = (width + 1) >> 1
-    y = plane(width, height, rng, 0.05 * index).astype(np.float64)
-    cb = plane(cw, height, rng, 0.05 * index).astype(np.float64)
-    cr = plane(cw, height, rng, 0.05 * index).astype(np.float64)
-    Y = np.rint(64 + y * (876.0 / 4095.0)).astype(np.uint16)
-    Cb = np.rint(64 + cb * (896.0 / 4095.0)).astype(np.uint16)
-    Cr = np.rint(64 + cr * (896.0 / 4095.0)).astype(np.uint16)
-    return np.concatenate([Y.ravel(), Cb.ravel(), Cr.ravel()])
+
+    def scaled(p, span):
+        v = p.astype(np.float32)
+        v *= np.float32(span / 4095.0)
+        v += np.float32(64.0)
+        np.rint(v, out=v)
+        return v.astype(np.uint16).ravel()
+
+    y = plane(width, height, rng, 0.05 * index)
+    cb = plane(cw, height, rng, 0.05 * index)
+    cr = plane(cw, height, rng, 0.05 * index)
+    return np.concatenate([scaled(y, 876.0), scaled(cb, 896.0), scaled(cr, 896.0)])
+
+
+def many(fn, count: int, *args, seed: int = 1000, threads: int = 0):
+    """fn(*args, seed, i) for i in range(count), generated on a thread pool (numpy releases
+    the interpreter lock in the heavy parts)."""
+    import concurrent.futures as cf
+    import os
+    workers = threads or min(16, os.cpu_count() or 1)
+    with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(lambda i: fn(*args, seed, i), range(count)))
