@@ -53,6 +53,22 @@ GB_API int gb_t1_encode_blocks(const uint32_t* coeffs, const int32_t* geom4, uin
                                const float* distScale, uint32_t* info4, uint32_t* passLen, int32_t* passDist,
                                uint8_t* data, uint32_t dataStride);
 
+/* gb_t1_encode_blocks without any allocation. No counterpart in the reference: it is for
+ * callers that must not allocate device memory themselves, such as a real-time frame
+ * thread (cudaMalloc may wait for the whole device and stall it) or a process whose
+ * device memory is budgeted up front. Same arguments and results as gb_t1_encode_blocks,
+ * but every call works in one static device array of 7.6 MB that this library reserves on
+ * each GPU it is loaded on, for the life of the process:
+ *   - at most 64 code-blocks per call; more is refused with GAIL_CUDA_MISUSE;
+ *   - the first call on a device looks up the array's device address and loads the
+ *     kernels' tables there; make that first call before any stream capture;
+ *   - calls share the array: two calls whose work overlaps on the GPU (other threads,
+ *     other streams) race and corrupt each other's results, so serialise them;
+ *   - the call waits for its work (it synchronises the device) before it returns. */
+GB_API int gb_t1_encode_blocks_noalloc(const uint32_t* coeffs, const int32_t* geom4, uint32_t n, float slope,
+                                       const float* distScale, uint32_t* info4, uint32_t* passLen, int32_t* passDist,
+                                       uint8_t* data, uint32_t dataStride);
+
 /* The DCI frame layout: subbands (with their quantisation steps) in the plugin ABI's
  * form, for callers that build GailCudaLayout themselves. Replaces makeLayout
  * (src/core/layout.h:87 with Profile::Cinema2K / Cinema4K). maxBands >= 3 * 19 + 3. */

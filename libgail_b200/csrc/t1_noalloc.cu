@@ -1,0 +1,139 @@
+// Tier-1 encoding without any allocation: gb_t1_encode_blocks_noalloc.
+//
+// Who this is for: callers that must not allocate device memory on their own. Examples
+// are a real-time frame thread, where cudaMalloc can wait for the whole device to go idle
+// and so turns into a latency spike, and a host process whose device memory is budgeted
+// up front (a serving loop that admits work against a fixed HBM budget, or an
+// application that hands this library a fixed share of a GPU it partitions among
+// tenants), where memory taken outside that budget is not allowed. gb_t1_encode_blocks
+// allocates its device buffers on every call; this entry point uses one static device
+// array instead.
+//
+// The array (kNoAllocBytes, 7.6 MB) is a file-scope __device__ variable: it is reserved
+// on every GPU that loads this library, from the load until the process exits, whether or
+// not the entry point is ever called. It holds at most kNoAllocMaxBlocks code-blocks per
+// call; a larger call is refused with GAIL_CUDA_MISUSE.
+//
+// Every call uses the same array and leaves its contents behind. The call clears the
+// control words the kernels count with before it starts; everything else is written
+// before it is read. Two calls whose device work overlaps (from different host threads,
+// or on different streams) race on the array and corrupt each other's results: callers
+// must serialise their calls.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+
+#include "capi_util.h"
+#include "common.cuh"
+#include "gail_b200.h"
+#include "t1_encode.cuh"
+
+namespace gb {
+
+namespace {
+
+constexpr uint32_t kNoAllocMaxBlocks = 64;
+// Every block gets the region of a block with the most bit-planes a band can signal.
+constexpr uint32_t kRegion = ((2560u * kMaxPlanes + 64u) + 15u) & ~15u;  // = t1SymbolBound(32, 32, 22)
+// Layout of the array, per call of up to kNoAllocMaxBlocks blocks (offsets in bytes):
+constexpr size_t kOffCtl = 0;                                                   // 16 words
+constexpr size_t kOffSlope = 64;                                                // 1 float
+constexpr size_t kOffJobs = 256;                                                // T1Job per block
+constexpr size_t kOffCoeffs = kOffJobs + kNoAllocMaxBlocks * sizeof(T1Job);     // 1024 words per block
+constexpr size_t kOffInfo = kOffCoeffs + (size_t)kNoAllocMaxBlocks * kCblkArea * 4;
+constexpr size_t kOffEnd = kOffInfo + kNoAllocMaxBlocks * 16;
+constexpr size_t kOffLen = kOffEnd + (size_t)kNoAllocMaxBlocks * kMaxPasses * 4;
+constexpr size_t kOffDist = kOffLen + (size_t)kNoAllocMaxBlocks * kMaxPasses * 4;
+constexpr size_t kOffSnaps = kOffDist + (size_t)kNoAllocMaxBlocks * kMaxPasses * 4;
+constexpr size_t kOffPerm = kOffSnaps + (size_t)kNoAllocMaxBlocks * kMaxPasses * 16;
+constexpr size_t kOffSym = (kOffPerm + kNoAllocMaxBlocks * 4 + 255) & ~(size_t)255;
+constexpr size_t kOffCw = kOffSym + (size_t)kNoAllocMaxBlocks * kRegion;
+constexpr size_t kNoAllocBytes = kOffCw + (size_t)kNoAllocMaxBlocks * kRegion;
+
+static __device__ __align__(256) unsigned char g_scratch[kNoAllocBytes];
+
+// The array's device address, looked up once per device (in host code the name
+// g_scratch is only a stand-in for the symbol, not an address a kernel may use).
+constexpr int kMaxDevices = 64;
+std::mutex g_mutex;
+unsigned char* g_address[kMaxDevices] = {};
+
+unsigned char* scratchAddress() {
+    int dev = 0;
+    GB_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) throw std::runtime_error("device index out of range");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!g_address[dev]) {
+        ensureDevice();
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw std::runtime_error(std::string("no device address for the Tier-1 scratch array: ") +
+                                     cudaGetErrorString(e));
+        }
+        g_address[dev] = static_cast<unsigned char*>(p);
+    }
+    return g_address[dev];
+}
+
+}  // namespace
+
+}  // namespace gb
+
+using namespace gb;
+
+extern "C" GB_API int gb_t1_encode_blocks_noalloc(const uint32_t* coeffs, const int32_t* geom4, uint32_t n, float slope,
+                                                  const float* distScale, uint32_t* info4, uint32_t* passLen,
+                                                  int32_t* passDist, uint8_t* data, uint32_t dataStride) {
+    return gbGuard([&] {
+        if (!coeffs || !geom4 || !info4 || !passLen || !passDist || !data) throw std::logic_error("null argument");
+        if (n > kNoAllocMaxBlocks)
+            throw std::logic_error("gb_t1_encode_blocks_noalloc takes at most " + std::to_string(kNoAllocMaxBlocks) +
+                                   " code-blocks per call (" + std::to_string(n) + " given)");
+        if (n == 0) return;
+        unsigned char* base = scratchAddress();
+        T1Job jobs[kNoAllocMaxBlocks];
+        for (uint32_t i = 0; i < n; ++i) {
+            const int w = geom4[4 * i], h = geom4[4 * i + 1], orient = geom4[4 * i + 2], mp = geom4[4 * i + 3];
+            if (w < 1 || w > 32 || h < 1 || h > 32 || orient < 0 || orient > 3 || mp < 0 || mp > 64)
+                throw std::logic_error("code-block geometry out of range");
+            jobs[i] = {i, i * kRegion, kRegion, t1Geom(w, h, orient, mp, 0), distScale ? distScale[i] : 1.f, {0, 0, 0}};
+        }
+        T1Launch L{reinterpret_cast<const uint32_t*>(base + kOffCoeffs),
+                   reinterpret_cast<const T1Job*>(base + kOffJobs),
+                   n,
+                   base + kOffSym,
+                   base + kOffCw,
+                   reinterpret_cast<uint32_t*>(base + kOffInfo),
+                   reinterpret_cast<uint32_t*>(base + kOffEnd),
+                   reinterpret_cast<uint32_t*>(base + kOffLen),
+                   reinterpret_cast<int32_t*>(base + kOffDist),
+                   reinterpret_cast<uint4*>(base + kOffSnaps),
+                   reinterpret_cast<uint32_t*>(base + kOffPerm),
+                   reinterpret_cast<uint32_t*>(base + kOffCtl),
+                   reinterpret_cast<const float*>(base + kOffSlope)};
+        // inputs in, the previous call's control words cleared
+        GB_CHECK(cudaMemcpy(base + kOffCoeffs, coeffs, (size_t)n * kCblkArea * 4, cudaMemcpyHostToDevice));
+        GB_CHECK(cudaMemcpy(base + kOffJobs, jobs, n * sizeof(T1Job), cudaMemcpyHostToDevice));
+        GB_CHECK(cudaMemcpy(base + kOffSlope, &slope, 4, cudaMemcpyHostToDevice));
+        GB_CHECK(cudaMemset(base + kOffCtl, 0, 64));
+        t1Encode(L, 0);
+        GB_CHECK(cudaDeviceSynchronize());
+        uint32_t ctl[4];
+        GB_CHECK(cudaMemcpy(ctl, base + kOffCtl, 16, cudaMemcpyDeviceToHost));
+        if (ctl[1]) throw std::runtime_error("Tier-1 encoder status " + std::to_string(ctl[1]));
+        GB_CHECK(cudaMemcpy(info4, base + kOffInfo, 16 * (size_t)n, cudaMemcpyDeviceToHost));
+        GB_CHECK(cudaMemcpy(passLen, base + kOffLen, (size_t)n * kMaxPasses * 4, cudaMemcpyDeviceToHost));
+        GB_CHECK(cudaMemcpy(passDist, base + kOffDist, (size_t)n * kMaxPasses * 4, cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < n; ++i)
+            if (info4[4 * i + 3] > dataStride) throw std::logic_error("dataStride too small for a codeword");
+        // codewords: the arena's block regions to the caller's rows of dataStride bytes
+        GB_CHECK(cudaMemcpy2D(data, dataStride, base + kOffCw, kRegion, std::min<size_t>(dataStride, kRegion), n,
+                              cudaMemcpyDeviceToHost));
+    });
+}
