@@ -102,6 +102,33 @@ GB_API int gb_encoder_finish(GailCudaEncoder* e);
 GB_API int gb_encoder_stage_timing(GailCudaEncoder* e, int on);
 GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
 
+/* The batched, served encoder: many frames (of any registered layouts) in flight on one
+ * GPU, their Tier-1 work batched into shared launches as they become ready (continuous
+ * batching), admission against an HBM budget. No counterpart in the reference, whose
+ * per-frame slots (src/cuda/cuda_backend.cu:870-977, driven by src/core/pipeline.cpp:170-249)
+ * each launch their own kernels; the results are the same Tier1Frame views, bit-identical.
+ *   gb_engine_create       maxBatch: most frames per Tier-1 launch; hbmBudget: device bytes for
+ *                          frames in flight (0: 90 % of the free memory)
+ *   gb_engine_add_encoder  a frame class (layout, input format, colour); frameBytes: its
+ *                          device footprint per frame in flight
+ *   gb_engine_submit       queue one frame (host memory, pinned for speed, or device memory
+ *                          with onDevice); the frame must stay valid until it is released
+ *   gb_engine_wait         the next finished frame (id -1 after timeoutMs without one), its
+ *                          Tier-1 view (valid until release), submit-to-finish latency and
+ *                          status
+ *   gb_engine_release      give the frame's slot back
+ *   gb_engine_stats        frames, batches, frames in batches, slots, slot bytes */
+typedef struct GbEngine GbEngine;
+GB_API int gb_engine_create(int device, uint64_t hbmBudget, int maxBatch, GbEngine** out);
+GB_API void gb_engine_destroy(GbEngine* e);
+GB_API int gb_engine_add_encoder(GbEngine* e, const GailCudaLayout* layout, const GailCudaEncodeSettings* settings,
+                                 int* classId, uint64_t* frameBytes);
+GB_API int gb_engine_submit(GbEngine* e, int classId, const void* frame, int onDevice, double slope, int64_t* id);
+GB_API int gb_engine_wait(GbEngine* e, int timeoutMs, int64_t* id, GailCudaTier1* out, double* latencyMs,
+                          int* frameStatus);
+GB_API int gb_engine_release(GbEngine* e, int64_t id);
+GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5);
+
 /* FNV hash of the ABI structure sizes, as the plugin table's `layout` field carries it
  * (cudaPluginLayout, src/cuda/cuda_plugin.h:208-217). */
 GB_API uint64_t gb_plugin_layout_hash(void);

@@ -38,15 +38,14 @@ GB_API int gb_t1_encode_blocks(const uint32_t* coeffs, const int32_t* geom4, uin
         if (n == 0) return;
         ensureDevice();
         std::vector<T1Job> jobs(n);
+        std::vector<uint64_t> offset(n);
         uint64_t region = 0;
         for (uint32_t i = 0; i < n; ++i) {
             const int w = geom4[4 * i], h = geom4[4 * i + 1], orient = geom4[4 * i + 2], mp = geom4[4 * i + 3];
             if (w < 1 || w > 32 || h < 1 || h > 32 || orient < 0 || orient > 3 || mp < 0 || mp > 64)
                 throw std::logic_error("code-block geometry out of range");
-            const uint32_t cap = t1SymbolBound(w, h, kMaxPlanes);
-            jobs[i] = {i, (uint32_t)region, cap, t1Geom(w, h, orient, mp, 0), distScale ? distScale[i] : 1.f, {0, 0, 0}};
-            region += cap;
-            if (region > 0xFFFFFFFFull) throw std::logic_error("too many code-blocks in one call");
+            offset[i] = region;
+            region += t1SymbolBound(w, h, kMaxPlanes);
         }
         DevBuf<uint32_t> dCoeffs((size_t)n * kCblkArea), dInfo(4 * (size_t)n), dEnd((size_t)n * kMaxPasses),
             dLen((size_t)n * kMaxPasses), dPerm(n), dCtl(4);
@@ -55,12 +54,16 @@ GB_API int gb_t1_encode_blocks(const uint32_t* coeffs, const int32_t* geom4, uin
         DevBuf<uint8_t> dSym(region), dCw(region);
         DevBuf<T1Job> dJobs(n);
         DevBuf<float> dSlope(1);
+        for (uint32_t i = 0; i < n; ++i) {
+            const int w = geom4[4 * i], h = geom4[4 * i + 1], orient = geom4[4 * i + 2], mp = geom4[4 * i + 3];
+            jobs[i] = {dCoeffs.p + (size_t)i * kCblkArea, dSym.p + offset[i], dCw.p + offset[i],
+                       t1SymbolBound(w, h, kMaxPlanes), t1Geom(w, h, orient, mp), distScale ? distScale[i] : 1.f, 0, {0, 0}};
+        }
         GB_CHECK(cudaMemcpy(dCoeffs.p, coeffs, (size_t)n * kCblkArea * 4, cudaMemcpyHostToDevice));
         GB_CHECK(cudaMemcpy(dJobs.p, jobs.data(), n * sizeof(T1Job), cudaMemcpyHostToDevice));
         GB_CHECK(cudaMemcpy(dSlope.p, &slope, 4, cudaMemcpyHostToDevice));
         GB_CHECK(cudaMemset(dCtl.p, 0, 16));
-        T1Launch L{dCoeffs.p, dJobs.p, n, dSym.p, dCw.p, dInfo.p, dEnd.p, dLen.p, dDist.p, dSnaps.p, dPerm.p, dCtl.p,
-                   dSlope.p};
+        T1Launch L{dJobs.p, n, dInfo.p, dEnd.p, dLen.p, dDist.p, dSnaps.p, dPerm.p, dCtl.p, dSlope.p};
         t1Encode(L, 0);
         GB_CHECK(cudaDeviceSynchronize());
         uint32_t ctl[4];
@@ -74,7 +77,7 @@ GB_API int gb_t1_encode_blocks(const uint32_t* coeffs, const int32_t* geom4, uin
         for (uint32_t i = 0; i < n; ++i) {
             const uint32_t len = info4[4 * i + 3];
             if (len > dataStride) throw std::logic_error("dataStride too small for a codeword");
-            std::memcpy(data + (size_t)i * dataStride, cw.data() + jobs[i].region, len);
+            std::memcpy(data + (size_t)i * dataStride, cw.data() + offset[i], len);
         }
     });
 }

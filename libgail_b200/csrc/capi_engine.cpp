@@ -1,0 +1,68 @@
+// C-ABI of the batched, served encode engine (engine.h).
+#include <memory>
+
+#include "capi_util.h"
+#include "engine.h"
+#include "gail_b200.h"
+
+struct GbEngine {
+    std::unique_ptr<gb::EncodeEngine> e;
+};
+
+using namespace gb;
+
+extern "C" {
+
+GB_API int gb_engine_create(int device, uint64_t hbmBudget, int maxBatch, GbEngine** out) {
+    return gbGuard([&] {
+        if (!out) throw std::logic_error("null argument");
+        auto g = std::make_unique<GbEngine>();
+        g->e = std::make_unique<EncodeEngine>(device, hbmBudget, maxBatch);
+        *out = g.release();
+    });
+}
+
+GB_API void gb_engine_destroy(GbEngine* e) { delete e; }
+
+GB_API int gb_engine_add_encoder(GbEngine* e, const GailCudaLayout* layout, const GailCudaEncodeSettings* settings,
+                                 int* classId, uint64_t* frameBytes) {
+    return gbGuard([&] {
+        if (!e || !layout || !settings || !classId) throw std::logic_error("null argument");
+        *classId = e->e->addClass(*layout, *settings, frameBytes);
+    });
+}
+
+GB_API int gb_engine_submit(GbEngine* e, int classId, const void* frame, int onDevice, double slope, int64_t* id) {
+    return gbGuard([&] {
+        if (!e || !id) throw std::logic_error("null argument");
+        *id = e->e->submit(classId, frame, onDevice != 0, slope);
+    });
+}
+
+GB_API int gb_engine_wait(GbEngine* e, int timeoutMs, int64_t* id, GailCudaTier1* out, double* latencyMs, int* frameStatus) {
+    return gbGuard([&] {
+        if (!e || !id || !out || !latencyMs || !frameStatus) throw std::logic_error("null argument");
+        if (!e->e->wait(timeoutMs, id, out, latencyMs, frameStatus)) *id = -1;
+    });
+}
+
+GB_API int gb_engine_release(GbEngine* e, int64_t id) {
+    return gbGuard([&] {
+        if (!e) throw std::logic_error("null argument");
+        e->e->release(id);
+    });
+}
+
+GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5) {
+    return gbGuard([&] {
+        if (!e || !out5) throw std::logic_error("null argument");
+        const EncodeEngine::Stats s = e->e->stats();
+        out5[0] = s.frames;
+        out5[1] = s.batches;
+        out5[2] = s.batchFrames;
+        out5[3] = s.slots;
+        out5[4] = s.slotBytes;
+    });
+}
+
+}  // extern "C"

@@ -82,9 +82,16 @@ __global__ void __launch_bounds__(256) packKernel(CompactArgs a) {
             a.outPassDist[pOff + lane + 32] = a.passDist[(size_t)i * kMaxPasses + lane + 32];
         }
         const uint32_t words = (len + 3u) >> 2;
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.cw + a.jobs[i].region);
+        if ((uint64_t)dOff + words * 4ull > a.dataCap) {
+            if (lane == 0) a.tot[2] = 1u;
+            continue;
+        }
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.jobs[i].cw);
         uint32_t* dst = reinterpret_cast<uint32_t*>(a.outData + dOff);
-        for (uint32_t k = lane; k < words; k += 32) dst[k] = src[k];
+        // whole words; the bytes past the codeword in its last word are zeroed so that the
+        // packed frame does not depend on what the region held before
+        const uint32_t tailMask = (len & 3u) ? (1u << (8 * (len & 3u))) - 1u : 0xFFFFFFFFu;
+        for (uint32_t k = lane; k < words; k += 32) dst[k] = k == words - 1 ? src[k] & tailMask : src[k];
     }
 }
 

@@ -13,13 +13,13 @@ struct CompactArgs {
     const uint32_t* info;      // 4 words per block (nbps, passes, decisions, bytes)
     const uint32_t* passLen;   // 64 per block
     const int32_t* passDist;   // 64 per block
-    const uint8_t* cw;         // codeword arena
     const T1Job* jobs;         // each block's codeword region
     uint32_t* outInfo;         // 5 words per block: CblkInfo
     uint32_t* outPassLen;
     int32_t* outPassDist;
     uint8_t* outData;
-    uint32_t* tot;             // [0] data bytes, [1] passes
+    uint32_t* tot;             // [0] data bytes, [1] passes, [2] set when outData was too small
+    uint64_t dataCap;          // bytes outData holds
 };
 
 void compactTier1(const CompactArgs& a, cudaStream_t st);

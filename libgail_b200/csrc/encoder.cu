@@ -34,7 +34,7 @@ BandOut bandOut(const GbSubband& b) {
 
 uint64_t SlotSizes::deviceBytes() const {
     const uint64_t sizes[] = {inBytes,     65536 * 4,   4096 * 4,    2 * llFloats * 4 * 3, n * kCblkArea * 4,
-                              n * 32,      arena,       arena,       n * 16,               n * kMaxPasses * 4 * 3,
+                              n * 48,      arena,       arena,       n * 16,               n * kMaxPasses * 4 * 3,
                               n * kMaxPasses * 16,      n * 4,       64,                   n * 20,
                               n * kMaxPasses * 8,       arena};
     uint64_t t = 0;
@@ -42,19 +42,57 @@ uint64_t SlotSizes::deviceBytes() const {
     return t;
 }
 
-uint64_t buildJobs(const Layout& L, int frame, uint32_t coeffBase, uint64_t regionBase, std::vector<T1Job>& jobs) {
-    uint64_t region = regionBase;
+uint64_t buildJobs(const Layout& L, const uint32_t* coeffs, uint8_t* sym, uint8_t* cw, uint32_t slope,
+                   std::vector<T1Job>& jobs) {
+    uint64_t region = 0;
     for (int i = 0; i < L.numCblks(); ++i) {
         const CodeBlock& cb = L.cblks[i];
         const GbSubband& b = L.bands[cb.band];
         const uint32_t cap = t1SymbolBound(cb.w, cb.h, std::max(1, std::min(b.Mb, kMaxPlanes)));
         const float dscale = (float)((double)b.delta * b.delta * b.weight);
-        jobs.push_back({coeffBase + (uint32_t)i, (uint32_t)region, cap, t1Geom(cb.w, cb.h, b.orient, kMaxPasses, frame),
-                        dscale, {0, 0, 0}});
+        jobs.push_back({coeffs ? coeffs + (size_t)i * kCblkArea : nullptr, sym ? sym + region : nullptr,
+                        cw ? cw + region : nullptr, cap, t1Geom(cb.w, cb.h, b.orient, kMaxPasses), dscale, slope, {0, 0}});
         region += cap;
-        if (region > 0xFFFFFFFFull) throw std::runtime_error("Tier-1 arena beyond 4 GiB");
     }
-    return region - regionBase;
+    return region;
+}
+
+void launchFrontEnd(const Layout& L, const ColorArgs& c, float* ll0, float* ll1, uint64_t llFloats, uint32_t* coeffs,
+                    float* tap, cudaStream_t st) {
+    const int NL = L.levels;
+    float* llBuf[2] = {ll0, ll1};
+    for (int l = 1; l <= NL; ++l) {
+        LevelArgs a{};
+        a.w = L.levelW(l - 1);
+        a.h = L.levelH(l - 1);
+        a.src = l == 1 ? nullptr : llBuf[(l - 1) & 1];
+        a.srcStride = L.levelW(1);
+        a.srcComp = llFloats;
+        a.last = l == NL;
+        a.ll = a.last ? nullptr : llBuf[l & 1];
+        a.llStride = L.levelW(1);
+        a.llComp = llFloats;
+        a.coeffs = coeffs;
+        a.tap = tap;
+        a.tapStride = L.width;
+        a.tapComp = (uint64_t)L.width * L.height;
+        const int r = NL - l + 1;
+        for (int comp = 0; comp < 3; ++comp) {
+            for (int o = 1; o <= 3; ++o) a.band[comp][o] = bandOut(L.bands[L.bandIndex(comp, r, o)]);
+            if (a.last) {
+                a.band[comp][0] = bandOut(L.bands[L.bandIndex(comp, 0, 0)]);
+            } else {
+                BandOut& b = a.band[comp][0];
+                b = BandOut{};
+                b.w = L.levelW(l);
+                b.h = L.levelH(l);
+                b.ncbx = (b.w + 31) / 32;
+                b.ncby = (b.h + 31) / 32;
+            }
+        }
+        if (l == 1) launchLevel1(c, a, st);
+        else launchLevel(a, st);
+    }
 }
 
 SlotSizes slotSizes(const Layout& L, const GbFrameFormat& in) {
@@ -63,7 +101,7 @@ SlotSizes slotSizes(const Layout& L, const GbFrameFormat& in) {
     z.n = (uint64_t)L.numCblks();
     z.inBytes = frameBytes(in);
     std::vector<T1Job> jobs;
-    z.arena = buildJobs(L, 0, 0, 0, jobs);
+    z.arena = buildJobs(L, nullptr, nullptr, nullptr, 0, jobs);
     z.llFloats = (uint64_t)L.levelW(1) * L.levelH(1);
     return z;
 }
@@ -80,8 +118,6 @@ EncoderSlot::EncoderSlot(int device, const Layout& L, const GailCudaEncodeSettin
     color_ = buildColorTables(s.color);
     std::memcpy(m_, color_.m, sizeof m_);
     z_ = slotSizes(L, s.input);
-    jobs_.clear();
-    buildJobs(L_, 0, 0, 0, jobs_);
     try {
         GB_CHECK(cudaSetDevice(dev_));
         GB_CHECK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
@@ -114,6 +150,8 @@ EncoderSlot::EncoderSlot(int device, const Layout& L, const GailCudaEncodeSettin
         alloc(dOutLen_, n * kMaxPasses * 4);
         alloc(dOutDist_, n * kMaxPasses * 4);
         alloc(dOutData_, z_.arena);
+        jobs_.clear();
+        buildJobs(L_, dCoeffs_, dSym_, dCw_, 0, jobs_);
         auto pinned = [&](auto*& p, uint64_t bytes) {
             void* q = nullptr;
             check(cudaHostAlloc(&q, std::max<uint64_t>(bytes, 16), cudaHostAllocDefault), "pinned host memory");
@@ -198,47 +236,16 @@ void EncoderSlot::enqueueStages(const void* dFrame, bool taps, bool full) {
     c.thr = dThr_;
     std::memcpy(c.m, m_, sizeof m_);
     c.xyz = taps ? dXyz_ : nullptr;
-    const int NL = L_.levels;
-    for (int l = 1; l <= NL; ++l) {
-        LevelArgs a{};
-        a.w = L_.levelW(l - 1);
-        a.h = L_.levelH(l - 1);
-        a.src = l == 1 ? nullptr : dLL_[(l - 1) & 1];
-        a.srcStride = L_.levelW(1);
-        a.srcComp = z_.llFloats;
-        a.last = l == NL;
-        a.ll = a.last ? nullptr : dLL_[l & 1];
-        a.llStride = L_.levelW(1);
-        a.llComp = z_.llFloats;
-        a.coeffs = dCoeffs_;
-        a.tap = full ? dTap_ : nullptr;
-        a.tapStride = L_.width;
-        a.tapComp = npix;
-        const int r = NL - l + 1;
-        for (int comp = 0; comp < 3; ++comp) {
-            for (int o = 1; o <= 3; ++o) a.band[comp][o] = bandOut(L_.bands[L_.bandIndex(comp, r, o)]);
-            if (a.last) {
-                a.band[comp][0] = bandOut(L_.bands[L_.bandIndex(comp, 0, 0)]);
-            } else {
-                BandOut& ll = a.band[comp][0];
-                ll = BandOut{};
-                ll.w = L_.levelW(l);
-                ll.h = L_.levelH(l);
-                ll.ncbx = (ll.w + 31) / 32;
-                ll.ncby = (ll.h + 31) / 32;
-            }
-        }
-        if (l == 1) launchLevel1(c, a, st);
-        else launchLevel(a, st);
-    }
+    launchFrontEnd(L_, c, dLL_[0], dLL_[1], z_.llFloats, dCoeffs_, full ? dTap_ : nullptr, st);
     GB_CHECK(cudaEventRecord(ev_[2], st));
     if (mark) GB_CHECK(cudaEventRecord(mark[1], st));
     const uint64_t n = z_.n;
-    T1Launch t{dCoeffs_, dJobs_, (uint32_t)n, dSym_, dCw_, dInfo_, dEnd_, dLen_, dDist_, dSnaps_, dPerm_, dCtl_, dSlope_};
+    T1Launch t{dJobs_, (uint32_t)n, dInfo_, dEnd_, dLen_, dDist_, dSnaps_, dPerm_, dCtl_, dSlope_};
     t1Encode(t, st, mark ? mark + 2 : nullptr);
     GB_CHECK(cudaEventRecord(ev_[3], st));
     if (mark) GB_CHECK(cudaEventRecord(mark[4], st));
-    CompactArgs ca{(uint32_t)n, dInfo_, dLen_, dDist_, dCw_, dJobs_, dOutInfo_, dOutLen_, dOutDist_, dOutData_, dCtl_ + 8};
+    CompactArgs ca{(uint32_t)n, dInfo_, dLen_, dDist_, dJobs_, dOutInfo_, dOutLen_, dOutDist_, dOutData_, dCtl_ + 8,
+                   z_.arena};
     compactTier1(ca, st);
     if (mark) GB_CHECK(cudaEventRecord(mark[5], st));
 }

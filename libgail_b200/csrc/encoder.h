@@ -10,6 +10,7 @@
 
 #include "color.h"
 #include "compact.cuh"
+#include "frontend.cuh"
 #include "gail_cuda_plugin_abi.h"
 #include "layout.h"
 #include "t1_encode.cuh"
@@ -23,9 +24,18 @@ struct SlotSizes {
 };
 SlotSizes slotSizes(const Layout& L, const GbFrameFormat& in);
 
-// The Tier-1 job table of a layout: per block its coefficient block, its symbol/codeword
-// region (sized for Mb bit-planes) and geometry; returns the arena size.
-uint64_t buildJobs(const Layout& L, int frame, uint32_t coeffBase, uint64_t regionBase, std::vector<T1Job>& jobs);
+// Appends the Tier-1 jobs of one frame: per block its coefficient words (coeffs + 1024 i),
+// its decision and codeword regions (sym / cw + offset, sized for the band's Mb
+// bit-planes), geometry and slope index. Returns the arena size one frame needs; with
+// NULL buffers it only counts.
+uint64_t buildJobs(const Layout& L, const uint32_t* coeffs, uint8_t* sym, uint8_t* cw, uint32_t slope,
+                   std::vector<T1Job>& jobs);
+
+// Enqueues the front end of one frame on st: colour + level 1 from c.src, then the deeper
+// levels through the LL ping-pong buffers (3 x llFloats each), quantised words into coeffs
+// (code-block-major), float planes into tap when not NULL.
+void launchFrontEnd(const Layout& L, const ColorArgs& c, float* ll0, float* ll1, uint64_t llFloats, uint32_t* coeffs,
+                    float* tap, cudaStream_t st);
 
 class EncoderSlot {
 public:

@@ -1,0 +1,431 @@
+// The batched, served encode engine (see engine.h).
+#include "engine.h"
+
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "capi_util.h"
+#include "common.cuh"
+#include "compact.cuh"
+#include "frontend.cuh"
+
+namespace gb {
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double msBetween(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+}  // namespace
+
+struct EncodeEngine::Class {
+    Layout L;
+    GailCudaEncodeSettings s;
+    SlotSizes z;
+    ColorTables color;
+    ColorArgs colorArgs{};
+    float* dEotf = nullptr;
+    float* dThr = nullptr;
+    float* dLL[2] = {nullptr, nullptr};
+    uint64_t slotBytes = 0, dataCap = 0;
+    std::vector<Slot*> free;
+    std::vector<void*> dev;
+};
+
+struct EncodeEngine::Slot {
+    int cls = 0, index = 0;
+    uint8_t* dIn = nullptr;
+    uint32_t* dCoeffs = nullptr;
+    uint8_t *dSym = nullptr, *dCw = nullptr;
+    T1Job* dJobs = nullptr;
+    uint32_t n = 0;
+    // the packed Tier-1 frame, written by the device straight into mapped host memory
+    uint32_t *hInfo = nullptr, *hLen = nullptr, *hTot = nullptr;
+    int32_t* hDist = nullptr;
+    uint8_t* hData = nullptr;
+    uint64_t dataCap = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t frontDone = nullptr;
+    std::vector<void*> dev, host;
+};
+
+struct EncodeEngine::Request {
+    int64_t id = 0;
+    int cls = 0;
+    const void* frame = nullptr;
+    bool onDevice = false;
+    double slope = 0;
+    Clock::time_point t0;
+    double latency = 0;
+    Slot* slot = nullptr;
+    uint32_t jobBase = 0;
+    int status = 0;
+};
+
+struct EncodeEngine::Batch {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    T1Job* dJobs = nullptr;
+    uint32_t *info = nullptr, *end = nullptr, *len = nullptr, *perm = nullptr, *ctl = nullptr, *hCtl = nullptr;
+    int32_t* dist = nullptr;
+    uint4* snaps = nullptr;
+    uint32_t cap = 0;
+    std::vector<Request*> frames;
+    bool busy = false;
+    std::vector<void*> dev;
+};
+
+EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(device), maxBatch_(std::max(1, maxBatch)) {
+    GB_CHECK(cudaSetDevice(dev_));
+    ensureDevice();
+    if (hbmBudget == 0) {
+        size_t f = 0, t = 0;
+        GB_CHECK(cudaMemGetInfo(&f, &t));
+        hbmBudget = (uint64_t)(f * 0.9);
+    }
+    budget_ = hbmBudget;
+    GB_CHECK(cudaStreamCreateWithFlags(&front_, cudaStreamNonBlocking));
+    constexpr int kMaxSlots = 1024;
+    check(cudaMalloc(&dSlope_, kMaxSlots * 4), "device memory for the engine");
+    check(cudaHostAlloc((void**)&hSlope_, kMaxSlots * 4, cudaHostAllocDefault), "pinned host memory");
+    for (int i = 0; i < 2; ++i) batches_.push_back(std::make_unique<Batch>());
+    for (auto& b : batches_) {
+        GB_CHECK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+        GB_CHECK(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+        check(cudaHostAlloc((void**)&b->hCtl, 64, cudaHostAllocDefault), "pinned host memory");
+    }
+    worker_ = std::thread([this] { run(); });
+}
+
+EncodeEngine::~EncodeEngine() {
+    stop_ = true;
+    cvWork_.notify_all();
+    if (worker_.joinable()) worker_.join();
+    cudaSetDevice(dev_);
+    cudaDeviceSynchronize();
+    for (auto& s : slots_) {
+        if (s->exec) cudaGraphExecDestroy(s->exec);
+        if (s->graph) cudaGraphDestroy(s->graph);
+        if (s->frontDone) cudaEventDestroy(s->frontDone);
+        for (void* p : s->dev) cudaFree(p);
+        for (void* p : s->host) cudaFreeHost(p);
+    }
+    for (auto& c : classes_)
+        for (void* p : c->dev) cudaFree(p);
+    for (auto& b : batches_) {
+        for (void* p : b->dev) cudaFree(p);
+        if (b->hCtl) cudaFreeHost(b->hCtl);
+        if (b->done) cudaEventDestroy(b->done);
+        if (b->st) cudaStreamDestroy(b->st);
+    }
+    if (dSlope_) cudaFree(dSlope_);
+    if (hSlope_) cudaFreeHost(hSlope_);
+    if (front_) cudaStreamDestroy(front_);
+    cudaGetLastError();
+}
+
+int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSettings& s, uint64_t* frameBytes) {
+    GB_CHECK(cudaSetDevice(dev_));
+    auto c = std::make_unique<Class>();
+    layoutFromAbi(layout, c->L);
+    if (c->L.levels < 1) throw std::logic_error("the encoder needs at least one decomposition level");
+    if (s.input.width != c->L.width || s.input.height != c->L.height)
+        throw std::logic_error("input frame size differs from the layout");
+    c->s = s;
+    c->z = slotSizes(c->L, s.input);
+    c->color = buildColorTables(s.color);
+    auto alloc = [&](auto*& p, uint64_t bytes) {
+        void* q = nullptr;
+        check(cudaMalloc(&q, std::max<uint64_t>(bytes, 16)), "device memory for the engine");
+        c->dev.push_back(q);
+        p = static_cast<std::remove_reference_t<decltype(p)>>(q);
+    };
+    alloc(c->dEotf, 65536 * 4);
+    alloc(c->dThr, 4096 * 4);
+    alloc(c->dLL[0], c->z.llFloats * 12);
+    alloc(c->dLL[1], c->z.llFloats * 12);
+    GB_CHECK(cudaMemcpy(c->dEotf, c->color.eotf.data(), 65536 * 4, cudaMemcpyHostToDevice));
+    GB_CHECK(cudaMemcpy(c->dThr, c->color.thr.data(), 4096 * 4, cudaMemcpyHostToDevice));
+    ColorArgs& a = c->colorArgs;
+    a.kind = s.input.kind == GB_FRAME_PLANAR ? 1 : 0;
+    a.pp = planarParams(s.input);
+    a.eotf = c->dEotf;
+    a.thr = c->dThr;
+    std::memcpy(a.m, c->color.m, sizeof a.m);
+    a.xyz = nullptr;
+    const uint64_t n = c->z.n, npix = c->z.npix;
+    // packed output bound: codewords of 6 bytes per sample would be beyond any 12-bit content
+    c->dataCap = std::min<uint64_t>(c->z.arena, npix * 6 + (64u << 10));
+    c->slotBytes = c->z.inBytes + n * kCblkArea * 4 + 2 * c->z.arena + n * sizeof(T1Job);
+    if (frameBytes) *frameBytes = c->slotBytes;
+    std::lock_guard<std::mutex> lock(m_);
+    classes_.push_back(std::move(c));
+    return (int)classes_.size() - 1;
+}
+
+EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
+    if (used_ + c.slotBytes > budget_) return nullptr;
+    auto s = std::make_unique<Slot>();
+    s->cls = (int)(std::find_if(classes_.begin(), classes_.end(), [&](auto& p) { return p.get() == &c; }) - classes_.begin());
+    s->index = (int)slots_.size();
+    if (s->index >= 1024) return nullptr;
+    s->n = (uint32_t)c.z.n;
+    auto alloc = [&](auto*& p, uint64_t bytes) {
+        void* q = nullptr;
+        check(cudaMalloc(&q, std::max<uint64_t>(bytes, 16)), "device memory for a frame slot");
+        s->dev.push_back(q);
+        p = static_cast<std::remove_reference_t<decltype(p)>>(q);
+    };
+    auto mapped = [&](auto*& p, uint64_t bytes) {
+        void* q = nullptr;
+        check(cudaHostAlloc(&q, std::max<uint64_t>(bytes, 16), cudaHostAllocMapped | cudaHostAllocPortable),
+              "pinned host memory for a frame slot");
+        s->host.push_back(q);
+        p = static_cast<std::remove_reference_t<decltype(p)>>(q);
+    };
+    try {
+        alloc(s->dIn, c.z.inBytes);
+        alloc(s->dCoeffs, (uint64_t)s->n * kCblkArea * 4);
+        alloc(s->dSym, c.z.arena);
+        alloc(s->dCw, c.z.arena);
+        alloc(s->dJobs, (uint64_t)s->n * sizeof(T1Job));
+        mapped(s->hInfo, (uint64_t)s->n * 20);
+        mapped(s->hLen, (uint64_t)s->n * kMaxPasses * 4);
+        mapped(s->hDist, (uint64_t)s->n * kMaxPasses * 4);
+        mapped(s->hData, c.dataCap);
+        mapped(s->hTot, 64);
+        s->dataCap = c.dataCap;
+        std::vector<T1Job> jobs;
+        buildJobs(c.L, s->dCoeffs, s->dSym, s->dCw, (uint32_t)s->index, jobs);
+        GB_CHECK(cudaMemcpy(s->dJobs, jobs.data(), jobs.size() * sizeof(T1Job), cudaMemcpyHostToDevice));
+        GB_CHECK(cudaEventCreateWithFlags(&s->frontDone, cudaEventDisableTiming));
+        // the slot's front end as one graph: it always reads the slot's input buffer and
+        // writes the slot's coefficient buffer
+        cudaStream_t cap;
+        GB_CHECK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        ColorArgs a = c.colorArgs;
+        a.src = s->dIn;
+        GB_CHECK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        launchFrontEnd(c.L, a, c.dLL[0], c.dLL[1], c.z.llFloats, s->dCoeffs, nullptr, cap);
+        GB_CHECK(cudaStreamEndCapture(cap, &s->graph));
+        GB_CHECK(cudaStreamDestroy(cap));
+        GB_CHECK(cudaGraphInstantiate(&s->exec, s->graph, 0));
+    } catch (...) {
+        for (void* p : s->dev) cudaFree(p);
+        for (void* p : s->host) cudaFreeHost(p);
+        if (s->exec) cudaGraphExecDestroy(s->exec);
+        if (s->graph) cudaGraphDestroy(s->graph);
+        if (s->frontDone) cudaEventDestroy(s->frontDone);
+        cudaGetLastError();
+        return nullptr;  // out of memory now: the request waits for a slot to free up
+    }
+    used_ += c.slotBytes;
+    Slot* raw = s.get();
+    slots_.push_back(std::move(s));
+    std::lock_guard<std::mutex> lock(m_);
+    stats_.slots = slots_.size();
+    stats_.slotBytes = used_;
+    return raw;
+}
+
+int64_t EncodeEngine::submit(int cls, const void* frame, bool onDevice, double slope) {
+    if (!frame) throw std::logic_error("no frame");
+    std::lock_guard<std::mutex> lock(m_);
+    if (cls < 0 || cls >= (int)classes_.size()) throw std::logic_error("unknown frame class");
+    if (!error_.empty()) throw std::runtime_error(error_);
+    auto r = std::make_unique<Request>();
+    r->id = nextId_++;
+    r->cls = cls;
+    r->frame = frame;
+    r->onDevice = onDevice;
+    r->slope = slope;
+    r->t0 = Clock::now();
+    pending_.push_back(r.get());
+    requests_.push_back(std::move(r));
+    cvWork_.notify_one();
+    return requests_.back()->id;
+}
+
+bool EncodeEngine::wait(int timeoutMs, int64_t* id, GailCudaTier1* out, double* latencyMs, int* status) {
+    std::unique_lock<std::mutex> lock(m_);
+    if (!cvDone_.wait_for(lock, std::chrono::milliseconds(timeoutMs), [&] { return !done_.empty() || !error_.empty(); }))
+        return false;
+    if (done_.empty()) throw std::runtime_error(error_);
+    Request* r = done_.front();
+    done_.pop_front();
+    *id = r->id;
+    *latencyMs = r->latency;
+    *status = r->status;
+    const Slot* s = r->slot;
+    *out = {reinterpret_cast<const GbCblkInfo*>(s->hInfo), s->hLen, s->hDist, s->hData, s->n, s->hTot[1], s->hTot[0]};
+    return true;
+}
+
+void EncodeEngine::release(int64_t id) {
+    std::lock_guard<std::mutex> lock(m_);
+    if (id < 0 || id >= (int64_t)requests_.size() || !requests_[id]) throw std::logic_error("unknown request");
+    Request* r = requests_[id].get();
+    if (!r->slot) throw std::logic_error("request not finished");
+    classes_[r->cls]->free.push_back(r->slot);
+    requests_[id].reset();
+    cvWork_.notify_one();
+}
+
+EncodeEngine::Stats EncodeEngine::stats() const {
+    std::lock_guard<std::mutex> lock(m_);
+    return stats_;
+}
+
+bool EncodeEngine::admit() {
+    bool progress = false;
+    for (;;) {
+        Request* r;
+        Slot* s = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            if (pending_.empty()) break;
+            r = pending_.front();
+            Class& c = *classes_[r->cls];
+            if (!c.free.empty()) {
+                s = c.free.back();
+                c.free.pop_back();
+            }
+        }
+        if (!s) s = newSlot(*classes_[r->cls]);
+        if (!s) break;  // first in, first admitted: later requests wait too
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            pending_.pop_front();
+        }
+        Class& c = *classes_[r->cls];
+        r->slot = s;
+        hSlope_[s->index] = (float)r->slope;
+        GB_CHECK(cudaMemcpyAsync(dSlope_ + s->index, hSlope_ + s->index, 4, cudaMemcpyHostToDevice, front_));
+        GB_CHECK(cudaMemcpyAsync(s->dIn, r->frame, c.z.inBytes, r->onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 front_));
+        GB_CHECK(cudaGraphLaunch(s->exec, front_));
+        GB_CHECK(cudaEventRecord(s->frontDone, front_));
+        std::lock_guard<std::mutex> lock(m_);
+        front_q_.push_back(r);
+        progress = true;
+    }
+    return progress;
+}
+
+bool EncodeEngine::launchBatch(Batch& b) {
+    std::vector<Request*> sel;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        if (front_q_.empty()) return false;
+        const bool otherBusy = std::any_of(batches_.begin(), batches_.end(), [&](auto& x) { return x.get() != &b && x->busy; });
+        for (Request* r : front_q_) {
+            if ((int)sel.size() >= maxBatch_) break;
+            if (cudaEventQuery(r->slot->frontDone) != cudaSuccess) break;  // in order: later ones are not done either
+            sel.push_back(r);
+        }
+        // while the other batch keeps the GPU busy, let small batches grow a little
+        if (sel.empty() || (otherBusy && (int)sel.size() < std::max(1, maxBatch_ / 4) &&
+                            msBetween(front_q_.front()->t0, Clock::now()) < 2.0 && sel.size() < front_q_.size()))
+            return false;
+        front_q_.erase(front_q_.begin(), front_q_.begin() + (long)sel.size());
+    }
+    uint64_t total = 0;
+    for (Request* r : sel) total += r->slot->n;
+    if (total > b.cap) {
+        // grow the batch's tables (kept for later batches)
+        for (void* p : b.dev) cudaFree(p);
+        b.dev.clear();
+        const uint64_t cap = std::max<uint64_t>(total, (uint64_t)b.cap * 2);
+        auto alloc = [&](auto*& p, uint64_t bytes) {
+            void* q = nullptr;
+            check(cudaMalloc(&q, std::max<uint64_t>(bytes, 16)), "device memory for a Tier-1 batch");
+            b.dev.push_back(q);
+            p = static_cast<std::remove_reference_t<decltype(p)>>(q);
+        };
+        alloc(b.dJobs, cap * sizeof(T1Job));
+        alloc(b.info, cap * 16);
+        alloc(b.end, cap * kMaxPasses * 4);
+        alloc(b.len, cap * kMaxPasses * 4);
+        alloc(b.dist, cap * kMaxPasses * 4);
+        alloc(b.snaps, cap * kMaxPasses * 16);
+        alloc(b.perm, cap * 4);
+        alloc(b.ctl, 64);
+        b.cap = (uint32_t)cap;
+    }
+    uint32_t base = 0;
+    for (Request* r : sel) {
+        GB_CHECK(cudaStreamWaitEvent(b.st, r->slot->frontDone, 0));
+        GB_CHECK(cudaMemcpyAsync(b.dJobs + base, r->slot->dJobs, (uint64_t)r->slot->n * sizeof(T1Job),
+                                 cudaMemcpyDeviceToDevice, b.st));
+        r->jobBase = base;
+        base += r->slot->n;
+    }
+    GB_CHECK(cudaMemsetAsync(b.ctl, 0, 64, b.st));
+    T1Launch L{b.dJobs, (uint32_t)total, b.info, b.end, b.len, b.dist, b.snaps, b.perm, b.ctl, dSlope_};
+    t1Encode(L, b.st);
+    for (Request* r : sel) {
+        Slot* s = r->slot;
+        std::memset(s->hTot, 0, 64);
+        const uint32_t j = r->jobBase;
+        CompactArgs ca{s->n,   b.info + 4 * (uint64_t)j, b.len + (uint64_t)kMaxPasses * j, b.dist + (uint64_t)kMaxPasses * j,
+                       b.dJobs + j, s->hInfo, s->hLen, s->hDist, s->hData, s->hTot, s->dataCap};
+        compactTier1(ca, b.st);
+    }
+    GB_CHECK(cudaMemcpyAsync(b.hCtl, b.ctl, 64, cudaMemcpyDeviceToHost, b.st));
+    GB_CHECK(cudaEventRecord(b.done, b.st));
+    b.frames = std::move(sel);
+    b.busy = true;
+    std::lock_guard<std::mutex> lock(m_);
+    stats_.batches++;
+    stats_.batchFrames += b.frames.size();
+    return true;
+}
+
+bool EncodeEngine::collect(Batch& b) {
+    if (!b.busy) return false;
+    const cudaError_t e = cudaEventQuery(b.done);
+    if (e == cudaErrorNotReady) return false;
+    GB_CHECK(e);
+    const auto now = Clock::now();
+    const uint32_t status = b.hCtl[1];
+    std::lock_guard<std::mutex> lock(m_);
+    for (Request* r : b.frames) {
+        r->latency = msBetween(r->t0, now);
+        r->status = (status || r->slot->hTot[2]) ? kError : kOk;
+        done_.push_back(r);
+        stats_.frames++;
+    }
+    b.frames.clear();
+    b.busy = false;
+    return true;
+}
+
+void EncodeEngine::run() {
+    try {
+        GB_CHECK(cudaSetDevice(dev_));
+        while (!stop_) {
+            bool did = admit();
+            bool finished = false;
+            for (auto& b : batches_) finished |= collect(*b);
+            for (auto& b : batches_)
+                if (!b->busy) did |= launchBatch(*b);
+            if (finished) cvDone_.notify_all();
+            if (!did && !finished) {
+                std::unique_lock<std::mutex> lock(m_);
+                cvWork_.wait_for(lock, std::chrono::microseconds(50));
+            }
+        }
+    } catch (const std::exception& ex) {
+        std::lock_guard<std::mutex> lock(m_);
+        error_ = ex.what();
+        cvDone_.notify_all();
+    }
+}
+
+}  // namespace gb

@@ -1,0 +1,96 @@
+// The batched, served encode path: frames of any number of profiles in flight on one GPU,
+// continuous batching of their Tier-1 work. No counterpart in the reference (whose
+// per-frame slots each run their own launches); it sits beside the plain path of
+// encoder.h, which stays the drop-in and the comparison.
+//
+// A request's life: submit() queues it; the engine thread admits it into a frame slot
+// when one is free or the HBM budget allows a new one; the slot's front end (upload,
+// colour, wavelet, quantisation) runs as one CUDA graph on the front stream; every frame
+// whose front end has finished joins the next Tier-1 batch, one launch of the Tier-1
+// kernels over all their code-blocks (largest first across frames), with two batches in
+// flight so that one batch's serial MQ tail overlaps the next batch's work; packing
+// writes each frame's Tier1Frame straight into mapped host memory; wait() hands out
+// finished frames, release() frees their slots.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "color.h"
+#include "encoder.h"
+#include "gail_cuda_plugin_abi.h"
+#include "layout.h"
+#include "t1_encode.cuh"
+
+namespace gb {
+
+class EncodeEngine {
+public:
+    // maxBatch: most frames per Tier-1 launch; hbmBudget: device bytes the engine's frame
+    // slots may take (0: 90 % of what is free when the engine starts).
+    EncodeEngine(int device, uint64_t hbmBudget, int maxBatch);
+    ~EncodeEngine();
+    EncodeEngine(const EncodeEngine&) = delete;
+    EncodeEngine& operator=(const EncodeEngine&) = delete;
+
+    // A frame class: one layout, input format and colour setting. Returns its id and the
+    // device bytes one of its frames in flight takes.
+    int addClass(const GailCudaLayout& layout, const GailCudaEncodeSettings& s, uint64_t* frameBytes);
+    // Queues a frame of class cls: frame is host memory (pinned for a fast upload) or,
+    // with onDevice, device memory; it must stay valid until the frame is released.
+    int64_t submit(int cls, const void* frame, bool onDevice, double slope);
+    // Waits up to timeoutMs for a finished frame. Returns false on timeout. latency: ms
+    // from submit() to the end of its packing; status: 0 or a GailCudaStatus.
+    bool wait(int timeoutMs, int64_t* id, GailCudaTier1* out, double* latencyMs, int* status);
+    void release(int64_t id);
+
+    struct Stats {
+        uint64_t frames = 0, batches = 0, batchFrames = 0, slots = 0, slotBytes = 0;
+    };
+    Stats stats() const;
+
+private:
+    struct Class;
+    struct Slot;
+    struct Request;
+    struct Batch;
+
+    void run();
+    bool admit();
+    bool launchBatch(Batch& b);
+    bool collect(Batch& b);
+    Slot* newSlot(Class& c);
+
+    int dev_;
+    uint64_t budget_ = 0, used_ = 0;
+    int maxBatch_;
+    cudaStream_t front_ = nullptr;
+    std::vector<std::unique_ptr<Class>> classes_;
+    std::vector<std::unique_ptr<Slot>> slots_;
+    std::vector<std::unique_ptr<Batch>> batches_;
+    float* dSlope_ = nullptr;  // per slot
+    float* hSlope_ = nullptr;
+    std::vector<std::unique_ptr<Request>> requests_;  // owned; index = id - base
+    int64_t nextId_ = 0;
+
+    mutable std::mutex m_;
+    std::condition_variable cvDone_, cvWork_;
+    std::deque<Request*> pending_;    // submitted, not admitted
+    std::vector<Request*> front_q_;   // front end enqueued, not yet in a batch
+    std::deque<Request*> done_;       // finished, not yet handed out
+    std::atomic<bool> stop_{false};
+    std::string error_;
+    Stats stats_;
+    std::thread worker_;
+};
+
+}  // namespace gb

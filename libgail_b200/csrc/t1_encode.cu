@@ -151,11 +151,11 @@ __global__ void __launch_bounds__(CM_THREADS) t1CmKernel(T1Launch P) {
         const T1Job J = P.jobs[job];
         const int w = (J.geom & 31u) + 1, h = ((J.geom >> 5) & 31u) + 1, orient = (J.geom >> 10) & 3u;
         const int maxPasses = (J.geom >> 12) & 127u;
-        const float slope = P.slope ? P.slope[J.geom >> 19] : 0.f;
+        const float slope = P.slope ? P.slope[J.slope] : 0.f;
         const uint8_t* zc = s_zc + 45 * orient;
 
         // Load: lane x reads column x, one 128-byte row per step.
-        const uint32_t* src = P.coeffs + (size_t)J.coeff * kCblkArea;
+        const uint32_t* src = J.coeffs;
         uint32_t sgn = 0, colMax = 0;
         for (int r = 0; r < 32; ++r) {
             const uint32_t v = (lane < w && r < h) ? src[r * 32 + lane] : 0u;
@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(CM_THREADS) t1CmKernel(T1Launch P) {
         uint32_t sig = 0, refined = 0, symTotal = 0;
         int np = 0;
         const int nstripes = (h + 3) >> 2;
-        uint8_t* gsym = P.sym + J.region;
+        uint8_t* gsym = J.sym;
 
         for (int p = nbps - 1; p >= 0 && np < maxPasses; --p) {
             uint32_t Bp = 0;
@@ -579,8 +579,8 @@ __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
             }
             if (qi >= P.n) break;
             const T1Job J = P.jobs[job];
-            sym = P.sym + J.region;
-            e.out = P.cw + J.region;
+            sym = J.sym;
+            e.out = J.cw;
             e.cap = J.cap;
             e.A = 0x8000u;
             e.C = 0;

@@ -8,19 +8,21 @@
 
 namespace gb {
 
-// One code-block to code. 32 bytes, read once per block by each kernel.
+// One code-block to code, wherever its frame's buffers are: a launch can take the blocks of
+// any number of frames. 48 bytes, read once per block by each kernel.
 struct T1Job {
-    uint32_t coeff;   // index of the block's 1024 sign-magnitude words in the coefficient buffer
-    uint32_t region;  // byte offset of its symbol region, and of its codeword region (16-aligned)
-    uint32_t cap;     // bytes in either region
-    uint32_t geom;    // (w-1) | (h-1) << 5 | orient << 10 | maxPasses << 12 | frame << 19
-    float dscale;     // band delta^2 * weight: distortion units of the early-termination rule
-    uint32_t pad[3];
+    const uint32_t* coeffs;  // its 1024 sign-magnitude words (32 x 32, zero outside w x h)
+    uint8_t* sym;            // its decision region (16-aligned)
+    uint8_t* cw;             // its codeword region (16-aligned)
+    uint32_t cap;            // bytes in either region
+    uint32_t geom;           // (w-1) | (h-1) << 5 | orient << 10 | maxPasses << 12
+    float dscale;            // band delta^2 * weight: distortion units of the early-termination rule
+    uint32_t slope;          // index of its frame's early-termination threshold
+    uint32_t pad[2];
 };
 
-inline uint32_t t1Geom(int w, int h, int orient, int maxPasses, int frame) {
-    return (uint32_t)(w - 1) | ((uint32_t)(h - 1) << 5) | ((uint32_t)orient << 10) | ((uint32_t)maxPasses << 12) |
-           ((uint32_t)frame << 19);
+inline uint32_t t1Geom(int w, int h, int orient, int maxPasses) {
+    return (uint32_t)(w - 1) | ((uint32_t)(h - 1) << 5) | ((uint32_t)orient << 10) | ((uint32_t)maxPasses << 12);
 }
 
 // Worst-case MQ decisions of a block: each sample is coded once per bit-plane with at most
@@ -31,13 +33,11 @@ inline uint32_t t1SymbolBound(int w, int h, int planes) {
     return ((perPlane * (uint32_t)planes + 64u) + 15u) & ~15u;
 }
 
-// Device pointers of one Tier-1 launch (any number of frames: the jobs say where).
+// Device pointers of one Tier-1 launch (any number of frames: the jobs say where). The
+// per-job tables are indexed by the job's position in `jobs`.
 struct T1Launch {
-    const uint32_t* coeffs;
     const T1Job* jobs;
     uint32_t n;
-    uint8_t* sym;        // symbol arena
-    uint8_t* cw;         // codeword arena, same offsets as the symbol arena
     uint32_t* info;      // 4 words per job: nbps, passes, symbols, codeword bytes
     uint32_t* passEnd;   // 64 per job: decisions coded by the end of each pass
     uint32_t* passLen;   // 64 per job: truncation length after each pass
@@ -45,7 +45,7 @@ struct T1Launch {
     uint4* snaps;        // 64 per job: MQ state at the end of each pass
     uint32_t* perm;      // n: jobs in MQ order (most decisions first)
     uint32_t* ctl;       // [0] MQ queue head, [1] status bits, [2] total decisions
-    const float* slope;  // per-frame early-termination threshold (NULL: code every pass)
+    const float* slope;  // early-termination thresholds, indexed by T1Job::slope (NULL: every pass)
 };
 
 // Enqueues the whole Tier-1 stage on st: context modelling, ordering, MQ coding.

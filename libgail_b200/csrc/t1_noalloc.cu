@@ -102,13 +102,17 @@ extern "C" GB_API int gb_t1_encode_blocks_noalloc(const uint32_t* coeffs, const 
             const int w = geom4[4 * i], h = geom4[4 * i + 1], orient = geom4[4 * i + 2], mp = geom4[4 * i + 3];
             if (w < 1 || w > 32 || h < 1 || h > 32 || orient < 0 || orient > 3 || mp < 0 || mp > 64)
                 throw std::logic_error("code-block geometry out of range");
-            jobs[i] = {i, i * kRegion, kRegion, t1Geom(w, h, orient, mp, 0), distScale ? distScale[i] : 1.f, {0, 0, 0}};
+            jobs[i] = {reinterpret_cast<const uint32_t*>(base + kOffCoeffs) + (size_t)i * kCblkArea,
+                       base + kOffSym + (size_t)i * kRegion,
+                       base + kOffCw + (size_t)i * kRegion,
+                       kRegion,
+                       t1Geom(w, h, orient, mp),
+                       distScale ? distScale[i] : 1.f,
+                       0,
+                       {0, 0}};
         }
-        T1Launch L{reinterpret_cast<const uint32_t*>(base + kOffCoeffs),
-                   reinterpret_cast<const T1Job*>(base + kOffJobs),
+        T1Launch L{reinterpret_cast<const T1Job*>(base + kOffJobs),
                    n,
-                   base + kOffSym,
-                   base + kOffCw,
                    reinterpret_cast<uint32_t*>(base + kOffInfo),
                    reinterpret_cast<uint32_t*>(base + kOffEnd),
                    reinterpret_cast<uint32_t*>(base + kOffLen),

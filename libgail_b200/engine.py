@@ -1,0 +1,77 @@
+"""The batched, served encoder from Python (gb_engine_* in include/gail_b200.h)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import GailError, check, lib
+from .plugin import Color, EncodeSettings, FrameFormat, LayoutHolder, Tier1, Tier1Frame
+
+
+def _bind():
+    L = lib()
+    if getattr(L, "_engine_bound", False):
+        return L
+    L.gb_engine_create.argtypes = [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_void_p)]
+    L.gb_engine_destroy.argtypes = [C.c_void_p]
+    L.gb_engine_destroy.restype = None
+    L.gb_engine_add_encoder.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]
+    L.gb_engine_submit.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_int64)]
+    L.gb_engine_wait.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(Tier1), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_int)]
+    L.gb_engine_release.argtypes = [C.c_void_p, C.c_int64]
+    L.gb_engine_stats.argtypes = [C.c_void_p, C.c_void_p]
+    L._engine_bound = True
+    return L
+
+
+class Engine:
+    def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch: int = 16):
+        L = _bind()
+        h = C.c_void_p()
+        check(L.gb_engine_create(device, hbm_budget, max_batch, C.byref(h)))
+        self.h = h
+        self._keep = {}   # frames the engine still reads, by request id
+        self._classes = []
+
+    def close(self):
+        if self.h:
+            lib().gb_engine_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def add_encoder(self, layout: LayoutHolder, fmt: FrameFormat, col: Color):
+        s = EncodeSettings(profile=layout.abi.profile, width=layout.width, height=layout.height,
+                           baseStep=layout.abi.baseStep, slopeFactor=0.0, bitsPerSymbol=0.5, input=fmt, color=col)
+        cid, nbytes = C.c_int(), C.c_uint64()
+        check(lib().gb_engine_add_encoder(self.h, C.byref(layout.abi), C.byref(s), C.byref(cid), C.byref(nbytes)))
+        self._classes.append((layout, s))
+        return cid.value, nbytes.value
+
+    def submit(self, cls: int, frame, slope: float = 0.0) -> int:
+        """frame: a numpy array (host) or a torch CUDA tensor (device)."""
+        on_device = hasattr(frame, "is_cuda") and frame.is_cuda
+        ptr = frame.data_ptr() if on_device or hasattr(frame, "data_ptr") else frame.ctypes.data
+        rid = C.c_int64()
+        check(lib().gb_engine_submit(self.h, cls, C.c_void_p(ptr), int(on_device), C.c_double(slope), C.byref(rid)))
+        self._keep[rid.value] = frame
+        return rid.value
+
+    def wait(self, timeout_ms: int = 60000, copy: bool = True):
+        """(id, Tier1Frame or None, latency ms, status); id -1 on timeout."""
+        rid, lat, st = C.c_int64(), C.c_double(), C.c_int()
+        t = Tier1()
+        check(lib().gb_engine_wait(self.h, timeout_ms, C.byref(rid), C.byref(t), C.byref(lat), C.byref(st)))
+        if rid.value < 0:
+            return -1, None, 0.0, 0
+        return rid.value, (Tier1Frame(t) if copy else t), lat.value, st.value
+
+    def release(self, rid: int):
+        check(lib().gb_engine_release(self.h, rid))
+        self._keep.pop(rid, None)
+
+    def stats(self):
+        out = np.zeros(5, np.uint64)
+        check(lib().gb_engine_stats(self.h, out.ctypes.data))
+        return dict(zip(["frames", "batches", "batch_frames", "slots", "slot_bytes"], (int(x) for x in out)))

@@ -1,0 +1,95 @@
+"""The batched, served encoder: every frame's Tier-1 frame must be the same whether it was
+encoded alone through the plain per-frame path (the plugin's encoder_encode) or in a mix
+of frames of several profiles batched into shared Tier-1 launches, and the admission by
+HBM budget must let every request finish."""
+import numpy as np
+import pytest
+
+from libgail_b200 import plugin as P
+from libgail_b200 import synth
+from libgail_b200.engine import Engine
+
+
+def _same(a: P.Tier1Frame, b: P.Tier1Frame):
+    return (np.array_equal(a.info, b.info) and np.array_equal(a.pass_len, b.pass_len)
+            and np.array_equal(a.pass_dist, b.pass_dist) and np.array_equal(a.data, b.data))
+
+
+@pytest.fixture(scope="module")
+def dev():
+    d = P.Plugin().device(0)
+    yield d
+    d.close()
+
+
+def _cases():
+    # (layout args, format, colour, frames)
+    out = []
+    for W, H, fk in [(1998, 1080, 0), (2048, 858, 0)]:
+        frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=100 + i)) for i in range(3)]
+        out.append(((W, H, fk), P.rgb48_format(W, H), P.color_passthrough(), frames))
+    W, H = 3996, 2160
+    frames = [synth.yuv422p10(W, H, seed=200 + i) for i in range(2)]
+    out.append(((W, H, 1), P.planar_format(W, H, bits=10, sx=1, sy=0), P.color("pq", "bt2020"), frames))
+    return out
+
+
+@pytest.mark.gpu
+def test_engine_mix_equals_alone(dev):
+    cases = _cases()
+    alone = []
+    for (W, H, fk), fmt, col, frames in cases:
+        enc = dev.encoder(P.LayoutHolder(W, H, fk), fmt, col)
+        alone.append([enc.encode(f)[0] for f in frames])
+        enc.close()
+    eng = Engine(0, 0, max_batch=16)
+    try:
+        layouts = [P.LayoutHolder(W, H, fk) for (W, H, fk), _, _, _ in cases]
+        classes = [eng.add_encoder(lay, fmt, col)[0] for lay, (_, fmt, col, _) in zip(layouts, cases)]
+        want = {}
+        order = [(ci, fi) for fi in range(3) for ci in range(len(cases)) if fi < len(cases[ci][3])]
+        for ci, fi in order:  # interleaved profiles
+            rid = eng.submit(classes[ci], cases[ci][3][fi])
+            want[rid] = alone[ci][fi]
+        got = 0
+        while got < len(want):
+            rid, t1, lat, st = eng.wait(60000)
+            assert rid >= 0, "timed out"
+            assert st == 0
+            assert _same(t1, want[rid]), f"request {rid} differs from its plain encode"
+            eng.release(rid)
+            got += 1
+        s = eng.stats()
+        assert s["frames"] == len(want)
+        assert s["batch_frames"] == len(want)
+    finally:
+        eng.close()
+
+
+@pytest.mark.gpu
+def test_engine_admission_by_budget(dev):
+    """A budget of two 2K frame slots: ten requests still all finish, in bounded slots."""
+    W, H = 1998, 1080
+    frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=300 + i)) for i in range(10)]
+    lay = P.LayoutHolder(W, H, 0)
+    enc = dev.encoder(lay, P.rgb48_format(W, H), P.color_passthrough())
+    ref = [enc.encode(f)[0] for f in frames[:2]]
+    enc.close()
+    probe = Engine(0, 0, 4)
+    _, per_frame = probe.add_encoder(lay, P.rgb48_format(W, H), P.color_passthrough())
+    probe.close()
+    eng = Engine(0, 2 * per_frame + 1, max_batch=4)
+    try:
+        cid, _ = eng.add_encoder(lay, P.rgb48_format(W, H), P.color_passthrough())
+        ids = [eng.submit(cid, f) for f in frames]
+        seen = 0
+        while seen < len(ids):
+            rid, t1, _, st = eng.wait(60000)
+            assert rid >= 0 and st == 0
+            if rid < 2:
+                assert _same(t1, ref[rid])
+            eng.release(rid)
+            seen += 1
+        assert eng.stats()["slots"] <= 2
+    finally:
+        eng.close()
