@@ -42,7 +42,11 @@ namespace {
 
 constexpr int CM_WARPS = 4;          // warps (code-blocks in flight) per CTA
 constexpr int CM_THREADS = CM_WARPS * 32;
-constexpr int STAGE = 2560 + 64;     // staging bytes per warp: one plane's decisions
+// Staging bytes per warp: one plane's decisions. A sample takes one refinement decision
+// or at most two (zero coding and sign) in a plane, and a run-length stripe column adds at
+// most two more (run, two position decisions, sign, in place of one zero-coding decision):
+// 2 * 1024 + 2 * 256 = 2560 for a 32x32 block.
+constexpr int STAGE = 2560 + 64;
 constexpr int MQ_THREADS = 128;
 constexpr int ORDER_BUCKETS = 128;
 
@@ -66,30 +70,12 @@ struct Nbr {
     uint32_t Gl, Gr, G;  // signs of left, right, own column
 };
 
-// Per-lane decision buffer for one stripe (at most 10 decisions of 6 bits).
-struct Emit {
-    unsigned long long acc;
-    uint32_t n;
-    __device__ __forceinline__ void put(uint32_t cx, uint32_t d) {
-        acc |= (unsigned long long)((cx << 1) | d) << (6 * n);
-        ++n;
-    }
-};
-
 // Zero-coding decision of row r; SN = own column with the rows above r already updated.
 __device__ __forceinline__ uint32_t zcContext(const uint8_t* zc, const Nbr& q, uint32_t SN, int r) {
     const uint32_t h = bit(q.L, r) + bit(q.R, r);
     const uint32_t v = bit(SN << 1, r) + bit(q.S >> 1, r);
     const uint32_t d = bit(q.L << 1, r) + bit(q.L >> 1, r) + bit(q.R << 1, r) + bit(q.R >> 1, r);
     return zc[h + 3 * v + 9 * d];
-}
-
-// Sign decision of row r (its neighbours as the scan order sees them).
-__device__ __forceinline__ void codeSign(Emit& e, const uint8_t* sc, const Nbr& q, uint32_t SN, int r) {
-    const int hc = clamp1(chi(q.L, q.Gl, r) + chi(q.R, q.Gr, r));
-    const int vc = clamp1(chi(SN << 1, q.G << 1, r) + chi(q.S >> 1, q.G >> 1, r));
-    const uint32_t t = sc[(hc + 1) * 3 + (vc + 1)];
-    e.put(t & 31u, bit(q.G, r) ^ (t >> 5));
 }
 
 // Warp-inclusive prefix sum.
@@ -117,22 +103,7 @@ __device__ __forceinline__ uint32_t shDown(uint32_t v, int lane) {
     return lane == 31 ? 0u : t;
 }
 
-// Places the stripe's decisions of every lane after `count` in the staging buffer.
-__device__ __forceinline__ uint32_t stage(Emit& e, uint8_t* buf, uint32_t count, int lane, uint32_t* status) {
-    const uint32_t incl = warpScan(e.n, lane);
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    const uint32_t at = count + incl - e.n;
-    if (count + total <= (uint32_t)STAGE) {
-        for (uint32_t i = 0; i < e.n; ++i) buf[at + i] = (uint8_t)((e.acc >> (6 * i)) & 63u);
-    } else if (lane == 0) {
-        atomicOr(status, kErrSymbolSpace);
-    }
-    e.acc = 0;
-    e.n = 0;
-    return count + total;
-}
-
-__global__ void __launch_bounds__(CM_THREADS) t1CmKernel(T1Launch P) {
+__global__ void __launch_bounds__(CM_THREADS, 5) t1CmKernel(T1Launch P) {
     __shared__ uint32_t s_mag[CM_WARPS][32][32];
     __shared__ __align__(16) uint8_t s_stage[CM_WARPS][STAGE];
     __shared__ uint8_t s_zc[4 * 45];
@@ -197,116 +168,154 @@ __global__ void __launch_bounds__(CM_THREADS) t1CmKernel(T1Launch P) {
             uint32_t vis = 0, count = 0;
             int32_t planeDist = 0;
             for (int type = (p == nbps - 1 ? 2 : 0); type < 3 && np < maxPasses; ++type) {
-                int32_t dist = 0;
-                Emit e{0ull, 0u};
-                for (int s = 0; s < nstripes; ++s) {
-                    const int r0 = 4 * s;
-                    const uint32_t sm = (0xFu << r0) & valid;
-                    Nbr q;
-                    q.S = sig;
-                    q.R = shDown(sig, lane);
-                    q.G = sgn;
-                    q.Gl = sgnL;
-                    q.Gr = sgnR;
-                    const uint32_t SL = shUp(sig, lane);
-                    if (type == 0) {
-                        // significance propagation: eligible = insignificant with a
-                        // significant neighbour, in scan order
-                        const uint32_t cand = sm & ~q.S;
-                        const uint32_t spreadLR = SL | (SL << 1) | (SL >> 1) | q.R | (q.R << 1) | (q.R >> 1);
-                        if (!__any_sync(kFull, cand & (spreadLR | (q.S << 1) | (q.S >> 1)))) continue;
-                        uint32_t NEW = 0, E = 0;
+                // (1) the pass's row masks: E = rows coded, NEW = rows that become significant
+                const uint32_t Spass = sig;
+                uint32_t E = 0, NEW = 0;
+                if (type == 0) {
+                    // significance propagation: eligible = insignificant with a significant
+                    // neighbour in scan order; stripes in order, each a warp fixpoint
+#pragma unroll 1
+                    for (int s = 0; s < nstripes; ++s) {
+                        const int r0 = 4 * s;
+                        const uint32_t S = sig, SL = shUp(S, lane), R = shDown(S, lane);
+                        const uint32_t cand = (0xFu << r0) & valid & ~S;
+                        const uint32_t spreadLR = SL | (SL << 1) | (SL >> 1) | R | (R << 1) | (R >> 1);
+                        if (!__any_sync(kFull, cand & (spreadLR | (S << 1) | (S >> 1)))) continue;
+                        uint32_t nn = 0, ee = 0;
+#pragma unroll 1
                         for (int it = 0; it < 34; ++it) {
-                            const uint32_t L = SL | shUp(NEW, lane);
-                            const uint32_t side = L | (L << 1) | (L >> 1) | q.R | (q.R << 1) | (q.R >> 1) | (q.S >> 1);
-                            uint32_t nn = 0, ee = 0;
+                            const uint32_t L = SL | shUp(nn, lane);
+                            const uint32_t side = L | (L << 1) | (L >> 1) | R | (R << 1) | (R >> 1) | (S >> 1);
+                            uint32_t n2 = 0, e2 = 0;
 #pragma unroll
                             for (int k = 0; k < 4; ++k) {
                                 const uint32_t b = 1u << (r0 + k);
                                 if (!(cand & b)) continue;
-                                const uint32_t above = ((q.S | nn) << 1) & b;
-                                if ((side & b) | above) {
-                                    ee |= b;
-                                    nn |= Bp & b;
+                                if ((side & b) | (((S | n2) << 1) & b)) {
+                                    e2 |= b;
+                                    n2 |= Bp & b;
                                 }
                             }
-                            const bool changed = nn != NEW;
-                            NEW = nn;
-                            E = ee;
+                            const bool changed = n2 != nn;
+                            nn = n2;
+                            ee = e2;
                             if (!__any_sync(kFull, changed)) break;
                         }
-                        q.L = SL | shUp(NEW, lane);
-                        const uint32_t SN = q.S | NEW;
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const int r = r0 + k;
-                            if (!bit(E, r)) continue;
-                            // above: rows < r are final; below: as before the stripe
-                            const uint32_t upto = SN & ((1u << r) - 1u);
-                            e.put(zcContext(zc, q, q.S | upto, r), bit(Bp, r));
-                            if (bit(NEW, r)) {
-                                codeSign(e, s_sc, q, q.S | upto, r);
-                                dist += distSig((mag[r][lane] >> p) & 0x7Fu);
-                            }
-                        }
-                        sig = SN;
-                        vis |= E;
-                    } else if (type == 1) {
-                        // magnitude refinement of what was significant before this plane
-                        const uint32_t coded = sig0 & sm;
-                        if (!__any_sync(kFull, coded)) continue;
-                        const uint32_t nAny = (q.S << 1) | (q.S >> 1) | SL | (SL << 1) | (SL >> 1) | q.R | (q.R << 1) |
-                                              (q.R >> 1);
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const int r = r0 + k;
-                            if (!bit(coded, r)) continue;
-                            const uint32_t cx = bit(refined, r) ? 16u : (bit(nAny, r) ? 15u : 14u);
-                            e.put(cx, bit(Bp, r));
-                            dist += distRef((mag[r][lane] >> p) & 0x7Fu);
-                        }
-                    } else {
-                        // cleanup: everything not yet significant and not coded this plane
-                        const uint32_t C = sm & ~q.S & ~vis;
-                        if (!__any_sync(kFull, C)) continue;
-                        const uint32_t NEW = C & Bp;
-                        q.L = SL | shUp(NEW, lane);
-                        const uint32_t SN = q.S | NEW;
-                        const uint32_t four = 0xFu << r0;
-                        int rs = r0;
-                        bool run = r0 + 3 < h && (C & four) == four;
-                        if (run) {
-                            const uint32_t win = r0 == 0 ? 0x1Fu : (0x3Fu << (r0 - 1));
-                            run = !(q.L & win) && !(q.R & win) && !(q.S & win);
-                        }
-                        if (run) {
-                            const uint32_t nb = (NEW >> r0) & 0xFu;
-                            if (nb == 0) {
-                                e.put(17u, 0u);
-                                rs = r0 + 4;
-                            } else {
-                                const int first = __ffs(nb) - 1;
-                                e.put(17u, 1u);
-                                e.put(18u, (uint32_t)first >> 1);
-                                e.put(18u, (uint32_t)first & 1u);
-                                const int r = r0 + first;
-                                codeSign(e, s_sc, q, q.S | (SN & ((1u << r) - 1u)), r);
-                                dist += distSig((mag[r][lane] >> p) & 0x7Fu);
-                                rs = r + 1;
-                            }
-                        }
-                        for (int r = rs; r < r0 + 4; ++r) {
-                            if (!bit(C, r)) continue;
-                            const uint32_t upto = q.S | (SN & ((1u << r) - 1u));
-                            e.put(zcContext(zc, q, upto, r), bit(Bp, r));
-                            if (bit(NEW, r)) {
-                                codeSign(e, s_sc, q, upto, r);
-                                dist += distSig((mag[r][lane] >> p) & 0x7Fu);
-                            }
-                        }
-                        sig = SN;
+                        E |= ee;
+                        NEW |= nn;
+                        sig = S | nn;
                     }
-                    count = stage(e, buf, count, lane, status);
+                    vis |= E;
+                } else if (type == 1) {
+                    E = sig0 & valid;  // refinement of what was significant before this plane
+                } else {
+                    E = valid & ~Spass & ~vis;  // cleanup: everything else
+                    NEW = E & Bp;
+                    sig = Spass | NEW;
+                }
+                int32_t dist = 0;
+                if (__any_sync(kFull, E)) {
+                    // (2) neighbourhoods as the scan order sees them, per stripe s with rows
+                    //     Q and the rows before it P: left column current up to the stripe,
+                    //     right column and own column as before the stripe
+                    const uint32_t SLp = shUp(Spass, lane), SRp = shDown(Spass, lane);
+                    const uint32_t NL = shUp(NEW, lane), NR = shDown(NEW, lane);
+                    const uint32_t nAny = (Spass << 1) | (Spass >> 1) | SLp | (SLp << 1) | (SLp >> 1) | SRp | (SRp << 1) |
+                                          (SRp >> 1);
+                    // cleanup run-length mode per stripe (bit s), first 1-bit of a run
+                    uint32_t runs = 0;
+                    // (3) decisions per stripe, 10-bit fields, three stripes per word
+                    uint32_t w0 = 0, w1 = 0, w2 = 0;
+#pragma unroll 1
+                    for (int s = 0; s < nstripes; ++s) {
+                        const int r0 = 4 * s;
+                        const uint32_t Q = 0xFu << r0, P = (1u << r0) - 1u;
+                        uint32_t cnt;
+                        if (type == 1) {
+                            cnt = __popc(E & Q);
+                        } else if (type == 0) {
+                            cnt = __popc(E & Q) + __popc(NEW & Q);
+                        } else {
+                            cnt = __popc(E & Q) + __popc(NEW & Q);
+                            if (r0 + 3 < h && (E & Q) == Q) {
+                                const uint32_t L = SLp | (NL & (P | Q)), R = SRp | (NR & P), Sb = Spass | (NEW & P);
+                                const uint32_t win = r0 == 0 ? 0x1Fu : (0x3Fu << (r0 - 1));
+                                if (!(L & win) && !(R & win) && !(Sb & win)) {
+                                    runs |= 1u << s;
+                                    const uint32_t nb = (NEW >> r0) & 0xFu;
+                                    if (nb == 0) {
+                                        cnt = 1;
+                                    } else {
+                                        const uint32_t after = Q & ~((2u << (r0 + __ffs(nb) - 1)) - 1u);
+                                        cnt = 4 + __popc(E & after) + __popc(NEW & after);
+                                    }
+                                }
+                            }
+                        }
+                        const uint32_t f = cnt << (10 * (s % 3));
+                        if (s < 3) w0 |= f;
+                        else if (s < 6) w1 |= f;
+                        else w2 |= f;
+                    }
+                    const uint32_t i0 = warpScan(w0, lane), i1 = warpScan(w1, lane), i2 = warpScan(w2, lane);
+                    const uint32_t t0 = __shfl_sync(kFull, i0, 31), t1 = __shfl_sync(kFull, i1, 31),
+                                   t2 = __shfl_sync(kFull, i2, 31);
+                    const uint32_t x0 = i0 - w0, x1 = i1 - w1, x2 = i2 - w2;
+                    // (4) every lane writes its decisions for every stripe at its place
+                    uint32_t sbase = count;
+#pragma unroll 1
+                    for (int s = 0; s < nstripes; ++s) {
+                        const int r0 = 4 * s;
+                        const int sh = 10 * (s % 3);
+                        uint32_t pos = sbase + (((s < 3 ? x0 : (s < 6 ? x1 : x2)) >> sh) & 1023u);
+                        sbase += ((s < 3 ? t0 : (s < 6 ? t1 : t2)) >> sh) & 1023u;
+                        const uint32_t Q = 0xFu << r0, P = (1u << r0) - 1u;
+                        uint32_t rows = E & Q;
+                        if (!rows) continue;
+                        if (type == 1) {
+#pragma unroll 1
+                            for (; rows; rows &= rows - 1) {
+                                const int r = __ffs(rows) - 1;
+                                buf[pos++] = (uint8_t)(((bit(refined, r) ? 16u : (bit(nAny, r) ? 15u : 14u)) << 1) | bit(Bp, r));
+                                dist += distRef((mag[r][lane] >> p) & 0x7Fu);
+                            }
+                            continue;
+                        }
+                        Nbr q;
+                        q.L = SLp | (NL & (P | Q));
+                        q.R = SRp | (NR & P);
+                        q.S = Spass | (NEW & P);
+                        q.G = sgn;
+                        q.Gl = sgnL;
+                        q.Gr = sgnR;
+                        const uint32_t SN = q.S | (NEW & Q);
+                        uint32_t skip = 0;  // the row whose zero-coding decision the run decisions replace
+                        if ((runs >> s) & 1u) {
+                            const uint32_t nb = (NEW >> r0) & 0xFu;
+                            buf[pos++] = (uint8_t)((17u << 1) | (nb != 0));
+                            if (nb == 0) continue;
+                            const uint32_t first = __ffs(nb) - 1;
+                            buf[pos++] = (uint8_t)((18u << 1) | (first >> 1));
+                            buf[pos++] = (uint8_t)((18u << 1) | (first & 1u));
+                            skip = 1u << (r0 + first);
+                            rows &= ~(skip - 1u);
+                        }
+#pragma unroll 1
+                        for (; rows; rows &= rows - 1) {
+                            const int r = __ffs(rows) - 1;
+                            // above: rows < r are final; below: as before the stripe
+                            const uint32_t upto = q.S | (SN & ((1u << r) - 1u));
+                            if (!((skip >> r) & 1u)) buf[pos++] = (uint8_t)((zcContext(zc, q, upto, r) << 1) | bit(Bp, r));
+                            if (bit(NEW, r)) {
+                                const int hc = clamp1(chi(q.L, q.Gl, r) + chi(q.R, q.Gr, r));
+                                const int vc = clamp1(chi(upto << 1, q.G << 1, r) + chi(q.S >> 1, q.G >> 1, r));
+                                const uint32_t t = s_sc[(hc + 1) * 3 + (vc + 1)];
+                                buf[pos++] = (uint8_t)(((t & 31u) << 1) | (bit(q.G, r) ^ (t >> 5)));
+                                dist += distSig((mag[r][lane] >> p) & 0x7Fu);
+                            }
+                        }
+                    }
+                    count = sbase;
                 }
                 if (type == 1) refined |= sig0;
                 const int32_t total = warpSum(dist);
@@ -521,11 +530,6 @@ __device__ uint32_t truncLen(uint4 s, const uint8_t* buf, uint32_t len, uint32_t
     return len;
 }
 
-__device__ __forceinline__ uint32_t byteOf(const uint4& v, uint32_t i) {
-    const uint32_t w = i < 8 ? (i < 4 ? v.x : v.y) : (i < 12 ? v.z : v.w);
-    return (w >> (8 * (i & 3u))) & 0xFFu;
-}
-
 __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
     __shared__ uint32_t s_tab[48];
     __shared__ uint32_t s_ctx[19 * MQ_THREADS];
@@ -537,7 +541,7 @@ __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
     // Per-lane state of the block in hand.
     uint32_t job = 0, pos = 0, nsym = 0, np = 0, k = 0, nextEnd = 0;
     const uint8_t* sym = nullptr;
-    uint4 cur = make_uint4(0, 0, 0, 0), nxt = cur;
+    uint4 nxt = make_uint4(0, 0, 0, 0);  // the block's next 16 decisions
     Coder e;
     e.cap = 0;
     bool have = false;
@@ -597,23 +601,36 @@ __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
             pos = 0;
             k = 0;
             nextEnd = P.passEnd[(size_t)job * kMaxPasses];
-            cur = nsym ? *reinterpret_cast<const uint4*>(sym) : make_uint4(0, 0, 0, 0);
-            nxt = nsym > 16 ? *reinterpret_cast<const uint4*>(sym + 16) : make_uint4(0, 0, 0, 0);
+            nxt = nsym ? *reinterpret_cast<const uint4*>(sym) : make_uint4(0, 0, 0, 0);
             have = true;
             if (nsym == 0) continue;
         }
-        while (pos == nextEnd && k < np) {
-            P.snaps[(size_t)job * kMaxPasses + k] = make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
-            ++k;
-            nextEnd = k < np ? P.passEnd[(size_t)job * kMaxPasses + k] : 0xFFFFFFFFu;
-        }
-        const uint32_t s = byteOf(cur, pos & 15u);
-        const uint32_t cx = s >> 1;
-        ctx[cx * MQ_THREADS] = e.encode(ctx[cx * MQ_THREADS], s & 1u, s_tab);
-        ++pos;
-        if ((pos & 15u) == 0) {
-            cur = nxt;
-            if (pos + 16 < nsym) nxt = *reinterpret_cast<const uint4*>(sym + pos + 16);
+        // One aligned chunk of 16 decisions (fewer at the block's end), unrolled so that
+        // every byte is taken from a fixed place; the next decision's context state is
+        // read ahead, off the serial chain of the coder.
+        const uint4 v = nxt;
+        nxt = (pos + 16 < nsym) ? *reinterpret_cast<const uint4*>(sym + pos + 16) : make_uint4(0, 0, 0, 0);
+        const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+        uint32_t s = words[0] & 0xFFu;
+        uint32_t t = ctx[(s >> 1) * MQ_THREADS];
+#pragma unroll
+        for (int b = 0; b < 16; ++b) {
+            if (pos >= nsym) break;
+            while (pos == nextEnd && k < np) {
+                P.snaps[(size_t)job * kMaxPasses + k] = make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
+                ++k;
+                nextEnd = k < np ? P.passEnd[(size_t)job * kMaxPasses + k] : 0xFFFFFFFFu;
+            }
+            // the byte past the block's last decision is not a decision: the clamp keeps
+            // its look-ahead read inside the lane's 19 contexts
+            const uint32_t sn = b < 15 ? (words[(b + 1) >> 2] >> (8 * ((b + 1) & 3))) & 0xFFu : 0u;
+            const uint32_t tn = ctx[min(sn >> 1, 18u) * MQ_THREADS];
+            const uint32_t cx = s >> 1;
+            const uint32_t tNew = e.encode(t, s & 1u, s_tab);
+            ctx[cx * MQ_THREADS] = tNew;
+            t = (sn >> 1) == cx ? tNew : tn;
+            s = sn;
+            ++pos;
         }
     }
 }

@@ -1,0 +1,76 @@
+"""Small, fixed encode cases for profiler captures.
+
+  python -m libgail_b200.profile_case --path plain --frames 2
+  python -m libgail_b200.profile_case --path served --frames 8 --batch 8
+
+Encodes seeded synthetic 4K frames (3996x2160 Y'CbCr 4:2:2 10-bit, BT.2020 PQ, as the
+benchmark uses) that are already in device memory, through the plain per-frame encoder or
+the batched engine, and prints the stage times of the plain path. Exits non-zero on any
+encoder error, so that a profiler run after it sees the same launches of a program that
+ended cleanly.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+
+import numpy as np
+
+W4K, H4K = 3996, 2160
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--path", choices=["plain", "served"], default="plain")
+    ap.add_argument("--frames", type=int, default=2)
+    ap.add_argument("--batch", type=int, default=8)
+    args = ap.parse_args()
+
+    import torch
+
+    import libgail_b200 as gb
+    from libgail_b200 import plugin as P
+    from libgail_b200 import synth
+    from libgail_b200.engine import Engine
+
+    frames = synth.many(synth.yuv422p10, args.frames, W4K, H4K, seed=1000)
+    dframes = [torch.from_numpy(f.view(np.int16)).to("cuda:0") for f in frames]
+    torch.cuda.synchronize()
+    lay = P.LayoutHolder(W4K, H4K, 1)
+    fmt = P.planar_format(W4K, H4K, bits=10, sx=1, sy=0)
+    col = P.color("pq", "bt2020")
+    dev = P.Plugin().device(0)
+    try:
+        if args.path == "plain":
+            L = gb.lib()
+            L.gb_encoder_enqueue_device.argtypes = [C.c_void_p, C.c_void_p]
+            L.gb_encoder_finish.argtypes = [C.c_void_p]
+            L.gb_encoder_stage_timing.argtypes = [C.c_void_p, C.c_int]
+            L.gb_encoder_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+            enc = dev.encoder(lay, fmt, col)
+            gb.check(L.gb_encoder_stage_timing(enc.h, 1))
+            for f in dframes:
+                gb.check(L.gb_encoder_enqueue_device(enc.h, C.c_void_p(f.data_ptr())))
+            gb.check(L.gb_encoder_finish(enc.h))
+            ms = np.zeros(5)
+            n = C.c_int()
+            gb.check(L.gb_encoder_stage_times(enc.h, ms.ctypes.data, C.byref(n)))
+            print("ms per frame (front, cm, order, mq, pack):", np.round(ms / max(n.value, 1), 4).tolist())
+            enc.close()
+        else:
+            eng = Engine(0, 0, max_batch=args.batch)
+            cid, _ = eng.add_encoder(lay, fmt, col)
+            ids = [eng.submit(cid, f) for f in dframes]
+            for _ in ids:
+                rid, _, _, st = eng.wait(120000, copy=False)
+                if rid < 0 or st != 0:
+                    raise SystemExit(f"engine frame failed (id {rid}, status {st})")
+                eng.release(rid)
+            print("engine:", eng.stats())
+            eng.close()
+    finally:
+        dev.close()
+
+
+if __name__ == "__main__":
+    main()
