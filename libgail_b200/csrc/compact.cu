@@ -2,6 +2,11 @@
 // the packed Tier1Frame form the host codec consumes (Josephur/libgail
 // core/tier1_types.h:12-28): CblkInfo per block, pass lengths and distortions back to
 // back, codewords back to back on 4-byte boundaries.
+//
+// Two launches over tiles of 1024 blocks: the tile sums, then per tile one CTA that adds
+// up the sums of the tiles before it, scans its own blocks in shared memory, writes the
+// CblkInfo records as contiguous words and copies the pass tables and codewords, a warp
+// per block. Nothing is read from the output buffers, which may be mapped host memory.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -11,7 +16,8 @@ namespace gb {
 
 namespace {
 
-constexpr int SCAN_THREADS = 1024;
+constexpr int TILE = 1024;
+constexpr int INFO_WORDS = 5;
 
 __device__ __forceinline__ uint32_t warpInclusive(uint32_t v, int lane) {
 #pragma unroll
@@ -22,88 +28,131 @@ __device__ __forceinline__ uint32_t warpInclusive(uint32_t v, int lane) {
     return v;
 }
 
-// One CTA: exclusive scans of (codeword bytes rounded to 4) and pass counts, and the
-// CblkInfo records. Totals go to tot[0] (bytes) and tot[1] (passes).
-__global__ void __launch_bounds__(SCAN_THREADS) scanKernel(CompactArgs a) {
-    __shared__ uint32_t sBytes[32], sPasses[32];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const uint32_t per = divUp(a.n, SCAN_THREADS);
-    const uint32_t b = min(a.n, tid * per), e = min(a.n, b + per);
-    uint32_t bytes = 0, passes = 0;
-    for (uint32_t i = b; i < e; ++i) {
-        bytes += (a.info[4 * (size_t)i + 3] + 3u) & ~3u;
-        passes += a.info[4 * (size_t)i + 1];
-    }
-    const uint32_t ib = warpInclusive(bytes, lane), ip = warpInclusive(passes, lane);
-    if (lane == 31) {
-        sBytes[wid] = ib;
-        sPasses[wid] = ip;
-    }
-    __syncthreads();
-    if (wid == 0) {
-        const uint32_t vb = sBytes[lane], vp = sPasses[lane];
-        const uint32_t xb = warpInclusive(vb, lane), xp = warpInclusive(vp, lane);
-        sBytes[lane] = xb - vb;
-        sPasses[lane] = xp - vp;
-        if (lane == 31) {
-            a.tot[0] = xb;
-            a.tot[1] = xp;
-        }
-    }
-    __syncthreads();
-    uint32_t ob = sBytes[wid] + ib - bytes, op = sPasses[wid] + ip - passes;
-    for (uint32_t i = b; i < e; ++i) {
-        const uint32_t* in = a.info + 4 * (size_t)i;
-        const uint32_t np = in[1], len = in[3];
-        uint32_t* o = a.outInfo + 5 * (size_t)i;
-        o[0] = in[0];
-        o[1] = np;
-        o[2] = ob;
-        o[3] = len;
-        o[4] = op;
-        ob += (len + 3u) & ~3u;
-        op += np;
+__device__ __forceinline__ uint32_t warpTotal(uint32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// Codeword bytes rounded to whole words, and passes, of block i (zero past the end).
+__device__ __forceinline__ void blockCounts(const CompactArgs& a, uint32_t i, uint32_t& bytes, uint32_t& passes) {
+    bytes = passes = 0;
+    if (i < a.n) {
+        const uint4 in = reinterpret_cast<const uint4*>(a.info)[i];
+        bytes = (in.w + 3u) & ~3u;
+        passes = in.y;
     }
 }
 
-// One warp per block: its pass tables and codeword to their packed places.
-__global__ void __launch_bounds__(256) packKernel(CompactArgs a) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < a.n; i += warps) {
-        const uint32_t* o = a.outInfo + 5 * (size_t)i;
-        const uint32_t np = o[1], dOff = o[2], len = o[3], pOff = o[4];
-        if (lane < (int)np) {
-            a.outPassLen[pOff + lane] = a.passLen[(size_t)i * kMaxPasses + lane];
-            a.outPassDist[pOff + lane] = a.passDist[(size_t)i * kMaxPasses + lane];
+__global__ void __launch_bounds__(TILE) tileSumKernel(CompactArgs a) {
+    __shared__ uint32_t sB[32], sP[32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    uint32_t b, p;
+    blockCounts(a, blockIdx.x * TILE + tid, b, p);
+    b = warpTotal(b);
+    p = warpTotal(p);
+    if (lane == 0) {
+        sB[wid] = b;
+        sP[wid] = p;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        b = warpTotal(sB[lane]);
+        p = warpTotal(sP[lane]);
+        if (lane == 0) {
+            a.scratch[2 * blockIdx.x] = b;
+            a.scratch[2 * blockIdx.x + 1] = p;
         }
-        if (lane + 32 < (int)np) {
-            a.outPassLen[pOff + lane + 32] = a.passLen[(size_t)i * kMaxPasses + lane + 32];
-            a.outPassDist[pOff + lane + 32] = a.passDist[(size_t)i * kMaxPasses + lane + 32];
+    }
+}
+
+__global__ void __launch_bounds__(TILE) packKernel(CompactArgs a) {
+    __shared__ uint32_t sRec[TILE * INFO_WORDS];
+    __shared__ uint32_t sB[32], sP[32], sBase[2];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint32_t tile = blockIdx.x, first = tile * TILE;
+    const uint32_t count = min((uint32_t)TILE, a.n - first);
+
+    // offsets of this tile: the sums of the tiles before it
+    if (wid == 0) {
+        uint32_t b = 0, p = 0;
+        for (uint32_t t = lane; t < tile; t += 32) {
+            b += a.scratch[2 * t];
+            p += a.scratch[2 * t + 1];
+        }
+        b = warpTotal(b);
+        p = warpTotal(p);
+        if (lane == 0) {
+            sBase[0] = b;
+            sBase[1] = p;
+        }
+    }
+    // exclusive scan of the tile's blocks
+    const uint32_t i = first + tid;
+    uint32_t bytes, passes;
+    blockCounts(a, i, bytes, passes);
+    const uint32_t ib = warpInclusive(bytes, lane), ip = warpInclusive(passes, lane);
+    if (lane == 31) {
+        sB[wid] = ib;
+        sP[wid] = ip;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const uint32_t vb = sB[lane], vp = sP[lane];
+        const uint32_t xb = warpInclusive(vb, lane), xp = warpInclusive(vp, lane);
+        sB[lane] = xb - vb;
+        sP[lane] = xp - vp;
+        if (tile == gridDim.x - 1 && lane == 31) {
+            a.tot[0] = sBase[0] + xb;
+            a.tot[1] = sBase[1] + xp;
+        }
+    }
+    __syncthreads();
+    const uint32_t dOff = sBase[0] + sB[wid] + ib - bytes, pOff = sBase[1] + sP[wid] + ip - passes;
+    if ((uint32_t)tid < count) {
+        uint32_t* r = sRec + INFO_WORDS * tid;
+        r[0] = a.info[4 * (size_t)i];
+        r[1] = passes;
+        r[2] = dOff;
+        r[3] = a.info[4 * (size_t)i + 3];
+        r[4] = pOff;
+    }
+    __syncthreads();
+    // the CblkInfo records, contiguous words
+    uint32_t* outInfo = a.outInfo + (size_t)INFO_WORDS * first;
+    for (uint32_t k = tid; k < count * INFO_WORDS; k += TILE) outInfo[k] = sRec[k];
+    // pass tables and codewords, a warp per block
+    bool over = false;
+    for (uint32_t k = wid; k < count; k += TILE / 32) {
+        const uint32_t* r = sRec + INFO_WORDS * k;
+        const uint32_t blk = first + k, np = r[1], off = r[2], len = r[3], po = r[4];
+        const size_t src = (size_t)blk * kMaxPasses;
+        for (uint32_t q = lane; q < np; q += 32) {
+            a.outPassLen[po + q] = a.passLen[src + q];
+            a.outPassDist[po + q] = a.passDist[src + q];
         }
         const uint32_t words = (len + 3u) >> 2;
-        if ((uint64_t)dOff + words * 4ull > a.dataCap) {
-            if (lane == 0) a.tot[2] = 1u;
+        if ((uint64_t)off + words * 4ull > a.dataCap) {
+            over = true;
             continue;
         }
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.jobs[i].cw);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(a.outData + dOff);
-        // whole words; the bytes past the codeword in its last word are zeroed so that the
-        // packed frame does not depend on what the region held before
+        const uint32_t* cw = reinterpret_cast<const uint32_t*>(a.jobs[blk].cw);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(a.outData + off);
+        // the bytes past the codeword in its last word are zeroed so that the packed frame
+        // does not depend on what the region held before
         const uint32_t tailMask = (len & 3u) ? (1u << (8 * (len & 3u))) - 1u : 0xFFFFFFFFu;
-        for (uint32_t k = lane; k < words; k += 32) dst[k] = k == words - 1 ? src[k] & tailMask : src[k];
+        for (uint32_t w = lane; w < words; w += 32) dst[w] = w == words - 1 ? cw[w] & tailMask : cw[w];
     }
+    if (__any_sync(kFull, over) && lane == 0) a.tot[2] = 1u;
 }
 
 }  // namespace
 
 void compactTier1(const CompactArgs& a, cudaStream_t st) {
     if (a.n == 0) return;
-    scanKernel<<<1, SCAN_THREADS, 0, st>>>(a);
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    packKernel<<<min(divUp(a.n, 8), (uint32_t)sms * 8), 256, 0, st>>>(a);
+    const uint32_t tiles = divUp(a.n, (uint32_t)TILE);
+    tileSumKernel<<<tiles, TILE, 0, st>>>(a);
+    packKernel<<<tiles, TILE, 0, st>>>(a);
     GB_CHECK(cudaGetLastError());
 }
 

@@ -20,7 +20,12 @@ struct CompactArgs {
     uint8_t* outData;
     uint32_t* tot;             // [0] data bytes, [1] passes, [2] set when outData was too small
     uint64_t dataCap;          // bytes outData holds
+    uint32_t* scratch;         // device, 2 words per 1024 blocks; free once MQ coding ended
+                               // on this stream, so the Tier-1 launch's perm table will do
 };
+
+// The out* pointers and tot may be mapped host memory: the kernels only write them, with
+// whole contiguous words, and read nothing back from them.
 
 void compactTier1(const CompactArgs& a, cudaStream_t st);
 

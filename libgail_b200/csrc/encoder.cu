@@ -244,8 +244,8 @@ void EncoderSlot::enqueueStages(const void* dFrame, bool taps, bool full) {
     t1Encode(t, st, mark ? mark + 2 : nullptr);
     GB_CHECK(cudaEventRecord(ev_[3], st));
     if (mark) GB_CHECK(cudaEventRecord(mark[4], st));
-    CompactArgs ca{(uint32_t)n, dInfo_, dLen_, dDist_, dJobs_, dOutInfo_, dOutLen_, dOutDist_, dOutData_, dCtl_ + 8,
-                   z_.arena};
+    CompactArgs ca{(uint32_t)n, dInfo_,    dLen_,      dDist_, dJobs_, dOutInfo_, dOutLen_,
+                   dOutDist_,   dOutData_, dCtl_ + 8, z_.arena, dPerm_};
     compactTier1(ca, st);
     if (mark) GB_CHECK(cudaEventRecord(mark[5], st));
 }

@@ -374,7 +374,7 @@ bool EncodeEngine::launchBatch(Batch& b) {
         std::memset(s->hTot, 0, 64);
         const uint32_t j = r->jobBase;
         CompactArgs ca{s->n,   b.info + 4 * (uint64_t)j, b.len + (uint64_t)kMaxPasses * j, b.dist + (uint64_t)kMaxPasses * j,
-                       b.dJobs + j, s->hInfo, s->hLen, s->hDist, s->hData, s->hTot, s->dataCap};
+                       b.dJobs + j, s->hInfo, s->hLen, s->hDist, s->hData, s->hTot, s->dataCap, b.perm};
         compactTier1(ca, b.st);
     }
     GB_CHECK(cudaMemcpyAsync(b.hCtl, b.ctl, 64, cudaMemcpyDeviceToHost, b.st));

@@ -1,9 +1,12 @@
 // Encoder front end: colour -> 9/7 DWT -> dead-zone quantisation, one kernel per level.
 //
-// Each CTA owns a 64 x 64 tile of the level's input and loads it with a 4-sample halo
-// (72 x 72, whole-sample symmetric mirror at the image edges) into shared memory, lifts
-// the columns, then the rows (the order of the reference, Annex F.4.2), and writes the
-// four 32 x 32 subband pieces it produced. Because tiles are 64-aligned, each piece is
+// Each CTA owns a 64 x 64 tile of the level's input, all three components, and loads it
+// with a 4-sample halo (72 x 72, whole-sample symmetric mirror at the image edges) into
+// shared memory. It lifts the columns, then the rows (the order of the reference, Annex
+// F.4.2): one thread per 72-sample line, in registers, the four lifting steps applied in
+// streaming order (alpha at j-1, beta at j-2, gamma at j-3, delta at j-4 as sample j
+// arrives), which gives every sample the same operands as step-by-step lifting. Then it
+// writes the four 32 x 32 subband pieces it produced. Because tiles are 64-aligned, each piece is
 // exactly one code-block of its band, so the high bands (and the LL band at the last
 // level) are quantised in registers and stored straight into the code-block-major
 // layout Tier-1 reads: 32 consecutive words per row, zero outside the band. The LL piece
@@ -11,8 +14,9 @@
 //
 // Level 1 also does the colour conversion in its tile loads (the frame is read once,
 // never written back as planes): R'G'B' from interleaved 16-bit or planar Y'CbCr,
-// EOTF lookup, 3x3 to XYZ, the 12-bit DCI encoding by binary search over 4096 host-built
-// thresholds in shared memory (no pow on the device), DC shift and forward ICT.
+// EOTF lookup, 3x3 to XYZ, the 12-bit DCI encoding as the count of 4096 host-built
+// thresholds at or below the value (a fast power gives the first guess, the thresholds
+// decide), DC shift and forward ICT.
 //
 // Float arithmetic is compiled without contraction and written in the reference's
 // operation order (Josephur/libgail core/dwt_cpu.cpp:24-93, core/color.cpp:142-189,
@@ -29,12 +33,16 @@ namespace {
 
 constexpr int TS = 64, HALO = 4, TW = TS + 2 * HALO, TP = TW + 1;
 constexpr int FE_THREADS = 256;
-__constant__ float kLiftF[4] = {(float)-1.586134342059924, (float)-0.052980118572961, (float)0.882911075530934,
-                             (float)0.443506852043971};
+// lifting coefficients alpha, beta, gamma, delta
+__device__ __forceinline__ constexpr float liftCoef(int s) {
+    return s == 0 ? (float)-1.586134342059924
+                  : s == 1 ? (float)-0.052980118572961 : s == 2 ? (float)0.882911075530934 : (float)0.443506852043971;
+}
 constexpr float kLowScale = (float)(1.0 / 1.230174104914001);
 constexpr float kHighScale = (float)1.230174104914001;
 
 __device__ __forceinline__ int mirror(int i, int n) {
+    if ((unsigned)i < (unsigned)n) return i;
     if (n == 1) return 0;
     const int period = 2 * (n - 1);
     i %= period;
@@ -81,11 +89,18 @@ __device__ void planarRgb(const void* src, const PlanarParams& p, int x, int y, 
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const size_t off = k ? vOff : uOff;
+        // a weight of exactly zero multiplies a finite sample >= 0 to +0, and adding +0
+        // changes nothing: those loads are skipped, the arithmetic kept
         const float a = sampleAt(src, p.bits, off + (size_t)y0 * p.cw + x0);
-        const float b = sampleAt(src, p.bits, off + (size_t)y0 * p.cw + x1);
-        const float c = sampleAt(src, p.bits, off + (size_t)y1 * p.cw + x0);
-        const float d = sampleAt(src, p.bits, off + (size_t)y1 * p.cw + x1);
-        uv[k] = (a * (1 - fx) + b * fx) * (1 - fy) + (c * (1 - fx) + d * fx) * fy;
+        const float b = fx != 0.f ? sampleAt(src, p.bits, off + (size_t)y0 * p.cw + x1) : 0.f;
+        const float top = a * (1 - fx) + b * fx;
+        float bot = 0.f;
+        if (fy != 0.f) {
+            const float c = sampleAt(src, p.bits, off + (size_t)y1 * p.cw + x0);
+            const float d = fx != 0.f ? sampleAt(src, p.bits, off + (size_t)y1 * p.cw + x1) : 0.f;
+            bot = c * (1 - fx) + d * fx;
+        }
+        uv[k] = top * (1 - fy) + bot * fy;
     }
     float Y = sampleAt(src, p.bits, (size_t)ay * p.aw + ax), U = uv[0], V = uv[1];
     float v[3];
@@ -111,58 +126,48 @@ __device__ void planarRgb(const void* src, const PlanarParams& p, int x, int y, 
     for (int c = 0; c < 3; ++c) rgb[c] = round16(clamp01(v[c]) * 65535.f);
 }
 
-// 12-bit code: the number of thresholds at or below n (thr[0] = 0).
-__device__ __forceinline__ int dciCode(const float* thr, float n) {
-    int k = 0;
-#pragma unroll
+// 12-bit code: the number of thresholds at or below n (thr[0] = 0, thr ascending). A
+// fast power gives a guess within a code or two; the thresholds then decide exactly, with
+// a binary search when the guess is further off than a few steps.
+__device__ __forceinline__ int dciCode(const float* __restrict__ thr, float n) {
+    int k = (int)(4095.f * __powf(n, 1.f / 2.6f) + 0.5f);
+    k = min(max(k, 0), 4095);
+#pragma unroll 1
+    for (int it = 0; it < 8; ++it) {
+        if (k < 4095 && __ldg(thr + k + 1) <= n) {
+            ++k;
+        } else if (k > 0 && __ldg(thr + k) > n) {
+            --k;
+        } else {
+            return k;
+        }
+    }
+    k = 0;
+#pragma unroll 1
     for (int step = 2048; step > 0; step >>= 1)
-        if (k + step <= 4095 && thr[k + step] <= n) k += step;
+        if (k + step <= 4095 && __ldg(thr + k + step) <= n) k += step;
     return k;
 }
 
-__device__ __forceinline__ int eotfIndex(uint32_t code16) {
-    const float v = code16 / 65535.f;
-    return (int)floorf(clamp01(v) * 65535.0f + 0.5f);
-}
-
-// Lifting steps along columns (rows of the tile) of one component, then the scaling.
-__device__ void liftColumns(float* t, int tid) {
-#pragma unroll 1
-    for (int s = 0; s < 4; ++s) {
-        const int first = (s & 1) ? 2 : 1;  // alpha, gamma: odd samples; beta, delta: even
-        const float c = kLiftF[s];
-        for (int idx = tid; idx < TW * 35; idx += FE_THREADS) {
-            const int col = idx % TW, i = first + 2 * (idx / TW);
-            float* x = t + i * TP + col;
-            x[0] += c * (x[-TP] + x[TP]);
+// One 72-sample line of a tile, `step` floats between samples: the four lifting steps
+// (x[i] += c * (x[i-1] + x[i+1]) on odd 1..69, even 2..70, odd, even), then the scaling of
+// the 64 samples the tile outputs, written back in place. Sample k is final once delta
+// has passed k + 1, so it is stored five samples behind the loads.
+__device__ __forceinline__ void liftLine(float* t, int step) {
+    float x[TW];
+#pragma unroll
+    for (int j = 0; j < TW + 5; ++j) {
+        if (j < TW) x[j] = t[j * step];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int i = j - 1 - s;
+            const bool odd = !(s & 1);
+            if (i >= (odd ? 1 : 2) && i <= (odd ? 69 : 70) && (i & 1) == (odd ? 1 : 0))
+                x[i] = x[i] + liftCoef(s) * (x[i - 1] + x[i + 1]);
         }
-        __syncthreads();
+        const int k = j - 5;
+        if (k >= HALO && k < HALO + TS) t[k * step] = x[k] * ((k & 1) ? kHighScale : kLowScale);
     }
-    for (int idx = tid; idx < TS * TW; idx += FE_THREADS) {
-        const int col = idx % TW, r = HALO + idx / TW;
-        t[r * TP + col] *= (r & 1) ? kHighScale : kLowScale;
-    }
-    __syncthreads();
-}
-
-// Lifting along rows for the rows that produce output, then the scaling.
-__device__ void liftRows(float* t, int tid) {
-#pragma unroll 1
-    for (int s = 0; s < 4; ++s) {
-        const int first = (s & 1) ? 2 : 1;
-        const float c = kLiftF[s];
-        for (int idx = tid; idx < TS * 35; idx += FE_THREADS) {
-            const int r = HALO + idx % TS, i = first + 2 * (idx / TS);
-            float* x = t + r * TP + i;
-            x[0] += c * (x[-1] + x[1]);
-        }
-        __syncthreads();
-    }
-    for (int idx = tid; idx < TS * TS; idx += FE_THREADS) {
-        const int r = HALO + idx % TS, col = HALO + idx / TS;
-        t[r * TP + col] *= (col & 1) ? kHighScale : kLowScale;
-    }
-    __syncthreads();
 }
 
 // The tile's outputs for component comp: its code-block of each band (and LL floats).
@@ -193,16 +198,12 @@ __device__ void writeOutputs(const LevelArgs& a, const float* t, int comp, int t
 }
 
 template <bool COLOR>
-__global__ void __launch_bounds__(FE_THREADS) levelKernel(ColorArgs c, LevelArgs a) {
+__global__ void __launch_bounds__(FE_THREADS, 3) levelKernel(ColorArgs c, LevelArgs a) {
     extern __shared__ float smem[];
-    constexpr int NC = COLOR ? 3 : 1;
-    float* thr = smem + NC * TW * TP;
     const int tid = threadIdx.x, tx = blockIdx.x, ty = blockIdx.y;
     const int x0 = tx * TS - HALO, y0 = ty * TS - HALO;
     const int w = a.w, h = a.h;
     if (COLOR) {
-        for (int i = tid; i < 4096; i += FE_THREADS) thr[i] = c.thr[i];
-        __syncthreads();
         for (int idx = tid; idx < TW * TW; idx += FE_THREADS) {
             const int ly = idx / TW, lx = idx % TW;
             const int gy = mirror(y0 + ly, h), gx = mirror(x0 + lx, w);
@@ -215,13 +216,15 @@ __global__ void __launch_bounds__(FE_THREADS) levelKernel(ColorArgs c, LevelArgs
             } else {
                 planarRgb(c.src, c.pp, gx, gy, rgb);
             }
-            const float R = c.eotf[eotfIndex(rgb[0])], G = c.eotf[eotfIndex(rgb[1])], B = c.eotf[eotfIndex(rgb[2])];
+            // the EOTF table index floor(clamp(code / 65535) * 65535 + 0.5) is the code
+            // itself for every 16-bit code (checked exhaustively in float32)
+            const float R = __ldg(c.eotf + rgb[0]), G = __ldg(c.eotf + rgb[1]), B = __ldg(c.eotf + rgb[2]);
             const float X = c.m[0] * R + c.m[1] * G + c.m[2] * B;
             const float Yv = c.m[3] * R + c.m[4] * G + c.m[5] * B;
             const float Z = c.m[6] * R + c.m[7] * G + c.m[8] * B;
-            const int cx = dciCode(thr, clamp01(X / 52.37f));
-            const int cy = dciCode(thr, clamp01(Yv / 52.37f));
-            const int cz = dciCode(thr, clamp01(Z / 52.37f));
+            const int cx = dciCode(c.thr, clamp01(X / 52.37f));
+            const int cy = dciCode(c.thr, clamp01(Yv / 52.37f));
+            const int cz = dciCode(c.thr, clamp01(Z / 52.37f));
             if (c.xyz && lx >= HALO && lx < HALO + TS && ly >= HALO && ly < HALO + TS && x0 + lx < w && y0 + ly < h) {
                 uint16_t* o = c.xyz + ((size_t)(y0 + ly) * w + (x0 + lx)) * 3;
                 o[0] = (uint16_t)cx;
@@ -234,24 +237,31 @@ __global__ void __launch_bounds__(FE_THREADS) levelKernel(ColorArgs c, LevelArgs
             smem[2 * TW * TP + ly * TP + lx] = (float)0.5 * fx + (float)(-0.41869) * fy + (float)(-0.08131) * fz;
         }
     } else {
-        const int comp = blockIdx.z;
-        const float* src = a.src + comp * a.srcComp;
-        for (int idx = tid; idx < TW * TW; idx += FE_THREADS) {
-            const int ly = idx / TW, lx = idx % TW;
-            smem[ly * TP + lx] = src[(size_t)mirror(y0 + ly, h) * a.srcStride + mirror(x0 + lx, w)];
+        for (int idx = tid; idx < 3 * TW * TW; idx += FE_THREADS) {
+            const int comp = idx / (TW * TW), e = idx - comp * TW * TW;
+            const int ly = e / TW, lx = e % TW;
+            smem[comp * TW * TP + ly * TP + lx] =
+                a.src[comp * a.srcComp + (size_t)mirror(y0 + ly, h) * a.srcStride + mirror(x0 + lx, w)];
         }
     }
     __syncthreads();
-    for (int k = 0; k < NC; ++k) {
-        float* t = smem + k * TW * TP;
-        if (h >= 2) liftColumns(t, tid);
-        if (w >= 2) liftRows(t, tid);
-        writeOutputs(a, t, COLOR ? k : (int)blockIdx.z, tx, ty, tid);
+    // columns: one thread per (component, column), all 72 columns
+    if (h >= 2 && tid < 3 * TW) {
+        const int comp = tid / TW, col = tid - comp * TW;
+        liftLine(smem + comp * TW * TP + col, TP);
     }
+    __syncthreads();
+    // rows: one thread per (component, output row)
+    if (w >= 2 && tid < 3 * TS) {
+        const int comp = tid / TS, r = HALO + (tid - comp * TS);
+        liftLine(smem + comp * TW * TP + r * TP, 1);
+    }
+    __syncthreads();
+    for (int k = 0; k < 3; ++k) writeOutputs(a, smem + k * TW * TP, k, tx, ty, tid);
 }
 
-constexpr size_t kSmemColor = (size_t)3 * TW * TP * 4 + 4096 * 4;
-constexpr size_t kSmemPlain = (size_t)TW * TP * 4;
+constexpr size_t kSmemColor = (size_t)3 * TW * TP * 4;
+constexpr size_t kSmemPlain = (size_t)3 * TW * TP * 4;
 
 }  // namespace
 
@@ -267,7 +277,7 @@ void launchLevel1(const ColorArgs& c, const LevelArgs& a, cudaStream_t st) {
 }
 
 void launchLevel(const LevelArgs& a, cudaStream_t st) {
-    const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 3);
+    const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 1);
     levelKernel<false><<<grid, FE_THREADS, kSmemPlain, st>>>(ColorArgs{}, a);
     GB_CHECK(cudaGetLastError());
 }
