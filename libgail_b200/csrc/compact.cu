@@ -3,11 +3,14 @@
 // core/tier1_types.h:12-28): CblkInfo per block, pass lengths and distortions back to
 // back, codewords back to back on 4-byte boundaries.
 //
-// Two launches over tiles of 1024 blocks: the tile sums, then per tile one CTA that adds
-// up the sums of the tiles before it, scans its own blocks in shared memory, writes the
-// CblkInfo records as contiguous words and copies the pass tables and codewords, a warp
-// per block. Nothing is read from the output buffers, which may be mapped host memory.
+// Three launches: the sums of tiles of 1024 blocks; per tile one CTA that adds up the
+// sums of the tiles before it, scans its own blocks in shared memory and writes the
+// CblkInfo records as contiguous words and each block's offsets to a device table; then
+// a warp per block copies the pass tables and the codeword. Nothing is read from the
+// output buffers, which may be mapped host memory.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "common.cuh"
 #include "compact.cuh"
@@ -66,7 +69,7 @@ __global__ void __launch_bounds__(TILE) tileSumKernel(CompactArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(TILE) packKernel(CompactArgs a) {
+__global__ void __launch_bounds__(TILE) scanKernel(CompactArgs a) {
     __shared__ uint32_t sRec[TILE * INFO_WORDS];
     __shared__ uint32_t sB[32], sP[32], sBase[2];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -116,32 +119,47 @@ __global__ void __launch_bounds__(TILE) packKernel(CompactArgs a) {
         r[2] = dOff;
         r[3] = a.info[4 * (size_t)i + 3];
         r[4] = pOff;
+        a.offsets[i] = make_uint2(dOff, pOff);
     }
     __syncthreads();
     // the CblkInfo records, contiguous words
     uint32_t* outInfo = a.outInfo + (size_t)INFO_WORDS * first;
     for (uint32_t k = tid; k < count * INFO_WORDS; k += TILE) outInfo[k] = sRec[k];
-    // pass tables and codewords, a warp per block
+}
+
+// A warp per block: its pass tables and codeword to their packed places.
+__global__ void __launch_bounds__(256) copyKernel(CompactArgs a) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     bool over = false;
-    for (uint32_t k = wid; k < count; k += TILE / 32) {
-        const uint32_t* r = sRec + INFO_WORDS * k;
-        const uint32_t blk = first + k, np = r[1], off = r[2], len = r[3], po = r[4];
+    for (uint32_t blk = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); blk < a.n; blk += warps) {
+        const uint2 o = a.offsets[blk];
+        const uint4 in = reinterpret_cast<const uint4*>(a.info)[blk];
+        const uint32_t np = in.y, len = in.w;
         const size_t src = (size_t)blk * kMaxPasses;
         for (uint32_t q = lane; q < np; q += 32) {
-            a.outPassLen[po + q] = a.passLen[src + q];
-            a.outPassDist[po + q] = a.passDist[src + q];
+            a.outPassLen[o.y + q] = a.passLen[src + q];
+            a.outPassDist[o.y + q] = a.passDist[src + q];
         }
         const uint32_t words = (len + 3u) >> 2;
-        if ((uint64_t)off + words * 4ull > a.dataCap) {
+        if ((uint64_t)o.x + words * 4ull > a.dataCap) {
             over = true;
             continue;
         }
         const uint32_t* cw = reinterpret_cast<const uint32_t*>(a.jobs[blk].cw);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(a.outData + off);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(a.outData + o.x);
         // the bytes past the codeword in its last word are zeroed so that the packed frame
         // does not depend on what the region held before
         const uint32_t tailMask = (len & 3u) ? (1u << (8 * (len & 3u))) - 1u : 0xFFFFFFFFu;
-        for (uint32_t w = lane; w < words; w += 32) dst[w] = w == words - 1 ? cw[w] & tailMask : cw[w];
+        uint32_t w = lane;
+        for (; w + 97 < words; w += 128) {  // four loads in flight per lane, never the last word
+            const uint32_t v0 = cw[w], v1 = cw[w + 32], v2 = cw[w + 64], v3 = cw[w + 96];
+            dst[w] = v0;
+            dst[w + 32] = v1;
+            dst[w + 64] = v2;
+            dst[w + 96] = v3;
+        }
+        for (; w < words; w += 32) dst[w] = w == words - 1 ? cw[w] & tailMask : cw[w];
     }
     if (__any_sync(kFull, over) && lane == 0) a.tot[2] = 1u;
 }
@@ -152,7 +170,14 @@ void compactTier1(const CompactArgs& a, cudaStream_t st) {
     if (a.n == 0) return;
     const uint32_t tiles = divUp(a.n, (uint32_t)TILE);
     tileSumKernel<<<tiles, TILE, 0, st>>>(a);
-    packKernel<<<tiles, TILE, 0, st>>>(a);
+    scanKernel<<<tiles, TILE, 0, st>>>(a);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // into host memory the copy is bound by the bus: a third of the SMs keep it busy and
+    // leave the rest to the kernels of other streams
+    const uint32_t cap = a.hostOut ? (uint32_t)std::max(1, sms / 3) : (uint32_t)sms * 8;
+    copyKernel<<<std::min(divUp(a.n, 8u), cap), 256, 0, st>>>(a);
     GB_CHECK(cudaGetLastError());
 }
 

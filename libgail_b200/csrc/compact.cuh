@@ -22,6 +22,8 @@ struct CompactArgs {
     uint64_t dataCap;          // bytes outData holds
     uint32_t* scratch;         // device, 2 words per 1024 blocks; free once MQ coding ended
                                // on this stream, so the Tier-1 launch's perm table will do
+    uint2* offsets;            // device, per block: codeword byte offset, pass offset
+    int hostOut;               // the out* buffers are mapped host memory: fewer copying CTAs
 };
 
 // The out* pointers and tot may be mapped host memory: the kernels only write them, with

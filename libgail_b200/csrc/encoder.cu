@@ -36,7 +36,7 @@ uint64_t SlotSizes::deviceBytes() const {
     const uint64_t sizes[] = {inBytes,     65536 * 4,   4096 * 4,    2 * llFloats * 4 * 3, n * kCblkArea * 4,
                               n * 48,      arena,       arena,       n * 16,               n * kMaxPasses * 4 * 3,
                               n * kMaxPasses * 16,      n * 4,       64,                   n * 20,
-                              n * kMaxPasses * 8,       arena};
+                              n * 8,                    n * kMaxPasses * 8,       arena};
     uint64_t t = 0;
     for (uint64_t b : sizes) t += page(b);
     return t;
@@ -147,6 +147,7 @@ EncoderSlot::EncoderSlot(int device, const Layout& L, const GailCudaEncodeSettin
         alloc(dCtl_, 64);
         alloc(dSlope_, 16);
         alloc(dOutInfo_, n * 20);
+        alloc(dOffsets_, n * 8);
         alloc(dOutLen_, n * kMaxPasses * 4);
         alloc(dOutDist_, n * kMaxPasses * 4);
         alloc(dOutData_, z_.arena);
@@ -244,8 +245,8 @@ void EncoderSlot::enqueueStages(const void* dFrame, bool taps, bool full) {
     t1Encode(t, st, mark ? mark + 2 : nullptr);
     GB_CHECK(cudaEventRecord(ev_[3], st));
     if (mark) GB_CHECK(cudaEventRecord(mark[4], st));
-    CompactArgs ca{(uint32_t)n, dInfo_,    dLen_,      dDist_, dJobs_, dOutInfo_, dOutLen_,
-                   dOutDist_,   dOutData_, dCtl_ + 8, z_.arena, dPerm_};
+    CompactArgs ca{(uint32_t)n, dInfo_,    dLen_,      dDist_,   dJobs_,    dOutInfo_, dOutLen_,
+                   dOutDist_,   dOutData_, dCtl_ + 8, z_.arena, dPerm_,    dOffsets_, 0};
     compactTier1(ca, st);
     if (mark) GB_CHECK(cudaEventRecord(mark[5], st));
 }

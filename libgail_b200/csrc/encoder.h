@@ -94,6 +94,7 @@ private:
              *dCtl_ = nullptr, *dOutInfo_ = nullptr, *dOutLen_ = nullptr;
     int32_t *dDist_ = nullptr, *dOutDist_ = nullptr;
     uint4* dSnaps_ = nullptr;
+    uint2* dOffsets_ = nullptr;
     uint8_t *dSym_ = nullptr, *dCw_ = nullptr, *dOutData_ = nullptr;
     uint16_t* dXyz_ = nullptr;
     T1Job* dJobs_ = nullptr;

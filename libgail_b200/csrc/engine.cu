@@ -75,6 +75,7 @@ struct EncodeEngine::Batch {
     uint32_t *info = nullptr, *end = nullptr, *len = nullptr, *perm = nullptr, *ctl = nullptr, *hCtl = nullptr;
     int32_t* dist = nullptr;
     uint4* snaps = nullptr;
+    uint2* offs = nullptr;
     uint32_t cap = 0;
     std::vector<Request*> frames;
     bool busy = false;
@@ -355,6 +356,7 @@ bool EncodeEngine::launchBatch(Batch& b) {
         alloc(b.dist, cap * kMaxPasses * 4);
         alloc(b.snaps, cap * kMaxPasses * 16);
         alloc(b.perm, cap * 4);
+        alloc(b.offs, cap * 8);
         alloc(b.ctl, 64);
         b.cap = (uint32_t)cap;
     }
@@ -374,7 +376,7 @@ bool EncodeEngine::launchBatch(Batch& b) {
         std::memset(s->hTot, 0, 64);
         const uint32_t j = r->jobBase;
         CompactArgs ca{s->n,   b.info + 4 * (uint64_t)j, b.len + (uint64_t)kMaxPasses * j, b.dist + (uint64_t)kMaxPasses * j,
-                       b.dJobs + j, s->hInfo, s->hLen, s->hDist, s->hData, s->hTot, s->dataCap, b.perm};
+                       b.dJobs + j, s->hInfo, s->hLen, s->hDist, s->hData, s->hTot, s->dataCap, b.perm, b.offs, 1};
         compactTier1(ca, b.st);
     }
     GB_CHECK(cudaMemcpyAsync(b.hCtl, b.ctl, 64, cudaMemcpyDeviceToHost, b.st));

@@ -32,7 +32,9 @@ namespace gb {
 namespace {
 
 constexpr int TS = 64, HALO = 4, TW = TS + 2 * HALO, TP = TW + 1;
-constexpr int FE_THREADS = 256;
+// level 1: the three components of a tile per CTA (the colour conversion yields all
+// three at once); later levels: one component per CTA
+constexpr int FE_THREADS_COLOR = 384, FE_THREADS_PLAIN = 128;
 // lifting coefficients alpha, beta, gamma, delta
 __device__ __forceinline__ constexpr float liftCoef(int s) {
     return s == 0 ? (float)-1.586134342059924
@@ -171,6 +173,7 @@ __device__ __forceinline__ void liftLine(float* t, int step) {
 }
 
 // The tile's outputs for component comp: its code-block of each band (and LL floats).
+template <int THREADS>
 __device__ void writeOutputs(const LevelArgs& a, const float* t, int comp, int tx, int ty, int tid) {
     const int x0 = tx * TS - HALO, y0 = ty * TS - HALO;
     for (int o = 0; o < 4; ++o) {
@@ -178,7 +181,7 @@ __device__ void writeOutputs(const LevelArgs& a, const float* t, int comp, int t
         const bool quant = o != 0 || a.last;
         if (tx >= b.ncbx || ty >= b.ncby) continue;
         uint32_t* blk = a.coeffs + ((size_t)b.cblkBase + (size_t)ty * b.ncbx + tx) * kCblkArea;
-        for (int idx = tid; idx < kCblkArea; idx += FE_THREADS) {
+        for (int idx = tid; idx < kCblkArea; idx += THREADS) {
             const int i = idx & 31, j = idx >> 5;
             const int bx = tx * 32 + i, by = ty * 32 + j;
             const bool in = bx < b.w && by < b.h;
@@ -198,13 +201,16 @@ __device__ void writeOutputs(const LevelArgs& a, const float* t, int comp, int t
 }
 
 template <bool COLOR>
-__global__ void __launch_bounds__(FE_THREADS, 3) levelKernel(ColorArgs c, LevelArgs a) {
+__global__ void __launch_bounds__(COLOR ? FE_THREADS_COLOR : FE_THREADS_PLAIN, COLOR ? 3 : 8)
+    levelKernel(ColorArgs c, LevelArgs a) {
     extern __shared__ float smem[];
+    constexpr int THREADS = COLOR ? FE_THREADS_COLOR : FE_THREADS_PLAIN;
+    constexpr int NC = COLOR ? 3 : 1;
     const int tid = threadIdx.x, tx = blockIdx.x, ty = blockIdx.y;
     const int x0 = tx * TS - HALO, y0 = ty * TS - HALO;
     const int w = a.w, h = a.h;
     if (COLOR) {
-        for (int idx = tid; idx < TW * TW; idx += FE_THREADS) {
+        for (int idx = tid; idx < TW * TW; idx += THREADS) {
             const int ly = idx / TW, lx = idx % TW;
             const int gy = mirror(y0 + ly, h), gx = mirror(x0 + lx, w);
             uint32_t rgb[3];
@@ -237,31 +243,30 @@ __global__ void __launch_bounds__(FE_THREADS, 3) levelKernel(ColorArgs c, LevelA
             smem[2 * TW * TP + ly * TP + lx] = (float)0.5 * fx + (float)(-0.41869) * fy + (float)(-0.08131) * fz;
         }
     } else {
-        for (int idx = tid; idx < 3 * TW * TW; idx += FE_THREADS) {
-            const int comp = idx / (TW * TW), e = idx - comp * TW * TW;
-            const int ly = e / TW, lx = e % TW;
-            smem[comp * TW * TP + ly * TP + lx] =
-                a.src[comp * a.srcComp + (size_t)mirror(y0 + ly, h) * a.srcStride + mirror(x0 + lx, w)];
+        const float* src = a.src + blockIdx.z * a.srcComp;
+        for (int idx = tid; idx < TW * TW; idx += THREADS) {
+            const int ly = idx / TW, lx = idx % TW;
+            smem[ly * TP + lx] = src[(size_t)mirror(y0 + ly, h) * a.srcStride + mirror(x0 + lx, w)];
         }
     }
     __syncthreads();
     // columns: one thread per (component, column), all 72 columns
-    if (h >= 2 && tid < 3 * TW) {
+    if (h >= 2 && tid < NC * TW) {
         const int comp = tid / TW, col = tid - comp * TW;
         liftLine(smem + comp * TW * TP + col, TP);
     }
     __syncthreads();
     // rows: one thread per (component, output row)
-    if (w >= 2 && tid < 3 * TS) {
+    if (w >= 2 && tid < NC * TS) {
         const int comp = tid / TS, r = HALO + (tid - comp * TS);
         liftLine(smem + comp * TW * TP + r * TP, 1);
     }
     __syncthreads();
-    for (int k = 0; k < 3; ++k) writeOutputs(a, smem + k * TW * TP, k, tx, ty, tid);
+    for (int k = 0; k < NC; ++k) writeOutputs<THREADS>(a, smem + k * TW * TP, COLOR ? k : (int)blockIdx.z, tx, ty, tid);
 }
 
 constexpr size_t kSmemColor = (size_t)3 * TW * TP * 4;
-constexpr size_t kSmemPlain = (size_t)3 * TW * TP * 4;
+constexpr size_t kSmemPlain = (size_t)TW * TP * 4;
 
 }  // namespace
 
@@ -272,13 +277,13 @@ void frontendInit() {
 
 void launchLevel1(const ColorArgs& c, const LevelArgs& a, cudaStream_t st) {
     const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 1);
-    levelKernel<true><<<grid, FE_THREADS, kSmemColor, st>>>(c, a);
+    levelKernel<true><<<grid, FE_THREADS_COLOR, kSmemColor, st>>>(c, a);
     GB_CHECK(cudaGetLastError());
 }
 
 void launchLevel(const LevelArgs& a, cudaStream_t st) {
-    const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 1);
-    levelKernel<false><<<grid, FE_THREADS, kSmemPlain, st>>>(ColorArgs{}, a);
+    const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 3);
+    levelKernel<false><<<grid, FE_THREADS_PLAIN, kSmemPlain, st>>>(ColorArgs{}, a);
     GB_CHECK(cudaGetLastError());
 }
 
