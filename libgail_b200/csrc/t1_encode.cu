@@ -431,6 +431,16 @@ __global__ void __launch_bounds__(1024) t1OrderKernel(T1Launch P) {
 }
 
 // ---------------------------------------------------------------------------- MQ coding
+// Context state word: Qe | MPS << 16 | state index << 17. The next-state table has four
+// entries per state, by (MPS, LPS): the state word after a renormalising decision.
+__device__ __forceinline__ uint32_t nextStateEntry(uint32_t k) {
+    const uint32_t idx = k >> 2, mps = (k >> 1) & 1u, lps = k & 1u, e = c_mq[idx];
+    const uint32_t nidx = lps ? (e >> 24) & 63u : (e >> 18) & 63u;
+    const uint32_t nm = mps ^ (lps ? (e >> 17) & 1u : 0u);
+    return (c_mq[nidx] & 0xFFFFu) | (nm << 16) | (nidx << 17);
+}
+__device__ __forceinline__ uint32_t initialState(uint32_t idx) { return (c_mq[idx] & 0xFFFFu) | (idx << 17); }
+
 struct Coder {
     uint32_t A, C, B;
     int CT, bp;
@@ -438,56 +448,46 @@ struct Coder {
     uint32_t cap;
     bool overflow;
 
+    // Annex C BYTEOUT with its three cases as selects: after 0xFF a stuffed bit (7 bits
+    // next); otherwise a carry into the pending byte, which may make it 0xFF.
     __device__ __forceinline__ void byteout() {
-        bool stuff = B == 0xFFu;
-        if (!stuff && C >= 0x8000000u) {
-            B += 1u;  // carry into the pending byte
-            if (B == 0xFFu) {
-                C &= 0x7FFFFFFu;
-                stuff = true;
-            }
-        }
+        const bool carry = B != 0xFFu && C >= 0x8000000u;
+        B += carry ? 1u : 0u;
+        C &= carry ? 0x7FFFFFFu : 0xFFFFFFFFu;
+        const bool stuff = B == 0xFFu;
         if (bp >= 0) {
             if ((uint32_t)bp < cap) out[bp] = (uint8_t)B;
             else overflow = true;
         }
         ++bp;
-        if (stuff) {
-            B = C >> 20;
-            C &= 0xFFFFFu;
-            CT = 7;
-        } else {
-            B = (C >> 19) & 0xFFu;
-            C &= 0x7FFFFu;
-            CT = 8;
-        }
+        B = (C >> (stuff ? 20 : 19)) & 0xFFu;
+        C &= stuff ? 0xFFFFFu : 0x7FFFFu;
+        CT = stuff ? 7 : 8;
     }
-    __device__ __forceinline__ void renorm() {
-        int n = __clz(A) - 16;
-        do {
-            const int s = min(n, CT);
-            A <<= s;
-            C <<= s;
-            CT -= s;
-            n -= s;
-            if (CT == 0) byteout();
-        } while (n > 0);
-    }
-    // One decision in context state t (table entry | mps << 16); returns the new state.
-    __device__ __forceinline__ uint32_t encode(uint32_t t, uint32_t d, const uint32_t* tab) {
-        const uint32_t qe = t & 0xFFFFu, mps = (t >> 16) & 1u;
+    // One decision in context state t; returns the context's next state. Renormalisation
+    // shifts by clz(A) - 16, which is 0 when A stayed at or above 0x8000; the byte-out is the
+    // only branch.
+    __device__ __forceinline__ uint32_t encode(uint32_t t, uint32_t d, const uint32_t* next) {
+        const uint32_t qe = t & 0xFFFFu;
         const uint32_t a = A - qe;
-        const bool lps = d != mps;
+        const bool lps = d != ((t >> 16) & 1u);
         const bool upper = (a >= qe) != lps;  // which sub-interval the decision takes
         C += upper ? qe : 0u;
         A = upper ? a : qe;
-        if (lps || !(a & 0x8000u)) {
-            const uint32_t nidx = lps ? (t >> 24) & 63u : (t >> 18) & 63u;
-            const uint32_t nm = mps ^ (lps ? (t >> 17) & 1u : 0u);
-            t = tab[nidx] | (nm << 16);
-            renorm();
+        const bool rn = lps || !(a & 0x8000u);
+        const uint32_t nt = next[((t >> 15) & ~1u) | (lps ? 1u : 0u)];
+        int n = __clz(A) - 16;
+        A <<= n;
+        for (;;) {
+            const int sh = min(n, CT);
+            C <<= sh;
+            CT -= sh;
+            n -= sh;
+            if (CT != 0) break;
+            byteout();
+            if (n == 0) break;
         }
-        return t;
+        return rn ? nt : t;
     }
     __device__ __forceinline__ uint32_t flush() {
         const uint32_t tempc = C + A;
@@ -531,15 +531,23 @@ __device__ uint32_t truncLen(uint4 s, const uint8_t* buf, uint32_t len, uint32_t
 }
 
 __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
-    __shared__ uint32_t s_tab[48];
+    __shared__ uint32_t s_next[4 * 47];
+    __shared__ uint32_t s_init[4];
     __shared__ uint32_t s_ctx[19 * MQ_THREADS];
-    for (int i = threadIdx.x; i < 47; i += blockDim.x) s_tab[i] = c_mq[i];
+    for (int i = threadIdx.x; i < 4 * 47; i += blockDim.x) s_next[i] = nextStateEntry(i);
+    if (threadIdx.x == 0) {
+        s_init[0] = initialState(0);
+        s_init[1] = initialState(4);
+        s_init[2] = initialState(3);
+        s_init[3] = initialState(46);
+    }
     __syncthreads();
     uint32_t* ctx = s_ctx + threadIdx.x;
     uint32_t* status = P.ctl + 1;
 
-    // Per-lane state of the block in hand.
-    uint32_t job = 0, pos = 0, nsym = 0, np = 0, k = 0, nextEnd = 0;
+    // Per-lane state of the block in hand. Invariant between decisions: s is the decision
+    // at pos and t the state of its context.
+    uint32_t job = 0, pos = 0, nsym = 0, np = 0, k = 0, nextEnd = 0, stop = 0, s = 0, t = 0;
     const uint8_t* sym = nullptr;
     uint4 nxt = make_uint4(0, 0, 0, 0);  // the block's next 16 decisions
     Coder e;
@@ -547,7 +555,8 @@ __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
     bool have = false;
 
     for (;;) {
-        if (!have || pos == nsym) {
+        uint4 v;
+        if (!have || pos >= nsym) {
             if (have) {
                 // end of block: remaining pass ends, flush, truncation points
                 while (k < np) {
@@ -594,43 +603,63 @@ __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
             e.overflow = false;
             // initial states, Table D.7: ZC context 0 state 4, run-length 3, uniform 46
 #pragma unroll
-            for (int c = 0; c < 19; ++c) ctx[c * MQ_THREADS] = s_tab[0];
-            ctx[0] = s_tab[4];
-            ctx[17 * MQ_THREADS] = s_tab[3];
-            ctx[18 * MQ_THREADS] = s_tab[46];
+            for (int c = 0; c < 19; ++c) ctx[c * MQ_THREADS] = s_init[0];
+            ctx[0] = s_init[1];
+            ctx[17 * MQ_THREADS] = s_init[2];
+            ctx[18 * MQ_THREADS] = s_init[3];
             pos = 0;
             k = 0;
             nextEnd = P.passEnd[(size_t)job * kMaxPasses];
-            nxt = nsym ? *reinterpret_cast<const uint4*>(sym) : make_uint4(0, 0, 0, 0);
+            stop = min(nsym, nextEnd);
             have = true;
             if (nsym == 0) continue;
+            v = *reinterpret_cast<const uint4*>(sym);
+            nxt = nsym > 16 ? *reinterpret_cast<const uint4*>(sym + 16) : make_uint4(0, 0, 0, 0);
+            s = v.x & 0xFFu;
+            t = ctx[(s >> 1) * MQ_THREADS];
+        } else {
+            v = nxt;
+            nxt = (pos + 16 < nsym) ? *reinterpret_cast<const uint4*>(sym + pos + 16) : make_uint4(0, 0, 0, 0);
         }
-        // One aligned chunk of 16 decisions (fewer at the block's end), unrolled so that
-        // every byte is taken from a fixed place; the next decision's context state is
-        // read ahead, off the serial chain of the coder.
-        const uint4 v = nxt;
-        nxt = (pos + 16 < nsym) ? *reinterpret_cast<const uint4*>(sym + pos + 16) : make_uint4(0, 0, 0, 0);
-        const uint32_t words[4] = {v.x, v.y, v.z, v.w};
-        uint32_t s = words[0] & 0xFFu;
-        uint32_t t = ctx[(s >> 1) * MQ_THREADS];
+        // one aligned chunk of 16 decisions (fewer at the block's end): a word of four
+        // decisions unrolled at a time, the next decision's context state read ahead, off
+        // the serial chain of the coder
+        uint32_t w0 = v.x, w1 = v.y, w2 = v.z, w3 = v.w;
+        const uint32_t w4 = nxt.x;
+        bool done = false;
+#pragma unroll 1
+        for (int q = 0; q < 4 && !done; ++q) {
+            const uint32_t cur = w0;
 #pragma unroll
-        for (int b = 0; b < 16; ++b) {
-            if (pos >= nsym) break;
-            while (pos == nextEnd && k < np) {
-                P.snaps[(size_t)job * kMaxPasses + k] = make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
-                ++k;
-                nextEnd = k < np ? P.passEnd[(size_t)job * kMaxPasses + k] : 0xFFFFFFFFu;
+            for (int b = 0; b < 4; ++b) {
+                if (pos >= stop) {
+                    if (pos >= nsym) {
+                        done = true;
+                        break;
+                    }
+                    while (pos == nextEnd && k < np) {  // pass ends before this decision
+                        P.snaps[(size_t)job * kMaxPasses + k] =
+                            make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
+                        ++k;
+                        nextEnd = k < np ? P.passEnd[(size_t)job * kMaxPasses + k] : 0xFFFFFFFFu;
+                    }
+                    stop = min(nsym, nextEnd);
+                }
+                // the byte past the block's last decision is not a decision: the clamp keeps
+                // its look-ahead read inside the lane's 19 contexts
+                const uint32_t sn = b < 3 ? (cur >> (8 * (b + 1))) & 0xFFu : w1 & 0xFFu;
+                const uint32_t cn = min(sn >> 1, 18u), cx = s >> 1;
+                const uint32_t tn = ctx[cn * MQ_THREADS];
+                const uint32_t tNew = e.encode(t, s & 1u, s_next);
+                ctx[cx * MQ_THREADS] = tNew;
+                t = cn == cx ? tNew : tn;
+                s = sn;
+                ++pos;
             }
-            // the byte past the block's last decision is not a decision: the clamp keeps
-            // its look-ahead read inside the lane's 19 contexts
-            const uint32_t sn = b < 15 ? (words[(b + 1) >> 2] >> (8 * ((b + 1) & 3))) & 0xFFu : 0u;
-            const uint32_t tn = ctx[min(sn >> 1, 18u) * MQ_THREADS];
-            const uint32_t cx = s >> 1;
-            const uint32_t tNew = e.encode(t, s & 1u, s_tab);
-            ctx[cx * MQ_THREADS] = tNew;
-            t = (sn >> 1) == cx ? tNew : tn;
-            s = sn;
-            ++pos;
+            w0 = w1;
+            w1 = w2;
+            w2 = w3;
+            w3 = w4;
         }
     }
 }
