@@ -66,10 +66,6 @@ def parse():
     return ap.parse_args()
 
 
-def rank_info():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
-
-
 class Clocks:
     """nvidia-smi samples during the timed region."""
 
@@ -117,9 +113,9 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def gen_frames(count):
+def gen_frames(count, seed=1000):
     from libgail_b200 import synth
-    return synth.many(synth.yuv422p10, count, W4K, H4K, seed=1000)
+    return synth.many(synth.yuv422p10, count, W4K, H4K, seed=seed)
 
 
 def cpu_baseline(frames, sample=2):
@@ -155,6 +151,7 @@ def cpu_baseline(frames, sample=2):
 
 
 def run_reference(args):
+    from libgail_b200.replicas import rank_info
     rank, local, world = rank_info()
     if rank != 0:
         return
@@ -199,12 +196,11 @@ def poisson_arrivals(n, rate, seed=7):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
 
+    from libgail_b200.replicas import Replicas, rank_info
     rank, local, world = rank_info()
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
+    rep = Replicas("nccl", timeout_s=120, device=f"cuda:{local}")
     import libgail_b200 as gb
     from libgail_b200 import plugin as P
     from libgail_b200.engine import Engine
@@ -218,19 +214,14 @@ def run_ours(args):
     L.gb_encoder_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     cuda = f"cuda:{local}"
 
-    def reduce_max(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device=cuda, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    reduce_max = rep.max
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        torch.cuda.synchronize()
+        rep.barrier()
         torch.cuda.synchronize()
 
-    frames = gen_frames(args.frames)
+    frames = gen_frames(args.frames, seed=rep.frame_seed(1000))
     nbytes = frames[0].nbytes
     pinned = [torch.from_numpy(f.view(np.int16)).pin_memory() for f in frames]
     dframes = [p.to(cuda) for p in pinned]
@@ -433,8 +424,7 @@ def run_ours(args):
             except Exception as e:  # a missing baseline must not hide the measurement
                 out["cpu_baseline"] = {"unavailable": str(e)}
     dev.close()
-    if world > 1:
-        dist.destroy_process_group()
+    rep.close()
     if out is not None:
         print(json.dumps(out))
 

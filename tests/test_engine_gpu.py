@@ -1,7 +1,7 @@
 """The batched, served encoder: every frame's Tier-1 frame must be the same whether it was
 encoded alone through the plain per-frame path (the plugin's encoder_encode) or in a mix
-of frames of several profiles batched into shared Tier-1 launches, and the admission by
-HBM budget must let every request finish."""
+of frames of all six DCI profiles batched into shared Tier-1 launches, and the admission
+by HBM budget must let every request finish."""
 import numpy as np
 import pytest
 
@@ -22,11 +22,17 @@ def dev():
     d.close()
 
 
+# the six DCI profiles (width, height, 4K layout flag) and frames of each in the mix: 16
+# X'Y'Z' 12-bit frames in all, plus two Y'CbCr 4:2:2 PQ 4K frames for the colour path
+PROFILES = [(1998, 1080, 0, 3), (2048, 858, 0, 3), (2048, 1080, 0, 3), (3996, 2160, 1, 3), (4096, 1716, 1, 2),
+            (4096, 2160, 1, 2)]
+
+
 def _cases():
     # (layout args, format, colour, frames)
     out = []
-    for W, H, fk in [(1998, 1080, 0), (2048, 858, 0)]:
-        frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=100 + i)) for i in range(3)]
+    for W, H, fk, nf in PROFILES:
+        frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=100 * (1 + fk) + W % 97 + i)) for i in range(nf)]
         out.append(((W, H, fk), P.rgb48_format(W, H), P.color_passthrough(), frames))
     W, H = 3996, 2160
     frames = [synth.yuv422p10(W, H, seed=200 + i) for i in range(2)]
@@ -48,6 +54,7 @@ def test_engine_mix_equals_alone(dev):
         classes = [eng.add_encoder(lay, fmt, col)[0] for lay, (_, fmt, col, _) in zip(layouts, cases)]
         want = {}
         order = [(ci, fi) for fi in range(3) for ci in range(len(cases)) if fi < len(cases[ci][3])]
+        assert sum(len(c[3]) for c in cases[:6]) == 16
         for ci, fi in order:  # interleaved profiles
             rid = eng.submit(classes[ci], cases[ci][3][fi])
             want[rid] = alone[ci][fi]
