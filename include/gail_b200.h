@@ -129,6 +129,39 @@ GB_API int gb_engine_wait(GbEngine* e, int timeoutMs, int64_t* id, GailCudaTier1
 GB_API int gb_engine_release(GbEngine* e, int64_t id);
 GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5);
 
+/* The host codec around a Tier-1 frame, byte-identical to libgail's core for the same
+ * frame. Thread-safe across threads (each keeps its own writer per layout and label).
+ *   gb_dci_limits              DCI byte budgets at fps: whole frame under maxMbps (the
+ *                              reference's rate target is 230) and each component under
+ *                              compMbps (200); replaces dciLimits (src/core/rate_control.h:30)
+ *   gb_empty_codestream_bytes  the codestream with no pass: the smallest budget that can be
+ *                              met (emptyCodestreamBytes, src/core/t2.h:47)
+ *   gb_build_codestream        Tier-2 packets and the DCI codestream with passes[i] coding
+ *                              passes of block i (buildCodestream, src/core/t2.h:41); label +
+ *                              " " + tag (tag at most 9 bytes, none when empty) is the COM text
+ *   gb_rate_and_build          PCRD rate control under gb_dci_limits(fps, maxMbps, compMbps),
+ *                              then the codestream (allocateRate, src/core/rate_control.h:32,
+ *                              followed by buildCodestream, as src/core/pipeline.cpp:210-219);
+ *                              passesOut: one byte per block; out may be NULL to get the size
+ *   gb_check_dci               DCI compliance of a codestream at fps: *ok 1 or 0, msg the COM
+ *                              text or the first error (checkDciCodestream,
+ *                              src/core/codestream_check.h:33)
+ *   gb_parse_codestream        a DCI codestream read back for decoder_decode: its bands
+ *                              (geometry and signalled steps) and per-block code
+ *                              (parseCodestream + parsePackets, src/core/codestream_parse.h:53,
+ *                              src/core/t2_parse.h:27); arrays may be NULL to get the counts */
+GB_API int gb_dci_limits(double fps, double maxMbps, double compMbps, uint64_t* total, uint64_t* comp);
+GB_API int gb_empty_codestream_bytes(const GailCudaLayout* layout, const char* label, uint64_t* bytes);
+GB_API int gb_build_codestream(const GailCudaLayout* layout, const GailCudaTier1* t1, const uint8_t* passes,
+                               const char* label, const char* tag, uint8_t* out, uint64_t cap, uint64_t* size);
+GB_API int gb_rate_and_build(const GailCudaLayout* layout, const GailCudaTier1* t1, double fps, double maxMbps,
+                             double compMbps, const char* label, const char* tag, uint8_t* passesOut, uint8_t* out,
+                             uint64_t cap, uint64_t* size, double* lambda);
+GB_API int gb_check_dci(const uint8_t* data, uint64_t size, double fps, char* msg, uint64_t msgCap, int* ok);
+GB_API int gb_parse_codestream(const uint8_t* data, uint64_t size, GbSubband* bands, int maxBands, int* numBands,
+                               GbCblkCode* blocks, uint64_t maxBlocks, uint64_t* numBlocks, int* width, int* height,
+                               int* profile);
+
 /* FNV hash of the ABI structure sizes, as the plugin table's `layout` field carries it
  * (cudaPluginLayout, src/cuda/cuda_plugin.h:208-217). */
 GB_API uint64_t gb_plugin_layout_hash(void);

@@ -204,6 +204,15 @@ Layout makeLayout(int width, int height, int profile, double baseStep) {
     return L;
 }
 
+void setSignalledSteps(Layout& L, int comp, const int* eps, const int* mu) {
+    for (GbSubband& b : L.bands) {
+        if (b.comp != comp) continue;
+        const int i = b.res == 0 ? 0 : 1 + 3 * (b.res - 1) + (b.orient - 1);
+        applyStep(b, L.guardBits, eps[i], mu[i]);
+        b.weight = 0.0;  // only the encoder's rate control uses it
+    }
+}
+
 void layoutFromAbi(const GailCudaLayout& p, Layout& L) {
     if (p.numBands < 0 || p.numCblks < 0 || !p.bands) throw std::logic_error("frame layout is empty");
     if (L.profile != p.profile || L.width != p.width || L.height != p.height || L.levels != p.levels ||

@@ -61,6 +61,9 @@ Layout makeLayout(int width, int height, int profile, double baseStep);
 // Throws std::logic_error when the bands do not have the geometry of the size and levels.
 void layoutFromAbi(const GailCudaLayout& p, Layout& L);
 GailCudaLayout layoutToAbi(const Layout& L);
+// The steps of component comp's bands from a QCD's (eps, mu) pairs, in QCD band order.
+// Throws std::runtime_error on a step that needs more than 22 magnitude bit-planes.
+void setSignalledSteps(Layout& L, int comp, const int* eps, const int* mu);
 
 double synthesisNorm(int level, int orient);
 double ictSynthesisNorm(int comp);
