@@ -7,22 +7,26 @@ to 12-bit X'Y'Z', 9/7 wavelet with 6 levels, 32x32 code-blocks, Tier-1 with ever
 pass (bit-exact with the CPU reference). One step = encoding all 48 frames; the 48 frames
 (1.66 GB) are larger than L2, so no flush is needed between steps.
 
-  value   frames/s of the served path: the batched engine (continuous batching of Tier-1
-          over every frame in flight) on frames resident in HBM, Tier-1 frames written to
-          mapped host memory. The engine's work spans its own streams, so the timed region
-          is bracketed by a barrier and a device synchronisation on both sides; max over
-          ranks.
-  plain   the drop-in per-frame path beside it: frames/s with the frames resident in HBM
-          (CUDA events on the encoder's stream, with the per-stage split), frames/s end to
-          end through the plugin table's encoder_encode, and p50/p99 latency at a Poisson
-          load of 80 % of that end-to-end rate; served latency is taken at the same load.
-  e2e     frames/s of the served path with the frames in pinned host memory: each frame's
-          upload and its Tier-1 output in host memory are inside the timed region.
+  value   DCI codestreams/s of the served path: the batched engine (continuous batching of
+          Tier-1 over every frame in flight) on frames resident in HBM, Tier-1 frames written
+          to mapped host memory, each frame's rate control, Tier-2 and DCI check on the
+          engine's host workers. The work spans the engine's streams and threads, so the
+          timed region is bracketed by a barrier and a device synchronisation on both sides;
+          max over ranks.
+  plain   the drop-in per-frame path beside it, as libgail drives the plugin: slot threads,
+          each encoder_encode from host memory then rate control, Tier-2 and the DCI check;
+          codestreams/s and p50/p99 latency at a Poisson load of 80 % of that rate (served
+          latency at the same load); and, frames resident in HBM, the device stages alone
+          with the per-stage split (CUDA events on the encoder's stream).
+  e2e     codestreams/s of the served path with the frames in pinned host memory: each
+          frame's upload and its Tier-1 output in host memory are inside the timed region.
+  dci     every codestream of the timed runs checked: how many passed, the largest.
   stages  per stage of the plain path: live ms per frame, algorithmic bytes, GB/s and the
           fraction of the measured HBM bandwidth; roofline is the dominant stage.
 
---impl reference times the reference's own CPU encoder (the CpuSlot path, built from the
-reference sources into oracle/_ref) on the same frames with all host threads.
+--impl reference times the reference's own CPU path (the CpuSlot encoder, then its rate
+control, codestream writer and DCI checker, built from the reference sources into
+oracle/_ref) on the same frames with all host threads.
 """
 from __future__ import annotations
 
@@ -42,9 +46,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 W4K, H4K, FRAMES = 3996, 2160, 48
+FPS = 24.0  # DCI frame rate of the byte budgets
 METRIC = "4K encode fps & p99 frame latency, served vs plain, 1 B200, Tier-1 bit-exact"
 WORKLOAD = ("4K 3996x2160 Y'CbCr 4:2:2 10-bit BT.2020 PQ -> 12-bit X'Y'Z', 9/7 6 levels, 32x32 code-blocks, "
-            "Tier-1 all passes, 48 preloaded frames")
+            "Tier-1 all passes, PCRD to the 230 Mbit/s DCI budget at 24 fps, every codestream DCI-checked, "
+            "48 preloaded frames")
 
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on one 4K
@@ -63,6 +69,7 @@ def parse():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=16, help="most frames per Tier-1 launch (served path)")
+    ap.add_argument("--slots", type=int, default=3, help="slot threads of the plain path")
     return ap.parse_args()
 
 
@@ -126,15 +133,18 @@ def cpu_baseline(frames, sample=2):
     if have_reference():
         ref = Reference()
         cores = ref.lib.ref_usable_cpus()
+        from oracle.oracle import ref_codestream
         enc = RefEncoder(ref, W4K, H4K, 1, transfer=2, primaries=1, planar=pl, threads=0)
         enc.encode(frames[0])  # warm-up
         t0 = time.perf_counter()
         for i in range(sample):
-            enc.encode(frames[1 + i % (len(frames) - 1)])
+            t1 = enc.encode(frames[1 + i % (len(frames) - 1)])
+            ref_codestream(ref, W4K, H4K, 1, t1, fps=FPS, tag=b"cpu")
         dt = time.perf_counter() - t0
         enc.close()
         return {"value": sample / dt, "unit": "frames/s", "cores": cores, "kind": "reference",
-                "sample": f"{sample} 4K frames (after 1 warm-up) through the reference CpuSlot encoder, all passes"}
+                "sample": f"{sample} 4K frames (after 1 warm-up) through the reference CpuSlot encoder, all "
+                          f"passes, then its rate control and codestream writer"}
     from oracle.oracle import Oracle
     o = Oracle()
     t0 = time.perf_counter()
@@ -155,7 +165,7 @@ def run_reference(args):
     rank, local, world = rank_info()
     if rank != 0:
         return
-    from oracle.oracle import Planar, Reference, RefEncoder, have_reference
+    from oracle.oracle import Planar, Reference, RefEncoder, have_reference, ref_check, ref_codestream
     if not have_reference():
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not present"}))
         return
@@ -165,13 +175,19 @@ def run_reference(args):
     pl = Planar(width=W4K, height=H4K, active_w=W4K, active_h=H4K, ox=0, oy=0, sx=1, sy=0, rgb=0, bits=10,
                 full_range=0, chroma=0, kr=0.2627, kb=0.0593)
     enc = RefEncoder(ref, W4K, H4K, 1, transfer=2, primaries=1, planar=pl, threads=0)
+
+    def step(f):
+        t1 = enc.encode(f)
+        cs, _, _, _ = ref_codestream(ref, W4K, H4K, 1, t1, fps=FPS, tag=b"cpu")
+        return ref_check(ref, cs, FPS)[0]
+
     for i in range(args.warmup):
-        enc.encode(frames[i % len(frames)])
-    lat = []
+        step(frames[i % len(frames)])
+    lat, valid = [], 0
     t0 = time.perf_counter()
     for i in range(args.steps):
         t = time.perf_counter()
-        enc.encode(frames[(args.warmup + i) % len(frames)])
+        valid += step(frames[(args.warmup + i) % len(frames)])
         lat.append((time.perf_counter() - t) * 1e3)
     dt = time.perf_counter() - t0
     enc.close()
@@ -181,7 +197,9 @@ def run_reference(args):
            "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32 (integer Tier-1), f32 (colour, wavelet)",
            "data": "synthetic (seeded generator)",
            "config": {"workload": WORKLOAD, "step": "one frame (bounded sample of the 48-frame workload)",
-                      "path": "reference CpuSlot (colour, wavelet, quantisation, Tier-1), all host threads"},
+                      "path": "reference CpuSlot (colour, wavelet, quantisation, Tier-1), then its rate control, "
+                              "codestream writer and DCI checker, all host threads"},
+           "dci": {"frames": args.steps, "valid": int(valid)},
            "latency_ms": {"p50": statistics.median(lat), "p99": float(np.percentile(lat, 99))},
            "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "reference",
                             "sample": f"{args.steps} 4K frames after {args.warmup} warm-up"},
@@ -202,8 +220,10 @@ def run_ours(args):
     torch.cuda.set_device(local)
     rep = Replicas("nccl", timeout_s=120, device=f"cuda:{local}")
     import libgail_b200 as gb
+    from libgail_b200 import codestream as CS
     from libgail_b200 import plugin as P
     from libgail_b200.engine import Engine
+    from libgail_b200.slots import SlotPipeline
 
     L = gb.lib()
     L.gb_encoder_stream.restype = C.c_void_p
@@ -213,7 +233,6 @@ def run_ours(args):
     L.gb_encoder_stage_timing.argtypes = [C.c_void_p, C.c_int]
     L.gb_encoder_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     cuda = f"cuda:{local}"
-
     reduce_max = rep.max
 
     def barrier():
@@ -231,8 +250,11 @@ def run_ours(args):
     lay = P.LayoutHolder(W4K, H4K, 1)
     fmt = P.planar_format(W4K, H4K, bits=10, sx=1, sy=0)
     col = P.color("pq", "bt2020")
+    ncblk = lay.abi.numCblks
+    budget, _ = CS.dci_limits(FPS)
+    workers = max(2, min(16, (os.cpu_count() or 8) - 2))
 
-    # ---- plain per-frame path (the plugin's slot, one frame at a time) ----------------
+    # ---- device stages of the plain path, frames resident in HBM: the per-stage split ---
     enc = dev.encoder(lay, fmt, col)
     h = enc.h
     stream = torch.cuda.ExternalStream(L.gb_encoder_stream(h), device=cuda)
@@ -256,55 +278,58 @@ def run_ours(args):
     e1.record(stream)
     gb.check(L.gb_encoder_finish(h))
     torch.cuda.synchronize()
-    plain_ms = reduce_max(e0.elapsed_time(e1))
+    plain_dev_ms = reduce_max(e0.elapsed_time(e1))
     gb.check(L.gb_encoder_stage_times(h, ms5.ctypes.data, C.byref(cnt)))
     gb.check(L.gb_encoder_stage_timing(h, 0))
     stage = ms5 / max(cnt.value, 1)  # ms per frame: front, cm, order, mq, pack
-    plain_fps = args.steps * len(dframes) * world / (plain_ms / 1e3)
-
-    # plain end to end: host frames through encoder_encode (upload from the pinned input
-    # buffer, Tier-1 frame back in pinned memory), one at a time
+    plain_dev_fps = args.steps * len(dframes) * world / (plain_dev_ms / 1e3)
+    # decisions and codeword bytes per frame, from the plugin's own timings
     inbuf = enc.input_buffer()
-    as_frame = lambda: np.ctypeslib.as_array(C.cast(inbuf, C.POINTER(C.c_uint16)), (nbytes // 2,))  # noqa: E731
-    C.memmove(inbuf, frames[0].ctypes.data, nbytes)
-    enc.encode(as_frame())
     decisions, coded, passes = [], [], []
-    t0 = time.perf_counter()
-    for f in frames:
+    for f in frames[: min(4, len(frames))]:
         C.memmove(inbuf, f.ctypes.data, nbytes)
-        t1, tm, _ = enc.encode(as_frame())
+        view, tm = enc.encode_view(inbuf)
         decisions.append(tm.symbols)
-        coded.append(len(t1.data))
-        passes.append(len(t1.pass_len))
-    plain_e2e_fps = len(frames) * world / reduce_max(time.perf_counter() - t0)
-    ncblk = lay.abi.numCblks
-
-    # latency at a Poisson load the plain end-to-end path can carry (80 % of its rate)
-    rate = 0.8 * plain_e2e_fps / world
-    nlat = min(2 * len(frames), 96)
-    arr = poisson_arrivals(nlat, rate)
-    plain_lat = []
-    t0 = time.perf_counter()
-    for i in range(nlat):
-        while time.perf_counter() - t0 < arr[i]:
-            pass
-        C.memmove(inbuf, frames[i % len(frames)].ctypes.data, nbytes)
-        enc.encode(np.ctypeslib.as_array(C.cast(inbuf, C.POINTER(C.c_uint16)), (nbytes // 2,)))
-        plain_lat.append((time.perf_counter() - t0 - arr[i]) * 1e3)
+        coded.append(view.numData)
+        passes.append(view.numPasses)
     enc.close()
 
-    # ---- served: the batched engine -----------------------------------------------------
+    # ---- plain: slot threads, each encoder_encode + rate control + codestream + check ----
+    slots = SlotPipeline(dev, lay, fmt, col, slots=args.slots, fps=FPS, tag="b200")
+    slots.run(frames[: min(len(frames), 2 * args.slots)])  # warm-up
+    barrier()
+    plain_res, plain_s = [], 0.0
+    for _ in range(args.steps):
+        r, dt = slots.run(frames)
+        plain_res += r
+        plain_s += dt
+    plain_fps = len(plain_res) * world / reduce_max(plain_s)
+    # latency at a Poisson load both paths carry: 80 % of the plain rate
+    rate = 0.8 * plain_fps / world
+    nlat = min(2 * len(frames), 96)
+    arr = poisson_arrivals(nlat, rate)
+    lat_frames = [frames[i % len(frames)] for i in range(nlat)]
+    plain_lat_res, _ = slots.run(lat_frames, arrivals=arr)
+    slots.close()
+    plain_lat = [r[2] for r in plain_lat_res]
+
+    # ---- served: the batched engine, codestreams on host workers -----------------------
     eng = Engine(local, 0, max_batch=args.batch)
     cid, frame_bytes = eng.add_encoder(lay, fmt, col)
+    eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
+    served_cs = []
 
-    def served_step(src, slope=0.0):
-        ids = [eng.submit(cid, f, slope) for f in src]
+    def served_step(src, keep=False):
+        ids = [eng.submit(cid, f) for f in src]
         d2h = 0
         for _ in ids:
             rid, t, _, st = eng.wait(120000, copy=False)
             if rid < 0 or st != 0:
                 raise RuntimeError(f"engine frame failed (id {rid}, status {st})")
             d2h += t.numInfo * 20 + t.numPasses * 8 + t.numData
+            (p, n), ok = eng.codestream(rid, copy=False)
+            if keep:
+                served_cs.append((n, ok))
             eng.release(rid)
         return d2h
 
@@ -315,7 +340,7 @@ def run_ours(args):
     clocks.start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        served_step(dframes)
+        served_step(dframes, keep=True)
     torch.cuda.synchronize()
     served_s = reduce_max(time.perf_counter() - t0)
     clk = clocks.stop()
@@ -333,7 +358,7 @@ def run_ours(args):
     e2e_s = reduce_max(time.perf_counter() - t0)
     e2e_fps = args.steps * len(pinned) * world / e2e_s
 
-    # served latency at the same Poisson load as the plain path
+    # served latency at the same Poisson load
     served_lat = []
     import threading
 
@@ -381,7 +406,7 @@ def run_ours(args):
         # the dominant stage of the plain step: its roofline, with the DRAM traffic of one
         # launch from the committed ncu capture of the same workload
         k = int(np.argmax(stage))
-        traffic = {0: None, 1: NCU_TRAFFIC.get("t1CmKernel"), 3: NCU_TRAFFIC.get("t1MqKernel")}.get(k)
+        traffic = {1: NCU_TRAFFIC.get("t1CmKernel"), 3: NCU_TRAFFIC.get("t1MqKernel")}.get(k)
         roofline = {"bound": "hbm", "kernel": names[k], "achieved": stages[k]["achieved_gbs"], "peak": hbm,
                     "unit": "GB/s", "frac": stages[k]["frac"], "traffic": traffic,
                     "peak_source": "measured" if peaks else "fallback",
@@ -394,25 +419,33 @@ def run_ours(args):
                  "code_blocks_per_s_per_sm_served": ncblk * value / sms,
                  "ncu": NCU_TIER1}
         pct = lambda a, q: float(np.percentile(a, q))  # noqa: E731
+        dci = {"fps": FPS, "budget_bytes": budget,
+               "served": {"frames": len(served_cs), "valid": sum(1 for _, ok in served_cs if ok == 1),
+                          "max_bytes": max(n for n, _ in served_cs)},
+               "plain": {"frames": len(plain_res), "valid": sum(1 for r in plain_res if r[1]),
+                         "max_bytes": max(len(r[0]) for r in plain_res)}}
         out = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": served_s * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32 (integer Tier-1), f32 (colour, wavelet)",
-            "data": "synthetic (seeded generator, 48 frames)",
+            "data": f"synthetic (seeded generator, {len(dframes)} frames)",
             "config": {"workload": WORKLOAD, "frames_per_step": len(dframes), "path": "served (batched engine)",
-                       "max_batch": args.batch, "parallelism": f"replicas x{world}",
+                       "max_batch": args.batch, "codestream_workers": workers, "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2 ({len(dframes)} frames, {len(dframes) * nbytes / 1e9:.2f} GB)"},
             "served": {"fps": value, "latency_ms": {"p50": pct(served_lat, 50), "p99": pct(served_lat, 99)},
                        "offered_fps": rate, "batches": st_eng["batches"],
                        "frames_per_batch": st_eng["batch_frames"] / max(1, st_eng["batches"]),
                        "slots": st_eng["slots"], "frame_bytes": frame_bytes},
-            "plain": {"fps": plain_fps, "e2e_fps": plain_e2e_fps, "latency_ms": {"p50": pct(plain_lat, 50), "p99": pct(plain_lat, 99)},
-                      "offered_fps": rate, "stage_ms_per_frame": dict(zip(["front", "t1_cm", "t1_order", "t1_mq", "pack"],
-                                                                          [round(x, 4) for x in stage]))},
+            "plain": {"fps": plain_fps, "slots": args.slots,
+                      "latency_ms": {"p50": pct(plain_lat, 50), "p99": pct(plain_lat, 99)}, "offered_fps": rate,
+                      "device_resident_fps_tier1_only": plain_dev_fps,
+                      "stage_ms_per_frame": dict(zip(["front", "t1_cm", "t1_order", "t1_mq", "pack"],
+                                                     [round(x, 4) for x in stage]))},
+            "dci": dci,
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": nbytes * len(pinned),
                     "d2h_bytes_per_step": int(d2h), "path": "served engine, frames in pinned host memory, Tier-1 "
-                                                            "frames out to host memory"},
-            "gpu_launches": args.steps * len(dframes) * (6 + 2) + st_eng["batches"] * 3,
+                                                            "frames out to host memory, codestreams on host workers"},
+            "gpu_launches": args.steps * len(dframes) * (6 + 3) + st_eng["batches"] * 3,
             "roofline": roofline,
             "stages": stages,
             "tier1": tier1,

@@ -117,7 +117,14 @@ GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
  *                          Tier-1 view (valid until release), submit-to-finish latency and
  *                          status
  *   gb_engine_release      give the frame's slot back
- *   gb_engine_stats        frames, batches, frames in batches, slots, slot bytes */
+ *   gb_engine_stats        frames, batches, frames in batches, slots, slot bytes
+ *   gb_engine_set_codestream  from now on, every frame also gets its DCI codestream on
+ *                          `threads` host workers: gb_rate_and_build's rate control and
+ *                          codestream (fps, maxMbps, compMbps, label, tag), then with check
+ *                          the DCI check; the frame is handed out by gb_engine_wait once its
+ *                          codestream is made (the latency includes it)
+ *   gb_engine_codestream   a handed-out frame's codestream (valid until release) and its
+ *                          DCI verdict (1, 0, or -1 when not checked) */
 typedef struct GbEngine GbEngine;
 GB_API int gb_engine_create(int device, uint64_t hbmBudget, int maxBatch, GbEngine** out);
 GB_API void gb_engine_destroy(GbEngine* e);
@@ -128,6 +135,9 @@ GB_API int gb_engine_wait(GbEngine* e, int timeoutMs, int64_t* id, GailCudaTier1
                           int* frameStatus);
 GB_API int gb_engine_release(GbEngine* e, int64_t id);
 GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5);
+GB_API int gb_engine_set_codestream(GbEngine* e, double fps, double maxMbps, double compMbps, const char* label,
+                                    const char* tag, int threads, int check);
+GB_API int gb_engine_codestream(GbEngine* e, int64_t id, const uint8_t** data, uint64_t* size, int* dciOk);
 
 /* The host codec around a Tier-1 frame, byte-identical to libgail's core for the same
  * frame. Thread-safe across threads (each keeps its own writer per layout and label).

@@ -47,8 +47,18 @@ class Tier1Arrays:
                          numPasses=len(self.pass_len), numData=len(self.data))
 
 
-def _t1(t) -> Tier1Arrays:
-    return t if isinstance(t, Tier1Arrays) else Tier1Arrays(t)
+class _View:
+    def __init__(self, t: Tier1):
+        self.abi = t
+
+
+def _t1(t):
+    """Tier1Arrays as given; a plugin's Tier1 view used in place; else its arrays wrapped."""
+    if isinstance(t, (Tier1Arrays, _View)):
+        return t
+    if isinstance(t, Tier1):
+        return _View(t)
+    return Tier1Arrays(t)
 
 
 def dci_limits(fps: float, max_mbps: float = 230.0, comp_mbps: float = 200.0):

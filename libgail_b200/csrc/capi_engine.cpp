@@ -53,6 +53,29 @@ GB_API int gb_engine_release(GbEngine* e, int64_t id) {
     });
 }
 
+GB_API int gb_engine_set_codestream(GbEngine* e, double fps, double maxMbps, double compMbps, const char* label,
+                                    const char* tag, int threads, int check) {
+    return gbGuard([&] {
+        if (!e) throw std::logic_error("null argument");
+        EncodeEngine::CodestreamConfig c;
+        c.fps = fps;
+        c.maxMbps = maxMbps;
+        c.compMbps = compMbps;
+        c.label = label ? label : "";
+        c.tag = tag ? tag : "";
+        c.threads = threads;
+        c.check = check != 0;
+        e->e->setCodestream(c);
+    });
+}
+
+GB_API int gb_engine_codestream(GbEngine* e, int64_t id, const uint8_t** data, uint64_t* size, int* dciOk) {
+    return gbGuard([&] {
+        if (!e || !data || !size || !dciOk) throw std::logic_error("null argument");
+        if (!e->e->codestream(id, data, size, dciOk)) throw std::logic_error("codestreams are off");
+    });
+}
+
 GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5) {
     return gbGuard([&] {
         if (!e || !out5) throw std::logic_error("null argument");

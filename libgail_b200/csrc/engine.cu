@@ -7,6 +7,7 @@
 #include <string>
 
 #include "capi_util.h"
+#include "codestream.h"
 #include "common.cuh"
 #include "compact.cuh"
 #include "frontend.cuh"
@@ -66,6 +67,8 @@ struct EncodeEngine::Request {
     Slot* slot = nullptr;
     uint32_t jobBase = 0;
     int status = 0;
+    std::vector<uint8_t> cs;  // the codestream, when the engine makes them
+    int dciOk = -1;
 };
 
 struct EncodeEngine::Batch {
@@ -105,9 +108,15 @@ EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(
 }
 
 EncodeEngine::~EncodeEngine() {
-    stop_ = true;
+    {
+        std::lock_guard<std::mutex> lock(m_);  // so that no worker misses the wake-up
+        stop_ = true;
+    }
     cvWork_.notify_all();
     if (worker_.joinable()) worker_.join();
+    cvCs_.notify_all();
+    for (auto& t : csWorkers_)
+        if (t.joinable()) t.join();
     cudaSetDevice(dev_);
     cudaDeviceSynchronize();
     for (auto& s : slots_) {
@@ -278,6 +287,76 @@ void EncodeEngine::release(int64_t id) {
     cvWork_.notify_one();
 }
 
+void EncodeEngine::setCodestream(const CodestreamConfig& c) {
+    if (c.threads < 1 || c.threads > 256) throw std::logic_error("codestream workers out of range");
+    if (c.tag.size() > kMaxDeviceTagBytes) throw std::logic_error("device tag too long");
+    const RateLimits lim = dciLimits(c.fps, c.maxMbps, c.compMbps);
+    for (auto& cl : classes_) {
+        CodestreamWriter w(cl->L, c.label);
+        if (w.emptyBytes() > lim.maxTotal) throw std::logic_error("the frame budget is below the smallest codestream");
+    }
+    std::lock_guard<std::mutex> lock(m_);
+    if (csOn_) throw std::logic_error("codestreams are already on");
+    cs_ = c;
+    csOn_ = true;
+    for (int i = 0; i < c.threads; ++i) csWorkers_.emplace_back([this] { codestreamWorker(); });
+}
+
+bool EncodeEngine::codestream(int64_t id, const uint8_t** data, uint64_t* size, int* dciOk) {
+    std::lock_guard<std::mutex> lock(m_);
+    if (id < 0 || id >= (int64_t)requests_.size() || !requests_[id]) throw std::logic_error("unknown request");
+    const Request* r = requests_[id].get();
+    if (!csOn_) return false;
+    *data = r->cs.data();
+    *size = r->cs.size();
+    *dciOk = r->dciOk;
+    return true;
+}
+
+void EncodeEngine::codestreamWorker() {
+    // one writer per frame class on this worker (the packet order is flattened once)
+    std::vector<std::unique_ptr<CodestreamWriter>> writers;
+    for (;;) {
+        Request* r;
+        const Class* c;
+        {
+            std::unique_lock<std::mutex> lock(m_);
+            cvCs_.wait(lock, [&] { return stop_.load() || !csq_.empty(); });
+            if (csq_.empty()) return;
+            r = csq_.front();
+            csq_.pop_front();
+            c = classes_[r->cls].get();
+            if (writers.size() < classes_.size()) writers.resize(classes_.size());
+        }
+        auto& w = writers[r->cls];
+        if (!w) w = std::make_unique<CodestreamWriter>(c->L, cs_.label);
+        const Slot* s = r->slot;
+        if (r->status == kOk) {
+            try {
+                Tier1View v;
+                v.info = reinterpret_cast<const GbCblkInfo*>(s->hInfo);
+                v.passLen = s->hLen;
+                v.passDist = s->hDist;
+                v.data = s->hData;
+                v.numInfo = s->n;
+                v.numPasses = s->hTot[1];
+                v.numData = s->hTot[0];
+                const RateResult rr = allocateRate(*w, v, dciLimits(cs_.fps, cs_.maxMbps, cs_.compMbps));
+                w->build(v, rr.passes.data(), &r->cs, cs_.tag);
+                if (cs_.check) r->dciOk = checkDci(r->cs.data(), r->cs.size(), cs_.fps).ok ? 1 : 0;
+            } catch (const std::exception&) {
+                r->status = kError;
+            }
+        }
+        const auto now = Clock::now();
+        std::lock_guard<std::mutex> lock(m_);
+        r->latency = msBetween(r->t0, now);
+        done_.push_back(r);
+        stats_.frames++;
+        cvDone_.notify_all();
+    }
+}
+
 EncodeEngine::Stats EncodeEngine::stats() const {
     std::lock_guard<std::mutex> lock(m_);
     return stats_;
@@ -400,9 +479,14 @@ bool EncodeEngine::collect(Batch& b) {
     for (Request* r : b.frames) {
         r->latency = msBetween(r->t0, now);
         r->status = (status || r->slot->hTot[2]) ? kError : kOk;
-        done_.push_back(r);
-        stats_.frames++;
+        if (csOn_) {
+            csq_.push_back(r);
+        } else {
+            done_.push_back(r);
+            stats_.frames++;
+        }
     }
+    if (csOn_) cvCs_.notify_all();
     b.frames.clear();
     b.busy = false;
     return true;

@@ -9,8 +9,10 @@
 // whose front end has finished joins the next Tier-1 batch, one launch of the Tier-1
 // kernels over all their code-blocks (largest first across frames), with two batches in
 // flight so that one batch's serial MQ tail overlaps the next batch's work; packing
-// writes each frame's Tier1Frame straight into mapped host memory; wait() hands out
-// finished frames, release() frees their slots.
+// writes each frame's Tier1Frame straight into mapped host memory. With codestreams on,
+// a pool of host workers then makes each frame's DCI codestream (PCRD rate control,
+// Tier-2, optionally the DCI check) while the GPU carries on with later frames. wait()
+// hands out finished frames, release() frees their slots.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -53,6 +55,20 @@ public:
     bool wait(int timeoutMs, int64_t* id, GailCudaTier1* out, double* latencyMs, int* status);
     void release(int64_t id);
 
+    // Codestreams for every frame from now on: rate control to the DCI budgets at fps
+    // (whole frame under maxMbps, each component under compMbps), the COM text label +
+    // " " + tag, the DCI check when check is set, on `threads` host workers.
+    struct CodestreamConfig {
+        double fps = 24.0, maxMbps = 230.0, compMbps = 200.0;
+        std::string label, tag;
+        bool check = true;
+        int threads = 4;
+    };
+    void setCodestream(const CodestreamConfig& c);
+    // The codestream of a finished frame (valid until release): its bytes and whether it
+    // passed the DCI check (-1 when not checked). False when codestreams are off.
+    bool codestream(int64_t id, const uint8_t** data, uint64_t* size, int* dciOk);
+
     struct Stats {
         uint64_t frames = 0, batches = 0, batchFrames = 0, slots = 0, slotBytes = 0;
     };
@@ -65,6 +81,7 @@ private:
     struct Batch;
 
     void run();
+    void codestreamWorker();
     bool admit();
     bool launchBatch(Batch& b);
     bool collect(Batch& b);
@@ -91,6 +108,12 @@ private:
     std::string error_;
     Stats stats_;
     std::thread worker_;
+    // codestream stage
+    CodestreamConfig cs_;
+    bool csOn_ = false;
+    std::deque<Request*> csq_;  // Tier-1 done, codestream to make
+    std::condition_variable cvCs_;
+    std::vector<std::thread> csWorkers_;
 };
 
 }  // namespace gb

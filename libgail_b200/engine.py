@@ -22,6 +22,10 @@ def _bind():
                                  C.POINTER(C.c_int)]
     L.gb_engine_release.argtypes = [C.c_void_p, C.c_int64]
     L.gb_engine_stats.argtypes = [C.c_void_p, C.c_void_p]
+    L.gb_engine_set_codestream.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_char_p, C.c_char_p,
+                                           C.c_int, C.c_int]
+    L.gb_engine_codestream.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_uint8)),
+                                       C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
     L._engine_bound = True
     return L
 
@@ -66,6 +70,20 @@ class Engine:
         if rid.value < 0:
             return -1, None, 0.0, 0
         return rid.value, (Tier1Frame(t) if copy else t), lat.value, st.value
+
+    def set_codestream(self, fps: float = 24.0, max_mbps: float = 230.0, comp_mbps: float = 200.0,
+                       label: str = "GAIL 1.1.0", tag: str = "", threads: int = 4, check_dci: bool = True):
+        """Every frame from now on also gets its DCI codestream on `threads` host workers."""
+        check(lib().gb_engine_set_codestream(self.h, fps, max_mbps, comp_mbps, label.encode(), tag.encode(), threads,
+                                             int(check_dci)))
+
+    def codestream(self, rid: int, copy: bool = True):
+        """(codestream bytes, or (pointer, size) without copy; DCI verdict 1/0, -1 unchecked)."""
+        p, n, ok = C.POINTER(C.c_uint8)(), C.c_uint64(), C.c_int()
+        check(lib().gb_engine_codestream(self.h, rid, C.byref(p), C.byref(n), C.byref(ok)))
+        if not copy:
+            return (p, n.value), ok.value
+        return (C.string_at(p, n.value) if n.value else b""), ok.value
 
     def release(self, rid: int):
         check(lib().gb_engine_release(self.h, rid))

@@ -274,6 +274,14 @@ class Encoder:
     def set_slope(self, thr: float):
         self.d.p.t.encoder_set_slope(self.h, C.c_double(thr))
 
+    def encode_view(self, frame_ptr):
+        """encoder_encode of the frame at host address frame_ptr (the input buffer, or any
+        host memory of the input format). Returns (the plugin's Tier1 view, valid until the
+        next call on this encoder, and the timings), without copying the output."""
+        out, tm = Tier1(), FrameTimings()
+        self.d.p.check(self.d.p.t.encoder_encode(self.h, C.c_void_p(frame_ptr), C.byref(out), C.byref(tm), None))
+        return out, tm
+
     def encode(self, frame: np.ndarray, debug: bool = False, full: bool = True):
         """frame: the input bytes (RGB48 interleaved or planar). Returns (Tier1Frame,
         timings, taps) where taps = dict(xyz12, coeffs, wavelet) when debug."""

@@ -100,3 +100,74 @@ def test_engine_admission_by_budget(dev):
         assert eng.stats()["slots"] <= 2
     finally:
         eng.close()
+
+
+@pytest.mark.gpu
+def test_engine_codestreams(dev):
+    """Codestreams made by the engine's host workers: each equals the host codec's on the
+    frame's plain Tier-1 output, passes the DCI check, and (for one frame) equals the
+    reference's rate control and codestream on the same Tier-1 frame."""
+    from libgail_b200 import codestream as CS
+    from oracle.oracle import Reference, have_reference, ref_codestream
+    cases = [c for c in _cases() if c[0] in ((1998, 1080, 0), (3996, 2160, 1))]
+    alone = []
+    for (W, H, fk), fmt, col, frames in cases:
+        enc = dev.encoder(P.LayoutHolder(W, H, fk), fmt, col)
+        alone.append([enc.encode(f)[0] for f in frames[:2]])
+        enc.close()
+    eng = Engine(0, 0, max_batch=8)
+    try:
+        layouts = [P.LayoutHolder(W, H, fk) for (W, H, fk), _, _, _ in cases]
+        classes = [eng.add_encoder(lay, fmt, col)[0] for lay, (_, fmt, col, _) in zip(layouts, cases)]
+        eng.set_codestream(fps=24.0, label=CS.DEFAULT_LABEL, tag="b200", threads=3)
+        want = {}
+        for fi in range(2):
+            for ci in range(len(cases)):
+                rid = eng.submit(classes[ci], cases[ci][3][fi])
+                want[rid] = (ci, fi)
+        for _ in want:
+            rid, t1, _, st = eng.wait(120000)
+            assert rid >= 0 and st == 0
+            cs, ok = eng.codestream(rid)
+            ci, fi = want[rid]
+            assert _same(t1, alone[ci][fi])
+            host, _, _ = CS.rate_and_build(layouts[ci], alone[ci][fi], fps=24.0, label=CS.DEFAULT_LABEL, tag="b200")
+            assert cs == host
+            assert ok == 1 and CS.check_dci(cs)[0]
+            if have_reference() and fi == 0:
+                (W, H, fk) = cases[ci][0]
+                ref_cs, _, _, _ = ref_codestream(Reference(), W, H, fk, alone[ci][fi], fps=24.0, tag=b"b200")
+                assert cs == ref_cs
+            eng.release(rid)
+    finally:
+        eng.close()
+
+
+@pytest.mark.gpu
+def test_slot_pipeline_codestreams(dev):
+    """The plain path with slots gives each frame the same codestream as the engine."""
+    from libgail_b200 import codestream as CS
+    from libgail_b200.slots import SlotPipeline
+    W, H = 1998, 1080
+    frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=400 + i)) for i in range(5)]
+    lay = P.LayoutHolder(W, H, 0)
+    sp = SlotPipeline(dev, lay, P.rgb48_format(W, H), P.color_passthrough(), slots=2, tag="b200")
+    try:
+        res, _ = sp.run(frames)
+    finally:
+        sp.close()
+    eng = Engine(0, 0, max_batch=4)
+    try:
+        cid, _ = eng.add_encoder(lay, P.rgb48_format(W, H), P.color_passthrough())
+        eng.set_codestream(label=CS.DEFAULT_LABEL, tag="b200", threads=2)
+        ids = [eng.submit(cid, f) for f in frames]
+        got = {}
+        for _ in ids:
+            rid, _, _, st = eng.wait(60000)
+            assert st == 0
+            got[rid] = eng.codestream(rid)
+            eng.release(rid)
+    finally:
+        eng.close()
+    for i, rid in enumerate(ids):
+        assert res[i][0] == got[rid][0] and res[i][1] and got[rid][1] == 1
