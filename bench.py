@@ -10,9 +10,10 @@ pass (bit-exact with the CPU reference). One step = encoding all 48 frames; the 
   value   DCI codestreams/s of the served path: the batched engine (continuous batching of
           Tier-1 over every frame in flight) on frames resident in HBM, Tier-1 frames written
           to mapped host memory, each frame's rate control, Tier-2 and DCI check on the
-          engine's host workers. The work spans the engine's streams and threads, so the
-          timed region is bracketed by a barrier and a device synchronisation on both sides;
-          max over ranks.
+          engine's host workers. The K steps run as one job (all K x 48 requests submitted
+          at once, the time to the last codestream). The work spans the engine's streams and
+          threads, so the timed region is bracketed by a barrier and a device
+          synchronisation on both sides; max over ranks.
   plain   the drop-in per-frame path beside it, as libgail drives the plugin: slot threads,
           each encoder_encode from host memory then rate control, Tier-2 and the DCI check;
           codestreams/s and p50/p99 latency at a Poisson load of 80 % of that rate (served
@@ -21,6 +22,8 @@ pass (bit-exact with the CPU reference). One step = encoding all 48 frames; the 
   e2e     codestreams/s of the served path with the frames in pinned host memory: each
           frame's upload and its Tier-1 output in host memory are inside the timed region.
   dci     every codestream of the timed runs checked: how many passed, the largest.
+  decode  the served codestreams of one step decoded through decoder_decode (host
+          codestream in, 12-bit picture out) one after another, with the stage split.
   stages  per stage of the plain path: live ms per frame, algorithmic bytes, GB/s and the
           fraction of the measured HBM bandwidth; roofline is the dominant stage.
 
@@ -142,9 +145,18 @@ def cpu_baseline(frames, sample=2):
             ref_codestream(ref, W4K, H4K, 1, t1, fps=FPS, tag=b"cpu")
         dt = time.perf_counter() - t0
         enc.close()
+        from oracle.oracle import ref_decode
+        cs, _, _, _ = ref_codestream(ref, W4K, H4K, 1, t1, fps=FPS, tag=b"cpu")
+        ref_decode(ref, cs, W4K, H4K)  # warm-up
+        t0 = time.perf_counter()
+        for _ in range(sample):
+            ref_decode(ref, cs, W4K, H4K)
+        ddt = time.perf_counter() - t0
         return {"value": sample / dt, "unit": "frames/s", "cores": cores, "kind": "reference",
                 "sample": f"{sample} 4K frames (after 1 warm-up) through the reference CpuSlot encoder, all "
-                          f"passes, then its rate control and codestream writer"}
+                          f"passes, then its rate control and codestream writer",
+                "decode": {"value": sample / ddt, "unit": "frames/s",
+                           "sample": f"{sample} decodes of one 4K codestream through the reference CPU decoder"}}
     from oracle.oracle import Oracle
     o = Oracle()
     t0 = time.perf_counter()
@@ -314,13 +326,20 @@ def run_ours(args):
     plain_lat = [r[2] for r in plain_lat_res]
 
     # ---- served: the batched engine, codestreams on host workers -----------------------
-    eng = Engine(local, 0, max_batch=args.batch)
+    # a budget of 48 frame slots: deep enough to keep two Tier-1 batches and the front ends
+    # busy; every slot is made during the warm-up, none inside the timed region
+    probe = Engine(local, 0, max_batch=args.batch)
+    _, frame_bytes = probe.add_encoder(lay, fmt, col)
+    probe.close()
+    eng = Engine(local, 48 * frame_bytes + 1, max_batch=args.batch)
     cid, frame_bytes = eng.add_encoder(lay, fmt, col)
     eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
     served_cs = []
 
-    def served_step(src, keep=False):
-        ids = [eng.submit(cid, f) for f in src]
+    kept_cs = []  # codestreams of one step, for the decode run
+
+    def served_step(src, keep=False, repeat=1):
+        ids = [eng.submit(cid, f) for _ in range(repeat) for f in src]
         d2h = 0
         for _ in ids:
             rid, t, _, st = eng.wait(120000, copy=False)
@@ -330,17 +349,19 @@ def run_ours(args):
             (p, n), ok = eng.codestream(rid, copy=False)
             if keep:
                 served_cs.append((n, ok))
+                if len(kept_cs) < len(src):
+                    kept_cs.append(C.string_at(p, n))
             eng.release(rid)
         return d2h
 
-    for _ in range(args.warmup):
-        served_step(dframes)
+    served_step(dframes, repeat=args.warmup)
     barrier()
     clocks = Clocks(local)
     clocks.start()
+    # the K steps as one continuous job: every step's frames submitted at once, so that the
+    # pipeline drains once at the end rather than after each step
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        served_step(dframes, keep=True)
+    served_step(dframes, keep=True, repeat=args.steps)
     torch.cuda.synchronize()
     served_s = reduce_max(time.perf_counter() - t0)
     clk = clocks.stop()
@@ -351,9 +372,7 @@ def run_ours(args):
     served_step(pinned)
     barrier()
     t0 = time.perf_counter()
-    d2h = 0
-    for _ in range(args.steps):
-        d2h = served_step(pinned)
+    d2h = served_step(pinned, repeat=args.steps) / args.steps
     torch.cuda.synchronize()
     e2e_s = reduce_max(time.perf_counter() - t0)
     e2e_fps = args.steps * len(pinned) * world / e2e_s
@@ -377,6 +396,28 @@ def run_ours(args):
         eng.submit(cid, pinned[i % len(pinned)])
     th.join()
     eng.close()
+
+    # ---- decode: the served codestreams back to 12-bit pictures -------------------------
+    # the host parses each codestream (gb_parse_codestream), decoder_decode does Tier-1
+    # decode, dequantisation, the inverse 9/7 and ICT on the device and returns the picture
+    parse_ms = []
+    parsed = []
+    for c in kept_cs:
+        t = time.perf_counter()
+        parsed.append(CS.parse(c)[1].view(P.CBLK_CODE_DTYPE))
+        parse_ms.append((time.perf_counter() - t) * 1e3)
+    dec = dev.decoder(lay, reduce=0)
+    pic = np.zeros((H4K, W4K, 3), np.uint16)
+    for i in range(min(3, len(kept_cs))):
+        dec.decode(kept_cs[i], parsed[i], out=pic)
+    dstage = np.zeros(3)
+    t0 = time.perf_counter()
+    for c, b in zip(kept_cs, parsed):
+        _, tm, _ = dec.decode(c, b, out=pic)
+        dstage += (tm.t1, tm.dwt, tm.color)
+    dec_s = reduce_max(time.perf_counter() - t0)
+    dec.close()
+    decode_fps = len(kept_cs) * world / dec_s
 
     out = None
     if rank == 0:
@@ -442,6 +483,11 @@ def run_ours(args):
                       "stage_ms_per_frame": dict(zip(["front", "t1_cm", "t1_order", "t1_mq", "pack"],
                                                      [round(x, 4) for x in stage]))},
             "dci": dci,
+            "decode": {"fps": decode_fps, "unit": "frames/s", "frames": len(kept_cs),
+                       "path": "decoder_decode per frame: codestream from host memory, 12-bit picture to host memory",
+                       "parse_ms_per_frame": float(np.mean(parse_ms)),
+                       "stage_ms_per_frame": dict(zip(["t1_decode_dequant", "inverse_dwt", "ict_pack"],
+                                                      [round(x / max(1, len(kept_cs)), 4) for x in dstage]))},
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": nbytes * len(pinned),
                     "d2h_bytes_per_step": int(d2h), "path": "served engine, frames in pinned host memory, Tier-1 "
                                                             "frames out to host memory, codestreams on host workers"},

@@ -319,12 +319,17 @@ class Decoder:
             self.d.p.t.decoder_destroy(self.h)
             self.h = None
 
-    def decode(self, codestream: bytes, blocks: np.ndarray, frame_layout: LayoutHolder = None, wavelet=False):
-        """blocks: structured CblkCode array (one per code-block). Returns (picture
-        (H, W, 3) uint16, timings, wavelet planes or None)."""
+    def decode(self, codestream: bytes, blocks: np.ndarray, frame_layout: LayoutHolder = None, wavelet=False,
+               out: np.ndarray = None):
+        """blocks: structured CblkCode array (one per code-block); out: an (H, W, 3) uint16
+        picture to write into (a new one when None). Returns (picture, timings, wavelet
+        planes or None)."""
         lay = frame_layout or self.layout
         data = np.frombuffer(codestream, np.uint8)
-        out = np.zeros((self.out_h, self.out_w, 3), np.uint16)
+        if out is None:
+            out = np.zeros((self.out_h, self.out_w, 3), np.uint16)
+        elif out.shape != (self.out_h, self.out_w, 3) or out.dtype != np.uint16 or not out.flags.c_contiguous:
+            raise ValueError("picture buffer of the wrong shape or type")
         tm = DecodeTimings(wantWavelet=int(wavelet))
         b = np.ascontiguousarray(blocks)
         st = self.d.p.t.decoder_decode(self.h, C.byref(lay.abi), data.ctypes.data_as(C.c_void_p), data.size,

@@ -1,13 +1,14 @@
 """Small, fixed encode cases for profiler captures.
 
   python -m libgail_b200.profile_case --path plain --frames 2
-  python -m libgail_b200.profile_case --path served --frames 8 --batch 8
+  python -m libgail_b200.profile_case --path served --frames 8 --batch 8 [--size 2k]
 
-Encodes seeded synthetic 4K frames (3996x2160 Y'CbCr 4:2:2 10-bit, BT.2020 PQ, as the
-benchmark uses) that are already in device memory, through the plain per-frame encoder or
-the batched engine, and prints the stage times of the plain path. Exits non-zero on any
-encoder error, so that a profiler run after it sees the same launches of a program that
-ended cleanly.
+Encodes seeded synthetic frames that are already in device memory, through the plain
+per-frame encoder or the batched engine, and prints the stage times of the plain path:
+4K (3996x2160 Y'CbCr 4:2:2 10-bit, BT.2020 PQ, as the benchmark uses) or 2K (1998x1080
+X'Y'Z' 12-bit, whose small frame slots keep a batched case to a few GB of device memory).
+Exits non-zero on any encoder error, so that a profiler run after it sees the same
+launches of a program that ended cleanly.
 """
 from __future__ import annotations
 
@@ -24,6 +25,7 @@ def main():
     ap.add_argument("--path", choices=["plain", "served"], default="plain")
     ap.add_argument("--frames", type=int, default=2)
     ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--size", choices=["4k", "2k"], default="4k")
     args = ap.parse_args()
 
     import torch
@@ -33,12 +35,19 @@ def main():
     from libgail_b200 import synth
     from libgail_b200.engine import Engine
 
-    frames = synth.many(synth.yuv422p10, args.frames, W4K, H4K, seed=1000)
+    if args.size == "4k":
+        frames = synth.many(synth.yuv422p10, args.frames, W4K, H4K, seed=1000)
+        lay = P.LayoutHolder(W4K, H4K, 1)
+        fmt = P.planar_format(W4K, H4K, bits=10, sx=1, sy=0)
+        col = P.color("pq", "bt2020")
+    else:
+        W, H = 1998, 1080
+        frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=1000 + i)) for i in range(args.frames)]
+        lay = P.LayoutHolder(W, H, 0)
+        fmt = P.rgb48_format(W, H)
+        col = P.color_passthrough()
     dframes = [torch.from_numpy(f.view(np.int16)).to("cuda:0") for f in frames]
     torch.cuda.synchronize()
-    lay = P.LayoutHolder(W4K, H4K, 1)
-    fmt = P.planar_format(W4K, H4K, bits=10, sx=1, sy=0)
-    col = P.color("pq", "bt2020")
     dev = P.Plugin().device(0)
     try:
         if args.path == "plain":
