@@ -2,8 +2,9 @@
 // ICT and 12-bit packing.
 //
 // Tier-1 (decodeKernel): one lane per code-block. The MQ decoder is serial per block, so
-// lanes pull blocks from a device queue ordered longest codeword first (orderKernel) and
-// take the next as soon as theirs is done. A block's state is kept as row masks in
+// blocks are ordered longest codeword first (orderKernel); a warp takes either one of the
+// heaviest blocks alone (its lane 0 decodes it, free of divergent neighbours) or the next
+// 32 lighter ones, which have similar lengths. A block's state is kept as row masks in
 // shared memory (significance and sign for rows -1..32, coded-this-plane and refined),
 // the scan visits only columns that have something to code (bit scans over candidate
 // masks), and the decoded words (sign, twice the magnitude plus the mid-point of the
@@ -53,8 +54,14 @@ struct DecArgs {
     uint32_t* planes;   // float planes seen as words while decoding
     uint32_t W;
     uint32_t* perm;
-    uint32_t* ctl;      // [0] queue head, [1] status, [2] wanted blocks
+    uint32_t* ctl;      // [0] light queue head, [1] status, [2] wanted blocks, [3] heavy blocks,
+                        // [4] heavy queue head
 };
+
+// Blocks with at least this many codeword bytes are decoded one per warp: the longest
+// serial chains of the frame, which would otherwise run with 31 divergent neighbours.
+// A power of two, so that they sort ahead of every lighter block.
+constexpr uint32_t kHeavyBytes = 128;
 
 __device__ __forceinline__ uint32_t lenBucket(uint32_t len) {
     if (len < 4) return ORDER_BUCKETS - 1;
@@ -68,10 +75,14 @@ __global__ void __launch_bounds__(1024) orderKernel(DecArgs a) {
     for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
     if (threadIdx.x == 0) total = 0;
     __syncthreads();
+    __shared__ uint32_t heavy;
+    if (threadIdx.x == 0) heavy = 0;
+    __syncthreads();
     for (uint32_t i = threadIdx.x; i < a.n; i += blockDim.x)
         if (a.blocks[i].wanted) {
             atomicAdd(&hist[lenBucket(a.codes[i].len)], 1u);
             atomicAdd(&total, 1u);
+            if (a.codes[i].len >= kHeavyBytes) atomicAdd(&heavy, 1u);
         }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -82,6 +93,7 @@ __global__ void __launch_bounds__(1024) orderKernel(DecArgs a) {
             run += c;
         }
         a.ctl[2] = total;
+        a.ctl[3] = heavy;
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < a.n; i += blockDim.x)
@@ -220,17 +232,32 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
     b.sc = s_sc;
     b.tab = s_tab;
     b.W = a.W;
-    const uint32_t count = a.ctl[2];
+    const uint32_t count = a.ctl[2], heavy = a.ctl[3];
+    const int lane = tid & 31;
     for (;;) {
-        const uint32_t q = atomicAdd(a.ctl, 1u);
-        if (q >= count) break;
+        // a warp claims one heavy block (its lane 0 decodes it) or 32 light ones, which
+        // sort next to each other and so have similar lengths
+        uint32_t base = 0, cnt = 0;
+        if (lane == 0) {
+            const uint32_t h = heavy ? atomicAdd(a.ctl + 4, 1u) : heavy;
+            if (h < heavy) {
+                base = h;
+                cnt = 1;
+            } else {
+                base = heavy + atomicAdd(a.ctl, 32u);
+                cnt = 32;
+            }
+        }
+        base = __shfl_sync(kFull, base, 0);
+        cnt = __shfl_sync(kFull, cnt, 0);
+        if (base >= count) break;
+        const uint32_t q = base + (uint32_t)lane;
+        if ((uint32_t)lane >= cnt || q >= count) continue;
         const uint32_t j = a.perm[q];
         const DecBlock blk = a.blocks[j];
         const GbCblkCode code = a.codes[j];
         const int w = blk.w, h = blk.h;
-        uint32_t* out = a.planes + blk.dst;
-        for (int y = 0; y < h; ++y)
-            for (int x = 0; x < w; ++x) out[(size_t)y * a.W + x] = 0u;
+        uint32_t* out = a.planes + blk.dst;  // zeroed before the launch: only significant samples are written
         const int nbps = code.nbps;
         const bool valid = code.passes > 0 && nbps >= 1 && nbps <= 30 && (uint64_t)code.offset + code.len <= a.size;
         if (valid) {
@@ -325,16 +352,18 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                 }
                 for (int i = 0; i < 32; ++i) b.vis[i * DEC_THREADS] = 0;
             }
+            // dequantise in place, the significant samples only (every other word is 0,
+            // which is 0.0f): word * step / 2, sign from bit 31
+            const float half = a.half[blk.band];
+            float* f = reinterpret_cast<float*>(out);
+            for (int y = 0; y < h; ++y)
+                for (uint32_t m = b.S(y) & wmask; m; m &= m - 1) {
+                    const int x = __ffs(m) - 1;
+                    const uint32_t v = out[(size_t)y * a.W + x];
+                    const float mag = (float)(v & 0x7FFFFFFFu) * half;
+                    f[(size_t)y * a.W + x] = (v & 0x80000000u) ? -mag : mag;
+                }
         }
-        // dequantise in place: word * step / 2, sign from bit 31
-        const float half = a.half[blk.band];
-        float* f = reinterpret_cast<float*>(out);
-        for (int y = 0; y < h; ++y)
-            for (int x = 0; x < w; ++x) {
-                const uint32_t v = out[(size_t)y * a.W + x];
-                const float m = (float)(v & 0x7FFFFFFFu) * half;
-                f[(size_t)y * a.W + x] = (v & 0x80000000u) ? -m : m;
-            }
     }
 }
 
@@ -599,7 +628,7 @@ void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, 
     GB_CHECK(cudaMemcpyAsync(dCodes_, hCodes_, n * sizeof(GbCblkCode), cudaMemcpyHostToDevice, st));
     GB_CHECK(cudaMemcpyAsync(dHalf_, hHalf_, frame.bands.size() * 4, cudaMemcpyHostToDevice, st));
     GB_CHECK(cudaMemsetAsync(dCtl_, 0, 64, st));
-    if (wantWavelet) GB_CHECK(cudaMemsetAsync(dPlanes_, 0, npix * 12, st));
+    GB_CHECK(cudaMemsetAsync(dPlanes_, 0, npix * 12, st));  // coefficients of uncoded samples
     DecArgs da{dBytes_, size, dCodes_, dBlocks_, (uint32_t)n, dHalf_, (uint32_t*)dPlanes_, (uint32_t)L_.width, dPerm_, dCtl_};
     orderKernel<<<1, 1024, 0, st>>>(da);
     int sms = 148;

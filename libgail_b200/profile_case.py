@@ -2,9 +2,12 @@
 
   python -m libgail_b200.profile_case --path plain --frames 2
   python -m libgail_b200.profile_case --path served --frames 8 --batch 8 [--size 2k]
+  python -m libgail_b200.profile_case --path decode --frames 2
 
 Encodes seeded synthetic frames that are already in device memory, through the plain
-per-frame encoder or the batched engine, and prints the stage times of the plain path:
+per-frame encoder or the batched engine, and prints the stage times of the plain path, or
+decodes the frames' DCI codestreams (made and parsed by the host codec) through the
+plugin's decoder:
 4K (3996x2160 Y'CbCr 4:2:2 10-bit, BT.2020 PQ, as the benchmark uses) or 2K (1998x1080
 X'Y'Z' 12-bit, whose small frame slots keep a batched case to a few GB of device memory).
 Exits non-zero on any encoder error, so that a profiler run after it sees the same
@@ -22,7 +25,7 @@ W4K, H4K = 3996, 2160
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--path", choices=["plain", "served"], default="plain")
+    ap.add_argument("--path", choices=["plain", "served", "decode"], default="plain")
     ap.add_argument("--frames", type=int, default=2)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--size", choices=["4k", "2k"], default="4k")
@@ -66,6 +69,20 @@ def main():
             gb.check(L.gb_encoder_stage_times(enc.h, ms.ctypes.data, C.byref(n)))
             print("ms per frame (front, cm, order, mq, pack):", np.round(ms / max(n.value, 1), 4).tolist())
             enc.close()
+        elif args.path == "decode":
+            from libgail_b200 import codestream as CS
+            enc = dev.encoder(lay, fmt, col)
+            streams = []
+            for f in frames:
+                view, _ = enc.encode_view(f.ctypes.data)
+                streams.append(CS.rate_and_build(lay, view, 24.0)[0])
+            enc.close()
+            dec = dev.decoder(lay)
+            pic = np.zeros((dec.out_h, dec.out_w, 3), np.uint16)
+            for cs in streams:
+                _, tm, _ = dec.decode(cs, CS.parse(cs)[1].view(P.CBLK_CODE_DTYPE), out=pic)
+                print(f"decode ms: t1 {tm.t1:.3f} dwt {tm.dwt:.3f} colour+download {tm.color:.3f} ({len(cs)} bytes)")
+            dec.close()
         else:
             eng = Engine(0, 0, max_batch=args.batch)
             cid, _ = eng.add_encoder(lay, fmt, col)
