@@ -103,7 +103,7 @@ __device__ __forceinline__ uint32_t shDown(uint32_t v, int lane) {
     return lane == 31 ? 0u : t;
 }
 
-__global__ void __launch_bounds__(CM_THREADS, 5) t1CmKernel(T1Launch P) {
+__global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
     __shared__ uint32_t s_mag[CM_WARPS][32][32];
     __shared__ __align__(16) uint8_t s_stage[CM_WARPS][STAGE];
     __shared__ uint8_t s_zc[4 * 45];
