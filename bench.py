@@ -419,6 +419,8 @@ def run_ours(args):
     dec.close()
     decode_fps = len(kept_cs) * world / dec_s
 
+    mixed = run_mixed(args, local, dev, lay, fmt, col, pinned, kept_cs, frame_bytes, workers)
+
     out = None
     if rank == 0:
         peaks = {}
@@ -483,6 +485,7 @@ def run_ours(args):
                       "stage_ms_per_frame": dict(zip(["front", "t1_cm", "t1_order", "t1_mq", "pack"],
                                                      [round(x, 4) for x in stage]))},
             "dci": dci,
+            "mixed": mixed,
             "decode": {"fps": decode_fps, "unit": "frames/s", "frames": len(kept_cs),
                        "path": "decoder_decode per frame: codestream from host memory, 12-bit picture to host memory",
                        "parse_ms_per_frame": float(np.mean(parse_ms)),
@@ -506,6 +509,93 @@ def run_ours(args):
     rep.close()
     if out is not None:
         print(json.dumps(out))
+
+
+def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_bytes, workers, n=240,
+              loads=(100.0, 200.0, 300.0), seed=11):
+    """Serving a mix as it arrives: Poisson requests, 70 % encode / 30 % decode, 60 % 4K
+    (the benchmark's Y'CbCr frames and their codestreams) / 40 % 2K X'Y'Z', one engine with
+    codestreams on; per offered load the achieved rate and p50/p99 latency by kind."""
+    import threading
+
+    from libgail_b200 import codestream as CS
+    from libgail_b200 import plugin as P
+    from libgail_b200 import synth
+    from libgail_b200.engine import Engine
+    W2, H2 = 1998, 1080
+    lay2k = P.LayoutHolder(W2, H2, 0)
+    fmt2k, col2k = P.rgb48_format(W2, H2), P.color_passthrough()
+    frames2k = [synth.xyz12_to_rgb48(synth.xyz12_planes(W2, H2, seed=seed + i)) for i in range(8)]
+    eng = Engine(local, 64 * frame_bytes, max_batch=args.batch)
+    try:
+        e4, _ = eng.add_encoder(lay4k, fmt4k, col4k)
+        e2, _ = eng.add_encoder(lay2k, fmt2k, col2k)
+        d4, _ = eng.add_decoder(lay4k)
+        d2, _ = eng.add_decoder(lay2k)
+        eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
+        # 2K codestreams to decode, made by this engine; and a warm-up of every class
+        ids = [eng.submit(e2, f) for f in frames2k]
+        streams2k = []
+        for _ in ids:
+            rid, _, _, st = eng.wait(120000, copy=False)
+            streams2k.append(eng.codestream(rid)[0])
+            eng.release(rid)
+        # a burst of every class at once: the engine makes the frame and decoder slots the
+        # timed loads will use
+        warm = [eng.submit(e4, frames4k[i % len(frames4k)]) for i in range(32)]
+        warm += [eng.submit(e2, frames2k[i % len(frames2k)]) for i in range(24)]
+        warm += [eng.submit_decode(d4, streams4k[i % len(streams4k)]) for i in range(12)]
+        warm += [eng.submit_decode(d2, streams2k[i % len(streams2k)]) for i in range(12)]
+        for _ in warm:
+            rid, _, _, _ = eng.wait(120000, copy=False)
+            eng.release(rid)
+        rng = np.random.default_rng(seed)
+        kinds = rng.random(n) < 0.7           # encode
+        big = rng.random(n) < 0.6             # 4K
+        picks = rng.integers(0, 1 << 30, n)
+        out = []
+        for load in loads:
+            arr = poisson_arrivals(n, load, seed=seed + int(load))
+            lat = {}
+            kind_of = {}
+            done = threading.Event()
+
+            def collect():
+                for _ in range(n):
+                    rid, _, ms, st = eng.wait(120000, copy=False)
+                    if rid < 0 or st != 0:
+                        raise RuntimeError(f"mixed request failed (id {rid}, status {st})")
+                    lat[rid] = ms
+                    eng.release(rid)
+                done.set()
+
+            th = threading.Thread(target=collect)
+            th.start()
+            t0 = time.perf_counter()
+            for i in range(n):
+                while time.perf_counter() - t0 < arr[i]:
+                    pass
+                if kinds[i]:
+                    rid = eng.submit(e4, frames4k[picks[i] % len(frames4k)]) if big[i] else \
+                        eng.submit(e2, frames2k[picks[i] % len(frames2k)])
+                    kind_of[rid] = "encode"
+                else:
+                    rid = eng.submit_decode(d4, streams4k[picks[i] % len(streams4k)]) if big[i] else \
+                        eng.submit_decode(d2, streams2k[picks[i] % len(streams2k)])
+                    kind_of[rid] = "decode"
+            th.join()
+            elapsed = time.perf_counter() - t0
+            if len(lat) != n:
+                raise RuntimeError("mixed serving lost requests")
+            row = {"offered_fps": load, "achieved_fps": n / elapsed}
+            for k in ("encode", "decode"):
+                v = [lat[r] for r in lat if kind_of.get(r) == k]
+                row[k] = {"requests": len(v), "p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99))}
+            out.append(row)
+        return {"requests_per_load": n, "mix": "70 % encode / 30 % decode; 60 % 4K Y'CbCr PQ / 40 % 2K X'Y'Z'",
+                "loads": out}
+    finally:
+        eng.close()
 
 
 def main():

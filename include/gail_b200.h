@@ -124,7 +124,16 @@ GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
  *                          the DCI check; the frame is handed out by gb_engine_wait once its
  *                          codestream is made (the latency includes it)
  *   gb_engine_codestream   a handed-out frame's codestream (valid until release) and its
- *                          DCI verdict (1, 0, or -1 when not checked) */
+ *                          DCI verdict (1, 0, or -1 when not checked)
+ *   gb_engine_add_decoder  a decode class (layout, decode settings as decoder_create takes
+ *                          them); frameBytes: its device footprint per decode in flight
+ *   gb_engine_submit_decode  queue a codestream (copied) for decoding: host workers parse it
+ *                          (gb_parse_codestream) and decode it on a decoder slot of its class
+ *                          (decoder_decode's stages, each slot on its own stream, sharing the
+ *                          HBM budget); handed out by gb_engine_wait like an encode (its Tier-1
+ *                          view empty)
+ *   gb_engine_picture      a handed-out decode's picture (valid until release): height rows
+ *                          of width x 3 codes */
 typedef struct GbEngine GbEngine;
 GB_API int gb_engine_create(int device, uint64_t hbmBudget, int maxBatch, GbEngine** out);
 GB_API void gb_engine_destroy(GbEngine* e);
@@ -138,6 +147,10 @@ GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5);
 GB_API int gb_engine_set_codestream(GbEngine* e, double fps, double maxMbps, double compMbps, const char* label,
                                     const char* tag, int threads, int check);
 GB_API int gb_engine_codestream(GbEngine* e, int64_t id, const uint8_t** data, uint64_t* size, int* dciOk);
+GB_API int gb_engine_add_decoder(GbEngine* e, const GailCudaLayout* layout, const GailCudaDecodeSettings* settings,
+                                 int* classId, uint64_t* frameBytes);
+GB_API int gb_engine_submit_decode(GbEngine* e, int classId, const uint8_t* data, uint64_t size, int64_t* id);
+GB_API int gb_engine_picture(GbEngine* e, int64_t id, const uint16_t** pix, int* width, int* height);
 
 /* The host codec around a Tier-1 frame, byte-identical to libgail's core for the same
  * frame. Thread-safe across threads (each keeps its own writer per layout and label).

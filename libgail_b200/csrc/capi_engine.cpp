@@ -76,6 +76,28 @@ GB_API int gb_engine_codestream(GbEngine* e, int64_t id, const uint8_t** data, u
     });
 }
 
+GB_API int gb_engine_add_decoder(GbEngine* e, const GailCudaLayout* layout, const GailCudaDecodeSettings* settings,
+                                 int* classId, uint64_t* frameBytes) {
+    return gbGuard([&] {
+        if (!e || !layout || !settings || !classId) throw std::logic_error("null argument");
+        *classId = e->e->addDecodeClass(*layout, *settings, frameBytes);
+    });
+}
+
+GB_API int gb_engine_submit_decode(GbEngine* e, int classId, const uint8_t* data, uint64_t size, int64_t* id) {
+    return gbGuard([&] {
+        if (!e || !id) throw std::logic_error("null argument");
+        *id = e->e->submitDecode(classId, data, size);
+    });
+}
+
+GB_API int gb_engine_picture(GbEngine* e, int64_t id, const uint16_t** pix, int* width, int* height) {
+    return gbGuard([&] {
+        if (!e || !pix || !width || !height) throw std::logic_error("null argument");
+        if (!e->e->picture(id, pix, width, height)) throw std::logic_error("not a decode request");
+    });
+}
+
 GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5) {
     return gbGuard([&] {
         if (!e || !out5) throw std::logic_error("null argument");

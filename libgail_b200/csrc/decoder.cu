@@ -596,7 +596,21 @@ void DecoderSlot::release() {
 
 void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, const GbCblkCode* blocks, size_t numBlocks,
                          void* dst, ptrdiff_t strideBytes, GailCudaDecodeTimings* tm) {
-    const auto t0 = std::chrono::steady_clock::now();
+    enqueue(frame, data, size, blocks, numBlocks, tm && tm->wantWavelet);
+    const uint16_t* pic = finish(tm);
+    const uint64_t rowBytes = (uint64_t)outW_ * 6;
+    if (strideBytes == (ptrdiff_t)rowBytes) {
+        std::memcpy(dst, pic, rowBytes * outH_);
+    } else {
+        for (int y = 0; y < outH_; ++y)
+            std::memcpy((uint8_t*)dst + (ptrdiff_t)y * strideBytes, (const uint8_t*)pic + (uint64_t)y * rowBytes, rowBytes);
+    }
+    if (tm) tm->total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
+}
+
+void DecoderSlot::enqueue(const Layout& frame, const uint8_t* data, size_t size, const GbCblkCode* blocks,
+                          size_t numBlocks, bool wantWavelet) {
+    t0_ = std::chrono::steady_clock::now();
     if (frame.width != L_.width || frame.height != L_.height || frame.levels != L_.levels ||
         frame.bands.size() != L_.bands.size() || (int)numBlocks != L_.numCblks())
         throw std::logic_error("frame does not match the layout the slot was made for");
@@ -604,8 +618,8 @@ void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, 
     GB_CHECK(cudaSetDevice(dev_));
     const cudaStream_t st = st_;
     const uint64_t npix = (uint64_t)L_.width * L_.height, n = numBlocks;
+    GB_CHECK(cudaStreamSynchronize(st));  // the slot's pinned buffers are free again
     if (size > capBytes_) {
-        cudaStreamSynchronize(st);
         cudaFree(dBytes_);
         allocs_.erase(std::find(allocs_.begin(), allocs_.end(), (void*)dBytes_));
         cudaFreeHost(hBytes_);
@@ -621,7 +635,7 @@ void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, 
     std::memcpy(hBytes_, data, size);
     std::memcpy(hCodes_, blocks, n * sizeof(GbCblkCode));
     for (size_t i = 0; i < frame.bands.size(); ++i) hHalf_[i] = 0.5f * frame.bands[i].delta;
-    const bool wantWavelet = tm && tm->wantWavelet;
+    wantWavelet_ = wantWavelet;
 
     GB_CHECK(cudaEventRecord(ev_[0], st));
     GB_CHECK(cudaMemcpyAsync(dBytes_, hBytes_, size, cudaMemcpyHostToDevice, st));
@@ -636,14 +650,8 @@ void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, 
     decodeKernel<<<std::min<uint32_t>(divUp((uint32_t)n, DEC_THREADS), (uint32_t)sms * 16), DEC_THREADS, 0, st>>>(da);
     GB_CHECK(cudaGetLastError());
     GB_CHECK(cudaEventRecord(ev_[1], st));
-    if (wantWavelet) {
-        GB_CHECK(cudaStreamSynchronize(st));
-        for (int c = 0; c < 3; ++c) {
-            wavelet_[c].resize(npix);
-            GB_CHECK(cudaMemcpy(wavelet_[c].data(), dPlanes_ + c * npix, npix * 4, cudaMemcpyDeviceToHost));
-        }
-    }
-    // inverse wavelet, levels top down; the last one writes the picture
+    // inverse wavelet, levels top down; the last one writes the picture (the planes are only
+    // read, so the wavelet tap can still be copied out after it)
     const int stop = s_.reduce;
     const int llStride = L_.levelW(1);
     const uint64_t llComp = (uint64_t)L_.levelW(1) * L_.levelH(1);
@@ -680,15 +688,18 @@ void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, 
     GB_CHECK(cudaMemcpyAsync(hOut_, dOut_, outBytes, cudaMemcpyDeviceToHost, st));
     GB_CHECK(cudaMemcpyAsync(hCtl_, dCtl_, 64, cudaMemcpyDeviceToHost, st));
     GB_CHECK(cudaEventRecord(ev_[3], st));
-    GB_CHECK(cudaStreamSynchronize(st));
+}
+
+const uint16_t* DecoderSlot::finish(GailCudaDecodeTimings* tm) {
+    GB_CHECK(cudaSetDevice(dev_));
+    GB_CHECK(cudaStreamSynchronize(st_));
     GB_CHECK(cudaGetLastError());
-    const uint64_t rowBytes = (uint64_t)outW_ * 6;
-    if (strideBytes == (ptrdiff_t)rowBytes) {
-        std::memcpy(dst, hOut_, outBytes);
-    } else {
-        for (int y = 0; y < outH_; ++y)
-            std::memcpy((uint8_t*)dst + (ptrdiff_t)y * strideBytes, (const uint8_t*)hOut_ + (uint64_t)y * rowBytes, rowBytes);
-    }
+    const uint64_t npix = (uint64_t)L_.width * L_.height;
+    if (wantWavelet_)
+        for (int c = 0; c < 3; ++c) {
+            wavelet_[c].resize(npix);
+            GB_CHECK(cudaMemcpy(wavelet_[c].data(), dPlanes_ + c * npix, npix * 4, cudaMemcpyDeviceToHost));
+        }
     if (tm) {
         float a = 0, b = 0, c = 0;
         cudaEventElapsedTime(&a, ev_[0], ev_[1]);
@@ -697,10 +708,11 @@ void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, 
         tm->t1 = a;
         tm->dwt = b;
         tm->color = c;
-        tm->total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-        tm->numWavelet = wantWavelet ? npix : 0;
-        for (int k = 0; k < 3; ++k) tm->wavelet[k] = wantWavelet ? wavelet_[k].data() : nullptr;
+        tm->total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
+        tm->numWavelet = wantWavelet_ ? npix : 0;
+        for (int k = 0; k < 3; ++k) tm->wavelet[k] = wantWavelet_ ? wavelet_[k].data() : nullptr;
     }
+    return hOut_;
 }
 
 }  // namespace gb

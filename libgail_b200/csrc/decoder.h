@@ -5,6 +5,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdint>
 #include <vector>
 
@@ -36,6 +37,15 @@ public:
     // frame: this frame's layout (the slot's geometry, the stream's step sizes).
     void decode(const Layout& frame, const uint8_t* data, size_t size, const GbCblkCode* blocks, size_t numBlocks, void* dst,
                 ptrdiff_t strideBytes, GailCudaDecodeTimings* tm);
+    // The same in two halves: enqueue() copies the codestream and the blocks into the
+    // slot's pinned buffers and starts every stage on the slot's stream; finish() waits,
+    // checks the kernels' status and returns the picture in pinned host memory (outH rows
+    // of outW x 3 codes), valid until the next enqueue.
+    void enqueue(const Layout& frame, const uint8_t* data, size_t size, const GbCblkCode* blocks, size_t numBlocks,
+                 bool wantWavelet);
+    const uint16_t* finish(GailCudaDecodeTimings* tm);
+    int outW() const { return outW_; }
+    int outH() const { return outH_; }
 
 private:
     void release();
@@ -59,6 +69,8 @@ private:
     float* hHalf_ = nullptr;
     uint32_t* hCtl_ = nullptr;
     std::vector<float> wavelet_[3];
+    bool wantWavelet_ = false;
+    std::chrono::steady_clock::time_point t0_;
 };
 
 }  // namespace gb

@@ -69,6 +69,23 @@ struct EncodeEngine::Request {
     int status = 0;
     std::vector<uint8_t> cs;  // the codestream, when the engine makes them
     int dciOk = -1;
+    // decode requests
+    bool decode = false;
+    std::vector<uint8_t> input;  // the codestream to decode
+    DecSlot* dslot = nullptr;
+    const uint16_t* pix = nullptr;
+};
+
+struct EncodeEngine::DecClass {
+    Layout L;
+    GailCudaDecodeSettings s;
+    uint64_t slotBytes = 0;
+    std::vector<DecSlot*> free;
+};
+
+struct EncodeEngine::DecSlot {
+    int cls = 0;
+    std::unique_ptr<DecoderSlot> slot;
 };
 
 struct EncodeEngine::Batch {
@@ -180,7 +197,11 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
 }
 
 EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
-    if (used_ + c.slotBytes > budget_) return nullptr;
+    {
+        std::lock_guard<std::mutex> lock(budgetM_);
+        if (used_ + c.slotBytes > budget_) return nullptr;
+        used_ += c.slotBytes;  // reserved now, given back if the slot cannot be made
+    }
     auto s = std::make_unique<Slot>();
     s->cls = (int)(std::find_if(classes_.begin(), classes_.end(), [&](auto& p) { return p.get() == &c; }) - classes_.begin());
     s->index = (int)slots_.size();
@@ -233,14 +254,20 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         if (s->graph) cudaGraphDestroy(s->graph);
         if (s->frontDone) cudaEventDestroy(s->frontDone);
         cudaGetLastError();
+        std::lock_guard<std::mutex> lock(budgetM_);
+        used_ -= c.slotBytes;
         return nullptr;  // out of memory now: the request waits for a slot to free up
     }
-    used_ += c.slotBytes;
     Slot* raw = s.get();
     slots_.push_back(std::move(s));
+    uint64_t used;
+    {
+        std::lock_guard<std::mutex> lock(budgetM_);
+        used = used_;
+    }
     std::lock_guard<std::mutex> lock(m_);
     stats_.slots = slots_.size();
-    stats_.slotBytes = used_;
+    stats_.slotBytes = used;
     return raw;
 }
 
@@ -273,7 +300,8 @@ bool EncodeEngine::wait(int timeoutMs, int64_t* id, GailCudaTier1* out, double* 
     *latencyMs = r->latency;
     *status = r->status;
     const Slot* s = r->slot;
-    *out = {reinterpret_cast<const GbCblkInfo*>(s->hInfo), s->hLen, s->hDist, s->hData, s->n, s->hTot[1], s->hTot[0]};
+    if (r->decode || !s) *out = GailCudaTier1{};
+    else *out = {reinterpret_cast<const GbCblkInfo*>(s->hInfo), s->hLen, s->hDist, s->hData, s->n, s->hTot[1], s->hTot[0]};
     return true;
 }
 
@@ -281,6 +309,14 @@ void EncodeEngine::release(int64_t id) {
     std::lock_guard<std::mutex> lock(m_);
     if (id < 0 || id >= (int64_t)requests_.size() || !requests_[id]) throw std::logic_error("unknown request");
     Request* r = requests_[id].get();
+    if (r->decode) {
+        if (r->dslot) {
+            decClasses_[r->cls]->free.push_back(r->dslot);
+            cvDecSlot_.notify_all();
+        }
+        requests_[id].reset();
+        return;
+    }
     if (!r->slot) throw std::logic_error("request not finished");
     classes_[r->cls]->free.push_back(r->slot);
     requests_[id].reset();
@@ -299,7 +335,112 @@ void EncodeEngine::setCodestream(const CodestreamConfig& c) {
     if (csOn_) throw std::logic_error("codestreams are already on");
     cs_ = c;
     csOn_ = true;
-    for (int i = 0; i < c.threads; ++i) csWorkers_.emplace_back([this] { codestreamWorker(); });
+    startWorkers(c.threads);
+}
+
+// Grows the pool of host workers to at least n (m_ held).
+void EncodeEngine::startWorkers(int n) {
+    while ((int)csWorkers_.size() < n) csWorkers_.emplace_back([this] { codestreamWorker(); });
+}
+
+int EncodeEngine::addDecodeClass(const GailCudaLayout& layout, const GailCudaDecodeSettings& s, uint64_t* frameBytes) {
+    GB_CHECK(cudaSetDevice(dev_));
+    auto c = std::make_unique<DecClass>();
+    layoutFromAbi(layout, c->L);
+    if (s.reduce < 0 || s.reduce > c->L.levels) throw std::logic_error("more resolution levels left out than the layout has");
+    c->s = s;
+    c->slotBytes = decoderSlotBytes(c->L, s);
+    if (frameBytes) *frameBytes = c->slotBytes;
+    std::lock_guard<std::mutex> lock(m_);
+    decClasses_.push_back(std::move(c));
+    startWorkers(4);
+    return (int)decClasses_.size() - 1;
+}
+
+int64_t EncodeEngine::submitDecode(int cls, const uint8_t* data, uint64_t size) {
+    if (!data || size == 0) throw std::logic_error("no codestream");
+    auto r = std::make_unique<Request>();
+    r->decode = true;
+    r->cls = cls;
+    r->input.assign(data, data + size);
+    r->t0 = Clock::now();
+    std::lock_guard<std::mutex> lock(m_);
+    if (cls < 0 || cls >= (int)decClasses_.size()) throw std::logic_error("unknown decode class");
+    if (!error_.empty()) throw std::runtime_error(error_);
+    r->id = nextId_++;
+    csq_.push_back(r.get());
+    requests_.push_back(std::move(r));
+    cvCs_.notify_one();
+    return requests_.back()->id;
+}
+
+bool EncodeEngine::picture(int64_t id, const uint16_t** pix, int* width, int* height) {
+    std::lock_guard<std::mutex> lock(m_);
+    if (id < 0 || id >= (int64_t)requests_.size() || !requests_[id]) throw std::logic_error("unknown request");
+    const Request* r = requests_[id].get();
+    if (!r->decode) return false;
+    *pix = r->pix;
+    *width = r->dslot ? r->dslot->slot->outW() : 0;
+    *height = r->dslot ? r->dslot->slot->outH() : 0;
+    return true;
+}
+
+// A decode request on a worker: parse, a decoder slot of its class (made when the budget
+// allows, else the next one released), decode on the slot's stream, hand out.
+void EncodeEngine::decodeJob(Request* r) {
+    DecClass* c;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        c = decClasses_[r->cls].get();
+    }
+    Layout frame;
+    std::vector<GbCblkCode> blocks;
+    try {
+        parseCodestream(r->input.data(), r->input.size(), frame, blocks);
+        if (frame.width != c->L.width || frame.height != c->L.height || frame.levels != c->L.levels)
+            throw std::runtime_error("codestream of another frame size than its decode class");
+        DecSlot* ds = nullptr;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lock(m_);
+                if (!c->free.empty()) {
+                    ds = c->free.back();
+                    c->free.pop_back();
+                    break;
+                }
+            }
+            bool room;
+            {
+                std::lock_guard<std::mutex> lock(budgetM_);
+                room = used_ + c->slotBytes <= budget_;
+                if (room) used_ += c->slotBytes;
+            }
+            if (room) {
+                auto d = std::make_unique<DecSlot>();
+                d->cls = r->cls;
+                try {
+                    d->slot = std::make_unique<DecoderSlot>(dev_, c->L, c->s);
+                } catch (...) {
+                    std::lock_guard<std::mutex> lock(budgetM_);
+                    used_ -= c->slotBytes;
+                    throw;
+                }
+                ds = d.get();
+                std::lock_guard<std::mutex> lock(m_);
+                decSlots_.push_back(std::move(d));
+                break;
+            }
+            std::unique_lock<std::mutex> lock(m_);  // no room: the next released slot
+            cvDecSlot_.wait_for(lock, std::chrono::milliseconds(50), [&] { return !c->free.empty() || stop_.load(); });
+            if (stop_) throw std::runtime_error("engine stopping");
+        }
+        r->dslot = ds;
+        ds->slot->enqueue(frame, r->input.data(), r->input.size(), blocks.data(), blocks.size(), false);
+        r->pix = ds->slot->finish(nullptr);
+        r->status = kOk;
+    } catch (const std::exception&) {
+        r->status = kError;
+    }
 }
 
 bool EncodeEngine::codestream(int64_t id, const uint8_t** data, uint64_t* size, int* dciOk) {
@@ -314,19 +455,32 @@ bool EncodeEngine::codestream(int64_t id, const uint8_t** data, uint64_t* size, 
 }
 
 void EncodeEngine::codestreamWorker() {
+    cudaSetDevice(dev_);
     // one writer per frame class on this worker (the packet order is flattened once)
     std::vector<std::unique_ptr<CodestreamWriter>> writers;
     for (;;) {
         Request* r;
-        const Class* c;
+        const Class* c = nullptr;
         {
             std::unique_lock<std::mutex> lock(m_);
             cvCs_.wait(lock, [&] { return stop_.load() || !csq_.empty(); });
             if (csq_.empty()) return;
             r = csq_.front();
             csq_.pop_front();
-            c = classes_[r->cls].get();
-            if (writers.size() < classes_.size()) writers.resize(classes_.size());
+            if (!r->decode) {
+                c = classes_[r->cls].get();
+                if (writers.size() < classes_.size()) writers.resize(classes_.size());
+            }
+        }
+        if (r->decode) {
+            decodeJob(r);
+            const auto now = Clock::now();
+            std::lock_guard<std::mutex> lock(m_);
+            r->latency = msBetween(r->t0, now);
+            done_.push_back(r);
+            stats_.frames++;
+            cvDone_.notify_all();
+            continue;
         }
         auto& w = writers[r->cls];
         if (!w) w = std::make_unique<CodestreamWriter>(c->L, cs_.label);

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "color.h"
+#include "decoder.h"
 #include "encoder.h"
 #include "gail_cuda_plugin_abi.h"
 #include "layout.h"
@@ -69,6 +70,17 @@ public:
     // passed the DCI check (-1 when not checked). False when codestreams are off.
     bool codestream(int64_t id, const uint8_t** data, uint64_t* size, int* dciOk);
 
+    // Decode requests beside the encodes. A decode class is a layout and decode settings;
+    // its frames in flight take decoder slots from the same HBM budget. A decode request
+    // (the codestream is copied on submit) is parsed, decoded and handed out by the host
+    // workers (those of setCodestream, or four started with the first decode class), each
+    // slot on its own stream, so decodes overlap each other and the encode batches.
+    int addDecodeClass(const GailCudaLayout& layout, const GailCudaDecodeSettings& s, uint64_t* frameBytes);
+    int64_t submitDecode(int cls, const uint8_t* data, uint64_t size);
+    // The picture of a finished decode (valid until release): height rows of width x 3
+    // codes. False for an encode request.
+    bool picture(int64_t id, const uint16_t** pix, int* width, int* height);
+
     struct Stats {
         uint64_t frames = 0, batches = 0, batchFrames = 0, slots = 0, slotBytes = 0;
     };
@@ -79,16 +91,21 @@ private:
     struct Slot;
     struct Request;
     struct Batch;
+    struct DecClass;
+    struct DecSlot;
 
     void run();
     void codestreamWorker();
+    void decodeJob(Request* r);
+    void startWorkers(int n);
     bool admit();
     bool launchBatch(Batch& b);
     bool collect(Batch& b);
     Slot* newSlot(Class& c);
 
     int dev_;
-    uint64_t budget_ = 0, used_ = 0;
+    uint64_t budget_ = 0, used_ = 0;  // used_ under budgetM_
+    std::mutex budgetM_;
     int maxBatch_;
     cudaStream_t front_ = nullptr;
     std::vector<std::unique_ptr<Class>> classes_;
@@ -111,9 +128,13 @@ private:
     // codestream stage
     CodestreamConfig cs_;
     bool csOn_ = false;
-    std::deque<Request*> csq_;  // Tier-1 done, codestream to make
+    std::deque<Request*> csq_;  // Tier-1 done, codestream to make; or a decode to run
     std::condition_variable cvCs_;
     std::vector<std::thread> csWorkers_;
+    // decode requests
+    std::vector<std::unique_ptr<DecClass>> decClasses_;
+    std::vector<std::unique_ptr<DecSlot>> decSlots_;
+    std::condition_variable cvDecSlot_;
 };
 
 }  // namespace gb

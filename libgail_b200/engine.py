@@ -6,7 +6,7 @@ import ctypes as C
 import numpy as np
 
 from . import GailError, check, lib
-from .plugin import Color, EncodeSettings, FrameFormat, LayoutHolder, Tier1, Tier1Frame
+from .plugin import Color, DecodeSettings, EncodeSettings, FrameFormat, LayoutHolder, Tier1, Tier1Frame
 
 
 def _bind():
@@ -26,6 +26,10 @@ def _bind():
                                            C.c_int, C.c_int]
     L.gb_engine_codestream.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_uint8)),
                                        C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
+    L.gb_engine_add_decoder.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]
+    L.gb_engine_submit_decode.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_int64)]
+    L.gb_engine_picture.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_uint16)), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int)]
     L._engine_bound = True
     return L
 
@@ -84,6 +88,26 @@ class Engine:
         if not copy:
             return (p, n.value), ok.value
         return (C.string_at(p, n.value) if n.value else b""), ok.value
+
+    def add_decoder(self, layout: LayoutHolder, reduce: int = 0, high_bits: bool = False):
+        """A decode class; returns its id and the device bytes one decode in flight takes."""
+        ds = DecodeSettings(reduce=reduce, highBits=int(high_bits))
+        cid, nbytes = C.c_int(), C.c_uint64()
+        check(lib().gb_engine_add_decoder(self.h, C.byref(layout.abi), C.byref(ds), C.byref(cid), C.byref(nbytes)))
+        self._classes.append((layout, ds))
+        return cid.value, nbytes.value
+
+    def submit_decode(self, cls: int, codestream: bytes) -> int:
+        rid = C.c_int64()
+        check(lib().gb_engine_submit_decode(self.h, cls, codestream, len(codestream), C.byref(rid)))
+        return rid.value
+
+    def picture(self, rid: int, copy: bool = True):
+        """A finished decode's picture, (height, width, 3) uint16."""
+        p, w, h = C.POINTER(C.c_uint16)(), C.c_int(), C.c_int()
+        check(lib().gb_engine_picture(self.h, rid, C.byref(p), C.byref(w), C.byref(h)))
+        a = np.ctypeslib.as_array(p, (h.value, w.value, 3))
+        return a.copy() if copy else a
 
     def release(self, rid: int):
         check(lib().gb_engine_release(self.h, rid))

@@ -171,3 +171,45 @@ def test_slot_pipeline_codestreams(dev):
         eng.close()
     for i, rid in enumerate(ids):
         assert res[i][0] == got[rid][0] and res[i][1] and got[rid][1] == 1
+
+
+@pytest.mark.gpu
+def test_engine_mixed_encode_decode(dev):
+    """Encode and decode requests of several profiles in one engine: every decode gives the
+    picture the plugin's decoder gives alone, every encode its plain Tier-1 output."""
+    from libgail_b200 import codestream as CS
+    jobs = []  # (kind, class index, payload, expected)
+    profiles = [(1998, 1080, 0), (3996, 2160, 1)]
+    eng = Engine(0, 0, max_batch=8)
+    try:
+        enc_cls, dec_cls = {}, {}
+        for W, H, fk in profiles:
+            lay = P.LayoutHolder(W, H, fk)
+            frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=500 + i + W)) for i in range(3)]
+            enc = dev.encoder(lay, P.rgb48_format(W, H), P.color_passthrough())
+            t1s = [enc.encode(f)[0] for f in frames]
+            enc.close()
+            streams = [CS.rate_and_build(lay, t, 24.0)[0] for t in t1s]
+            dec = dev.decoder(lay)
+            pics = [dec.decode(cs, CS.parse(cs)[1].view(P.CBLK_CODE_DTYPE))[0] for cs in streams]
+            dec.close()
+            enc_cls[(W, H)] = eng.add_encoder(lay, P.rgb48_format(W, H), P.color_passthrough())[0]
+            dec_cls[(W, H)] = eng.add_decoder(lay)[0]
+            for i in range(3):
+                jobs.append(("enc", (W, H), frames[i], t1s[i]))
+                jobs.append(("dec", (W, H), streams[i], pics[i]))
+        want = {}
+        for kind, key, payload, expect in jobs:  # interleaved kinds and profiles
+            rid = eng.submit(enc_cls[key], payload) if kind == "enc" else eng.submit_decode(dec_cls[key], payload)
+            want[rid] = (kind, expect)
+        for _ in want:
+            rid, t1, _, st = eng.wait(120000)
+            assert rid >= 0 and st == 0
+            kind, expect = want[rid]
+            if kind == "enc":
+                assert _same(t1, expect)
+            else:
+                assert np.array_equal(eng.picture(rid), expect)
+            eng.release(rid)
+    finally:
+        eng.close()
