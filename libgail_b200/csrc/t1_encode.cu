@@ -404,12 +404,25 @@ __device__ __forceinline__ uint32_t orderBucket(uint32_t s) {
     return ORDER_BUCKETS - 1 - cls;
 }
 
-__global__ void __launch_bounds__(1024) t1OrderKernel(T1Launch P) {
+// Blocks with at least this many decisions are MQ-coded alone in a warp (its lane 0), at
+// most one per warp for half the launch's warps: the longest serial chains, which would
+// otherwise run beside 31 divergent neighbours. A power of two, so that they are exactly
+// the first blocks of the order.
+constexpr uint32_t kSoloDecisions = 8192;
+
+__global__ void __launch_bounds__(1024) t1OrderKernel(T1Launch P, uint32_t maxSolo) {
     __shared__ uint32_t hist[ORDER_BUCKETS];
+    __shared__ uint32_t solo;
     for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
+    if (threadIdx.x == 0) solo = 0;
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < P.n; i += blockDim.x) atomicAdd(&hist[orderBucket(P.info[4 * (size_t)i + 2])], 1u);
+    for (uint32_t i = threadIdx.x; i < P.n; i += blockDim.x) {
+        const uint32_t d = P.info[4 * (size_t)i + 2];
+        atomicAdd(&hist[orderBucket(d)], 1u);
+        if (d >= kSoloDecisions) atomicAdd(&solo, 1u);
+    }
     __syncthreads();
+    if (threadIdx.x == 0) P.ctl[3] = min(solo, maxSolo);
     if (threadIdx.x < 32) {
         // exclusive scan of 128 counters by one warp, four per lane
         const int lane = threadIdx.x;
@@ -544,18 +557,69 @@ __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
     __syncthreads();
     uint32_t* ctx = s_ctx + threadIdx.x;
     uint32_t* status = P.ctl + 1;
+    const int lane = threadIdx.x & 31;
+    const uint32_t solo = P.ctl[3];  // blocks coded alone, perm[0 .. solo)
+    const uint32_t warpId = blockIdx.x * (MQ_THREADS / 32) + (threadIdx.x >> 5);
 
     // Per-lane state of the block in hand. Invariant between decisions: s is the decision
-    // at pos and t the state of its context.
+    // at pos and t the state of its context; nxt holds the decisions from pos on.
     uint32_t job = 0, pos = 0, nsym = 0, np = 0, k = 0, nextEnd = 0, stop = 0, s = 0, t = 0;
     const uint8_t* sym = nullptr;
-    uint4 nxt = make_uint4(0, 0, 0, 0);  // the block's next 16 decisions
+    uint4 nxt = make_uint4(0, 0, 0, 0);
     Coder e;
     e.cap = 0;
     bool have = false;
 
+    // starts block j; false when it has no coding pass (nothing to code)
+    auto begin = [&](uint32_t j) {
+        job = j;
+        np = P.info[4 * (size_t)job + 1];
+        nsym = P.info[4 * (size_t)job + 2];
+        if (np == 0) {
+            P.info[4 * (size_t)job + 3] = 0;
+            return false;
+        }
+        const T1Job J = P.jobs[job];
+        sym = J.sym;
+        e.out = J.cw;
+        e.cap = J.cap;
+        e.A = 0x8000u;
+        e.C = 0;
+        e.CT = 12;
+        e.bp = -1;
+        e.B = 0;
+        e.overflow = false;
+        // initial states, Table D.7: ZC context 0 state 4, run-length 3, uniform 46
+#pragma unroll
+        for (int c = 0; c < 19; ++c) ctx[c * MQ_THREADS] = s_init[0];
+        ctx[0] = s_init[1];
+        ctx[17 * MQ_THREADS] = s_init[2];
+        ctx[18 * MQ_THREADS] = s_init[3];
+        pos = 0;
+        k = 0;
+        nextEnd = P.passEnd[(size_t)job * kMaxPasses];
+        stop = min(nsym, nextEnd);
+        nxt = nsym ? *reinterpret_cast<const uint4*>(sym) : make_uint4(0, 0, 0, 0);
+        s = nxt.x & 0xFFu;
+        t = ctx[(s >> 1) * MQ_THREADS];
+        have = true;
+        return true;
+    };
+
+    // A warp below `solo` first codes block perm[warpId] on its lane 0 while the other
+    // lanes wait; then all its lanes take blocks from the shared queue, one at a time.
+    bool soloPhase = warpId < solo;
+    bool soloJob = false;
+    if (soloPhase && lane == 0) soloJob = begin(P.perm[warpId]);
+
     for (;;) {
-        uint4 v;
+        if (soloPhase) {  // warp-uniform; every lane of the warp is still in the loop
+            if (__shfl_sync(kFull, (int)soloJob, 0)) {
+                if (lane != 0) continue;
+            } else {
+                soloPhase = false;
+            }
+        }
         if (!have || pos >= nsym) {
             if (have) {
                 // end of block: remaining pass ends, flush, truncation points
@@ -575,55 +639,26 @@ __global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
                 }
                 P.info[4 * (size_t)job + 3] = e.overflow ? 0u : len;
                 have = false;
+                soloJob = false;
             }
-            // next block
-            uint32_t qi;
+            // next block from the shared queue (after the solo blocks)
+            bool got = false;
             for (;;) {
-                qi = atomicAdd(P.ctl, 1u);
+                const uint32_t qi = solo + atomicAdd(P.ctl, 1u);
                 if (qi >= P.n) break;
-                job = P.perm[qi];
-                np = P.info[4 * (size_t)job + 1];
-                nsym = P.info[4 * (size_t)job + 2];
-                if (np == 0) {
-                    P.info[4 * (size_t)job + 3] = 0;
-                    continue;
+                if (begin(P.perm[qi])) {
+                    got = true;
+                    break;
                 }
-                break;
             }
-            if (qi >= P.n) break;
-            const T1Job J = P.jobs[job];
-            sym = J.sym;
-            e.out = J.cw;
-            e.cap = J.cap;
-            e.A = 0x8000u;
-            e.C = 0;
-            e.CT = 12;
-            e.bp = -1;
-            e.B = 0;
-            e.overflow = false;
-            // initial states, Table D.7: ZC context 0 state 4, run-length 3, uniform 46
-#pragma unroll
-            for (int c = 0; c < 19; ++c) ctx[c * MQ_THREADS] = s_init[0];
-            ctx[0] = s_init[1];
-            ctx[17 * MQ_THREADS] = s_init[2];
-            ctx[18 * MQ_THREADS] = s_init[3];
-            pos = 0;
-            k = 0;
-            nextEnd = P.passEnd[(size_t)job * kMaxPasses];
-            stop = min(nsym, nextEnd);
-            have = true;
-            if (nsym == 0) continue;
-            v = *reinterpret_cast<const uint4*>(sym);
-            nxt = nsym > 16 ? *reinterpret_cast<const uint4*>(sym + 16) : make_uint4(0, 0, 0, 0);
-            s = v.x & 0xFFu;
-            t = ctx[(s >> 1) * MQ_THREADS];
-        } else {
-            v = nxt;
-            nxt = (pos + 16 < nsym) ? *reinterpret_cast<const uint4*>(sym + pos + 16) : make_uint4(0, 0, 0, 0);
+            if (!got) break;
+            continue;  // a block without decisions finishes at once
         }
         // one aligned chunk of 16 decisions (fewer at the block's end): a word of four
         // decisions unrolled at a time, the next decision's context state read ahead, off
         // the serial chain of the coder
+        const uint4 v = nxt;
+        nxt = (pos + 16 < nsym) ? *reinterpret_cast<const uint4*>(sym + pos + 16) : make_uint4(0, 0, 0, 0);
         uint32_t w0 = v.x, w1 = v.y, w2 = v.z, w3 = v.w;
         const uint32_t w4 = nxt.x;
         bool done = false;
@@ -688,9 +723,9 @@ void t1Encode(const T1Launch& L, cudaStream_t st, cudaEvent_t* marks) {
     const uint32_t cmBlocks = min(divUp(L.n, CM_WARPS), (uint32_t)sms * 16u);
     t1CmKernel<<<cmBlocks, CM_THREADS, 0, st>>>(L);
     if (marks) GB_CHECK(cudaEventRecord(marks[0], st));
-    t1OrderKernel<<<1, 1024, 0, st>>>(L);
-    if (marks) GB_CHECK(cudaEventRecord(marks[1], st));
     const uint32_t mqBlocks = min(divUp(L.n, MQ_THREADS), (uint32_t)sms * 16u);
+    t1OrderKernel<<<1, 1024, 0, st>>>(L, mqBlocks * (MQ_THREADS / 32) / 2);
+    if (marks) GB_CHECK(cudaEventRecord(marks[1], st));
     t1MqKernel<<<mqBlocks, MQ_THREADS, 0, st>>>(L);
     GB_CHECK(cudaGetLastError());
 }
