@@ -181,10 +181,12 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                         const uint32_t cand = (0xFu << r0) & valid & ~S;
                         const uint32_t spreadLR = SL | (SL << 1) | (SL >> 1) | R | (R << 1) | (R >> 1);
                         if (!__any_sync(kFull, cand & (spreadLR | (S << 1) | (S >> 1)))) continue;
-                        uint32_t nn = 0, ee = 0;
+                        // from nn = 0 upwards; done when the left columns' new significance
+                        // makes no further sample eligible (the right column, the row below
+                        // and the in-column chain do not change between iterations)
+                        uint32_t nn = 0, ee = 0, L = SL;
 #pragma unroll 1
                         for (int it = 0; it < 34; ++it) {
-                            const uint32_t L = SL | shUp(nn, lane);
                             const uint32_t side = L | (L << 1) | (L >> 1) | R | (R << 1) | (R >> 1) | (S >> 1);
                             uint32_t n2 = 0, e2 = 0;
 #pragma unroll
@@ -196,10 +198,11 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                                     n2 |= Bp & b;
                                 }
                             }
-                            const bool changed = n2 != nn;
                             nn = n2;
                             ee = e2;
-                            if (!__any_sync(kFull, changed)) break;
+                            const uint32_t Ln = SL | shUp(nn, lane);
+                            if (!__any_sync(kFull, cand & ~ee & (Ln | (Ln << 1) | (Ln >> 1)))) break;
+                            L = Ln;
                         }
                         E |= ee;
                         NEW |= nn;
@@ -408,7 +411,7 @@ __device__ __forceinline__ uint32_t orderBucket(uint32_t s) {
 // most one per warp for half the launch's warps: the longest serial chains, which would
 // otherwise run beside 31 divergent neighbours. A power of two, so that they are exactly
 // the first blocks of the order.
-constexpr uint32_t kSoloDecisions = 8192;
+constexpr uint32_t kSoloDecisions = 16384;
 
 __global__ void __launch_bounds__(1024) t1OrderKernel(T1Launch P, uint32_t maxSolo) {
     __shared__ uint32_t hist[ORDER_BUCKETS];
@@ -543,7 +546,10 @@ __device__ uint32_t truncLen(uint4 s, const uint8_t* buf, uint32_t len, uint32_t
     return len;
 }
 
-__global__ void __launch_bounds__(MQ_THREADS) t1MqKernel(T1Launch P) {
+// MINB: CTAs per SM the registers must allow. A launch of a frame or two has fewer lanes
+// than the GPU holds and runs uncapped; wide batched launches run at 12 CTAs per SM.
+template <int MINB>
+__global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
     __shared__ uint32_t s_next[4 * 47];
     __shared__ uint32_t s_init[4];
     __shared__ uint32_t s_ctx[19 * MQ_THREADS];
@@ -726,7 +732,8 @@ void t1Encode(const T1Launch& L, cudaStream_t st, cudaEvent_t* marks) {
     const uint32_t mqBlocks = min(divUp(L.n, MQ_THREADS), (uint32_t)sms * 16u);
     t1OrderKernel<<<1, 1024, 0, st>>>(L, mqBlocks * (MQ_THREADS / 32) / 2);
     if (marks) GB_CHECK(cudaEventRecord(marks[1], st));
-    t1MqKernel<<<mqBlocks, MQ_THREADS, 0, st>>>(L);
+    if (mqBlocks <= (uint32_t)sms * 4u) t1MqKernel<1><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
+    else t1MqKernel<12><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
     GB_CHECK(cudaGetLastError());
 }
 
