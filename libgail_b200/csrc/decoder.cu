@@ -1,10 +1,10 @@
 // Decoder on sm_100a: Tier-1 decoding with dequantisation, inverse 9/7 wavelet, inverse
 // ICT and 12-bit packing.
 //
-// Tier-1 (decodeKernel): one lane per code-block. The MQ decoder is serial per block, so
-// blocks are ordered longest codeword first (orderKernel); a warp takes either one of the
-// heaviest blocks alone (its lane 0 decodes it, free of divergent neighbours) or the next
-// 32 lighter ones, which have similar lengths. A block's state is kept as row masks in
+// Tier-1 (decodeKernel): one code-block per warp at a time, decoded by its lane 0 (the
+// decode's control flow depends on every decoded bit, so lanes of one warp decoding
+// different blocks would only run one after another); up to 32 such warps per SM pull
+// blocks from a device queue ordered longest codeword first (orderKernel). A block's state is kept as row masks in
 // shared memory (significance and sign for rows -1..32, coded-this-plane and refined),
 // the scan visits only columns that have something to code (bit scans over candidate
 // masks), and the decoded words (sign, twice the magnitude plus the mid-point of the
@@ -37,7 +37,12 @@ namespace gb {
 
 namespace {
 
-constexpr int DEC_THREADS = 64;
+// One code-block per warp: its lane 0 decodes it (the decode of a block is a serial chain
+// whose control flow depends on every decoded bit, so lanes of one warp decoding different
+// blocks would run one after another anyway); up to 32 such warps per SM keep the
+// schedulers busy. DEC_STRIDE: the state arrays hold one block.
+constexpr int DEC_THREADS = 32;
+constexpr int DEC_STRIDE = 1;
 constexpr int ORDER_BUCKETS = 128;
 
 __constant__ uint8_t c_zc[4 * 45];
@@ -54,14 +59,8 @@ struct DecArgs {
     uint32_t* planes;   // float planes seen as words while decoding
     uint32_t W;
     uint32_t* perm;
-    uint32_t* ctl;      // [0] light queue head, [1] status, [2] wanted blocks, [3] heavy blocks,
-                        // [4] heavy queue head
+    uint32_t* ctl;      // [0] queue head, [1] status, [2] wanted blocks
 };
-
-// Blocks with at least this many codeword bytes are decoded one per warp: the longest
-// serial chains of the frame, which would otherwise run with 31 divergent neighbours.
-// A power of two, so that they sort ahead of every lighter block.
-constexpr uint32_t kHeavyBytes = 128;
 
 __device__ __forceinline__ uint32_t lenBucket(uint32_t len) {
     if (len < 4) return ORDER_BUCKETS - 1;
@@ -75,14 +74,10 @@ __global__ void __launch_bounds__(1024) orderKernel(DecArgs a) {
     for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
     if (threadIdx.x == 0) total = 0;
     __syncthreads();
-    __shared__ uint32_t heavy;
-    if (threadIdx.x == 0) heavy = 0;
-    __syncthreads();
     for (uint32_t i = threadIdx.x; i < a.n; i += blockDim.x)
         if (a.blocks[i].wanted) {
             atomicAdd(&hist[lenBucket(a.codes[i].len)], 1u);
             atomicAdd(&total, 1u);
-            if (a.codes[i].len >= kHeavyBytes) atomicAdd(&heavy, 1u);
         }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -93,7 +88,6 @@ __global__ void __launch_bounds__(1024) orderKernel(DecArgs a) {
             run += c;
         }
         a.ctl[2] = total;
-        a.ctl[3] = heavy;
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < a.n; i += blockDim.x)
@@ -147,7 +141,7 @@ struct MqDecoder {
     }
     // One decision in context cx (state word: table entry | mps << 16).
     __device__ __forceinline__ uint32_t decode(uint32_t* ctx, int cx, const uint32_t* tab) {
-        uint32_t t = ctx[cx * DEC_THREADS];
+        uint32_t t = ctx[cx * DEC_STRIDE];
         const uint32_t qe = t & 0xFFFFu, mps = (t >> 16) & 1u;
         A -= qe;
         bool lps;
@@ -161,7 +155,7 @@ struct MqDecoder {
         }
         const uint32_t nidx = lps ? (t >> 24) & 63u : (t >> 18) & 63u;
         const uint32_t nm = mps ^ (lps ? (t >> 17) & 1u : 0u);
-        ctx[cx * DEC_THREADS] = tab[nidx] | (nm << 16);
+        ctx[cx * DEC_STRIDE] = tab[nidx] | (nm << 16);
         renorm();
         return lps ? mps ^ 1u : mps;
     }
@@ -173,7 +167,7 @@ __device__ __forceinline__ int chiAt(uint32_t s, uint32_t g, int x) {
 }
 
 struct BlockState {
-    uint32_t* sig;  // rows -1..32 at index (y + 1) * DEC_THREADS
+    uint32_t* sig;  // rows -1..32 at index (y + 1) * DEC_STRIDE
     uint32_t* sgn;
     uint32_t* vis;  // rows 0..31
     uint32_t* ref;
@@ -185,8 +179,8 @@ struct BlockState {
     uint32_t* ctx;
     MqDecoder mq;
 
-    __device__ __forceinline__ uint32_t S(int y) const { return sig[(y + 1) * DEC_THREADS]; }
-    __device__ __forceinline__ uint32_t G(int y) const { return sgn[(y + 1) * DEC_THREADS]; }
+    __device__ __forceinline__ uint32_t S(int y) const { return sig[(y + 1) * DEC_STRIDE]; }
+    __device__ __forceinline__ uint32_t G(int y) const { return sgn[(y + 1) * DEC_STRIDE]; }
 
     __device__ __forceinline__ uint32_t zcAt(int x, int y) const {
         const uint32_t U = S(y - 1), M = S(y), D = S(y + 1);
@@ -207,52 +201,35 @@ struct BlockState {
         const int vc = max(-1, min(1, chiAt(U, G(y - 1), x) + chiAt(D, G(y + 1), x)));
         const uint32_t t = sc[(hc + 1) * 3 + (vc + 1)];
         const uint32_t neg = mq.decode(ctx, t & 31u, tab) ^ (t >> 5);
-        sig[(y + 1) * DEC_THREADS] |= 1u << x;
-        if (neg) sgn[(y + 1) * DEC_THREADS] |= 1u << x;
+        sig[(y + 1) * DEC_STRIDE] |= 1u << x;
+        if (neg) sgn[(y + 1) * DEC_STRIDE] |= 1u << x;
         out[(size_t)y * W + x] = (neg << 31) | (3u << p);
     }
 };
 
 __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
-    __shared__ uint32_t s_sig[34 * DEC_THREADS], s_sgn[34 * DEC_THREADS], s_vis[32 * DEC_THREADS], s_ref[32 * DEC_THREADS];
-    __shared__ uint32_t s_ctx[19 * DEC_THREADS];
+    __shared__ uint32_t s_sig[34 * DEC_STRIDE], s_sgn[34 * DEC_STRIDE], s_vis[32 * DEC_STRIDE], s_ref[32 * DEC_STRIDE];
+    __shared__ uint32_t s_ctx[19 * DEC_STRIDE];
     __shared__ uint32_t s_tab[48];
     __shared__ uint8_t s_zc[4 * 45], s_sc[16];
     for (int i = threadIdx.x; i < 47; i += blockDim.x) s_tab[i] = c_mq[i];
     for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) s_zc[i] = c_zc[i];
     if (threadIdx.x < 9) s_sc[threadIdx.x] = c_sc[threadIdx.x];
     __syncthreads();
-    const int tid = threadIdx.x;
+    if (threadIdx.x != 0) return;  // lane 0 decodes; the tables above were loaded by the whole warp
     BlockState b;
-    b.sig = s_sig + tid;
-    b.sgn = s_sgn + tid;
-    b.vis = s_vis + tid;
-    b.ref = s_ref + tid;
-    b.ctx = s_ctx + tid;
+    b.sig = s_sig;
+    b.sgn = s_sgn;
+    b.vis = s_vis;
+    b.ref = s_ref;
+    b.ctx = s_ctx;
     b.sc = s_sc;
     b.tab = s_tab;
     b.W = a.W;
-    const uint32_t count = a.ctl[2], heavy = a.ctl[3];
-    const int lane = tid & 31;
+    const uint32_t count = a.ctl[2];
     for (;;) {
-        // a warp claims one heavy block (its lane 0 decodes it) or 32 light ones, which
-        // sort next to each other and so have similar lengths
-        uint32_t base = 0, cnt = 0;
-        if (lane == 0) {
-            const uint32_t h = heavy ? atomicAdd(a.ctl + 4, 1u) : heavy;
-            if (h < heavy) {
-                base = h;
-                cnt = 1;
-            } else {
-                base = heavy + atomicAdd(a.ctl, 32u);
-                cnt = 32;
-            }
-        }
-        base = __shfl_sync(kFull, base, 0);
-        cnt = __shfl_sync(kFull, cnt, 0);
-        if (base >= count) break;
-        const uint32_t q = base + (uint32_t)lane;
-        if ((uint32_t)lane >= cnt || q >= count) continue;
+        const uint32_t q = atomicAdd(a.ctl, 1u);  // longest codewords first
+        if (q >= count) break;
         const uint32_t j = a.perm[q];
         const DecBlock blk = a.blocks[j];
         const GbCblkCode code = a.codes[j];
@@ -264,17 +241,17 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
             b.out = out;
             b.zc = s_zc + 45 * blk.orient;
             for (int i = 0; i < 34; ++i) {
-                b.sig[i * DEC_THREADS] = 0;
-                b.sgn[i * DEC_THREADS] = 0;
+                b.sig[i * DEC_STRIDE] = 0;
+                b.sgn[i * DEC_STRIDE] = 0;
             }
             for (int i = 0; i < 32; ++i) {
-                b.vis[i * DEC_THREADS] = 0;
-                b.ref[i * DEC_THREADS] = 0;
+                b.vis[i * DEC_STRIDE] = 0;
+                b.ref[i * DEC_STRIDE] = 0;
             }
-            for (int c = 0; c < 19; ++c) b.ctx[c * DEC_THREADS] = s_tab[0];
+            for (int c = 0; c < 19; ++c) b.ctx[c * DEC_STRIDE] = s_tab[0];
             b.ctx[0] = s_tab[4];
-            b.ctx[17 * DEC_THREADS] = s_tab[3];
-            b.ctx[18 * DEC_THREADS] = s_tab[46];
+            b.ctx[17 * DEC_STRIDE] = s_tab[3];
+            b.ctx[18 * DEC_STRIDE] = s_tab[46];
             b.mq.init(a.bytes + code.offset, code.len);
             const uint32_t wmask = w >= 32 ? 0xFFFFFFFFu : (1u << w) - 1u;
             int done = 0;
@@ -297,7 +274,7 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                                     const int y = y0 + k;
                                     if (bt(b.S(y), x) || !b.anyNbr(x, y)) continue;
                                     const uint32_t bit = b.mq.decode(b.ctx, b.zcAt(x, y), b.tab);
-                                    b.vis[y * DEC_THREADS] |= 1u << x;
+                                    b.vis[y * DEC_STRIDE] |= 1u << x;
                                     if (bit) {
                                         b.becomeSig(x, y, p);
                                         cm |= (2u << x) & wmask;  // the next column may now be eligible
@@ -306,23 +283,23 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                             }
                         } else if (type == 1) {
                             uint32_t cm = 0;
-                            for (int k = 0; k < n; ++k) cm |= b.S(y0 + k) & ~b.vis[(y0 + k) * DEC_THREADS];
+                            for (int k = 0; k < n; ++k) cm |= b.S(y0 + k) & ~b.vis[(y0 + k) * DEC_STRIDE];
                             while (cm) {
                                 const int x = __ffs(cm) - 1;
                                 cm &= cm - 1;
                                 for (int k = 0; k < n; ++k) {
                                     const int y = y0 + k;
-                                    if (!bt(b.S(y), x) || bt(b.vis[y * DEC_THREADS], x)) continue;
-                                    const int cx = bt(b.ref[y * DEC_THREADS], x) ? 16 : (b.anyNbr(x, y) ? 15 : 14);
+                                    if (!bt(b.S(y), x) || bt(b.vis[y * DEC_STRIDE], x)) continue;
+                                    const int cx = bt(b.ref[y * DEC_STRIDE], x) ? 16 : (b.anyNbr(x, y) ? 15 : 14);
                                     const uint32_t bit = b.mq.decode(b.ctx, cx, b.tab);
                                     uint32_t& word = out[(size_t)y * a.W + x];
                                     word = bit ? word + (1u << p) : word - (1u << p);
-                                    b.ref[y * DEC_THREADS] |= 1u << x;
+                                    b.ref[y * DEC_STRIDE] |= 1u << x;
                                 }
                             }
                         } else {
                             uint32_t cm = 0;
-                            for (int k = 0; k < n; ++k) cm |= ~b.S(y0 + k) & ~b.vis[(y0 + k) * DEC_THREADS] & wmask;
+                            for (int k = 0; k < n; ++k) cm |= ~b.S(y0 + k) & ~b.vis[(y0 + k) * DEC_STRIDE] & wmask;
                             while (cm) {
                                 const int x = __ffs(cm) - 1;
                                 cm &= cm - 1;
@@ -331,7 +308,7 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                                     bool quiet = true;
                                     for (int k = 0; k < 4 && quiet; ++k) {
                                         const int y = y0 + k;
-                                        if (bt(b.S(y) | b.vis[y * DEC_THREADS], x) || b.anyNbr(x, y)) quiet = false;
+                                        if (bt(b.S(y) | b.vis[y * DEC_STRIDE], x) || b.anyNbr(x, y)) quiet = false;
                                     }
                                     if (quiet) {
                                         if (!b.mq.decode(b.ctx, 17, b.tab)) continue;
@@ -343,14 +320,14 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                                 }
                                 for (int k = r; k < n; ++k) {
                                     const int y = y0 + k;
-                                    if (bt(b.S(y) | b.vis[y * DEC_THREADS], x)) continue;
+                                    if (bt(b.S(y) | b.vis[y * DEC_STRIDE], x)) continue;
                                     if (b.mq.decode(b.ctx, b.zcAt(x, y), b.tab)) b.becomeSig(x, y, p);
                                 }
                             }
                         }
                     }
                 }
-                for (int i = 0; i < 32; ++i) b.vis[i * DEC_THREADS] = 0;
+                for (int i = 0; i < 32; ++i) b.vis[i * DEC_STRIDE] = 0;
             }
             // dequantise in place, the significant samples only (every other word is 0,
             // which is 0.0f): word * step / 2, sign from bit 31
@@ -647,7 +624,7 @@ void DecoderSlot::enqueue(const Layout& frame, const uint8_t* data, size_t size,
     orderKernel<<<1, 1024, 0, st>>>(da);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_);
-    decodeKernel<<<std::min<uint32_t>(divUp((uint32_t)n, DEC_THREADS), (uint32_t)sms * 16), DEC_THREADS, 0, st>>>(da);
+    decodeKernel<<<std::min<uint32_t>((uint32_t)n, (uint32_t)sms * 32), DEC_THREADS, 0, st>>>(da);
     GB_CHECK(cudaGetLastError());
     GB_CHECK(cudaEventRecord(ev_[1], st));
     // inverse wavelet, levels top down; the last one writes the picture (the planes are only
