@@ -72,7 +72,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch", type=int, default=16, help="most frames per Tier-1 launch (served path)")
+    ap.add_argument("--batch", type=int, default=None,
+                    help="most frames per Tier-1 launch (served path; default: the tuning file's, else 16)")
+    ap.add_argument("--tuning", default=os.path.join(ROOT, "libgail_b200", "tuning_b200.json"),
+                    help="autotuner file applied when it was made on this GPU ('' for the defaults)")
     ap.add_argument("--slots", type=int, default=3, help="slot threads of the plain path")
     return ap.parse_args()
 
@@ -258,6 +261,16 @@ def run_ours(args):
     pinned = [torch.from_numpy(f.view(np.int16)).pin_memory() for f in frames]
     dframes = [p.to(cuda) for p in pinned]
     torch.cuda.synchronize()
+    # the autotuner's choices for this GPU (launch knobs per profile, batch policy)
+    from libgail_b200 import autotune as AT
+    policy = dict(AT.POLICY_DEFAULT)
+    tuned = False
+    if args.tuning and os.path.exists(args.tuning):
+        policy = AT.apply(args.tuning, device_name=torch.cuda.get_device_name(local))
+        tuned = json.load(open(args.tuning)).get("device") == torch.cuda.get_device_name(local)
+    if args.batch is not None:
+        policy["maxBatch"] = args.batch
+    args.batch = policy["maxBatch"]
     plugin = P.Plugin()
     dev = plugin.device(local)
     lay = P.LayoutHolder(W4K, H4K, 1)
@@ -333,6 +346,7 @@ def run_ours(args):
     _, frame_bytes = probe.add_encoder(lay, fmt, col)
     probe.close()
     eng = Engine(local, 48 * frame_bytes + 1, max_batch=args.batch)
+    eng.set_policy(policy["maxBatch"], policy["minBatchPct"], policy["maxWaitMs"])
     cid, frame_bytes = eng.add_encoder(lay, fmt, col)
     eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
     served_cs = []
@@ -420,7 +434,7 @@ def run_ours(args):
     dec.close()
     decode_fps = len(kept_cs) * world / dec_s
 
-    mixed = run_mixed(args, local, dev, lay, fmt, col, pinned, kept_cs, frame_bytes, workers)
+    mixed = run_mixed(args, local, dev, lay, fmt, col, pinned, kept_cs, frame_bytes, workers, policy)
 
     out = None
     if rank == 0:
@@ -475,6 +489,8 @@ def run_ours(args):
             "data": f"synthetic (seeded generator, {len(dframes)} frames)",
             "config": {"workload": WORKLOAD, "frames_per_step": len(dframes), "path": "served (batched engine)",
                        "max_batch": args.batch, "codestream_workers": workers, "parallelism": f"replicas x{world}",
+                       "tuning": {"file": os.path.relpath(args.tuning, ROOT) if tuned else None,
+                                  "profiles": {"2k": AT.get_tuning(0), "4k": AT.get_tuning(1)}, "policy": policy},
                        "l2": f"inputs larger than L2 ({len(dframes)} frames, {len(dframes) * nbytes / 1e9:.2f} GB)"},
             "served": {"fps": value, "latency_ms": {"p50": pct(served_lat, 50), "p99": pct(served_lat, 99)},
                        "offered_fps": rate, "batches": st_eng["batches"],
@@ -512,7 +528,7 @@ def run_ours(args):
         print(json.dumps(out))
 
 
-def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_bytes, workers, n=240,
+def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_bytes, workers, policy, n=240,
               loads=(100.0, 200.0, 300.0), seed=11):
     """Serving a mix as it arrives: Poisson requests, 70 % encode / 30 % decode, 60 % 4K
     (the benchmark's Y'CbCr frames and their codestreams) / 40 % 2K X'Y'Z', one engine with
@@ -528,6 +544,7 @@ def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_
     fmt2k, col2k = P.rgb48_format(W2, H2), P.color_passthrough()
     frames2k = [synth.xyz12_to_rgb48(synth.xyz12_planes(W2, H2, seed=seed + i)) for i in range(8)]
     eng = Engine(local, 64 * frame_bytes, max_batch=args.batch)
+    eng.set_policy(policy["maxBatch"], policy["minBatchPct"], policy["maxWaitMs"])
     try:
         e4, _ = eng.add_encoder(lay4k, fmt4k, col4k)
         e2, _ = eng.add_encoder(lay2k, fmt2k, col2k)

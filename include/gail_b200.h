@@ -80,6 +80,21 @@ GB_API int gb_make_layout(int width, int height, int fourk, double baseStep, GbS
  * ColorConverter's lut()/params() (src/core/color.h:105-108). Any pointer may be NULL. */
 GB_API int gb_color_tables(const GailCudaColor* color, float* eotf65536, float* matrix9, float* thresholds4096);
 
+/* Launch tuning per frame profile (0 = 2K, 1 = 4K), read by every launch of that profile
+ * made after the call (plain encoders and decoders, engine batches). No counterpart in the
+ * reference, whose launch shapes are fixed; libgail_b200/autotune.py measures candidates
+ * on the GPU and keeps the fastest. gb_set_tuning(profile, NULL) restores the defaults.
+ *   soloDecisions  MQ coding: blocks with at least this many decisions are coded alone in
+ *                  a warp first (rounded down to a power of two; default 16384)
+ *   cmCtasPerSm, mqCtasPerSm, decCtasPerSm  grid caps in CTAs per SM of context modelling,
+ *                  MQ coding and Tier-1 decoding (defaults 16, 16, 32; 1..64) */
+typedef struct GbTuning {
+    uint32_t soloDecisions;
+    int32_t cmCtasPerSm, mqCtasPerSm, decCtasPerSm;
+} GbTuning;
+GB_API int gb_set_tuning(int profile, const GbTuning* t);
+GB_API int gb_get_tuning(int profile, GbTuning* t);
+
 /* Frames already in device memory (a serving layer that keeps them resident). The
  * encoder is one made by the plugin table's encoder_create; these replace the upload half
  * of encoder_encode (the reference's CudaSlot::encodeView, src/cuda/cuda_backend.cu:870-977).
@@ -144,6 +159,10 @@ GB_API int gb_engine_wait(GbEngine* e, int timeoutMs, int64_t* id, GailCudaTier1
                           int* frameStatus);
 GB_API int gb_engine_release(GbEngine* e, int64_t id);
 GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5);
+/* Batch policy: at most maxBatch frames per Tier-1 launch; while another batch keeps the GPU
+ * busy, a batch waits to gather minBatchPct % of maxBatch ready frames, but not past
+ * maxWaitMs after its oldest frame (defaults: the create call's maxBatch, 25 %, 2 ms). */
+GB_API int gb_engine_set_policy(GbEngine* e, int maxBatch, int minBatchPct, double maxWaitMs);
 GB_API int gb_engine_set_codestream(GbEngine* e, double fps, double maxMbps, double compMbps, const char* label,
                                     const char* tag, int threads, int check);
 GB_API int gb_engine_codestream(GbEngine* e, int64_t id, const uint8_t** data, uint64_t* size, int* dciOk);

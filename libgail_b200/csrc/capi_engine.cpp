@@ -98,6 +98,13 @@ GB_API int gb_engine_picture(GbEngine* e, int64_t id, const uint16_t** pix, int*
     });
 }
 
+GB_API int gb_engine_set_policy(GbEngine* e, int maxBatch, int minBatchPct, double maxWaitMs) {
+    return gbGuard([&] {
+        if (!e) throw std::logic_error("null argument");
+        e->e->setPolicy(maxBatch, minBatchPct, maxWaitMs);
+    });
+}
+
 GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5) {
     return gbGuard([&] {
         if (!e || !out5) throw std::logic_error("null argument");

@@ -7,6 +7,7 @@
 #include "color.h"
 #include "gail_b200.h"
 #include "layout.h"
+#include "tuning.h"
 
 using namespace gb;
 
@@ -29,6 +30,31 @@ GB_API int gb_color_tables(const GailCudaColor* color, float* eotf65536, float* 
         if (eotf65536) std::memcpy(eotf65536, t.eotf.data(), 65536 * 4);
         if (matrix9) std::memcpy(matrix9, t.m, 36);
         if (thresholds4096) std::memcpy(thresholds4096, t.thr.data(), 4096 * 4);
+    });
+}
+
+GB_API int gb_set_tuning(int profile, const GbTuning* t) {
+    return gbGuard([&] {
+        if (!t) {
+            if (profile != 0 && profile != 1) throw std::logic_error("tuning profile must be 0 (2K) or 1 (4K)");
+            resetTuning(profile);
+            return;
+        }
+        Tuning v;
+        v.soloDecisions = t->soloDecisions;
+        v.cmCtasPerSm = t->cmCtasPerSm;
+        v.mqCtasPerSm = t->mqCtasPerSm;
+        v.decCtasPerSm = t->decCtasPerSm;
+        setTuning(profile, v);
+    });
+}
+
+GB_API int gb_get_tuning(int profile, GbTuning* t) {
+    return gbGuard([&] {
+        if (!t) throw std::logic_error("null argument");
+        if (profile != 0 && profile != 1) throw std::logic_error("tuning profile must be 0 (2K) or 1 (4K)");
+        const Tuning v = tuningFor(profile);
+        *t = {v.soloDecisions, v.cmCtasPerSm, v.mqCtasPerSm, v.decCtasPerSm};
     });
 }
 

@@ -32,6 +32,7 @@
 #include "common.cuh"
 #include "decoder.h"
 #include "t1_tables.h"
+#include "tuning.h"
 
 namespace gb {
 
@@ -624,7 +625,8 @@ void DecoderSlot::enqueue(const Layout& frame, const uint8_t* data, size_t size,
     orderKernel<<<1, 1024, 0, st>>>(da);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_);
-    decodeKernel<<<std::min<uint32_t>((uint32_t)n, (uint32_t)sms * 32), DEC_THREADS, 0, st>>>(da);
+    decodeKernel<<<std::min<uint32_t>((uint32_t)n, (uint32_t)(sms * tuningFor(L_.profile).decCtasPerSm)), DEC_THREADS, 0,
+                   st>>>(da);
     GB_CHECK(cudaGetLastError());
     GB_CHECK(cudaEventRecord(ev_[1], st));
     // inverse wavelet, levels top down; the last one writes the picture (the planes are only

@@ -9,6 +9,7 @@
 
 #include "common.cuh"
 #include "frontend.cuh"
+#include "tuning.h"
 
 namespace gb {
 
@@ -242,6 +243,10 @@ void EncoderSlot::enqueueStages(const void* dFrame, bool taps, bool full) {
     if (mark) GB_CHECK(cudaEventRecord(mark[1], st));
     const uint64_t n = z_.n;
     T1Launch t{dJobs_, (uint32_t)n, dInfo_, dEnd_, dLen_, dDist_, dSnaps_, dPerm_, dCtl_, dSlope_};
+    const Tuning tu = tuningFor(L_.profile);
+    t.soloDecisions = tu.soloDecisions;
+    t.cmCtasPerSm = (uint16_t)tu.cmCtasPerSm;
+    t.mqCtasPerSm = (uint16_t)tu.mqCtasPerSm;
     t1Encode(t, st, mark ? mark + 2 : nullptr);
     GB_CHECK(cudaEventRecord(ev_[3], st));
     if (mark) GB_CHECK(cudaEventRecord(mark[4], st));

@@ -11,6 +11,7 @@
 #include "common.cuh"
 #include "compact.cuh"
 #include "frontend.cuh"
+#include "tuning.h"
 
 namespace gb {
 
@@ -323,6 +324,15 @@ void EncodeEngine::release(int64_t id) {
     cvWork_.notify_one();
 }
 
+void EncodeEngine::setPolicy(int maxBatch, int minBatchPct, double maxWaitMs) {
+    if (maxBatch < 1 || maxBatch > 1024 || minBatchPct < 0 || minBatchPct > 100 || !(maxWaitMs >= 0) || maxWaitMs > 1000)
+        throw std::logic_error("batch policy out of range");
+    std::lock_guard<std::mutex> lock(m_);
+    maxBatch_ = maxBatch;
+    minBatchPct_ = minBatchPct;
+    maxWaitMs_ = maxWaitMs;
+}
+
 void EncodeEngine::setCodestream(const CodestreamConfig& c) {
     if (c.threads < 1 || c.threads > 256) throw std::logic_error("codestream workers out of range");
     if (c.tag.size() > kMaxDeviceTagBytes) throw std::logic_error("device tag too long");
@@ -564,8 +574,8 @@ bool EncodeEngine::launchBatch(Batch& b) {
             sel.push_back(r);
         }
         // while the other batch keeps the GPU busy, let small batches grow a little
-        if (sel.empty() || (otherBusy && (int)sel.size() < std::max(1, maxBatch_ / 4) &&
-                            msBetween(front_q_.front()->t0, Clock::now()) < 2.0 && sel.size() < front_q_.size()))
+        if (sel.empty() || (otherBusy && (int)sel.size() < std::max(1, maxBatch_ * minBatchPct_ / 100) &&
+                            msBetween(front_q_.front()->t0, Clock::now()) < maxWaitMs_ && sel.size() < front_q_.size()))
             return false;
         front_q_.erase(front_q_.begin(), front_q_.begin() + (long)sel.size());
     }
@@ -603,6 +613,12 @@ bool EncodeEngine::launchBatch(Batch& b) {
     }
     GB_CHECK(cudaMemsetAsync(b.ctl, 0, 64, b.st));
     T1Launch L{b.dJobs, (uint32_t)total, b.info, b.end, b.len, b.dist, b.snaps, b.perm, b.ctl, dSlope_};
+    bool any4k = false;  // a batch with a 4K frame is launched with the 4K tuning
+    for (Request* r : sel) any4k = any4k || classes_[r->cls]->L.profile == 1;
+    const Tuning tu = tuningFor(any4k ? 1 : 0);
+    L.soloDecisions = tu.soloDecisions;
+    L.cmCtasPerSm = (uint16_t)tu.cmCtasPerSm;
+    L.mqCtasPerSm = (uint16_t)tu.mqCtasPerSm;
     t1Encode(L, b.st);
     for (Request* r : sel) {
         Slot* s = r->slot;

@@ -41,6 +41,10 @@ public:
     // maxBatch: most frames per Tier-1 launch; hbmBudget: device bytes the engine's frame
     // slots may take (0: 90 % of what is free when the engine starts).
     EncodeEngine(int device, uint64_t hbmBudget, int maxBatch);
+    // Batch policy: at most maxBatch frames per Tier-1 launch; while another batch keeps the
+    // GPU busy, a batch waits to gather minBatchPct % of maxBatch ready frames, but not longer
+    // than maxWaitMs after its oldest frame arrived (defaults 25 % and 2 ms).
+    void setPolicy(int maxBatch, int minBatchPct, double maxWaitMs);
     ~EncodeEngine();
     EncodeEngine(const EncodeEngine&) = delete;
     EncodeEngine& operator=(const EncodeEngine&) = delete;
@@ -107,6 +111,8 @@ private:
     uint64_t budget_ = 0, used_ = 0;  // used_ under budgetM_
     std::mutex budgetM_;
     int maxBatch_;
+    int minBatchPct_ = 25;
+    double maxWaitMs_ = 2.0;
     cudaStream_t front_ = nullptr;
     std::vector<std::unique_ptr<Class>> classes_;
     std::vector<std::unique_ptr<Slot>> slots_;

@@ -35,6 +35,7 @@
 #include "t1_encode.cuh"
 #include "capi_util.h"
 #include "t1_tables.h"
+#include "tuning.h"
 
 namespace gb {
 
@@ -407,12 +408,10 @@ __device__ __forceinline__ uint32_t orderBucket(uint32_t s) {
     return ORDER_BUCKETS - 1 - cls;
 }
 
-// Blocks with at least this many decisions are MQ-coded alone in a warp (its lane 0), at
-// most one per warp for half the launch's warps: the longest serial chains, which would
+// Blocks with at least P.soloDecisions decisions are MQ-coded alone in a warp (its lane 0),
+// at most one per warp for half the launch's warps: the longest serial chains, which would
 // otherwise run beside 31 divergent neighbours. A power of two, so that they are exactly
 // the first blocks of the order.
-constexpr uint32_t kSoloDecisions = 16384;
-
 __global__ void __launch_bounds__(1024) t1OrderKernel(T1Launch P, uint32_t maxSolo) {
     __shared__ uint32_t hist[ORDER_BUCKETS];
     __shared__ uint32_t solo;
@@ -422,7 +421,7 @@ __global__ void __launch_bounds__(1024) t1OrderKernel(T1Launch P, uint32_t maxSo
     for (uint32_t i = threadIdx.x; i < P.n; i += blockDim.x) {
         const uint32_t d = P.info[4 * (size_t)i + 2];
         atomicAdd(&hist[orderBucket(d)], 1u);
-        if (d >= kSoloDecisions) atomicAdd(&solo, 1u);
+        if (d >= P.soloDecisions) atomicAdd(&solo, 1u);
     }
     __syncthreads();
     if (threadIdx.x == 0) P.ctl[3] = min(solo, maxSolo);
@@ -721,15 +720,20 @@ void t1Init() {
     GB_CHECK(cudaMemcpyToSymbol(c_mq, mq, sizeof mq));
 }
 
-void t1Encode(const T1Launch& L, cudaStream_t st, cudaEvent_t* marks) {
-    if (L.n == 0) return;
+void t1Encode(const T1Launch& launch, cudaStream_t st, cudaEvent_t* marks) {
+    if (launch.n == 0) return;
+    T1Launch L = launch;
+    const Tuning def = defaultTuning();
+    if (!L.soloDecisions) L.soloDecisions = def.soloDecisions;
+    if (!L.cmCtasPerSm) L.cmCtasPerSm = (uint16_t)def.cmCtasPerSm;
+    if (!L.mqCtasPerSm) L.mqCtasPerSm = (uint16_t)def.mqCtasPerSm;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const uint32_t cmBlocks = min(divUp(L.n, CM_WARPS), (uint32_t)sms * 16u);
+    const uint32_t cmBlocks = min(divUp(L.n, CM_WARPS), (uint32_t)sms * L.cmCtasPerSm);
     t1CmKernel<<<cmBlocks, CM_THREADS, 0, st>>>(L);
     if (marks) GB_CHECK(cudaEventRecord(marks[0], st));
-    const uint32_t mqBlocks = min(divUp(L.n, MQ_THREADS), (uint32_t)sms * 16u);
+    const uint32_t mqBlocks = min(divUp(L.n, MQ_THREADS), (uint32_t)sms * L.mqCtasPerSm);
     t1OrderKernel<<<1, 1024, 0, st>>>(L, mqBlocks * (MQ_THREADS / 32) / 2);
     if (marks) GB_CHECK(cudaEventRecord(marks[1], st));
     if (mqBlocks <= (uint32_t)sms * 4u) t1MqKernel<1><<<mqBlocks, MQ_THREADS, 0, st>>>(L);

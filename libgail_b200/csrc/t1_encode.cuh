@@ -46,6 +46,10 @@ struct T1Launch {
     uint32_t* perm;      // n: jobs in MQ order (most decisions first)
     uint32_t* ctl;       // [0] MQ queue head, [1] status bits, [2] total decisions
     const float* slope;  // early-termination thresholds, indexed by T1Job::slope (NULL: every pass)
+    // launch tuning (0: the defaults): blocks of at least soloDecisions decisions are
+    // MQ-coded alone in a warp (a power of two); grids of at most so many CTAs per SM
+    uint32_t soloDecisions;
+    uint16_t cmCtasPerSm, mqCtasPerSm;
 };
 
 // Enqueues the whole Tier-1 stage on st: context modelling, ordering, MQ coding.

@@ -1,0 +1,23 @@
+// Launch tuning per frame profile (0 = 2K, 1 = 4K): the knobs whose best value depends on the
+// workload and the GPU, set by the autotuner (libgail_b200/autotune.py) through
+// gb_set_tuning and read by every launch of that profile.
+#pragma once
+#include <cstdint>
+
+namespace gb {
+
+struct Tuning {
+    uint32_t soloDecisions = 16384;  // MQ: blocks with at least this many decisions coded alone in a warp
+    int cmCtasPerSm = 16;            // context modelling grid cap
+    int mqCtasPerSm = 16;            // MQ grid cap
+    int decCtasPerSm = 32;           // Tier-1 decode grid cap
+};
+
+Tuning defaultTuning();
+Tuning tuningFor(int profile);
+// Validates and stores (soloDecisions rounded down to a power of two, caps clamped to the
+// hardware's resident limits); throws std::logic_error on a value out of range.
+void setTuning(int profile, const Tuning& t);
+void resetTuning(int profile);
+
+}  // namespace gb

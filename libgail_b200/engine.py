@@ -26,6 +26,7 @@ def _bind():
                                            C.c_int, C.c_int]
     L.gb_engine_codestream.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_uint8)),
                                        C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
+    L.gb_engine_set_policy.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double]
     L.gb_engine_add_decoder.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]
     L.gb_engine_submit_decode.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_int64)]
     L.gb_engine_picture.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_uint16)), C.POINTER(C.c_int),
@@ -74,6 +75,10 @@ class Engine:
         if rid.value < 0:
             return -1, None, 0.0, 0
         return rid.value, (Tier1Frame(t) if copy else t), lat.value, st.value
+
+    def set_policy(self, max_batch: int = 16, min_batch_pct: int = 25, max_wait_ms: float = 2.0):
+        """Batch policy (the autotuner's engine knobs)."""
+        check(lib().gb_engine_set_policy(self.h, max_batch, min_batch_pct, max_wait_ms))
 
     def set_codestream(self, fps: float = 24.0, max_mbps: float = 230.0, comp_mbps: float = 200.0,
                        label: str = "GAIL 1.1.0", tag: str = "", threads: int = 4, check_dci: bool = True):

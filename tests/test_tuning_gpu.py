@@ -1,0 +1,36 @@
+"""Tuning changes launch shapes and work order, never results: Tier-1 frames and decoded
+pictures are bit-identical under extreme tunings."""
+import numpy as np
+import pytest
+
+from libgail_b200 import autotune as AT
+from libgail_b200 import codestream as CS
+from libgail_b200 import plugin as P
+from libgail_b200 import synth
+
+
+@pytest.mark.gpu
+def test_tuning_does_not_change_results():
+    W, H = 1998, 1080
+    dev = P.Plugin().device(0)
+    lay = P.LayoutHolder(W, H, 0)
+    frame = synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=77))
+    try:
+        enc = dev.encoder(lay, P.rgb48_format(W, H), P.color_passthrough())
+        ref = enc.encode(frame)[0]
+        cs = CS.rate_and_build(lay, ref, 24.0)[0]
+        blocks = CS.parse(cs)[1].view(P.CBLK_CODE_DTYPE)
+        dec = dev.decoder(lay)
+        pic = dec.decode(cs, blocks)[0]
+        for t in ({"soloDecisions": 256, "cmCtasPerSm": 1, "mqCtasPerSm": 1, "decCtasPerSm": 1},
+                  {"soloDecisions": 1 << 30, "cmCtasPerSm": 64, "mqCtasPerSm": 64, "decCtasPerSm": 64}):
+            AT.set_tuning(0, t)
+            got = enc.encode(frame)[0]
+            assert np.array_equal(got.info, ref.info) and np.array_equal(got.data, ref.data)
+            assert np.array_equal(got.pass_len, ref.pass_len) and np.array_equal(got.pass_dist, ref.pass_dist)
+            assert np.array_equal(dec.decode(cs, blocks)[0], pic)
+        dec.close()
+        enc.close()
+    finally:
+        AT.set_tuning(0, None)
+        dev.close()
