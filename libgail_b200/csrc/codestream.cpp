@@ -10,7 +10,10 @@
 // (codestream_check.cpp:43-280).
 #include "codestream.h"
 
+#include "pool.h"
+
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -27,6 +30,21 @@ enum : uint32_t {
 constexpr int kCblkLog2 = 5;
 
 int floorLog2(uint32_t v) { return 31 - __builtin_clz(v); }  // v > 0
+
+constexpr int kChunks = 16;  // work items per parallel phase
+template <class F> void forChunks(int n, F&& f) {  // f(begin, end) over [0, n) in chunks
+    if (n <= 0) return;
+    if (n < 2 * kChunks) {  // too little to share out
+        f(0, n);
+        return;
+    }
+    const int per = (n + kChunks - 1) / kChunks;
+    parallelFor(kChunks, [&](int c) {
+        const int b = c * per, e = std::min(n, b + per);
+        if (b < e) f(b, e);
+    });
+}
+
 
 // ------------------------------------------------------------------ packet-header bits
 // B.10.1: bits fill each byte from the top; the byte after an 0xFF byte carries only 7
@@ -445,45 +463,59 @@ CodestreamSizes CodestreamWriter::build(const Tier1View& t1, const uint8_t* pass
     std::vector<uint8_t> hdr;
     mainHeader(hdr, comment);
     const size_t tlmAt = hdr.size() - 5 * (size_t)ntp_;
-    if (out) {
-        out->clear();
-        out->reserve(1 << 20);
-        out->insert(out->end(), hdr.begin(), hdr.end());
-    }
+    // every packet's size, in parallel
+    const int np = numPackets();
+    std::vector<uint32_t> pk((size_t)np);
+    forChunks(np, [&](int b, int e) {
+        for (int p = b; p < e; ++p) pk[(size_t)p] = (uint32_t)packet(p, t1, passes, nullptr);
+    });
     CodestreamSizes sz;
     sz.numTileParts = ntp_;
-    size_t total = hdr.size() + slack;
+    size_t total = hdr.size();
+    std::vector<size_t> at((size_t)np);  // each packet's offset in the codestream
     for (int tp = 0; tp < ntp_; ++tp) {
-        const int c = tp % 3;
-        size_t sot = 0;
-        if (out) {
-            sot = out->size();
-            put16(*out, kSOT);
-            put16(*out, 10);
-            put16(*out, 0);
-            put32(*out, 0);  // Psot, below
-            out->push_back((uint8_t)tp);
-            out->push_back((uint8_t)ntp_);
-            put16(*out, kSOD);
-        }
         size_t bytes = 14;  // SOT segment and SOD
-        for (int p = tpStart_[tp]; p < tpStart_[tp + 1]; ++p) bytes += packet(p, t1, passes, out);
-        if (out) {
-            const uint32_t psot = (uint32_t)(out->size() - sot);
-            if (psot != bytes) throw std::logic_error("tile-part size mismatch");
-            for (int k = 0; k < 4; ++k) {
-                (*out)[sot + 6 + k] = (uint8_t)(psot >> (24 - 8 * k));
-                (*out)[tlmAt + 5 * tp + 1 + k] = (uint8_t)(psot >> (24 - 8 * k));
-            }
+        for (int p = tpStart_[tp]; p < tpStart_[tp + 1]; ++p) {
+            at[(size_t)p] = total + bytes;
+            bytes += pk[(size_t)p];
         }
         sz.tilePart[tp] = bytes;
-        sz.comp[c] += bytes;
+        sz.comp[tp % 3] += bytes;
         total += bytes;
     }
-    total += 2;
-    if (out) put16(*out, kEOC);
-    sz.total = total;
-    if (out && out->size() + slack != total) throw std::logic_error("codestream size mismatch");
+    sz.total = total + slack + 2;
+    if (out) {
+        out->assign(total + 2, 0);
+        uint8_t* d = out->data();
+        std::memcpy(d, hdr.data(), hdr.size());
+        size_t pos = hdr.size();
+        for (int tp = 0; tp < ntp_; ++tp) {
+            const uint32_t psot = (uint32_t)sz.tilePart[tp];
+            const uint8_t sot[14] = {0xFF, 0x90, 0, 10, 0, 0, (uint8_t)(psot >> 24), (uint8_t)(psot >> 16),
+                                     (uint8_t)(psot >> 8), (uint8_t)psot, (uint8_t)tp, (uint8_t)ntp_, 0xFF, 0x93};
+            std::memcpy(d + pos, sot, 14);
+            for (int k = 0; k < 4; ++k) d[tlmAt + 5 * tp + 1 + k] = (uint8_t)(psot >> (24 - 8 * k));
+            pos += psot;
+        }
+        d[total] = 0xFF;  // EOC
+        d[total + 1] = 0xD9;
+        // the packets into their places, in parallel
+        std::atomic<bool> mismatch{false};
+        forChunks(np, [&](int b, int e) {
+            thread_local std::vector<uint8_t> tmp;
+            for (int p = b; p < e; ++p) {
+                tmp.clear();
+                packet(p, t1, passes, &tmp);
+                if (tmp.size() != pk[(size_t)p]) {
+                    mismatch.store(true);
+                    continue;
+                }
+                std::memcpy(d + at[(size_t)p], tmp.data(), tmp.size());
+            }
+        });
+        if (mismatch.load()) throw std::logic_error("packet size mismatch");
+        if (out->size() + slack != sz.total) throw std::logic_error("codestream size mismatch");
+    }
     return sz;
 }
 
@@ -491,7 +523,9 @@ CodestreamSizes CodestreamWriter::measure(const Tier1View& t1, const uint8_t* pa
     const int np = numPackets(), n = L_.numCblks();
     if (!measured_) {
         pkBytes_.assign((size_t)np, 0);
-        for (int p = 0; p < np; ++p) pkBytes_[(size_t)p] = (uint32_t)packet(p, t1, passes, nullptr);
+        forChunks(np, [&](int b, int e) {
+            for (int p = b; p < e; ++p) pkBytes_[(size_t)p] = (uint32_t)packet(p, t1, passes, nullptr);
+        });
         lastPasses_.assign(passes, passes + n);
         dirty_.assign((size_t)np, 0);
         measured_ = true;
@@ -501,11 +535,15 @@ CodestreamSizes CodestreamWriter::measure(const Tier1View& t1, const uint8_t* pa
                 dirty_[(size_t)blockPacket_[(size_t)i]] = 1;
                 lastPasses_[(size_t)i] = passes[i];
             }
+        std::vector<int> todo;
         for (int p = 0; p < np; ++p)
             if (dirty_[(size_t)p]) {
-                pkBytes_[(size_t)p] = (uint32_t)packet(p, t1, passes, nullptr);
+                todo.push_back(p);
                 dirty_[(size_t)p] = 0;
             }
+        forChunks((int)todo.size(), [&](int b, int e) {
+            for (int q = b; q < e; ++q) pkBytes_[(size_t)todo[(size_t)q]] = (uint32_t)packet(todo[(size_t)q], t1, passes, nullptr);
+        });
     }
     if (!hdrLongest_) {
         std::vector<uint8_t> hdr;
@@ -549,12 +587,15 @@ RateLimits dciLimits(double fps, double maxMbps, double compMbps) {
 namespace {
 
 // Per block, the points of the lower convex hull of its (rate, distortion reduction)
-// curve: passes, rate, slope to the previous point, distortion gained from it.
+// curve: passes, rate, slope to the previous point, distortion gained from it. A block has
+// at most as many points as passes, so block i's points sit at its pass offset:
+// [first[i], first[i] + count[i]) (the arrays have gaps between blocks).
 struct Hull {
-    std::vector<uint32_t> first;  // points of block i: [first[i], first[i + 1])
+    std::vector<uint32_t> first, count;
     std::vector<uint8_t> passes;
     std::vector<uint32_t> rate;
     std::vector<double> slope, gain;
+    uint32_t end(size_t i) const { return first[i] + count[i]; }
 };
 
 constexpr int kMaxHull = 165;  // the origin and up to 164 passes
@@ -566,26 +607,21 @@ double planeScale(int nbps, int k) {
     return (double)(1ull << (2 * plane)) / 4096.0;
 }
 
-Hull buildHull(const Layout& L, const Tier1View& t1) {
-    const int n = L.numCblks();
-    Hull H;
-    H.first.resize((size_t)n + 1);
-    H.passes.reserve(t1.numPasses);
-    H.rate.reserve(t1.numPasses);
-    H.slope.reserve(t1.numPasses);
-    H.gain.reserve(t1.numPasses);
+// The hull points of blocks [b, e), written at their blocks' pass offsets.
+void hullRange(const Layout& L, const Tier1View& t1, int b, int e, Hull& H) {
     uint32_t R[kMaxHull];
     double D[kMaxHull], S[kMaxHull];  // S[m]: slope from point m - 1 to point m
     int K[kMaxHull];
     double planes[64];  // 4^plane / 4096, exact powers of two
     for (int p = 0; p < 64; ++p) planes[p] = p < 32 ? (double)(1ull << (2 * p)) / 4096.0 : 0.0;
-    for (int i = 0; i < n; ++i) {
-        H.first[(size_t)i] = (uint32_t)H.passes.size();
+    for (int i = b; i < e; ++i) {
         const GbCblkInfo& ci = t1.info[i];
         const int np = (int)ci.numPasses;
+        H.first[(size_t)i] = ci.passBase;
+        H.count[(size_t)i] = 0;
         if (np == 0) continue;
-        const GbSubband& b = L.bands[L.cblks[(size_t)i].band];
-        const double scale = (double)b.delta * b.delta * b.weight;
+        const GbSubband& band = L.bands[L.cblks[(size_t)i].band];
+        const double scale = (double)band.delta * band.delta * band.weight;
         const uint32_t* len = t1.passLen + ci.passBase;
         const int32_t* dist = t1.passDist + ci.passBase;
         int m = 0;  // top of the hull stack; point 0 is the origin
@@ -611,15 +647,28 @@ Hull buildHull(const Layout& L, const Tier1View& t1) {
             K[m] = k + 1;
             S[m] = R[m] == R[m - 1] ? INFINITY : (D[m] - D[m - 1]) / (double)(R[m] - R[m - 1]);
         }
+        const size_t o = ci.passBase;
         for (int q = 1; q <= m; ++q) {
-            H.passes.push_back((uint8_t)K[q]);
-            H.rate.push_back(R[q]);
+            H.passes[o + q - 1] = (uint8_t)K[q];
+            H.rate[o + q - 1] = R[q];
             const double dr = (double)R[q] - (double)R[q - 1];
-            H.slope.push_back(dr <= 0 ? INFINITY : (D[q] - D[q - 1]) / dr);
-            H.gain.push_back(D[q] - D[q - 1]);
+            H.slope[o + q - 1] = dr <= 0 ? INFINITY : (D[q] - D[q - 1]) / dr;
+            H.gain[o + q - 1] = D[q] - D[q - 1];
         }
+        H.count[(size_t)i] = (uint32_t)m;
     }
-    H.first[(size_t)n] = (uint32_t)H.passes.size();
+}
+
+Hull buildHull(const Layout& L, const Tier1View& t1) {
+    const int n = L.numCblks();
+    Hull H;
+    H.first.assign((size_t)n, 0);
+    H.count.assign((size_t)n, 0);
+    H.passes.resize(t1.numPasses);
+    H.rate.resize(t1.numPasses);
+    H.slope.resize(t1.numPasses);
+    H.gain.resize(t1.numPasses);
+    forChunks(n, [&](int b, int e) { hullRange(L, t1, b, e, H); });
     return H;
 }
 
@@ -633,11 +682,18 @@ public:
             bytes_[c].assign((size_t)nb_ + 1, 0.0);
             blocks_[c].assign((size_t)nb_ + 1, 0.0);
         }
+        // the bin of every hull point in parallel (the log2 is the cost); the sums of
+        // integer-valued doubles below are exact in any order
+        std::vector<int> binOf(H.slope.size());
+        forChunks(L.numCblks(), [&](int b, int e) {
+            for (int i = b; i < e; ++i)
+                for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h) binOf[h] = bin(H.slope[h]);
+        });
         for (int i = 0; i < L.numCblks(); ++i) {
             const int c = L.bands[L.cblks[(size_t)i].band].comp;
             uint32_t prev = 0;
-            for (uint32_t h = H.first[(size_t)i]; h < H.first[(size_t)i + 1]; ++h) {
-                const int b = bin(H.slope[h]);
+            for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h) {
+                const int b = binOf[h];
                 bytes_[c][(size_t)b] += (double)H.rate[h] - prev;
                 if (h == H.first[(size_t)i]) blocks_[c][(size_t)b] += 1;
                 prev = H.rate[h];
@@ -683,15 +739,17 @@ RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimi
 
     // every block's passes at the thresholds: its hull points down to the first flatter one
     auto select = [&](const double l[3]) {
-        for (int i = 0; i < n; ++i) {
-            const double t = l[compOf[(size_t)i]];
-            uint8_t np = 0;
-            for (uint32_t h = H.first[(size_t)i]; h < H.first[(size_t)i + 1]; ++h) {
-                if (H.slope[h] < t) break;
-                np = H.passes[h];
+        forChunks(n, [&](int b, int e) {
+            for (int i = b; i < e; ++i) {
+                const double t = l[compOf[(size_t)i]];
+                uint8_t np = 0;
+                for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h) {
+                    if (H.slope[h] < t) break;
+                    np = H.passes[h];
+                }
+                res.passes[(size_t)i] = np;
             }
-            res.passes[(size_t)i] = np;
-        }
+        });
     };
     w.restart();
     auto measure = [&](const double l[3]) {
@@ -701,11 +759,29 @@ RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimi
     };
 
     double maxSlope = 0, minSlope = INFINITY;
-    for (double s : H.slope)
-        if (std::isfinite(s) && s > 0) {
-            maxSlope = std::max(maxSlope, s);
-            minSlope = std::min(minSlope, s);
+    {
+        double mx[kChunks], mn[kChunks];
+        std::fill(mx, mx + kChunks, 0.0);
+        std::fill(mn, mn + kChunks, INFINITY);
+        const int per = (n + kChunks - 1) / kChunks;
+        parallelFor(kChunks, [&](int c) {
+            double hi = 0, lo = INFINITY;  // in registers: one store per chunk
+            for (int i = c * per; i < std::min(n, (c + 1) * per); ++i)
+                for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h) {
+                    const double s = H.slope[h];
+                    if (std::isfinite(s) && s > 0) {
+                        hi = std::max(hi, s);
+                        lo = std::min(lo, s);
+                    }
+                }
+            mx[c] = hi;
+            mn[c] = lo;
+        });
+        for (int c = 0; c < kChunks; ++c) {
+            maxSlope = std::max(maxSlope, mx[c]);
+            minSlope = std::min(minSlope, mn[c]);
         }
+    }
     if (maxSlope == 0) maxSlope = minSlope = 1;
     const double loBound = std::log2(minSlope) - 1, hiBound = std::log2(maxSlope) + 1;
     const SlopeBins bins(L, H, loBound, hiBound);
@@ -791,8 +867,8 @@ RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimi
     res.lambda = std::max({lam[0], lam[1], lam[2]});
     for (int c = 0; c < 3; ++c) res.lambdaComp[c] = lam[c];
     double dist = 0;
-    for (int i = 0; i < n; ++i)
-        for (uint32_t h = H.first[(size_t)i]; h < H.first[(size_t)i + 1]; ++h)
+    for (int i = 0; i < n; ++i)  // in block order, as the sum is not exact in any other
+        for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h)
             if (H.passes[h] > res.passes[(size_t)i]) dist += H.gain[h];
     res.distortion = dist;
     res.sizes = sz;
