@@ -1240,68 +1240,96 @@ void parseCodestream(const uint8_t* data, size_t size, Layout& L, std::vector<Gb
     }
     if (parts.empty()) bad("no tile-parts");
 
-    // packets
+    // packets. One packet from pos (within [pos, end)); returns where the next one starts.
     blocks.assign((size_t)L.numCblks(), GbCblkCode{});
-    TagTree& incl = t_incl;
-    TagTree& msbTree = t_msb;
-    size_t tp = 0, pos = parts[0].b, end = parts[0].e;
-    for (size_t v = 0; v < volRs.size(); ++v)
-        for (int c = 0; c < kNumComps; ++c)
-            forEachPacket(L, volRs[v], volRe[v], c, [&](int r, int prec) {
-                while (pos >= end) {
-                    if (++tp >= parts.size()) bad("the tile-parts end before the last packet");
-                    pos = parts[tp].b;
-                    end = parts[tp].e;
+    auto parsePacket = [&](int c, int r, int prec, size_t pos, size_t end) {
+        TagTree& incl = t_incl;
+        TagTree& msbTree = t_msb;
+        if (sop && end - pos >= 6 && data[pos] == 0xFF && data[pos + 1] == (kSOP & 0xFF)) pos += 6;
+        const Precinct& P = L.resolution(c, r).precincts[(size_t)prec];
+        HeaderReader hr(data + pos, end - pos);
+        size_t body = 0;
+        const bool present = hr.bit() != 0;
+        for (int k = 0; present && k < P.nb; ++k) {
+            const PrecinctBand& pb = P.bands[k];
+            if (pb.ncbx <= 0 || pb.ncby <= 0) continue;
+            const GbSubband& b = L.bands[pb.band];
+            incl.shape(pb.ncbx, pb.ncby);
+            msbTree.shape(pb.ncbx, pb.ncby);
+            for (int j = 0; j < pb.ncby; ++j)
+                for (int i = 0; i < pb.ncbx; ++i) {
+                    const int leaf = j * pb.ncbx + i;
+                    if (!incl.decode(hr, leaf, 1)) continue;
+                    if (!msbTree.decode(hr, leaf, b.Mb + 1)) bad("more missing bit-planes than the band has");
+                    const int nbps = b.Mb - msbTree.value(leaf);
+                    const int np = getPasses(hr);
+                    int lblock = 3;
+                    while (hr.bit())
+                        if (++lblock > 24) bad("code-block length field too wide");
+                    const uint32_t len = hr.get(lblock + floorLog2((uint32_t)np));
+                    if (hr.overrun()) bad("packet header runs past its tile-part");
+                    if (nbps < 1 || np > 3 * nbps - 2) bad("more coding passes than bit-planes allow");
+                    GbCblkCode& cb = blocks[(size_t)(b.cblkBase + (pb.cby0 + j) * b.ncbx + pb.cbx0 + i)];
+                    cb.len = len;
+                    cb.passes = (uint8_t)np;
+                    cb.nbps = (uint8_t)nbps;
+                    body += len;
                 }
-                if (sop && end - pos >= 6 && data[pos] == 0xFF && data[pos + 1] == (kSOP & 0xFF)) pos += 6;
-                const Precinct& P = L.resolution(c, r).precincts[(size_t)prec];
-                HeaderReader hr(data + pos, end - pos);
-                size_t body = 0;
-                const bool present = hr.bit() != 0;
-                for (int k = 0; present && k < P.nb; ++k) {
-                    const PrecinctBand& pb = P.bands[k];
-                    if (pb.ncbx <= 0 || pb.ncby <= 0) continue;
-                    const GbSubband& b = L.bands[pb.band];
-                    incl.shape(pb.ncbx, pb.ncby);
-                    msbTree.shape(pb.ncbx, pb.ncby);
-                    for (int j = 0; j < pb.ncby; ++j)
-                        for (int i = 0; i < pb.ncbx; ++i) {
-                            const int leaf = j * pb.ncbx + i;
-                            if (!incl.decode(hr, leaf, 1)) continue;
-                            if (!msbTree.decode(hr, leaf, b.Mb + 1)) bad("more missing bit-planes than the band has");
-                            const int nbps = b.Mb - msbTree.value(leaf);
-                            const int np = getPasses(hr);
-                            int lblock = 3;
-                            while (hr.bit())
-                                if (++lblock > 24) bad("code-block length field too wide");
-                            const uint32_t len = hr.get(lblock + floorLog2((uint32_t)np));
-                            if (hr.overrun()) bad("packet header runs past its tile-part");
-                            if (nbps < 1 || np > 3 * nbps - 2) bad("more coding passes than bit-planes allow");
-                            GbCblkCode& cb = blocks[(size_t)(b.cblkBase + (pb.cby0 + j) * b.ncbx + pb.cbx0 + i)];
-                            cb.len = len;
-                            cb.passes = (uint8_t)np;
-                            cb.nbps = (uint8_t)nbps;
-                            body += len;
-                        }
+        }
+        const size_t hdr = hr.end();
+        if (hr.overrun() || hdr > end - pos) bad("packet header runs past its tile-part");
+        pos += hdr;
+        if (eph && end - pos >= 2 && data[pos] == 0xFF && data[pos + 1] == (kEPH & 0xFF)) pos += 2;
+        if (body > end - pos) bad("code-block data runs past its tile-part");
+        for (int k = 0; present && k < P.nb; ++k) {
+            const PrecinctBand& pb = P.bands[k];
+            if (pb.ncbx <= 0 || pb.ncby <= 0) continue;
+            const GbSubband& b = L.bands[pb.band];
+            for (int j = 0; j < pb.ncby; ++j)
+                for (int i = 0; i < pb.ncbx; ++i) {
+                    GbCblkCode& cb = blocks[(size_t)(b.cblkBase + (pb.cby0 + j) * b.ncbx + pb.cbx0 + i)];
+                    if (!cb.passes) continue;
+                    cb.offset = (uint32_t)pos;
+                    pos += cb.len;
                 }
-                const size_t hdr = hr.end();
-                if (hr.overrun() || hdr > end - pos) bad("packet header runs past its tile-part");
-                pos += hdr;
-                if (eph && end - pos >= 2 && data[pos] == 0xFF && data[pos + 1] == (kEPH & 0xFF)) pos += 2;
-                if (body > end - pos) bad("code-block data runs past its tile-part");
-                for (int k = 0; present && k < P.nb; ++k) {
-                    const PrecinctBand& pb = P.bands[k];
-                    if (pb.ncbx <= 0 || pb.ncby <= 0) continue;
-                    const GbSubband& b = L.bands[pb.band];
-                    for (int j = 0; j < pb.ncby; ++j)
-                        for (int i = 0; i < pb.ncbx; ++i) {
-                            GbCblkCode& cb = blocks[(size_t)(b.cblkBase + (pb.cby0 + j) * b.ncbx + pb.cbx0 + i)];
-                            if (!cb.passes) continue;
-                            cb.offset = (uint32_t)pos;
-                            pos += cb.len;
-                        }
-                }
+        }
+        return pos;
+    };
+    // The DCI organisation: tile-part g holds exactly the packets of (volume g / 3,
+    // component g % 3), so the tile-parts are read in parallel. Any other organisation
+    // (packets spilling over tile-part boundaries) is read in order below.
+    struct NotOneGroupPerPart {};
+    bool done = false;
+    if (parts.size() == volRs.size() * 3) {
+        try {
+            parallelFor((int)parts.size(), [&](int g) {
+                const int v = g / 3, c = g % 3;
+                size_t pos = parts[(size_t)g].b;
+                const size_t end = parts[(size_t)g].e;
+                forEachPacket(L, volRs[(size_t)v], volRe[(size_t)v], c, [&](int r, int prec) {
+                    if (pos >= end) throw NotOneGroupPerPart{};
+                    pos = parsePacket(c, r, prec, pos, end);
+                });
+                if (pos != end) throw NotOneGroupPerPart{};
             });
+            done = true;
+        } catch (const NotOneGroupPerPart&) {
+            blocks.assign((size_t)L.numCblks(), GbCblkCode{});
+        }
+    }
+    if (!done) {
+        size_t tp = 0, pos = parts[0].b, end = parts[0].e;
+        for (size_t v = 0; v < volRs.size(); ++v)
+            for (int c = 0; c < kNumComps; ++c)
+                forEachPacket(L, volRs[v], volRe[v], c, [&](int r, int prec) {
+                    while (pos >= end) {
+                        if (++tp >= parts.size()) bad("the tile-parts end before the last packet");
+                        pos = parts[tp].b;
+                        end = parts[tp].e;
+                    }
+                    pos = parsePacket(c, r, prec, pos, end);
+                });
+    }
 }
 
 }  // namespace gb
