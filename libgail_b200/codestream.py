@@ -112,13 +112,12 @@ def parse(cs: bytes):
     L = _bind()
     d = np.frombuffer(cs, np.uint8)
     nb, nblk, w, h, prof = C.c_int(), C.c_uint64(), C.c_int(), C.c_int(), C.c_int()
-    check(L.gb_parse_codestream(d.ctypes.data, d.size, None, 0, C.byref(nb), None, 0, C.byref(nblk), C.byref(w),
-                                C.byref(h), C.byref(prof)))
-    bands = (Subband * nb.value)()
-    blocks = np.zeros(nblk.value, dtype=np.dtype([("offset", "<u4"), ("len", "<u4"), ("passes", "u1"),
-                                                  ("nbps", "u1"), ("_pad", "u1", 2)]))
+    # room for the largest DCI layout (4096 x 2160: 57 bands, 26,292 code-blocks): one call
+    bands = (Subband * 64)()
+    blocks = np.zeros(60000, dtype=np.dtype([("offset", "<u4"), ("len", "<u4"), ("passes", "u1"), ("nbps", "u1"),
+                                             ("_pad", "u1", 2)]))
     assert blocks.itemsize == C.sizeof(CblkCode)
-    check(L.gb_parse_codestream(d.ctypes.data, d.size, bands, nb.value, C.byref(nb), blocks.ctypes.data, blocks.size,
+    check(L.gb_parse_codestream(d.ctypes.data, d.size, bands, 64, C.byref(nb), blocks.ctypes.data, blocks.size,
                                 C.byref(nblk), C.byref(w), C.byref(h), C.byref(prof)))
-    lay = LayoutHolder(w.value, h.value, prof.value, bands=list(bands))
-    return lay, blocks
+    lay = LayoutHolder(w.value, h.value, prof.value, bands=list(bands)[: nb.value])
+    return lay, blocks[: nblk.value]
