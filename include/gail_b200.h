@@ -148,7 +148,10 @@ GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
  *                          HBM budget); handed out by gb_engine_wait like an encode (its Tier-1
  *                          view empty)
  *   gb_engine_picture      a handed-out decode's picture (valid until release): height rows
- *                          of width x 3 codes */
+ *                          of width x 3 codes
+ *   gb_engine_hull         a handed-out encode's PCRD hull points, computed on the GPU after
+ *                          Tier-1 (valid until release; the layout of gb_tier1_hull, over the
+ *                          frame's numPasses slots); its codestream's rate control takes them */
 typedef struct GbEngine GbEngine;
 GB_API int gb_engine_create(int device, uint64_t hbmBudget, int maxBatch, GbEngine** out);
 GB_API void gb_engine_destroy(GbEngine* e);
@@ -170,6 +173,7 @@ GB_API int gb_engine_add_decoder(GbEngine* e, const GailCudaLayout* layout, cons
                                  int* classId, uint64_t* frameBytes);
 GB_API int gb_engine_submit_decode(GbEngine* e, int classId, const uint8_t* data, uint64_t size, int64_t* id);
 GB_API int gb_engine_picture(GbEngine* e, int64_t id, const uint16_t** pix, int* width, int* height);
+GB_API int gb_engine_hull(GbEngine* e, int64_t id, const uint8_t** passes, const double** slope);
 
 /* The host codec around a Tier-1 frame, byte-identical to libgail's core for the same
  * frame. Thread-safe across threads (each keeps its own writer per layout and label).
@@ -185,6 +189,17 @@ GB_API int gb_engine_picture(GbEngine* e, int64_t id, const uint16_t** pix, int*
  *                              then the codestream (allocateRate, src/core/rate_control.h:32,
  *                              followed by buildCodestream, as src/core/pipeline.cpp:210-219);
  *                              passesOut: one byte per block; out may be NULL to get the size
+ *   gb_rate_and_build_hull     gb_rate_and_build taking each block's PCRD hull points instead of
+ *                              computing them (the convex hull of buildHull,
+ *                              src/core/rate_control.cpp:38-86): hullPasses/hullSlope as
+ *                              gb_tier1_hull lays them out, e.g. from gb_engine_hull; the
+ *                              result is the same as gb_rate_and_build's
+ *   gb_tier1_hull              the hull points on the host: per pass slot of the Tier-1 frame
+ *                              (numPasses entries), block i's points from its passBase on, in
+ *                              order, each the coding passes at the point and the slope from
+ *                              the previous point (distortion reduction per byte, +inf for no
+ *                              added bytes); a block's points end at its pass count or at the
+ *                              first entry with passes 0
  *   gb_check_dci               DCI compliance of a codestream at fps: *ok 1 or 0, msg the COM
  *                              text or the first error (checkDciCodestream,
  *                              src/core/codestream_check.h:33)
@@ -199,6 +214,11 @@ GB_API int gb_build_codestream(const GailCudaLayout* layout, const GailCudaTier1
 GB_API int gb_rate_and_build(const GailCudaLayout* layout, const GailCudaTier1* t1, double fps, double maxMbps,
                              double compMbps, const char* label, const char* tag, uint8_t* passesOut, uint8_t* out,
                              uint64_t cap, uint64_t* size, double* lambda);
+GB_API int gb_rate_and_build_hull(const GailCudaLayout* layout, const GailCudaTier1* t1, const uint8_t* hullPasses,
+                                  const double* hullSlope, double fps, double maxMbps, double compMbps,
+                                  const char* label, const char* tag, uint8_t* passesOut, uint8_t* out, uint64_t cap,
+                                  uint64_t* size, double* lambda);
+GB_API int gb_tier1_hull(const GailCudaLayout* layout, const GailCudaTier1* t1, uint8_t* passes, double* slope);
 GB_API int gb_check_dci(const uint8_t* data, uint64_t size, double fps, char* msg, uint64_t msgCap, int* ok);
 GB_API int gb_parse_codestream(const uint8_t* data, uint64_t size, GbSubband* bands, int maxBands, int* numBands,
                                GbCblkCode* blocks, uint64_t maxBlocks, uint64_t* numBlocks, int* width, int* height,

@@ -25,6 +25,10 @@ def _bind():
                                       C.c_uint64, u64p]
     L.gb_rate_and_build.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_char_p,
                                     C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint64, u64p, C.POINTER(C.c_double)]
+    L.gb_rate_and_build_hull.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                         C.c_double, C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint64, u64p,
+                                         C.POINTER(C.c_double)]
+    L.gb_tier1_hull.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.gb_check_dci.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_char_p, C.c_uint64, C.POINTER(C.c_int)]
     L.gb_parse_codestream.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,
                                       C.c_uint64, u64p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -86,16 +90,36 @@ def build(layout: LayoutHolder, t1, passes, label: str = DEFAULT_LABEL, tag: str
 
 
 def rate_and_build(layout: LayoutHolder, t1, fps: float = 24.0, max_mbps: float = 230.0, comp_mbps: float = 200.0,
-                   label: str = DEFAULT_LABEL, tag: str = ""):
-    """(codestream bytes, passes per block, lambda)."""
+                   label: str = DEFAULT_LABEL, tag: str = "", hull_points=None):
+    """(codestream bytes, passes per block, lambda). hull_points: (passes, slope) arrays as
+    hull() gives them (e.g. computed on the GPU by the engine), taken instead of computing
+    the hull."""
     L, t = _bind(), _t1(t1)
     passes = np.zeros(layout.abi.numCblks, np.uint8)
     cap = 1 << 22
     out = np.empty(cap, np.uint8)
     n, lam = C.c_uint64(), C.c_double()
-    check(L.gb_rate_and_build(C.byref(layout.abi), C.byref(t.abi), fps, max_mbps, comp_mbps, label.encode(),
-                              tag.encode(), passes.ctypes.data, out.ctypes.data, cap, C.byref(n), C.byref(lam)))
+    hp = hs = None
+    if hull_points is not None:
+        hp = np.ascontiguousarray(hull_points[0], np.uint8)
+        hs = np.ascontiguousarray(hull_points[1], np.float64)
+        if hp.size < t.abi.numPasses or hs.size < t.abi.numPasses:
+            raise ValueError("hull arrays shorter than the Tier-1 frame's passes")
+    check(L.gb_rate_and_build_hull(C.byref(layout.abi), C.byref(t.abi), None if hp is None else hp.ctypes.data,
+                                   None if hs is None else hs.ctypes.data, fps, max_mbps, comp_mbps, label.encode(),
+                                   tag.encode(), passes.ctypes.data, out.ctypes.data, cap, C.byref(n), C.byref(lam)))
     return out[: n.value].tobytes(), passes, lam.value
+
+
+def hull(layout: LayoutHolder, t1):
+    """Every block's PCRD hull points on the host: (passes uint8, slope float64) per pass slot
+    of the Tier-1 frame; block i's points from its passBase on, ending at its pass count or
+    the first 0 in passes."""
+    L, t = _bind(), _t1(t1)
+    n = t.abi.numPasses
+    p, s = np.zeros(max(n, 1), np.uint8), np.zeros(max(n, 1), np.float64)
+    check(L.gb_tier1_hull(C.byref(layout.abi), C.byref(t.abi), p.ctypes.data, s.ctypes.data))
+    return p[:n], s[:n]
 
 
 def check_dci(cs: bytes, fps: float = 24.0):

@@ -99,17 +99,20 @@ GB_API int gb_build_codestream(const GailCudaLayout* layout, const GailCudaTier1
     });
 }
 
-GB_API int gb_rate_and_build(const GailCudaLayout* layout, const GailCudaTier1* t1, double fps, double maxMbps,
-                             double compMbps, const char* label, const char* tag, uint8_t* passesOut, uint8_t* out,
-                             uint64_t cap, uint64_t* size, double* lambda) {
+GB_API int gb_rate_and_build_hull(const GailCudaLayout* layout, const GailCudaTier1* t1, const uint8_t* hullPasses,
+                                  const double* hullSlope, double fps, double maxMbps, double compMbps,
+                                  const char* label, const char* tag, uint8_t* passesOut, uint8_t* out, uint64_t cap,
+                                  uint64_t* size, double* lambda) {
     return gbGuard([&] {
         if (!layout || !t1 || !size) throw std::logic_error("null argument");
+        if (!hullPasses != !hullSlope) throw std::logic_error("hull passes and slopes go together");
         checkTier1(*layout, *t1);
         const Tier1View v = viewOf(*t1);
         CodestreamWriter& w = writerFor(*layout, label);
         const RateLimits lim = dciLimits(fps, maxMbps, compMbps);
         if (w.emptyBytes() > lim.maxTotal) throw std::logic_error("the frame budget is below the smallest codestream");
-        const RateResult rr = allocateRate(w, v, lim);
+        const HullView hv{hullPasses, hullSlope};
+        const RateResult rr = allocateRate(w, v, lim, hullPasses ? &hv : nullptr);
         thread_local std::vector<uint8_t> cs;
         w.build(v, rr.passes.data(), &cs, tag ? tag : "");
         *size = cs.size();
@@ -119,6 +122,23 @@ GB_API int gb_rate_and_build(const GailCudaLayout* layout, const GailCudaTier1* 
             if (cs.size() > cap) throw std::logic_error("codestream buffer too small");
             std::memcpy(out, cs.data(), cs.size());
         }
+    });
+}
+
+GB_API int gb_rate_and_build(const GailCudaLayout* layout, const GailCudaTier1* t1, double fps, double maxMbps,
+                             double compMbps, const char* label, const char* tag, uint8_t* passesOut, uint8_t* out,
+                             uint64_t cap, uint64_t* size, double* lambda) {
+    return gb_rate_and_build_hull(layout, t1, nullptr, nullptr, fps, maxMbps, compMbps, label, tag, passesOut, out,
+                                  cap, size, lambda);
+}
+
+GB_API int gb_tier1_hull(const GailCudaLayout* layout, const GailCudaTier1* t1, uint8_t* passes, double* slope) {
+    return gbGuard([&] {
+        if (!layout || !t1 || !passes || !slope) throw std::logic_error("null argument");
+        checkTier1(*layout, *t1);
+        Layout L;
+        layoutFromAbi(*layout, L);
+        computeHull(L, viewOf(*t1), passes, slope);
     });
 }
 

@@ -98,6 +98,13 @@ GB_API int gb_engine_picture(GbEngine* e, int64_t id, const uint16_t** pix, int*
     });
 }
 
+GB_API int gb_engine_hull(GbEngine* e, int64_t id, const uint8_t** passes, const double** slope) {
+    return gbGuard([&] {
+        if (!e || !passes || !slope) throw std::logic_error("null argument");
+        if (!e->e->hull(id, passes, slope)) throw std::logic_error("not an encode request");
+    });
+}
+
 GB_API int gb_engine_set_policy(GbEngine* e, int maxBatch, int minBatchPct, double maxWaitMs) {
     return gbGuard([&] {
         if (!e) throw std::logic_error("null argument");

@@ -592,9 +592,13 @@ namespace {
 // [first[i], first[i] + count[i]) (the arrays have gaps between blocks).
 struct Hull {
     std::vector<uint32_t> first, count;
-    std::vector<uint8_t> passes;
     std::vector<uint32_t> rate;
-    std::vector<double> slope, gain;
+    std::vector<double> gain;  // empty for a hull that came precomputed
+    const uint8_t* passes = nullptr;
+    const double* slope = nullptr;
+    size_t slots = 0;
+    std::vector<uint8_t> ownPasses;  // the storage of a hull computed here
+    std::vector<double> ownSlope;
     uint32_t end(size_t i) const { return first[i] + count[i]; }
 };
 
@@ -607,8 +611,18 @@ double planeScale(int nbps, int k) {
     return (double)(1ull << (2 * plane)) / 4096.0;
 }
 
-// The hull points of blocks [b, e), written at their blocks' pass offsets.
-void hullRange(const Layout& L, const Tier1View& t1, int b, int e, Hull& H) {
+// The hull points of blocks [b, e), written at their blocks' pass offsets: passes, slope,
+// and where given, rate and gain; first/count where given.
+struct HullOut {
+    uint8_t* passes;
+    double* slope;
+    uint32_t* rate;
+    double* gain;
+    uint32_t* first;
+    uint32_t* count;
+};
+
+void hullRange(const Layout& L, const Tier1View& t1, int b, int e, const HullOut& H) {
     uint32_t R[kMaxHull];
     double D[kMaxHull], S[kMaxHull];  // S[m]: slope from point m - 1 to point m
     int K[kMaxHull];
@@ -617,8 +631,8 @@ void hullRange(const Layout& L, const Tier1View& t1, int b, int e, Hull& H) {
     for (int i = b; i < e; ++i) {
         const GbCblkInfo& ci = t1.info[i];
         const int np = (int)ci.numPasses;
-        H.first[(size_t)i] = ci.passBase;
-        H.count[(size_t)i] = 0;
+        if (H.first) H.first[(size_t)i] = ci.passBase;
+        if (H.count) H.count[(size_t)i] = 0;
         if (np == 0) continue;
         const GbSubband& band = L.bands[L.cblks[(size_t)i].band];
         const double scale = (double)band.delta * band.delta * band.weight;
@@ -650,12 +664,16 @@ void hullRange(const Layout& L, const Tier1View& t1, int b, int e, Hull& H) {
         const size_t o = ci.passBase;
         for (int q = 1; q <= m; ++q) {
             H.passes[o + q - 1] = (uint8_t)K[q];
-            H.rate[o + q - 1] = R[q];
             const double dr = (double)R[q] - (double)R[q - 1];
             H.slope[o + q - 1] = dr <= 0 ? INFINITY : (D[q] - D[q - 1]) / dr;
-            H.gain[o + q - 1] = D[q] - D[q - 1];
+            if (H.rate) H.rate[o + q - 1] = R[q];
+            if (H.gain) H.gain[o + q - 1] = D[q] - D[q - 1];
         }
-        H.count[(size_t)i] = (uint32_t)m;
+        if (H.count) H.count[(size_t)i] = (uint32_t)m;
+        for (int q = m; q < np; ++q) {  // the rest of the block's entries: the end mark
+            H.passes[o + q] = 0;
+            H.slope[o + q] = 0;
+        }
     }
 }
 
@@ -664,11 +682,51 @@ Hull buildHull(const Layout& L, const Tier1View& t1) {
     Hull H;
     H.first.assign((size_t)n, 0);
     H.count.assign((size_t)n, 0);
-    H.passes.resize(t1.numPasses);
+    H.ownPasses.resize(t1.numPasses);
+    H.ownSlope.resize(t1.numPasses);
     H.rate.resize(t1.numPasses);
-    H.slope.resize(t1.numPasses);
     H.gain.resize(t1.numPasses);
-    forChunks(n, [&](int b, int e) { hullRange(L, t1, b, e, H); });
+    H.passes = H.ownPasses.data();
+    H.slope = H.ownSlope.data();
+    H.slots = t1.numPasses;
+    const HullOut out{H.ownPasses.data(), H.ownSlope.data(), H.rate.data(), H.gain.data(), H.first.data(),
+                      H.count.data()};
+    forChunks(n, [&](int b, int e) { hullRange(L, t1, b, e, out); });
+    return H;
+}
+
+// A hull computed elsewhere (the GPU), in the HullView layout: its points are checked to
+// be well formed (strictly increasing pass counts within the block's passes) and their
+// rates looked up in the pass tables.
+Hull hullFromView(const Layout& L, const Tier1View& t1, const HullView& v) {
+    const int n = L.numCblks();
+    Hull H;
+    H.first.assign((size_t)n, 0);
+    H.count.assign((size_t)n, 0);
+    H.rate.resize(t1.numPasses);
+    H.passes = v.passes;
+    H.slope = v.slope;
+    H.slots = t1.numPasses;
+    std::atomic<bool> bad{false};
+    forChunks(n, [&](int b, int e) {
+        for (int i = b; i < e; ++i) {
+            const GbCblkInfo& ci = t1.info[i];
+            const uint32_t o = ci.passBase, np = ci.numPasses;
+            H.first[(size_t)i] = o;
+            uint32_t m = 0, prev = 0;
+            for (; m < np && v.passes[o + m] != 0; ++m) {
+                const uint32_t k = v.passes[o + m];
+                if (k <= prev || k > np) {
+                    bad = true;
+                    break;
+                }
+                H.rate[o + m] = t1.passLen[o + k - 1];
+                prev = k;
+            }
+            H.count[(size_t)i] = m;
+        }
+    });
+    if (bad) throw std::runtime_error("malformed hull points");
     return H;
 }
 
@@ -684,7 +742,7 @@ public:
         }
         // the bin of every hull point in parallel (the log2 is the cost); the sums of
         // integer-valued doubles below are exact in any order
-        std::vector<int> binOf(H.slope.size());
+        std::vector<int> binOf(H.slots);
         forChunks(L.numCblks(), [&](int b, int e) {
             for (int i = b; i < e; ++i)
                 for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h) binOf[h] = bin(H.slope[h]);
@@ -727,10 +785,15 @@ private:
 
 }  // namespace
 
-RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimits& lim) {
+void computeHull(const Layout& L, const Tier1View& t1, uint8_t* passes, double* slope) {
+    const HullOut out{passes, slope, nullptr, nullptr, nullptr, nullptr};
+    forChunks(L.numCblks(), [&](int b, int e) { hullRange(L, t1, b, e, out); });
+}
+
+RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimits& lim, const HullView* hull) {
     const Layout& L = w.layout();
     const int n = L.numCblks();
-    const Hull H = buildHull(L, t1);
+    const Hull H = hull ? hullFromView(L, t1, *hull) : buildHull(L, t1);
     RateResult res;
     res.passes.assign((size_t)n, 0);
     double lam[3] = {0, 0, 0};
@@ -866,10 +929,11 @@ RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimi
     }
     res.lambda = std::max({lam[0], lam[1], lam[2]});
     for (int c = 0; c < 3; ++c) res.lambdaComp[c] = lam[c];
-    double dist = 0;
-    for (int i = 0; i < n; ++i)  // in block order, as the sum is not exact in any other
-        for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h)
-            if (H.passes[h] > res.passes[(size_t)i]) dist += H.gain[h];
+    double dist = H.gain.empty() ? NAN : 0.0;
+    if (!H.gain.empty())
+        for (int i = 0; i < n; ++i)  // in block order, as the sum is not exact in any other
+            for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h)
+                if (H.passes[h] > res.passes[(size_t)i]) dist += H.gain[h];
     res.distortion = dist;
     res.sizes = sz;
     return res;

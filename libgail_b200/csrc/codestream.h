@@ -101,15 +101,32 @@ struct RateResult {
     std::vector<uint8_t> passes;  // passes included per block
     double lambda = 0;            // the final slope threshold (largest of the components')
     double lambdaComp[3] = {0, 0, 0};
-    double distortion = 0;        // estimated remaining weighted squared error
+    double distortion = 0;        // estimated remaining weighted squared error (NaN when
+                                  // the hull came precomputed, without the gains)
     CodestreamSizes sizes;
     int iterations = 0;           // exact measurements taken
 };
 
+// Per block, the points of the lower convex hull of its (truncation length, weighted
+// distortion reduction) curve, laid out like the Tier-1 pass tables: block i's points at
+// its passBase, in order, ending at its pass count or at the first entry with passes 0.
+// passes: coding passes at the point; slope: distortion reduction per byte from the
+// previous point (+inf for no added bytes).
+struct HullView {
+    const uint8_t* passes = nullptr;
+    const double* slope = nullptr;
+};
+
+// The hull points of every block into passes/slope (t1.numPasses entries each), by the
+// arithmetic allocateRate uses.
+void computeHull(const Layout& L, const Tier1View& t1, uint8_t* passes, double* slope);
+
 // PCRD-opt: per block the convex hull of (rate, weighted distortion reduction) over its
 // truncation points, one slope threshold per component, the largest set of passes whose
-// codestream fits the limits.
-RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimits& lim);
+// codestream fits the limits. With hull, its points are taken instead of computed (they
+// must be those computeHull gives; a malformed hull throws).
+RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimits& lim,
+                        const HullView* hull = nullptr);
 
 struct DciReport {
     bool ok = true;

@@ -24,6 +24,14 @@ struct CompactArgs {
                                // on this stream, so the Tier-1 launch's perm table will do
     uint2* offsets;            // device, per block: codeword byte offset, pass offset
     int hostOut;               // the out* buffers are mapped host memory: fewer copying CTAs
+    // PCRD hull points (optional: none when scale is null). Per block, the points of the
+    // lower convex hull of its (rate, weighted distortion reduction) curve, computed with the
+    // host rate control's double arithmetic, so the host can take them in place of its own.
+    const double* scale;       // device, per block: its band's step^2 x weight
+    uint8_t* hullPasses;       // device, kMaxPasses per block: coding passes at each point
+    double* hullSlope;         // device, kMaxPasses per block: slope from the previous point
+    uint8_t* outHullPasses;    // packed at the pass offsets like outPassLen; a block's points
+    double* outHullSlope;      // end at its pass count or at the first 0 in outHullPasses
 };
 
 // The out* pointers and tot may be mapped host memory: the kernels only write them, with

@@ -58,6 +58,15 @@ uint64_t buildJobs(const Layout& L, const uint32_t* coeffs, uint8_t* sym, uint8_
     return region;
 }
 
+std::vector<double> blockScales(const Layout& L) {
+    std::vector<double> v((size_t)L.numCblks());
+    for (int i = 0; i < L.numCblks(); ++i) {
+        const GbSubband& b = L.bands[L.cblks[(size_t)i].band];
+        v[(size_t)i] = (double)b.delta * b.delta * b.weight;
+    }
+    return v;
+}
+
 void launchFrontEnd(const Layout& L, const ColorArgs& c, float* ll0, float* ll1, uint64_t llFloats, uint32_t* coeffs,
                     float* tap, cudaStream_t st) {
     const int NL = L.levels;

@@ -31,6 +31,10 @@ SlotSizes slotSizes(const Layout& L, const GbFrameFormat& in);
 uint64_t buildJobs(const Layout& L, const uint32_t* coeffs, uint8_t* sym, uint8_t* cw, uint32_t slope,
                    std::vector<T1Job>& jobs);
 
+// Per block, the weight of its Tier-1 distortions in the PCRD hull: its band's
+// step^2 x weight, in double (as the host rate control forms it).
+std::vector<double> blockScales(const Layout& L);
+
 // Enqueues the front end of one frame on st: colour + level 1 from c.src, then the deeper
 // levels through the LL ping-pong buffers (3 x llFloats each), quantised words into coeffs
 // (code-block-major), float planes into tap when not NULL.

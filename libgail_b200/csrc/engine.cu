@@ -34,6 +34,7 @@ struct EncodeEngine::Class {
     float* dEotf = nullptr;
     float* dThr = nullptr;
     float* dLL[2] = {nullptr, nullptr};
+    double* dScale = nullptr;  // per block: the hull's distortion weight
     uint64_t slotBytes = 0, dataCap = 0;
     std::vector<Slot*> free;
     std::vector<void*> dev;
@@ -50,6 +51,8 @@ struct EncodeEngine::Slot {
     uint32_t *hInfo = nullptr, *hLen = nullptr, *hTot = nullptr;
     int32_t* hDist = nullptr;
     uint8_t* hData = nullptr;
+    uint8_t* hHullPasses = nullptr;  // the PCRD hull points, packed like hLen
+    double* hHullSlope = nullptr;
     uint64_t dataCap = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -97,6 +100,8 @@ struct EncodeEngine::Batch {
     int32_t* dist = nullptr;
     uint4* snaps = nullptr;
     uint2* offs = nullptr;
+    uint8_t* hullPasses = nullptr;
+    double* hullSlope = nullptr;
     uint32_t cap = 0;
     std::vector<Request*> frames;
     bool busy = false;
@@ -178,6 +183,9 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
     alloc(c->dThr, 4096 * 4);
     alloc(c->dLL[0], c->z.llFloats * 12);
     alloc(c->dLL[1], c->z.llFloats * 12);
+    alloc(c->dScale, c->z.n * 8);
+    const std::vector<double> scales = blockScales(c->L);
+    GB_CHECK(cudaMemcpy(c->dScale, scales.data(), scales.size() * 8, cudaMemcpyHostToDevice));
     GB_CHECK(cudaMemcpy(c->dEotf, c->color.eotf.data(), 65536 * 4, cudaMemcpyHostToDevice));
     GB_CHECK(cudaMemcpy(c->dThr, c->color.thr.data(), 4096 * 4, cudaMemcpyHostToDevice));
     ColorArgs& a = c->colorArgs;
@@ -231,6 +239,8 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         mapped(s->hLen, (uint64_t)s->n * kMaxPasses * 4);
         mapped(s->hDist, (uint64_t)s->n * kMaxPasses * 4);
         mapped(s->hData, c.dataCap);
+        mapped(s->hHullPasses, (uint64_t)s->n * kMaxPasses);
+        mapped(s->hHullSlope, (uint64_t)s->n * kMaxPasses * 8);
         mapped(s->hTot, 64);
         s->dataCap = c.dataCap;
         std::vector<T1Job> jobs;
@@ -395,6 +405,16 @@ bool EncodeEngine::picture(int64_t id, const uint16_t** pix, int* width, int* he
     return true;
 }
 
+bool EncodeEngine::hull(int64_t id, const uint8_t** passes, const double** slope) {
+    std::lock_guard<std::mutex> lock(m_);
+    if (id < 0 || id >= (int64_t)requests_.size() || !requests_[id]) throw std::logic_error("unknown request");
+    const Request* r = requests_[id].get();
+    if (r->decode || !r->slot) return false;
+    *passes = r->slot->hHullPasses;
+    *slope = r->slot->hHullSlope;
+    return true;
+}
+
 // A decode request on a worker: parse, a decoder slot of its class (made when the budget
 // allows, else the next one released), decode on the slot's stream, hand out.
 void EncodeEngine::decodeJob(Request* r) {
@@ -505,7 +525,8 @@ void EncodeEngine::codestreamWorker() {
                 v.numInfo = s->n;
                 v.numPasses = s->hTot[1];
                 v.numData = s->hTot[0];
-                const RateResult rr = allocateRate(*w, v, dciLimits(cs_.fps, cs_.maxMbps, cs_.compMbps));
+                const HullView hull{s->hHullPasses, s->hHullSlope};  // computed on the GPU
+                const RateResult rr = allocateRate(*w, v, dciLimits(cs_.fps, cs_.maxMbps, cs_.compMbps), &hull);
                 w->build(v, rr.passes.data(), &r->cs, cs_.tag);
                 if (cs_.check) r->dciOk = checkDci(r->cs.data(), r->cs.size(), cs_.fps).ok ? 1 : 0;
             } catch (const std::exception&) {
@@ -600,6 +621,8 @@ bool EncodeEngine::launchBatch(Batch& b) {
         alloc(b.snaps, cap * kMaxPasses * 16);
         alloc(b.perm, cap * 4);
         alloc(b.offs, cap * 8);
+        alloc(b.hullPasses, cap * kMaxPasses);
+        alloc(b.hullSlope, cap * kMaxPasses * 8);
         alloc(b.ctl, 64);
         b.cap = (uint32_t)cap;
     }
@@ -624,8 +647,11 @@ bool EncodeEngine::launchBatch(Batch& b) {
         Slot* s = r->slot;
         std::memset(s->hTot, 0, 64);
         const uint32_t j = r->jobBase;
+        const Class& c = *classes_[r->cls];
         CompactArgs ca{s->n,   b.info + 4 * (uint64_t)j, b.len + (uint64_t)kMaxPasses * j, b.dist + (uint64_t)kMaxPasses * j,
-                       b.dJobs + j, s->hInfo, s->hLen, s->hDist, s->hData, s->hTot, s->dataCap, b.perm, b.offs, 1};
+                       b.dJobs + j, s->hInfo, s->hLen, s->hDist, s->hData, s->hTot, s->dataCap, b.perm, b.offs, 1,
+                       c.dScale, b.hullPasses + (uint64_t)kMaxPasses * j, b.hullSlope + (uint64_t)kMaxPasses * j,
+                       s->hHullPasses, s->hHullSlope};
         compactTier1(ca, b.st);
     }
     GB_CHECK(cudaMemcpyAsync(b.hCtl, b.ctl, 64, cudaMemcpyDeviceToHost, b.st));

@@ -84,6 +84,9 @@ public:
     // The picture of a finished decode (valid until release): height rows of width x 3
     // codes. False for an encode request.
     bool picture(int64_t id, const uint16_t** pix, int* width, int* height);
+    // The PCRD hull points of a finished encode (valid until release), computed on the GPU
+    // after Tier-1, in the HullView layout over its Tier-1 frame. False for a decode.
+    bool hull(int64_t id, const uint8_t** passes, const double** slope);
 
     struct Stats {
         uint64_t frames = 0, batches = 0, batchFrames = 0, slots = 0, slotBytes = 0;

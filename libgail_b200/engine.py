@@ -31,6 +31,8 @@ def _bind():
     L.gb_engine_submit_decode.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_int64)]
     L.gb_engine_picture.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_uint16)), C.POINTER(C.c_int),
                                     C.POINTER(C.c_int)]
+    L.gb_engine_hull.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_uint8)),
+                                 C.POINTER(C.POINTER(C.c_double))]
     L._engine_bound = True
     return L
 
@@ -113,6 +115,17 @@ class Engine:
         check(lib().gb_engine_picture(self.h, rid, C.byref(p), C.byref(w), C.byref(h)))
         a = np.ctypeslib.as_array(p, (h.value, w.value, 3))
         return a.copy() if copy else a
+
+    def hull(self, rid: int, num_passes: int, copy: bool = True):
+        """A finished encode's PCRD hull points computed on the GPU: (passes uint8, slope
+        float64), num_passes entries each (its Tier-1 frame's pass count), in the layout of
+        codestream.hull()."""
+        p, s = C.POINTER(C.c_uint8)(), C.POINTER(C.c_double)()
+        check(lib().gb_engine_hull(self.h, rid, C.byref(p), C.byref(s)))
+        if num_passes == 0:
+            return np.zeros(0, np.uint8), np.zeros(0, np.float64)
+        a, b = np.ctypeslib.as_array(p, (num_passes,)), np.ctypeslib.as_array(s, (num_passes,))
+        return (a.copy(), b.copy()) if copy else (a, b)
 
     def release(self, rid: int):
         check(lib().gb_engine_release(self.h, rid))

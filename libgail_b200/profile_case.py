@@ -1,7 +1,7 @@
 """Small, fixed encode cases for profiler captures.
 
   python -m libgail_b200.profile_case --path plain --frames 2
-  python -m libgail_b200.profile_case --path served --frames 8 --batch 8 [--size 2k]
+  python -m libgail_b200.profile_case --path served --frames 8 --batch 8 [--size 2k] [--repeat 3]
   python -m libgail_b200.profile_case --path decode --frames 2
 
 Encodes seeded synthetic frames that are already in device memory, through the plain
@@ -29,6 +29,7 @@ def main():
     ap.add_argument("--frames", type=int, default=2)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--size", choices=["4k", "2k"], default="4k")
+    ap.add_argument("--repeat", type=int, default=1, help="served: passes over the frames (the first warms up)")
     args = ap.parse_args()
 
     import torch
@@ -84,14 +85,19 @@ def main():
                 print(f"decode ms: t1 {tm.t1:.3f} dwt {tm.dwt:.3f} colour+download {tm.color:.3f} ({len(cs)} bytes)")
             dec.close()
         else:
+            import time
             eng = Engine(0, 0, max_batch=args.batch)
             cid, _ = eng.add_encoder(lay, fmt, col)
-            ids = [eng.submit(cid, f) for f in dframes]
-            for _ in ids:
-                rid, _, _, st = eng.wait(120000, copy=False)
-                if rid < 0 or st != 0:
-                    raise SystemExit(f"engine frame failed (id {rid}, status {st})")
-                eng.release(rid)
+            for rep in range(args.repeat):
+                t0 = time.perf_counter()
+                ids = [eng.submit(cid, f) for f in dframes]
+                for _ in ids:
+                    rid, _, _, st = eng.wait(120000, copy=False)
+                    if rid < 0 or st != 0:
+                        raise SystemExit(f"engine frame failed (id {rid}, status {st})")
+                    eng.release(rid)
+                dt = time.perf_counter() - t0
+                print(f"engine pass {rep}: {len(ids) / dt:.1f} frames/s (Tier-1 frames to host memory)")
             print("engine:", eng.stats())
             eng.close()
     finally:

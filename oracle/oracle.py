@@ -324,6 +324,8 @@ def _ref_bind(L):
     L.ref_build.restype = C.c_longlong
     L.ref_build.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                             C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64]
+    L.ref_hull.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                           C.c_uint64, C.c_void_p, C.c_void_p]
     L.ref_check_dci.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_char_p, C.c_uint64]
     L.ref_parse.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_int),
                             C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -386,6 +388,21 @@ def ref_codestream(ref: "Reference", width, height, fourk, t1, fps=24.0, mbps=23
     if size < 0:
         raise RuntimeError(ref.error())
     return bytes(cs[:size]), passes, lam.value, ms.value
+
+
+def ref_hull(ref: "Reference", width, height, fourk, t1, base_step=1.0):
+    """The reference's PCRD hull points (buildHull) per pass slot of the Tier-1 frame:
+    (passes uint8, slope float64), a block's points from its passBase on, then zeros."""
+    _ref_bind(ref.lib)
+    info = np.ascontiguousarray(t1.info, np.uint32)
+    pl = np.ascontiguousarray(t1.pass_len, np.uint32)
+    pd = np.ascontiguousarray(t1.pass_dist, np.int32)
+    passes = np.zeros(max(pl.size, 1), np.uint8)
+    slope = np.zeros(max(pl.size, 1), np.float64)
+    if ref.lib.ref_hull(width, height, int(fourk), C.c_double(base_step), _p(info), info.shape[0], _p(pl), _p(pd),
+                        pl.size, _p(passes), _p(slope)) != 0:
+        raise RuntimeError(ref.error())
+    return passes[: pl.size], slope[: pl.size]
 
 
 def ref_parse(ref: "Reference", cs: bytes, reduce=0):

@@ -30,6 +30,10 @@
 #include "core/thread_pool.h"
 #include "cuda/cuda_plugin.h"
 
+// The reference's rate control, compiled here rather than as its own object so that
+// ref_hull below can call its file-local buildHull.
+#include "core/rate_control.cpp"
+
 using namespace gail;
 
 // build_version.cpp needs a header the reference's CMake generates; a build from this
@@ -311,6 +315,32 @@ long long ref_rate_and_build(int width, int height, int fourk, double baseStep, 
         if (cs.size() > csCap) return -1;
         std::memcpy(csOut, cs.data(), cs.size());
         return (long long)cs.size();
+    } catch (const std::exception& ex) {
+        g_err = ex.what();
+        return -1;
+    }
+}
+
+// The reference's PCRD hull points (buildHull), laid out per pass slot of the Tier-1 frame:
+// block i's points from its passBase on, the entries after them passes 0, slope 0.
+// Returns 0, or -1.
+int ref_hull(int width, int height, int fourk, double baseStep, const uint32_t* info5, uint64_t n,
+             const uint32_t* passLen, const int32_t* passDist, uint64_t numPasses, uint8_t* passesOut,
+             double* slopeOut) {
+    try {
+        FrameLayout L = layoutOf(width, height, fourk, baseStep);
+        Tier1Frame t = tier1Of(info5, n, passLen, passDist, numPasses, nullptr, 0);
+        const Hull H = buildHull(L, t);
+        std::memset(passesOut, 0, numPasses);
+        std::memset(slopeOut, 0, numPasses * sizeof(double));
+        for (uint64_t i = 0; i < n; ++i) {
+            const uint32_t base = t.info[i].passBase;
+            for (uint32_t h = H.start[i]; h < H.start[i + 1]; ++h) {
+                passesOut[base + h - H.start[i]] = H.passes[h];
+                slopeOut[base + h - H.start[i]] = H.slope[h];
+            }
+        }
+        return 0;
     } catch (const std::exception& ex) {
         g_err = ex.what();
         return -1;

@@ -12,7 +12,7 @@ from libgail_b200 import codestream as CS
 from libgail_b200 import plugin as P
 from libgail_b200 import synth
 from oracle.oracle import (RefEncoder, Reference, _p, _ref_bind, have_reference, ref_check, ref_codestream,
-                           ref_parse)
+                           ref_hull, ref_parse)
 
 pytestmark = pytest.mark.skipif(not have_reference(), reason="reference CPU build (oracle/_ref) not present")
 
@@ -64,6 +64,43 @@ def test_rate_and_build_matches_reference(ref, frames, prof, mbps):
     ok, msg = CS.check_dci(got)
     assert ok, msg
     assert msg == LABEL + " cuda13.0"
+
+
+@pytest.mark.parametrize("prof", PROFILES)
+def test_hull_matches_reference(ref, frames, prof):
+    """The host PCRD hull points equal the reference's buildHull bit for bit (the pass
+    counts, and the slopes as IEEE bit patterns)."""
+    W, H, fk = prof
+    t1 = frames[prof]
+    passes, slope = CS.hull(P.LayoutHolder(W, H, fk), t1)
+    wp, ws = ref_hull(ref, W, H, fk, t1)
+    assert np.array_equal(passes, wp)
+    assert np.array_equal(slope.view(np.uint64), ws.view(np.uint64))
+    assert (passes > 0).sum() > len(t1.info)  # blocks with several points
+
+
+@pytest.mark.parametrize("prof", PROFILES)
+def test_rate_and_build_with_given_hull(ref, frames, prof):
+    """Rate control fed the hull points (as the engine feeds it those computed on the GPU)
+    gives the same codestream as computing them; a malformed hull is refused."""
+    W, H, fk = prof
+    t1 = frames[prof]
+    lay = P.LayoutHolder(W, H, fk)
+    hp, hs = CS.hull(lay, t1)
+    for mbps in (230.0, 90.0):
+        want = CS.rate_and_build(lay, t1, max_mbps=mbps, tag="cuda13.0")
+        got = CS.rate_and_build(lay, t1, max_mbps=mbps, tag="cuda13.0", hull_points=(hp, hs))
+        assert got[0] == want[0] and np.array_equal(got[1], want[1]) and got[2] == want[2]
+    b = int(np.argmax(t1.info[:, 1] >= 2))  # a block with two or more passes
+    base = int(t1.info[b, 4])
+    bad = hp.copy()
+    bad[base], bad[base + 1] = 2, 1  # pass counts not increasing
+    with pytest.raises(P.GailError):
+        CS.rate_and_build(lay, t1, hull_points=(bad, hs))
+    bad = hp.copy()
+    bad[base] = t1.info[b, 1] + 1  # beyond the block's passes
+    with pytest.raises(P.GailError):
+        CS.rate_and_build(lay, t1, hull_points=(bad, hs))
 
 
 @pytest.mark.parametrize("prof", PROFILES)

@@ -1,7 +1,8 @@
 """The batched, served encoder: every frame's Tier-1 frame must be the same whether it was
 encoded alone through the plain per-frame path (the plugin's encoder_encode) or in a mix
-of frames of all six DCI profiles batched into shared Tier-1 launches, and the admission
-by HBM budget must let every request finish."""
+of frames of all six DCI profiles batched into shared Tier-1 launches, its PCRD hull points
+computed on the GPU must equal the host's, and the admission by HBM budget must let every
+request finish."""
 import numpy as np
 import pytest
 
@@ -13,6 +14,15 @@ from libgail_b200.engine import Engine
 def _same(a: P.Tier1Frame, b: P.Tier1Frame):
     return (np.array_equal(a.info, b.info) and np.array_equal(a.pass_len, b.pass_len)
             and np.array_equal(a.pass_dist, b.pass_dist) and np.array_equal(a.data, b.data))
+
+
+def _same_hull(eng, rid, layout, t1):
+    """The PCRD hull points the engine computed on the GPU equal the host's (themselves
+    pinned to the reference's buildHull) bit for bit."""
+    from libgail_b200 import codestream as CS
+    gp, gs = eng.hull(rid, len(t1.pass_len))
+    hp, hs = CS.hull(layout, t1)
+    return np.array_equal(gp, hp) and np.array_equal(gs.view(np.uint64), hs.view(np.uint64))
 
 
 @pytest.fixture(scope="module")
@@ -55,15 +65,18 @@ def test_engine_mix_equals_alone(dev):
         want = {}
         order = [(ci, fi) for fi in range(3) for ci in range(len(cases)) if fi < len(cases[ci][3])]
         assert sum(len(c[3]) for c in cases[:6]) == 16
+        lay_of = {}
         for ci, fi in order:  # interleaved profiles
             rid = eng.submit(classes[ci], cases[ci][3][fi])
             want[rid] = alone[ci][fi]
+            lay_of[rid] = layouts[ci]
         got = 0
         while got < len(want):
             rid, t1, lat, st = eng.wait(60000)
             assert rid >= 0, "timed out"
             assert st == 0
             assert _same(t1, want[rid]), f"request {rid} differs from its plain encode"
+            assert _same_hull(eng, rid, lay_of[rid], t1), f"request {rid}: GPU hull differs from the host's"
             eng.release(rid)
             got += 1
         s = eng.stats()
@@ -131,6 +144,7 @@ def test_engine_codestreams(dev):
             cs, ok = eng.codestream(rid)
             ci, fi = want[rid]
             assert _same(t1, alone[ci][fi])
+            assert _same_hull(eng, rid, layouts[ci], t1)
             host, _, _ = CS.rate_and_build(layouts[ci], alone[ci][fi], fps=24.0, label=CS.DEFAULT_LABEL, tag="b200")
             assert cs == host
             assert ok == 1 and CS.check_dci(cs)[0]
