@@ -20,8 +20,12 @@
 // instead of idling while its warp-mates finish. The coder is in branch-free
 // select form (both MPS and LPS take the same instruction path until renormalisation),
 // its contexts live in shared memory, and its input is prefetched 16 decisions ahead.
-// After the flush, each pass's truncation length is computed from the MQ state recorded
-// at its end and the final codeword bytes.
+// The MQ state at each pass's end is recorded.
+//
+// Stage 4, truncation lengths (t1TruncKernel): a warp per block, a lane per pass; each
+// pass's length is found from its recorded MQ state and the final codeword bytes. Kept
+// out of the MQ kernel, whose lanes would otherwise stall on these byte reads one block
+// end at a time while their warp-mates code.
 //
 // Semantics restated from ISO/IEC 15444-1 Annexes C and D as the reference coder applies
 // them (Josephur/libgail core/t1_ref.cpp:52-292, kernels/mq_encoder.h:48-169,
@@ -635,13 +639,7 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
                 }
                 const uint32_t len = e.flush();
                 if (e.overflow) atomicOr(status, kErrCodewordSpace);
-                uint32_t prev = 1;
-                for (uint32_t q = 0; q < np; ++q) {
-                    const uint32_t L =
-                        q == np - 1 ? len : truncLen(P.snaps[(size_t)job * kMaxPasses + q], e.out, min(len, e.cap), prev);
-                    P.passLen[(size_t)job * kMaxPasses + q] = L;
-                    prev = max(prev, L);
-                }
+                // the truncation lengths are found afterwards, by t1TruncKernel
                 P.info[4 * (size_t)job + 3] = e.overflow ? 0u : len;
                 have = false;
                 soloJob = false;
@@ -704,6 +702,41 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
     }
 }
 
+// Truncation lengths, a warp per block after MQ coding: lane q finds the shortest prefix
+// for pass q from the MQ state recorded at its end, as if no earlier pass constrained it;
+// lane 0 then walks the passes in order and, where a pass's shortest prefix is shorter
+// than an earlier pass's length, searches again from that length (the lengths of a
+// block never decrease). The last pass takes the whole codeword.
+constexpr int TRUNC_THREADS = 256;
+
+__global__ void __launch_bounds__(TRUNC_THREADS) t1TruncKernel(T1Launch P) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (TRUNC_THREADS / 32);
+    for (uint32_t job = blockIdx.x * (TRUNC_THREADS / 32) + (threadIdx.x >> 5); job < P.n; job += warps) {
+        const uint32_t np = P.info[4 * (size_t)job + 1], len = P.info[4 * (size_t)job + 3];
+        if (np == 0 || len == 0) continue;  // nothing coded, or an overflow already reported
+        const uint8_t* cw = P.jobs[job].cw;
+        const size_t base = (size_t)job * kMaxPasses;
+        uint32_t c0 = 0, c1 = 0;  // the unconstrained lengths of passes lane and lane + 32
+        if ((uint32_t)lane + 1 < np) c0 = truncLen(P.snaps[base + lane], cw, len, 1);
+        if ((uint32_t)lane + 33 < np) c1 = truncLen(P.snaps[base + lane + 32], cw, len, 1);
+        uint32_t prev = 1, mine0 = 0, mine1 = 0;
+        for (uint32_t q = 0; q < np; ++q) {
+            const uint32_t c = __shfl_sync(kFull, q < 32 ? c0 : c1, q & 31);
+            uint32_t L = len;
+            if (q + 1 < np) {
+                L = c;
+                if (L < prev && lane == 0) L = truncLen(P.snaps[base + q], cw, len, prev);
+                L = __shfl_sync(kFull, L, 0);
+            }
+            if ((q & 31) == (uint32_t)lane) (q < 32 ? mine0 : mine1) = L;
+            prev = max(prev, L);
+        }
+        if ((uint32_t)lane < np) P.passLen[base + lane] = mine0;
+        if ((uint32_t)lane + 32 < np) P.passLen[base + lane + 32] = mine1;
+    }
+}
+
 }  // namespace
 
 cudaError_t kernelsLoadable() {
@@ -738,6 +771,7 @@ void t1Encode(const T1Launch& launch, cudaStream_t st, cudaEvent_t* marks) {
     if (marks) GB_CHECK(cudaEventRecord(marks[1], st));
     if (mqBlocks <= (uint32_t)sms * 4u) t1MqKernel<1><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
     else t1MqKernel<12><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
+    t1TruncKernel<<<min(divUp(L.n, (uint32_t)(TRUNC_THREADS / 32)), (uint32_t)sms * 8u), TRUNC_THREADS, 0, st>>>(L);
     GB_CHECK(cudaGetLastError());
 }
 
