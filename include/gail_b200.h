@@ -194,6 +194,11 @@ GB_API int gb_engine_hull(GbEngine* e, int64_t id, const uint8_t** passes, const
  *                              src/core/rate_control.cpp:38-86): hullPasses/hullSlope as
  *                              gb_tier1_hull lays them out, e.g. from gb_engine_hull; the
  *                              result is the same as gb_rate_and_build's
+ *   gb_device_rate_and_build   gb_rate_and_build on a GPU: the Tier-1 frame (host memory) is
+ *                              uploaded; its hull points, slope histogram, every size
+ *                              measurement of the threshold search and the final packets are
+ *                              computed there (the host runs only the search over a few numbers
+ *                              per measurement); the same codestream, passes and lambda
  *   gb_tier1_hull              the hull points on the host: per pass slot of the Tier-1 frame
  *                              (numPasses entries), block i's points from its passBase on, in
  *                              order, each the coding passes at the point and the slope from
@@ -218,6 +223,9 @@ GB_API int gb_rate_and_build_hull(const GailCudaLayout* layout, const GailCudaTi
                                   const double* hullSlope, double fps, double maxMbps, double compMbps,
                                   const char* label, const char* tag, uint8_t* passesOut, uint8_t* out, uint64_t cap,
                                   uint64_t* size, double* lambda);
+GB_API int gb_device_rate_and_build(int device, const GailCudaLayout* layout, const GailCudaTier1* t1, double fps,
+                                    double maxMbps, double compMbps, const char* label, const char* tag,
+                                    uint8_t* passesOut, uint8_t* out, uint64_t cap, uint64_t* size, double* lambda);
 GB_API int gb_tier1_hull(const GailCudaLayout* layout, const GailCudaTier1* t1, uint8_t* passes, double* slope);
 GB_API int gb_check_dci(const uint8_t* data, uint64_t size, double fps, char* msg, uint64_t msgCap, int* ok);
 GB_API int gb_parse_codestream(const uint8_t* data, uint64_t size, GbSubband* bands, int maxBands, int* numBands,

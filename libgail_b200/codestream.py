@@ -28,6 +28,9 @@ def _bind():
     L.gb_rate_and_build_hull.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                          C.c_double, C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint64, u64p,
                                          C.POINTER(C.c_double)]
+    L.gb_device_rate_and_build.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                           C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint64, u64p,
+                                           C.POINTER(C.c_double)]
     L.gb_tier1_hull.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.gb_check_dci.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_char_p, C.c_uint64, C.POINTER(C.c_int)]
     L.gb_parse_codestream.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,
@@ -108,6 +111,21 @@ def rate_and_build(layout: LayoutHolder, t1, fps: float = 24.0, max_mbps: float 
     check(L.gb_rate_and_build_hull(C.byref(layout.abi), C.byref(t.abi), None if hp is None else hp.ctypes.data,
                                    None if hs is None else hs.ctypes.data, fps, max_mbps, comp_mbps, label.encode(),
                                    tag.encode(), passes.ctypes.data, out.ctypes.data, cap, C.byref(n), C.byref(lam)))
+    return out[: n.value].tobytes(), passes, lam.value
+
+
+def device_rate_and_build(layout: LayoutHolder, t1, fps: float = 24.0, max_mbps: float = 230.0,
+                          comp_mbps: float = 200.0, label: str = DEFAULT_LABEL, tag: str = "", device: int = 0):
+    """rate_and_build on a GPU (hull, slope histogram, size measurements and packets
+    computed there): (codestream bytes, passes per block, lambda), the same as rate_and_build."""
+    L, t = _bind(), _t1(t1)
+    passes = np.zeros(layout.abi.numCblks, np.uint8)
+    cap = 1 << 22
+    out = np.empty(cap, np.uint8)
+    n, lam = C.c_uint64(), C.c_double()
+    check(L.gb_device_rate_and_build(device, C.byref(layout.abi), C.byref(t.abi), fps, max_mbps, comp_mbps,
+                                     label.encode(), tag.encode(), passes.ctypes.data, out.ctypes.data, cap,
+                                     C.byref(n), C.byref(lam)))
     return out[: n.value].tobytes(), passes, lam.value
 
 

@@ -11,6 +11,7 @@
 #include "codestream.h"
 #include "gail_b200.h"
 #include "layout.h"
+#include "rate_gpu.h"
 
 using namespace gb;
 
@@ -130,6 +131,66 @@ GB_API int gb_rate_and_build(const GailCudaLayout* layout, const GailCudaTier1* 
                              uint64_t cap, uint64_t* size, double* lambda) {
     return gb_rate_and_build_hull(layout, t1, nullptr, nullptr, fps, maxMbps, compMbps, label, tag, passesOut, out,
                                   cap, size, lambda);
+}
+
+GB_API int gb_device_rate_and_build(int device, const GailCudaLayout* layout, const GailCudaTier1* t1, double fps,
+                                    double maxMbps, double compMbps, const char* label, const char* tag,
+                                    uint8_t* passesOut, uint8_t* out, uint64_t cap, uint64_t* size, double* lambda) {
+    return gbGuard([&] {
+        if (!layout || !t1 || !size) throw std::logic_error("null argument");
+        checkTier1(*layout, *t1);
+        int count = 0;
+        GB_CHECK(cudaGetDeviceCount(&count));
+        if (device < 0 || device >= count) throw std::logic_error("no such device");
+        GB_CHECK(cudaSetDevice(device));
+        ensureDevice();
+        // a device rate control per (calling thread, device, layout, label), on its own stream
+        struct Cached {
+            int device = -1;
+            GailCudaLayout key{};
+            std::vector<GbSubband> bands;
+            std::string label;
+            std::unique_ptr<DeviceRateControl> rc;
+            cudaStream_t st = nullptr;
+            ~Cached() {
+                rc.reset();
+                if (st) cudaStreamDestroy(st);
+            }
+        };
+        thread_local Cached c;
+        const std::string lab = label ? label : "";
+        const bool same = c.rc && c.device == device && c.key.profile == layout->profile &&
+                          c.key.width == layout->width && c.key.height == layout->height &&
+                          c.key.levels == layout->levels && c.key.guardBits == layout->guardBits &&
+                          c.key.numBands == layout->numBands && c.key.baseStep == layout->baseStep && c.label == lab &&
+                          std::memcmp(c.bands.data(), layout->bands, sizeof(GbSubband) * (size_t)layout->numBands) == 0;
+        if (!same) {
+            c.rc.reset();
+            if (c.st && c.device != device) {
+                cudaStreamDestroy(c.st);
+                c.st = nullptr;
+            }
+            Layout L;
+            layoutFromAbi(*layout, L);
+            c.rc = std::make_unique<DeviceRateControl>(device, L, lab);
+            if (!c.st) GB_CHECK(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
+            c.device = device;
+            c.key = *layout;
+            c.bands.assign(layout->bands, layout->bands + layout->numBands);
+            c.label = lab;
+        }
+        const RateLimits lim = dciLimits(fps, maxMbps, compMbps);
+        if (c.rc->emptyBytes() > lim.maxTotal) throw std::logic_error("the frame budget is below the smallest codestream");
+        thread_local std::vector<uint8_t> cs;
+        const RateResult rr = c.rc->runHost(viewOf(*t1), lim, tag ? tag : "", cs, c.st);
+        *size = cs.size();
+        if (lambda) *lambda = rr.lambda;
+        if (passesOut) std::memcpy(passesOut, rr.passes.data(), rr.passes.size());
+        if (out) {
+            if (cs.size() > cap) throw std::logic_error("codestream buffer too small");
+            std::memcpy(out, cs.data(), cs.size());
+        }
+    });
 }
 
 GB_API int gb_tier1_hull(const GailCudaLayout* layout, const GailCudaTier1* t1, uint8_t* passes, double* slope) {

@@ -9,6 +9,7 @@
 // so that the same passes are chosen), and the DCI rules of its checker
 // (codestream_check.cpp:43-280).
 #include "codestream.h"
+#include "rate_search.h"
 
 #include "pool.h"
 
@@ -545,14 +546,9 @@ CodestreamSizes CodestreamWriter::measure(const Tier1View& t1, const uint8_t* pa
             for (int q = b; q < e; ++q) pkBytes_[(size_t)todo[(size_t)q]] = (uint32_t)packet(todo[(size_t)q], t1, passes, nullptr);
         });
     }
-    if (!hdrLongest_) {
-        std::vector<uint8_t> hdr;
-        mainHeader(hdr, label_ + std::string(1 + kMaxDeviceTagBytes, ' '));
-        hdrLongest_ = hdr.size();
-    }
     CodestreamSizes sz;
     sz.numTileParts = ntp_;
-    size_t total = hdrLongest_;
+    size_t total = longestHeaderBytes();
     for (int tp = 0; tp < ntp_; ++tp) {
         size_t bytes = 14;
         for (int p = tpStart_[tp]; p < tpStart_[tp + 1]; ++p) bytes += pkBytes_[(size_t)p];
@@ -561,6 +557,50 @@ CodestreamSizes CodestreamWriter::measure(const Tier1View& t1, const uint8_t* pa
         total += bytes;
     }
     sz.total = total + 2;
+    return sz;
+}
+
+size_t CodestreamWriter::longestHeaderBytes() {
+    if (!hdrLongest_) {
+        std::vector<uint8_t> hdr;
+        mainHeader(hdr, label_ + std::string(1 + kMaxDeviceTagBytes, ' '));
+        hdrLongest_ = hdr.size();
+    }
+    return hdrLongest_;
+}
+
+CodestreamSizes CodestreamWriter::assemble(const uint8_t* body, const uint64_t* tpBytes, const std::string& tag,
+                                           std::vector<uint8_t>& out) const {
+    if (tag.size() > kMaxDeviceTagBytes) throw std::logic_error("device tag \"" + tag + "\" is too long");
+    const std::string comment = tag.empty() ? label_ : label_ + " " + tag;
+    const size_t slack = label_.size() + 1 + kMaxDeviceTagBytes - comment.size();
+    out.clear();
+    mainHeader(out, comment);
+    const size_t hdr = out.size(), tlmAt = hdr - 5 * (size_t)ntp_;
+    CodestreamSizes sz;
+    sz.numTileParts = ntp_;
+    size_t body_ = 0;
+    for (int tp = 0; tp < ntp_; ++tp) {
+        if (tpBytes[tp] < 14 || tpBytes[tp] > 0xFFFFFFFFull) throw std::logic_error("tile-part size out of range");
+        sz.tilePart[tp] = tpBytes[tp];
+        sz.comp[tp % 3] += tpBytes[tp];
+        body_ += tpBytes[tp];
+    }
+    out.resize(hdr + body_ + 2);
+    uint8_t* d = out.data();
+    std::memcpy(d + hdr, body, body_);
+    size_t pos = hdr;
+    for (int tp = 0; tp < ntp_; ++tp) {
+        const uint32_t psot = (uint32_t)tpBytes[tp];
+        const uint8_t sot[14] = {0xFF, 0x90, 0, 10, 0, 0, (uint8_t)(psot >> 24), (uint8_t)(psot >> 16),
+                                 (uint8_t)(psot >> 8), (uint8_t)psot, (uint8_t)tp, (uint8_t)ntp_, 0xFF, 0x93};
+        std::memcpy(d + pos, sot, 14);
+        for (int k = 0; k < 4; ++k) d[tlmAt + 5 * tp + 1 + k] = (uint8_t)(psot >> (24 - 8 * k));
+        pos += psot;
+    }
+    d[hdr + body_] = 0xFF;  // EOC
+    d[hdr + body_ + 1] = 0xD9;
+    sz.total = out.size() + slack;
     return sz;
 }
 
@@ -730,60 +770,144 @@ Hull hullFromView(const Layout& L, const Tier1View& t1, const HullView& v) {
     return H;
 }
 
-// Per component, the hull points binned by log2(slope) (1/1024 octave): the data bytes
-// and the number of blocks included above each bin, so the size model costs O(1).
-class SlopeBins {
-public:
-    SlopeBins(const Layout& L, const Hull& H, double lo, double hi) : lo_(lo) {
-        nb_ = std::max(16, (int)std::ceil((hi - lo) * kPerOctave) + 2);
-        for (int c = 0; c < 3; ++c) {
-            bytes_[c].assign((size_t)nb_ + 1, 0.0);
-            blocks_[c].assign((size_t)nb_ + 1, 0.0);
-        }
-        // the bin of every hull point in parallel (the log2 is the cost); the sums of
-        // integer-valued doubles below are exact in any order
-        std::vector<int> binOf(H.slots);
-        forChunks(L.numCblks(), [&](int b, int e) {
-            for (int i = b; i < e; ++i)
-                for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h) binOf[h] = bin(H.slope[h]);
-        });
-        for (int i = 0; i < L.numCblks(); ++i) {
-            const int c = L.bands[L.cblks[(size_t)i].band].comp;
-            uint32_t prev = 0;
-            for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h) {
-                const int b = binOf[h];
-                bytes_[c][(size_t)b] += (double)H.rate[h] - prev;
-                if (h == H.first[(size_t)i]) blocks_[c][(size_t)b] += 1;
-                prev = H.rate[h];
-            }
-        }
-        for (int c = 0; c < 3; ++c)  // totals over the bins at or above each
-            for (int b = nb_ - 1; b >= 0; --b) {
-                bytes_[c][(size_t)b] += bytes_[c][(size_t)b + 1];
-                blocks_[c][(size_t)b] += blocks_[c][(size_t)b + 1];
-            }
-    }
-    void at(const double lam[3], double bytes[3], double blocks[3]) const {
-        for (int c = 0; c < 3; ++c) {
-            const int b = lam[c] <= 0 ? 0 : std::min(nb_, bin(lam[c]));
-            bytes[c] = bytes_[c][(size_t)b];
-            blocks[c] = blocks_[c][(size_t)b];
+// The hull points into the bins: the bin of every point in parallel (the log2 is the
+// cost), then the sums of integer-valued doubles, exact in any order.
+void binHull(const Layout& L, const Hull& H, SlopeBins& bins) {
+    std::vector<int> binOf(H.slots);
+    forChunks(L.numCblks(), [&](int b, int e) {
+        for (int i = b; i < e; ++i)
+            for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h) binOf[h] = bins.bin(H.slope[h]);
+    });
+    for (int i = 0; i < L.numCblks(); ++i) {
+        const int c = L.bands[L.cblks[(size_t)i].band].comp;
+        uint32_t prev = 0;
+        for (uint32_t h = H.first[(size_t)i]; h < H.end((size_t)i); ++h) {
+            bins.add(c, binOf[h], (double)H.rate[h] - prev, h == H.first[(size_t)i] ? 1.0 : 0.0);
+            prev = H.rate[h];
         }
     }
-
-private:
-    static constexpr double kPerOctave = 1024;
-    int bin(double slope) const {
-        if (!std::isfinite(slope)) return nb_ - 1;
-        const int b = (int)std::floor((std::log2(slope) - lo_) * kPerOctave);
-        return std::clamp(b, 0, nb_ - 1);
-    }
-    double lo_;
-    int nb_ = 0;
-    std::vector<double> bytes_[3], blocks_[3];
-};
+    bins.finish();
+}
 
 }  // namespace
+
+SlopeBins::SlopeBins(double lo, double hi) : lo_(lo) {
+    nb_ = std::max(16, (int)std::ceil((hi - lo) * kPerOctave) + 2);
+    for (int c = 0; c < 3; ++c) {
+        bytes_[c].assign((size_t)nb_ + 1, 0.0);
+        blocks_[c].assign((size_t)nb_ + 1, 0.0);
+    }
+}
+
+int SlopeBins::bin(double slope) const {
+    if (!std::isfinite(slope)) return nb_ - 1;
+    const int b = (int)std::floor((std::log2(slope) - lo_) * kPerOctave);
+    return std::clamp(b, 0, nb_ - 1);
+}
+
+void SlopeBins::finish() {
+    for (int c = 0; c < 3; ++c)
+        for (int b = nb_ - 1; b >= 0; --b) {
+            bytes_[c][(size_t)b] += bytes_[c][(size_t)b + 1];
+            blocks_[c][(size_t)b] += blocks_[c][(size_t)b + 1];
+        }
+}
+
+void SlopeBins::at(const double lam[3], double bytes[3], double blocks[3]) const {
+    for (int c = 0; c < 3; ++c) {
+        const int b = lam[c] <= 0 ? 0 : std::min(nb_, bin(lam[c]));
+        bytes[c] = bytes_[c][(size_t)b];
+        blocks[c] = blocks_[c][(size_t)b];
+    }
+}
+
+void slopeBounds(double& minSlope, double& maxSlope, double& lo, double& hi) {
+    if (maxSlope == 0) maxSlope = minSlope = 1;
+    lo = std::log2(minSlope) - 1;
+    hi = std::log2(maxSlope) + 1;
+}
+
+void rateSearch(const RateLimits& lim, double minSlope, double maxSlope, double loBound, double hiBound,
+                const SlopeBins& bins, const MeasureFn& measure, double lam[3], CodestreamSizes& sz) {
+    sz = measure(lam);
+    // size model per component: header bytes ~ calibrated + beta * (blocks included - calibrated)
+    double hdrCal[3], blkCal[3], beta[3];
+    auto calibrate = [&](const double l[3], const CodestreamSizes& ex) {
+        double bytes[3], blocks[3];
+        bins.at(l, bytes, blocks);
+        for (int c = 0; c < 3; ++c) {
+            hdrCal[c] = (double)ex.comp[c] - bytes[c];
+            blkCal[c] = blocks[c];
+            beta[c] = blocks[c] > 0 ? std::max(1.0, std::min(8.0, hdrCal[c] / blocks[c])) : 3.0;
+        }
+    };
+    auto model = [&](const double l[3], double comp[3]) {
+        double bytes[3], blocks[3];
+        bins.at(l, bytes, blocks);
+        double tot = (double)(sz.total - sz.comp[0] - sz.comp[1] - sz.comp[2]);  // main header, EOC
+        for (int c = 0; c < 3; ++c) {
+            comp[c] = bytes[c] + hdrCal[c] + beta[c] * (blocks[c] - blkCal[c]);
+            tot += comp[c];
+        }
+        return tot;
+    };
+    // the smallest log2 threshold in [lo, hi] for which fits() holds, by bisection
+    auto search = [](auto fits, double lo, double hi) {
+        for (int it = 0; it < 48 && hi - lo > 1e-5; ++it) {
+            const double mid = 0.5 * (lo + hi);
+            if (fits(mid)) hi = mid;
+            else lo = mid;
+        }
+        return hi;
+    };
+
+    if (sz.total > lim.maxTotal) {
+        calibrate(lam, sz);
+        const double target = (double)lim.maxTotal;
+        for (int round = 0; round < 6; ++round) {
+            const double lg = search(
+                [&](double m) {
+                    const double l = std::exp2(m), ll[3] = {l, l, l};
+                    double comp[3];
+                    return model(ll, comp) <= target;
+                },
+                loBound, hiBound);
+            lam[0] = lam[1] = lam[2] = std::exp2(lg);
+            sz = measure(lam);
+            if (sz.total <= lim.maxTotal && sz.total + lim.maxTotal / 500 >= lim.maxTotal) break;
+            calibrate(lam, sz);
+        }
+        // raise the thresholds in small steps until the exact size fits; past the steepest
+        // slope nothing more can be dropped
+        while (sz.total > lim.maxTotal && lam[0] <= maxSlope) {
+            for (int c = 0; c < 3; ++c) lam[c] = lam[c] > 0 ? lam[c] * 1.002 : minSlope;
+            sz = measure(lam);
+        }
+    }
+    for (int c = 0; c < kNumComps; ++c) {  // each component under its own cap
+        if (sz.comp[c] <= lim.maxComp) continue;
+        calibrate(lam, sz);
+        for (int round = 0; round < 6; ++round) {
+            const double lg = search(
+                [&](double m) {
+                    double ll[3] = {lam[0], lam[1], lam[2]};
+                    ll[c] = std::exp2(m);
+                    double comp[3];
+                    model(ll, comp);
+                    return comp[c] <= (double)lim.maxComp;
+                },
+                std::log2(std::max(lam[c], minSlope)), hiBound);
+            lam[c] = std::exp2(lg);
+            sz = measure(lam);
+            if (sz.comp[c] <= lim.maxComp && sz.comp[c] + lim.maxComp / 500 >= lim.maxComp) break;
+            calibrate(lam, sz);
+        }
+        while (sz.comp[c] > lim.maxComp && lam[c] <= maxSlope) {
+            lam[c] = lam[c] > 0 ? lam[c] * 1.002 : minSlope;
+            sz = measure(lam);
+        }
+    }
+}
 
 void computeHull(const Layout& L, const Tier1View& t1, uint8_t* passes, double* slope) {
     const HullOut out{passes, slope, nullptr, nullptr, nullptr, nullptr};
@@ -845,88 +969,13 @@ RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimi
             minSlope = std::min(minSlope, mn[c]);
         }
     }
-    if (maxSlope == 0) maxSlope = minSlope = 1;
-    const double loBound = std::log2(minSlope) - 1, hiBound = std::log2(maxSlope) + 1;
-    const SlopeBins bins(L, H, loBound, hiBound);
+    double loBound, hiBound;
+    slopeBounds(minSlope, maxSlope, loBound, hiBound);
+    SlopeBins bins(loBound, hiBound);
+    binHull(L, H, bins);
 
-    CodestreamSizes sz = measure(lam);
-    // size model per component: header bytes ~ calibrated + beta * (blocks included - calibrated)
-    double hdrCal[3], blkCal[3], beta[3];
-    auto calibrate = [&](const double l[3], const CodestreamSizes& ex) {
-        double bytes[3], blocks[3];
-        bins.at(l, bytes, blocks);
-        for (int c = 0; c < 3; ++c) {
-            hdrCal[c] = (double)ex.comp[c] - bytes[c];
-            blkCal[c] = blocks[c];
-            beta[c] = blocks[c] > 0 ? std::max(1.0, std::min(8.0, hdrCal[c] / blocks[c])) : 3.0;
-        }
-    };
-    auto model = [&](const double l[3], double comp[3]) {
-        double bytes[3], blocks[3];
-        bins.at(l, bytes, blocks);
-        double tot = (double)(sz.total - sz.comp[0] - sz.comp[1] - sz.comp[2]);  // main header, EOC
-        for (int c = 0; c < 3; ++c) {
-            comp[c] = bytes[c] + hdrCal[c] + beta[c] * (blocks[c] - blkCal[c]);
-            tot += comp[c];
-        }
-        return tot;
-    };
-    // the smallest log2 threshold in [lo, hi] for which fits() holds, by bisection
-    auto search = [](auto fits, double lo, double hi) {
-        for (int it = 0; it < 48 && hi - lo > 1e-5; ++it) {
-            const double mid = 0.5 * (lo + hi);
-            if (fits(mid)) hi = mid;
-            else lo = mid;
-        }
-        return hi;
-    };
-
-    if (sz.total > lim.maxTotal) {
-        calibrate(lam, sz);
-        const double target = (double)lim.maxTotal;
-        for (int round = 0; round < 6; ++round) {
-            const double lg = search(
-                [&](double m) {
-                    const double l = std::exp2(m), ll[3] = {l, l, l};
-                    double comp[3];
-                    return model(ll, comp) <= target;
-                },
-                loBound, hiBound);
-            lam[0] = lam[1] = lam[2] = std::exp2(lg);
-            sz = measure(lam);
-            if (sz.total <= lim.maxTotal && sz.total + lim.maxTotal / 500 >= lim.maxTotal) break;
-            calibrate(lam, sz);
-        }
-        // raise the thresholds in small steps until the exact size fits; past the steepest
-        // slope nothing more can be dropped
-        while (sz.total > lim.maxTotal && lam[0] <= maxSlope) {
-            for (double& l : lam) l = l > 0 ? l * 1.002 : minSlope;
-            sz = measure(lam);
-        }
-    }
-    for (int c = 0; c < kNumComps; ++c) {  // each component under its own cap
-        if (sz.comp[c] <= lim.maxComp) continue;
-        calibrate(lam, sz);
-        for (int round = 0; round < 6; ++round) {
-            const double lg = search(
-                [&](double m) {
-                    double ll[3] = {lam[0], lam[1], lam[2]};
-                    ll[c] = std::exp2(m);
-                    double comp[3];
-                    model(ll, comp);
-                    return comp[c] <= (double)lim.maxComp;
-                },
-                std::log2(std::max(lam[c], minSlope)), hiBound);
-            lam[c] = std::exp2(lg);
-            sz = measure(lam);
-            if (sz.comp[c] <= lim.maxComp && sz.comp[c] + lim.maxComp / 500 >= lim.maxComp) break;
-            calibrate(lam, sz);
-        }
-        while (sz.comp[c] > lim.maxComp && lam[c] <= maxSlope) {
-            lam[c] = lam[c] > 0 ? lam[c] * 1.002 : minSlope;
-            sz = measure(lam);
-        }
-    }
+    CodestreamSizes sz;
+    rateSearch(lim, minSlope, maxSlope, loBound, hiBound, bins, measure, lam, sz);
     res.lambda = std::max({lam[0], lam[1], lam[2]});
     for (int c = 0; c < 3; ++c) res.lambdaComp[c] = lam[c];
     double dist = H.gain.empty() ? NAN : 0.0;

@@ -67,10 +67,25 @@ public:
     const std::string& label() const { return label_; }
     int numPackets() const { return (int)pkStart_.size() - 1; }
 
-private:
+    // The packet structure, for writers elsewhere (the device Tier-2): the segments (one
+    // precinct-band each) of packet p are [packetSegments()[p], packetSegments()[p + 1]);
+    // the packets of tile-part t are [tilePartPackets()[t], tilePartPackets()[t + 1]).
     struct Seg {  // one precinct-band of a packet
         int32_t band, cbx0, cby0, ncbx, ncby;
     };
+    const std::vector<Seg>& segments() const { return segs_; }
+    const std::vector<int32_t>& packetSegments() const { return pkStart_; }
+    const std::vector<int32_t>& tilePartPackets() const { return tpStart_; }
+    int numTileParts() const { return ntp_; }
+    // The main header with the longest comment the label allows (what sizes budget for).
+    size_t longestHeaderBytes();
+    // The codestream around packets written elsewhere. body: the tile-parts back to back,
+    // each 14 bytes of room for its SOT segment and SOD, then its packets; tpBytes: each
+    // tile-part's bytes (those 14 included). Returns the sizes as build() reports them.
+    CodestreamSizes assemble(const uint8_t* body, const uint64_t* tpBytes, const std::string& tag,
+                             std::vector<uint8_t>& out) const;
+
+private:
     size_t packet(int p, const Tier1View& t1, const uint8_t* passes, std::vector<uint8_t>* out);
     void mainHeader(std::vector<uint8_t>& v, const std::string& comment) const;
 

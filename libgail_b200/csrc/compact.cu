@@ -9,12 +9,12 @@
 // a warp per block copies the pass tables and the codeword. Nothing is read from the
 // output buffers, which may be mapped host memory.
 #include <cuda_runtime.h>
-#include <math_constants.h>
 
 #include <algorithm>
 
 #include "common.cuh"
 #include "compact.cuh"
+#include "hull.cuh"
 
 namespace gb {
 
@@ -170,68 +170,16 @@ __global__ void __launch_bounds__(256) copyKernel(CompactArgs a) {
     if (__any_sync(kFull, over) && lane == 0) a.tot[2] = 1u;
 }
 
-// PCRD hull points, a thread per block: the lower convex hull of the block's (truncation
-// length, accumulated weighted distortion reduction) points, by the same sequence of IEEE
-// double operations as the host rate control (the hull construction of Josephur/libgail
-// src/core/rate_control.cpp:38-86), each written with an explicit round-to-nearest intrinsic so that
-// nothing is contracted or reordered: the points and slopes are bit-identical to the
-// host's. The hull stack lives in shared memory, one column per thread.
-constexpr int HULL_THREADS = 32;
-constexpr int HULL_DEPTH = kMaxPasses + 1;  // the origin and one point per pass
-
+// PCRD hull points, a thread per block, from the fixed-stride pass tables.
 __global__ void __launch_bounds__(HULL_THREADS) hullKernel(CompactArgs a) {
-    __shared__ double sD[HULL_DEPTH][HULL_THREADS];
-    __shared__ uint32_t sR[HULL_DEPTH][HULL_THREADS];
-    __shared__ uint8_t sK[HULL_DEPTH][HULL_THREADS];
+    __shared__ HullStack st;
     const int t = threadIdx.x;
     const uint32_t blk = blockIdx.x * HULL_THREADS + t;
     if (blk >= a.n) return;
     const uint4 in = reinterpret_cast<const uint4*>(a.info)[blk];
-    const int nbps = (int)in.x, np = min((int)in.y, kMaxPasses);
-    const double scale = a.scale[blk];
-    const uint32_t* len = a.passLen + (size_t)blk * kMaxPasses;
-    const int32_t* dist = a.passDist + (size_t)blk * kMaxPasses;
-    // slope from stack point m - 1 to point m, as the host computes it when m is pushed
-    // (its inputs stay unchanged while m is on the stack, so recomputing it is exact)
-    auto slopeAt = [&](int m) {
-        const uint32_t r1 = sR[m][t], r0 = sR[m - 1][t];
-        return r1 == r0 ? CUDART_INF : __ddiv_rn(__dsub_rn(sD[m][t], sD[m - 1][t]), (double)(r1 - r0));
-    };
-    int m = 0;
-    sD[0][t] = 0.0;
-    sR[0][t] = 0;
-    sK[0][t] = 0;
-    double acc = 0.0;
-    for (int k = 0; k < np; ++k) {
-        // the plane pass k codes and its weight 4^plane / 4096 (shift counts taken mod 64,
-        // as the host's shift instruction does)
-        const int plane = k == 0 ? nbps - 1 : nbps - 2 - (k - 1) / 3;
-        const double ps = (double)(1ull << ((2 * plane) & 63)) / 4096.0;
-        acc = __dadd_rn(acc, __dmul_rn(__dmul_rn((double)dist[k], ps), scale));
-        const uint32_t r = len[k];
-        if (acc <= sD[m][t]) continue;  // no gain: never a hull point
-        while (m >= 1) {  // drop the points the new one makes concave
-            const uint32_t rm = sR[m][t];
-            const double sNew = r == rm ? CUDART_INF : __ddiv_rn(__dsub_rn(acc, sD[m][t]), (double)(r - rm));
-            if (sNew < slopeAt(m)) break;
-            --m;
-        }
-        ++m;
-        sR[m][t] = r;
-        sD[m][t] = acc;
-        sK[m][t] = (uint8_t)(k + 1);
-    }
-    uint8_t* hp = a.hullPasses + (size_t)blk * kMaxPasses;
-    double* hs = a.hullSlope + (size_t)blk * kMaxPasses;
-    for (int q = 1; q <= m; ++q) {
-        const double dr = __dsub_rn((double)sR[q][t], (double)sR[q - 1][t]);
-        hp[q - 1] = sK[q][t];
-        hs[q - 1] = dr <= 0 ? CUDART_INF : __ddiv_rn(__dsub_rn(sD[q][t], sD[q - 1][t]), dr);
-    }
-    for (int q = m; q < np; ++q) {
-        hp[q] = 0;
-        hs[q] = 0.0;
-    }
+    const size_t o = (size_t)blk * kMaxPasses;
+    hullOfBlock(st, t, (int)in.x, min((int)in.y, kMaxPasses), a.scale[blk], a.passLen + o, a.passDist + o,
+                a.hullPasses + o, a.hullSlope + o);
 }
 
 }  // namespace

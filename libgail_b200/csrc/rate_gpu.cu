@@ -1,0 +1,658 @@
+// Device rate control and Tier-2 (rate_gpu.h).
+//
+// Per frame: the range of the hull slopes (one reduction), the slope histogram (a thread
+// per block, 32-bit atomic sums of whole bytes and blocks, exact in any order), then per
+// measurement of the threshold search one launch of the packet coder (a warp per packet:
+// its lanes select the passes of the packet's blocks from their hull points and fetch
+// their lengths in parallel, lane 0 codes the header bits as the host writer does) and a
+// read-back of the tile-parts' sizes. At the final thresholds, packet offsets by a scan
+// and the packets themselves: lane 0 writes the header, the warp copies the codewords.
+#include "rate_gpu.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+#include "capi_util.h"
+#include "common.cuh"
+#include "encoder.h"
+#include "hull.cuh"
+#include "rate_search.h"
+
+namespace gb {
+
+namespace {
+
+constexpr int kPacketBlocks = 64;     // blocks of one packet the device coder holds (DCI: 48)
+constexpr int kTagNodes = 32;         // nodes of one tag tree (DCI: 4 x 4 leaves, 21 nodes)
+constexpr uint32_t kMaxAmbiguous = 4096;
+constexpr double kBinMargin = 1e-7;   // bin units from an edge within which the host bins
+constexpr int T2_WARPS = 4;
+
+struct PlanArgs {
+    const int4* segs;       // x: first block, y: blocks across the band, z: ncbx | ncby << 16, w: Mb | comp << 8
+    const int32_t* pkSeg;   // segments of packet p: [pkSeg[p], pkSeg[p + 1])
+    const uint8_t* pkTp;    // tile-part of each packet
+    const uint8_t* comp;    // component of each block
+    uint32_t numPackets, numBlocks;
+};
+
+struct FrameArgs {
+    const GbCblkInfo* info;
+    const uint32_t* passLen;
+    const uint8_t* data;
+    const uint8_t* hp;
+    const double* hs;
+};
+
+__device__ __forceinline__ int floorLog2(uint32_t v) { return 31 - __clz(v); }  // v > 0
+
+// Passes of a block at threshold t: its hull points down to the first flatter one.
+__device__ __forceinline__ uint32_t passesAt(const FrameArgs& f, const GbCblkInfo& ci, double t) {
+    uint32_t np = 0;
+    for (uint32_t q = 0; q < ci.numPasses; ++q) {
+        const uint32_t k = f.hp[ci.passBase + q];
+        if (k == 0 || f.hs[ci.passBase + q] < t) break;
+        np = k;
+    }
+    return np;
+}
+
+// ------------------------------------------------------------- packet-header bits
+// B.10.1: bits fill each byte from the top; the byte after an 0xFF byte carries only 7.
+// out null: count only.
+struct Bits {
+    uint8_t* out;
+    uint32_t cur, last, bytes;
+    int fill, room;
+    __device__ void init(uint8_t* o) {
+        out = o;
+        cur = last = bytes = 0;
+        fill = 0;
+        room = 8;
+    }
+    __device__ void push() {
+        last = cur & 0xFFu;
+        if (out) out[bytes] = (uint8_t)last;
+        ++bytes;
+        room = last == 0xFFu ? 7 : 8;
+        cur = 0;
+        fill = 0;
+    }
+    __device__ void put(uint32_t v, int n) {  // the n (<= 32) low bits of v, most significant first
+        while (n > 0) {
+            const int k = min(n, room - fill);
+            n -= k;
+            cur = (cur << k) | ((v >> n) & ((1u << k) - 1u));
+            fill += k;
+            if (fill == room) push();
+        }
+    }
+    __device__ void zeros(int n) {
+        for (; n > 8; n -= 8) put(0, 8);
+        put(0, n);
+    }
+    // pads the byte in progress; a header ending on 0xFF owes its stuffed 0x00; a header
+    // with no bits is one 0x00
+    __device__ uint32_t end() {
+        if (fill > 0 || bytes == 0) {
+            cur <<= room - fill;
+            push();
+        }
+        if (last == 0xFFu) push();
+        return bytes;
+    }
+};
+
+// ------------------------------------------------------------------- tag trees
+// B.10.2 over w x h leaves: a node's value is the minimum of its children's; coding a leaf
+// against a threshold walks from the root, each node sending a 0 per unit its value is
+// known to exceed (from where it stopped, at least its parent's bound) up to the
+// threshold, and a 1 when its value is reached below the threshold.
+struct Tag {
+    int8_t parent[kTagNodes];
+    uint8_t known[kTagNodes];
+    int value[kTagNodes], low[kTagNodes];
+    int n, leaves;
+    __device__ void shape(int w, int h) {
+        int lw = w, lh = h, base = 0;
+        leaves = w * h;
+        for (;;) {
+            const int nb = base + lw * lh, pw = (lw + 1) / 2;
+            for (int y = 0; y < lh; ++y)
+                for (int x = 0; x < lw; ++x)
+                    parent[base + y * lw + x] = (int8_t)((lw == 1 && lh == 1) ? -1 : nb + (y / 2) * pw + x / 2);
+            n = nb;
+            if (lw == 1 && lh == 1) break;
+            base = nb;
+            lw = pw;
+            lh = (lh + 1) / 2;
+        }
+        for (int i = 0; i < n; ++i) {
+            low[i] = 0;
+            known[i] = 0;
+        }
+    }
+    __device__ void close() {
+        for (int i = leaves; i < n; ++i) value[i] = 1 << 30;
+        for (int i = 0; i < n; ++i)
+            if (parent[i] >= 0) value[parent[i]] = min(value[parent[i]], value[i]);
+    }
+    __device__ void encode(Bits& hb, int leaf, int threshold) {
+        int path[8], d = 0;
+        for (int i = leaf; i >= 0; i = parent[i]) path[d++] = i;
+        int floorv = 0;
+        while (d > 0) {
+            const int i = path[--d];
+            int lo = max(low[i], floorv);
+            const int to = min(value[i], threshold);
+            if (to > lo) {
+                hb.zeros(to - lo);
+                lo = to;
+            }
+            low[i] = lo;
+            if (lo >= value[i] && lo < threshold && !known[i]) {
+                hb.put(1, 1);
+                known[i] = 1;
+            }
+            floorv = lo;
+        }
+    }
+};
+
+// The pass-count code of Table B.4 (n <= 64 here).
+__device__ __forceinline__ void putPasses(Bits& hb, int n) {
+    if (n == 1) hb.put(0, 1);
+    else if (n == 2) hb.put(0x2, 2);
+    else if (n <= 5) hb.put(0xC | (uint32_t)(n - 3), 4);
+    else if (n <= 36) hb.put(0x1E0 | (uint32_t)(n - 6), 9);
+    else hb.put(0xFF80 | (uint32_t)(n - 37), 16);
+}
+
+// One warp's packet: its blocks in packet order with their passes, planes, lengths and
+// codeword offsets, and the two tag trees.
+struct WarpPacket {
+    uint8_t np[kPacketBlocks], nbps[kPacketBlocks];
+    uint32_t len[kPacketBlocks], dataOff[kPacketBlocks];
+    Tag incl, msb;
+};
+
+// The header of packet p (lane 0), as the host writer codes it; out null: count only.
+__device__ uint32_t codeHeader(const PlanArgs& P, WarpPacket& W, int s0, int s1, bool any, uint8_t* out,
+                               uint32_t* body) {
+    Bits hb;
+    hb.init(out);
+    *body = 0;
+    if (!any) {
+        hb.put(0, 1);
+        return hb.end();
+    }
+    hb.put(1, 1);
+    int base = 0;
+    for (int s = s0; s < s1; ++s) {
+        const int4 g = P.segs[s];
+        const int ncbx = g.z & 0xFFFF, ncby = g.z >> 16, Mb = g.w & 0xFF, nl = ncbx * ncby;
+        W.incl.shape(ncbx, ncby);
+        W.msb.shape(ncbx, ncby);
+        for (int k = 0; k < nl; ++k) {
+            W.incl.value[k] = W.np[base + k] ? 0 : 1;
+            W.msb.value[k] = Mb - (int)W.nbps[base + k];
+        }
+        W.incl.close();
+        W.msb.close();
+        for (int k = 0; k < nl; ++k) {
+            W.incl.encode(hb, k, 1);
+            const int np = W.np[base + k];
+            if (!np) continue;
+            W.msb.encode(hb, k, 999);
+            putPasses(hb, np);
+            const uint32_t len = W.len[base + k];
+            // Lblock starts at 3; the length takes Lblock + floor(log2 passes) bits
+            const int extra = floorLog2((uint32_t)np);
+            const int need = len ? floorLog2(len) + 1 : 1;
+            const int incr = max(0, need - (3 + extra));
+            hb.put(((1u << incr) - 1u) << 1, incr + 1);  // incr ones and a zero
+            hb.put(len, 3 + incr + extra);
+            *body += len;
+        }
+        base += nl;
+    }
+    return hb.end();
+}
+
+// A warp per packet. WRITE false: its size into pkBytes and its tile-part's total;
+// WRITE true: the packet at body + pkOff[p] and every block's passes into passesOut.
+template <bool WRITE>
+__global__ void __launch_bounds__(T2_WARPS * 32) t2Kernel(PlanArgs P, FrameArgs F, double l0, double l1, double l2,
+                                                          uint32_t* pkBytes, unsigned long long* tpBytes,
+                                                          const uint32_t* pkOff, uint8_t* body, uint8_t* passesOut) {
+    __shared__ WarpPacket ws[T2_WARPS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t p = blockIdx.x * T2_WARPS + wid;
+    if (p >= P.numPackets) return;
+    WarpPacket& W = ws[wid];
+    const int s0 = P.pkSeg[p], s1 = P.pkSeg[p + 1];
+    const double lam[3] = {l0, l1, l2};
+    // the packet's blocks, a lane each
+    bool any = false;
+    int nb = 0;
+    for (int s = s0; s < s1; ++s) {
+        const int4 g = P.segs[s];
+        const int ncbx = g.z & 0xFFFF, nl = ncbx * (g.z >> 16);
+        const double t = lam[(g.w >> 8) & 3];
+        for (int k = lane; k < nl; k += 32) {
+            const uint32_t blk = (uint32_t)(g.x + (k / ncbx) * g.y + k % ncbx);
+            const GbCblkInfo ci = F.info[blk];
+            const uint32_t np = passesAt(F, ci, t);
+            W.np[nb + k] = (uint8_t)np;
+            W.nbps[nb + k] = (uint8_t)ci.nbps;
+            W.len[nb + k] = np ? F.passLen[ci.passBase + np - 1] : 0u;
+            W.dataOff[nb + k] = ci.dataOffset;
+            any = any || np != 0;
+            if (WRITE) passesOut[blk] = (uint8_t)np;
+        }
+        nb += nl;
+    }
+    any = __any_sync(kFull, any);
+    __syncwarp();
+    uint32_t hdr = 0, bodyBytes = 0;
+    if (lane == 0) hdr = codeHeader(P, W, s0, s1, any, WRITE ? body + pkOff[p] : nullptr, &bodyBytes);
+    hdr = __shfl_sync(kFull, hdr, 0);
+    bodyBytes = __shfl_sync(kFull, bodyBytes, 0);
+    if (!WRITE) {
+        if (lane == 0) {
+            pkBytes[p] = hdr + bodyBytes;
+            atomicAdd(&tpBytes[P.pkTp[p]], (unsigned long long)(hdr + bodyBytes));
+        }
+        return;
+    }
+    __syncwarp();
+    uint8_t* dst = body + pkOff[p] + hdr;
+    for (int k = 0; k < nb; ++k) {
+        const uint32_t len = W.len[k];
+        const uint8_t* src = F.data + W.dataOff[k];
+        for (uint32_t i = lane; i < len; i += 32) dst[i] = src[i];
+        dst += len;
+    }
+}
+
+// Packet offsets in the codestream body: the packets before, and 14 bytes (SOT segment
+// and SOD) before each tile-part's packets. One CTA.
+__global__ void __launch_bounds__(1024) offsetsKernel(PlanArgs P, const uint32_t* pkBytes, uint32_t* pkOff) {
+    __shared__ uint32_t sW[32];
+    __shared__ uint32_t sCarry;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) sCarry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < P.numPackets; base += 1024) {
+        const uint32_t i = base + tid;
+        const uint32_t v = i < P.numPackets ? pkBytes[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += t;
+        }
+        if (lane == 31) sW[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            const uint32_t w = sW[lane];
+            uint32_t y = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(kFull, y, o);
+                if (lane >= o) y += t;
+            }
+            sW[lane] = y - w;
+        }
+        __syncthreads();
+        const uint32_t carry = sCarry;
+        if (i < P.numPackets) pkOff[i] = carry + sW[wid] + x - v + 14u * (P.pkTp[i] + 1u);
+        __syncthreads();
+        if (tid == 1023) sCarry = carry + sW[wid] + x;
+        __syncthreads();
+    }
+}
+
+// The range of the finite positive hull slopes: range[0] = max of ~bits (the smallest),
+// range[1] = max of the bits (the largest); positive doubles order as their bit patterns.
+__global__ void __launch_bounds__(256) rangeKernel(FrameArgs F, uint32_t n, unsigned long long* range) {
+    unsigned long long lo = 0, hi = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const GbCblkInfo ci = F.info[i];
+        for (uint32_t q = 0; q < ci.numPasses && F.hp[ci.passBase + q] != 0; ++q) {
+            const double s = F.hs[ci.passBase + q];
+            if (isfinite(s) && s > 0) {
+                const unsigned long long b = (unsigned long long)__double_as_longlong(s);
+                lo = max(lo, ~b);
+                hi = max(hi, b);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = max(lo, __shfl_xor_sync(kFull, lo, o));
+        hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (lo) atomicMax(&range[0], lo);
+        if (hi) atomicMax(&range[1], hi);
+    }
+}
+
+// The slope histogram: per component, bytes (each point's rate step) and blocks (a
+// block's first point) by bin; bins is [bytes c0, c1, c2, blocks c0, c1, c2] x nb. A
+// point whose bin value lies within kBinMargin of an edge goes to amb (count, then per
+// point: comp | first << 8, bytes, slope as two words) for the host to bin.
+__global__ void __launch_bounds__(256) binsKernel(PlanArgs P, FrameArgs F, double lo, int nb, uint32_t* bins,
+                                                  uint32_t* amb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.numBlocks) return;
+    const GbCblkInfo ci = F.info[i];
+    const int c = P.comp[i];
+    uint32_t prev = 0;
+    bool first = true;
+    for (uint32_t q = 0; q < ci.numPasses; ++q) {
+        const uint32_t k = F.hp[ci.passBase + q];
+        if (k == 0) break;
+        const uint32_t rate = F.passLen[ci.passBase + k - 1];
+        const double s = F.hs[ci.passBase + q];
+        int b = nb - 1;
+        bool sure = true;
+        if (isfinite(s)) {
+            const double v = (log2(s) - lo) * 1024.0;
+            const double fl = floor(v), fr = v - fl;
+            sure = fr >= kBinMargin && fr <= 1.0 - kBinMargin;
+            b = (int)fmin(fmax(fl, 0.0), (double)(nb - 1));
+        }
+        if (sure) {
+            atomicAdd(&bins[(size_t)c * nb + b], rate - prev);
+            if (first) atomicAdd(&bins[(size_t)(3 + c) * nb + b], 1u);
+        } else {
+            const uint32_t slot = atomicAdd(amb, 1u);
+            if (slot < kMaxAmbiguous) {
+                uint32_t* e = amb + 1 + 4 * slot;
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(s);
+                e[0] = (uint32_t)c | (first ? 256u : 0u);
+                e[1] = rate - prev;
+                e[2] = (uint32_t)bits;
+                e[3] = (uint32_t)(bits >> 32);
+            }
+        }
+        prev = rate;
+        first = false;
+    }
+}
+
+// Hull points of a packed frame (pass tables at each block's passBase).
+__global__ void __launch_bounds__(HULL_THREADS) packedHullKernel(const GbCblkInfo* info, const uint32_t* passLen,
+                                                                 const int32_t* passDist, const double* scale,
+                                                                 uint32_t n, uint8_t* hp, double* hs) {
+    __shared__ HullStack st;
+    const int t = threadIdx.x;
+    const uint32_t blk = blockIdx.x * HULL_THREADS + t;
+    if (blk >= n) return;
+    const GbCblkInfo ci = info[blk];
+    hullOfBlock(st, t, (int)ci.nbps, (int)ci.numPasses, scale[blk], passLen + ci.passBase, passDist + ci.passBase,
+                hp + ci.passBase, hs + ci.passBase);
+}
+
+double asDouble(unsigned long long bits) {
+    double d;
+    std::memcpy(&d, &bits, 8);
+    return d;
+}
+
+template <class T>
+struct DevBuf {  // a growable device buffer
+    T* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t n) {
+        if (n <= cap) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        check(cudaMalloc((void**)&p, std::max<size_t>(n, 16) * sizeof(T)), "device memory for rate control");
+        cap = n;
+    }
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+template <class T>
+struct HostBuf {  // a growable pinned host buffer
+    T* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t n) {
+        if (n <= cap) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        check(cudaHostAlloc((void**)&p, std::max<size_t>(n, 16) * sizeof(T), cudaHostAllocDefault),
+              "pinned host memory for rate control");
+        cap = n;
+    }
+    ~HostBuf() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+}  // namespace
+
+struct DeviceRateControl::Impl {
+    int dev;
+    CodestreamWriter w;
+    PlanArgs plan{};
+    int ntp = 0;
+    DevBuf<int4> segs;
+    DevBuf<int32_t> pkSeg;
+    DevBuf<uint8_t> pkTp, comp;
+    DevBuf<double> scale;
+    // per frame
+    DevBuf<unsigned long long> range, tp;
+    DevBuf<uint32_t> bins, amb, pk, pkOff;
+    DevBuf<uint8_t> body, passes;
+    HostBuf<unsigned long long> hRange, hTp;
+    HostBuf<uint32_t> hBins, hAmb;
+    HostBuf<uint8_t> hBody, hPasses;
+    // frames uploaded from host memory
+    DevBuf<GbCblkInfo> upInfo;
+    DevBuf<uint32_t> upLen;
+    DevBuf<int32_t> upDist;
+    DevBuf<uint8_t> upData, upHp;
+    DevBuf<double> upHs;
+
+    Impl(int device, const Layout& L, const std::string& label) : dev(device), w(L, label) {
+        GB_CHECK(cudaSetDevice(dev));
+        const auto& sg = w.segments();
+        const auto& ps = w.packetSegments();
+        const auto& tps = w.tilePartPackets();
+        ntp = w.numTileParts();
+        std::vector<int4> hs(sg.size());
+        for (size_t s = 0; s < sg.size(); ++s) {
+            const auto& g = sg[s];
+            const GbSubband& b = L.bands[(size_t)g.band];
+            if (g.ncbx * g.ncby > 16 || g.ncbx > 16 || g.ncby > 16)
+                throw std::logic_error("precinct-band too large for the device Tier-2 (at most 4 x 4 code-blocks)");
+            hs[s] = make_int4(b.cblkBase + g.cby0 * b.ncbx + g.cbx0, b.ncbx, g.ncbx | (g.ncby << 16), b.Mb | (b.comp << 8));
+        }
+        std::vector<uint8_t> tpOf((size_t)w.numPackets());
+        for (int t = 0; t < ntp; ++t)
+            for (int p = tps[(size_t)t]; p < tps[(size_t)t + 1]; ++p) tpOf[(size_t)p] = (uint8_t)t;
+        for (int p = 0; p < w.numPackets(); ++p) {
+            int blocks = 0;
+            for (int s = ps[(size_t)p]; s < ps[(size_t)p + 1]; ++s) blocks += sg[(size_t)s].ncbx * sg[(size_t)s].ncby;
+            if (blocks > kPacketBlocks) throw std::logic_error("packet with too many code-blocks for the device Tier-2");
+        }
+        std::vector<uint8_t> cmp((size_t)L.numCblks());
+        for (int i = 0; i < L.numCblks(); ++i) cmp[(size_t)i] = (uint8_t)L.bands[L.cblks[(size_t)i].band].comp;
+        const std::vector<double> sc = blockScales(L);
+        segs.ensure(hs.size());
+        pkSeg.ensure(ps.size());
+        pkTp.ensure(tpOf.size());
+        comp.ensure(cmp.size());
+        scale.ensure(sc.size());
+        GB_CHECK(cudaMemcpy(segs.p, hs.data(), hs.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        GB_CHECK(cudaMemcpy(pkSeg.p, ps.data(), ps.size() * 4, cudaMemcpyHostToDevice));
+        GB_CHECK(cudaMemcpy(pkTp.p, tpOf.data(), tpOf.size(), cudaMemcpyHostToDevice));
+        GB_CHECK(cudaMemcpy(comp.p, cmp.data(), cmp.size(), cudaMemcpyHostToDevice));
+        GB_CHECK(cudaMemcpy(scale.p, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice));
+        plan = {segs.p, pkSeg.p, pkTp.p, comp.p, (uint32_t)w.numPackets(), (uint32_t)L.numCblks()};
+        range.ensure(2);
+        tp.ensure((size_t)ntp);
+        amb.ensure(1 + 4 * (size_t)kMaxAmbiguous);
+        pk.ensure((size_t)w.numPackets());
+        pkOff.ensure((size_t)w.numPackets());
+        passes.ensure((size_t)L.numCblks());
+        hRange.ensure(2);
+        hTp.ensure((size_t)ntp);
+        hAmb.ensure(1 + 4 * (size_t)kMaxAmbiguous);
+        hPasses.ensure((size_t)L.numCblks());
+    }
+
+    RateResult run(const DeviceTier1& d, const RateLimits& lim, const std::string& tag, std::vector<uint8_t>& out,
+                   cudaStream_t st) {
+        GB_CHECK(cudaSetDevice(dev));
+        const Layout& L = w.layout();
+        const uint32_t n = (uint32_t)L.numCblks();
+        const FrameArgs F{d.info, d.passLen, d.data, d.hullPasses, d.hullSlope};
+        RateResult res;
+        // the slope range and the search bounds
+        GB_CHECK(cudaMemsetAsync(range.p, 0, 16, st));
+        rangeKernel<<<std::min(divUp(n, 256u), 296u), 256, 0, st>>>(F, n, range.p);
+        GB_CHECK(cudaMemcpyAsync(hRange.p, range.p, 16, cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaStreamSynchronize(st));
+        double minSlope = hRange.p[0] ? asDouble(~hRange.p[0]) : INFINITY;
+        double maxSlope = hRange.p[1] ? asDouble(hRange.p[1]) : 0.0;
+        double lo, hi;
+        slopeBounds(minSlope, maxSlope, lo, hi);
+        // the histogram
+        SlopeBins sb(lo, hi);
+        const int nb = sb.size();
+        bins.ensure((size_t)6 * nb);
+        hBins.ensure((size_t)6 * nb);
+        GB_CHECK(cudaMemsetAsync(bins.p, 0, (size_t)6 * nb * 4, st));
+        GB_CHECK(cudaMemsetAsync(amb.p, 0, 4, st));
+        binsKernel<<<divUp(n, 256u), 256, 0, st>>>(plan, F, lo, nb, bins.p, amb.p);
+        GB_CHECK(cudaMemcpyAsync(hBins.p, bins.p, (size_t)6 * nb * 4, cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaMemcpyAsync(hAmb.p, amb.p, (1 + 4 * (size_t)kMaxAmbiguous) * 4, cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaStreamSynchronize(st));
+        GB_CHECK(cudaGetLastError());
+        for (int c = 0; c < 3; ++c)
+            for (int b = 0; b < nb; ++b) {
+                const uint32_t by = hBins.p[(size_t)c * nb + b], bl = hBins.p[(size_t)(3 + c) * nb + b];
+                if (by | bl) sb.add(c, b, (double)by, (double)bl);
+            }
+        const uint32_t na = hAmb.p[0];
+        if (na > kMaxAmbiguous) throw std::runtime_error("too many hull slopes on slope-bin edges");
+        for (uint32_t a = 0; a < na; ++a) {
+            const uint32_t* e = hAmb.p + 1 + 4 * a;
+            const double s = asDouble((unsigned long long)e[2] | ((unsigned long long)e[3] << 32));
+            sb.add((int)(e[0] & 255u), sb.bin(s), (double)e[1], (e[0] & 256u) ? 1.0 : 0.0);
+        }
+        sb.finish();
+        // the threshold search with exact sizes measured on the device
+        const size_t hdrLongest = w.longestHeaderBytes();
+        const uint32_t t2Blocks = divUp(plan.numPackets, (uint32_t)T2_WARPS);
+        auto measure = [&](const double l[3]) {
+            GB_CHECK(cudaMemsetAsync(tp.p, 0, (size_t)ntp * 8, st));
+            t2Kernel<false><<<t2Blocks, T2_WARPS * 32, 0, st>>>(plan, F, l[0], l[1], l[2], pk.p, tp.p, nullptr, nullptr,
+                                                                 nullptr);
+            GB_CHECK(cudaMemcpyAsync(hTp.p, tp.p, (size_t)ntp * 8, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaStreamSynchronize(st));
+            GB_CHECK(cudaGetLastError());
+            ++res.iterations;
+            CodestreamSizes sz;
+            sz.numTileParts = ntp;
+            size_t total = hdrLongest;
+            for (int t = 0; t < ntp; ++t) {
+                const size_t bytes = 14 + hTp.p[t];
+                sz.tilePart[t] = bytes;
+                sz.comp[t % 3] += bytes;
+                total += bytes;
+            }
+            sz.total = total + 2;
+            return sz;
+        };
+        double lam[3] = {0, 0, 0};
+        CodestreamSizes sz;
+        rateSearch(lim, minSlope, maxSlope, lo, hi, sb, measure, lam, sz);
+        // the packets at the final thresholds (the last measurement's sizes)
+        uint64_t tpBytes[6] = {};
+        size_t bodyBytes = 0;
+        for (int t = 0; t < ntp; ++t) {
+            tpBytes[t] = 14 + hTp.p[t];
+            bodyBytes += tpBytes[t];
+        }
+        body.ensure(bodyBytes);
+        hBody.ensure(bodyBytes);
+        offsetsKernel<<<1, 1024, 0, st>>>(plan, pk.p, pkOff.p);
+        t2Kernel<true><<<t2Blocks, T2_WARPS * 32, 0, st>>>(plan, F, lam[0], lam[1], lam[2], nullptr, nullptr, pkOff.p,
+                                                            body.p, passes.p);
+        GB_CHECK(cudaMemcpyAsync(hBody.p, body.p, bodyBytes, cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaMemcpyAsync(hPasses.p, passes.p, n, cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaStreamSynchronize(st));
+        GB_CHECK(cudaGetLastError());
+        const CodestreamSizes made = w.assemble(hBody.p, tpBytes, tag, out);
+        if (made.total != sz.total) throw std::logic_error("device codestream size differs from its measurement");
+        res.passes.assign(hPasses.p, hPasses.p + n);
+        res.lambda = std::max({lam[0], lam[1], lam[2]});
+        for (int c = 0; c < 3; ++c) res.lambdaComp[c] = lam[c];
+        res.distortion = NAN;
+        res.sizes = sz;
+        return res;
+    }
+
+    RateResult runHost(const Tier1View& t1, const RateLimits& lim, const std::string& tag, std::vector<uint8_t>& out,
+                       cudaStream_t st) {
+        GB_CHECK(cudaSetDevice(dev));
+        const uint32_t n = (uint32_t)w.layout().numCblks();
+        if (t1.numInfo != n) throw std::logic_error("Tier-1 frame and layout have different code-block counts");
+        for (uint32_t i = 0; i < n; ++i) {
+            const GbCblkInfo& c = t1.info[i];
+            if (c.numPasses > (uint32_t)kMaxPasses) throw std::logic_error("more coding passes than the device holds");
+            for (uint32_t k = 1; k < c.numPasses; ++k)
+                if (t1.passLen[c.passBase + k] < t1.passLen[c.passBase + k - 1])
+                    throw std::logic_error("pass lengths that decrease");
+        }
+        const size_t np = std::max<size_t>(t1.numPasses, 1), nd = std::max<size_t>(t1.numData, 1);
+        upInfo.ensure(n);
+        upLen.ensure(np);
+        upDist.ensure(np);
+        upData.ensure(nd);
+        upHp.ensure(np);
+        upHs.ensure(np);
+        GB_CHECK(cudaMemcpyAsync(upInfo.p, t1.info, (size_t)n * sizeof(GbCblkInfo), cudaMemcpyHostToDevice, st));
+        if (t1.numPasses) {
+            GB_CHECK(cudaMemcpyAsync(upLen.p, t1.passLen, (size_t)t1.numPasses * 4, cudaMemcpyHostToDevice, st));
+            GB_CHECK(cudaMemcpyAsync(upDist.p, t1.passDist, (size_t)t1.numPasses * 4, cudaMemcpyHostToDevice, st));
+        }
+        if (t1.numData) GB_CHECK(cudaMemcpyAsync(upData.p, t1.data, t1.numData, cudaMemcpyHostToDevice, st));
+        packedHullKernel<<<divUp(n, (uint32_t)HULL_THREADS), HULL_THREADS, 0, st>>>(upInfo.p, upLen.p, upDist.p, scale.p,
+                                                                                   n, upHp.p, upHs.p);
+        GB_CHECK(cudaGetLastError());
+        DeviceTier1 d{upInfo.p, upLen.p, upData.p, upHp.p, upHs.p};
+        return run(d, lim, tag, out, st);
+    }
+};
+
+DeviceRateControl::DeviceRateControl(int device, const Layout& L, const std::string& label)
+    : p_(std::make_unique<Impl>(device, L, label)) {}
+DeviceRateControl::~DeviceRateControl() = default;
+
+RateResult DeviceRateControl::run(const DeviceTier1& f, const RateLimits& lim, const std::string& tag,
+                                  std::vector<uint8_t>& out, cudaStream_t st) {
+    return p_->run(f, lim, tag, out, st);
+}
+
+RateResult DeviceRateControl::runHost(const Tier1View& t1, const RateLimits& lim, const std::string& tag,
+                                      std::vector<uint8_t>& out, cudaStream_t st) {
+    return p_->runHost(t1, lim, tag, out, st);
+}
+
+const Layout& DeviceRateControl::layout() const { return p_->w.layout(); }
+size_t DeviceRateControl::emptyBytes() { return p_->w.emptyBytes(); }
+
+}  // namespace gb
