@@ -133,11 +133,20 @@ GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
  *                          status
  *   gb_engine_release      give the frame's slot back
  *   gb_engine_stats        frames, batches, frames in batches, slots, slot bytes
- *   gb_engine_set_codestream  from now on, every frame also gets its DCI codestream on
- *                          `threads` host workers: gb_rate_and_build's rate control and
+ *   gb_engine_set_codestream  from now on, every frame also gets its DCI codestream, driven
+ *                          by `threads` host workers: gb_rate_and_build's rate control and
  *                          codestream (fps, maxMbps, compMbps, label, tag), then with check
  *                          the DCI check; the frame is handed out by gb_engine_wait once its
- *                          codestream is made (the latency includes it)
+ *                          codestream is made (the latency includes it). flags 0: rate control
+ *                          and Tier-2 on the device (gb_device_rate_and_build's path; the
+ *                          Tier-1 frame stays in device memory and gb_engine_wait hands out an
+ *                          empty Tier-1 view); GB_CS_HOST: on the host workers from the Tier-1
+ *                          frame in host memory, with the hull points computed on the GPU
+ *                          (gb_rate_and_build_hull's path); GB_CS_TIER1: the Tier-1 frame and
+ *                          its hull points also in host memory, as without codestreams
+ *   gb_engine_counters     for the engine's encodes so far: host-to-device and device-to-host
+ *                          bytes copied (frames in; Tier-1 frames, rate-control read-backs and
+ *                          codestreams out) and kernels launched (any pointer may be NULL)
  *   gb_engine_codestream   a handed-out frame's codestream (valid until release) and its
  *                          DCI verdict (1, 0, or -1 when not checked)
  *   gb_engine_add_decoder  a decode class (layout, decode settings as decoder_create takes
@@ -166,8 +175,10 @@ GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5);
  * busy, a batch waits to gather minBatchPct % of maxBatch ready frames, but not past
  * maxWaitMs after its oldest frame (defaults: the create call's maxBatch, 25 %, 2 ms). */
 GB_API int gb_engine_set_policy(GbEngine* e, int maxBatch, int minBatchPct, double maxWaitMs);
+enum { GB_CS_HOST = 1, GB_CS_TIER1 = 2 };
 GB_API int gb_engine_set_codestream(GbEngine* e, double fps, double maxMbps, double compMbps, const char* label,
-                                    const char* tag, int threads, int check);
+                                    const char* tag, int threads, int check, int flags);
+GB_API int gb_engine_counters(GbEngine* e, uint64_t* h2d, uint64_t* d2h, uint64_t* launches);
 GB_API int gb_engine_codestream(GbEngine* e, int64_t id, const uint8_t** data, uint64_t* size, int* dciOk);
 GB_API int gb_engine_add_decoder(GbEngine* e, const GailCudaLayout* layout, const GailCudaDecodeSettings* settings,
                                  int* classId, uint64_t* frameBytes);

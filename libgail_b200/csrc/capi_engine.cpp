@@ -54,10 +54,13 @@ GB_API int gb_engine_release(GbEngine* e, int64_t id) {
 }
 
 GB_API int gb_engine_set_codestream(GbEngine* e, double fps, double maxMbps, double compMbps, const char* label,
-                                    const char* tag, int threads, int check) {
+                                    const char* tag, int threads, int check, int flags) {
     return gbGuard([&] {
         if (!e) throw std::logic_error("null argument");
+        if (flags & ~(GB_CS_HOST | GB_CS_TIER1)) throw std::logic_error("unknown codestream flags");
         EncodeEngine::CodestreamConfig c;
+        c.onDevice = !(flags & GB_CS_HOST);
+        c.tier1 = (flags & GB_CS_TIER1) != 0;
         c.fps = fps;
         c.maxMbps = maxMbps;
         c.compMbps = compMbps;
@@ -109,6 +112,16 @@ GB_API int gb_engine_set_policy(GbEngine* e, int maxBatch, int minBatchPct, doub
     return gbGuard([&] {
         if (!e) throw std::logic_error("null argument");
         e->e->setPolicy(maxBatch, minBatchPct, maxWaitMs);
+    });
+}
+
+GB_API int gb_engine_counters(GbEngine* e, uint64_t* h2d, uint64_t* d2h, uint64_t* launches) {
+    return gbGuard([&] {
+        if (!e) throw std::logic_error("null argument");
+        const EncodeEngine::Stats s = e->e->stats();
+        if (h2d) *h2d = s.h2dBytes;
+        if (d2h) *d2h = s.d2hBytes;
+        if (launches) *launches = s.launches;
     });
 }
 

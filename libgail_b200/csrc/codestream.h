@@ -120,6 +120,7 @@ struct RateResult {
                                   // the hull came precomputed, without the gains)
     CodestreamSizes sizes;
     int iterations = 0;           // exact measurements taken
+    size_t d2hBytes = 0;          // device-to-host bytes the device rate control read back
 };
 
 // Per block, the points of the lower convex hull of its (truncation length, weighted

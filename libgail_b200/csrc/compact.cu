@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(256) copyKernel(CompactArgs a) {
         const size_t src = (size_t)blk * kMaxPasses;
         for (uint32_t q = lane; q < np; q += 32) {
             a.outPassLen[o.y + q] = a.passLen[src + q];
-            a.outPassDist[o.y + q] = a.passDist[src + q];
+            if (a.outPassDist) a.outPassDist[o.y + q] = a.passDist[src + q];
         }
         if (a.outHullPasses)
             for (uint32_t q = lane; q < np; q += 32) {

@@ -16,7 +16,7 @@ struct CompactArgs {
     const T1Job* jobs;         // each block's codeword region
     uint32_t* outInfo;         // 5 words per block: CblkInfo
     uint32_t* outPassLen;
-    int32_t* outPassDist;
+    int32_t* outPassDist;      // may be null: no distortions
     uint8_t* outData;
     uint32_t* tot;             // [0] data bytes, [1] passes, [2] set when outData was too small
     uint64_t dataCap;          // bytes outData holds

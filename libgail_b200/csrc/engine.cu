@@ -11,6 +11,7 @@
 #include "common.cuh"
 #include "compact.cuh"
 #include "frontend.cuh"
+#include "rate_gpu.h"
 #include "tuning.h"
 
 namespace gb {
@@ -53,9 +54,14 @@ struct EncodeEngine::Slot {
     uint8_t* hData = nullptr;
     uint8_t* hHullPasses = nullptr;  // the PCRD hull points, packed like hLen
     double* hHullSlope = nullptr;
+    // the packed Tier-1 frame and hull points in device memory, for device rate control
+    uint32_t *dInfoP = nullptr, *dLenP = nullptr;
+    uint8_t *dDataP = nullptr, *dHullP = nullptr;
+    double* dHullS = nullptr;
     uint64_t dataCap = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int graphKernels = 0;  // kernel launches one front-end graph makes
     cudaEvent_t frontDone = nullptr;
     std::vector<void*> dev, host;
 };
@@ -71,6 +77,8 @@ struct EncodeEngine::Request {
     Slot* slot = nullptr;
     uint32_t jobBase = 0;
     int status = 0;
+    bool tier1 = true;      // the Tier-1 frame was packed into host memory
+    bool devFrame = false;  // ... and into the slot's device buffers
     std::vector<uint8_t> cs;  // the codestream, when the engine makes them
     int dciOk = -1;
     // decode requests
@@ -198,7 +206,8 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
     const uint64_t n = c->z.n, npix = c->z.npix;
     // packed output bound: codewords of 6 bytes per sample would be beyond any 12-bit content
     c->dataCap = std::min<uint64_t>(c->z.arena, npix * 6 + (64u << 10));
-    c->slotBytes = c->z.inBytes + n * kCblkArea * 4 + 2 * c->z.arena + n * sizeof(T1Job);
+    c->slotBytes = c->z.inBytes + n * kCblkArea * 4 + 2 * c->z.arena + n * sizeof(T1Job) +
+                   n * 20 + n * kMaxPasses * (4 + 1 + 8) + c->dataCap;
     if (frameBytes) *frameBytes = c->slotBytes;
     std::lock_guard<std::mutex> lock(m_);
     classes_.push_back(std::move(c));
@@ -235,6 +244,11 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         alloc(s->dSym, c.z.arena);
         alloc(s->dCw, c.z.arena);
         alloc(s->dJobs, (uint64_t)s->n * sizeof(T1Job));
+        alloc(s->dInfoP, (uint64_t)s->n * 20);
+        alloc(s->dLenP, (uint64_t)s->n * kMaxPasses * 4);
+        alloc(s->dHullP, (uint64_t)s->n * kMaxPasses);
+        alloc(s->dHullS, (uint64_t)s->n * kMaxPasses * 8);
+        alloc(s->dDataP, c.dataCap);
         mapped(s->hInfo, (uint64_t)s->n * 20);
         mapped(s->hLen, (uint64_t)s->n * kMaxPasses * 4);
         mapped(s->hDist, (uint64_t)s->n * kMaxPasses * 4);
@@ -257,6 +271,15 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         launchFrontEnd(c.L, a, c.dLL[0], c.dLL[1], c.z.llFloats, s->dCoeffs, nullptr, cap);
         GB_CHECK(cudaStreamEndCapture(cap, &s->graph));
         GB_CHECK(cudaStreamDestroy(cap));
+        size_t nodes = 0;
+        GB_CHECK(cudaGraphGetNodes(s->graph, nullptr, &nodes));
+        std::vector<cudaGraphNode_t> nv(nodes);
+        if (nodes) GB_CHECK(cudaGraphGetNodes(s->graph, nv.data(), &nodes));
+        for (cudaGraphNode_t nd : nv) {
+            cudaGraphNodeType ty;
+            GB_CHECK(cudaGraphNodeGetType(nd, &ty));
+            if (ty == cudaGraphNodeTypeKernel) ++s->graphKernels;
+        }
         GB_CHECK(cudaGraphInstantiate(&s->exec, s->graph, 0));
     } catch (...) {
         for (void* p : s->dev) cudaFree(p);
@@ -311,7 +334,7 @@ bool EncodeEngine::wait(int timeoutMs, int64_t* id, GailCudaTier1* out, double* 
     *latencyMs = r->latency;
     *status = r->status;
     const Slot* s = r->slot;
-    if (r->decode || !s) *out = GailCudaTier1{};
+    if (r->decode || !s || !r->tier1) *out = GailCudaTier1{};
     else *out = {reinterpret_cast<const GbCblkInfo*>(s->hInfo), s->hLen, s->hDist, s->hData, s->n, s->hTot[1], s->hTot[0]};
     return true;
 }
@@ -409,7 +432,7 @@ bool EncodeEngine::hull(int64_t id, const uint8_t** passes, const double** slope
     std::lock_guard<std::mutex> lock(m_);
     if (id < 0 || id >= (int64_t)requests_.size() || !requests_[id]) throw std::logic_error("unknown request");
     const Request* r = requests_[id].get();
-    if (r->decode || !r->slot) return false;
+    if (r->decode || !r->slot || !r->tier1) return false;
     *passes = r->slot->hHullPasses;
     *slope = r->slot->hHullSlope;
     return true;
@@ -486,8 +509,18 @@ bool EncodeEngine::codestream(int64_t id, const uint8_t** data, uint64_t* size, 
 
 void EncodeEngine::codestreamWorker() {
     cudaSetDevice(dev_);
-    // one writer per frame class on this worker (the packet order is flattened once)
+    // one writer (host path) or device rate control per frame class on this worker (the
+    // packet order is flattened once), the latter on the worker's own stream at the
+    // highest priority, so that its short launches go ahead of the Tier-1 batches
     std::vector<std::unique_ptr<CodestreamWriter>> writers;
+    std::vector<std::unique_ptr<DeviceRateControl>> drc;
+    cudaStream_t st = nullptr;
+    struct StreamGuard {
+        cudaStream_t& s;
+        ~StreamGuard() {
+            if (s) cudaStreamDestroy(s);
+        }
+    } guard{st};
     for (;;) {
         Request* r;
         const Class* c = nullptr;
@@ -500,6 +533,7 @@ void EncodeEngine::codestreamWorker() {
             if (!r->decode) {
                 c = classes_[r->cls].get();
                 if (writers.size() < classes_.size()) writers.resize(classes_.size());
+                if (drc.size() < classes_.size()) drc.resize(classes_.size());
             }
         }
         if (r->decode) {
@@ -512,22 +546,41 @@ void EncodeEngine::codestreamWorker() {
             cvDone_.notify_all();
             continue;
         }
-        auto& w = writers[r->cls];
-        if (!w) w = std::make_unique<CodestreamWriter>(c->L, cs_.label);
         const Slot* s = r->slot;
+        const RateLimits lim = dciLimits(cs_.fps, cs_.maxMbps, cs_.compMbps);
+        uint64_t d2h = r->tier1 ? (uint64_t)s->n * 20 + (uint64_t)s->hTot[1] * 17 + s->hTot[0] : 0, launches = 0;
         if (r->status == kOk) {
             try {
-                Tier1View v;
-                v.info = reinterpret_cast<const GbCblkInfo*>(s->hInfo);
-                v.passLen = s->hLen;
-                v.passDist = s->hDist;
-                v.data = s->hData;
-                v.numInfo = s->n;
-                v.numPasses = s->hTot[1];
-                v.numData = s->hTot[0];
-                const HullView hull{s->hHullPasses, s->hHullSlope};  // computed on the GPU
-                const RateResult rr = allocateRate(*w, v, dciLimits(cs_.fps, cs_.maxMbps, cs_.compMbps), &hull);
-                w->build(v, rr.passes.data(), &r->cs, cs_.tag);
+                if (r->devFrame) {
+                    auto& rc = drc[r->cls];
+                    if (!rc) {
+                        if (!st) {
+                            int lo = 0, hi = 0;
+                            GB_CHECK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+                            GB_CHECK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi));
+                        }
+                        rc = std::make_unique<DeviceRateControl>(dev_, c->L, cs_.label);
+                    }
+                    const DeviceTier1 f{reinterpret_cast<const GbCblkInfo*>(s->dInfoP), s->dLenP, s->dDataP, s->dHullP,
+                                        s->dHullS};
+                    const RateResult rr = rc->run(f, lim, cs_.tag, r->cs, st);
+                    d2h += rr.d2hBytes;
+                    launches = 4 + (uint64_t)rr.iterations;  // range, bins, measurements, offsets, packets
+                } else {
+                    auto& w = writers[r->cls];
+                    if (!w) w = std::make_unique<CodestreamWriter>(c->L, cs_.label);
+                    Tier1View v;
+                    v.info = reinterpret_cast<const GbCblkInfo*>(s->hInfo);
+                    v.passLen = s->hLen;
+                    v.passDist = s->hDist;
+                    v.data = s->hData;
+                    v.numInfo = s->n;
+                    v.numPasses = s->hTot[1];
+                    v.numData = s->hTot[0];
+                    const HullView hull{s->hHullPasses, s->hHullSlope};  // computed on the GPU
+                    const RateResult rr = allocateRate(*w, v, lim, &hull);
+                    w->build(v, rr.passes.data(), &r->cs, cs_.tag);
+                }
                 if (cs_.check) r->dciOk = checkDci(r->cs.data(), r->cs.size(), cs_.fps).ok ? 1 : 0;
             } catch (const std::exception&) {
                 r->status = kError;
@@ -538,6 +591,8 @@ void EncodeEngine::codestreamWorker() {
         r->latency = msBetween(r->t0, now);
         done_.push_back(r);
         stats_.frames++;
+        stats_.d2hBytes += d2h;
+        stats_.launches += launches;
         cvDone_.notify_all();
     }
 }
@@ -577,6 +632,8 @@ bool EncodeEngine::admit() {
         GB_CHECK(cudaGraphLaunch(s->exec, front_));
         GB_CHECK(cudaEventRecord(s->frontDone, front_));
         std::lock_guard<std::mutex> lock(m_);
+        if (!r->onDevice) stats_.h2dBytes += c.z.inBytes;
+        stats_.launches += (uint64_t)s->graphKernels;
         front_q_.push_back(r);
         progress = true;
     }
@@ -643,16 +700,37 @@ bool EncodeEngine::launchBatch(Batch& b) {
     L.cmCtasPerSm = (uint16_t)tu.cmCtasPerSm;
     L.mqCtasPerSm = (uint16_t)tu.mqCtasPerSm;
     t1Encode(L, b.st);
+    uint64_t launches = 4;  // context modelling, ordering, MQ coding, truncation lengths
+    bool onDevice, tier1;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        onDevice = csOn_ && cs_.onDevice;
+        tier1 = !onDevice || cs_.tier1;
+    }
     for (Request* r : sel) {
         Slot* s = r->slot;
         std::memset(s->hTot, 0, 64);
         const uint32_t j = r->jobBase;
         const Class& c = *classes_[r->cls];
-        CompactArgs ca{s->n,   b.info + 4 * (uint64_t)j, b.len + (uint64_t)kMaxPasses * j, b.dist + (uint64_t)kMaxPasses * j,
-                       b.dJobs + j, s->hInfo, s->hLen, s->hDist, s->hData, s->hTot, s->dataCap, b.perm, b.offs, 1,
-                       c.dScale, b.hullPasses + (uint64_t)kMaxPasses * j, b.hullSlope + (uint64_t)kMaxPasses * j,
-                       s->hHullPasses, s->hHullSlope};
-        compactTier1(ca, b.st);
+        uint8_t* hp = b.hullPasses + (uint64_t)kMaxPasses * j;
+        double* hs = b.hullSlope + (uint64_t)kMaxPasses * j;
+        if (onDevice) {  // packed into the slot's device buffers, for the device rate control
+            CompactArgs ca{s->n, b.info + 4 * (uint64_t)j, b.len + (uint64_t)kMaxPasses * j, b.dist + (uint64_t)kMaxPasses * j,
+                           b.dJobs + j, s->dInfoP, s->dLenP, nullptr, s->dDataP, s->hTot, s->dataCap, b.perm, b.offs, 0,
+                           c.dScale, hp, hs, s->dHullP, s->dHullS};
+            compactTier1(ca, b.st);
+            launches += 4;  // tile sums, scan, hull points, copy
+        }
+        if (tier1) {  // packed straight into mapped host memory
+            // (after a device compaction the hull points are computed already)
+            CompactArgs ca{s->n, b.info + 4 * (uint64_t)j, b.len + (uint64_t)kMaxPasses * j, b.dist + (uint64_t)kMaxPasses * j,
+                           b.dJobs + j, s->hInfo, s->hLen, s->hDist, s->hData, s->hTot, s->dataCap, b.perm, b.offs, 1,
+                           onDevice ? nullptr : c.dScale, hp, hs, s->hHullPasses, s->hHullSlope};
+            compactTier1(ca, b.st);
+            launches += onDevice ? 3 : 4;
+        }
+        r->tier1 = tier1;
+        r->devFrame = onDevice;
     }
     GB_CHECK(cudaMemcpyAsync(b.hCtl, b.ctl, 64, cudaMemcpyDeviceToHost, b.st));
     GB_CHECK(cudaEventRecord(b.done, b.st));
@@ -661,6 +739,7 @@ bool EncodeEngine::launchBatch(Batch& b) {
     std::lock_guard<std::mutex> lock(m_);
     stats_.batches++;
     stats_.batchFrames += b.frames.size();
+    stats_.launches += launches;
     return true;
 }
 
@@ -680,6 +759,8 @@ bool EncodeEngine::collect(Batch& b) {
         } else {
             done_.push_back(r);
             stats_.frames++;
+            const Slot* s = r->slot;
+            stats_.d2hBytes += (uint64_t)s->n * 20 + (uint64_t)s->hTot[1] * 17 + s->hTot[0];
         }
     }
     if (csOn_) cvCs_.notify_all();

@@ -63,11 +63,16 @@ public:
     // Codestreams for every frame from now on: rate control to the DCI budgets at fps
     // (whole frame under maxMbps, each component under compMbps), the COM text label +
     // " " + tag, the DCI check when check is set, on `threads` host workers.
+    // onDevice: rate control and Tier-2 on the device (the Tier-1 frame stays there; only
+    // the codestream and a few numbers per size measurement come back), else on the host
+    // workers from the Tier-1 frame in host memory; tier1: the Tier-1 frame (and its hull
+    // points) also in host memory for wait() / hull() (always so on the host path).
     struct CodestreamConfig {
         double fps = 24.0, maxMbps = 230.0, compMbps = 200.0;
         std::string label, tag;
         bool check = true;
         int threads = 4;
+        bool onDevice = true, tier1 = false;
     };
     void setCodestream(const CodestreamConfig& c);
     // The codestream of a finished frame (valid until release): its bytes and whether it
@@ -90,6 +95,8 @@ public:
 
     struct Stats {
         uint64_t frames = 0, batches = 0, batchFrames = 0, slots = 0, slotBytes = 0;
+        uint64_t h2dBytes = 0, d2hBytes = 0;  // bytes copied between host and device for encodes
+        uint64_t launches = 0;                // kernels launched for encodes
     };
     Stats stats() const;
 

@@ -537,9 +537,18 @@ struct DeviceRateControl::Impl {
         GB_CHECK(cudaMemsetAsync(amb.p, 0, 4, st));
         binsKernel<<<divUp(n, 256u), 256, 0, st>>>(plan, F, lo, nb, bins.p, amb.p);
         GB_CHECK(cudaMemcpyAsync(hBins.p, bins.p, (size_t)6 * nb * 4, cudaMemcpyDeviceToHost, st));
-        GB_CHECK(cudaMemcpyAsync(hAmb.p, amb.p, (1 + 4 * (size_t)kMaxAmbiguous) * 4, cudaMemcpyDeviceToHost, st));
+        // the points on bin edges: the count and the first few, the rest when there are more
+        constexpr uint32_t kFirst = 64;
+        GB_CHECK(cudaMemcpyAsync(hAmb.p, amb.p, (1 + 4 * (size_t)kFirst) * 4, cudaMemcpyDeviceToHost, st));
         GB_CHECK(cudaStreamSynchronize(st));
         GB_CHECK(cudaGetLastError());
+        res.d2hBytes += 16 + (size_t)6 * nb * 4 + (1 + 4 * (size_t)kFirst) * 4;
+        if (hAmb.p[0] > kFirst && hAmb.p[0] <= kMaxAmbiguous) {
+            const size_t more = 4 * (size_t)(hAmb.p[0] - kFirst) * 4;
+            GB_CHECK(cudaMemcpyAsync(hAmb.p + 1 + 4 * kFirst, amb.p + 1 + 4 * kFirst, more, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaStreamSynchronize(st));
+            res.d2hBytes += more;
+        }
         for (int c = 0; c < 3; ++c)
             for (int b = 0; b < nb; ++b) {
                 const uint32_t by = hBins.p[(size_t)c * nb + b], bl = hBins.p[(size_t)(3 + c) * nb + b];
@@ -564,6 +573,7 @@ struct DeviceRateControl::Impl {
             GB_CHECK(cudaStreamSynchronize(st));
             GB_CHECK(cudaGetLastError());
             ++res.iterations;
+            res.d2hBytes += (size_t)ntp * 8;
             CodestreamSizes sz;
             sz.numTileParts = ntp;
             size_t total = hdrLongest;
@@ -595,6 +605,7 @@ struct DeviceRateControl::Impl {
         GB_CHECK(cudaMemcpyAsync(hPasses.p, passes.p, n, cudaMemcpyDeviceToHost, st));
         GB_CHECK(cudaStreamSynchronize(st));
         GB_CHECK(cudaGetLastError());
+        res.d2hBytes += bodyBytes + n;
         const CodestreamSizes made = w.assemble(hBody.p, tpBytes, tag, out);
         if (made.total != sz.total) throw std::logic_error("device codestream size differs from its measurement");
         res.passes.assign(hPasses.p, hPasses.p + n);

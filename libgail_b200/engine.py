@@ -23,7 +23,8 @@ def _bind():
     L.gb_engine_release.argtypes = [C.c_void_p, C.c_int64]
     L.gb_engine_stats.argtypes = [C.c_void_p, C.c_void_p]
     L.gb_engine_set_codestream.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_char_p, C.c_char_p,
-                                           C.c_int, C.c_int]
+                                           C.c_int, C.c_int, C.c_int]
+    L.gb_engine_counters.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.gb_engine_codestream.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_uint8)),
                                        C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
     L.gb_engine_set_policy.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double]
@@ -83,10 +84,25 @@ class Engine:
         check(lib().gb_engine_set_policy(self.h, max_batch, min_batch_pct, max_wait_ms))
 
     def set_codestream(self, fps: float = 24.0, max_mbps: float = 230.0, comp_mbps: float = 200.0,
-                       label: str = "GAIL 1.1.0", tag: str = "", threads: int = 4, check_dci: bool = True):
-        """Every frame from now on also gets its DCI codestream on `threads` host workers."""
+                       label: str = "GAIL 1.1.0", tag: str = "", threads: int = 4, check_dci: bool = True,
+                       on_device: bool = True, tier1: bool = False):
+        """Every frame from now on also gets its DCI codestream, driven by `threads` host
+        workers: rate control and Tier-2 on the device (on_device) or on the host workers;
+        tier1: the Tier-1 frames (and hull points) also handed out in host memory."""
+        flags = (0 if on_device else 1) | (2 if tier1 else 0)
         check(lib().gb_engine_set_codestream(self.h, fps, max_mbps, comp_mbps, label.encode(), tag.encode(), threads,
-                                             int(check_dci)))
+                                             int(check_dci), flags))
+
+    def counters(self):
+        """For the engine's encodes so far: (host-to-device bytes, device-to-host bytes,
+        kernels launched)."""
+        a, b, k = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(lib().gb_engine_counters(self.h, C.byref(a), C.byref(b), C.byref(k)))
+        return a.value, b.value, k.value
+
+    def transfer_bytes(self):
+        """(host-to-device, device-to-host) bytes the engine's encodes copied so far."""
+        return self.counters()[:2]
 
     def codestream(self, rid: int, copy: bool = True):
         """(codestream bytes, or (pointer, size) without copy; DCI verdict 1/0, -1 unchecked)."""

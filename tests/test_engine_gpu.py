@@ -116,10 +116,12 @@ def test_engine_admission_by_budget(dev):
 
 
 @pytest.mark.gpu
-def test_engine_codestreams(dev):
-    """Codestreams made by the engine's host workers: each equals the host codec's on the
-    frame's plain Tier-1 output, passes the DCI check, and (for one frame) equals the
-    reference's rate control and codestream on the same Tier-1 frame."""
+@pytest.mark.parametrize("on_device", [True, False])
+def test_engine_codestreams(dev, on_device):
+    """Codestreams made by the engine (rate control and Tier-2 on the device, or on the host
+    workers): each equals the host codec's on the frame's plain Tier-1 output, passes the DCI
+    check, and (for one frame) equals the reference's rate control and codestream on the same
+    Tier-1 frame; the Tier-1 frames and hull points handed out alongside are the plain ones."""
     from libgail_b200 import codestream as CS
     from oracle.oracle import Reference, have_reference, ref_codestream
     cases = [c for c in _cases() if c[0] in ((1998, 1080, 0), (3996, 2160, 1))]
@@ -132,7 +134,7 @@ def test_engine_codestreams(dev):
     try:
         layouts = [P.LayoutHolder(W, H, fk) for (W, H, fk), _, _, _ in cases]
         classes = [eng.add_encoder(lay, fmt, col)[0] for lay, (_, fmt, col, _) in zip(layouts, cases)]
-        eng.set_codestream(fps=24.0, label=CS.DEFAULT_LABEL, tag="b200", threads=3)
+        eng.set_codestream(fps=24.0, label=CS.DEFAULT_LABEL, tag="b200", threads=3, on_device=on_device, tier1=True)
         want = {}
         for fi in range(2):
             for ci in range(len(cases)):
@@ -153,6 +155,39 @@ def test_engine_codestreams(dev):
                 ref_cs, _, _, _ = ref_codestream(Reference(), W, H, fk, alone[ci][fi], fps=24.0, tag=b"b200")
                 assert cs == ref_cs
             eng.release(rid)
+    finally:
+        eng.close()
+
+
+@pytest.mark.gpu
+def test_engine_device_codestreams_keep_tier1_on_device(dev):
+    """Device rate control without Tier-1 frames in host memory: the codestreams are the host
+    codec's, wait() hands out empty Tier-1 views, and far fewer bytes come back than the
+    Tier-1 frames hold."""
+    from libgail_b200 import codestream as CS
+    W, H = 3996, 2160
+    frames = [synth.yuv422p10(W, H, seed=600 + i) for i in range(3)]
+    lay = P.LayoutHolder(W, H, 1)
+    fmt, col = P.planar_format(W, H, bits=10, sx=1, sy=0), P.color("pq", "bt2020")
+    enc = dev.encoder(lay, fmt, col)
+    alone = [enc.encode(f)[0] for f in frames]
+    enc.close()
+    eng = Engine(0, 0, max_batch=4)
+    try:
+        cid, _ = eng.add_encoder(lay, fmt, col)
+        eng.set_codestream(label=CS.DEFAULT_LABEL, tag="b200", threads=2)
+        ids = [eng.submit(cid, f) for f in frames]
+        for _ in ids:
+            rid, t1, _, st = eng.wait(60000)
+            assert st == 0 and len(t1.info) == 0
+            cs, ok = eng.codestream(rid)
+            assert ok == 1
+            assert cs == CS.rate_and_build(lay, alone[ids.index(rid)], tag="b200")[0]
+            eng.release(rid)
+        h2d, d2h = eng.transfer_bytes()
+        tier1_bytes = sum(len(t.data) + 17 * len(t.pass_len) + 20 * len(t.info) for t in alone)
+        assert h2d == sum(f.nbytes for f in frames)
+        assert d2h < tier1_bytes / 5
     finally:
         eng.close()
 
