@@ -121,6 +121,7 @@ struct RateResult {
     CodestreamSizes sizes;
     int iterations = 0;           // exact measurements taken
     size_t d2hBytes = 0;          // device-to-host bytes the device rate control read back
+    int launches = 0;             // kernels the device rate control launched
 };
 
 // Per block, the points of the lower convex hull of its (truncation length, weighted

@@ -565,7 +565,7 @@ void EncodeEngine::codestreamWorker() {
                                         s->dHullS};
                     const RateResult rr = rc->run(f, lim, cs_.tag, r->cs, st);
                     d2h += rr.d2hBytes;
-                    launches = 4 + (uint64_t)rr.iterations;  // range, bins, measurements, offsets, packets
+                    launches = (uint64_t)rr.launches;
                 } else {
                     auto& w = writers[r->cls];
                     if (!w) w = std::make_unique<CodestreamWriter>(c->L, cs_.label);

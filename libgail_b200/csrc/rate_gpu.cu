@@ -15,6 +15,8 @@
 #include <stdexcept>
 
 #include "capi_util.h"
+#include <math_constants.h>
+
 #include "common.cuh"
 #include "encoder.h"
 #include "hull.cuh"
@@ -28,7 +30,6 @@ constexpr int kPacketBlocks = 64;     // blocks of one packet the device coder h
 constexpr int kTagNodes = 32;         // nodes of one tag tree (DCI: 4 x 4 leaves, 21 nodes)
 constexpr uint32_t kMaxAmbiguous = 4096;
 constexpr double kBinMargin = 1e-7;   // bin units from an edge within which the host bins
-constexpr int T2_WARPS = 4;
 
 struct PlanArgs {
     const int4* segs;       // x: first block, y: blocks across the band, z: ncbx | ncby << 16, w: Mb | comp << 8
@@ -221,17 +222,26 @@ __device__ uint32_t codeHeader(const PlanArgs& P, WarpPacket& W, int s0, int s1,
     return hb.end();
 }
 
-// A warp per packet. WRITE false: its size into pkBytes and its tile-part's total;
-// WRITE true: the packet at body + pkOff[p] and every block's passes into passesOut.
+// Control words of one frame's device rate control.
+struct RcCtl {
+    unsigned long long range[2];  // max of ~bits (the smallest slope), max of bits (the largest)
+    double lo, hi;                // the search bounds, log2 of the range widened by an octave
+    int nb;                       // slope bins
+    uint32_t flags;               // kFlagBins: the bins did not fit; kFlagBody: the body did not
+};
+constexpr uint32_t kFlagBins = 1u, kFlagBody = 2u;
+
+// A warp (the whole CTA) per packet: small CTAs fit beside the resident Tier-1 kernels.
+// WRITE false: the packet's size into pkBytes and its tile-part's total; WRITE true: the
+// packet at body + pkOff[p] (when it fits in bodyCap) and its blocks' passes.
 template <bool WRITE>
-__global__ void __launch_bounds__(T2_WARPS * 32) t2Kernel(PlanArgs P, FrameArgs F, double l0, double l1, double l2,
-                                                          uint32_t* pkBytes, unsigned long long* tpBytes,
-                                                          const uint32_t* pkOff, uint8_t* body, uint8_t* passesOut) {
-    __shared__ WarpPacket ws[T2_WARPS];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const uint32_t p = blockIdx.x * T2_WARPS + wid;
+__global__ void __launch_bounds__(32) t2Kernel(PlanArgs P, FrameArgs F, double l0, double l1, double l2,
+                                               uint32_t* pkBytes, unsigned long long* tpBytes, const uint32_t* pkOff,
+                                               uint8_t* body, uint64_t bodyCap, uint8_t* passesOut, RcCtl* ctl) {
+    __shared__ WarpPacket W;
+    const int lane = threadIdx.x;
+    const uint32_t p = blockIdx.x;
     if (p >= P.numPackets) return;
-    WarpPacket& W = ws[wid];
     const int s0 = P.pkSeg[p], s1 = P.pkSeg[p + 1];
     const double lam[3] = {l0, l1, l2};
     // the packet's blocks, a lane each
@@ -256,6 +266,10 @@ __global__ void __launch_bounds__(T2_WARPS * 32) t2Kernel(PlanArgs P, FrameArgs 
     }
     any = __any_sync(kFull, any);
     __syncwarp();
+    if (WRITE && (uint64_t)pkOff[p] + pkBytes[p] > bodyCap) {  // sized by the measurement before
+        if (lane == 0) atomicOr(&ctl->flags, kFlagBody);
+        return;
+    }
     uint32_t hdr = 0, bodyBytes = 0;
     if (lane == 0) hdr = codeHeader(P, W, s0, s1, any, WRITE ? body + pkOff[p] : nullptr, &bodyBytes);
     hdr = __shfl_sync(kFull, hdr, 0);
@@ -278,15 +292,12 @@ __global__ void __launch_bounds__(T2_WARPS * 32) t2Kernel(PlanArgs P, FrameArgs 
 }
 
 // Packet offsets in the codestream body: the packets before, and 14 bytes (SOT segment
-// and SOD) before each tile-part's packets. One CTA.
-__global__ void __launch_bounds__(1024) offsetsKernel(PlanArgs P, const uint32_t* pkBytes, uint32_t* pkOff) {
-    __shared__ uint32_t sW[32];
-    __shared__ uint32_t sCarry;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    if (tid == 0) sCarry = 0;
-    __syncthreads();
-    for (uint32_t base = 0; base < P.numPackets; base += 1024) {
-        const uint32_t i = base + tid;
+// and SOD) before each tile-part's packets. One warp.
+__global__ void __launch_bounds__(32) offsetsKernel(PlanArgs P, const uint32_t* pkBytes, uint32_t* pkOff) {
+    const int lane = threadIdx.x;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < P.numPackets; base += 32) {
+        const uint32_t i = base + lane;
         const uint32_t v = i < P.numPackets ? pkBytes[i] : 0u;
         uint32_t x = v;
 #pragma unroll
@@ -294,30 +305,14 @@ __global__ void __launch_bounds__(1024) offsetsKernel(PlanArgs P, const uint32_t
             const uint32_t t = __shfl_up_sync(kFull, x, o);
             if (lane >= o) x += t;
         }
-        if (lane == 31) sW[wid] = x;
-        __syncthreads();
-        if (wid == 0) {
-            const uint32_t w = sW[lane];
-            uint32_t y = w;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(kFull, y, o);
-                if (lane >= o) y += t;
-            }
-            sW[lane] = y - w;
-        }
-        __syncthreads();
-        const uint32_t carry = sCarry;
-        if (i < P.numPackets) pkOff[i] = carry + sW[wid] + x - v + 14u * (P.pkTp[i] + 1u);
-        __syncthreads();
-        if (tid == 1023) sCarry = carry + sW[wid] + x;
-        __syncthreads();
+        if (i < P.numPackets) pkOff[i] = carry + x - v + 14u * (P.pkTp[i] + 1u);
+        carry += __shfl_sync(kFull, x, 31);
     }
 }
 
-// The range of the finite positive hull slopes: range[0] = max of ~bits (the smallest),
-// range[1] = max of the bits (the largest); positive doubles order as their bit patterns.
-__global__ void __launch_bounds__(256) rangeKernel(FrameArgs F, uint32_t n, unsigned long long* range) {
+// The range of the finite positive hull slopes into ctl->range; positive doubles order as
+// their bit patterns.
+__global__ void __launch_bounds__(64) rangeKernel(FrameArgs F, uint32_t n, RcCtl* ctl) {
     unsigned long long lo = 0, hi = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const GbCblkInfo ci = F.info[i];
@@ -336,18 +331,38 @@ __global__ void __launch_bounds__(256) rangeKernel(FrameArgs F, uint32_t n, unsi
         hi = max(hi, __shfl_xor_sync(kFull, hi, o));
     }
     if ((threadIdx.x & 31) == 0) {
-        if (lo) atomicMax(&range[0], lo);
-        if (hi) atomicMax(&range[1], hi);
+        if (lo) atomicMax(&ctl->range[0], lo);
+        if (hi) atomicMax(&ctl->range[1], hi);
     }
 }
 
+// The search bounds and bin count from the range, as the host forms them but with the
+// device's log2; the host compares them with its own before it takes the bins.
+__global__ void boundsKernel(RcCtl* ctl) {
+    const unsigned long long r0 = ctl->range[0], r1 = ctl->range[1];
+    double mn = r0 ? __longlong_as_double((long long)~r0) : CUDART_INF;
+    double mx = r1 ? __longlong_as_double((long long)r1) : 0.0;
+    if (mx == 0) mx = mn = 1;
+    const double lo = log2(mn) - 1, hi = log2(mx) + 1;
+    ctl->lo = lo;
+    ctl->hi = hi;
+    ctl->nb = max(16, (int)ceil((hi - lo) * 1024.0) + 2);
+}
+
 // The slope histogram: per component, bytes (each point's rate step) and blocks (a
-// block's first point) by bin; bins is [bytes c0, c1, c2, blocks c0, c1, c2] x nb. A
-// point whose bin value lies within kBinMargin of an edge goes to amb (count, then per
-// point: comp | first << 8, bytes, slope as two words) for the host to bin.
-__global__ void __launch_bounds__(256) binsKernel(PlanArgs P, FrameArgs F, double lo, int nb, uint32_t* bins,
-                                                  uint32_t* amb) {
+// block's first point) by bin; bins is [bytes c0, c1, c2, blocks c0, c1, c2] x cap, for
+// ctl->nb <= cap bins from ctl->lo (else only the flag). A point whose bin value lies within
+// kBinMargin of an edge goes to amb (count, then per point: comp | first << 8, bytes,
+// slope as two words) for the host to bin.
+__global__ void __launch_bounds__(64) binsKernel(PlanArgs P, FrameArgs F, const RcCtl* ctlIn, RcCtl* ctl, int cap,
+                                                 uint32_t* bins, uint32_t* amb) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double lo = ctlIn->lo;
+    const int nb = ctlIn->nb;
+    if (nb > cap) {
+        if (i == 0) atomicOr(&ctl->flags, kFlagBins);
+        return;
+    }
     if (i >= P.numBlocks) return;
     const GbCblkInfo ci = F.info[i];
     const int c = P.comp[i];
@@ -367,8 +382,8 @@ __global__ void __launch_bounds__(256) binsKernel(PlanArgs P, FrameArgs F, doubl
             b = (int)fmin(fmax(fl, 0.0), (double)(nb - 1));
         }
         if (sure) {
-            atomicAdd(&bins[(size_t)c * nb + b], rate - prev);
-            if (first) atomicAdd(&bins[(size_t)(3 + c) * nb + b], 1u);
+            atomicAdd(&bins[(size_t)c * cap + b], rate - prev);
+            if (first) atomicAdd(&bins[(size_t)(3 + c) * cap + b], 1u);
         } else {
             const uint32_t slot = atomicAdd(amb, 1u);
             if (slot < kMaxAmbiguous) {
@@ -451,12 +466,16 @@ struct DeviceRateControl::Impl {
     DevBuf<uint8_t> pkTp, comp;
     DevBuf<double> scale;
     // per frame
-    DevBuf<unsigned long long> range, tp;
+    DevBuf<RcCtl> ctl;  // [0] the device's, [1] the host's bounds for a second histogram
+    DevBuf<unsigned long long> tp;
     DevBuf<uint32_t> bins, amb, pk, pkOff;
     DevBuf<uint8_t> body, passes;
-    HostBuf<unsigned long long> hRange, hTp;
+    HostBuf<RcCtl> hCtl;
+    HostBuf<unsigned long long> hTp;
     HostBuf<uint32_t> hBins, hAmb;
     HostBuf<uint8_t> hBody, hPasses;
+    int binsCap = 1 << 16;  // bins per array the histogram holds
+    int nbGuess = 48 << 10; // bins read back with the first copy (the last frame's count)
     // frames uploaded from host memory
     DevBuf<GbCblkInfo> upInfo;
     DevBuf<uint32_t> upLen;
@@ -500,112 +519,190 @@ struct DeviceRateControl::Impl {
         GB_CHECK(cudaMemcpy(comp.p, cmp.data(), cmp.size(), cudaMemcpyHostToDevice));
         GB_CHECK(cudaMemcpy(scale.p, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice));
         plan = {segs.p, pkSeg.p, pkTp.p, comp.p, (uint32_t)w.numPackets(), (uint32_t)L.numCblks()};
-        range.ensure(2);
+        ctl.ensure(2);
+        hCtl.ensure(2);
         tp.ensure((size_t)ntp);
         amb.ensure(1 + 4 * (size_t)kMaxAmbiguous);
         pk.ensure((size_t)w.numPackets());
         pkOff.ensure((size_t)w.numPackets());
         passes.ensure((size_t)L.numCblks());
-        hRange.ensure(2);
         hTp.ensure((size_t)ntp);
         hAmb.ensure(1 + 4 * (size_t)kMaxAmbiguous);
         hPasses.ensure((size_t)L.numCblks());
     }
 
+    // The tile-parts' sizes of the last measurement as CodestreamWriter::measure() reports them.
+    CodestreamSizes sizesOf(const unsigned long long* tpb) {
+        CodestreamSizes sz;
+        sz.numTileParts = ntp;
+        size_t total = w.longestHeaderBytes();
+        for (int t = 0; t < ntp; ++t) {
+            const size_t bytes = 14 + tpb[t];
+            sz.tilePart[t] = bytes;
+            sz.comp[t % 3] += bytes;
+            total += bytes;
+        }
+        sz.total = total + 2;
+        return sz;
+    }
+
+    // Reads back the first `count` bins of each of the six histogram arrays into hBins
+    // (the same layout, stride binsCap), from entry `from` on.
+    void copyBins(int from, int count, cudaStream_t st, RateResult& res) {
+        if (count <= 0) return;
+        GB_CHECK(cudaMemcpy2DAsync(hBins.p + from, (size_t)binsCap * 4, bins.p + from, (size_t)binsCap * 4,
+                                   (size_t)count * 4, 6, cudaMemcpyDeviceToHost, st));
+        res.d2hBytes += (size_t)6 * count * 4;
+    }
+
+    // Round trips to the device per frame: one for the slope range, bounds, histogram and the
+    // size with every pass; one per further size measurement, each of which also writes the
+    // packets at its thresholds and reads them back (the last one is the codestream's).
     RateResult run(const DeviceTier1& d, const RateLimits& lim, const std::string& tag, std::vector<uint8_t>& out,
                    cudaStream_t st) {
         GB_CHECK(cudaSetDevice(dev));
         const Layout& L = w.layout();
         const uint32_t n = (uint32_t)L.numCblks();
         const FrameArgs F{d.info, d.passLen, d.data, d.hullPasses, d.hullSlope};
+        const uint32_t np = plan.numPackets;
         RateResult res;
-        // the slope range and the search bounds
-        GB_CHECK(cudaMemsetAsync(range.p, 0, 16, st));
-        rangeKernel<<<std::min(divUp(n, 256u), 296u), 256, 0, st>>>(F, n, range.p);
-        GB_CHECK(cudaMemcpyAsync(hRange.p, range.p, 16, cudaMemcpyDeviceToHost, st));
-        GB_CHECK(cudaStreamSynchronize(st));
-        double minSlope = hRange.p[0] ? asDouble(~hRange.p[0]) : INFINITY;
-        double maxSlope = hRange.p[1] ? asDouble(hRange.p[1]) : 0.0;
-        double lo, hi;
-        slopeBounds(minSlope, maxSlope, lo, hi);
-        // the histogram
-        SlopeBins sb(lo, hi);
-        const int nb = sb.size();
-        bins.ensure((size_t)6 * nb);
-        hBins.ensure((size_t)6 * nb);
-        GB_CHECK(cudaMemsetAsync(bins.p, 0, (size_t)6 * nb * 4, st));
+        bins.ensure((size_t)6 * binsCap);
+        hBins.ensure((size_t)6 * binsCap);
+        constexpr uint32_t kFirst = 64;  // edge points read back with the first copy
+        // (1) range, bounds, histogram, the size with every pass
+        GB_CHECK(cudaMemsetAsync(ctl.p, 0, sizeof(RcCtl), st));
+        GB_CHECK(cudaMemsetAsync(bins.p, 0, (size_t)6 * binsCap * 4, st));
         GB_CHECK(cudaMemsetAsync(amb.p, 0, 4, st));
-        binsKernel<<<divUp(n, 256u), 256, 0, st>>>(plan, F, lo, nb, bins.p, amb.p);
-        GB_CHECK(cudaMemcpyAsync(hBins.p, bins.p, (size_t)6 * nb * 4, cudaMemcpyDeviceToHost, st));
-        // the points on bin edges: the count and the first few, the rest when there are more
-        constexpr uint32_t kFirst = 64;
+        GB_CHECK(cudaMemsetAsync(tp.p, 0, (size_t)ntp * 8, st));
+        rangeKernel<<<std::min(divUp(n, 64u), 592u), 64, 0, st>>>(F, n, ctl.p);
+        boundsKernel<<<1, 1, 0, st>>>(ctl.p);
+        binsKernel<<<divUp(n, 64u), 64, 0, st>>>(plan, F, ctl.p, ctl.p, binsCap, bins.p, amb.p);
+        t2Kernel<false><<<np, 32, 0, st>>>(plan, F, 0.0, 0.0, 0.0, pk.p, tp.p, nullptr, nullptr, 0, nullptr, ctl.p);
+        GB_CHECK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(RcCtl), cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaMemcpyAsync(hTp.p, tp.p, (size_t)ntp * 8, cudaMemcpyDeviceToHost, st));
         GB_CHECK(cudaMemcpyAsync(hAmb.p, amb.p, (1 + 4 * (size_t)kFirst) * 4, cudaMemcpyDeviceToHost, st));
+        const int guess = std::min(nbGuess, binsCap);
+        copyBins(0, guess, st, res);
         GB_CHECK(cudaStreamSynchronize(st));
         GB_CHECK(cudaGetLastError());
-        res.d2hBytes += 16 + (size_t)6 * nb * 4 + (1 + 4 * (size_t)kFirst) * 4;
-        if (hAmb.p[0] > kFirst && hAmb.p[0] <= kMaxAmbiguous) {
-            const size_t more = 4 * (size_t)(hAmb.p[0] - kFirst) * 4;
-            GB_CHECK(cudaMemcpyAsync(hAmb.p + 1 + 4 * kFirst, amb.p + 1 + 4 * kFirst, more, cudaMemcpyDeviceToHost, st));
+        res.launches += 4;
+        res.d2hBytes += sizeof(RcCtl) + (size_t)ntp * 8 + (1 + 4 * (size_t)kFirst) * 4;
+        const CodestreamSizes size0 = sizesOf(hTp.p);
+        // the host's own bounds from the exact range; the device's bins count only if its
+        // bounds are the same
+        double minSlope = hCtl.p[0].range[0] ? asDouble(~hCtl.p[0].range[0]) : INFINITY;
+        double maxSlope = hCtl.p[0].range[1] ? asDouble(hCtl.p[0].range[1]) : 0.0;
+        double lo, hi;
+        slopeBounds(minSlope, maxSlope, lo, hi);
+        SlopeBins sb(lo, hi);
+        const int nb = sb.size();
+        const bool same = hCtl.p[0].lo == lo && hCtl.p[0].hi == hi && hCtl.p[0].nb == nb &&
+                          !(hCtl.p[0].flags & kFlagBins);
+        if (!same) {  // a histogram at the host's bounds, in a larger buffer if need be
+            if (nb > binsCap) {
+                binsCap = nb + 4096;
+                bins.ensure((size_t)6 * binsCap);
+                hBins.ensure((size_t)6 * binsCap);
+            }
+            hCtl.p[1] = RcCtl{};
+            hCtl.p[1].lo = lo;
+            hCtl.p[1].hi = hi;
+            hCtl.p[1].nb = nb;
+            GB_CHECK(cudaMemcpyAsync(ctl.p + 1, hCtl.p + 1, sizeof(RcCtl), cudaMemcpyHostToDevice, st));
+            GB_CHECK(cudaMemsetAsync(bins.p, 0, (size_t)6 * binsCap * 4, st));
+            GB_CHECK(cudaMemsetAsync(amb.p, 0, 4, st));
+            binsKernel<<<divUp(n, 64u), 64, 0, st>>>(plan, F, ctl.p + 1, ctl.p, binsCap, bins.p, amb.p);
+            GB_CHECK(cudaMemcpyAsync(hAmb.p, amb.p, (1 + 4 * (size_t)kFirst) * 4, cudaMemcpyDeviceToHost, st));
+            copyBins(0, nb, st, res);
             GB_CHECK(cudaStreamSynchronize(st));
-            res.d2hBytes += more;
+            GB_CHECK(cudaGetLastError());
+            res.launches += 1;
+            res.d2hBytes += (1 + 4 * (size_t)kFirst) * 4;
+        } else if (nb > guess) {
+            copyBins(guess, nb - guess, st, res);
+            GB_CHECK(cudaStreamSynchronize(st));
         }
+        nbGuess = nb + 4096;
         for (int c = 0; c < 3; ++c)
             for (int b = 0; b < nb; ++b) {
-                const uint32_t by = hBins.p[(size_t)c * nb + b], bl = hBins.p[(size_t)(3 + c) * nb + b];
+                const uint32_t by = hBins.p[(size_t)c * binsCap + b], bl = hBins.p[(size_t)(3 + c) * binsCap + b];
                 if (by | bl) sb.add(c, b, (double)by, (double)bl);
             }
         const uint32_t na = hAmb.p[0];
         if (na > kMaxAmbiguous) throw std::runtime_error("too many hull slopes on slope-bin edges");
+        if (na > kFirst) {
+            const size_t more = 4 * (size_t)(na - kFirst) * 4;
+            GB_CHECK(cudaMemcpyAsync(hAmb.p + 1 + 4 * kFirst, amb.p + 1 + 4 * kFirst, more, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaStreamSynchronize(st));
+            res.d2hBytes += more;
+        }
         for (uint32_t a = 0; a < na; ++a) {
             const uint32_t* e = hAmb.p + 1 + 4 * a;
-            const double s = asDouble((unsigned long long)e[2] | ((unsigned long long)e[3] << 32));
-            sb.add((int)(e[0] & 255u), sb.bin(s), (double)e[1], (e[0] & 256u) ? 1.0 : 0.0);
+            const double sl = asDouble((unsigned long long)e[2] | ((unsigned long long)e[3] << 32));
+            sb.add((int)(e[0] & 255u), sb.bin(sl), (double)e[1], (e[0] & 256u) ? 1.0 : 0.0);
         }
         sb.finish();
-        // the threshold search with exact sizes measured on the device
-        const size_t hdrLongest = w.longestHeaderBytes();
-        const uint32_t t2Blocks = divUp(plan.numPackets, (uint32_t)T2_WARPS);
-        auto measure = [&](const double l[3]) {
+        // the body buffer: room for the packets with every pass (no threshold gives more)
+        uint64_t body0 = 0;
+        for (int t = 0; t < ntp; ++t) body0 += 14 + hTp.p[t];
+        const uint64_t bodyCap = body0 + 65536;
+        body.ensure(bodyCap);
+        const uint64_t bodyCopy = std::min<uint64_t>(bodyCap, (uint64_t)lim.maxTotal + 65536);
+        hBody.ensure(bodyCopy);
+        // (2) the threshold search; each measurement also writes its packets
+        bool zeroPending = true;   // the first measurement (every pass) is the one above
+        bool written = false;      // the last measurement's packets are in hBody / hPasses
+        uint64_t lastBody = 0;
+        auto measureWrite = [&](const double l[3]) {
+            ++res.iterations;
+            if (zeroPending && l[0] == 0 && l[1] == 0 && l[2] == 0) {
+                zeroPending = false;
+                written = false;
+                return size0;
+            }
+            zeroPending = false;
             GB_CHECK(cudaMemsetAsync(tp.p, 0, (size_t)ntp * 8, st));
-            t2Kernel<false><<<t2Blocks, T2_WARPS * 32, 0, st>>>(plan, F, l[0], l[1], l[2], pk.p, tp.p, nullptr, nullptr,
-                                                                 nullptr);
+            GB_CHECK(cudaMemsetAsync(&ctl.p->flags, 0, 4, st));
+            t2Kernel<false><<<np, 32, 0, st>>>(plan, F, l[0], l[1], l[2], pk.p, tp.p, nullptr, nullptr, 0, nullptr, ctl.p);
+            offsetsKernel<<<1, 32, 0, st>>>(plan, pk.p, pkOff.p);
+            t2Kernel<true><<<np, 32, 0, st>>>(plan, F, l[0], l[1], l[2], pk.p, nullptr, pkOff.p, body.p, bodyCap,
+                                              passes.p, ctl.p);
             GB_CHECK(cudaMemcpyAsync(hTp.p, tp.p, (size_t)ntp * 8, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(RcCtl), cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaMemcpyAsync(hBody.p, body.p, bodyCopy, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaMemcpyAsync(hPasses.p, passes.p, n, cudaMemcpyDeviceToHost, st));
             GB_CHECK(cudaStreamSynchronize(st));
             GB_CHECK(cudaGetLastError());
-            ++res.iterations;
-            res.d2hBytes += (size_t)ntp * 8;
-            CodestreamSizes sz;
-            sz.numTileParts = ntp;
-            size_t total = hdrLongest;
-            for (int t = 0; t < ntp; ++t) {
-                const size_t bytes = 14 + hTp.p[t];
-                sz.tilePart[t] = bytes;
-                sz.comp[t % 3] += bytes;
-                total += bytes;
-            }
-            sz.total = total + 2;
-            return sz;
+            res.launches += 3;
+            res.d2hBytes += (size_t)ntp * 8 + sizeof(RcCtl) + bodyCopy + n;
+            lastBody = 0;
+            for (int t = 0; t < ntp; ++t) lastBody += 14 + hTp.p[t];
+            written = !(hCtl.p[0].flags & kFlagBody) && lastBody <= bodyCopy;
+            return sizesOf(hTp.p);
         };
         double lam[3] = {0, 0, 0};
         CodestreamSizes sz;
-        rateSearch(lim, minSlope, maxSlope, lo, hi, sb, measure, lam, sz);
-        // the packets at the final thresholds (the last measurement's sizes)
-        uint64_t tpBytes[6] = {};
-        size_t bodyBytes = 0;
-        for (int t = 0; t < ntp; ++t) {
-            tpBytes[t] = 14 + hTp.p[t];
-            bodyBytes += tpBytes[t];
+        rateSearch(lim, minSlope, maxSlope, lo, hi, sb, measureWrite, lam, sz);
+        if (!written) {  // the frame fits with every pass, or its packets outgrew the copy
+            lastBody = 0;
+            for (int t = 0; t < ntp; ++t) lastBody += 14 + hTp.p[t];
+            if (lastBody > bodyCap) throw std::logic_error("codestream body larger than with every pass");
+            hBody.ensure(lastBody);
+            GB_CHECK(cudaMemsetAsync(&ctl.p->flags, 0, 4, st));
+            offsetsKernel<<<1, 32, 0, st>>>(plan, pk.p, pkOff.p);
+            t2Kernel<true><<<np, 32, 0, st>>>(plan, F, lam[0], lam[1], lam[2], pk.p, nullptr, pkOff.p, body.p, bodyCap,
+                                              passes.p, ctl.p);
+            GB_CHECK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(RcCtl), cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaMemcpyAsync(hBody.p, body.p, lastBody, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaMemcpyAsync(hPasses.p, passes.p, n, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaStreamSynchronize(st));
+            GB_CHECK(cudaGetLastError());
+            if (hCtl.p[0].flags & kFlagBody) throw std::logic_error("codestream body outgrew its buffer");
+            res.launches += 2;
+            res.d2hBytes += sizeof(RcCtl) + lastBody + n;
         }
-        body.ensure(bodyBytes);
-        hBody.ensure(bodyBytes);
-        offsetsKernel<<<1, 1024, 0, st>>>(plan, pk.p, pkOff.p);
-        t2Kernel<true><<<t2Blocks, T2_WARPS * 32, 0, st>>>(plan, F, lam[0], lam[1], lam[2], nullptr, nullptr, pkOff.p,
-                                                            body.p, passes.p);
-        GB_CHECK(cudaMemcpyAsync(hBody.p, body.p, bodyBytes, cudaMemcpyDeviceToHost, st));
-        GB_CHECK(cudaMemcpyAsync(hPasses.p, passes.p, n, cudaMemcpyDeviceToHost, st));
-        GB_CHECK(cudaStreamSynchronize(st));
-        GB_CHECK(cudaGetLastError());
-        res.d2hBytes += bodyBytes + n;
+        uint64_t tpBytes[6] = {};
+        for (int t = 0; t < ntp; ++t) tpBytes[t] = 14 + hTp.p[t];
         const CodestreamSizes made = w.assemble(hBody.p, tpBytes, tag, out);
         if (made.total != sz.total) throw std::logic_error("device codestream size differs from its measurement");
         res.passes.assign(hPasses.p, hPasses.p + n);
