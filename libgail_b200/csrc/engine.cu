@@ -100,6 +100,15 @@ struct EncodeEngine::DecSlot {
     std::unique_ptr<DecoderSlot> slot;
 };
 
+struct EncodeEngine::WorkerRc {
+    cudaStream_t st = nullptr;
+    std::vector<std::unique_ptr<DeviceRateControl>> rc;  // by frame class
+    ~WorkerRc() {
+        rc.clear();
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
 struct EncodeEngine::Batch {
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
@@ -150,6 +159,7 @@ EncodeEngine::~EncodeEngine() {
         if (t.joinable()) t.join();
     cudaSetDevice(dev_);
     cudaDeviceSynchronize();
+    workerRc_.clear();
     for (auto& s : slots_) {
         if (s->exec) cudaGraphExecDestroy(s->exec);
         if (s->graph) cudaGraphDestroy(s->graph);
@@ -211,6 +221,7 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
     if (frameBytes) *frameBytes = c->slotBytes;
     std::lock_guard<std::mutex> lock(m_);
     classes_.push_back(std::move(c));
+    if (csOn_ && cs_.onDevice) prepareRc();
     return (int)classes_.size() - 1;
 }
 
@@ -377,13 +388,34 @@ void EncodeEngine::setCodestream(const CodestreamConfig& c) {
     std::lock_guard<std::mutex> lock(m_);
     if (csOn_) throw std::logic_error("codestreams are already on");
     cs_ = c;
-    csOn_ = true;
     startWorkers(c.threads);
+    if (c.onDevice) prepareRc();
+    csOn_ = true;
 }
 
 // Grows the pool of host workers to at least n (m_ held).
 void EncodeEngine::startWorkers(int n) {
-    while ((int)csWorkers_.size() < n) csWorkers_.emplace_back([this] { codestreamWorker(); });
+    while ((int)csWorkers_.size() < n) {
+        const int id = (int)csWorkers_.size();
+        csWorkers_.emplace_back([this, id] { codestreamWorker(id); });
+    }
+}
+
+// A stream and a device rate control per frame class for every worker (m_ held).
+void EncodeEngine::prepareRc() {
+    GB_CHECK(cudaSetDevice(dev_));
+    const RateLimits lim = dciLimits(cs_.fps, cs_.maxMbps, cs_.compMbps);
+    const size_t hint = 2 * lim.maxTotal + (64u << 10);
+    while (workerRc_.size() < csWorkers_.size()) workerRc_.push_back(std::make_unique<WorkerRc>());
+    for (auto& w : workerRc_) {
+        if (!w->st) {
+            int lo = 0, hi = 0;
+            GB_CHECK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            GB_CHECK(cudaStreamCreateWithPriority(&w->st, cudaStreamNonBlocking, hi));
+        }
+        while (w->rc.size() < classes_.size())
+            w->rc.push_back(std::make_unique<DeviceRateControl>(dev_, classes_[w->rc.size()]->L, cs_.label, hint));
+    }
 }
 
 int EncodeEngine::addDecodeClass(const GailCudaLayout& layout, const GailCudaDecodeSettings& s, uint64_t* frameBytes) {
@@ -397,6 +429,7 @@ int EncodeEngine::addDecodeClass(const GailCudaLayout& layout, const GailCudaDec
     std::lock_guard<std::mutex> lock(m_);
     decClasses_.push_back(std::move(c));
     startWorkers(4);
+    if (csOn_ && cs_.onDevice) prepareRc();
     return (int)decClasses_.size() - 1;
 }
 
@@ -507,23 +540,18 @@ bool EncodeEngine::codestream(int64_t id, const uint8_t** data, uint64_t* size, 
     return true;
 }
 
-void EncodeEngine::codestreamWorker() {
+void EncodeEngine::codestreamWorker(int id) {
     cudaSetDevice(dev_);
-    // one writer (host path) or device rate control per frame class on this worker (the
-    // packet order is flattened once), the latter on the worker's own stream at the
-    // highest priority, so that its short launches go ahead of the Tier-1 batches
+    // one writer per frame class on this worker for the host path (the packet order is
+    // flattened once); the device path uses the worker's device rate controls, on its own
+    // stream at the highest priority, so that their short launches go ahead of the Tier-1
+    // batches
     std::vector<std::unique_ptr<CodestreamWriter>> writers;
-    std::vector<std::unique_ptr<DeviceRateControl>> drc;
-    cudaStream_t st = nullptr;
-    struct StreamGuard {
-        cudaStream_t& s;
-        ~StreamGuard() {
-            if (s) cudaStreamDestroy(s);
-        }
-    } guard{st};
     for (;;) {
         Request* r;
         const Class* c = nullptr;
+        DeviceRateControl* rc = nullptr;
+        cudaStream_t st = nullptr;
         {
             std::unique_lock<std::mutex> lock(m_);
             cvCs_.wait(lock, [&] { return stop_.load() || !csq_.empty(); });
@@ -533,7 +561,10 @@ void EncodeEngine::codestreamWorker() {
             if (!r->decode) {
                 c = classes_[r->cls].get();
                 if (writers.size() < classes_.size()) writers.resize(classes_.size());
-                if (drc.size() < classes_.size()) drc.resize(classes_.size());
+                if (r->devFrame && (size_t)id < workerRc_.size() && (size_t)r->cls < workerRc_[id]->rc.size()) {
+                    rc = workerRc_[id]->rc[r->cls].get();
+                    st = workerRc_[id]->st;
+                }
             }
         }
         if (r->decode) {
@@ -552,15 +583,7 @@ void EncodeEngine::codestreamWorker() {
         if (r->status == kOk) {
             try {
                 if (r->devFrame) {
-                    auto& rc = drc[r->cls];
-                    if (!rc) {
-                        if (!st) {
-                            int lo = 0, hi = 0;
-                            GB_CHECK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-                            GB_CHECK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi));
-                        }
-                        rc = std::make_unique<DeviceRateControl>(dev_, c->L, cs_.label);
-                    }
+                    if (!rc) throw std::logic_error("no device rate control for this worker and class");
                     const DeviceTier1 f{reinterpret_cast<const GbCblkInfo*>(s->dInfoP), s->dLenP, s->dDataP, s->dHullP,
                                         s->dHullS};
                     const RateResult rr = rc->run(f, lim, cs_.tag, r->cs, st);

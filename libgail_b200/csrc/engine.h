@@ -109,9 +109,10 @@ private:
     struct DecSlot;
 
     void run();
-    void codestreamWorker();
+    void codestreamWorker(int id);
     void decodeJob(Request* r);
     void startWorkers(int n);
+    void prepareRc();
     bool admit();
     bool launchBatch(Batch& b);
     bool collect(Batch& b);
@@ -147,6 +148,10 @@ private:
     std::deque<Request*> csq_;  // Tier-1 done, codestream to make; or a decode to run
     std::condition_variable cvCs_;
     std::vector<std::thread> csWorkers_;
+    // per worker: its stream and a device rate control per frame class, made before any
+    // frame needs them (their buffers are allocated once, not while frames are served)
+    struct WorkerRc;
+    std::vector<std::unique_ptr<WorkerRc>> workerRc_;
     // decode requests
     std::vector<std::unique_ptr<DecClass>> decClasses_;
     std::vector<std::unique_ptr<DecSlot>> decSlots_;

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <stdexcept>
 
@@ -456,26 +457,40 @@ struct HostBuf {  // a growable pinned host buffer
 
 }  // namespace
 
+// The control words, tile-part totals and edge points of one frame, one block of device
+// memory so that each round trip clears and reads back one range.
+struct RcState {
+    RcCtl ctl;
+    unsigned long long tp[8];
+    uint32_t amb[1 + 4 * kMaxAmbiguous];
+};
+constexpr uint32_t kFirstAmb = 64;  // edge points read back with the first copy
+constexpr size_t kHeadBytes = offsetof(RcState, amb) + 4;                  // ctl, tp, edge count
+constexpr size_t kFirstBytes = offsetof(RcState, amb) + (1 + 4 * kFirstAmb) * 4;
+constexpr size_t kFlagsAt = offsetof(RcState, ctl) + offsetof(RcCtl, flags);
+constexpr size_t kMeasureBytes = offsetof(RcState, amb);                   // ctl and tp
+
 struct DeviceRateControl::Impl {
     int dev;
     CodestreamWriter w;
     PlanArgs plan{};
     int ntp = 0;
+    uint32_t n = 0, nPad = 0;  // blocks; the passes' bytes at the head of the output buffer
     DevBuf<int4> segs;
     DevBuf<int32_t> pkSeg;
     DevBuf<uint8_t> pkTp, comp;
     DevBuf<double> scale;
-    // per frame
-    DevBuf<RcCtl> ctl;  // [0] the device's, [1] the host's bounds for a second histogram
-    DevBuf<unsigned long long> tp;
-    DevBuf<uint32_t> bins, amb, pk, pkOff;
-    DevBuf<uint8_t> body, passes;
-    HostBuf<RcCtl> hCtl;
-    HostBuf<unsigned long long> hTp;
-    HostBuf<uint32_t> hBins, hAmb;
-    HostBuf<uint8_t> hBody, hPasses;
-    int binsCap = 1 << 16;  // bins per array the histogram holds
-    int nbGuess = 48 << 10; // bins read back with the first copy (the last frame's count)
+    // per frame, sized once
+    DevBuf<RcState> state;
+    DevBuf<RcCtl> ctl2;  // the host's bounds, for a second histogram
+    DevBuf<uint32_t> bins, pk, pkOff;
+    DevBuf<uint8_t> outBuf;  // passes (nPad bytes), then the codestream body
+    HostBuf<RcState> hState;
+    HostBuf<RcCtl> hCtl2;
+    HostBuf<uint32_t> hBins;
+    HostBuf<uint8_t> hOut;
+    int binsCap = 1 << 16;   // bins per array the histogram holds
+    int nbGuess = 48 << 10;  // bins read back with the first copy (the last frame's count)
     // frames uploaded from host memory
     DevBuf<GbCblkInfo> upInfo;
     DevBuf<uint32_t> upLen;
@@ -483,12 +498,13 @@ struct DeviceRateControl::Impl {
     DevBuf<uint8_t> upData, upHp;
     DevBuf<double> upHs;
 
-    Impl(int device, const Layout& L, const std::string& label) : dev(device), w(L, label) {
+    Impl(int device, const Layout& L, const std::string& label, size_t bodyHint) : dev(device), w(L, label) {
         GB_CHECK(cudaSetDevice(dev));
         const auto& sg = w.segments();
         const auto& ps = w.packetSegments();
         const auto& tps = w.tilePartPackets();
         ntp = w.numTileParts();
+        if (ntp > 8) throw std::logic_error("more tile-parts than the device rate control counts");
         std::vector<int4> hs(sg.size());
         for (size_t s = 0; s < sg.size(); ++s) {
             const auto& g = sg[s];
@@ -505,8 +521,10 @@ struct DeviceRateControl::Impl {
             for (int s = ps[(size_t)p]; s < ps[(size_t)p + 1]; ++s) blocks += sg[(size_t)s].ncbx * sg[(size_t)s].ncby;
             if (blocks > kPacketBlocks) throw std::logic_error("packet with too many code-blocks for the device Tier-2");
         }
-        std::vector<uint8_t> cmp((size_t)L.numCblks());
-        for (int i = 0; i < L.numCblks(); ++i) cmp[(size_t)i] = (uint8_t)L.bands[L.cblks[(size_t)i].band].comp;
+        n = (uint32_t)L.numCblks();
+        nPad = (n + 15u) & ~15u;
+        std::vector<uint8_t> cmp(n);
+        for (uint32_t i = 0; i < n; ++i) cmp[i] = (uint8_t)L.bands[L.cblks[i].band].comp;
         const std::vector<double> sc = blockScales(L);
         segs.ensure(hs.size());
         pkSeg.ensure(ps.size());
@@ -518,17 +536,17 @@ struct DeviceRateControl::Impl {
         GB_CHECK(cudaMemcpy(pkTp.p, tpOf.data(), tpOf.size(), cudaMemcpyHostToDevice));
         GB_CHECK(cudaMemcpy(comp.p, cmp.data(), cmp.size(), cudaMemcpyHostToDevice));
         GB_CHECK(cudaMemcpy(scale.p, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice));
-        plan = {segs.p, pkSeg.p, pkTp.p, comp.p, (uint32_t)w.numPackets(), (uint32_t)L.numCblks()};
-        ctl.ensure(2);
-        hCtl.ensure(2);
-        tp.ensure((size_t)ntp);
-        amb.ensure(1 + 4 * (size_t)kMaxAmbiguous);
+        plan = {segs.p, pkSeg.p, pkTp.p, comp.p, (uint32_t)w.numPackets(), n};
+        state.ensure(1);
+        ctl2.ensure(1);
+        hState.ensure(1);
+        hCtl2.ensure(1);
         pk.ensure((size_t)w.numPackets());
         pkOff.ensure((size_t)w.numPackets());
-        passes.ensure((size_t)L.numCblks());
-        hTp.ensure((size_t)ntp);
-        hAmb.ensure(1 + 4 * (size_t)kMaxAmbiguous);
-        hPasses.ensure((size_t)L.numCblks());
+        bins.ensure((size_t)6 * binsCap);
+        hBins.ensure((size_t)6 * binsCap);
+        outBuf.ensure(nPad + bodyHint);
+        hOut.ensure(nPad + bodyHint);
     }
 
     // The tile-parts' sizes of the last measurement as CodestreamWriter::measure() reports them.
@@ -546,13 +564,27 @@ struct DeviceRateControl::Impl {
         return sz;
     }
 
-    // Reads back the first `count` bins of each of the six histogram arrays into hBins
-    // (the same layout, stride binsCap), from entry `from` on.
+    uint64_t bodyBytesOf(const unsigned long long* tpb) const {
+        uint64_t b = 0;
+        for (int t = 0; t < ntp; ++t) b += 14 + tpb[t];
+        return b;
+    }
+
+    // Reads back `count` bins of each of the six histogram arrays into hBins (the same
+    // layout, stride binsCap), from entry `from` on.
     void copyBins(int from, int count, cudaStream_t st, RateResult& res) {
         if (count <= 0) return;
         GB_CHECK(cudaMemcpy2DAsync(hBins.p + from, (size_t)binsCap * 4, bins.p + from, (size_t)binsCap * 4,
                                    (size_t)count * 4, 6, cudaMemcpyDeviceToHost, st));
         res.d2hBytes += (size_t)6 * count * 4;
+    }
+
+    // The packets at thresholds l into outBuf (passes, then the body from nPad), with the
+    // offsets from the sizes in pk.
+    void enqueueWrite(const FrameArgs& F, const double l[3], cudaStream_t st) {
+        offsetsKernel<<<1, 32, 0, st>>>(plan, pk.p, pkOff.p);
+        t2Kernel<true><<<plan.numPackets, 32, 0, st>>>(plan, F, l[0], l[1], l[2], pk.p, nullptr, pkOff.p, outBuf.p + nPad,
+                                                       outBuf.cap - nPad, outBuf.p, &state.p->ctl);
     }
 
     // Round trips to the device per frame: one for the slope range, bounds, histogram and the
@@ -561,63 +593,57 @@ struct DeviceRateControl::Impl {
     RateResult run(const DeviceTier1& d, const RateLimits& lim, const std::string& tag, std::vector<uint8_t>& out,
                    cudaStream_t st) {
         GB_CHECK(cudaSetDevice(dev));
-        const Layout& L = w.layout();
-        const uint32_t n = (uint32_t)L.numCblks();
         const FrameArgs F{d.info, d.passLen, d.data, d.hullPasses, d.hullSlope};
         const uint32_t np = plan.numPackets;
+        RcState* S = state.p;
+        RcState& H = *hState.p;
+        hOut.ensure(outBuf.cap);
         RateResult res;
-        bins.ensure((size_t)6 * binsCap);
-        hBins.ensure((size_t)6 * binsCap);
-        constexpr uint32_t kFirst = 64;  // edge points read back with the first copy
         // (1) range, bounds, histogram, the size with every pass
-        GB_CHECK(cudaMemsetAsync(ctl.p, 0, sizeof(RcCtl), st));
+        GB_CHECK(cudaMemsetAsync(S, 0, kHeadBytes, st));
         GB_CHECK(cudaMemsetAsync(bins.p, 0, (size_t)6 * binsCap * 4, st));
-        GB_CHECK(cudaMemsetAsync(amb.p, 0, 4, st));
-        GB_CHECK(cudaMemsetAsync(tp.p, 0, (size_t)ntp * 8, st));
-        rangeKernel<<<std::min(divUp(n, 64u), 592u), 64, 0, st>>>(F, n, ctl.p);
-        boundsKernel<<<1, 1, 0, st>>>(ctl.p);
-        binsKernel<<<divUp(n, 64u), 64, 0, st>>>(plan, F, ctl.p, ctl.p, binsCap, bins.p, amb.p);
-        t2Kernel<false><<<np, 32, 0, st>>>(plan, F, 0.0, 0.0, 0.0, pk.p, tp.p, nullptr, nullptr, 0, nullptr, ctl.p);
-        GB_CHECK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(RcCtl), cudaMemcpyDeviceToHost, st));
-        GB_CHECK(cudaMemcpyAsync(hTp.p, tp.p, (size_t)ntp * 8, cudaMemcpyDeviceToHost, st));
-        GB_CHECK(cudaMemcpyAsync(hAmb.p, amb.p, (1 + 4 * (size_t)kFirst) * 4, cudaMemcpyDeviceToHost, st));
+        rangeKernel<<<std::min(divUp(n, 64u), 592u), 64, 0, st>>>(F, n, &S->ctl);
+        boundsKernel<<<1, 1, 0, st>>>(&S->ctl);
+        binsKernel<<<divUp(n, 64u), 64, 0, st>>>(plan, F, &S->ctl, &S->ctl, binsCap, bins.p, S->amb);
+        t2Kernel<false><<<np, 32, 0, st>>>(plan, F, 0.0, 0.0, 0.0, pk.p, S->tp, nullptr, nullptr, 0, nullptr, &S->ctl);
+        GB_CHECK(cudaMemcpyAsync(&H, S, kFirstBytes, cudaMemcpyDeviceToHost, st));
         const int guess = std::min(nbGuess, binsCap);
         copyBins(0, guess, st, res);
         GB_CHECK(cudaStreamSynchronize(st));
         GB_CHECK(cudaGetLastError());
         res.launches += 4;
-        res.d2hBytes += sizeof(RcCtl) + (size_t)ntp * 8 + (1 + 4 * (size_t)kFirst) * 4;
-        const CodestreamSizes size0 = sizesOf(hTp.p);
+        res.d2hBytes += kFirstBytes;
+        const CodestreamSizes size0 = sizesOf(H.tp);
+        const uint64_t body0 = bodyBytesOf(H.tp);
         // the host's own bounds from the exact range; the device's bins count only if its
         // bounds are the same
-        double minSlope = hCtl.p[0].range[0] ? asDouble(~hCtl.p[0].range[0]) : INFINITY;
-        double maxSlope = hCtl.p[0].range[1] ? asDouble(hCtl.p[0].range[1]) : 0.0;
+        double minSlope = H.ctl.range[0] ? asDouble(~H.ctl.range[0]) : INFINITY;
+        double maxSlope = H.ctl.range[1] ? asDouble(H.ctl.range[1]) : 0.0;
         double lo, hi;
         slopeBounds(minSlope, maxSlope, lo, hi);
         SlopeBins sb(lo, hi);
         const int nb = sb.size();
-        const bool same = hCtl.p[0].lo == lo && hCtl.p[0].hi == hi && hCtl.p[0].nb == nb &&
-                          !(hCtl.p[0].flags & kFlagBins);
+        const bool same = H.ctl.lo == lo && H.ctl.hi == hi && H.ctl.nb == nb && !(H.ctl.flags & kFlagBins);
         if (!same) {  // a histogram at the host's bounds, in a larger buffer if need be
             if (nb > binsCap) {
                 binsCap = nb + 4096;
                 bins.ensure((size_t)6 * binsCap);
                 hBins.ensure((size_t)6 * binsCap);
             }
-            hCtl.p[1] = RcCtl{};
-            hCtl.p[1].lo = lo;
-            hCtl.p[1].hi = hi;
-            hCtl.p[1].nb = nb;
-            GB_CHECK(cudaMemcpyAsync(ctl.p + 1, hCtl.p + 1, sizeof(RcCtl), cudaMemcpyHostToDevice, st));
+            *hCtl2.p = RcCtl{};
+            hCtl2.p->lo = lo;
+            hCtl2.p->hi = hi;
+            hCtl2.p->nb = nb;
+            GB_CHECK(cudaMemcpyAsync(ctl2.p, hCtl2.p, sizeof(RcCtl), cudaMemcpyHostToDevice, st));
             GB_CHECK(cudaMemsetAsync(bins.p, 0, (size_t)6 * binsCap * 4, st));
-            GB_CHECK(cudaMemsetAsync(amb.p, 0, 4, st));
-            binsKernel<<<divUp(n, 64u), 64, 0, st>>>(plan, F, ctl.p + 1, ctl.p, binsCap, bins.p, amb.p);
-            GB_CHECK(cudaMemcpyAsync(hAmb.p, amb.p, (1 + 4 * (size_t)kFirst) * 4, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaMemsetAsync(S->amb, 0, 4, st));
+            binsKernel<<<divUp(n, 64u), 64, 0, st>>>(plan, F, ctl2.p, &S->ctl, binsCap, bins.p, S->amb);
+            GB_CHECK(cudaMemcpyAsync(H.amb, S->amb, (1 + 4 * kFirstAmb) * 4, cudaMemcpyDeviceToHost, st));
             copyBins(0, nb, st, res);
             GB_CHECK(cudaStreamSynchronize(st));
             GB_CHECK(cudaGetLastError());
             res.launches += 1;
-            res.d2hBytes += (1 + 4 * (size_t)kFirst) * 4;
+            res.d2hBytes += (1 + 4 * kFirstAmb) * 4;
         } else if (nb > guess) {
             copyBins(guess, nb - guess, st, res);
             GB_CHECK(cudaStreamSynchronize(st));
@@ -628,31 +654,26 @@ struct DeviceRateControl::Impl {
                 const uint32_t by = hBins.p[(size_t)c * binsCap + b], bl = hBins.p[(size_t)(3 + c) * binsCap + b];
                 if (by | bl) sb.add(c, b, (double)by, (double)bl);
             }
-        const uint32_t na = hAmb.p[0];
+        const uint32_t na = H.amb[0];
         if (na > kMaxAmbiguous) throw std::runtime_error("too many hull slopes on slope-bin edges");
-        if (na > kFirst) {
-            const size_t more = 4 * (size_t)(na - kFirst) * 4;
-            GB_CHECK(cudaMemcpyAsync(hAmb.p + 1 + 4 * kFirst, amb.p + 1 + 4 * kFirst, more, cudaMemcpyDeviceToHost, st));
+        if (na > kFirstAmb) {
+            const size_t more = 4 * (size_t)(na - kFirstAmb) * 4;
+            GB_CHECK(cudaMemcpyAsync(H.amb + 1 + 4 * kFirstAmb, S->amb + 1 + 4 * kFirstAmb, more, cudaMemcpyDeviceToHost,
+                                     st));
             GB_CHECK(cudaStreamSynchronize(st));
             res.d2hBytes += more;
         }
         for (uint32_t a = 0; a < na; ++a) {
-            const uint32_t* e = hAmb.p + 1 + 4 * a;
+            const uint32_t* e = H.amb + 1 + 4 * a;
             const double sl = asDouble((unsigned long long)e[2] | ((unsigned long long)e[3] << 32));
             sb.add((int)(e[0] & 255u), sb.bin(sl), (double)e[1], (e[0] & 256u) ? 1.0 : 0.0);
         }
         sb.finish();
-        // the body buffer: room for the packets with every pass (no threshold gives more)
-        uint64_t body0 = 0;
-        for (int t = 0; t < ntp; ++t) body0 += 14 + hTp.p[t];
-        const uint64_t bodyCap = body0 + 65536;
-        body.ensure(bodyCap);
-        const uint64_t bodyCopy = std::min<uint64_t>(bodyCap, (uint64_t)lim.maxTotal + 65536);
-        hBody.ensure(bodyCopy);
-        // (2) the threshold search; each measurement also writes its packets
-        bool zeroPending = true;   // the first measurement (every pass) is the one above
-        bool written = false;      // the last measurement's packets are in hBody / hPasses
-        uint64_t lastBody = 0;
+        // (2) the threshold search; each measurement also writes its packets and reads back
+        // as much of them as a codestream under the limit can hold
+        const uint64_t bodyCopy = std::min<uint64_t>(outBuf.cap - nPad, (uint64_t)lim.maxTotal + 65536);
+        bool zeroPending = true;  // the first measurement (every pass) is the one above
+        bool written = false;     // the last measurement's packets are in hOut
         auto measureWrite = [&](const double l[3]) {
             ++res.iterations;
             if (zeroPending && l[0] == 0 && l[1] == 0 && l[2] == 0) {
@@ -661,51 +682,42 @@ struct DeviceRateControl::Impl {
                 return size0;
             }
             zeroPending = false;
-            GB_CHECK(cudaMemsetAsync(tp.p, 0, (size_t)ntp * 8, st));
-            GB_CHECK(cudaMemsetAsync(&ctl.p->flags, 0, 4, st));
-            t2Kernel<false><<<np, 32, 0, st>>>(plan, F, l[0], l[1], l[2], pk.p, tp.p, nullptr, nullptr, 0, nullptr, ctl.p);
-            offsetsKernel<<<1, 32, 0, st>>>(plan, pk.p, pkOff.p);
-            t2Kernel<true><<<np, 32, 0, st>>>(plan, F, l[0], l[1], l[2], pk.p, nullptr, pkOff.p, body.p, bodyCap,
-                                              passes.p, ctl.p);
-            GB_CHECK(cudaMemcpyAsync(hTp.p, tp.p, (size_t)ntp * 8, cudaMemcpyDeviceToHost, st));
-            GB_CHECK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(RcCtl), cudaMemcpyDeviceToHost, st));
-            GB_CHECK(cudaMemcpyAsync(hBody.p, body.p, bodyCopy, cudaMemcpyDeviceToHost, st));
-            GB_CHECK(cudaMemcpyAsync(hPasses.p, passes.p, n, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaMemsetAsync(reinterpret_cast<uint8_t*>(S) + kFlagsAt, 0, kMeasureBytes - kFlagsAt, st));
+            t2Kernel<false><<<np, 32, 0, st>>>(plan, F, l[0], l[1], l[2], pk.p, S->tp, nullptr, nullptr, 0, nullptr,
+                                               &S->ctl);
+            enqueueWrite(F, l, st);
+            GB_CHECK(cudaMemcpyAsync(&H, S, kMeasureBytes, cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaMemcpyAsync(hOut.p, outBuf.p, nPad + bodyCopy, cudaMemcpyDeviceToHost, st));
             GB_CHECK(cudaStreamSynchronize(st));
             GB_CHECK(cudaGetLastError());
             res.launches += 3;
-            res.d2hBytes += (size_t)ntp * 8 + sizeof(RcCtl) + bodyCopy + n;
-            lastBody = 0;
-            for (int t = 0; t < ntp; ++t) lastBody += 14 + hTp.p[t];
-            written = !(hCtl.p[0].flags & kFlagBody) && lastBody <= bodyCopy;
-            return sizesOf(hTp.p);
+            res.d2hBytes += kMeasureBytes + nPad + bodyCopy;
+            written = !(H.ctl.flags & kFlagBody) && bodyBytesOf(H.tp) <= bodyCopy;
+            return sizesOf(H.tp);
         };
         double lam[3] = {0, 0, 0};
         CodestreamSizes sz;
         rateSearch(lim, minSlope, maxSlope, lo, hi, sb, measureWrite, lam, sz);
-        if (!written) {  // the frame fits with every pass, or its packets outgrew the copy
-            lastBody = 0;
-            for (int t = 0; t < ntp; ++t) lastBody += 14 + hTp.p[t];
-            if (lastBody > bodyCap) throw std::logic_error("codestream body larger than with every pass");
-            hBody.ensure(lastBody);
-            GB_CHECK(cudaMemsetAsync(&ctl.p->flags, 0, 4, st));
-            offsetsKernel<<<1, 32, 0, st>>>(plan, pk.p, pkOff.p);
-            t2Kernel<true><<<np, 32, 0, st>>>(plan, F, lam[0], lam[1], lam[2], pk.p, nullptr, pkOff.p, body.p, bodyCap,
-                                              passes.p, ctl.p);
-            GB_CHECK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(RcCtl), cudaMemcpyDeviceToHost, st));
-            GB_CHECK(cudaMemcpyAsync(hBody.p, body.p, lastBody, cudaMemcpyDeviceToHost, st));
-            GB_CHECK(cudaMemcpyAsync(hPasses.p, passes.p, n, cudaMemcpyDeviceToHost, st));
+        const uint64_t body = bodyBytesOf(H.tp);
+        if (!written) {  // the frame fits with every pass, or its packets outgrew the buffer or the copy
+            if (body > body0) throw std::logic_error("codestream body larger than with every pass");
+            if (nPad + body > outBuf.cap) outBuf.ensure(nPad + body + 65536);
+            hOut.ensure(nPad + body);
+            GB_CHECK(cudaMemsetAsync(reinterpret_cast<uint8_t*>(S) + kFlagsAt, 0, 4, st));
+            enqueueWrite(F, lam, st);
+            GB_CHECK(cudaMemcpyAsync(&H.ctl, &S->ctl, sizeof(RcCtl), cudaMemcpyDeviceToHost, st));
+            GB_CHECK(cudaMemcpyAsync(hOut.p, outBuf.p, nPad + body, cudaMemcpyDeviceToHost, st));
             GB_CHECK(cudaStreamSynchronize(st));
             GB_CHECK(cudaGetLastError());
-            if (hCtl.p[0].flags & kFlagBody) throw std::logic_error("codestream body outgrew its buffer");
+            if (H.ctl.flags & kFlagBody) throw std::logic_error("codestream body outgrew its buffer");
             res.launches += 2;
-            res.d2hBytes += sizeof(RcCtl) + lastBody + n;
+            res.d2hBytes += sizeof(RcCtl) + nPad + body;
         }
-        uint64_t tpBytes[6] = {};
-        for (int t = 0; t < ntp; ++t) tpBytes[t] = 14 + hTp.p[t];
-        const CodestreamSizes made = w.assemble(hBody.p, tpBytes, tag, out);
+        uint64_t tpBytes[8] = {};
+        for (int t = 0; t < ntp; ++t) tpBytes[t] = 14 + H.tp[t];
+        const CodestreamSizes made = w.assemble(hOut.p + nPad, tpBytes, tag, out);
         if (made.total != sz.total) throw std::logic_error("device codestream size differs from its measurement");
-        res.passes.assign(hPasses.p, hPasses.p + n);
+        res.passes.assign(hOut.p, hOut.p + n);
         res.lambda = std::max({lam[0], lam[1], lam[2]});
         for (int c = 0; c < 3; ++c) res.lambdaComp[c] = lam[c];
         res.distortion = NAN;
@@ -716,7 +728,6 @@ struct DeviceRateControl::Impl {
     RateResult runHost(const Tier1View& t1, const RateLimits& lim, const std::string& tag, std::vector<uint8_t>& out,
                        cudaStream_t st) {
         GB_CHECK(cudaSetDevice(dev));
-        const uint32_t n = (uint32_t)w.layout().numCblks();
         if (t1.numInfo != n) throw std::logic_error("Tier-1 frame and layout have different code-block counts");
         for (uint32_t i = 0; i < n; ++i) {
             const GbCblkInfo& c = t1.info[i];
@@ -725,13 +736,13 @@ struct DeviceRateControl::Impl {
                 if (t1.passLen[c.passBase + k] < t1.passLen[c.passBase + k - 1])
                     throw std::logic_error("pass lengths that decrease");
         }
-        const size_t np = std::max<size_t>(t1.numPasses, 1), nd = std::max<size_t>(t1.numData, 1);
+        const size_t npass = std::max<size_t>(t1.numPasses, 1), nd = std::max<size_t>(t1.numData, 1);
         upInfo.ensure(n);
-        upLen.ensure(np);
-        upDist.ensure(np);
+        upLen.ensure(npass);
+        upDist.ensure(npass);
         upData.ensure(nd);
-        upHp.ensure(np);
-        upHs.ensure(np);
+        upHp.ensure(npass);
+        upHs.ensure(npass);
         GB_CHECK(cudaMemcpyAsync(upInfo.p, t1.info, (size_t)n * sizeof(GbCblkInfo), cudaMemcpyHostToDevice, st));
         if (t1.numPasses) {
             GB_CHECK(cudaMemcpyAsync(upLen.p, t1.passLen, (size_t)t1.numPasses * 4, cudaMemcpyHostToDevice, st));
@@ -742,12 +753,14 @@ struct DeviceRateControl::Impl {
                                                                                    n, upHp.p, upHs.p);
         GB_CHECK(cudaGetLastError());
         DeviceTier1 d{upInfo.p, upLen.p, upData.p, upHp.p, upHs.p};
-        return run(d, lim, tag, out, st);
+        RateResult r = run(d, lim, tag, out, st);
+        r.launches += 1;
+        return r;
     }
 };
 
-DeviceRateControl::DeviceRateControl(int device, const Layout& L, const std::string& label)
-    : p_(std::make_unique<Impl>(device, L, label)) {}
+DeviceRateControl::DeviceRateControl(int device, const Layout& L, const std::string& label, size_t bodyHint)
+    : p_(std::make_unique<Impl>(device, L, label, bodyHint)) {}
 DeviceRateControl::~DeviceRateControl() = default;
 
 RateResult DeviceRateControl::run(const DeviceTier1& f, const RateLimits& lim, const std::string& tag,

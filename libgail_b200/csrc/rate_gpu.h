@@ -39,7 +39,9 @@ struct DeviceTier1 {
 // run on the given stream and wait for it.
 class DeviceRateControl {
 public:
-    DeviceRateControl(int device, const Layout& L, const std::string& label);
+    // bodyHint: codestream bytes the buffers are first sized for (they grow when a frame
+    // needs more, which waits for the device)
+    DeviceRateControl(int device, const Layout& L, const std::string& label, size_t bodyHint = 4u << 20);
     ~DeviceRateControl();
     DeviceRateControl(const DeviceRateControl&) = delete;
     DeviceRateControl& operator=(const DeviceRateControl&) = delete;
