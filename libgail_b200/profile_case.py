@@ -1,7 +1,7 @@
 """Small, fixed encode cases for profiler captures.
 
   python -m libgail_b200.profile_case --path plain --frames 2
-  python -m libgail_b200.profile_case --path served --frames 8 --batch 8 [--size 2k] [--repeat 3]
+  python -m libgail_b200.profile_case --path served --frames 8 --batch 8 [--size 2k] [--repeat 3] [--codestreams]
   python -m libgail_b200.profile_case --path decode --frames 2
 
 Encodes seeded synthetic frames that are already in device memory, through the plain
@@ -30,6 +30,8 @@ def main():
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--size", choices=["4k", "2k"], default="4k")
     ap.add_argument("--repeat", type=int, default=1, help="served: passes over the frames (the first warms up)")
+    ap.add_argument("--codestreams", action="store_true",
+                    help="served: DCI codestreams too (rate control and Tier-2 on the device)")
     args = ap.parse_args()
 
     import torch
@@ -88,16 +90,24 @@ def main():
             import time
             eng = Engine(0, 0, max_batch=args.batch)
             cid, _ = eng.add_encoder(lay, fmt, col)
+            if args.codestreams:
+                from libgail_b200 import codestream as CS
+                eng.set_codestream(label=CS.DEFAULT_LABEL, tag="b200", threads=8)
             for rep in range(args.repeat):
                 t0 = time.perf_counter()
                 ids = [eng.submit(cid, f) for f in dframes]
+                lat = []
                 for _ in ids:
-                    rid, _, _, st = eng.wait(120000, copy=False)
+                    rid, _, ms, st = eng.wait(120000, copy=False)
                     if rid < 0 or st != 0:
                         raise SystemExit(f"engine frame failed (id {rid}, status {st})")
+                    if args.codestreams and eng.codestream(rid, copy=False)[1] != 1:
+                        raise SystemExit(f"codestream of request {rid} failed the DCI check")
+                    lat.append(ms)
                     eng.release(rid)
                 dt = time.perf_counter() - t0
-                print(f"engine pass {rep}: {len(ids) / dt:.1f} frames/s (Tier-1 frames to host memory)")
+                what = "DCI codestreams" if args.codestreams else "Tier-1 frames to host memory"
+                print(f"engine pass {rep}: {len(ids) / dt:.1f} frames/s ({what}), mean latency {np.mean(lat):.1f} ms")
             print("engine:", eng.stats())
             eng.close()
     finally:
