@@ -623,7 +623,12 @@ struct DeviceRateControl::Impl {
         slopeBounds(minSlope, maxSlope, lo, hi);
         SlopeBins sb(lo, hi);
         const int nb = sb.size();
-        const bool same = H.ctl.lo == lo && H.ctl.hi == hi && H.ctl.nb == nb && !(H.ctl.flags & kFlagBins);
+        // The device's bins are the host's when the bin counts agree and the lower bounds
+        // differ by at most kLoTolerance (the two log2s may differ in the last place): such a
+        // shift moves a point's bin value by ~1e-9 bin, so only points within the edge
+        // margin could change bins, and those are binned here with the host's own bounds.
+        constexpr double kLoTolerance = 1e-12;
+        const bool same = H.ctl.nb == nb && std::fabs(H.ctl.lo - lo) <= kLoTolerance && !(H.ctl.flags & kFlagBins);
         if (!same) {  // a histogram at the host's bounds, in a larger buffer if need be
             if (nb > binsCap) {
                 binsCap = nb + 4096;
