@@ -3,10 +3,10 @@
 // Per frame: the range of the hull slopes (one reduction), the slope histogram (a thread
 // per block, 32-bit atomic sums of whole bytes and blocks, exact in any order), then per
 // measurement of the threshold search one launch of the packet coder (a warp per packet:
-// its lanes select the passes of the packet's blocks from their hull points and fetch
-// their lengths in parallel, lane 0 codes the header bits as the host writer does) and a
-// read-back of the tile-parts' sizes. At the final thresholds, packet offsets by a scan
-// and the packets themselves: lane 0 writes the header, the warp copies the codewords.
+// its lanes select the passes of the packet's blocks from their hull points, fetch their
+// lengths and make each block's header bits in parallel, and one lane applies the bit
+// stuffing) and a read-back of the tile-parts' sizes; with it, the packets at the same
+// thresholds are placed by a scan and written, the warp copying the codewords.
 #include "rate_gpu.h"
 
 #include <algorithm>
@@ -28,7 +28,6 @@ namespace gb {
 namespace {
 
 constexpr int kPacketBlocks = 64;     // blocks of one packet the device coder holds (DCI: 48)
-constexpr int kTagNodes = 32;         // nodes of one tag tree (DCI: 4 x 4 leaves, 21 nodes)
 constexpr uint32_t kMaxAmbiguous = 4096;
 constexpr double kBinMargin = 1e-7;   // bin units from an edge within which the host bins
 
@@ -61,166 +60,157 @@ __device__ __forceinline__ uint32_t passesAt(const FrameArgs& f, const GbCblkInf
     return np;
 }
 
-// ------------------------------------------------------------- packet-header bits
-// B.10.1: bits fill each byte from the top; the byte after an 0xFF byte carries only 7.
-// out null: count only.
-struct Bits {
-    uint8_t* out;
-    uint32_t cur, last, bytes;
-    int fill, room;
-    __device__ void init(uint8_t* o) {
-        out = o;
-        cur = last = bytes = 0;
-        fill = 0;
-        room = 8;
+// ---------------------------------------------------------- packet-header bits
+// A packet header (B.10) is, after its first bit, each block's bits in packet order: its
+// inclusion tag-tree bits, and for an included block its zero-bit-plane tag-tree bits, the
+// pass-count code (Table B.4) and its length with the Lblock increment (B.10.7). Bit
+// stuffing (B.10.1: the byte after an 0xFF carries 7 bits) applies to the concatenation.
+//
+// A tag-tree node sends bits only the first time a coding walk passes it: zeros from its
+// parent's value (capped at the threshold) up to its own, then a 1 when its value is below
+// the threshold; later walks find it known or at the threshold and send nothing. The first
+// walk through a node of the inclusion tree is that of the first leaf in raster order of its
+// rectangle (every block is coded, in raster order); through a node of the zero-bit-plane
+// tree, that of the first included leaf of its rectangle. So each block's bits follow from
+// its rectangles alone: a lane per block makes them, a scan places them, and one lane walks
+// the bytes for the stuffing.
+
+constexpr int kPacketSegs = 8;            // precinct-bands of one packet (DCI: 3)
+constexpr int kRawWords = 2 * kPacketBlocks * 4 + 8;  // raw header bits, 115 at most per block
+
+// A bit string of up to 128 bits, right-aligned in (hi, lo), first bit most significant.
+struct BitStr {
+    unsigned long long hi = 0, lo = 0;
+    int n = 0;
+    __device__ void put(uint32_t v, int k) {  // the k (<= 32) low bits of v
+        if (k == 0) return;
+        const unsigned long long x = (unsigned long long)(v & (k == 32 ? 0xFFFFFFFFu : ((1u << k) - 1u)));
+        hi = (hi << k) | (lo >> (64 - k));
+        lo = (lo << k) | x;
+        n += k;
     }
-    __device__ void push() {
-        last = cur & 0xFFu;
-        if (out) out[bytes] = (uint8_t)last;
-        ++bytes;
-        room = last == 0xFFu ? 7 : 8;
-        cur = 0;
-        fill = 0;
+    __device__ void zeros(int k) {
+        for (; k > 32; k -= 32) put(0, 32);
+        put(0, k);
     }
-    __device__ void put(uint32_t v, int n) {  // the n (<= 32) low bits of v, most significant first
-        while (n > 0) {
-            const int k = min(n, room - fill);
-            n -= k;
-            cur = (cur << k) | ((v >> n) & ((1u << k) - 1u));
-            fill += k;
-            if (fill == room) push();
-        }
-    }
-    __device__ void zeros(int n) {
-        for (; n > 8; n -= 8) put(0, 8);
-        put(0, n);
-    }
-    // pads the byte in progress; a header ending on 0xFF owes its stuffed 0x00; a header
-    // with no bits is one 0x00
-    __device__ uint32_t end() {
-        if (fill > 0 || bytes == 0) {
-            cur <<= room - fill;
-            push();
-        }
-        if (last == 0xFFu) push();
-        return bytes;
+    // bits [from, from + k) counted from the least significant end, k <= 32
+    __device__ uint32_t take(int from, int k) const {
+        unsigned long long x;
+        if (from >= 64) x = hi >> (from - 64);
+        else if (from == 0) x = lo;
+        else x = (lo >> from) | (hi << (64 - from));
+        return (uint32_t)(x & (k == 32 ? 0xFFFFFFFFull : ((1ull << k) - 1ull)));
     }
 };
 
-// ------------------------------------------------------------------- tag trees
-// B.10.2 over w x h leaves: a node's value is the minimum of its children's; coding a leaf
-// against a threshold walks from the root, each node sending a 0 per unit its value is
-// known to exceed (from where it stopped, at least its parent's bound) up to the
-// threshold, and a 1 when its value is reached below the threshold.
-struct Tag {
-    int8_t parent[kTagNodes];
-    uint8_t known[kTagNodes];
-    int value[kTagNodes], low[kTagNodes];
-    int n, leaves;
-    __device__ void shape(int w, int h) {
-        int lw = w, lh = h, base = 0;
-        leaves = w * h;
-        for (;;) {
-            const int nb = base + lw * lh, pw = (lw + 1) / 2;
-            for (int y = 0; y < lh; ++y)
-                for (int x = 0; x < lw; ++x)
-                    parent[base + y * lw + x] = (int8_t)((lw == 1 && lh == 1) ? -1 : nb + (y / 2) * pw + x / 2);
-            n = nb;
-            if (lw == 1 && lh == 1) break;
-            base = nb;
-            lw = pw;
-            lh = (lh + 1) / 2;
-        }
-        for (int i = 0; i < n; ++i) {
-            low[i] = 0;
-            known[i] = 0;
-        }
-    }
-    __device__ void close() {
-        for (int i = leaves; i < n; ++i) value[i] = 1 << 30;
-        for (int i = 0; i < n; ++i)
-            if (parent[i] >= 0) value[parent[i]] = min(value[parent[i]], value[i]);
-    }
-    __device__ void encode(Bits& hb, int leaf, int threshold) {
-        int path[8], d = 0;
-        for (int i = leaf; i >= 0; i = parent[i]) path[d++] = i;
-        int floorv = 0;
-        while (d > 0) {
-            const int i = path[--d];
-            int lo = max(low[i], floorv);
-            const int to = min(value[i], threshold);
-            if (to > lo) {
-                hb.zeros(to - lo);
-                lo = to;
-            }
-            low[i] = lo;
-            if (lo >= value[i] && lo < threshold && !known[i]) {
-                hb.put(1, 1);
-                known[i] = 1;
-            }
-            floorv = lo;
-        }
-    }
+// One warp's packet: its blocks in packet order (passes, planes, lengths, codeword offsets,
+// segment), its segments (first block, geometry) and the raw header bits.
+struct WarpPacket {
+    uint8_t np[kPacketBlocks], nbps[kPacketBlocks], seg[kPacketBlocks];
+    uint32_t len[kPacketBlocks], dataOff[kPacketBlocks];
+    int segBase[kPacketSegs], segW[kPacketSegs], segH[kPacketSegs], segMb[kPacketSegs];
+    uint32_t raw[kRawWords];
 };
 
-// The pass-count code of Table B.4 (n <= 64 here).
-__device__ __forceinline__ void putPasses(Bits& hb, int n) {
-    if (n == 1) hb.put(0, 1);
-    else if (n == 2) hb.put(0x2, 2);
-    else if (n <= 5) hb.put(0xC | (uint32_t)(n - 3), 4);
-    else if (n <= 36) hb.put(0x1E0 | (uint32_t)(n - 6), 9);
-    else hb.put(0xFF80 | (uint32_t)(n - 37), 16);
+// Over the leaves of the rectangle of node (l, nx, ny) of a segment's tag trees: whether
+// any is included, the least zero-bit-plane count, the raster index of the first included.
+__device__ __forceinline__ void rectOf(const WarpPacket& W, int base, int w, int h, int Mb, int l, int nx, int ny,
+                                       bool& any, int& minMsb, int& firstIncl) {
+    const int x0 = nx << l, y0 = ny << l, x1 = min(w, (nx + 1) << l), y1 = min(h, (ny + 1) << l);
+    any = false;
+    minMsb = 1 << 30;
+    firstIncl = -1;
+    for (int y = y0; y < y1; ++y)
+        for (int x = x0; x < x1; ++x) {
+            const int k = y * w + x;
+            minMsb = min(minMsb, Mb - (int)W.nbps[base + k]);
+            if (W.np[base + k] && !any) {
+                any = true;
+                firstIncl = k;
+            }
+        }
 }
 
-// One warp's packet: its blocks in packet order with their passes, planes, lengths and
-// codeword offsets, and the two tag trees.
-struct WarpPacket {
-    uint8_t np[kPacketBlocks], nbps[kPacketBlocks];
-    uint32_t len[kPacketBlocks], dataOff[kPacketBlocks];
-    Tag incl, msb;
-};
+// The header bits of block k of the packet (without the packet's first bit).
+__device__ BitStr blockBits(const WarpPacket& W, int k) {
+    const int s = W.seg[k], base = W.segBase[s], w = W.segW[s], h = W.segH[s], Mb = W.segMb[s];
+    const int kk = k - base, x = kk % w, y = kk / w;
+    int levels = 1;
+    while (((w - 1) >> (levels - 1)) > 0 || ((h - 1) >> (levels - 1)) > 0) ++levels;
+    BitStr b;
+    // inclusion (threshold 1: a node's value is 0 when its rectangle has an included leaf)
+    for (int l = levels - 1; l >= 0; --l) {
+        const int nx = x >> l, ny = y >> l;
+        if (x != (nx << l) || y != (ny << l)) continue;  // not the rectangle's first leaf
+        bool any, anyP = true;
+        int mm, fi;
+        rectOf(W, base, w, h, Mb, l, nx, ny, any, mm, fi);
+        if (l < levels - 1) rectOf(W, base, w, h, Mb, l + 1, nx >> 1, ny >> 1, anyP, mm, fi);
+        const int v = any ? 0 : 1, vp = anyP ? 0 : 1;  // the root's floor is 0
+        b.zeros(v - vp);
+        if (v == 0) b.put(1, 1);
+    }
+    const int np = W.np[k];
+    if (!np) return b;
+    // zero bit-planes (no threshold is reached: every first visit ends with a 1)
+    for (int l = levels - 1; l >= 0; --l) {
+        const int nx = x >> l, ny = y >> l;
+        bool any;
+        int v, fi, vp = 0;
+        rectOf(W, base, w, h, Mb, l, nx, ny, any, v, fi);
+        if (fi != kk) continue;  // an earlier included leaf passed this node
+        if (l < levels - 1) rectOf(W, base, w, h, Mb, l + 1, nx >> 1, ny >> 1, any, vp, fi);
+        b.zeros(v - vp);
+        b.put(1, 1);
+    }
+    // the pass count (Table B.4)
+    if (np == 1) b.put(0, 1);
+    else if (np == 2) b.put(0x2, 2);
+    else if (np <= 5) b.put(0xC | (uint32_t)(np - 3), 4);
+    else if (np <= 36) b.put(0x1E0 | (uint32_t)(np - 6), 9);
+    else b.put(0xFF80 | (uint32_t)(np - 37), 16);
+    // Lblock starts at 3; the length takes Lblock + floor(log2 passes) bits
+    const uint32_t len = W.len[k];
+    const int extra = floorLog2((uint32_t)np);
+    const int need = len ? floorLog2(len) + 1 : 1;
+    const int incr = max(0, need - (3 + extra));
+    b.put(((1u << incr) - 1u) << 1, incr + 1);  // incr ones and a zero
+    b.put(len, 3 + incr + extra);
+    return b;
+}
 
-// The header of packet p (lane 0), as the host writer codes it; out null: count only.
-__device__ uint32_t codeHeader(const PlanArgs& P, WarpPacket& W, int s0, int s1, bool any, uint8_t* out,
-                               uint32_t* body) {
-    Bits hb;
-    hb.init(out);
-    *body = 0;
-    if (!any) {
-        hb.put(0, 1);
-        return hb.end();
+// Ors bit string b into the raw bits from bit position pos on.
+__device__ __forceinline__ void orBits(uint32_t* raw, uint32_t pos, const BitStr& b) {
+    int rem = b.n;
+    while (rem > 0) {
+        const int k = min(32 - (int)(pos & 31), rem);
+        const uint32_t v = b.take(rem - k, k);
+        atomicOr(&raw[pos >> 5], v << (32 - (int)(pos & 31) - k));
+        pos += k;
+        rem -= k;
     }
-    hb.put(1, 1);
-    int base = 0;
-    for (int s = s0; s < s1; ++s) {
-        const int4 g = P.segs[s];
-        const int ncbx = g.z & 0xFFFF, ncby = g.z >> 16, Mb = g.w & 0xFF, nl = ncbx * ncby;
-        W.incl.shape(ncbx, ncby);
-        W.msb.shape(ncbx, ncby);
-        for (int k = 0; k < nl; ++k) {
-            W.incl.value[k] = W.np[base + k] ? 0 : 1;
-            W.msb.value[k] = Mb - (int)W.nbps[base + k];
-        }
-        W.incl.close();
-        W.msb.close();
-        for (int k = 0; k < nl; ++k) {
-            W.incl.encode(hb, k, 1);
-            const int np = W.np[base + k];
-            if (!np) continue;
-            W.msb.encode(hb, k, 999);
-            putPasses(hb, np);
-            const uint32_t len = W.len[base + k];
-            // Lblock starts at 3; the length takes Lblock + floor(log2 passes) bits
-            const int extra = floorLog2((uint32_t)np);
-            const int need = len ? floorLog2(len) + 1 : 1;
-            const int incr = max(0, need - (3 + extra));
-            hb.put(((1u << incr) - 1u) << 1, incr + 1);  // incr ones and a zero
-            hb.put(len, 3 + incr + extra);
-            *body += len;
-        }
-        base += nl;
+}
+
+// The header bytes from `bits` raw bits (one lane): each byte takes 8 bits, or 7 after an
+// 0xFF byte; the last is padded with zeros, and an 0xFF at the end is followed by 0x00.
+// out null: count only.
+__device__ uint32_t stuffBytes(const uint32_t* raw, uint32_t bits, uint8_t* out) {
+    uint32_t pos = 0, bytes = 0, last = 0;
+    while (pos < bits) {
+        const int room = last == 0xFFu ? 7 : 8;
+        const int k = (int)min((uint32_t)room, bits - pos);
+        const unsigned long long win = ((unsigned long long)raw[pos >> 5] << 32) | raw[(pos >> 5) + 1];
+        const uint32_t v = (uint32_t)((win << (pos & 31)) >> (64 - k));
+        last = v << (room - k);
+        if (out) out[bytes] = (uint8_t)last;
+        ++bytes;
+        pos += k;
     }
-    return hb.end();
+    if (last == 0xFFu) {
+        if (out) out[bytes] = 0;
+        ++bytes;
+    }
+    return bytes;
 }
 
 // Control words of one frame's device rate control.
@@ -248,33 +238,68 @@ __global__ void __launch_bounds__(32) t2Kernel(PlanArgs P, FrameArgs F, double l
     // the packet's blocks, a lane each
     bool any = false;
     int nb = 0;
+    uint32_t bodyBytes = 0;
     for (int s = s0; s < s1; ++s) {
         const int4 g = P.segs[s];
-        const int ncbx = g.z & 0xFFFF, nl = ncbx * (g.z >> 16);
+        const int ncbx = g.z & 0xFFFF, ncby = g.z >> 16, nl = ncbx * ncby;
+        if (lane == 0) {
+            W.segBase[s - s0] = nb;
+            W.segW[s - s0] = ncbx;
+            W.segH[s - s0] = ncby;
+            W.segMb[s - s0] = g.w & 0xFF;
+        }
         const double t = lam[(g.w >> 8) & 3];
         for (int k = lane; k < nl; k += 32) {
             const uint32_t blk = (uint32_t)(g.x + (k / ncbx) * g.y + k % ncbx);
             const GbCblkInfo ci = F.info[blk];
             const uint32_t np = passesAt(F, ci, t);
+            const uint32_t len = np ? F.passLen[ci.passBase + np - 1] : 0u;
             W.np[nb + k] = (uint8_t)np;
             W.nbps[nb + k] = (uint8_t)ci.nbps;
-            W.len[nb + k] = np ? F.passLen[ci.passBase + np - 1] : 0u;
+            W.seg[nb + k] = (uint8_t)(s - s0);
+            W.len[nb + k] = len;
             W.dataOff[nb + k] = ci.dataOffset;
             any = any || np != 0;
+            bodyBytes += len;
             if (WRITE) passesOut[blk] = (uint8_t)np;
         }
         nb += nl;
     }
+    for (int i = lane; i < kRawWords; i += 32) W.raw[i] = 0;
     any = __any_sync(kFull, any);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bodyBytes += __shfl_xor_sync(kFull, bodyBytes, o);
     __syncwarp();
     if (WRITE && (uint64_t)pkOff[p] + pkBytes[p] > bodyCap) {  // sized by the measurement before
         if (lane == 0) atomicOr(&ctl->flags, kFlagBody);
         return;
     }
-    uint32_t hdr = 0, bodyBytes = 0;
-    if (lane == 0) hdr = codeHeader(P, W, s0, s1, any, WRITE ? body + pkOff[p] : nullptr, &bodyBytes);
+    // the header: the packet's bit, then each block's bits at its place
+    uint32_t bits = 1;
+    if (any) {
+        BitStr b0, b1;
+        if (lane < nb) b0 = blockBits(W, lane);
+        if (lane + 32 < nb) b1 = blockBits(W, lane + 32);
+        uint32_t x0 = (uint32_t)b0.n, x1 = (uint32_t)b1.n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t0 = __shfl_up_sync(kFull, x0, o), t1 = __shfl_up_sync(kFull, x1, o);
+            if (lane >= o) {
+                x0 += t0;
+                x1 += t1;
+            }
+        }
+        const uint32_t tot0 = __shfl_sync(kFull, x0, 31), tot1 = __shfl_sync(kFull, x1, 31);
+        if (lane == 0) atomicOr(&W.raw[0], 0x80000000u);  // the packet is not empty
+        orBits(W.raw, 1 + x0 - (uint32_t)b0.n, b0);
+        orBits(W.raw, 1 + tot0 + x1 - (uint32_t)b1.n, b1);
+        bits = 1 + tot0 + tot1;
+    }
+    __syncwarp();
+    uint32_t hdr = 0;
+    if (lane == 0) hdr = stuffBytes(W.raw, bits, WRITE ? body + pkOff[p] : nullptr);
     hdr = __shfl_sync(kFull, hdr, 0);
-    bodyBytes = __shfl_sync(kFull, bodyBytes, 0);
+    if (!any) bodyBytes = 0;
     if (!WRITE) {
         if (lane == 0) {
             pkBytes[p] = hdr + bodyBytes;
@@ -520,6 +545,8 @@ struct DeviceRateControl::Impl {
             int blocks = 0;
             for (int s = ps[(size_t)p]; s < ps[(size_t)p + 1]; ++s) blocks += sg[(size_t)s].ncbx * sg[(size_t)s].ncby;
             if (blocks > kPacketBlocks) throw std::logic_error("packet with too many code-blocks for the device Tier-2");
+            if (ps[(size_t)p + 1] - ps[(size_t)p] > kPacketSegs)
+                throw std::logic_error("packet with too many precinct-bands for the device Tier-2");
         }
         n = (uint32_t)L.numCblks();
         nPad = (n + 15u) & ~15u;
