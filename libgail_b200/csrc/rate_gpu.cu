@@ -222,6 +222,21 @@ struct RcCtl {
 };
 constexpr uint32_t kFlagBins = 1u, kFlagBody = 2u;
 
+// Copies a codeword of len bytes from src (on a 4-byte boundary, the codeword padded with
+// zeros to whole words, as the packed frame keeps it) to dst (any alignment): the bytes up to
+// dst's next word boundary, whole words each made from two source words by a funnel shift,
+// then the rest. Lanes lane, lane + step, ... share the work.
+__device__ __forceinline__ void copyCodeword(uint8_t* dst, const uint8_t* src, uint32_t len, uint32_t lane,
+                                             uint32_t step) {
+    const uint32_t head = min(len, (uint32_t)((4u - ((uint32_t)(uintptr_t)dst & 3u)) & 3u));
+    for (uint32_t i = lane; i < head; i += step) dst[i] = src[i];
+    const uint32_t words = (len - head) >> 2, sh = 8 * head;
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(dst + head);
+    for (uint32_t j = lane; j < words; j += step) d[j] = head ? __funnelshift_r(s[j], s[j + 1], sh) : s[j];
+    for (uint32_t i = head + 4 * words + lane; i < len; i += step) dst[i] = src[i];
+}
+
 // A warp (the whole CTA) per packet: small CTAs fit beside the resident Tier-1 kernels.
 // WRITE false: the packet's size into pkBytes and its tile-part's total; WRITE true: the
 // packet at body + pkOff[p] (when it fits in bodyCap) and its blocks' passes.
@@ -308,12 +323,27 @@ __global__ void __launch_bounds__(32) t2Kernel(PlanArgs P, FrameArgs F, double l
         return;
     }
     __syncwarp();
+    // the codewords after the header: short ones each by its own lane, long ones by the warp
+    const uint32_t len0 = lane < nb ? W.len[lane] : 0u, len1 = lane + 32 < nb ? W.len[lane + 32] : 0u;
+    uint32_t x0 = len0, x1 = len1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t0 = __shfl_up_sync(kFull, x0, o), t1 = __shfl_up_sync(kFull, x1, o);
+        if (lane >= o) {
+            x0 += t0;
+            x1 += t1;
+        }
+    }
+    const uint32_t off0 = x0 - len0, off1 = __shfl_sync(kFull, x0, 31) + x1 - len1;
     uint8_t* dst = body + pkOff[p] + hdr;
+    constexpr uint32_t kShort = 256;
+    if (len0 && len0 <= kShort) copyCodeword(dst + off0, F.data + W.dataOff[lane], len0, 0, 1);
+    if (len1 && len1 <= kShort) copyCodeword(dst + off1, F.data + W.dataOff[lane + 32], len1, 0, 1);
     for (int k = 0; k < nb; ++k) {
         const uint32_t len = W.len[k];
-        const uint8_t* src = F.data + W.dataOff[k];
-        for (uint32_t i = lane; i < len; i += 32) dst[i] = src[i];
-        dst += len;
+        if (len <= kShort) continue;
+        const uint32_t off = __shfl_sync(kFull, k < 32 ? off0 : off1, k & 31);
+        copyCodeword(dst + off, F.data + W.dataOff[k], len, (uint32_t)lane, 32);
     }
 }
 
@@ -768,19 +798,31 @@ struct DeviceRateControl::Impl {
                 if (t1.passLen[c.passBase + k] < t1.passLen[c.passBase + k - 1])
                     throw std::logic_error("pass lengths that decrease");
         }
-        const size_t npass = std::max<size_t>(t1.numPasses, 1), nd = std::max<size_t>(t1.numData, 1);
+        // the codewords on 4-byte boundaries, zero-padded to whole words, as the device's packed
+        // frames hold them (the packet writer copies them by words)
+        std::vector<GbCblkInfo> info(t1.info, t1.info + n);
+        size_t total = 0;
+        for (const GbCblkInfo& c : info) total += (c.dataLen + 3u) & ~3u;
+        std::vector<uint8_t> data(std::max<size_t>(total, 16), 0);
+        size_t at = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (info[i].dataLen) std::memcpy(data.data() + at, t1.data + t1.info[i].dataOffset, info[i].dataLen);
+            info[i].dataOffset = (uint32_t)at;
+            at += (info[i].dataLen + 3u) & ~3u;
+        }
+        const size_t npass = std::max<size_t>(t1.numPasses, 1), nd = data.size();
         upInfo.ensure(n);
         upLen.ensure(npass);
         upDist.ensure(npass);
         upData.ensure(nd);
         upHp.ensure(npass);
         upHs.ensure(npass);
-        GB_CHECK(cudaMemcpyAsync(upInfo.p, t1.info, (size_t)n * sizeof(GbCblkInfo), cudaMemcpyHostToDevice, st));
+        GB_CHECK(cudaMemcpyAsync(upInfo.p, info.data(), (size_t)n * sizeof(GbCblkInfo), cudaMemcpyHostToDevice, st));
         if (t1.numPasses) {
             GB_CHECK(cudaMemcpyAsync(upLen.p, t1.passLen, (size_t)t1.numPasses * 4, cudaMemcpyHostToDevice, st));
             GB_CHECK(cudaMemcpyAsync(upDist.p, t1.passDist, (size_t)t1.numPasses * 4, cudaMemcpyHostToDevice, st));
         }
-        if (t1.numData) GB_CHECK(cudaMemcpyAsync(upData.p, t1.data, t1.numData, cudaMemcpyHostToDevice, st));
+        GB_CHECK(cudaMemcpyAsync(upData.p, data.data(), nd, cudaMemcpyHostToDevice, st));
         packedHullKernel<<<divUp(n, (uint32_t)HULL_THREADS), HULL_THREADS, 0, st>>>(upInfo.p, upLen.p, upDist.p, scale.p,
                                                                                    n, upHp.p, upHs.p);
         GB_CHECK(cudaGetLastError());
