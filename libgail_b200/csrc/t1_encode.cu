@@ -60,9 +60,8 @@ __constant__ uint8_t c_sc[9];        // sign context | xor bit << 5, by (hc+1) *
 __constant__ uint32_t c_mq[47];      // Qe | switch << 17 | NMPS << 18 | NLPS << 24
 
 __device__ __forceinline__ uint32_t bit(uint32_t m, int r) { return (m >> r) & 1u; }
-__device__ __forceinline__ int chi(uint32_t sig, uint32_t sgn, int r) {
-    return bit(sig, r) ? (bit(sgn, r) ? -1 : 1) : 0;
-}
+// A neighbour's contribution to the sign context: 0 when insignificant, else -1 / +1 by sign.
+__device__ __forceinline__ int chiBits(int sig, int sgn) { return sig ? (sgn ? -1 : 1) : 0; }
 __device__ __forceinline__ int clamp1(int v) { return v < -1 ? -1 : (v > 1 ? 1 : v); }
 __device__ __forceinline__ int32_t distSig(uint32_t w) { return 192 * (int32_t)w - 9216; }
 __device__ __forceinline__ int32_t distRef(uint32_t w) { return w >= 64u ? 64 * (int32_t)w - 5120 : 3072 - 64 * (int32_t)w; }
@@ -72,16 +71,7 @@ struct Nbr {
     uint32_t L;    // left column, current (includes its new significance in this stripe)
     uint32_t R;    // right column, as before this stripe (it is visited later)
     uint32_t S;    // own column as before this stripe
-    uint32_t Gl, Gr, G;  // signs of left, right, own column
 };
-
-// Zero-coding decision of row r; SN = own column with the rows above r already updated.
-__device__ __forceinline__ uint32_t zcContext(const uint8_t* zc, const Nbr& q, uint32_t SN, int r) {
-    const uint32_t h = bit(q.L, r) + bit(q.R, r);
-    const uint32_t v = bit(SN << 1, r) + bit(q.S >> 1, r);
-    const uint32_t d = bit(q.L << 1, r) + bit(q.L >> 1, r) + bit(q.R << 1, r) + bit(q.R >> 1, r);
-    return zc[h + 3 * v + 9 * d];
-}
 
 // Warp-inclusive prefix sum.
 __device__ __forceinline__ uint32_t warpScan(uint32_t v, int lane) {
@@ -111,11 +101,27 @@ __device__ __forceinline__ uint32_t shDown(uint32_t v, int lane) {
 __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
     __shared__ uint32_t s_mag[CM_WARPS][32][32];
     __shared__ __align__(16) uint8_t s_stage[CM_WARPS][STAGE];
-    __shared__ uint8_t s_zc[4 * 45];
-    __shared__ uint8_t s_sc[16];
+    // the contexts as tables of a sample's neighbour bits. Zero coding, per orientation, by
+    // bits 0-2: left column rows r-1..r+1, 3-5: right column rows r-1..r+1, 6: row above,
+    // 7: row below. Sign coding, the whole decision byte (context << 1 | coded bit), by
+    // bits 0-2: own signs rows r-1..r+1, 3: left significant, 4: its sign, 5: right
+    // significant, 6: its sign, 7: row above significant, 8: row below significant.
+    __shared__ uint8_t s_zk[4 * 256];
+    __shared__ uint8_t s_sk[512];
     __shared__ uint32_t s_hist[CM_WARPS][19];
-    for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) s_zc[i] = c_zc[i];
-    if (threadIdx.x < 9) s_sc[threadIdx.x] = c_sc[threadIdx.x];
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
+        const int o = i >> 8, k = i & 255;
+        const int h = ((k >> 1) & 1) + ((k >> 4) & 1);
+        const int v = ((k >> 6) & 1) + ((k >> 7) & 1);
+        const int d = (k & 1) + ((k >> 2) & 1) + ((k >> 3) & 1) + ((k >> 5) & 1);
+        s_zk[i] = c_zc[45 * o + h + 3 * v + 9 * d];
+    }
+    for (int k = threadIdx.x; k < 512; k += blockDim.x) {
+        const int hc = clamp1(chiBits((k >> 3) & 1, (k >> 4) & 1) + chiBits((k >> 5) & 1, (k >> 6) & 1));
+        const int vc = clamp1(chiBits((k >> 7) & 1, k & 1) + chiBits((k >> 8) & 1, (k >> 2) & 1));
+        const uint32_t t = c_sc[(hc + 1) * 3 + (vc + 1)];
+        s_sk[k] = (uint8_t)(((t & 31u) << 1) | (((uint32_t)k >> 1 & 1u) ^ (t >> 5)));
+    }
     __syncthreads();
 
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -128,7 +134,7 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
         const int w = (J.geom & 31u) + 1, h = ((J.geom >> 5) & 31u) + 1, orient = (J.geom >> 10) & 3u;
         const int maxPasses = (J.geom >> 12) & 127u;
         const float slope = P.slope ? P.slope[J.slope] : 0.f;
-        const uint8_t* zc = s_zc + 45 * orient;
+        const uint8_t* zk = s_zk + 256 * orient;
 
         // Load: lane x reads column x, one 128-byte row per step.
         const uint32_t* src = J.coeffs;
@@ -293,10 +299,16 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                         q.L = SLp | (NL & (P | Q));
                         q.R = SRp | (NR & P);
                         q.S = Spass | (NEW & P);
-                        q.G = sgn;
-                        q.Gl = sgnL;
-                        q.Gr = sgnR;
                         const uint32_t SN = q.S | (NEW & Q);
+                        // neighbour windows of the stripe, bit i about row r0 + i: left / right
+                        // columns and own signs at rows r-1..r+1 from bit i, the row above (final:
+                        // SN) at bit i, the row below (before the stripe) at bit i + 1; the
+                        // neighbouring columns' signs are read at row r itself
+                        const uint32_t wL = (uint32_t)(((unsigned long long)q.L << 1) >> r0);
+                        const uint32_t wR = (uint32_t)(((unsigned long long)q.R << 1) >> r0);
+                        const uint32_t wU = (uint32_t)(((unsigned long long)SN << 1) >> r0);
+                        const uint32_t wS = q.S >> r0;
+                        const uint32_t wG = (uint32_t)(((unsigned long long)sgn << 1) >> r0);
                         uint32_t skip = 0;  // the row whose zero-coding decision the run decisions replace
                         if ((runs >> s) & 1u) {
                             const uint32_t nb = (NEW >> r0) & 0xFu;
@@ -310,15 +322,17 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                         }
 #pragma unroll 1
                         for (; rows; rows &= rows - 1) {
-                            const int r = __ffs(rows) - 1;
-                            // above: rows < r are final; below: as before the stripe
-                            const uint32_t upto = q.S | (SN & ((1u << r) - 1u));
-                            if (!((skip >> r) & 1u)) buf[pos++] = (uint8_t)((zcContext(zc, q, upto, r) << 1) | bit(Bp, r));
+                            const int r = __ffs(rows) - 1, i = r - r0;
+                            const uint32_t up = (wU >> i) & 1u, down = (wS >> (i + 1)) & 1u;
+                            if (!((skip >> r) & 1u)) {
+                                const uint32_t key = ((wL >> i) & 7u) | (((wR >> i) & 7u) << 3) | (up << 6) | (down << 7);
+                                buf[pos++] = (uint8_t)((zk[key] << 1) | bit(Bp, r));
+                            }
                             if (bit(NEW, r)) {
-                                const int hc = clamp1(chi(q.L, q.Gl, r) + chi(q.R, q.Gr, r));
-                                const int vc = clamp1(chi(upto << 1, q.G << 1, r) + chi(q.S >> 1, q.G >> 1, r));
-                                const uint32_t t = s_sc[(hc + 1) * 3 + (vc + 1)];
-                                buf[pos++] = (uint8_t)(((t & 31u) << 1) | (bit(q.G, r) ^ (t >> 5)));
+                                const uint32_t key = ((wG >> i) & 7u) | (((wL >> (i + 1)) & 1u) << 3) | (((sgnL >> r) & 1u) << 4) |
+                                                     (((wR >> (i + 1)) & 1u) << 5) | (((sgnR >> r) & 1u) << 6) | (up << 7) |
+                                                     (down << 8);
+                                buf[pos++] = s_sk[key];
                                 dist += distSig((mag[r][lane] >> p) & 0x7Fu);
                             }
                         }
