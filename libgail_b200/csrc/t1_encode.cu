@@ -295,6 +295,17 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                             }
                             continue;
                         }
+                        uint32_t skip = 0;  // the row whose zero-coding decision the run decisions replace
+                        if ((runs >> s) & 1u) {
+                            const uint32_t nb = (NEW >> r0) & 0xFu;
+                            buf[pos++] = (uint8_t)((17u << 1) | (nb != 0));
+                            if (nb == 0) continue;
+                            const uint32_t first = __ffs(nb) - 1;
+                            buf[pos++] = (uint8_t)((18u << 1) | (first >> 1));
+                            buf[pos++] = (uint8_t)((18u << 1) | (first & 1u));
+                            skip = 1u << (r0 + first);
+                            rows &= ~(skip - 1u);
+                        }
                         Nbr q;
                         q.L = SLp | (NL & (P | Q));
                         q.R = SRp | (NR & P);
@@ -309,17 +320,6 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                         const uint32_t wU = (uint32_t)(((unsigned long long)SN << 1) >> r0);
                         const uint32_t wS = q.S >> r0;
                         const uint32_t wG = (uint32_t)(((unsigned long long)sgn << 1) >> r0);
-                        uint32_t skip = 0;  // the row whose zero-coding decision the run decisions replace
-                        if ((runs >> s) & 1u) {
-                            const uint32_t nb = (NEW >> r0) & 0xFu;
-                            buf[pos++] = (uint8_t)((17u << 1) | (nb != 0));
-                            if (nb == 0) continue;
-                            const uint32_t first = __ffs(nb) - 1;
-                            buf[pos++] = (uint8_t)((18u << 1) | (first >> 1));
-                            buf[pos++] = (uint8_t)((18u << 1) | (first & 1u));
-                            skip = 1u << (r0 + first);
-                            rows &= ~(skip - 1u);
-                        }
 #pragma unroll 1
                         for (; rows; rows &= rows - 1) {
                             const int r = __ffs(rows) - 1, i = r - r0;
