@@ -73,6 +73,12 @@ struct Nbr {
     uint32_t S;    // own column as before this stripe
 };
 
+// Per 4-bit group of x, its number of set bits.
+__device__ __forceinline__ uint32_t nibbleCounts(uint32_t x) {
+    x = x - ((x >> 1) & 0x55555555u);
+    return (x & 0x33333333u) + ((x >> 2) & 0x33333333u);
+}
+
 // Warp-inclusive prefix sum.
 __device__ __forceinline__ uint32_t warpScan(uint32_t v, int lane) {
 #pragma unroll
@@ -240,17 +246,19 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                     uint32_t runs = 0;
                     // (3) decisions per stripe, 10-bit fields, three stripes per word
                     uint32_t w0 = 0, w1 = 0, w2 = 0;
+                    if (type != 2) {
+                        // one decision per coded row, and a sign decision per new one: the
+                        // popcounts of the 4-row groups, all stripes at once
+                        const uint32_t c = nibbleCounts(E) + (type == 0 ? nibbleCounts(NEW) : 0u);
+                        w0 = (c & 0xFu) | (((c >> 4) & 0xFu) << 10) | (((c >> 8) & 0xFu) << 20);
+                        w1 = ((c >> 12) & 0xFu) | (((c >> 16) & 0xFu) << 10) | (((c >> 20) & 0xFu) << 20);
+                        w2 = ((c >> 24) & 0xFu) | (((c >> 28) & 0xFu) << 10);
+                    } else {
 #pragma unroll 1
-                    for (int s = 0; s < nstripes; ++s) {
-                        const int r0 = 4 * s;
-                        const uint32_t Q = 0xFu << r0, P = (1u << r0) - 1u;
-                        uint32_t cnt;
-                        if (type == 1) {
-                            cnt = __popc(E & Q);
-                        } else if (type == 0) {
-                            cnt = __popc(E & Q) + __popc(NEW & Q);
-                        } else {
-                            cnt = __popc(E & Q) + __popc(NEW & Q);
+                        for (int s = 0; s < nstripes; ++s) {
+                            const int r0 = 4 * s;
+                            const uint32_t Q = 0xFu << r0, P = (1u << r0) - 1u;
+                            uint32_t cnt = __popc(E & Q) + __popc(NEW & Q);
                             if (r0 + 3 < h && (E & Q) == Q) {
                                 const uint32_t L = SLp | (NL & (P | Q)), R = SRp | (NR & P), Sb = Spass | (NEW & P);
                                 const uint32_t win = r0 == 0 ? 0x1Fu : (0x3Fu << (r0 - 1));
@@ -265,11 +273,11 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                                     }
                                 }
                             }
+                            const uint32_t f = cnt << (10 * (s % 3));
+                            if (s < 3) w0 |= f;
+                            else if (s < 6) w1 |= f;
+                            else w2 |= f;
                         }
-                        const uint32_t f = cnt << (10 * (s % 3));
-                        if (s < 3) w0 |= f;
-                        else if (s < 6) w1 |= f;
-                        else w2 |= f;
                     }
                     const uint32_t i0 = warpScan(w0, lane), i1 = warpScan(w1, lane), i2 = warpScan(w2, lane);
                     const uint32_t t0 = __shfl_sync(kFull, i0, 31), t1 = __shfl_sync(kFull, i1, 31),
