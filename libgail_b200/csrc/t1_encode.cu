@@ -190,18 +190,10 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                 uint32_t E = 0, NEW = 0;
                 if (type == 0) {
                     // significance propagation: eligible = insignificant with a significant
-                    // neighbour in scan order; stripes in order, each a warp fixpoint. A
-                    // neighbour significant when a sample is coded was significant before the
-                    // pass or has a 1 in this plane, so a stripe where no insignificant sample
-                    // of any column is next to such a one codes nothing and is skipped.
-                    const uint32_t sup = sig | Bp, supL = shUp(sup, lane), supR = shDown(sup, lane);
-                    const uint32_t near = supL | (supL << 1) | (supL >> 1) | supR | (supR << 1) | (supR >> 1) |
-                                          (sup << 1) | (sup >> 1);
-                    const uint32_t live = __reduce_or_sync(kFull, valid & ~sig & near);
+                    // neighbour in scan order; stripes in order, each a warp fixpoint
 #pragma unroll 1
                     for (int s = 0; s < nstripes; ++s) {
                         const int r0 = 4 * s;
-                        if (!((live >> r0) & 0xFu)) continue;
                         const uint32_t S = sig, SL = shUp(S, lane), R = shDown(S, lane);
                         const uint32_t cand = (0xFu << r0) & valid & ~S;
                         const uint32_t spreadLR = SL | (SL << 1) | (SL >> 1) | R | (R << 1) | (R >> 1);
