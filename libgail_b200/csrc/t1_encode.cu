@@ -472,8 +472,9 @@ __global__ void __launch_bounds__(1024) t1OrderKernel(T1Launch P, uint32_t maxSo
 }
 
 // ---------------------------------------------------------------------------- MQ coding
-// Context state word: Qe | MPS << 16 | state index << 17. The next-state table has four
-// entries per state, by (MPS, LPS): the state word after a renormalising decision.
+// Context state word: Qe | MPS << 16 | state index << 17. nextStateEntry(k), k = state
+// index << 2 | MPS << 1 | LPS: the state word after a renormalising decision; the coder keeps
+// the two entries of each (state, MPS) side by side.
 __device__ __forceinline__ uint32_t nextStateEntry(uint32_t k) {
     const uint32_t idx = k >> 2, mps = (k >> 1) & 1u, lps = k & 1u, e = c_mq[idx];
     const uint32_t nidx = lps ? (e >> 24) & 63u : (e >> 18) & 63u;
@@ -507,16 +508,18 @@ struct Coder {
     }
     // One decision in context state t; returns the context's next state. Renormalisation
     // shifts by clz(A) - 16, which is 0 when A stayed at or above 0x8000; the byte-out is the
-    // only branch.
-    __device__ __forceinline__ uint32_t encode(uint32_t t, uint32_t d, const uint32_t* next) {
+    // only branch. next[t >> 16] holds both successors of the state (after an MPS that
+    // renormalises, after an LPS), so the load does not wait for the decision's outcome.
+    __device__ __forceinline__ uint32_t encode(uint32_t t, uint32_t d, const uint2* next) {
+        const uint2 succ = next[t >> 16];
         const uint32_t qe = t & 0xFFFFu;
         const uint32_t a = A - qe;
-        const bool lps = d != ((t >> 16) & 1u);
+        const bool lps = ((d ^ (t >> 16)) & 1u) != 0;
         const bool upper = (a >= qe) != lps;  // which sub-interval the decision takes
         C += upper ? qe : 0u;
         A = upper ? a : qe;
         const bool rn = lps || !(a & 0x8000u);
-        const uint32_t nt = next[((t >> 15) & ~1u) | (lps ? 1u : 0u)];
+        const uint32_t nt = lps ? succ.y : succ.x;
         int n = __clz(A) - 16;
         A <<= n;
         for (;;) {
@@ -575,10 +578,11 @@ __device__ uint32_t truncLen(uint4 s, const uint8_t* buf, uint32_t len, uint32_t
 // than the GPU holds and runs uncapped; wide batched launches run at 12 CTAs per SM.
 template <int MINB>
 __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
-    __shared__ uint32_t s_next[4 * 47];
+    __shared__ uint2 s_next[2 * 47];  // by (state, MPS): next state after an MPS renormalisation, after an LPS
     __shared__ uint32_t s_init[4];
     __shared__ uint32_t s_ctx[19 * MQ_THREADS];
-    for (int i = threadIdx.x; i < 4 * 47; i += blockDim.x) s_next[i] = nextStateEntry(i);
+    for (int i = threadIdx.x; i < 2 * 47; i += blockDim.x)
+        s_next[i] = make_uint2(nextStateEntry(2 * i), nextStateEntry(2 * i + 1));
     if (threadIdx.x == 0) {
         s_init[0] = initialState(0);
         s_init[1] = initialState(4);
@@ -686,6 +690,33 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
         nxt = (pos + 16 < nsym) ? *reinterpret_cast<const uint4*>(sym + pos + 16) : make_uint4(0, 0, 0, 0);
         uint32_t w0 = v.x, w1 = v.y, w2 = v.z, w3 = v.w;
         const uint32_t w4 = nxt.x;
+        // one decision: s (context and bit) in state t; sn the next decision
+        auto one = [&](uint32_t sn) {
+            // the byte past the block's last decision is not a decision: the clamp keeps its
+            // look-ahead read inside the lane's 19 contexts
+            const uint32_t cn = min(sn >> 1, 18u), cx = s >> 1;
+            const uint32_t tn = ctx[cn * MQ_THREADS];
+            const uint32_t tNew = e.encode(t, s & 1u, s_next);
+            ctx[cx * MQ_THREADS] = tNew;
+            t = cn == cx ? tNew : tn;
+            s = sn;
+            ++pos;
+        };
+        if (pos + 16 <= stop) {  // no pass or block end in the chunk: no checks
+#pragma unroll 1
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t cur = w0;
+                one((cur >> 8) & 0xFFu);
+                one((cur >> 16) & 0xFFu);
+                one(cur >> 24);
+                one(w1 & 0xFFu);
+                w0 = w1;
+                w1 = w2;
+                w2 = w3;
+                w3 = w4;
+            }
+            continue;
+        }
         bool done = false;
 #pragma unroll 1
         for (int q = 0; q < 4 && !done; ++q) {
@@ -705,16 +736,7 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
                     }
                     stop = min(nsym, nextEnd);
                 }
-                // the byte past the block's last decision is not a decision: the clamp keeps
-                // its look-ahead read inside the lane's 19 contexts
-                const uint32_t sn = b < 3 ? (cur >> (8 * (b + 1))) & 0xFFu : w1 & 0xFFu;
-                const uint32_t cn = min(sn >> 1, 18u), cx = s >> 1;
-                const uint32_t tn = ctx[cn * MQ_THREADS];
-                const uint32_t tNew = e.encode(t, s & 1u, s_next);
-                ctx[cx * MQ_THREADS] = tNew;
-                t = cn == cx ? tNew : tn;
-                s = sn;
-                ++pos;
+                one(b < 3 ? (cur >> (8 * (b + 1))) & 0xFFu : w1 & 0xFFu);
             }
             w0 = w1;
             w1 = w2;
