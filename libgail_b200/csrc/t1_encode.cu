@@ -702,21 +702,6 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
             s = sn;
             ++pos;
         };
-        if (pos + 16 <= stop) {  // no pass or block end in the chunk: no checks
-#pragma unroll 1
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t cur = w0;
-                one((cur >> 8) & 0xFFu);
-                one((cur >> 16) & 0xFFu);
-                one(cur >> 24);
-                one(w1 & 0xFFu);
-                w0 = w1;
-                w1 = w2;
-                w2 = w3;
-                w3 = w4;
-            }
-            continue;
-        }
         bool done = false;
 #pragma unroll 1
         for (int q = 0; q < 4 && !done; ++q) {
