@@ -575,7 +575,8 @@ __device__ uint32_t truncLen(uint4 s, const uint8_t* buf, uint32_t len, uint32_t
 }
 
 // MINB: CTAs per SM the registers must allow. A launch of a frame or two has fewer lanes
-// than the GPU holds and runs uncapped; wide batched launches run at 12 CTAs per SM.
+// than the GPU holds and runs uncapped; wide batched launches run at 10 CTAs per SM (the
+// registers that allows need no spill; measured faster on B200 than 12 with a spill).
 template <int MINB>
 __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
     __shared__ uint2 s_next[2 * 47];  // by (state, MPS): next state after an MPS renormalisation, after an LPS
@@ -599,6 +600,7 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
     // Per-lane state of the block in hand. Invariant between decisions: s is the decision
     // at pos and t the state of its context; nxt holds the decisions from pos on.
     uint32_t job = 0, pos = 0, nsym = 0, np = 0, k = 0, nextEnd = 0, stop = 0, s = 0, t = 0;
+    uint32_t laterEnd = 0;  // the pass end after nextEnd, loaded one pass ahead
     const uint8_t* sym = nullptr;
     uint4 nxt = make_uint4(0, 0, 0, 0);
     Coder e;
@@ -633,6 +635,7 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
         pos = 0;
         k = 0;
         nextEnd = P.passEnd[(size_t)job * kMaxPasses];
+        laterEnd = np > 1 ? P.passEnd[(size_t)job * kMaxPasses + 1] : 0xFFFFFFFFu;
         stop = min(nsym, nextEnd);
         nxt = nsym ? *reinterpret_cast<const uint4*>(sym) : make_uint4(0, 0, 0, 0);
         s = nxt.x & 0xFFu;
@@ -717,7 +720,8 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
                         P.snaps[(size_t)job * kMaxPasses + k] =
                             make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
                         ++k;
-                        nextEnd = k < np ? P.passEnd[(size_t)job * kMaxPasses + k] : 0xFFFFFFFFu;
+                        nextEnd = laterEnd;  // loaded a pass ago: no wait here
+                        laterEnd = k + 1 < np ? P.passEnd[(size_t)job * kMaxPasses + k + 1] : 0xFFFFFFFFu;
                     }
                     stop = min(nsym, nextEnd);
                 }
@@ -799,7 +803,7 @@ void t1Encode(const T1Launch& launch, cudaStream_t st, cudaEvent_t* marks) {
     t1OrderKernel<<<1, 1024, 0, st>>>(L, mqBlocks * (MQ_THREADS / 32) / 2);
     if (marks) GB_CHECK(cudaEventRecord(marks[1], st));
     if (mqBlocks <= (uint32_t)sms * 4u) t1MqKernel<1><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
-    else t1MqKernel<12><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
+    else t1MqKernel<10><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
     t1TruncKernel<<<min(divUp(L.n, (uint32_t)(TRUNC_THREADS / 32)), (uint32_t)sms * 8u), TRUNC_THREADS, 0, st>>>(L);
     GB_CHECK(cudaGetLastError());
 }
