@@ -59,8 +59,8 @@ WORKLOAD = ("4K 3996x2160 Y'CbCr 4:2:2 10-bit BT.2020 PQ -> 12-bit X'Y'Z', 9/7 6
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on one 4K
 # frame, and Tier-1 issue figures, from the ncu capture summarised in the file below
 NCU_SOURCE = "profiles/kernels_4k_encode_frame.md"
-NCU_TRAFFIC = {"t1CmKernel": 215.30e6, "t1MqKernel": 192.05e6}
-NCU_TIER1 = {"cm_issue_active_pct": 71.4, "cm_warps_per_sm": 23.3, "mq_issue_active_pct": 29.6, "mq_warps_per_sm": 4.8,
+NCU_TRAFFIC = {"t1CmKernel": 214.53e6, "t1MqKernel": 180.17e6}
+NCU_TIER1 = {"cm_issue_active_pct": 72.2, "cm_warps_per_sm": 23.1, "mq_issue_active_pct": 30.8, "mq_warps_per_sm": 4.7,
              "decode_issue_active_pct": 23.4, "decode_warps_per_sm": 4.4}
 
 
