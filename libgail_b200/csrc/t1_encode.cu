@@ -799,10 +799,13 @@ void t1Encode(const T1Launch& launch, cudaStream_t st, cudaEvent_t* marks) {
     const uint32_t cmBlocks = min(divUp(L.n, CM_WARPS), (uint32_t)sms * L.cmCtasPerSm);
     t1CmKernel<<<cmBlocks, CM_THREADS, 0, st>>>(L);
     if (marks) GB_CHECK(cudaEventRecord(marks[0], st));
-    const uint32_t mqBlocks = min(divUp(L.n, MQ_THREADS), (uint32_t)sms * L.mqCtasPerSm);
+    // a wide (batched) launch gives each lane two blocks on average, so that lanes whose
+    // blocks end early take more from the queue
+    const bool wide = divUp(L.n, MQ_THREADS) > (uint32_t)sms * 4u;
+    const uint32_t mqBlocks = min(divUp(L.n, MQ_THREADS * (wide ? 2u : 1u)), (uint32_t)sms * L.mqCtasPerSm);
     t1OrderKernel<<<1, 1024, 0, st>>>(L, mqBlocks * (MQ_THREADS / 32) / 2);
     if (marks) GB_CHECK(cudaEventRecord(marks[1], st));
-    if (mqBlocks <= (uint32_t)sms * 4u) t1MqKernel<1><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
+    if (!wide) t1MqKernel<1><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
     else t1MqKernel<10><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
     t1TruncKernel<<<min(divUp(L.n, (uint32_t)(TRUNC_THREADS / 32)), (uint32_t)sms * 8u), TRUNC_THREADS, 0, st>>>(L);
     GB_CHECK(cudaGetLastError());
