@@ -63,6 +63,7 @@ struct EncodeEngine::Slot {
     cudaGraphExec_t exec = nullptr;
     int graphKernels = 0;  // kernel launches one front-end graph makes
     cudaEvent_t frontDone = nullptr;
+    cudaEvent_t upDone = nullptr;  // the frame's upload (on the copy stream) is done
     std::vector<void*> dev, host;
 };
 
@@ -135,6 +136,7 @@ EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(
     }
     budget_ = hbmBudget;
     GB_CHECK(cudaStreamCreateWithFlags(&front_, cudaStreamNonBlocking));
+    GB_CHECK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
     constexpr int kMaxSlots = 1024;
     check(cudaMalloc(&dSlope_, kMaxSlots * 4), "device memory for the engine");
     check(cudaHostAlloc((void**)&hSlope_, kMaxSlots * 4, cudaHostAllocDefault), "pinned host memory");
@@ -164,6 +166,7 @@ EncodeEngine::~EncodeEngine() {
         if (s->exec) cudaGraphExecDestroy(s->exec);
         if (s->graph) cudaGraphDestroy(s->graph);
         if (s->frontDone) cudaEventDestroy(s->frontDone);
+        if (s->upDone) cudaEventDestroy(s->upDone);
         for (void* p : s->dev) cudaFree(p);
         for (void* p : s->host) cudaFreeHost(p);
     }
@@ -178,6 +181,7 @@ EncodeEngine::~EncodeEngine() {
     if (dSlope_) cudaFree(dSlope_);
     if (hSlope_) cudaFreeHost(hSlope_);
     if (front_) cudaStreamDestroy(front_);
+    if (copy_) cudaStreamDestroy(copy_);
     cudaGetLastError();
 }
 
@@ -272,6 +276,7 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         buildJobs(c.L, s->dCoeffs, s->dSym, s->dCw, (uint32_t)s->index, jobs);
         GB_CHECK(cudaMemcpy(s->dJobs, jobs.data(), jobs.size() * sizeof(T1Job), cudaMemcpyHostToDevice));
         GB_CHECK(cudaEventCreateWithFlags(&s->frontDone, cudaEventDisableTiming));
+        GB_CHECK(cudaEventCreateWithFlags(&s->upDone, cudaEventDisableTiming));
         // the slot's front end as one graph: it always reads the slot's input buffer and
         // writes the slot's coefficient buffer
         cudaStream_t cap;
@@ -298,6 +303,7 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         if (s->exec) cudaGraphExecDestroy(s->exec);
         if (s->graph) cudaGraphDestroy(s->graph);
         if (s->frontDone) cudaEventDestroy(s->frontDone);
+        if (s->upDone) cudaEventDestroy(s->upDone);
         cudaGetLastError();
         std::lock_guard<std::mutex> lock(budgetM_);
         used_ -= c.slotBytes;
@@ -649,9 +655,13 @@ bool EncodeEngine::admit() {
         Class& c = *classes_[r->cls];
         r->slot = s;
         hSlope_[s->index] = (float)r->slope;
-        GB_CHECK(cudaMemcpyAsync(dSlope_ + s->index, hSlope_ + s->index, 4, cudaMemcpyHostToDevice, front_));
+        // the upload on the copy stream, so that it overlaps the front ends of the frames
+        // before; the front end waits for it
+        GB_CHECK(cudaMemcpyAsync(dSlope_ + s->index, hSlope_ + s->index, 4, cudaMemcpyHostToDevice, copy_));
         GB_CHECK(cudaMemcpyAsync(s->dIn, r->frame, c.z.inBytes, r->onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                 front_));
+                                 copy_));
+        GB_CHECK(cudaEventRecord(s->upDone, copy_));
+        GB_CHECK(cudaStreamWaitEvent(front_, s->upDone, 0));
         GB_CHECK(cudaGraphLaunch(s->exec, front_));
         GB_CHECK(cudaEventRecord(s->frontDone, front_));
         std::lock_guard<std::mutex> lock(m_);

@@ -125,6 +125,7 @@ private:
     int minBatchPct_ = 25;
     double maxWaitMs_ = 2.0;
     cudaStream_t front_ = nullptr;
+    cudaStream_t copy_ = nullptr;  // frame uploads
     std::vector<std::unique_ptr<Class>> classes_;
     std::vector<std::unique_ptr<Slot>> slots_;
     std::vector<std::unique_ptr<Batch>> batches_;
