@@ -144,6 +144,16 @@ GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
  *                          frame in host memory, with the hull points computed on the GPU
  *                          (gb_rate_and_build_hull's path); GB_CS_TIER1: the Tier-1 frame and
  *                          its hull points also in host memory, as without codestreams
+ *   gb_engine_set_slope_factor  Tier-1 early termination as libgail's pipeline drives it
+ *                          (src/core/pipeline.cpp:194-217; gail.h's encoder forces 0.25,
+ *                          src/api/gail_api.cpp:607): each encode admitted from now on stops
+ *                          coding a block's bit-planes below lastLambda x factor, lastLambda the
+ *                          smallest per-component slope threshold of the last finished frame's
+ *                          rate control (0 at first: every pass); a frame whose own threshold
+ *                          comes out below the one it was coded with is coded again with every
+ *                          pass. 0 turns it off. Needs codestreams on
+ *   gb_engine_frame_info   a finished encode's first early-termination threshold and whether
+ *                          it was coded again with every pass
  *   gb_engine_counters     for the engine's encodes so far: host-to-device and device-to-host
  *                          bytes copied (frames in; Tier-1 frames, rate-control read-backs and
  *                          codestreams out) and kernels launched (any pointer may be NULL)
@@ -179,6 +189,8 @@ enum { GB_CS_HOST = 1, GB_CS_TIER1 = 2 };
 GB_API int gb_engine_set_codestream(GbEngine* e, double fps, double maxMbps, double compMbps, const char* label,
                                     const char* tag, int threads, int check, int flags);
 GB_API int gb_engine_counters(GbEngine* e, uint64_t* h2d, uint64_t* d2h, uint64_t* launches);
+GB_API int gb_engine_set_slope_factor(GbEngine* e, double factor);
+GB_API int gb_engine_frame_info(GbEngine* e, int64_t id, double* threshold, int* recoded);
 GB_API int gb_engine_codestream(GbEngine* e, int64_t id, const uint8_t** data, uint64_t* size, int* dciOk);
 GB_API int gb_engine_add_decoder(GbEngine* e, const GailCudaLayout* layout, const GailCudaDecodeSettings* settings,
                                  int* classId, uint64_t* frameBytes);

@@ -108,6 +108,20 @@ GB_API int gb_engine_hull(GbEngine* e, int64_t id, const uint8_t** passes, const
     });
 }
 
+GB_API int gb_engine_set_slope_factor(GbEngine* e, double factor) {
+    return gbGuard([&] {
+        if (!e) throw std::logic_error("null argument");
+        e->e->setSlopeFactor(factor);
+    });
+}
+
+GB_API int gb_engine_frame_info(GbEngine* e, int64_t id, double* threshold, int* recoded) {
+    return gbGuard([&] {
+        if (!e || !threshold || !recoded) throw std::logic_error("null argument");
+        if (!e->e->frameInfo(id, threshold, recoded)) throw std::logic_error("not an encode request");
+    });
+}
+
 GB_API int gb_engine_set_policy(GbEngine* e, int maxBatch, int minBatchPct, double maxWaitMs) {
     return gbGuard([&] {
         if (!e) throw std::logic_error("null argument");

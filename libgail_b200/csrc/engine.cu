@@ -78,6 +78,8 @@ struct EncodeEngine::Request {
     Slot* slot = nullptr;
     uint32_t jobBase = 0;
     int status = 0;
+    double thr = 0;         // the early-termination threshold it was first coded with
+    bool recoded = false;   // coded again with every pass
     bool tier1 = true;      // the Tier-1 frame was packed into host memory
     bool devFrame = false;  // ... and into the slot's device buffers
     std::vector<uint8_t> cs;  // the codestream, when the engine makes them
@@ -140,6 +142,8 @@ EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(
     constexpr int kMaxSlots = 1024;
     check(cudaMalloc(&dSlope_, kMaxSlots * 4), "device memory for the engine");
     check(cudaHostAlloc((void**)&hSlope_, kMaxSlots * 4, cudaHostAllocDefault), "pinned host memory");
+    check(cudaHostAlloc((void**)&hZero_, 16, cudaHostAllocDefault), "pinned host memory");
+    *hZero_ = 0.f;
     for (int i = 0; i < 2; ++i) batches_.push_back(std::make_unique<Batch>());
     for (auto& b : batches_) {
         GB_CHECK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
@@ -180,6 +184,7 @@ EncodeEngine::~EncodeEngine() {
     }
     if (dSlope_) cudaFree(dSlope_);
     if (hSlope_) cudaFreeHost(hSlope_);
+    if (hZero_) cudaFreeHost(hZero_);
     if (front_) cudaStreamDestroy(front_);
     if (copy_) cudaStreamDestroy(copy_);
     cudaGetLastError();
@@ -583,11 +588,16 @@ void EncodeEngine::codestreamWorker(int id) {
             cvDone_.notify_all();
             continue;
         }
-        const Slot* s = r->slot;
+        Slot* s = r->slot;
         const RateLimits lim = dciLimits(cs_.fps, cs_.maxMbps, cs_.compMbps);
         uint64_t d2h = r->tier1 ? (uint64_t)s->n * 20 + (uint64_t)s->hTot[1] * 17 + s->hTot[0] : 0, launches = 0;
+        bool again = false;  // coded with early termination past what rate control keeps: code again
         if (r->status == kOk) {
             try {
+                double lam = 0;  // the smallest per-component slope threshold of the rate control
+                auto minComp = [](const RateResult& rr) {
+                    return std::min({rr.lambdaComp[0], rr.lambdaComp[1], rr.lambdaComp[2]});
+                };
                 if (r->devFrame) {
                     if (!rc) throw std::logic_error("no device rate control for this worker and class");
                     const DeviceTier1 f{reinterpret_cast<const GbCblkInfo*>(s->dInfoP), s->dLenP, s->dDataP, s->dHullP,
@@ -595,6 +605,8 @@ void EncodeEngine::codestreamWorker(int id) {
                     const RateResult rr = rc->run(f, lim, cs_.tag, r->cs, st);
                     d2h += rr.d2hBytes;
                     launches = (uint64_t)rr.launches;
+                    lam = minComp(rr);
+                    again = r->thr > 0 && !r->recoded && lam < r->thr;
                 } else {
                     auto& w = writers[r->cls];
                     if (!w) w = std::make_unique<CodestreamWriter>(c->L, cs_.label);
@@ -608,22 +620,59 @@ void EncodeEngine::codestreamWorker(int id) {
                     v.numData = s->hTot[0];
                     const HullView hull{s->hHullPasses, s->hHullSlope};  // computed on the GPU
                     const RateResult rr = allocateRate(*w, v, lim, &hull);
-                    w->build(v, rr.passes.data(), &r->cs, cs_.tag);
+                    lam = minComp(rr);
+                    again = r->thr > 0 && !r->recoded && lam < r->thr;
+                    if (!again) w->build(v, rr.passes.data(), &r->cs, cs_.tag);
                 }
-                if (cs_.check) r->dciOk = checkDci(r->cs.data(), r->cs.size(), cs_.fps).ok ? 1 : 0;
+                if (!again) {
+                    lastLambda_.store(lam);
+                    if (cs_.check) r->dciOk = checkDci(r->cs.data(), r->cs.size(), cs_.fps).ok ? 1 : 0;
+                } else {
+                    // the frame is easier than the one its threshold came from: passes the rate
+                    // control now keeps may have been left out; its Tier-1 again, every pass
+                    // (the coefficients are still in its slot)
+                    r->recoded = true;
+                    r->cs.clear();
+                    GB_CHECK(cudaMemcpyAsync(dSlope_ + s->index, hZero_, 4, cudaMemcpyHostToDevice, copy_));
+                    GB_CHECK(cudaEventRecord(s->frontDone, copy_));
+                }
             } catch (const std::exception&) {
                 r->status = kError;
+                again = false;
             }
         }
-        const auto now = Clock::now();
         std::lock_guard<std::mutex> lock(m_);
-        r->latency = msBetween(r->t0, now);
-        done_.push_back(r);
-        stats_.frames++;
         stats_.d2hBytes += d2h;
         stats_.launches += launches;
+        if (again) {
+            front_q_.push_back(r);
+            cvWork_.notify_all();
+            continue;
+        }
+        r->latency = msBetween(r->t0, Clock::now());
+        done_.push_back(r);
+        stats_.frames++;
         cvDone_.notify_all();
     }
+}
+
+void EncodeEngine::setSlopeFactor(double factor) {
+    if (!(factor >= 0)) throw std::logic_error("slope factor must be 0 or more");
+    if (factor > 0) {
+        std::lock_guard<std::mutex> lock(m_);
+        if (!csOn_) throw std::logic_error("early termination needs codestreams on (its thresholds come from them)");
+    }
+    slopeFactor_.store(factor);
+}
+
+bool EncodeEngine::frameInfo(int64_t id, double* threshold, int* recoded) {
+    std::lock_guard<std::mutex> lock(m_);
+    if (id < 0 || id >= (int64_t)requests_.size() || !requests_[id]) throw std::logic_error("unknown request");
+    const Request* r = requests_[id].get();
+    if (r->decode) return false;
+    *threshold = r->thr;
+    *recoded = r->recoded ? 1 : 0;
+    return true;
 }
 
 EncodeEngine::Stats EncodeEngine::stats() const {
@@ -654,6 +703,9 @@ bool EncodeEngine::admit() {
         }
         Class& c = *classes_[r->cls];
         r->slot = s;
+        const double factor = slopeFactor_.load();
+        if (factor > 0) r->slope = lastLambda_.load() * factor;  // as libgail's pipeline
+        r->thr = r->slope;
         hSlope_[s->index] = (float)r->slope;
         // the upload on the copy stream, so that it overlaps the front ends of the frames
         // before; the front end waits for it

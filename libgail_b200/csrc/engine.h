@@ -75,6 +75,16 @@ public:
         bool onDevice = true, tier1 = false;
     };
     void setCodestream(const CodestreamConfig& c);
+    // Tier-1 early termination as libgail's pipeline drives it (src/core/pipeline.cpp:194-217):
+    // with factor > 0 each encode admitted from now on stops coding a block's bit-planes
+    // below the threshold lastLambda x factor, lastLambda being the smallest per-component
+    // slope threshold of the rate control of the frame finished last (0 at first: every
+    // pass); a frame whose own threshold comes out below the one it was coded with is coded
+    // again with every pass before its codestream is made. Needs codestreams on.
+    void setSlopeFactor(double factor);
+    // The early-termination threshold a finished encode was first coded with, and whether
+    // it was coded again with every pass.
+    bool frameInfo(int64_t id, double* threshold, int* recoded);
     // The codestream of a finished frame (valid until release): its bytes and whether it
     // passed the DCI check (-1 when not checked). False when codestreams are off.
     bool codestream(int64_t id, const uint8_t** data, uint64_t* size, int* dciOk);
@@ -140,6 +150,8 @@ private:
     std::vector<Request*> front_q_;   // front end enqueued, not yet in a batch
     std::deque<Request*> done_;       // finished, not yet handed out
     std::atomic<bool> stop_{false};
+    std::atomic<double> slopeFactor_{0.0}, lastLambda_{0.0};
+    float* hZero_ = nullptr;  // a pinned 0 threshold for frames coded again
     std::string error_;
     Stats stats_;
     std::thread worker_;

@@ -24,6 +24,8 @@ def _bind():
     L.gb_engine_stats.argtypes = [C.c_void_p, C.c_void_p]
     L.gb_engine_set_codestream.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_char_p, C.c_char_p,
                                            C.c_int, C.c_int, C.c_int]
+    L.gb_engine_set_slope_factor.argtypes = [C.c_void_p, C.c_double]
+    L.gb_engine_frame_info.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_int)]
     L.gb_engine_counters.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.gb_engine_codestream.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_uint8)),
                                        C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
@@ -92,6 +94,19 @@ class Engine:
         flags = (0 if on_device else 1) | (2 if tier1 else 0)
         check(lib().gb_engine_set_codestream(self.h, fps, max_mbps, comp_mbps, label.encode(), tag.encode(), threads,
                                              int(check_dci), flags))
+
+    def set_slope_factor(self, factor: float):
+        """Tier-1 early termination at threshold = last frame's lambda x factor, with the
+        frame coded again with every pass when its own lambda comes out lower (libgail's
+        pipeline; its gail.h encoder uses 0.25). Needs codestreams on; 0 turns it off."""
+        check(lib().gb_engine_set_slope_factor(self.h, factor))
+
+    def frame_info(self, rid: int):
+        """(the early-termination threshold a finished encode was first coded with, whether
+        it was coded again with every pass)."""
+        t, rc = C.c_double(), C.c_int()
+        check(lib().gb_engine_frame_info(self.h, rid, C.byref(t), C.byref(rc)))
+        return t.value, bool(rc.value)
 
     def counters(self):
         """For the engine's encodes so far: (host-to-device bytes, device-to-host bytes,

@@ -262,3 +262,48 @@ def test_engine_mixed_encode_decode(dev):
             eng.release(rid)
     finally:
         eng.close()
+
+
+@pytest.mark.gpu
+def test_engine_early_termination(dev):
+    """Early termination as libgail's pipeline drives it: each frame's threshold is the last
+    frame's lambda x factor. Every codestream equals the one the plain encoder and the host
+    codec give for the same frame at the threshold it was coded with (every pass when it was
+    coded again) and is DCI-valid; at 0.25 the thresholds leave passes out; a factor that puts
+    the threshold above the frame's own lambda makes the engine code it again with every pass."""
+    from libgail_b200 import codestream as CS
+    W, H = 1998, 1080
+    frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=700 + i)) for i in range(4)]
+    lay = P.LayoutHolder(W, H, 0)
+    fmt, col = P.rgb48_format(W, H), P.color_passthrough()
+    enc = dev.encoder(lay, fmt, col)
+    eng = Engine(0, 0, max_batch=4)
+    try:
+        cid, _ = eng.add_encoder(lay, fmt, col)
+        eng.set_codestream(label=CS.DEFAULT_LABEL, tag="b200", threads=2)
+        for factor in (0.25, 1e9):
+            eng.set_slope_factor(factor)
+            active = recoded_n = 0
+            for f in frames:  # one at a time: each threshold comes from the frame before
+                rid = eng.submit(cid, f)
+                got, _, _, st = eng.wait(60000)
+                assert got == rid and st == 0
+                cs, ok = eng.codestream(rid)
+                thr, recoded = eng.frame_info(rid)
+                eng.release(rid)
+                assert ok == 1
+                enc.set_slope(0.0 if recoded else thr)
+                t1 = enc.encode(f)[0]
+                assert cs == CS.rate_and_build(lay, t1, tag="b200")[0]
+                if thr > 0 and not recoded:
+                    active += 1
+                    enc.set_slope(0.0)
+                    assert len(t1.pass_len) < len(enc.encode(f)[0].pass_len)  # passes left out
+                recoded_n += recoded
+            if factor == 0.25:
+                assert active >= 2
+            else:
+                assert recoded_n == len(frames)  # the first threshold comes from the 0.25 run
+    finally:
+        eng.close()
+        enc.close()
