@@ -7,7 +7,9 @@
 // blocks from a device queue ordered longest codeword first (orderKernel). A block's state is kept as row masks in
 // shared memory (significance and sign for rows -1..32, coded-this-plane and refined),
 // the scan visits only columns that have something to code (bit scans over candidate
-// masks), and the decoded words (sign, twice the magnitude plus the mid-point of the
+// masks) with the rows above, at and below the sample in registers (one shared load per
+// sample), zero-coding and sign contexts come from shared tables keyed by the neighbour
+// bits, and the decoded words (sign, twice the magnitude plus the mid-point of the
 // planes not decoded) are built in place in the wavelet plane and turned into floats
 // (word * step / 2) when the block is done. Untrusted input: bytes past the codeword read
 // as 0xFF, a block whose bytes lie outside the codestream decodes as zero, and nothing
@@ -41,9 +43,8 @@ namespace {
 // One code-block per warp: its lane 0 decodes it (the decode of a block is a serial chain
 // whose control flow depends on every decoded bit, so lanes of one warp decoding different
 // blocks would run one after another anyway); up to 32 such warps per SM keep the
-// schedulers busy. DEC_STRIDE: the state arrays hold one block.
+// schedulers busy.
 constexpr int DEC_THREADS = 32;
-constexpr int DEC_STRIDE = 1;
 constexpr int ORDER_BUCKETS = 128;
 
 __constant__ uint8_t c_zc[4 * 45];
@@ -142,7 +143,7 @@ struct MqDecoder {
     }
     // One decision in context cx (state word: table entry | mps << 16).
     __device__ __forceinline__ uint32_t decode(uint32_t* ctx, int cx, const uint32_t* tab) {
-        uint32_t t = ctx[cx * DEC_STRIDE];
+        uint32_t t = ctx[cx];
         const uint32_t qe = t & 0xFFFFu, mps = (t >> 16) & 1u;
         A -= qe;
         bool lps;
@@ -156,76 +157,82 @@ struct MqDecoder {
         }
         const uint32_t nidx = lps ? (t >> 24) & 63u : (t >> 18) & 63u;
         const uint32_t nm = mps ^ (lps ? (t >> 17) & 1u : 0u);
-        ctx[cx * DEC_STRIDE] = tab[nidx] | (nm << 16);
+        ctx[cx] = tab[nidx] | (nm << 16);
         renorm();
         return lps ? mps ^ 1u : mps;
     }
 };
 
 __device__ __forceinline__ uint32_t bt(uint32_t m, int x) { return (m >> x) & 1u; }
-__device__ __forceinline__ int chiAt(uint32_t s, uint32_t g, int x) {
-    return (x < 0 || x > 31) ? 0 : (bt(s, x) ? (bt(g, x) ? -1 : 1) : 0);
+// Row bits x-1, x, x+1 of a 32-column row mask at bits 0..2 (zero outside the block).
+__device__ __forceinline__ uint32_t win3(uint32_t row, int x) { return __funnelshift_r(row << 1, row >> 31, x) & 7u; }
+// Neighbour key of sample (x, row M) from the rows above (U) and below (D): bits 0-2 row
+// above columns x-1..x+1, 3 and 5 same row columns x-1 and x+1, 6-8 row below.
+__device__ __forceinline__ uint32_t nbKey(uint32_t U, uint32_t M, uint32_t D, int x) {
+    return win3(U, x) | ((win3(M, x) & 5u) << 3) | (win3(D, x) << 6);
 }
 
-struct BlockState {
-    uint32_t* sig;  // rows -1..32 at index (y + 1) * DEC_STRIDE
-    uint32_t* sgn;
-    uint32_t* vis;  // rows 0..31
-    uint32_t* ref;
+struct BlockCtx {
+    uint32_t* sig;  // significance rows -1..32 at index y + 1
+    uint32_t* sgn;  // sign rows, the same indexing
     uint32_t* out;  // the block's top-left word in the plane
     uint32_t W;
-    const uint8_t* zc;
-    const uint8_t* sc;
+    const uint8_t* zk;  // zero-coding context by neighbour key, this block's orientation
+    const uint8_t* sk;  // sign context | xor bit << 5 by the sign key
     const uint32_t* tab;
     uint32_t* ctx;
     MqDecoder mq;
 
-    __device__ __forceinline__ uint32_t S(int y) const { return sig[(y + 1) * DEC_STRIDE]; }
-    __device__ __forceinline__ uint32_t G(int y) const { return sgn[(y + 1) * DEC_STRIDE]; }
-
-    __device__ __forceinline__ uint32_t zcAt(int x, int y) const {
-        const uint32_t U = S(y - 1), M = S(y), D = S(y + 1);
-        const uint32_t h = bt(M << 1, x) + bt(M >> 1, x);
-        const uint32_t v = bt(U, x) + bt(D, x);
-        const uint32_t d = bt(U << 1, x) + bt(U >> 1, x) + bt(D << 1, x) + bt(D >> 1, x);
-        return zc[h + 3 * v + 9 * d];
-    }
-    __device__ __forceinline__ bool anyNbr(int x, int y) const {
-        const uint32_t U = S(y - 1), M = S(y), D = S(y + 1);
-        const uint32_t all = U | (U << 1) | (U >> 1) | (M << 1) | (M >> 1) | D | (D << 1) | (D >> 1);
-        return bt(all, x);
-    }
-    // The sample's first 1-bit is in plane p: decode its sign and set bit plus mid-point.
-    __device__ __forceinline__ void becomeSig(int x, int y, int p) {
-        const uint32_t U = S(y - 1), M = S(y), D = S(y + 1);
-        const int hc = max(-1, min(1, chiAt(M, G(y), x - 1) + chiAt(M, G(y), x + 1)));
-        const int vc = max(-1, min(1, chiAt(U, G(y - 1), x) + chiAt(D, G(y + 1), x)));
-        const uint32_t t = sc[(hc + 1) * 3 + (vc + 1)];
-        const uint32_t neg = mq.decode(ctx, t & 31u, tab) ^ (t >> 5);
-        sig[(y + 1) * DEC_STRIDE] |= 1u << x;
-        if (neg) sgn[(y + 1) * DEC_STRIDE] |= 1u << x;
+    // Sample (x, y) with significance rows U, M, D (y - 1, y, y + 1) has its first 1-bit
+    // in plane p: decode its sign, set its significance (M too) and write sign, bit and
+    // mid-point.
+    __device__ __forceinline__ void becomeSig(uint32_t U, uint32_t& M, uint32_t D, int x, int y, int p) {
+        const uint32_t GU = sgn[y], GM = sgn[y + 1], GD = sgn[y + 2];
+        const uint32_t key = (win3(M, x) & 5u) | ((win3(GM, x) & 5u) << 1) | (bt(U, x) << 4) | (bt(GU, x) << 5) |
+                             (bt(D, x) << 6) | (bt(GD, x) << 7);
+        const uint32_t c = sk[key];
+        const uint32_t neg = mq.decode(ctx, c & 31u, tab) ^ (c >> 5);
+        M |= 1u << x;
+        sig[y + 1] = M;
+        sgn[y + 1] = GM | (neg << x);
         out[(size_t)y * W + x] = (neg << 31) | (3u << p);
     }
 };
 
 __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
-    __shared__ uint32_t s_sig[34 * DEC_STRIDE], s_sgn[34 * DEC_STRIDE], s_vis[32 * DEC_STRIDE], s_ref[32 * DEC_STRIDE];
-    __shared__ uint32_t s_ctx[19 * DEC_STRIDE];
+    // per block: significance and sign of rows -1..32, coded-this-plane and refined rows 0..31
+    __shared__ uint32_t s_sig[34], s_sgn[34], s_vis[32], s_ref[32];
+    __shared__ uint32_t s_ctx[19];
     __shared__ uint32_t s_tab[48];
     __shared__ uint8_t s_zc[4 * 45], s_sc[16];
+    // zero coding by orientation and neighbour key (nbKey); sign coding by the sign key:
+    // bits 0/1 left neighbour significant/negative, 2/3 right, 4/5 above, 6/7 below
+    __shared__ uint8_t s_zk[4 * 512], s_sk[256];
     for (int i = threadIdx.x; i < 47; i += blockDim.x) s_tab[i] = c_mq[i];
     for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) s_zc[i] = c_zc[i];
     if (threadIdx.x < 9) s_sc[threadIdx.x] = c_sc[threadIdx.x];
     __syncthreads();
-    if (threadIdx.x != 0) return;  // lane 0 decodes; the tables above were loaded by the whole warp
-    BlockState b;
+    for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) {
+        const int o = i >> 9, k = i & 511;
+        const int h = ((k >> 3) & 1) + ((k >> 5) & 1);
+        const int v = ((k >> 1) & 1) + ((k >> 7) & 1);
+        const int d = (k & 1) + ((k >> 2) & 1) + ((k >> 6) & 1) + ((k >> 8) & 1);
+        s_zk[i] = s_zc[45 * o + h + 3 * v + 9 * d];
+    }
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) {
+        auto chi = [&](int bit) { return ((k >> bit) & 1) ? (((k >> (bit + 1)) & 1) ? -1 : 1) : 0; };
+        const int hc = max(-1, min(1, chi(0) + chi(2)));
+        const int vc = max(-1, min(1, chi(4) + chi(6)));
+        s_sk[k] = s_sc[(hc + 1) * 3 + (vc + 1)];
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;  // lane 0 decodes; the tables above were built by the whole warp
+    BlockCtx b;
     b.sig = s_sig;
     b.sgn = s_sgn;
-    b.vis = s_vis;
-    b.ref = s_ref;
-    b.ctx = s_ctx;
-    b.sc = s_sc;
+    b.sk = s_sk;
     b.tab = s_tab;
+    b.ctx = s_ctx;
     b.W = a.W;
     const uint32_t count = a.ctl[2];
     for (;;) {
@@ -238,110 +245,133 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
         uint32_t* out = a.planes + blk.dst;  // zeroed before the launch: only significant samples are written
         const int nbps = code.nbps;
         const bool valid = code.passes > 0 && nbps >= 1 && nbps <= 30 && (uint64_t)code.offset + code.len <= a.size;
-        if (valid) {
-            b.out = out;
-            b.zc = s_zc + 45 * blk.orient;
-            for (int i = 0; i < 34; ++i) {
-                b.sig[i * DEC_STRIDE] = 0;
-                b.sgn[i * DEC_STRIDE] = 0;
-            }
-            for (int i = 0; i < 32; ++i) {
-                b.vis[i * DEC_STRIDE] = 0;
-                b.ref[i * DEC_STRIDE] = 0;
-            }
-            for (int c = 0; c < 19; ++c) b.ctx[c * DEC_STRIDE] = s_tab[0];
-            b.ctx[0] = s_tab[4];
-            b.ctx[17 * DEC_STRIDE] = s_tab[3];
-            b.ctx[18 * DEC_STRIDE] = s_tab[46];
-            b.mq.init(a.bytes + code.offset, code.len);
-            const uint32_t wmask = w >= 32 ? 0xFFFFFFFFu : (1u << w) - 1u;
-            int done = 0;
-            const int passes = code.passes;
-            for (int p = nbps - 1; p >= 0 && done < passes; --p) {
-                for (int type = (p == nbps - 1 ? 2 : 0); type < 3 && done < passes; ++type, ++done) {
-                    for (int y0 = 0; y0 < h; y0 += 4) {
-                        const int n = min(4, h - y0);
-                        if (type == 0) {
-                            uint32_t cm = 0;
+        if (!valid) continue;
+        b.out = out;
+        b.zk = s_zk + 512 * blk.orient;
+        for (int i = 0; i < 34; ++i) s_sig[i] = s_sgn[i] = 0;
+        for (int i = 0; i < 32; ++i) s_vis[i] = s_ref[i] = 0;
+        for (int c = 0; c < 19; ++c) s_ctx[c] = s_tab[0];
+        s_ctx[0] = s_tab[4];
+        s_ctx[17] = s_tab[3];
+        s_ctx[18] = s_tab[46];
+        b.mq.init(a.bytes + code.offset, code.len);
+        const uint32_t wmask = w >= 32 ? 0xFFFFFFFFu : (1u << w) - 1u;
+        int done = 0;
+        const int passes = code.passes;
+        for (int p = nbps - 1; p >= 0 && done < passes; --p) {
+            for (int type = (p == nbps - 1 ? 2 : 0); type < 3 && done < passes; ++type, ++done) {
+                // stripes of four rows from y0; rows y0-1..y0+4 lie in -1..32 (y0 <= 28) and
+                // rows at or past h are zero. Each column is scanned top to bottom with the
+                // rows above, at and below the sample in U, M, D.
+                for (int y0 = 0; y0 < h; y0 += 4) {
+                    const int n = min(4, h - y0);
+                    if (type == 0) {  // significance propagation
+                        uint32_t cm = 0;
+                        for (int k = 0; k < n; ++k) {
+                            const uint32_t U = s_sig[y0 + k], M = s_sig[y0 + k + 1], D = s_sig[y0 + k + 2];
+                            cm |= (U | (U << 1) | (U >> 1) | (M << 1) | (M >> 1) | D | (D << 1) | (D >> 1)) & ~M;
+                        }
+                        cm &= wmask;
+                        while (cm) {
+                            const int x = __ffs(cm) - 1;
+                            cm &= cm - 1;
+                            uint32_t U = s_sig[y0], M = s_sig[y0 + 1];
                             for (int k = 0; k < n; ++k) {
-                                const uint32_t U = b.S(y0 + k - 1), M = b.S(y0 + k), D = b.S(y0 + k + 1);
-                                const uint32_t nb = U | (U << 1) | (U >> 1) | (M << 1) | (M >> 1) | D | (D << 1) | (D >> 1);
-                                cm |= nb & ~M & wmask;
-                            }
-                            while (cm) {
-                                const int x = __ffs(cm) - 1;
-                                cm &= cm - 1;
-                                for (int k = 0; k < n; ++k) {
-                                    const int y = y0 + k;
-                                    if (bt(b.S(y), x) || !b.anyNbr(x, y)) continue;
-                                    const uint32_t bit = b.mq.decode(b.ctx, b.zcAt(x, y), b.tab);
-                                    b.vis[y * DEC_STRIDE] |= 1u << x;
-                                    if (bit) {
-                                        b.becomeSig(x, y, p);
-                                        cm |= (2u << x) & wmask;  // the next column may now be eligible
+                                const int y = y0 + k;
+                                const uint32_t D = s_sig[y + 2];
+                                if (!bt(M, x)) {
+                                    const uint32_t key = nbKey(U, M, D, x);
+                                    if (key) {
+                                        const uint32_t bit = b.mq.decode(s_ctx, b.zk[key], s_tab);
+                                        s_vis[y] |= 1u << x;
+                                        if (bit) {
+                                            b.becomeSig(U, M, D, x, y, p);
+                                            cm |= (2u << x) & wmask;  // the next column may now be eligible
+                                        }
                                     }
                                 }
+                                U = M;
+                                M = D;
                             }
-                        } else if (type == 1) {
-                            uint32_t cm = 0;
-                            for (int k = 0; k < n; ++k) cm |= b.S(y0 + k) & ~b.vis[(y0 + k) * DEC_STRIDE];
-                            while (cm) {
-                                const int x = __ffs(cm) - 1;
-                                cm &= cm - 1;
-                                for (int k = 0; k < n; ++k) {
-                                    const int y = y0 + k;
-                                    if (!bt(b.S(y), x) || bt(b.vis[y * DEC_STRIDE], x)) continue;
-                                    const int cx = bt(b.ref[y * DEC_STRIDE], x) ? 16 : (b.anyNbr(x, y) ? 15 : 14);
-                                    const uint32_t bit = b.mq.decode(b.ctx, cx, b.tab);
+                        }
+                    } else if (type == 1) {  // magnitude refinement
+                        uint32_t cm = 0;
+                        for (int k = 0; k < n; ++k) cm |= s_sig[y0 + k + 1] & ~s_vis[y0 + k];
+                        while (cm) {
+                            const int x = __ffs(cm) - 1;
+                            cm &= cm - 1;
+                            uint32_t U = s_sig[y0], M = s_sig[y0 + 1];
+                            for (int k = 0; k < n; ++k) {
+                                const int y = y0 + k;
+                                const uint32_t D = s_sig[y + 2];
+                                if (bt(M & ~s_vis[y], x)) {
+                                    const uint32_t ref = s_ref[y];
+                                    const int cx = bt(ref, x) ? 16 : (nbKey(U, M, D, x) ? 15 : 14);
+                                    const uint32_t bit = b.mq.decode(s_ctx, cx, s_tab);
                                     uint32_t& word = out[(size_t)y * a.W + x];
                                     word = bit ? word + (1u << p) : word - (1u << p);
-                                    b.ref[y * DEC_STRIDE] |= 1u << x;
+                                    s_ref[y] = ref | (1u << x);
                                 }
+                                U = M;
+                                M = D;
                             }
-                        } else {
-                            uint32_t cm = 0;
-                            for (int k = 0; k < n; ++k) cm |= ~b.S(y0 + k) & ~b.vis[(y0 + k) * DEC_STRIDE] & wmask;
-                            while (cm) {
-                                const int x = __ffs(cm) - 1;
-                                cm &= cm - 1;
-                                int r = 0;
-                                if (n == 4) {
-                                    bool quiet = true;
-                                    for (int k = 0; k < 4 && quiet; ++k) {
-                                        const int y = y0 + k;
-                                        if (bt(b.S(y) | b.vis[y * DEC_STRIDE], x) || b.anyNbr(x, y)) quiet = false;
-                                    }
-                                    if (quiet) {
-                                        if (!b.mq.decode(b.ctx, 17, b.tab)) continue;
-                                        int first = (int)b.mq.decode(b.ctx, 18, b.tab) << 1;
-                                        first |= (int)b.mq.decode(b.ctx, 18, b.tab);
-                                        b.becomeSig(x, y0 + first, p);
-                                        r = first + 1;
+                        }
+                    } else {  // cleanup, with run-length coding of quiet columns
+                        uint32_t cm = 0, any = s_sig[y0], vis = 0;
+                        for (int k = 0; k < n; ++k) {
+                            const uint32_t M = s_sig[y0 + k + 1], V = s_vis[y0 + k];
+                            cm |= ~M & ~V;
+                            any |= M;
+                            vis |= V;
+                        }
+                        any |= s_sig[y0 + n + 1];
+                        cm &= wmask;
+                        while (cm) {
+                            const int x = __ffs(cm) - 1;
+                            cm &= cm - 1;
+                            int r = 0;
+                            // quiet column: nothing significant in rows y0-1..y0+4 around it and
+                            // nothing coded in this plane in it
+                            if (n == 4 && !win3(any, x) && !bt(vis, x)) {
+                                if (!b.mq.decode(s_ctx, 17, s_tab)) continue;
+                                int first = (int)b.mq.decode(s_ctx, 18, s_tab) << 1;
+                                first |= (int)b.mq.decode(s_ctx, 18, s_tab);
+                                uint32_t M = s_sig[y0 + first + 1];
+                                b.becomeSig(s_sig[y0 + first], M, s_sig[y0 + first + 2], x, y0 + first, p);
+                                any |= 1u << x;
+                                r = first + 1;
+                            }
+                            uint32_t U = s_sig[y0 + r], M = s_sig[y0 + r + 1];
+                            for (int k = r; k < n; ++k) {
+                                const int y = y0 + k;
+                                const uint32_t D = s_sig[y + 2];
+                                if (!bt(M | s_vis[y], x)) {
+                                    const uint32_t bit = b.mq.decode(s_ctx, b.zk[nbKey(U, M, D, x)], s_tab);
+                                    if (bit) {
+                                        b.becomeSig(U, M, D, x, y, p);
+                                        any |= 1u << x;
                                     }
                                 }
-                                for (int k = r; k < n; ++k) {
-                                    const int y = y0 + k;
-                                    if (bt(b.S(y) | b.vis[y * DEC_STRIDE], x)) continue;
-                                    if (b.mq.decode(b.ctx, b.zcAt(x, y), b.tab)) b.becomeSig(x, y, p);
-                                }
+                                U = M;
+                                M = D;
                             }
                         }
                     }
                 }
-                for (int i = 0; i < 32; ++i) b.vis[i * DEC_STRIDE] = 0;
             }
-            // dequantise in place, the significant samples only (every other word is 0,
-            // which is 0.0f): word * step / 2, sign from bit 31
-            const float half = a.half[blk.band];
-            float* f = reinterpret_cast<float*>(out);
-            for (int y = 0; y < h; ++y)
-                for (uint32_t m = b.S(y) & wmask; m; m &= m - 1) {
-                    const int x = __ffs(m) - 1;
-                    const uint32_t v = out[(size_t)y * a.W + x];
-                    const float mag = (float)(v & 0x7FFFFFFFu) * half;
-                    f[(size_t)y * a.W + x] = (v & 0x80000000u) ? -mag : mag;
-                }
+            for (int i = 0; i < 32; ++i) s_vis[i] = 0;
         }
+        // dequantise in place, the significant samples only (every other word is 0,
+        // which is 0.0f): word * step / 2, sign from bit 31
+        const float half = a.half[blk.band];
+        float* f = reinterpret_cast<float*>(out);
+        for (int y = 0; y < h; ++y)
+            for (uint32_t m = s_sig[y + 1] & wmask; m; m &= m - 1) {
+                const int x = __ffs(m) - 1;
+                const uint32_t v = out[(size_t)y * a.W + x];
+                const float mag = (float)(v & 0x7FFFFFFFu) * half;
+                f[(size_t)y * a.W + x] = (v & 0x80000000u) ? -mag : mag;
+            }
     }
 }
 
