@@ -87,10 +87,14 @@ GB_API int gb_color_tables(const GailCudaColor* color, float* eotf65536, float* 
  *   soloDecisions  MQ coding: blocks with at least this many decisions are coded alone in
  *                  a warp first (rounded down to a power of two; default 16384)
  *   cmCtasPerSm, mqCtasPerSm, decCtasPerSm  grid caps in CTAs per SM of context modelling,
- *                  MQ coding and Tier-1 decoding (defaults 16, 16, 32; 1..64) */
+ *                  MQ coding and Tier-1 decoding (defaults 16, 16, 32; 1..64)
+ *   t1Persistent   1: Tier-1 encoding as one persistent launch whose warps take context
+ *                  modelling, the order, MQ coding and truncation lengths from device
+ *                  queues in turn; 0 (default): four launches. Same results either way. */
 typedef struct GbTuning {
     uint32_t soloDecisions;
     int32_t cmCtasPerSm, mqCtasPerSm, decCtasPerSm;
+    int32_t t1Persistent;
 } GbTuning;
 GB_API int gb_set_tuning(int profile, const GbTuning* t);
 GB_API int gb_get_tuning(int profile, GbTuning* t);

@@ -1,6 +1,7 @@
 """The project's autotuner: per frame profile (2K, 4K) on this GPU, the launch knobs whose
 best value depends on the workload and the device -- the MQ solo threshold, the grid caps of
-context modelling, MQ coding and Tier-1 decoding -- and the engine's batch policy, chosen by
+context modelling, MQ coding and Tier-1 decoding, Tier-1 as one persistent launch or four --
+and the engine's batch policy, chosen by
 timing candidates on seeded synthetic frames. Every candidate gives bit-identical output
 (the knobs change launch shapes and work order, never the arithmetic), so only speed is
 compared. The result is a JSON file keyed by the GPU's name; apply() loads it into the
@@ -19,14 +20,14 @@ import numpy as np
 
 from . import check, lib
 
-DEFAULTS = {"soloDecisions": 16384, "cmCtasPerSm": 16, "mqCtasPerSm": 16, "decCtasPerSm": 32}
+DEFAULTS = {"soloDecisions": 16384, "cmCtasPerSm": 16, "mqCtasPerSm": 16, "decCtasPerSm": 32, "t1Persistent": 0}
 POLICY_DEFAULT = {"maxBatch": 16, "minBatchPct": 25, "maxWaitMs": 2.0}
 PROFILES = {"2k": 0, "4k": 1}
 
 
 class GbTuning(C.Structure):
     _fields_ = [("soloDecisions", C.c_uint32), ("cmCtasPerSm", C.c_int32), ("mqCtasPerSm", C.c_int32),
-                ("decCtasPerSm", C.c_int32)]
+                ("decCtasPerSm", C.c_int32), ("t1Persistent", C.c_int32)]
 
 
 def _bind():
@@ -39,12 +40,13 @@ def _bind():
 
 
 def set_tuning(profile: int, t: dict | None):
-    """Stores a profile's knobs in the library (None restores the defaults)."""
+    """Stores a profile's knobs in the library (None restores the defaults; a knob left out
+    takes its default)."""
     L = _bind()
     if t is None:
         check(L.gb_set_tuning(profile, None))
     else:
-        v = GbTuning(**{k: int(t[k]) for k in DEFAULTS})
+        v = GbTuning(**{k: int(t.get(k, DEFAULTS[k])) for k in DEFAULTS})
         check(L.gb_set_tuning(profile, C.byref(v)))
 
 
@@ -165,7 +167,7 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
             solo = {"soloDecisions": [4096, 8192, 32768, 1 << 30]}
             cfg, _, seen1 = coordinate_search(cfg, solo, _best_of(tier1_ms, runs), log=log)
             log(f"[{name}] grid caps (served ms per frame)")
-            caps = {"cmCtasPerSm": [8, 12, 24], "mqCtasPerSm": [8, 12, 24]}
+            caps = {"cmCtasPerSm": [8, 12, 24], "mqCtasPerSm": [8, 12, 24], "t1Persistent": [1]}
             cfg, _, seen2 = coordinate_search(cfg, caps, _best_of(served_ms, runs), log=log)
             # the decoder's cap on this profile's own codestreams
             streams = []

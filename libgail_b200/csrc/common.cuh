@@ -21,6 +21,7 @@ enum : uint32_t {
     kErrSymbolSpace = 2u,     // a block's symbol region was too small (cannot happen for valid input)
     kErrCodewordSpace = 4u,   // a codeword outgrew its region
     kErrDecodeInput = 8u,     // a decode descriptor pointed outside its buffers
+    kErrQueueWait = 16u,      // a persistent launch's wait for other warps' work gave up
 };
 
 struct CudaError : std::runtime_error {

@@ -36,7 +36,7 @@ BandOut bandOut(const GbSubband& b) {
 uint64_t SlotSizes::deviceBytes() const {
     const uint64_t sizes[] = {inBytes,     65536 * 4,   4096 * 4,    2 * llFloats * 4 * 3, n * kCblkArea * 4,
                               n * 48,      arena,       arena,       n * 16,               n * kMaxPasses * 4 * 3,
-                              n * kMaxPasses * 16,      n * 4,       64,                   n * 20,
+                              n * kMaxPasses * 16,      n * 4,       t1WorkWords((uint32_t)n) * 4, 64, n * 20,
                               n * 8,                    n * kMaxPasses * 8,       arena};
     uint64_t t = 0;
     for (uint64_t b : sizes) t += page(b);
@@ -154,6 +154,7 @@ EncoderSlot::EncoderSlot(int device, const Layout& L, const GailCudaEncodeSettin
         alloc(dDist_, n * kMaxPasses * 4);
         alloc(dSnaps_, n * kMaxPasses * 16);
         alloc(dPerm_, n * 4);
+        alloc(dWork_, t1WorkWords((uint32_t)n) * 4);
         alloc(dCtl_, 64);
         alloc(dSlope_, 16);
         alloc(dOutInfo_, n * 20);
@@ -256,6 +257,8 @@ void EncoderSlot::enqueueStages(const void* dFrame, bool taps, bool full) {
     t.soloDecisions = tu.soloDecisions;
     t.cmCtasPerSm = (uint16_t)tu.cmCtasPerSm;
     t.mqCtasPerSm = (uint16_t)tu.mqCtasPerSm;
+    t.persistent = (uint16_t)tu.t1Persistent;
+    t.work = dWork_;
     t1Encode(t, st, mark ? mark + 2 : nullptr);
     GB_CHECK(cudaEventRecord(ev_[3], st));
     if (mark) GB_CHECK(cudaEventRecord(mark[4], st));

@@ -95,7 +95,7 @@ private:
     void* dIn_ = nullptr;
     float *dEotf_ = nullptr, *dThr_ = nullptr, *dLL_[2] = {nullptr, nullptr}, *dSlope_ = nullptr, *dTap_ = nullptr;
     uint32_t *dCoeffs_ = nullptr, *dInfo_ = nullptr, *dEnd_ = nullptr, *dLen_ = nullptr, *dPerm_ = nullptr,
-             *dCtl_ = nullptr, *dOutInfo_ = nullptr, *dOutLen_ = nullptr;
+             *dCtl_ = nullptr, *dOutInfo_ = nullptr, *dOutLen_ = nullptr, *dWork_ = nullptr;
     int32_t *dDist_ = nullptr, *dOutDist_ = nullptr;
     uint4* dSnaps_ = nullptr;
     uint2* dOffsets_ = nullptr;

@@ -116,7 +116,8 @@ struct EncodeEngine::Batch {
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     T1Job* dJobs = nullptr;
-    uint32_t *info = nullptr, *end = nullptr, *len = nullptr, *perm = nullptr, *ctl = nullptr, *hCtl = nullptr;
+    uint32_t *info = nullptr, *end = nullptr, *len = nullptr, *perm = nullptr, *ctl = nullptr, *hCtl = nullptr,
+             *work = nullptr;
     int32_t* dist = nullptr;
     uint4* snaps = nullptr;
     uint2* offs = nullptr;
@@ -762,6 +763,7 @@ bool EncodeEngine::launchBatch(Batch& b) {
         alloc(b.dist, cap * kMaxPasses * 4);
         alloc(b.snaps, cap * kMaxPasses * 16);
         alloc(b.perm, cap * 4);
+        alloc(b.work, t1WorkWords((uint32_t)cap) * 4);
         alloc(b.offs, cap * 8);
         alloc(b.hullPasses, cap * kMaxPasses);
         alloc(b.hullSlope, cap * kMaxPasses * 8);
@@ -784,8 +786,11 @@ bool EncodeEngine::launchBatch(Batch& b) {
     L.soloDecisions = tu.soloDecisions;
     L.cmCtasPerSm = (uint16_t)tu.cmCtasPerSm;
     L.mqCtasPerSm = (uint16_t)tu.mqCtasPerSm;
+    L.persistent = (uint16_t)tu.t1Persistent;
+    L.work = b.work;
     t1Encode(L, b.st);
-    uint64_t launches = 4;  // context modelling, ordering, MQ coding, truncation lengths
+    // context modelling, ordering, MQ coding, truncation lengths: four launches or one
+    uint64_t launches = tu.t1Persistent ? 1 : 4;
     bool onDevice, tier1;
     {
         std::lock_guard<std::mutex> lock(m_);

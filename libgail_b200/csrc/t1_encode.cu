@@ -104,17 +104,12 @@ __device__ __forceinline__ uint32_t shDown(uint32_t v, int lane) {
     return lane == 31 ? 0u : t;
 }
 
-__global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
-    __shared__ uint32_t s_mag[CM_WARPS][32][32];
-    __shared__ __align__(16) uint8_t s_stage[CM_WARPS][STAGE];
-    // the contexts as tables of a sample's neighbour bits. Zero coding, per orientation, by
-    // bits 0-2: left column rows r-1..r+1, 3-5: right column rows r-1..r+1, 6: row above,
-    // 7: row below. Sign coding, the whole decision byte (context << 1 | coded bit), by
-    // bits 0-2: own signs rows r-1..r+1, 3: left significant, 4: its sign, 5: right
-    // significant, 6: its sign, 7: row above significant, 8: row below significant.
-    __shared__ uint8_t s_zk[4 * 256];
-    __shared__ uint8_t s_sk[512];
-    __shared__ uint32_t s_hist[CM_WARPS][19];
+// The contexts as tables of a sample's neighbour bits. Zero coding, per orientation, by
+// bits 0-2: left column rows r-1..r+1, 3-5: right column rows r-1..r+1, 6: row above,
+// 7: row below. Sign coding, the whole decision byte (context << 1 | coded bit), by
+// bits 0-2: own signs rows r-1..r+1, 3: left significant, 4: its sign, 5: right
+// significant, 6: its sign, 7: row above significant, 8: row below significant.
+__device__ __forceinline__ void cmTables(uint8_t* s_zk, uint8_t* s_sk) {
     for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
         const int o = i >> 8, k = i & 255;
         const int h = ((k >> 1) & 1) + ((k >> 4) & 1);
@@ -128,14 +123,16 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
         const uint32_t t = c_sc[(hc + 1) * 3 + (vc + 1)];
         s_sk[k] = (uint8_t)(((t & 31u) << 1) | (((uint32_t)k >> 1 & 1u) ^ (t >> 5)));
     }
-    __syncthreads();
+}
 
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t (*mag)[32] = s_mag[wid];
-    uint8_t* buf = s_stage[wid];
+// Context modelling of block `job` by one warp: its decisions to its symbol region, its
+// pass table and info words. mag: the warp's 32 x 32 magnitudes, buf: its plane staging,
+// hist: its 19 context counters (zero between blocks). Returns the block's decisions
+// (the same on every lane).
+__device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint32_t (*mag)[32], uint8_t* buf,
+                                          uint32_t* hist, const uint8_t* s_zk, const uint8_t* s_sk, int lane) {
     uint32_t* status = P.ctl + 1;
-
-    for (uint32_t job = blockIdx.x * CM_WARPS + wid; job < P.n; job += gridDim.x * CM_WARPS) {
+    {
         const T1Job J = P.jobs[job];
         const int w = (J.geom & 31u) + 1, h = ((J.geom >> 5) & 31u) + 1, orient = (J.geom >> 10) & 3u;
         const int maxPasses = (J.geom >> 12) & 127u;
@@ -166,9 +163,9 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                 if (nbps) atomicOr(status, kErrTooManyPlanes);
             }
             __syncwarp();
-            continue;
+            return 0u;
         }
-        if (lane < 19) s_hist[wid][lane] = 0;
+        if (lane < 19) hist[lane] = 0;
         __syncwarp();
 
         const uint32_t valid = lane < w ? (h >= 32 ? kFull : ((1u << h) - 1u)) : 0u;
@@ -370,13 +367,13 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                 // with every float operation in the CPU's order
                 for (uint32_t i = lane; i < count; i += 32) {
                     const uint32_t s = buf[i];
-                    atomicAdd(&s_hist[wid][s >> 1], (s & 1u) ? 0x10000u : 1u);
+                    atomicAdd(&hist[s >> 1], (s & 1u) ? 0x10000u : 1u);
                 }
                 __syncwarp();
                 if (lane == 0) {
                     float bits = 0.f;
                     for (int cx = 0; cx < 19; ++cx) {
-                        const uint32_t hv = s_hist[wid][cx];
+                        const uint32_t hv = hist[cx];
                         const float n0 = (float)(hv & 0xFFFFu), n1 = (float)(hv >> 16), n = __fadd_rn(n0, n1);
                         if (n > 0.f) {
                             const float l0 = log2f(__fdiv_rn(fmaxf(n0, 0.5f), n));
@@ -407,7 +404,7 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
                     }
                 }
                 __syncwarp();
-                if (lane < 19) s_hist[wid][lane] = 0;
+                if (lane < 19) hist[lane] = 0;
                 stop = __shfl_sync(kFull, stop, 0);
             }
             symTotal += count;
@@ -422,7 +419,21 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
             atomicAdd(P.ctl + 2, symTotal);
         }
         __syncwarp();
+        return symTotal;
     }
+}
+
+__global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
+    __shared__ uint32_t s_mag[CM_WARPS][32][32];
+    __shared__ __align__(16) uint8_t s_stage[CM_WARPS][STAGE];
+    __shared__ uint8_t s_zk[4 * 256];
+    __shared__ uint8_t s_sk[512];
+    __shared__ uint32_t s_hist[CM_WARPS][19];
+    cmTables(s_zk, s_sk);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (uint32_t job = blockIdx.x * CM_WARPS + wid; job < P.n; job += gridDim.x * CM_WARPS)
+        cmJob(P, job, s_mag[wid], s_stage[wid], s_hist[wid], s_zk, s_sk, lane);
 }
 
 // ---------------------------------------------------------------------------- ordering
@@ -550,8 +561,38 @@ struct Coder {
     }
 };
 
+// Control words of a persistent launch (T1Launch::work, zeroed before it), then the
+// order's bucket counters (offsets once scanned), then the list of blocks whose MQ coding
+// is done, in the order they finished (block + 1; 0 = not yet written).
+enum : uint32_t {
+    kWCmHead = 0,      // next block to model
+    kWCmDone = 1,      // blocks modelled
+    kWSolo = 2,        // blocks of soloDecisions decisions or more
+    kWUnused = 3,
+    kWScanDone = 4,
+    kWScatHead = 5,    // next chunk of the order's scatter
+    kWScatDone = 6,
+    kWSoloHead = 7,    // next solo block to claim
+    kWTruncTail = 8,   // entries in the list
+    kWTruncHead = 9,   // next entry to take for truncation lengths
+    kWHist = 16,
+    kWList = 16 + ORDER_BUCKETS,
+};
+static_assert(kWList == kT1WorkHead, "work layout");
+
+// Loads of what other warps of a persistent launch wrote during the launch, into lines an
+// SM may have read before (the info words, MQ states and codewords that truncation reads)
+// go around L1, which SMs do not keep coherent with one another; the separate kernels load
+// normally.
+template <bool PERS, class T>
+__device__ __forceinline__ T ldx(const T* p) {
+    if constexpr (PERS) return __ldcg(p);
+    else return *p;
+}
+
 // Shortest prefix >= minLen that a decoder reading 1-bits past the end decodes exactly
 // up to the snapshot, never ending on 0xFF. Same arithmetic as the oracle's mq_trunc.
+template <bool PERS>
 __device__ uint32_t truncLen(uint4 s, const uint8_t* buf, uint32_t len, uint32_t minLen) {
     const int bp = (int)s.x;
     const uint32_t C = s.y, A = s.z & 0xFFFFu, B = s.w;
@@ -562,7 +603,7 @@ __device__ uint32_t truncLen(uint4 s, const uint8_t* buf, uint32_t len, uint32_t
     unsigned long long acc = 0;
     int used = 0;
     for (int i = bp; i < (int)len; ++i) {
-        const uint32_t byte = i >= 0 ? buf[i] : 0u;
+        const uint32_t byte = i >= 0 ? ldx<PERS>(buf + i) : 0u;
         const int sh = base - used;
         if (sh < 0) break;
         acc += (unsigned long long)byte << sh;
@@ -574,14 +615,7 @@ __device__ uint32_t truncLen(uint4 s, const uint8_t* buf, uint32_t len, uint32_t
     return len;
 }
 
-// MINB: CTAs per SM the registers must allow. A launch of a frame or two has fewer lanes
-// than the GPU holds and runs uncapped; wide batched launches run at 10 CTAs per SM (the
-// registers that allows need no spill; measured faster on B200 than 12 with a spill).
-template <int MINB>
-__global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
-    __shared__ uint2 s_next[2 * 47];  // by (state, MPS): next state after an MPS renormalisation, after an LPS
-    __shared__ uint32_t s_init[4];
-    __shared__ uint32_t s_ctx[19 * MQ_THREADS];
+__device__ __forceinline__ void mqTables(uint2* s_next, uint32_t* s_init) {
     for (int i = threadIdx.x; i < 2 * 47; i += blockDim.x)
         s_next[i] = make_uint2(nextStateEntry(2 * i), nextStateEntry(2 * i + 1));
     if (threadIdx.x == 0) {
@@ -590,12 +624,17 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
         s_init[2] = initialState(3);
         s_init[3] = initialState(46);
     }
-    __syncthreads();
-    uint32_t* ctx = s_ctx + threadIdx.x;
+}
+
+// MQ coding, a lane per block, until the queue is empty. ctx: the lane's 19 context states,
+// CS words apart. warpId: the warp's place among the solo warps of a separate MQ launch.
+// PERS (a persistent launch): the solo blocks go to the first warps to get here, and each
+// block, coded or empty, is listed for its truncation lengths when it is done.
+template <int CS, bool PERS>
+__device__ __forceinline__ void mqRun(const T1Launch& P, uint32_t* ctx, const uint2* s_next, const uint32_t* s_init,
+                                      uint32_t warpId) {
     uint32_t* status = P.ctl + 1;
     const int lane = threadIdx.x & 31;
-    const uint32_t solo = P.ctl[3];  // blocks coded alone, perm[0 .. solo)
-    const uint32_t warpId = blockIdx.x * (MQ_THREADS / 32) + (threadIdx.x >> 5);
 
     // Per-lane state of the block in hand. Invariant between decisions: s is the decision
     // at pos and t the state of its context; nxt holds the decisions from pos on.
@@ -607,13 +646,21 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
     e.cap = 0;
     bool have = false;
 
+    auto listed = [&](uint32_t j) {
+        if constexpr (PERS) {
+            __threadfence();  // the block's results before its list entry
+            const uint32_t slot = atomicAdd(P.work + kWTruncTail, 1u);
+            atomicExch(P.work + kWList + slot, j + 1);
+        }
+    };
     // starts block j; false when it has no coding pass (nothing to code)
     auto begin = [&](uint32_t j) {
         job = j;
-        np = P.info[4 * (size_t)job + 1];
-        nsym = P.info[4 * (size_t)job + 2];
+        np = ldx<false>(P.info + 4 * (size_t)job + 1);
+        nsym = ldx<false>(P.info + 4 * (size_t)job + 2);
         if (np == 0) {
             P.info[4 * (size_t)job + 3] = 0;
+            listed(job);
             return false;
         }
         const T1Job J = P.jobs[job];
@@ -628,28 +675,39 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
         e.overflow = false;
         // initial states, Table D.7: ZC context 0 state 4, run-length 3, uniform 46
 #pragma unroll
-        for (int c = 0; c < 19; ++c) ctx[c * MQ_THREADS] = s_init[0];
+        for (int c = 0; c < 19; ++c) ctx[c * CS] = s_init[0];
         ctx[0] = s_init[1];
-        ctx[17 * MQ_THREADS] = s_init[2];
-        ctx[18 * MQ_THREADS] = s_init[3];
+        ctx[17 * CS] = s_init[2];
+        ctx[18 * CS] = s_init[3];
         pos = 0;
         k = 0;
-        nextEnd = P.passEnd[(size_t)job * kMaxPasses];
-        laterEnd = np > 1 ? P.passEnd[(size_t)job * kMaxPasses + 1] : 0xFFFFFFFFu;
+        nextEnd = ldx<false>(P.passEnd + (size_t)job * kMaxPasses);
+        laterEnd = np > 1 ? ldx<false>(P.passEnd + (size_t)job * kMaxPasses + 1) : 0xFFFFFFFFu;
         stop = min(nsym, nextEnd);
-        nxt = nsym ? *reinterpret_cast<const uint4*>(sym) : make_uint4(0, 0, 0, 0);
+        nxt = nsym ? ldx<false>(reinterpret_cast<const uint4*>(sym)) : make_uint4(0, 0, 0, 0);
         s = nxt.x & 0xFFu;
-        t = ctx[(s >> 1) * MQ_THREADS];
+        t = ctx[(s >> 1) * CS];
         have = true;
         return true;
     };
 
-    // A warp below `solo` first codes block perm[warpId] on its lane 0 while the other
+    // A solo warp first codes its solo block (perm[0 .. solo)) on its lane 0 while the other
     // lanes wait; then all its lanes take blocks from the shared queue, one at a time.
-    bool soloPhase = warpId < solo;
+    const uint32_t solo = ldx<false>(P.ctl + 3);
+    uint32_t mine = warpId;
+    if constexpr (PERS) {
+        if (lane == 0) mine = atomicAdd(P.work + kWSoloHead, 1u);
+        mine = __shfl_sync(kFull, mine, 0);
+    }
+    bool soloPhase = mine < solo;
     bool soloJob = false;
-    if (soloPhase && lane == 0) soloJob = begin(P.perm[warpId]);
+    if (soloPhase && lane == 0) soloJob = begin(ldx<false>(P.perm + mine));
 
+    // A lane leaves only at the loop's top, after the solo phase's shuffle: a solo warp's
+    // lane 0 whose queue is empty when its solo block ends still tells the other lanes,
+    // which wait in that shuffle (otherwise they would pair it with the next shuffle lane 0
+    // makes, wherever that is).
+    bool finished = false;
     for (;;) {
         if (soloPhase) {  // warp-uniform; every lane of the warp is still in the loop
             if (__shfl_sync(kFull, (int)soloJob, 0)) {
@@ -658,6 +716,7 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
                 soloPhase = false;
             }
         }
+        if (finished) break;
         if (!have || pos >= nsym) {
             if (have) {
                 // end of block: remaining pass ends, flush, truncation points
@@ -668,8 +727,9 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
                 }
                 const uint32_t len = e.flush();
                 if (e.overflow) atomicOr(status, kErrCodewordSpace);
-                // the truncation lengths are found afterwards, by t1TruncKernel
+                // the truncation lengths are found afterwards, a warp per block
                 P.info[4 * (size_t)job + 3] = e.overflow ? 0u : len;
+                listed(job);
                 have = false;
                 soloJob = false;
             }
@@ -678,19 +738,19 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
             for (;;) {
                 const uint32_t qi = solo + atomicAdd(P.ctl, 1u);
                 if (qi >= P.n) break;
-                if (begin(P.perm[qi])) {
+                if (begin(ldx<false>(P.perm + qi))) {
                     got = true;
                     break;
                 }
             }
-            if (!got) break;
+            finished = !got;
             continue;  // a block without decisions finishes at once
         }
         // one aligned chunk of 16 decisions (fewer at the block's end): a word of four
         // decisions unrolled at a time, the next decision's context state read ahead, off
         // the serial chain of the coder
         const uint4 v = nxt;
-        nxt = (pos + 16 < nsym) ? *reinterpret_cast<const uint4*>(sym + pos + 16) : make_uint4(0, 0, 0, 0);
+        nxt = (pos + 16 < nsym) ? ldx<false>(reinterpret_cast<const uint4*>(sym + pos + 16)) : make_uint4(0, 0, 0, 0);
         uint32_t w0 = v.x, w1 = v.y, w2 = v.z, w3 = v.w;
         const uint32_t w4 = nxt.x;
         // one decision: s (context and bit) in state t; sn the next decision
@@ -698,9 +758,9 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
             // the byte past the block's last decision is not a decision: the clamp keeps its
             // look-ahead read inside the lane's 19 contexts
             const uint32_t cn = min(sn >> 1, 18u), cx = s >> 1;
-            const uint32_t tn = ctx[cn * MQ_THREADS];
+            const uint32_t tn = ctx[cn * CS];
             const uint32_t tNew = e.encode(t, s & 1u, s_next);
-            ctx[cx * MQ_THREADS] = tNew;
+            ctx[cx * CS] = tNew;
             t = cn == cx ? tNew : tn;
             s = sn;
             ++pos;
@@ -721,7 +781,7 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
                             make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
                         ++k;
                         nextEnd = laterEnd;  // loaded a pass ago: no wait here
-                        laterEnd = k + 1 < np ? P.passEnd[(size_t)job * kMaxPasses + k + 1] : 0xFFFFFFFFu;
+                        laterEnd = k + 1 < np ? ldx<false>(P.passEnd + (size_t)job * kMaxPasses + k + 1) : 0xFFFFFFFFu;
                     }
                     stop = min(nsym, nextEnd);
                 }
@@ -735,38 +795,202 @@ __global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
     }
 }
 
-// Truncation lengths, a warp per block after MQ coding: lane q finds the shortest prefix
-// for pass q from the MQ state recorded at its end, as if no earlier pass constrained it;
-// lane 0 then walks the passes in order and, where a pass's shortest prefix is shorter
-// than an earlier pass's length, searches again from that length (the lengths of a
-// block never decrease). The last pass takes the whole codeword.
+// MINB: CTAs per SM the registers must allow. A launch of a frame or two has fewer lanes
+// than the GPU holds and runs uncapped; wide batched launches run at 10 CTAs per SM (the
+// registers that allows need no spill; measured faster on B200 than 12 with a spill).
+template <int MINB>
+__global__ void __launch_bounds__(MQ_THREADS, MINB) t1MqKernel(T1Launch P) {
+    __shared__ uint2 s_next[2 * 47];  // by (state, MPS): next state after an MPS renormalisation, after an LPS
+    __shared__ uint32_t s_init[4];
+    __shared__ uint32_t s_ctx[19 * MQ_THREADS];
+    mqTables(s_next, s_init);
+    __syncthreads();
+    mqRun<MQ_THREADS, false>(P, s_ctx + threadIdx.x, s_next, s_init,
+                             blockIdx.x * (MQ_THREADS / 32) + (threadIdx.x >> 5));
+}
+
+// Truncation lengths of one block by one warp: lane q finds the shortest prefix for pass q
+// from the MQ state recorded at its end, as if no earlier pass constrained it; lane 0 then
+// walks the passes in order and, where a pass's shortest prefix is shorter than an earlier
+// pass's length, searches again from that length (the lengths of a block never decrease).
+// The last pass takes the whole codeword.
+template <bool PERS>
+__device__ __forceinline__ void truncJob(const T1Launch& P, uint32_t job, int lane) {
+    const uint32_t np = ldx<PERS>(P.info + 4 * (size_t)job + 1), len = ldx<PERS>(P.info + 4 * (size_t)job + 3);
+    if (np == 0 || len == 0) return;  // nothing coded, or an overflow already reported
+    const uint8_t* cw = P.jobs[job].cw;
+    const size_t base = (size_t)job * kMaxPasses;
+    uint32_t c0 = 0, c1 = 0;  // the unconstrained lengths of passes lane and lane + 32
+    if ((uint32_t)lane + 1 < np) c0 = truncLen<PERS>(ldx<PERS>(P.snaps + base + lane), cw, len, 1);
+    if ((uint32_t)lane + 33 < np) c1 = truncLen<PERS>(ldx<PERS>(P.snaps + base + lane + 32), cw, len, 1);
+    uint32_t prev = 1, mine0 = 0, mine1 = 0;
+    for (uint32_t q = 0; q < np; ++q) {
+        const uint32_t c = __shfl_sync(kFull, q < 32 ? c0 : c1, q & 31);
+        uint32_t L = len;
+        if (q + 1 < np) {
+            L = c;
+            if (L < prev && lane == 0) L = truncLen<PERS>(ldx<PERS>(P.snaps + base + q), cw, len, prev);
+            L = __shfl_sync(kFull, L, 0);
+        }
+        if ((q & 31) == (uint32_t)lane) (q < 32 ? mine0 : mine1) = L;
+        prev = max(prev, L);
+    }
+    if ((uint32_t)lane < np) P.passLen[base + lane] = mine0;
+    if ((uint32_t)lane + 32 < np) P.passLen[base + lane + 32] = mine1;
+}
+
+// Kept out of the MQ kernel, whose lanes would otherwise stall on these byte reads one
+// block end at a time while their warp-mates code.
 constexpr int TRUNC_THREADS = 256;
 
 __global__ void __launch_bounds__(TRUNC_THREADS) t1TruncKernel(T1Launch P) {
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (TRUNC_THREADS / 32);
-    for (uint32_t job = blockIdx.x * (TRUNC_THREADS / 32) + (threadIdx.x >> 5); job < P.n; job += warps) {
-        const uint32_t np = P.info[4 * (size_t)job + 1], len = P.info[4 * (size_t)job + 3];
-        if (np == 0 || len == 0) continue;  // nothing coded, or an overflow already reported
-        const uint8_t* cw = P.jobs[job].cw;
-        const size_t base = (size_t)job * kMaxPasses;
-        uint32_t c0 = 0, c1 = 0;  // the unconstrained lengths of passes lane and lane + 32
-        if ((uint32_t)lane + 1 < np) c0 = truncLen(P.snaps[base + lane], cw, len, 1);
-        if ((uint32_t)lane + 33 < np) c1 = truncLen(P.snaps[base + lane + 32], cw, len, 1);
-        uint32_t prev = 1, mine0 = 0, mine1 = 0;
-        for (uint32_t q = 0; q < np; ++q) {
-            const uint32_t c = __shfl_sync(kFull, q < 32 ? c0 : c1, q & 31);
-            uint32_t L = len;
-            if (q + 1 < np) {
-                L = c;
-                if (L < prev && lane == 0) L = truncLen(P.snaps[base + q], cw, len, prev);
-                L = __shfl_sync(kFull, L, 0);
-            }
-            if ((q & 31) == (uint32_t)lane) (q < 32 ? mine0 : mine1) = L;
-            prev = max(prev, L);
+    for (uint32_t job = blockIdx.x * (TRUNC_THREADS / 32) + (threadIdx.x >> 5); job < P.n; job += warps)
+        truncJob<false>(P, job, lane);
+}
+
+// ---------------------------------------------------------------------------- one launch
+__device__ __forceinline__ uint32_t ldAcquire(const uint32_t* p) {
+    uint32_t x;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(x) : "l"(p) : "memory");
+    return x;
+}
+
+__device__ __forceinline__ uint32_t ldRelaxed(const uint32_t* p) {
+    uint32_t x;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(x) : "l"(p) : "memory");
+    return x;
+}
+
+// Waits until *p >= v (polling with relaxed loads, backing off from 0.25 to 8 us so that
+// thousands of waiting warps leave L2 to the working ones; the caller acquires once it
+// holds); gives up after 2 s with kErrQueueWait set, so that a launch whose other warps
+// stopped returns.
+__device__ bool waitFor(const uint32_t* p, uint32_t v, uint32_t* status) {
+    uint64_t t0, t1;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    uint32_t nap = 256;
+    for (uint32_t it = 0; it < (1u << 26); ++it) {
+        if (ldRelaxed(p) >= v) return true;
+        __nanosleep(nap);
+        nap = min(nap * 2, 8192u);
+        if ((it & 63u) == 63u) {
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+            if (t1 - t0 > 2000000000ull) break;
         }
-        if ((uint32_t)lane < np) P.passLen[base + lane] = mine0;
-        if ((uint32_t)lane + 32 < np) P.passLen[base + lane + 32] = mine1;
+    }
+    atomicOr(status, kErrQueueWait);
+    return false;
+}
+
+// Lane 0 waits until *p >= v, then every lane makes its own acquire load of *p: a lane that
+// only hears of the value from lane 0 is not ordered after the writes made before it was
+// set, and on B200 such a lane's loads were seen to return older data. Returns *p as
+// every lane read it, 0 when the wait gave up (warp-uniform).
+__device__ __forceinline__ uint32_t warpWaitFor(const uint32_t* p, uint32_t v, uint32_t* status, int lane) {
+    const bool ok = lane == 0 ? waitFor(p, v, status) : true;
+    if (!__shfl_sync(kFull, ok, 0)) return 0u;
+    return ldAcquire(p);
+}
+
+constexpr uint32_t SCAT_CHUNK = 256;  // blocks per claim of the order's scatter
+
+// The whole Tier-1 stage in one launch, every warp through the same phases, each fed by a
+// device queue: (1) context modelling, a block per claim; (2) the order (counting sort by
+// decision count, most first: the warp that models the last block scans the bucket
+// counters the modelling filled, every warp scatters chunks of blocks); (3) MQ coding, a
+// lane per block, the heaviest blocks alone in the first warps to arrive; (4) truncation
+// lengths, a warp per block in the order the blocks finished MQ coding, by every warp done
+// with MQ coding. A warp waits only for work that a running warp has claimed (it reaches
+// the wait after the queue it drew from ran dry), so the launch cannot deadlock whatever
+// its grid and whatever runs beside it; every wait is bounded all the same. A lane reads
+// what other warps wrote only after its own acquire load of the word that announced it.
+// Each warp's context-modelling memory holds its lanes' MQ contexts afterwards.
+__global__ void __launch_bounds__(CM_THREADS, 7) t1PersistentKernel(T1Launch P, uint32_t maxSolo) {
+    struct WarpCm {
+        uint32_t mag[32][32];
+        uint8_t stage[STAGE];
+    };
+    union WarpMem {
+        WarpCm cm;
+        uint32_t ctx[19 * 32];
+    };
+    __shared__ __align__(16) WarpMem s_w[CM_WARPS];
+    __shared__ uint8_t s_zk[4 * 256];
+    __shared__ uint8_t s_sk[512];
+    __shared__ uint32_t s_hist[CM_WARPS][19];
+    __shared__ uint2 s_next[2 * 47];
+    __shared__ uint32_t s_init[4];
+    cmTables(s_zk, s_sk);
+    mqTables(s_next, s_init);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t* work = P.work;
+    uint32_t* status = P.ctl + 1;
+
+    // (1) context modelling
+    for (;;) {
+        uint32_t job = 0;
+        if (lane == 0) job = atomicAdd(work + kWCmHead, 1u);
+        job = __shfl_sync(kFull, job, 0);
+        if (job >= P.n) break;
+        const uint32_t nsym = cmJob(P, job, s_w[wid].cm.mag, s_w[wid].cm.stage, s_hist[wid], s_zk, s_sk, lane);
+        if (lane == 0) {
+            atomicAdd(work + kWHist + orderBucket(nsym), 1u);
+            if (nsym >= P.soloDecisions) atomicAdd(work + kWSolo, 1u);
+        }
+        __threadfence();  // the block's decisions and tables before it counts as done
+        __syncwarp();
+        uint32_t done = 0;
+        if (lane == 0) done = atomicAdd(work + kWCmDone, 1u);
+        // (2) the order: bucket offsets by the warp that modelled the last block
+        if (__shfl_sync(kFull, done, 0) != P.n - 1) continue;
+        ldAcquire(work + kWCmDone);
+        uint32_t v[4], sum = 0;
+        for (int q = 0; q < 4; ++q) {
+            v[q] = __ldcg(work + kWHist + 4 * lane + q);
+            sum += v[q];
+        }
+        uint32_t run = warpScan(sum, lane) - sum;
+        for (int q = 0; q < 4; ++q) {
+            work[kWHist + 4 * lane + q] = run;
+            run += v[q];
+        }
+        if (lane == 0) P.ctl[3] = min(__ldcg(work + kWSolo), maxSolo);
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) atomicExch(work + kWScanDone, 1u);
+    }
+    if (!warpWaitFor(work + kWScanDone, 1u, status, lane)) return;
+    const uint32_t chunks = divUp(P.n, SCAT_CHUNK);
+    for (;;) {
+        uint32_t c = 0;
+        if (lane == 0) c = atomicAdd(work + kWScatHead, 1u);
+        c = __shfl_sync(kFull, c, 0);
+        if (c >= chunks) break;
+        const uint32_t end = min(P.n, (c + 1) * SCAT_CHUNK);
+        for (uint32_t i = c * SCAT_CHUNK + lane; i < end; i += 32)
+            P.perm[atomicAdd(work + kWHist + orderBucket(__ldcg(P.info + 4 * (size_t)i + 2)), 1u)] = i;
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) atomicAdd(work + kWScatDone, 1u);
+    }
+    if (!warpWaitFor(work + kWScatDone, chunks, status, lane)) return;
+    // (3) MQ coding, the lanes' contexts in the warp's modelling memory
+    __syncwarp();
+    mqRun<32, true>(P, s_w[wid].ctx + lane, s_next, s_init, 0);
+    __syncwarp();
+    // (4) truncation lengths, the list's entries in turn (an entry not yet written belongs
+    // to a block whose MQ coding a running lane holds)
+    for (;;) {
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(work + kWTruncHead, 1u);
+        i = __shfl_sync(kFull, i, 0);
+        if (i >= P.n) break;
+        const uint32_t j = warpWaitFor(work + kWList + i, 1u, status, lane);
+        if (j == 0) return;
+        truncJob<true>(P, j - 1, lane);
     }
 }
 
@@ -796,6 +1020,23 @@ void t1Encode(const T1Launch& launch, cudaStream_t st, cudaEvent_t* marks) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (L.persistent && L.work) {
+        // one CTA per resident slot (the kernel is correct with any grid; more would only wait)
+        static int occ = 0;
+        if (!occ) {
+            GB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, t1PersistentKernel, CM_THREADS, 0));
+            occ = max(occ, 1);
+        }
+        const uint32_t grid = min(divUp(L.n, CM_WARPS), (uint32_t)(sms * occ));
+        GB_CHECK(cudaMemsetAsync(L.work, 0, t1WorkWords(L.n) * 4, st));
+        t1PersistentKernel<<<grid, CM_THREADS, 0, st>>>(L, grid * CM_WARPS / 2);
+        GB_CHECK(cudaGetLastError());
+        if (marks) {
+            GB_CHECK(cudaEventRecord(marks[0], st));
+            GB_CHECK(cudaEventRecord(marks[1], st));
+        }
+        return;
+    }
     const uint32_t cmBlocks = min(divUp(L.n, CM_WARPS), (uint32_t)sms * L.cmCtasPerSm);
     t1CmKernel<<<cmBlocks, CM_THREADS, 0, st>>>(L);
     if (marks) GB_CHECK(cudaEventRecord(marks[0], st));

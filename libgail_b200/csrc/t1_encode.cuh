@@ -50,11 +50,22 @@ struct T1Launch {
     // MQ-coded alone in a warp (a power of two); grids of at most so many CTAs per SM
     uint32_t soloDecisions;
     uint16_t cmCtasPerSm, mqCtasPerSm;
+    // one persistent launch instead of four (when work is given): work holds
+    // t1WorkWords(n) words of its queues, zeroed by t1Encode
+    uint16_t persistent;
+    uint32_t* work;
 };
 
-// Enqueues the whole Tier-1 stage on st: context modelling, ordering, MQ coding.
+// Words of a persistent launch's work area: control words and the order's buckets, then
+// one list entry per block.
+constexpr uint32_t kT1WorkHead = 16 + 128;
+inline size_t t1WorkWords(uint32_t n) { return kT1WorkHead + (size_t)n; }
+
+// Enqueues the whole Tier-1 stage on st: context modelling, ordering, MQ coding and
+// truncation lengths, as four launches or (persistent and work set) as one.
 // ctl must be zeroed by the caller (it is part of the launch so that graphs can hold it).
-// marks (optional): two events recorded after context modelling and after ordering.
+// marks (optional): two events recorded after context modelling and after ordering (both
+// after the launch when it is one).
 void t1Encode(const T1Launch& L, cudaStream_t st, cudaEvent_t* marks = nullptr);
 
 // Uploads the context tables (once per device, before the first launch).

@@ -24,6 +24,7 @@ void setTuning(int profile, const Tuning& t) {
     if (t.cmCtasPerSm < 1 || t.cmCtasPerSm > 64 || t.mqCtasPerSm < 1 || t.mqCtasPerSm > 64 || t.decCtasPerSm < 1 ||
         t.decCtasPerSm > 64)
         throw std::logic_error("grid caps must be 1..64 CTAs per SM");
+    if (t.t1Persistent != 0 && t.t1Persistent != 1) throw std::logic_error("t1Persistent must be 0 or 1");
     Tuning v = t;
     uint32_t p = 1;
     while (p * 2 <= v.soloDecisions && p < (1u << 30)) p *= 2;

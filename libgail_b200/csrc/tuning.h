@@ -11,6 +11,7 @@ struct Tuning {
     int cmCtasPerSm = 16;            // context modelling grid cap
     int mqCtasPerSm = 16;            // MQ grid cap
     int decCtasPerSm = 32;           // Tier-1 decode grid cap
+    int t1Persistent = 0;            // Tier-1 encode as one persistent launch (1) or four (0)
 };
 
 Tuning defaultTuning();
