@@ -57,12 +57,14 @@ WORKLOAD = ("4K 3996x2160 Y'CbCr 4:2:2 10-bit BT.2020 PQ -> 12-bit X'Y'Z', 9/7 6
 
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on one 4K
-# frame, and Tier-1 issue figures, from the ncu capture summarised in the file below
+# frame, and Tier-1 issue figures, from the ncu captures summarised in the files below
+# (encode kernels; decodeKernel's in the second)
 NCU_SOURCE = "profiles/kernels_4k_encode_frame.md"
+NCU_DECODE_SOURCE = "profiles/kernels_4k_decode_frame.md"
 ET_FACTOR = 0.25  # the Tier-1 early-termination factor gail.h's encoder forces
 NCU_TRAFFIC = {"t1CmKernel": 214.53e6, "t1MqKernel": 180.17e6}
 NCU_TIER1 = {"cm_issue_active_pct": 72.2, "cm_warps_per_sm": 23.1, "mq_issue_active_pct": 30.8, "mq_warps_per_sm": 4.7,
-             "decode_issue_active_pct": 23.4, "decode_warps_per_sm": 4.4}
+             "decode_issue_active_pct": 72.5, "decode_warps_per_sm": 26.0}
 
 
 def parse():
@@ -533,7 +535,7 @@ def run_ours(args):
                  "mq_decisions_per_s": dec / (stage[3] * 1e-3),
                  "code_blocks_per_s_per_sm_plain": ncblk / ((stage[1] + stage[3]) * 1e-3) / sms,
                  "code_blocks_per_s_per_sm_served": ncblk * value / sms,
-                 "ncu": NCU_TIER1}
+                 "ncu": dict(NCU_TIER1, sources=[NCU_SOURCE, NCU_DECODE_SOURCE])}
         pct = lambda a, q: float(np.percentile(a, q))  # noqa: E731
         dci = {"fps": FPS, "budget_bytes": budget,
                "served": {"frames": len(served_cs), "valid": sum(1 for _, ok in served_cs if ok == 1),
