@@ -884,10 +884,10 @@ __device__ bool waitFor(const uint32_t* p, uint32_t v, uint32_t* status) {
     return false;
 }
 
-// Lane 0 waits until *p >= v, then every lane makes its own acquire load of *p: a lane that
-// only hears of the value from lane 0 is not ordered after the writes made before it was
-// set, and on B200 such a lane's loads were seen to return older data. Returns *p as
-// every lane read it, 0 when the wait gave up (warp-uniform).
+// Lane 0 waits until *p >= v, then every lane makes its own acquire load of *p: the memory
+// model orders later loads after the writes that preceded the release only for the thread
+// that performs the acquire, not for lanes that hear of the value from lane 0 by shuffle.
+// Returns *p as every lane read it, 0 when the wait gave up (warp-uniform).
 __device__ __forceinline__ uint32_t warpWaitFor(const uint32_t* p, uint32_t v, uint32_t* status, int lane) {
     const bool ok = lane == 0 ? waitFor(p, v, status) : true;
     if (!__shfl_sync(kFull, ok, 0)) return 0u;
