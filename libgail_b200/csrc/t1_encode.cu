@@ -1022,11 +1022,11 @@ void t1Encode(const T1Launch& launch, cudaStream_t st, cudaEvent_t* marks) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (L.persistent && L.work) {
         // one CTA per resident slot (the kernel is correct with any grid; more would only wait)
-        static int occ = 0;
-        if (!occ) {
-            GB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, t1PersistentKernel, CM_THREADS, 0));
-            occ = max(occ, 1);
-        }
+        static const int occ = [] {
+            int o = 0;
+            GB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, t1PersistentKernel, CM_THREADS, 0));
+            return max(o, 1);
+        }();
         const uint32_t grid = min(divUp(L.n, CM_WARPS), (uint32_t)(sms * occ));
         GB_CHECK(cudaMemsetAsync(L.work, 0, t1WorkWords(L.n) * 4, st));
         t1PersistentKernel<<<grid, CM_THREADS, 0, st>>>(L, grid * CM_WARPS / 2);
