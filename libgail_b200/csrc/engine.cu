@@ -438,11 +438,52 @@ int EncodeEngine::addDecodeClass(const GailCudaLayout& layout, const GailCudaDec
     c->s = s;
     c->slotBytes = decoderSlotBytes(c->L, s);
     if (frameBytes) *frameBytes = c->slotBytes;
+    int cls, workers;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        decClasses_.push_back(std::move(c));
+        startWorkers(4);
+        if (csOn_ && cs_.onDevice) prepareRc();
+        cls = (int)decClasses_.size() - 1;
+        workers = (int)csWorkers_.size();
+    }
+    // two slots per host worker now (one decoding, one holding a picture not yet released),
+    // while the HBM budget has room: making one while serving (device memory, pinned host
+    // memory) stalls its worker and the device
+    for (int i = 0; i < 2 * workers; ++i) {
+        DecSlot* ds = newDecSlot(cls);
+        if (!ds) break;
+        std::lock_guard<std::mutex> lock(m_);
+        decClasses_[cls]->free.push_back(ds);
+    }
+    return cls;
+}
+
+// A new decoder slot of decode class cls, or NULL when the HBM budget has no room.
+EncodeEngine::DecSlot* EncodeEngine::newDecSlot(int cls) {
+    DecClass* c;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        c = decClasses_[cls].get();
+    }
+    {
+        std::lock_guard<std::mutex> lock(budgetM_);
+        if (used_ + c->slotBytes > budget_) return nullptr;
+        used_ += c->slotBytes;
+    }
+    auto d = std::make_unique<DecSlot>();
+    d->cls = cls;
+    try {
+        d->slot = std::make_unique<DecoderSlot>(dev_, c->L, c->s);
+    } catch (...) {
+        std::lock_guard<std::mutex> lock(budgetM_);
+        used_ -= c->slotBytes;
+        throw;
+    }
+    DecSlot* ds = d.get();
     std::lock_guard<std::mutex> lock(m_);
-    decClasses_.push_back(std::move(c));
-    startWorkers(4);
-    if (csOn_ && cs_.onDevice) prepareRc();
-    return (int)decClasses_.size() - 1;
+    decSlots_.push_back(std::move(d));
+    return ds;
 }
 
 int64_t EncodeEngine::submitDecode(int cls, const uint8_t* data, uint64_t size) {
@@ -507,27 +548,8 @@ void EncodeEngine::decodeJob(Request* r) {
                     break;
                 }
             }
-            bool room;
-            {
-                std::lock_guard<std::mutex> lock(budgetM_);
-                room = used_ + c->slotBytes <= budget_;
-                if (room) used_ += c->slotBytes;
-            }
-            if (room) {
-                auto d = std::make_unique<DecSlot>();
-                d->cls = r->cls;
-                try {
-                    d->slot = std::make_unique<DecoderSlot>(dev_, c->L, c->s);
-                } catch (...) {
-                    std::lock_guard<std::mutex> lock(budgetM_);
-                    used_ -= c->slotBytes;
-                    throw;
-                }
-                ds = d.get();
-                std::lock_guard<std::mutex> lock(m_);
-                decSlots_.push_back(std::move(d));
-                break;
-            }
+            ds = newDecSlot(r->cls);
+            if (ds) break;
             std::unique_lock<std::mutex> lock(m_);  // no room: the next released slot
             cvDecSlot_.wait_for(lock, std::chrono::milliseconds(50), [&] { return !c->free.empty() || stop_.load(); });
             if (stop_) throw std::runtime_error("engine stopping");

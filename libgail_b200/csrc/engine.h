@@ -127,6 +127,7 @@ private:
     bool launchBatch(Batch& b);
     bool collect(Batch& b);
     Slot* newSlot(Class& c);
+    DecSlot* newDecSlot(int cls);
 
     int dev_;
     uint64_t budget_ = 0, used_ = 0;  // used_ under budgetM_
