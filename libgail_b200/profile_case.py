@@ -1,13 +1,14 @@
 """Small, fixed encode cases for profiler captures.
 
-  python -m libgail_b200.profile_case --path plain --frames 2
+  python -m libgail_b200.profile_case --path plain --frames 2 [--persistent]
   python -m libgail_b200.profile_case --path served --frames 8 --batch 8 [--size 2k] [--repeat 3] [--codestreams]
   python -m libgail_b200.profile_case --path decode --frames 2
 
 Encodes seeded synthetic frames that are already in device memory, through the plain
 per-frame encoder or the batched engine, and prints the stage times of the plain path, or
 decodes the frames' DCI codestreams (made and parsed by the host codec) through the
-plugin's decoder:
+plugin's decoder; --persistent runs Tier-1 encoding as one persistent launch (the
+t1Persistent tuning knob) instead of four:
 4K (3996x2160 Y'CbCr 4:2:2 10-bit, BT.2020 PQ, as the benchmark uses) or 2K (1998x1080
 X'Y'Z' 12-bit, whose small frame slots keep a batched case to a few GB of device memory).
 Exits non-zero on any encoder error, so that a profiler run after it sees the same
@@ -32,6 +33,7 @@ def main():
     ap.add_argument("--repeat", type=int, default=1, help="served: passes over the frames (the first warms up)")
     ap.add_argument("--codestreams", action="store_true",
                     help="served: DCI codestreams too (rate control and Tier-2 on the device)")
+    ap.add_argument("--persistent", action="store_true", help="Tier-1 encoding as one persistent launch")
     args = ap.parse_args()
 
     import torch
@@ -54,6 +56,9 @@ def main():
         col = P.color_passthrough()
     dframes = [torch.from_numpy(f.view(np.int16)).to("cuda:0") for f in frames]
     torch.cuda.synchronize()
+    if args.persistent:
+        from libgail_b200 import autotune as AT
+        AT.set_tuning(1 if args.size == "4k" else 0, {"t1Persistent": 1})
     dev = P.Plugin().device(0)
     try:
         if args.path == "plain":
