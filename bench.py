@@ -62,8 +62,8 @@ WORKLOAD = ("4K 3996x2160 Y'CbCr 4:2:2 10-bit BT.2020 PQ -> 12-bit X'Y'Z', 9/7 6
 NCU_SOURCE = "profiles/kernels_4k_encode_frame.md"
 NCU_DECODE_SOURCE = "profiles/kernels_4k_decode_frame.md"
 ET_FACTOR = 0.25  # the Tier-1 early-termination factor gail.h's encoder forces
-NCU_TRAFFIC = {"t1CmKernel": 214.53e6, "t1MqKernel": 180.17e6}
-NCU_TIER1 = {"cm_issue_active_pct": 72.2, "cm_warps_per_sm": 23.1, "mq_issue_active_pct": 30.8, "mq_warps_per_sm": 4.7,
+NCU_TRAFFIC = {"t1CmKernel": 214.29e6, "t1MqKernel": 182.01e6}
+NCU_TIER1 = {"cm_issue_active_pct": 71.1, "cm_warps_per_sm": 23.1, "mq_issue_active_pct": 27.1, "mq_warps_per_sm": 4.6,
              "decode_issue_active_pct": 72.5, "decode_warps_per_sm": 26.0}
 
 
