@@ -33,6 +33,7 @@
 
 #include "common.cuh"
 #include "decoder.h"
+#include "pool.h"
 #include "t1_tables.h"
 #include "tuning.h"
 
@@ -606,13 +607,20 @@ void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, 
                          void* dst, ptrdiff_t strideBytes, GailCudaDecodeTimings* tm) {
     enqueue(frame, data, size, blocks, numBlocks, tm && tm->wantWavelet);
     const uint16_t* pic = finish(tm);
+    // the picture from the pinned buffer into the caller's rows, in bands on the host pool
+    // and the calling thread (52 MB at 4K: one thread's copy took longer than the decode)
     const uint64_t rowBytes = (uint64_t)outW_ * 6;
-    if (strideBytes == (ptrdiff_t)rowBytes) {
-        std::memcpy(dst, pic, rowBytes * outH_);
-    } else {
-        for (int y = 0; y < outH_; ++y)
-            std::memcpy((uint8_t*)dst + (ptrdiff_t)y * strideBytes, (const uint8_t*)pic + (uint64_t)y * rowBytes, rowBytes);
-    }
+    constexpr int kBands = 8;
+    parallelFor(kBands, [&](int k) {
+        const int y0 = (int)((int64_t)outH_ * k / kBands), y1 = (int)((int64_t)outH_ * (k + 1) / kBands);
+        const uint8_t* src = (const uint8_t*)pic + (uint64_t)y0 * rowBytes;
+        uint8_t* out = (uint8_t*)dst + (ptrdiff_t)y0 * strideBytes;
+        if (strideBytes == (ptrdiff_t)rowBytes) {
+            std::memcpy(out, src, rowBytes * (uint64_t)(y1 - y0));
+        } else {
+            for (int y = y0; y < y1; ++y, src += rowBytes, out += strideBytes) std::memcpy(out, src, rowBytes);
+        }
+    });
     if (tm) tm->total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
 }
 
