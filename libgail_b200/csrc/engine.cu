@@ -451,7 +451,12 @@ int EncodeEngine::addDecodeClass(const GailCudaLayout& layout, const GailCudaDec
     // while the HBM budget has room: making one while serving (device memory, pinned host
     // memory) stalls its worker and the device
     for (int i = 0; i < 2 * workers; ++i) {
-        DecSlot* ds = newDecSlot(cls);
+        DecSlot* ds = nullptr;
+        try {
+            ds = newDecSlot(cls);
+        } catch (const std::exception&) {  // out of memory now: slots are made on demand
+            cudaGetLastError();
+        }
         if (!ds) break;
         std::lock_guard<std::mutex> lock(m_);
         decClasses_[cls]->free.push_back(ds);

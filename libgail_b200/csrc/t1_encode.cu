@@ -568,13 +568,12 @@ enum : uint32_t {
     kWCmHead = 0,      // next block to model
     kWCmDone = 1,      // blocks modelled
     kWSolo = 2,        // blocks of soloDecisions decisions or more
-    kWUnused = 3,
-    kWScanDone = 4,
-    kWScatHead = 5,    // next chunk of the order's scatter
-    kWScatDone = 6,
-    kWSoloHead = 7,    // next solo block to claim
-    kWTruncTail = 8,   // entries in the list
-    kWTruncHead = 9,   // next entry to take for truncation lengths
+    kWScanDone = 3,    // the order's bucket offsets are ready
+    kWScatHead = 4,    // next chunk of the order's scatter
+    kWScatDone = 5,
+    kWSoloHead = 6,    // next solo block to claim
+    kWTruncTail = 7,   // entries in the list
+    kWTruncHead = 8,   // next entry to take for truncation lengths
     kWHist = 16,
     kWList = 16 + ORDER_BUCKETS,
 };
