@@ -64,7 +64,12 @@ GB_API int gb_t1_encode_blocks(const uint32_t* coeffs, const int32_t* geom4, uin
  *     kernels' tables there; make that first call before any stream capture;
  *   - calls share the array: two calls whose work overlaps on the GPU (other threads,
  *     other streams) race and corrupt each other's results, so serialise them;
- *   - the call waits for its work (it synchronises the device) before it returns. */
+ *   - the work runs on a non-blocking stream the library makes for the device at the
+ *     first call, and the call waits for that stream alone before it returns;
+ *   - each codeword is copied into its row of data exactly (info4[4i+3] bytes); the row's
+ *     bytes after it are left untouched;
+ *   - cudaDeviceReset on a device after the first call there is not supported (the array's
+ *     address and the stream are kept for the life of the process). */
 GB_API int gb_t1_encode_blocks_noalloc(const uint32_t* coeffs, const int32_t* geom4, uint32_t n, float slope,
                                        const float* distScale, uint32_t* info4, uint32_t* passLen, int32_t* passDist,
                                        uint8_t* data, uint32_t dataStride);

@@ -19,9 +19,14 @@
 // before it is read. Two calls whose device work overlaps (from different host threads,
 // or on different streams) race on the array and corrupt each other's results: callers
 // must serialise their calls.
+//
+// The work runs on a non-blocking stream that the library makes once per device, together
+// with the array's address, and the call waits on that stream alone: other streams' work
+// on the device is neither waited for nor held up. The address and the stream are kept
+// for the life of the process, so cudaDeviceReset on a device after the first call there
+// is not supported (the kept address and stream would belong to the destroyed context).
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
@@ -56,18 +61,24 @@ constexpr size_t kNoAllocBytes = kOffCw + (size_t)kNoAllocMaxBlocks * kRegion;
 
 static __device__ __align__(256) unsigned char g_scratch[kNoAllocBytes];
 
-// The array's device address, looked up once per device (in host code the name
-// g_scratch is only a stand-in for the symbol, not an address a kernel may use).
+// Per device: the array's device address (in host code the name g_scratch is only a
+// stand-in for the symbol, not an address a kernel may use) and the stream the calls run
+// on, both made by the first call on that device.
 constexpr int kMaxDevices = 64;
+struct DeviceScratch {
+    unsigned char* address = nullptr;
+    cudaStream_t stream = nullptr;
+};
 std::mutex g_mutex;
-unsigned char* g_address[kMaxDevices] = {};
+DeviceScratch g_device[kMaxDevices];
 
-unsigned char* scratchAddress() {
+DeviceScratch scratchForCurrentDevice() {
     int dev = 0;
     GB_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) throw std::runtime_error("device index out of range");
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_address[dev]) {
+    DeviceScratch& d = g_device[dev];
+    if (!d.address) {
         ensureDevice();
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
@@ -76,9 +87,12 @@ unsigned char* scratchAddress() {
             throw std::runtime_error(std::string("no device address for the Tier-1 scratch array: ") +
                                      cudaGetErrorString(e));
         }
-        g_address[dev] = static_cast<unsigned char*>(p);
+        cudaStream_t st = nullptr;
+        GB_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        d.stream = st;
+        d.address = static_cast<unsigned char*>(p);
     }
-    return g_address[dev];
+    return d;
 }
 
 }  // namespace
@@ -96,7 +110,9 @@ extern "C" GB_API int gb_t1_encode_blocks_noalloc(const uint32_t* coeffs, const 
             throw std::logic_error("gb_t1_encode_blocks_noalloc takes at most " + std::to_string(kNoAllocMaxBlocks) +
                                    " code-blocks per call (" + std::to_string(n) + " given)");
         if (n == 0) return;
-        unsigned char* base = scratchAddress();
+        const DeviceScratch dev = scratchForCurrentDevice();
+        unsigned char* base = dev.address;
+        const cudaStream_t st = dev.stream;
         T1Job jobs[kNoAllocMaxBlocks];
         for (uint32_t i = 0; i < n; ++i) {
             const int w = geom4[4 * i], h = geom4[4 * i + 1], orient = geom4[4 * i + 2], mp = geom4[4 * i + 3];
@@ -122,22 +138,27 @@ extern "C" GB_API int gb_t1_encode_blocks_noalloc(const uint32_t* coeffs, const 
                    reinterpret_cast<uint32_t*>(base + kOffCtl),
                    reinterpret_cast<const float*>(base + kOffSlope)};
         // inputs in, the previous call's control words cleared
-        GB_CHECK(cudaMemcpy(base + kOffCoeffs, coeffs, (size_t)n * kCblkArea * 4, cudaMemcpyHostToDevice));
-        GB_CHECK(cudaMemcpy(base + kOffJobs, jobs, n * sizeof(T1Job), cudaMemcpyHostToDevice));
-        GB_CHECK(cudaMemcpy(base + kOffSlope, &slope, 4, cudaMemcpyHostToDevice));
-        GB_CHECK(cudaMemset(base + kOffCtl, 0, 64));
-        t1Encode(L, 0);
-        GB_CHECK(cudaDeviceSynchronize());
+        GB_CHECK(cudaMemcpyAsync(base + kOffCoeffs, coeffs, (size_t)n * kCblkArea * 4, cudaMemcpyHostToDevice, st));
+        GB_CHECK(cudaMemcpyAsync(base + kOffJobs, jobs, n * sizeof(T1Job), cudaMemcpyHostToDevice, st));
+        GB_CHECK(cudaMemcpyAsync(base + kOffSlope, &slope, 4, cudaMemcpyHostToDevice, st));
+        GB_CHECK(cudaMemsetAsync(base + kOffCtl, 0, 64, st));
+        t1Encode(L, st);
         uint32_t ctl[4];
-        GB_CHECK(cudaMemcpy(ctl, base + kOffCtl, 16, cudaMemcpyDeviceToHost));
+        GB_CHECK(cudaMemcpyAsync(ctl, base + kOffCtl, 16, cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaStreamSynchronize(st));
         if (ctl[1]) throw std::runtime_error("Tier-1 encoder status " + std::to_string(ctl[1]));
-        GB_CHECK(cudaMemcpy(info4, base + kOffInfo, 16 * (size_t)n, cudaMemcpyDeviceToHost));
-        GB_CHECK(cudaMemcpy(passLen, base + kOffLen, (size_t)n * kMaxPasses * 4, cudaMemcpyDeviceToHost));
-        GB_CHECK(cudaMemcpy(passDist, base + kOffDist, (size_t)n * kMaxPasses * 4, cudaMemcpyDeviceToHost));
+        GB_CHECK(cudaMemcpyAsync(info4, base + kOffInfo, 16 * (size_t)n, cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaMemcpyAsync(passLen, base + kOffLen, (size_t)n * kMaxPasses * 4, cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaMemcpyAsync(passDist, base + kOffDist, (size_t)n * kMaxPasses * 4, cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaStreamSynchronize(st));
         for (uint32_t i = 0; i < n; ++i)
             if (info4[4 * i + 3] > dataStride) throw std::logic_error("dataStride too small for a codeword");
-        // codewords: the arena's block regions to the caller's rows of dataStride bytes
-        GB_CHECK(cudaMemcpy2D(data, dataStride, base + kOffCw, kRegion, std::min<size_t>(dataStride, kRegion), n,
-                              cudaMemcpyDeviceToHost));
+        // each codeword, exactly its length, into the caller's row; the row's bytes after
+        // it are left as the caller had them
+        for (uint32_t i = 0; i < n; ++i)
+            if (const uint32_t len = info4[4 * i + 3])
+                GB_CHECK(cudaMemcpyAsync(data + (size_t)i * dataStride, base + kOffCw + (size_t)i * kRegion, len,
+                                         cudaMemcpyDeviceToHost, st));
+        GB_CHECK(cudaStreamSynchronize(st));
     });
 }

@@ -14,17 +14,22 @@ import libgail_b200 as gb
 MAX_BLOCKS = 64
 
 
-def _call(fn, coeffs, geom, slope=0.0, dscale=None, stride=65536):
+SENTINEL = 0xA5
+
+
+def _call(fn, coeffs, geom, slope=0.0, dscale=None, stride=65536, rows=None):
     n = len(geom)
     info = np.zeros((n, 4), np.uint32)
     plen = np.zeros((n, 64), np.uint32)
     pdist = np.zeros((n, 64), np.int32)
-    data = np.zeros((n, stride), np.uint8)
+    data = np.full((n, stride), SENTINEL, np.uint8)
     c = np.ascontiguousarray(coeffs, np.uint32)
     g = np.ascontiguousarray(geom, np.int32)
     ds = None if dscale is None else np.ascontiguousarray(dscale, np.float32)
     st = fn(c.ctypes.data, g.ctypes.data, n, C.c_float(slope), None if ds is None else ds.ctypes.data, info.ctypes.data,
             plen.ctypes.data, pdist.ctypes.data, data.ctypes.data, stride)
+    if rows is not None:
+        rows.append(data)
     return st, info, plen, pdist, [bytes(data[i, : info[i, 3]]) for i in range(n)]
 
 
@@ -73,3 +78,29 @@ def test_noalloc_refuses_more_than_its_maximum(golden_t1):
     st, *_ = _call(L.gb_t1_encode_blocks_noalloc, coeffs, meta)
     assert st == 4  # GAIL_CUDA_MISUSE
     assert b"at most 64" in gb.lib().gb_last_error()
+
+
+@pytest.mark.gpu
+def test_noalloc_writes_only_each_codeword(golden_t1):
+    """Rows narrower than the array's per-block region (8 KB here, where the region is
+    about 56 KB): each codeword lands in its row exactly, and the bytes after it keep the
+    caller's contents, as gb_t1_encode_blocks leaves them."""
+    L = _lib()
+    coeffs, meta = golden_t1["coeffs"], golden_t1["meta"]
+    sel = slice(2 * MAX_BLOCKS, 3 * MAX_BLOCKS)
+    geom = meta[sel].copy()
+    longest = 0
+    for fn in (L.gb_t1_encode_blocks, L.gb_t1_encode_blocks_noalloc):
+        rows = []
+        st, info, _, _, words = _call(fn, coeffs[sel], geom, stride=8192, rows=rows)
+        assert st == 0, gb.lib().gb_last_error()
+        data = rows[0]
+        for i in range(len(geom)):
+            n = int(info[i, 3])
+            longest = max(longest, n)
+            assert np.all(data[i, n:] == SENTINEL), f"block {i}: bytes after the codeword were overwritten"
+        if fn is L.gb_t1_encode_blocks:
+            want = words
+        else:
+            assert words == want, "codewords differ from the allocating entry point"
+    assert 0 < longest <= 8192
