@@ -34,6 +34,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 #include "t1_encode.cuh"
@@ -1009,6 +1010,22 @@ void t1Init() {
     GB_CHECK(cudaMemcpyToSymbol(c_mq, mq, sizeof mq));
 }
 
+// Resident CTAs per SM of the persistent kernel, queried once per device index (devices
+// of different kinds in one process each get their own figure).
+static int persistentOccupancy(int dev) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mutex;
+    static int occ[kMaxDevices] = {};
+    if (dev < 0 || dev >= kMaxDevices) dev = 0;
+    std::lock_guard<std::mutex> lock(mutex);
+    if (!occ[dev]) {
+        int o = 0;
+        GB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, t1PersistentKernel, CM_THREADS, 0));
+        occ[dev] = max(o, 1);
+    }
+    return occ[dev];
+}
+
 void t1Encode(const T1Launch& launch, cudaStream_t st, cudaEvent_t* marks) {
     if (launch.n == 0) return;
     T1Launch L = launch;
@@ -1021,11 +1038,7 @@ void t1Encode(const T1Launch& launch, cudaStream_t st, cudaEvent_t* marks) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (L.persistent && L.work) {
         // one CTA per resident slot (the kernel is correct with any grid; more would only wait)
-        static const int occ = [] {
-            int o = 0;
-            GB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, t1PersistentKernel, CM_THREADS, 0));
-            return max(o, 1);
-        }();
+        const int occ = persistentOccupancy(dev);
         const uint32_t grid = min(divUp(L.n, CM_WARPS), (uint32_t)(sms * occ));
         GB_CHECK(cudaMemsetAsync(L.work, 0, t1WorkWords(L.n) * 4, st));
         t1PersistentKernel<<<grid, CM_THREADS, 0, st>>>(L, grid * CM_WARPS / 2);
