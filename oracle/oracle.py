@@ -46,9 +46,11 @@ def _p(a, t=C.c_void_p):
 
 
 def build(ref: bool = True) -> None:
-    """Compile liboracle.so (and the reference library when its sources are present)."""
+    """Compile liboracle.so (and the reference library when GAIL_REFERENCE_SRC names the
+    reference source tree)."""
     import subprocess
-    subprocess.run(["make", "-s", "-C", HERE, "all" if ref else "liboracle.so"], check=True)
+    src = os.environ.get("GAIL_REFERENCE_SRC", "")
+    subprocess.run(["make", "-s", "-C", HERE, "all" if ref else "liboracle.so", f"REF={src}"], check=True)
 
 
 class T1Block:
@@ -197,6 +199,8 @@ class Reference(_Common):
         L.ref_quantize.restype = C.c_uint32
         L.ref_quantize.argtypes = [C.c_float, C.c_float, C.c_uint32]
         L.ref_t1_decode.argtypes = [C.c_void_p, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.ref_quantize_frame.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p]
         L.ref_fdwt97_2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
         L.ref_idwt97_2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
         L.ref_layout_counts.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
@@ -220,6 +224,18 @@ class Reference(_Common):
 
     def quantize(self, v, inv_delta, max_mag):
         return self.lib.ref_quantize(C.c_float(v), C.c_float(inv_delta), max_mag)
+
+    def quantize_frame(self, planes: np.ndarray, width, height, fourk, base_step=1.0) -> np.ndarray:
+        """The reference quantiser (quantizeFrame) on three Mallat planes: (numCblks, 1024) words."""
+        p = np.ascontiguousarray(planes, np.float32).reshape(3, height, width)
+        nb, nc = C.c_int(), C.c_int()
+        if self.lib.ref_layout_counts(width, height, int(fourk), C.byref(nb), C.byref(nc)) != 0:
+            raise RuntimeError(self.error())
+        out = np.zeros((nc.value, 1024), np.uint32)
+        if self.lib.ref_quantize_frame(width, height, int(fourk), C.c_double(base_step), _p(p[0]), _p(p[1]), _p(p[2]),
+                                       _p(out)) != 0:
+            raise RuntimeError(self.error())
+        return out
 
     def t1_decode(self, data: bytes, w, h, orient, nbps, passes, length=None) -> np.ndarray:
         out = np.zeros(1024, np.uint32)

@@ -99,6 +99,21 @@ void ref_t1_decode(const uint8_t* data, uint32_t len, int w, int h, int orient, 
     t1DecodeBlock(data, len, w, h, orient, nbps, passes, out);
 }
 
+// The reference quantiser over a whole frame: three Mallat planes -> the code-block-major
+// words of every code-block (quantizeFrame, src/core/quant.cpp:23-26).
+int ref_quantize_frame(int width, int height, int fourk, double baseStep, const float* p0, const float* p1,
+                       const float* p2, uint32_t* out) {
+    try {
+        FrameLayout L = layoutOf(width, height, fourk, baseStep);
+        const float* planes[3] = {p0, p1, p2};
+        quantizeFrame(L, planes, out);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
 // ---- wavelet ------------------------------------------------------------------------
 void ref_fdwt97_2d(float* plane, int width, int height, int levels) { fdwt97_2d(plane, width, height, levels); }
 
