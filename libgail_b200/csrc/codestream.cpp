@@ -988,9 +988,10 @@ RateResult allocateRate(CodestreamWriter& w, const Tier1View& t1, const RateLimi
     return res;
 }
 
-// --------------------------------------------------------------------------- checker
+// --------------------------------------------------------------- big-endian reading
 namespace {
 
+// Reads that set fail, and give 0, once they run past the end.
 struct Bytes {
     const uint8_t* p;
     const uint8_t* end;
@@ -1019,191 +1020,6 @@ std::string hexOf(uint32_t v) {
 }
 
 }  // namespace
-
-DciReport checkDci(const uint8_t* data, size_t size, double fps) {
-    DciReport r;
-    r.totalBytes = size;
-    Bytes in{data, data + size};
-    if (in.u16() != kSOC) {
-        r.error("no SOC at the start");
-        return r;
-    }
-    if (in.u16() != kSIZ) {
-        r.error("SIZ does not follow SOC");
-        return r;
-    }
-    const uint32_t lsiz = in.u16();
-    if (lsiz != 47) r.error("Lsiz " + std::to_string(lsiz) + " (47 for three components)");
-    r.rsiz = (int)in.u16();
-    r.width = (int)in.u32();
-    r.height = (int)in.u32();
-    const uint32_t xo = in.u32(), yo = in.u32(), tw = in.u32(), th = in.u32(), txo = in.u32(), tyo = in.u32();
-    const int comps = (int)in.u16();
-    const bool fourk = r.width > 2048;
-    if (r.rsiz != (fourk ? 4 : 3)) r.error("Rsiz " + std::to_string(r.rsiz) + " is not the profile of the size");
-    if (fourk ? (r.width > 4096 || r.height > 2160) : (r.width > 2048 || r.height > 1080))
-        r.error("size beyond the DCI container");
-    if (xo || yo) r.error("image offset");
-    if (tw != (uint32_t)r.width || th != (uint32_t)r.height) r.error("more than one tile");
-    if (txo || tyo) r.error("tile offset");
-    if (comps != 3) r.error("not three components");
-    for (int c = 0; c < comps && c < 3; ++c) {
-        const uint32_t s = in.u8(), xr = in.u8(), yr = in.u8();
-        if (s != 11) r.error("component " + std::to_string(c) + " is not 12-bit unsigned");
-        if (xr != 1 || yr != 1) r.error("subsampled component");
-    }
-
-    const int nres = fourk ? 7 : 6, ntp = fourk ? 6 : 3;
-    const double frameCap = std::rint(250e6 / (8 * fps)), nearCap = std::rint(230e6 / (8 * fps));
-    const double partCap = std::floor(200e6 / (8 * fps));
-    int cods = 0, qcds = 0, pocsMain = 0, pocsLate = 0, nextTp = 0;
-    bool inMain = true, eoc = false, tlm = false;
-    std::vector<uint32_t> tlmLen, psots;
-
-    // end of a segment whose length (which counts itself) was just read, or null when it
-    // runs past the data (reported; the parse stops)
-    auto segEnd = [&](uint32_t m, size_t at, uint32_t len) -> const uint8_t* {
-        if (len < 2 || (size_t)(in.end - in.p) < (size_t)len - 2) {
-            r.error("marker " + hexOf(m) + " at " + std::to_string(at) + " runs past the end");
-            in.fail = true;
-            return nullptr;
-        }
-        return in.p + len - 2;
-    };
-    while (!in.fail && in.p < in.end) {
-        const size_t at = (size_t)(in.p - data);
-        const uint32_t m = in.u16();
-        if ((m >> 8) != 0xFF) {
-            r.error("no marker at " + std::to_string(at));
-            break;
-        }
-        if (m == kCOD) {
-            ++cods;
-            if (!inMain) r.error("COD in a tile-part header");
-            const uint32_t len = in.u16();
-            const uint8_t* next = segEnd(m, at, len);
-            if (!next) break;
-            const uint32_t scod = in.u8(), prog = in.u8(), layers = in.u16(), mct = in.u8();
-            r.levels = (int)in.u8();
-            const uint32_t xcb = in.u8(), ycb = in.u8(), style = in.u8(), xform = in.u8();
-            if (scod != 1) r.error("Scod " + hexOf(scod) + " (precincts given, no SOP/EPH)");
-            if (prog != 4) r.error("progression is not CPRL");
-            if (layers != 1) r.error("not one quality layer");
-            if (mct != 1) r.error("no component transform");
-            if (r.levels != (fourk ? 6 : 5)) r.error("wrong number of decomposition levels");
-            if (xcb != 3 || ycb != 3) r.error("code-blocks are not 32x32");
-            if (style != 0) r.error("code-block mode switches");
-            if (xform != 0) r.error("not the 9/7 wavelet");
-            if (len != (uint32_t)(12 + nres)) r.error("Lcod");
-            for (int i = 0; i < nres; ++i)
-                if (in.u8() != (i == 0 ? 0x77u : 0x88u)) r.error("precincts other than 128 (lowest resolution) / 256");
-            in.p = next;
-        } else if (m == kQCD) {
-            ++qcds;
-            const uint32_t len = in.u16();
-            const uint8_t* next = segEnd(m, at, len);
-            if (!next) break;
-            const uint32_t sq = in.u8();
-            const int guard = (int)(sq >> 5);
-            if ((sq & 0x1F) != 2) r.error("quantisation not scalar expounded");
-            if (guard != (fourk ? 2 : 1)) r.error("guard bits");
-            const int nb = 3 * (fourk ? 6 : 5) + 1;
-            if (len != (uint32_t)(3 + 2 * nb)) r.error("Lqcd");
-            for (int i = 0; i < nb && in.p + 1 < next; ++i)
-                if (guard + (int)(in.u16() >> 11) - 1 > 30) r.error("band " + std::to_string(i) + " needs over 30 bit-planes");
-            in.p = next;
-        } else if (m == kPOC) {
-            (inMain ? pocsMain : pocsLate)++;
-            const uint32_t len = in.u16();
-            const uint8_t* next = segEnd(m, at, len);
-            if (!next) break;
-            if (len != 16) {
-                r.error("Lpoc");
-            } else {
-                // RSpoc CSpoc LYEpoc REpoc CEpoc Ppoc, twice: 0 0 1 6 3 4 and 6 0 1 7 3 4
-                static const uint32_t want[12] = {0, 0, 1, 6, 3, 4, 6, 0, 1, 7, 3, 4};
-                const uint32_t got[12] = {in.u8(), in.u8(), in.u16(), in.u8(), in.u8(), in.u8(),
-                                          in.u8(), in.u8(), in.u16(), in.u8(), in.u8(), in.u8()};
-                for (int i = 0; i < 12; ++i)
-                    if (got[i] != want[i]) r.error("POC is not the DCI 4K progression");
-            }
-            in.p = next;
-        } else if (m == kTLM) {
-            tlm = true;
-            const uint32_t len = in.u16();
-            const uint8_t* next = segEnd(m, at, len);
-            if (!next) break;
-            in.u8();
-            const uint32_t st = in.u8();
-            const int tBytes = (st >> 4) & 3, pBytes = ((st >> 6) & 1) ? 4 : 2;
-            const int each = (tBytes == 3 ? 0 : tBytes) + pBytes;
-            for (int i = 0, k = (int)(len - 4) / each; i < k; ++i) {
-                for (int b = 0; b < (tBytes == 3 ? 0 : tBytes); ++b) in.u8();
-                tlmLen.push_back(pBytes == 4 ? in.u32() : in.u16());
-            }
-            in.p = next;
-        } else if (m == kCOC || m == kQCC || m == kCOM) {
-            const uint32_t len = in.u16();
-            const uint8_t* next = segEnd(m, at, len);
-            if (!next) break;
-            if (m == kCOM && len >= 4 && inMain && in.p[0] == 0 && in.p[1] == 1) r.comment.assign((const char*)in.p + 2, len - 4);
-            if (m == kCOC) r.warnings.push_back("COC marker");
-            in.p = next;
-        } else if (m == kSOT) {
-            inMain = false;
-            const uint8_t* sot = in.p - 2;
-            const uint32_t lsot = in.u16(), isot = in.u16(), psot = in.u32(), tpsot = in.u8(), tnsot = in.u8();
-            if (lsot != 10) r.error("Lsot");
-            if (isot != 0) r.error("tile index");
-            if ((int)tnsot != ntp) r.error("TNsot " + std::to_string(tnsot) + " (" + std::to_string(ntp) + ")");
-            if ((int)tpsot != nextTp) r.error("tile-parts out of order");
-            ++nextTp;
-            psots.push_back(psot);
-            if (psot > partCap) r.error("tile-part " + std::to_string(tpsot) + " of " + std::to_string(psot) + " bytes over the 200 Mbit/s cap");
-            r.compBytes[tpsot % 3] += psot;
-            if (psot < 14 || (size_t)psot > (size_t)(in.end - sot)) {
-                r.error("Psot");
-                in.fail = true;
-                break;
-            }
-            if (in.u16() != kSOD) r.error("SOT not followed by SOD");
-            for (const uint8_t* q = in.p; q + 1 < sot + psot; ++q)  // no marker code in the packets
-                if (q[0] == 0xFF && q[1] >= 0x90) {
-                    r.error("marker code 0xFF" + hexOf(q[1]).substr(2) + " in packet data at " + std::to_string(q - data));
-                    break;
-                }
-            in.p = sot + psot;
-        } else if (m == kEOC) {
-            eoc = true;
-            if (in.p != in.end) r.error("data after EOC");
-            in.p = in.end;
-        } else {
-            r.error("marker " + hexOf(m) + " not allowed in a DCI codestream");
-            in.fail = true;
-        }
-    }
-    r.tileParts = nextTp;
-    if (in.fail) r.error("truncated or malformed");
-    if (!eoc) r.error("no EOC");
-    if (cods != 1) r.error("not exactly one COD");
-    if (qcds != 1) r.error("not exactly one QCD");
-    if (fourk && pocsMain != 1) r.error("4K needs one POC in the main header");
-    if (!fourk && pocsMain != 0) r.error("POC in a 2K codestream");
-    if (pocsLate) r.error("POC outside the main header");
-    if (!tlm) r.error("no TLM");
-    if (nextTp != ntp) r.error(std::to_string(nextTp) + " tile-parts (" + std::to_string(ntp) + ")");
-    if (tlm) {
-        if (tlmLen.size() != psots.size()) r.error("TLM entries do not match the tile-parts");
-        else
-            for (size_t i = 0; i < tlmLen.size(); ++i)
-                if (tlmLen[i] != psots[i]) r.error("TLM length of tile-part " + std::to_string(i));
-    }
-    for (int c = 0; c < 3; ++c)
-        if (r.compBytes[c] > partCap) r.error("component " + std::to_string(c) + " over the 200 Mbit/s cap");
-    if ((double)size > frameCap) r.error("frame of " + std::to_string(size) + " bytes over the 250 Mbit/s cap");
-    else if ((double)size > nearCap) r.warnings.push_back("frame above 230 Mbit/s");
-    return r;
-}
 
 // ---------------------------------------------------------------------------- reading
 void parseCodestream(const uint8_t* data, size_t size, Layout& L, std::vector<GbCblkCode>& blocks) {

@@ -165,6 +165,39 @@ def _damaged(cs: bytes):
     r = bytearray(b)
     r[2:4] = b"\xff\x52"  # SIZ missing
     out["no_siz"] = bytes(r)
+    r = bytearray(b)
+    r[5] ^= 2  # Lsiz
+    out["lsiz"] = bytes(r)
+    r = bytearray(b)
+    r[42] = 7  # Ssiz of component 0: 8-bit
+    out["ssiz"] = bytes(r)
+    r = bytearray(b)
+    r[44] = 2  # YRsiz of component 0: subsampled
+    out["subsampled"] = bytes(r)
+    qcd = b.find(b"\xff\x5c")
+    r = bytearray(b)
+    r[qcd + 4] ^= 0x20  # guard bits
+    out["guard"] = bytes(r)
+    r = bytearray(b)
+    r[cod + 14] = 0x66  # precincts of the lowest resolution
+    out["precinct"] = bytes(r)
+    r = bytearray(b)
+    r[sot + 11] ^= 1  # TNsot
+    out["tnsot"] = bytes(r)
+    r = bytearray(b)
+    r[sot + 6] = 0xFF  # Psot past the data
+    out["psot"] = bytes(r)
+    r = bytearray(b)
+    r[cod + 1] = 0x60  # COD becomes a marker DCI does not allow (PPM)
+    out["ppm"] = bytes(r)
+    poc = b.find(b"\xff\x5f", 0, sot)  # in the main header (4K only)
+    if poc > 0:
+        r = bytearray(b)
+        r[poc + 7] = 5  # POC: resolutions 0-4 first
+        out["poc"] = bytes(r)
+        out["no_poc"] = bytes(b[:poc]) + bytes(b[poc + 18:])
+    last = b.rfind(b"\xff\x90")
+    out["missing_tile_part"] = bytes(b[:last]) + b"\xff\xd9"
     return out
 
 
@@ -179,6 +212,32 @@ def test_checker_agrees_with_reference(ref, frames, prof):
             assert got == want, f"{name} at {fps} fps: ours {got} ({msg}), reference {want}"
     assert CS.check_dci(cs)[0]
     assert not CS.check_dci(cs, 400.0)[0]  # far over the byte cap at 400 fps
+
+
+@pytest.mark.parametrize("prof", PROFILES)
+def test_checker_agrees_with_reference_under_header_damage(ref, frames, prof):
+    """Seeded random damage to the main header, the tile-part headers and the bytes around
+    them (one to three bytes each): the verdict equals the reference checker's in every case,
+    at the frame rate and at the rate where the frame sits exactly on the 250 Mbit/s cap."""
+    W, H, fk = prof
+    cs, _, _, _ = ref_codestream(ref, W, H, fk, frames[prof], fps=24.0)
+    b = np.frombuffer(cs, np.uint8)
+    sots = [i for i in range(len(b) - 1) if b[i] == 0xFF and b[i + 1] == 0x90][:6]
+    hot = list(range(0, cs.find(b"\xff\x90") + 14)) + [s + k for s in sots for k in range(16)] + \
+        list(range(len(b) - 4, len(b)))
+    rng = np.random.default_rng(W + H)
+    exact = 250e6 / 8.0 / len(cs)  # frame rate whose cap is this frame's size
+    disagree = []
+    for t in range(300):
+        d = bytearray(cs)
+        for _ in range(int(rng.integers(1, 4))):
+            d[hot[int(rng.integers(0, len(hot)))]] = int(rng.integers(0, 256))
+        for fps in (24.0, exact):
+            want, _ = ref_check(ref, bytes(d), fps)
+            got, msg = CS.check_dci(bytes(d), fps)
+            if got != want:
+                disagree.append((t, fps, msg))
+    assert not disagree, disagree[:5]
 
 
 @pytest.mark.parametrize("prof", PROFILES)
