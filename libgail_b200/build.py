@@ -22,7 +22,10 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--fmad=false",
-          "-I", CSRC, "-I", INCLUDE, "-DGB_TOOLKIT=\"12.9.86\""]
+          "-I", CSRC, "-I", INCLUDE]
+# exported: the plugin entry point and the gb_* C API (include/*.h), nothing else (no
+# template instantiations of the C++ standard library, nothing of the static CUDA runtime)
+EXPORTS = os.path.join(CSRC, "exports.map")
 
 
 def _nvcc() -> str:
@@ -60,8 +63,10 @@ def build(verbose_ptxas: bool = False) -> str:
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [_nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lpthread"]
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max([os.path.getmtime(o) for o in objs] +
+                                                             [os.path.getmtime(EXPORTS)]):
+        cmd = [_nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lpthread", "-Xlinker",
+               f"--version-script={EXPORTS},--exclude-libs,ALL"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

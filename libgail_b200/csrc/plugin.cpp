@@ -209,23 +209,30 @@ int pDecoderDecode(GailCudaDecoder* d, const GailCudaLayout* frame, const uint8_
     });
 }
 
-uint64_t layoutHash() {
+// FNV-1a over the sizes of the structures that cross the boundary, as libgail computes
+// it (cudaPluginLayout, src/cuda/cuda_plugin.h:208-217); evaluated at compile time, so the
+// table below is a constant and nothing runs when the library loads.
+constexpr uint64_t layoutHash() {
+    constexpr uint64_t sizes[] = {sizeof(GbSubband),          sizeof(GbCblkInfo),         sizeof(GbCblkCode),
+                                  sizeof(GbFrameFormat),      sizeof(GbFrameTimings),     sizeof(GailCudaDeviceDesc),
+                                  sizeof(GailCudaLayout),     sizeof(GailCudaEncodeSettings), sizeof(GailCudaTier1),
+                                  sizeof(GailCudaDebug),      sizeof(GailCudaDecodeTimings), sizeof(GailCudaPlugin)};
     uint64_t h = 1469598103934665603ull;
-    for (uint64_t v : {(uint64_t)sizeof(GbSubband), (uint64_t)sizeof(GbCblkInfo), (uint64_t)sizeof(GbCblkCode),
-                       (uint64_t)sizeof(GbFrameFormat), (uint64_t)sizeof(GbFrameTimings), (uint64_t)sizeof(GailCudaDeviceDesc),
-                       (uint64_t)sizeof(GailCudaLayout), (uint64_t)sizeof(GailCudaEncodeSettings),
-                       (uint64_t)sizeof(GailCudaTier1), (uint64_t)sizeof(GailCudaDebug),
-                       (uint64_t)sizeof(GailCudaDecodeTimings), (uint64_t)sizeof(GailCudaPlugin)})
-        h = (h ^ v) * 1099511628211ull;
+    for (uint64_t v : sizes) h = (h ^ v) * 1099511628211ull;
     return h;
 }
 
-const GailCudaPlugin kPlugin = {
+// The toolkit that compiled this file: nvcc's own version macros.
+#define GB_STR2(x) #x
+#define GB_STR(x) GB_STR2(x)
+#define GB_TOOLKIT_VERSION GB_STR(__CUDACC_VER_MAJOR__) "." GB_STR(__CUDACC_VER_MINOR__) "." GB_STR(__CUDACC_VER_BUILD__)
+
+constexpr GailCudaPlugin kPlugin = {
     GAIL_CUDA_PLUGIN_ABI,
     (uint32_t)sizeof(GailCudaPlugin),
     layoutHash(),
     "gail_cuda13",
-    GB_TOOLKIT,
+    GB_TOOLKIT_VERSION,
     "100a",
     pLastError,
     pDeviceCount,
