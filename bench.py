@@ -8,24 +8,27 @@ pass (bit-exact with the CPU reference). One step = encoding all 48 frames; the 
 (1.66 GB) are larger than L2, so no flush is needed between steps.
 
   value   DCI codestreams/s of the served path: the batched engine (continuous batching of
-          Tier-1 over every frame in flight) on frames resident in HBM, Tier-1 frames written
-          to mapped host memory, each frame's rate control, Tier-2 and DCI check on the
-          engine's host workers. The K steps run as one job (all K x 48 requests submitted
-          at once, the time to the last codestream). The work spans the engine's streams and
-          threads, so the timed region is bracketed by a barrier and a device
-          synchronisation on both sides; max over ranks.
-  plain   the drop-in per-frame path beside it, as libgail drives the plugin: slot threads,
-          each encoder_encode from host memory then rate control, Tier-2 and the DCI check;
-          codestreams/s and p50/p99 latency at a Poisson load of 80 % of that rate (served
-          latency at the same load); and, frames resident in HBM, the device stages alone
-          with the per-stage split (CUDA events on the encoder's stream).
-  e2e     codestreams/s of the served path with the frames in pinned host memory: each
-          frame's upload and its Tier-1 output in host memory are inside the timed region.
-  dci     every codestream of the timed runs checked: how many passed, the largest.
-  decode  the served codestreams of one step decoded through decoder_decode (host
-          codestream in, 12-bit picture out) one after another, with the stage split.
-  stages  per stage of the plain path: live ms per frame, algorithmic bytes, GB/s and the
-          fraction of the measured HBM bandwidth; roofline is the dominant stage.
+          Tier-1 over every frame in flight) on frames resident in HBM, rate control and
+          Tier-2 on the device driven by host workers, every codestream DCI-checked. The K
+          steps run as one job (all K x 48 requests submitted at once, the time to the last
+          codestream). The work spans the engine's streams and threads, so the timed region
+          is bracketed by a barrier and a device synchronisation on both sides; max over ranks.
+  e2e     the same with the frames in pinned host memory: uploads and codestreams inside.
+  served_* / plain_*  codestreams/s and p50 / p99 latency of both paths at one Poisson load
+          (80 % of the plain rate), and the served p99 at 90 % of its own end-to-end rate.
+          plain: the drop-in per-frame path as libgail drives the plugin (slot threads, each
+          encoder_encode from host memory, then the host codec's rate control, Tier-2 and
+          the DCI check).
+  stages  the served path's stage split, live (the same job once more with the engine's
+          CUDA-event stage timing on): ms per frame, algorithmic bytes and HBM fraction.
+  roofline  the dominant kernel of the served run, t1CmKernel: integer-issue bound, so its
+          roofline is the SM issue rate.
+  decode  48 4K + 48 2K X'Y'Z' codestreams at 250 Mbit/s decoded at full and half size,
+          one at a time (decoder_decode) and as engine decode requests.
+  encode_decode_2k  the 2K configuration one frame at a time, encode and decode.
+  six_profiles  16 frames over the six DCI profiles: Tier-1 as one persistent launch in
+          the served engine against the plain per-frame path.
+  mixed   Poisson encode and decode requests of 4K and 2K at three loads.
 
 --impl reference times the reference's own CPU path (the CpuSlot encoder, then its rate
 control, codestream writer and DCI checker, built from the reference sources into
@@ -56,15 +59,15 @@ WORKLOAD = ("4K 3996x2160 Y'CbCr 4:2:2 10-bit BT.2020 PQ -> 12-bit X'Y'Z', 9/7 6
             "48 preloaded frames")
 
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on one 4K
-# frame, and Tier-1 issue figures, from the ncu captures summarised in the files below
-# (encode kernels; decodeKernel's in the second)
-NCU_SOURCE = "profiles/kernels_4k_encode_frame.md"
-NCU_DECODE_SOURCE = "profiles/kernels_4k_decode_frame.md"
 ET_FACTOR = 0.25  # the Tier-1 early-termination factor gail.h's encoder forces
-NCU_TRAFFIC = {"t1CmKernel": 214.29e6, "t1MqKernel": 182.01e6}
-NCU_TIER1 = {"cm_issue_active_pct": 71.1, "cm_warps_per_sm": 23.1, "mq_issue_active_pct": 27.1, "mq_warps_per_sm": 4.6,
-             "decode_issue_active_pct": 72.5, "decode_warps_per_sm": 26.0}
+DECODE_FRAMES = 48  # codestreams per profile of the decode configuration
+# Per 4K frame of this workload, one batched t1CmKernel launch (context modelling of the
+# frames' 25,986 code-blocks each) executes this many warp instructions and moves this many
+# DRAM bytes: ncu counters smsp__inst_executed.sum and dram__bytes_read.sum +
+# dram__bytes_write.sum of this build, divided by the frames in the launch. The achieved
+# issue rate in the roofline divides them by the launch time measured in the run.
+CM_WARP_INSTR_PER_FRAME = 912.5e6
+CM_DRAM_BYTES_PER_FRAME = 214.29e6
 
 
 def parse():
@@ -231,6 +234,48 @@ def poisson_arrivals(n, rate, seed=7):
     return np.cumsum(rng.exponential(1.0 / rate, n))
 
 
+def _pct(a, q):
+    return float(np.percentile(a, q)) if len(a) else None
+
+
+def served_latency(eng, cid, frames, rate, n, seed=7):
+    """p50 / p99 latency (ms, submit to codestream) of n requests at Poisson rate `rate`,
+    and the rate achieved."""
+    import threading
+    arr = poisson_arrivals(n, rate, seed=seed)
+    lat = []
+
+    def collect():
+        for _ in range(n):
+            rid, _, ms, st = eng.wait(120000, copy=False)
+            if rid < 0 or st != 0:
+                raise RuntimeError(f"engine frame failed (id {rid}, status {st})")
+            lat.append(ms)
+            eng.release(rid)
+
+    th = threading.Thread(target=collect)
+    th.start()
+    t0 = time.perf_counter()
+    for i in range(n):
+        while time.perf_counter() - t0 < arr[i]:
+            pass
+        eng.submit(cid, frames[i % len(frames)])
+    th.join()
+    dt = time.perf_counter() - t0
+    return {"offered_fps": rate, "achieved_fps": n / dt, "requests": n, "p50_ms": _pct(lat, 50),
+            "p99_ms": _pct(lat, 99)}
+
+
+def drain(eng, ids, keep=None):
+    for _ in ids:
+        rid, _, _, st = eng.wait(120000, copy=False)
+        if rid < 0 or st != 0:
+            raise RuntimeError(f"engine request failed (id {rid}, status {st})")
+        if keep is not None:
+            keep(rid)
+        eng.release(rid)
+
+
 def run_ours(args):
     import torch
 
@@ -238,19 +283,12 @@ def run_ours(args):
     rank, local, world = rank_info()
     torch.cuda.set_device(local)
     rep = Replicas("nccl", timeout_s=120, device=f"cuda:{local}")
-    import libgail_b200 as gb
+    import libgail_b200 as gb  # noqa: F401  (loads the CUDA library: no fallback exists)
     from libgail_b200 import codestream as CS
     from libgail_b200 import plugin as P
     from libgail_b200.engine import Engine
     from libgail_b200.slots import SlotPipeline
 
-    L = gb.lib()
-    L.gb_encoder_stream.restype = C.c_void_p
-    L.gb_encoder_stream.argtypes = [C.c_void_p]
-    L.gb_encoder_enqueue_device.argtypes = [C.c_void_p, C.c_void_p]
-    L.gb_encoder_finish.argtypes = [C.c_void_p]
-    L.gb_encoder_stage_timing.argtypes = [C.c_void_p, C.c_int]
-    L.gb_encoder_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     cuda = f"cuda:{local}"
     reduce_max = rep.max
 
@@ -282,68 +320,9 @@ def run_ours(args):
     ncblk = lay.abi.numCblks
     budget, _ = CS.dci_limits(FPS)
     workers = max(2, min(16, (os.cpu_count() or 8) - 2))
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
 
-    # ---- device stages of the plain path, frames resident in HBM: the per-stage split ---
-    enc = dev.encoder(lay, fmt, col)
-    h = enc.h
-    stream = torch.cuda.ExternalStream(L.gb_encoder_stream(h), device=cuda)
-
-    def plain_step():
-        for f in dframes:
-            gb.check(L.gb_encoder_enqueue_device(h, C.c_void_p(f.data_ptr())))
-
-    for _ in range(args.warmup):
-        plain_step()
-    gb.check(L.gb_encoder_finish(h))
-    ms5 = np.zeros(5)
-    cnt = C.c_int()
-    gb.check(L.gb_encoder_stage_timing(h, 1))
-    gb.check(L.gb_encoder_stage_times(h, ms5.ctypes.data, C.byref(cnt)))  # reset
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        plain_step()
-    e1.record(stream)
-    gb.check(L.gb_encoder_finish(h))
-    torch.cuda.synchronize()
-    plain_dev_ms = reduce_max(e0.elapsed_time(e1))
-    gb.check(L.gb_encoder_stage_times(h, ms5.ctypes.data, C.byref(cnt)))
-    gb.check(L.gb_encoder_stage_timing(h, 0))
-    stage = ms5 / max(cnt.value, 1)  # ms per frame: front, cm, order, mq, pack
-    plain_dev_fps = args.steps * len(dframes) * world / (plain_dev_ms / 1e3)
-    # decisions and codeword bytes per frame, from the plugin's own timings
-    inbuf = enc.input_buffer()
-    decisions, coded, passes = [], [], []
-    for f in frames[: min(4, len(frames))]:
-        C.memmove(inbuf, f.ctypes.data, nbytes)
-        view, tm = enc.encode_view(inbuf)
-        decisions.append(tm.symbols)
-        coded.append(view.numData)
-        passes.append(view.numPasses)
-    enc.close()
-
-    # ---- plain: slot threads, each encoder_encode + rate control + codestream + check ----
-    slots = SlotPipeline(dev, lay, fmt, col, slots=args.slots, fps=FPS, tag="b200")
-    slots.run(frames[: min(len(frames), 2 * args.slots)])  # warm-up
-    barrier()
-    plain_res, plain_s = [], 0.0
-    for _ in range(args.steps):
-        r, dt = slots.run(frames)
-        plain_res += r
-        plain_s += dt
-    plain_fps = len(plain_res) * world / reduce_max(plain_s)
-    # latency at a Poisson load both paths carry: 80 % of the plain rate
-    rate = 0.8 * plain_fps / world
-    nlat = min(2 * len(frames), 96)
-    arr = poisson_arrivals(nlat, rate)
-    lat_frames = [frames[i % len(frames)] for i in range(nlat)]
-    plain_lat_res, _ = slots.run(lat_frames, arrivals=arr)
-    slots.close()
-    plain_lat = [r[2] for r in plain_lat_res]
-
-    # ---- served: the batched engine; rate control and Tier-2 on the device, driven by
-    # host workers (the Tier-1 frames stay in device memory, only codestreams come back)
+    # ---- served: the batched engine, rate control and Tier-2 on the device -------------
     # a budget of 48 frame slots: deep enough to keep two Tier-1 batches and the front ends
     # busy; every slot is made during the warm-up, none inside the timed region
     probe = Engine(local, 0, max_batch=args.batch)
@@ -353,25 +332,21 @@ def run_ours(args):
     eng.set_policy(policy["maxBatch"], policy["minBatchPct"], policy["maxWaitMs"])
     cid, frame_bytes = eng.add_encoder(lay, fmt, col)
     eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
-    served_cs = []
-
-    kept_cs = []  # codestreams of one step, for the decode run
+    served_cs, kept_cs = [], []
 
     def served_step(src, keep=False, repeat=1):
         """Returns the host-to-device and device-to-host bytes the engine copied and the
         kernels it launched."""
         b0 = eng.counters()
         ids = [eng.submit(cid, f) for _ in range(repeat) for f in src]
-        for _ in ids:
-            rid, t, _, st = eng.wait(120000, copy=False)
-            if rid < 0 or st != 0:
-                raise RuntimeError(f"engine frame failed (id {rid}, status {st})")
-            (p, n), ok = eng.codestream(rid, copy=False)
+
+        def k(rid):
             if keep:
+                (p, n), ok = eng.codestream(rid, copy=False)
                 served_cs.append((n, ok))
                 if len(kept_cs) < len(src):
                     kept_cs.append(C.string_at(p, n))
-            eng.release(rid)
+        drain(eng, ids, k)
         b1 = eng.counters()
         return tuple(y - x for x, y in zip(b0, b1))
 
@@ -389,7 +364,7 @@ def run_ours(args):
     value = args.steps * len(dframes) * world / served_s
     st_eng = eng.stats()
 
-    # served end to end: frames in pinned host memory, uploads and Tier-1 output inside
+    # served end to end: frames in pinned host memory, uploads and codestreams inside
     served_step(pinned)
     barrier()
     t0 = time.perf_counter()
@@ -398,25 +373,50 @@ def run_ours(args):
     e2e_s = reduce_max(time.perf_counter() - t0)
     e2e_fps = args.steps * len(pinned) * world / e2e_s
 
-    # served latency at the same Poisson load
-    served_lat = []
-    import threading
-
-    def collect():
-        for _ in range(nlat):
-            rid, _, lat_ms, st = eng.wait(120000, copy=False)
-            served_lat.append(lat_ms)
-            eng.release(rid)
-
-    th = threading.Thread(target=collect)
-    th.start()
+    # the served path's stage split, live: the same job once more with the engine's stage
+    # timing on (CUDA events around each frame's front-end graph and each Tier-1 batch's
+    # stages; host wall time of each frame's rate-control round trips)
+    eng.stage_timing(True)
+    eng.stage_times(reset=True)
     t0 = time.perf_counter()
-    for i in range(nlat):
-        while time.perf_counter() - t0 < arr[i]:
-            pass
-        eng.submit(cid, pinned[i % len(pinned)])
-    th.join()
+    served_step(dframes, repeat=2)
+    split_s = time.perf_counter() - t0
+    stage_ms, stage_n = eng.stage_times(reset=True)
+    eng.stage_timing(False)
+    split_fps = 2 * len(dframes) / split_s
+
+    # ---- plain: slot threads, each encoder_encode + rate control + codestream + check ----
+    slots = SlotPipeline(dev, lay, fmt, col, slots=args.slots, fps=FPS, tag="b200")
+    slots.run(frames[: min(len(frames), 2 * args.slots)])  # warm-up
+    barrier()
+    plain_res, plain_s = [], 0.0
+    for _ in range(args.steps):
+        r, dt = slots.run(frames)
+        plain_res += r
+        plain_s += dt
+    plain_fps = len(plain_res) * world / reduce_max(plain_s)
+    # latency at a Poisson load both paths carry: 80 % of the plain rate
+    rate = 0.8 * plain_fps / world
+    nlat = min(2 * len(frames), 96)
+    arr = poisson_arrivals(nlat, rate)
+    plain_lat_res, _ = slots.run([frames[i % len(frames)] for i in range(nlat)], arrivals=arr)
+    slots.close()
+    plain_lat = [r[2] for r in plain_lat_res]
+    lat_equal = served_latency(eng, cid, pinned, rate, nlat)
+    # served latency near its own capacity: 90 % of the served end-to-end rate
+    lat_90 = served_latency(eng, cid, pinned, 0.9 * e2e_fps / world, 10 * len(pinned), seed=9)
     eng.close()
+
+    # decisions and codeword bytes per frame, from the plugin's own timings
+    enc = dev.encoder(lay, fmt, col)
+    inbuf = enc.input_buffer()
+    decisions, coded = [], []
+    for f in frames[: min(4, len(frames))]:
+        C.memmove(inbuf, f.ctypes.data, nbytes)
+        view, tm = enc.encode_view(inbuf)
+        decisions.append(tm.symbols)
+        coded.append(view.numData)
+    enc.close()
 
     # ---- served with Tier-1 early termination, as libgail's gail.h encoder runs it --------
     # (slope factor 0.25, src/api/gail_api.cpp:607: each frame's threshold is the lambda of
@@ -427,74 +427,24 @@ def run_ours(args):
     cid_et, _ = eng.add_encoder(lay, fmt, col)
     eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
     eng.set_slope_factor(ET_FACTOR)
+    et_res = []
 
-    def et_step(src, repeat=1):
-        ids = [eng.submit(cid_et, f) for _ in range(repeat) for f in src]
-        res = []
-        for _ in ids:
-            rid, _, _, st = eng.wait(120000, copy=False)
-            if rid < 0 or st != 0:
-                raise RuntimeError(f"engine frame failed (id {rid}, status {st})")
-            (p, n), ok = eng.codestream(rid, copy=False)
-            res.append((n, ok, eng.frame_info(rid)[1]))
-            eng.release(rid)
-        return res
+    def et_keep(rid):
+        (p, n), ok = eng.codestream(rid, copy=False)
+        et_res.append((n, ok, eng.frame_info(rid)[1]))
 
-    et_step(dframes, repeat=args.warmup)
+    drain(eng, [eng.submit(cid_et, f) for _ in range(args.warmup) for f in dframes])
     barrier()
     t0 = time.perf_counter()
-    et_res = et_step(dframes, repeat=args.steps)
+    drain(eng, [eng.submit(cid_et, f) for _ in range(args.steps) for f in dframes], et_keep)
     torch.cuda.synchronize()
-    et_s = reduce_max(time.perf_counter() - t0)
-    et_fps = args.steps * len(dframes) * world / et_s
+    et_fps = args.steps * len(dframes) * world / reduce_max(time.perf_counter() - t0)
     eng.close()
-
-    # ---- decode: the served codestreams back to 12-bit pictures -------------------------
-    # the host parses each codestream (gb_parse_codestream), decoder_decode does Tier-1
-    # decode, dequantisation, the inverse 9/7 and ICT on the device and returns the picture
-    parse_ms = []
-    parsed = []
-    for c in kept_cs:
-        t = time.perf_counter()
-        parsed.append(CS.parse(c)[1].view(P.CBLK_CODE_DTYPE))
-        parse_ms.append((time.perf_counter() - t) * 1e3)
-    dec = dev.decoder(lay, reduce=0)
-    pic = np.zeros((H4K, W4K, 3), np.uint16)
-    for i in range(min(3, len(kept_cs))):
-        dec.decode(kept_cs[i], parsed[i], out=pic)
-    dstage = np.zeros(3)
-    t0 = time.perf_counter()
-    for c, b in zip(kept_cs, parsed):
-        _, tm, _ = dec.decode(c, b, out=pic)
-        dstage += (tm.t1, tm.dwt, tm.color)
-    dec_s = reduce_max(time.perf_counter() - t0)
-    dec.close()
-    decode_fps = len(kept_cs) * world / dec_s
-
-    # the same codestreams as decode requests to the served engine: its host workers parse
-    # them and decode them on decoder slots, each on its own stream, several in flight (the
-    # pictures come back to host memory as above)
-    eng = Engine(local, 0, max_batch=args.batch)
-    dcls, _ = eng.add_decoder(lay)
-
-    def dec_burst():
-        ids = [eng.submit_decode(dcls, c) for c in kept_cs]
-        for _ in ids:
-            rid, _, _, st = eng.wait(120000, copy=False)
-            if rid < 0 or st != 0:
-                raise RuntimeError(f"engine decode failed (id {rid}, status {st})")
-            eng.release(rid)
-
-    dec_burst()  # makes the decoder slots
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(2):
-        dec_burst()
-    dec_srv_s = reduce_max(time.perf_counter() - t0)
-    eng.close()
-    decode_served_fps = 2 * len(kept_cs) * world / dec_srv_s
 
     mixed = run_mixed(args, local, dev, lay, fmt, col, pinned, kept_cs, frame_bytes, workers, policy)
+    cfg2 = run_decode_cfg(local, dev, workers, args.batch, policy)
+    cfg0 = run_2k_frame(dev)
+    cfg3 = run_six_profiles(local, dev, workers)
 
     out = None
     if rank == 0:
@@ -505,38 +455,57 @@ def run_ours(args):
             pass
         hbm = float(peaks.get("hbm_gbs", 6650.0))
         npix = W4K * H4K
-        sms = torch.cuda.get_device_properties(local).multi_processor_count
-        dec, cod, npas = float(np.mean(decisions)), float(np.mean(coded)), float(np.mean(passes))
-        # algorithmic bytes per frame (one launch of each stage): the front end at 60 B per
-        # pixel (colour 16, the 9/7 levels 32, the quantised words 12); context modelling
-        # reads the coefficient words and writes one byte per decision; MQ coding reads the
-        # decisions and writes the codewords; packing reads and writes the codewords and
-        # the per-block and per-pass tables
-        alg = [npix * 60, ncblk * 4096 + dec, ncblk * 16, dec + cod, 2 * cod + ncblk * 40 + npas * 16]
-        names = ["front end (colour + 9/7 + quantisation)", "Tier-1 context modelling", "Tier-1 ordering",
-                 "Tier-1 MQ coding", "Tier-1 packing"]
+        dec, cod = float(np.mean(decisions)), float(np.mean(coded))
+        nf = max(1, stage_n["batch_frames"])
+        per = {"front": stage_ms["front"] / max(1, stage_n["front_frames"]), "cm": stage_ms["cm"] / nf,
+               "order": stage_ms["order"] / nf, "mq": stage_ms["mq"] / nf, "pack": stage_ms["pack"] / nf,
+               "rc": stage_ms["rc"] / max(1, stage_n["rc_frames"])}
+        # algorithmic bytes per frame: the front end at 60 B per pixel (colour 16, the 9/7
+        # levels 32, the quantised words 12); context modelling reads the coefficient words
+        # and writes a byte per decision; MQ coding reads the decisions and writes the
+        # codewords; packing moves the codewords and the per-block and per-pass tables
+        alg = {"front": npix * 60, "cm": ncblk * 4096 + dec, "mq": dec + cod, "pack": 2 * cod + ncblk * 40}
+        names = {"front": "front end (colour + 9/7 + quantisation; one CUDA graph per frame)",
+                 "cm": "Tier-1 context modelling (t1CmKernel, batched)", "order": "Tier-1 ordering (t1OrderKernel)",
+                 "mq": "Tier-1 MQ coding + truncation lengths (t1MqKernel, t1TruncKernel)",
+                 "pack": "packing + PCRD hull points (tileSum, scan, hull, copy)",
+                 "rc": "rate control + Tier-2 on the device (host wall time of the round trips, per frame)"}
         stages = []
-        for i, nm in enumerate(names):
-            ms = float(stage[i])
-            ach = alg[i] / (ms * 1e-3) / 1e9 if ms > 0 else None
-            stages.append({"stage": nm, "ms_per_frame": round(ms, 4), "algorithmic_bytes": int(alg[i]),
-                           "achieved_gbs": ach, "frac": ach / hbm if ach else None})
-        # the dominant stage of the plain step: its roofline, with the DRAM traffic of one
-        # launch from the committed ncu capture of the same workload
-        k = int(np.argmax(stage))
-        traffic = {1: NCU_TRAFFIC.get("t1CmKernel"), 3: NCU_TRAFFIC.get("t1MqKernel")}.get(k)
-        roofline = {"bound": "hbm", "kernel": names[k], "achieved": stages[k]["achieved_gbs"], "peak": hbm,
-                    "unit": "GB/s", "frac": stages[k]["frac"], "traffic": traffic,
-                    "peak_source": "measured" if peaks else "fallback",
-                    "traffic_source": NCU_SOURCE if traffic else None,
-                    "note": "Tier-1 is integer-issue and latency bound (a serial MQ chain per code-block): "
-                            "bytes move far below HBM speed; see tier1 for its own measures"}
+        for k, nm in names.items():
+            ms = per[k]
+            row = {"stage": nm, "ms_per_frame": round(ms, 4)}
+            if k in alg and ms > 0:
+                ach = alg[k] / (ms * 1e-3) / 1e9
+                row.update({"algorithmic_bytes": int(alg[k]), "achieved_gbs": ach, "hbm_frac": ach / hbm})
+            stages.append(row)
+        # the dominant kernel of the served run: context modelling, integer-issue bound; its
+        # roofline is the SM issue rate (4 warp instructions per SM per cycle at the SM clock
+        # sampled during the timed region)
+        sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+        issue_peak = sms * 4 * sm_mhz * 1e6
+        batch_frames = stage_n["batch_frames"] / max(1, stage_n["batches"])
+        cm_launch_ms = stage_ms["cm"] / max(1, stage_n["batches"])
+        instr = CM_WARP_INSTR_PER_FRAME * batch_frames
+        achieved = instr / (cm_launch_ms * 1e-3)
+        roofline = {"bound": "issue", "kernel": "t1CmKernel (Tier-1 context modelling, batched launch)",
+                    "achieved": achieved / 1e12, "peak": issue_peak / 1e12, "unit": "T warp-instr/s",
+                    "frac": achieved / issue_peak, "traffic": CM_DRAM_BYTES_PER_FRAME * batch_frames,
+                    "traffic_unit": "DRAM bytes per launch",
+                    "algorithmic_bytes_per_launch": alg["cm"] * batch_frames,
+                    "launch_ms": cm_launch_ms, "frames_per_launch": batch_frames,
+                    "warp_instr_per_launch": instr,
+                    "sources": "launch_ms: CUDA events on the batch stream in this run; warp instructions and "
+                               "DRAM bytes per frame: ncu (smsp__inst_executed.sum, dram__bytes_read.sum + "
+                               "dram__bytes_write.sum) on one batched launch of this build; peak: SMs x 4 issue "
+                               "slots x the median SM clock sampled in this run",
+                    "note": "elapsed on its stream while the other batch's MQ coding and the next front ends "
+                            "run beside it; HBM is not the bound (traffic / launch_ms is far below the peak)"}
+        front = stages[0]
         tier1 = {"code_blocks": ncblk, "decisions_per_frame": dec, "codeword_bytes_per_frame": cod,
-                 "mq_decisions_per_s": dec / (stage[3] * 1e-3),
-                 "code_blocks_per_s_per_sm_plain": ncblk / ((stage[1] + stage[3]) * 1e-3) / sms,
+                 "mq_decisions_per_s_served": dec / (per["mq"] * 1e-3) if per["mq"] else None,
                  "code_blocks_per_s_per_sm_served": ncblk * value / sms,
-                 "ncu": dict(NCU_TIER1, sources=[NCU_SOURCE, NCU_DECODE_SOURCE])}
-        pct = lambda a, q: float(np.percentile(a, q))  # noqa: E731
+                 "cm_issue_frac_served": roofline["frac"]}
+        pct = _pct
         dci = {"fps": FPS, "budget_bytes": budget,
                "served": {"frames": len(served_cs), "valid": sum(1 for _, ok in served_cs if ok == 1),
                           "max_bytes": max(n for n, _ in served_cs)},
@@ -547,15 +516,20 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": served_s * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32 (integer Tier-1), f32 (colour, wavelet)",
             "data": f"synthetic (seeded generator, {len(dframes)} frames)",
+            "served_fps": value, "plain_fps": plain_fps,
+            "served_p50_ms": lat_equal["p50_ms"], "served_p99_ms": lat_equal["p99_ms"],
+            "plain_p50_ms": pct(plain_lat, 50), "plain_p99_ms": pct(plain_lat, 99), "latency_offered_fps": rate,
+            "served_p99_ms_at_90pct": lat_90["p99_ms"], "served_offered_fps_at_90pct": lat_90["offered_fps"],
             "config": {"workload": WORKLOAD, "frames_per_step": len(dframes), "path": "served (batched engine)",
                        "max_batch": args.batch, "codestream_workers": workers, "parallelism": f"replicas x{world}",
                        "tuning": {"file": os.path.relpath(args.tuning, ROOT) if tuned else None,
                                   "profiles": {"2k": AT.get_tuning(0), "4k": AT.get_tuning(1)}, "policy": policy},
                        "l2": f"inputs larger than L2 ({len(dframes)} frames, {len(dframes) * nbytes / 1e9:.2f} GB)"},
-            "served": {"fps": value, "latency_ms": {"p50": pct(served_lat, 50), "p99": pct(served_lat, 99)},
-                       "offered_fps": rate, "batches": st_eng["batches"],
+            "served": {"fps": value, "latency_equal_load": lat_equal, "latency_90pct_capacity": lat_90,
+                       "batches": st_eng["batches"],
                        "frames_per_batch": st_eng["batch_frames"] / max(1, st_eng["batches"]),
-                       "slots": st_eng["slots"], "frame_bytes": frame_bytes},
+                       "slots": st_eng["slots"], "frame_bytes": frame_bytes,
+                       "stage_split_fps": split_fps},
             "early_termination": {
                 "slope_factor": ET_FACTOR, "fps": et_fps, "frames": len(et_res),
                 "coded_again": sum(1 for r in et_res if r[2]),
@@ -565,22 +539,12 @@ def run_ours(args):
                 "reference_published": "171.1 frames/s on an RTX 3090 (CUDA backend, early termination 0.25, "
                                        "4 frames in flight, docs/BENCHMARKS.md:16)"},
             "plain": {"fps": plain_fps, "slots": args.slots,
-                      "latency_ms": {"p50": pct(plain_lat, 50), "p99": pct(plain_lat, 99)}, "offered_fps": rate,
-                      "device_resident_fps_tier1_only": plain_dev_fps,
-                      "stage_ms_per_frame": dict(zip(["front", "t1_cm", "t1_order", "t1_mq", "pack"],
-                                                     [round(x, 4) for x in stage]))},
+                      "latency_ms": {"p50": pct(plain_lat, 50), "p99": pct(plain_lat, 99)}, "offered_fps": rate},
             "dci": dci,
             "mixed": mixed,
-            "decode": {"fps": decode_fps, "unit": "frames/s", "frames": len(kept_cs),
-                       "path": "decoder_decode per frame: codestream from host memory, 12-bit picture to host memory",
-                       "parse_ms_per_frame": float(np.mean(parse_ms)),
-                       "served_fps": decode_served_fps,
-                       "served_path": "engine decode requests: host workers parse, decoder slots on their own streams, "
-                                      "several in flight, pictures to host memory",
-                       "reference_published": "121.4 frames/s on an RTX 3090 (CUDA backend, 250 Mbit/s, 3 in flight, "
-                                              "docs/BENCHMARKS.md:113)",
-                       "stage_ms_per_frame": dict(zip(["t1_decode_dequant", "inverse_dwt", "ict_pack"],
-                                                      [round(x / max(1, len(kept_cs)), 4) for x in dstage]))},
+            "decode": cfg2,
+            "encode_decode_2k": cfg0,
+            "six_profiles": cfg3,
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": int(h2d_e2e),
                     "d2h_bytes_per_step": int(d2h),
                     "path": "served engine, frames in pinned host memory; rate control and Tier-2 on the device, "
@@ -588,6 +552,9 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "roofline": roofline,
             "stages": stages,
+            "front_end_hbm": {"achieved_gbs": front.get("achieved_gbs"), "peak": hbm,
+                              "frac": front.get("hbm_frac"),
+                              "peak_source": "measured" if peaks else "fallback"},
             "tier1": tier1,
             "clocks": clk,
         }
@@ -600,6 +567,160 @@ def run_ours(args):
     rep.close()
     if out is not None:
         print(json.dumps(out))
+
+
+def _xyz_frames(w, h, count, seed):
+    from libgail_b200 import synth
+    return synth.many(lambda ww, hh, sd, i: synth.xyz12_to_rgb48(synth.xyz12_planes(ww, hh, sd, i)), count, w, h,
+                      seed=seed)
+
+
+def run_decode_cfg(local, dev, workers, batch, policy, count=DECODE_FRAMES):
+    """Decode of `count` 4K and `count` 2K X'Y'Z' codestreams at 250 Mbit/s, at full size
+    and at half size (reduce 1): one at a time through decoder_decode (host parse, device
+    Tier-1 decode, dequantisation, inverse 9/7 and ICT, picture to host memory) and as
+    engine decode requests with several in flight. The codestreams come from this
+    library's encoder, whose codestream bytes equal the reference CPU encoder's on the same
+    frames (the parity tests check that byte for byte)."""
+    from libgail_b200 import codestream as CS
+    from libgail_b200 import plugin as P
+    from libgail_b200.engine import Engine
+    out = {"frames_per_profile": count, "mbps": 250.0,
+           "source": "X'Y'Z' 12-bit generator frames encoded by this library at 250 Mbit/s (codestreams "
+                     "byte-identical to the reference CPU encoder's)",
+           "reference_published": "reduce 1: 301.4 (4K) / 566.6 (2K) frames/s on an RTX 3090 "
+                                  "(docs/BENCHMARKS.md:117-118)"}
+    for name, (w, h, fk) in (("4k", (W4K, H4K, 1)), ("2k", (1998, 1080, 0))):
+        lay = P.LayoutHolder(w, h, fk)
+        frames = _xyz_frames(w, h, count, 3000 + fk)
+        eng = Engine(local, 0, max_batch=batch)
+        eng.set_policy(policy["maxBatch"], policy["minBatchPct"], policy["maxWaitMs"])
+        cid, _ = eng.add_encoder(lay, P.rgb48_format(w, h), P.color_passthrough())
+        eng.set_codestream(fps=FPS, max_mbps=250.0, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
+        streams = []
+        drain(eng, [eng.submit(cid, f) for f in frames], lambda rid: streams.append(eng.codestream(rid)[0]))
+        eng.close()
+        del frames
+        parsed = [CS.parse(c)[1].view(P.CBLK_CODE_DTYPE) for c in streams]
+        row = {"max_bytes": max(len(c) for c in streams)}
+        for reduce in (0, 1):
+            dec = dev.decoder(lay, reduce=reduce)
+            pic = np.zeros((dec.out_h, dec.out_w, 3), np.uint16)
+            for i in range(3):
+                dec.decode(streams[i], parsed[i], out=pic)
+            t0 = time.perf_counter()
+            for c in streams:  # the host parse is part of each decode, as in decoder_decode's callers
+                _, blocks = CS.parse(c)
+                dec.decode(c, blocks.view(P.CBLK_CODE_DTYPE), out=pic)
+            plain = len(streams) / (time.perf_counter() - t0)
+            dec.close()
+            eng = Engine(local, 0, max_batch=batch)
+            dcls, _ = eng.add_decoder(lay, reduce=reduce)
+            drain(eng, [eng.submit_decode(dcls, c) for c in streams])  # makes the decoder slots
+            t0 = time.perf_counter()
+            drain(eng, [eng.submit_decode(dcls, c) for _ in range(2) for c in streams])
+            served = 2 * len(streams) / (time.perf_counter() - t0)
+            eng.close()
+            row[f"reduce{reduce}"] = {"plain_fps": plain, "served_fps": served}
+        out[name] = row
+    return out
+
+
+def run_2k_frame(dev, count=24):
+    """The 2K configuration one frame at a time through the drop-in, as libgail's pipeline
+    drives it: encoder_encode of a 1998x1080 X'Y'Z' frame, its codestream by the host codec
+    (rate control and Tier-2, 230 Mbit/s at 24 fps), then the parse and decoder_decode of that
+    codestream back to 12-bit X'Y'Z'."""
+    from libgail_b200 import codestream as CS
+    from libgail_b200 import plugin as P
+    w, h = 1998, 1080
+    lay = P.LayoutHolder(w, h, 0)
+    frames = _xyz_frames(w, h, count, 4000)
+    enc = dev.encoder(lay, P.rgb48_format(w, h), P.color_passthrough())
+    dec = dev.decoder(lay)
+    buf = enc.input_buffer()
+    pic = np.zeros((h, w, 3), np.uint16)
+
+    def one(f):
+        C.memmove(buf, f.ctypes.data, f.nbytes)
+        view, _ = enc.encode_view(buf)
+        cs, _, _ = CS.rate_and_build(lay, view, FPS, 230.0, tag="b200")
+        t = time.perf_counter()
+        _, blocks = CS.parse(cs)
+        dec.decode(cs, blocks.view(P.CBLK_CODE_DTYPE), out=pic)
+        return cs, time.perf_counter() - t
+
+    for f in frames[:3]:
+        one(f)
+    enc_s = dec_s = 0.0
+    ok = 0
+    for f in frames:
+        t = time.perf_counter()
+        cs, ds = one(f)
+        enc_s += time.perf_counter() - t - ds
+        dec_s += ds
+        ok += CS.check_dci(cs, FPS)[0]
+    enc.close()
+    dec.close()
+    return {"frames": count, "encode_fps": count / enc_s, "decode_fps": count / dec_s,
+            "encode_decode_fps": count / (enc_s + dec_s), "dci_valid": ok,
+            "path": "encoder_encode + host rate control and Tier-2, then parse + decoder_decode, one frame at a time"}
+
+
+SIX_PROFILES = [(1998, 1080, 0), (2048, 858, 0), (2048, 1080, 0), (3996, 2160, 1), (4096, 1716, 1), (4096, 2160, 1)]
+
+
+def run_six_profiles(local, dev, workers, count=16, repeat=4):
+    """16 X'Y'Z' frames over the six DCI profiles (uneven edge code-blocks): the served
+    engine with Tier-1 as one persistent launch from a device work queue over every frame in
+    flight (each frame's front end one CUDA graph; rate control and Tier-2 on the device),
+    against the plain per-frame path (encoder_encode, then the host codec's rate control and
+    Tier-2), both to DCI codestreams."""
+    from libgail_b200 import autotune as AT
+    from libgail_b200 import codestream as CS
+    from libgail_b200 import plugin as P
+    from libgail_b200.engine import Engine
+    from libgail_b200 import synth
+    profs = [SIX_PROFILES[i % 6] for i in range(count)]
+    frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(w, h, seed=5000 + i)) for i, (w, h, _) in enumerate(profs)]
+    lays = {p: P.LayoutHolder(*p) for p in SIX_PROFILES}
+    saved = {k: AT.get_tuning(k) for k in (0, 1)}
+    out = {"frames": count, "profiles": [f"{w}x{h}" for w, h, _ in SIX_PROFILES]}
+    try:
+        for k in (0, 1):
+            AT.set_tuning(k, dict(saved[k], t1Persistent=1))
+        eng = Engine(local, 0, max_batch=count)
+        eng.set_policy(count, 100, 5.0)
+        cls = {p: eng.add_encoder(lays[p], P.rgb48_format(p[0], p[1]), P.color_passthrough())[0] for p in SIX_PROFILES}
+        eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
+        drain(eng, [eng.submit(cls[p], f) for p, f in zip(profs, frames)])
+        t0 = time.perf_counter()
+        drain(eng, [eng.submit(cls[p], f) for _ in range(repeat) for p, f in zip(profs, frames)])
+        out["served_persistent_fps"] = repeat * count / (time.perf_counter() - t0)
+        st = eng.stats()
+        out["frames_per_tier1_launch"] = st["batch_frames"] / max(1, st["batches"])
+        eng.close()
+    finally:
+        for k in (0, 1):
+            AT.set_tuning(k, saved[k])
+    encs = {p: dev.encoder(lays[p], P.rgb48_format(p[0], p[1]), P.color_passthrough()) for p in SIX_PROFILES}
+
+    def plain_pass():
+        for p, f in zip(profs, frames):
+            e = encs[p]
+            buf = e.input_buffer()
+            C.memmove(buf, f.ctypes.data, f.nbytes)
+            view, _ = e.encode_view(buf)
+            CS.rate_and_build(lays[p], view, FPS, 230.0, tag="b200")
+
+    plain_pass()
+    t0 = time.perf_counter()
+    for _ in range(repeat):
+        plain_pass()
+    out["plain_fps"] = repeat * count / (time.perf_counter() - t0)
+    for e in encs.values():
+        e.close()
+    return out
 
 
 def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_bytes, workers, policy, n=240,

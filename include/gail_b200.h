@@ -179,7 +179,15 @@ GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
  *                          of width x 3 codes
  *   gb_engine_hull         a handed-out encode's PCRD hull points, computed on the GPU after
  *                          Tier-1 (valid until release; the layout of gb_tier1_hull, over the
- *                          frame's numPasses slots); its codestream's rate control takes them */
+ *                          frame's numPasses slots); its codestream's rate control takes them
+ *   gb_engine_stage_timing per-stage timing of the served path on (1) or off (0): CUDA events
+ *                          around each frame's front-end graph and each Tier-1 batch's stages,
+ *                          host wall time of each frame's device rate control
+ *   gb_engine_stage_times  the totals since the last reset: ms6 = front end, context
+ *                          modelling, ordering, MQ coding with truncation lengths, packing
+ *                          (elapsed on the batch stream), rate control and Tier-2 round trips;
+ *                          counts4 = frames timed in the front end, batches timed, frames in
+ *                          them, frames timed in rate control; reset 1 zeroes them */
 typedef struct GbEngine GbEngine;
 GB_API int gb_engine_create(int device, uint64_t hbmBudget, int maxBatch, GbEngine** out);
 GB_API void gb_engine_destroy(GbEngine* e);
@@ -190,6 +198,8 @@ GB_API int gb_engine_wait(GbEngine* e, int timeoutMs, int64_t* id, GailCudaTier1
                           int* frameStatus);
 GB_API int gb_engine_release(GbEngine* e, int64_t id);
 GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5);
+GB_API int gb_engine_stage_timing(GbEngine* e, int on);
+GB_API int gb_engine_stage_times(GbEngine* e, int reset, double* ms6, uint64_t* counts4);
 /* Batch policy: at most maxBatch frames per Tier-1 launch; while another batch keeps the GPU
  * busy, a batch waits to gather minBatchPct % of maxBatch ready frames, but not past
  * maxWaitMs after its oldest frame (defaults: the create call's maxBatch, 25 %, 2 ms). */

@@ -139,6 +139,24 @@ GB_API int gb_engine_counters(GbEngine* e, uint64_t* h2d, uint64_t* d2h, uint64_
     });
 }
 
+GB_API int gb_engine_stage_timing(GbEngine* e, int on) {
+    return gbGuard([&] {
+        if (!e) throw std::logic_error("null argument");
+        e->e->setStageTiming(on != 0);
+    });
+}
+
+GB_API int gb_engine_stage_times(GbEngine* e, int reset, double* ms6, uint64_t* counts4) {
+    return gbGuard([&] {
+        if (!e || !ms6 || !counts4) throw std::logic_error("null argument");
+        const EncodeEngine::StageTimes t = e->e->stageTimes(reset != 0);
+        const double ms[6] = {t.frontMs, t.cmMs, t.orderMs, t.mqMs, t.packMs, t.rcMs};
+        const uint64_t n[4] = {t.frontFrames, t.batches, t.batchFrames, t.rcFrames};
+        for (int i = 0; i < 6; ++i) ms6[i] = ms[i];
+        for (int i = 0; i < 4; ++i) counts4[i] = n[i];
+    });
+}
+
 GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5) {
     return gbGuard([&] {
         if (!e || !out5) throw std::logic_error("null argument");

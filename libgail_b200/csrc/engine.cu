@@ -64,6 +64,7 @@ struct EncodeEngine::Slot {
     int graphKernels = 0;  // kernel launches one front-end graph makes
     cudaEvent_t frontDone = nullptr;
     cudaEvent_t upDone = nullptr;  // the frame's upload (on the copy stream) is done
+    cudaEvent_t frontT[2] = {};    // stage timing: around the front-end graph
     std::vector<void*> dev, host;
 };
 
@@ -82,6 +83,7 @@ struct EncodeEngine::Request {
     bool recoded = false;   // coded again with every pass
     bool tier1 = true;      // the Tier-1 frame was packed into host memory
     bool devFrame = false;  // ... and into the slot's device buffers
+    bool frontTimed = false;  // its front end was bracketed by the slot's timing events
     std::vector<uint8_t> cs;  // the codestream, when the engine makes them
     int dciOk = -1;
     // decode requests
@@ -127,6 +129,10 @@ struct EncodeEngine::Batch {
     std::vector<Request*> frames;
     bool busy = false;
     std::vector<void*> dev;
+    // stage timing: start, after context modelling, after ordering, after MQ and
+    // truncation lengths, after packing
+    cudaEvent_t t[5] = {};
+    bool timed = false;
 };
 
 EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(device), maxBatch_(std::max(1, maxBatch)) {
@@ -149,6 +155,7 @@ EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(
     for (auto& b : batches_) {
         GB_CHECK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
         GB_CHECK(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+        for (auto& e : b->t) GB_CHECK(cudaEventCreate(&e));
         check(cudaHostAlloc((void**)&b->hCtl, 64, cudaHostAllocDefault), "pinned host memory");
     }
     worker_ = std::thread([this] { run(); });
@@ -172,6 +179,8 @@ EncodeEngine::~EncodeEngine() {
         if (s->graph) cudaGraphDestroy(s->graph);
         if (s->frontDone) cudaEventDestroy(s->frontDone);
         if (s->upDone) cudaEventDestroy(s->upDone);
+        for (auto e : s->frontT)
+            if (e) cudaEventDestroy(e);
         for (void* p : s->dev) cudaFree(p);
         for (void* p : s->host) cudaFreeHost(p);
     }
@@ -181,6 +190,8 @@ EncodeEngine::~EncodeEngine() {
         for (void* p : b->dev) cudaFree(p);
         if (b->hCtl) cudaFreeHost(b->hCtl);
         if (b->done) cudaEventDestroy(b->done);
+        for (auto e : b->t)
+            if (e) cudaEventDestroy(e);
         if (b->st) cudaStreamDestroy(b->st);
     }
     if (dSlope_) cudaFree(dSlope_);
@@ -283,6 +294,7 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         GB_CHECK(cudaMemcpy(s->dJobs, jobs.data(), jobs.size() * sizeof(T1Job), cudaMemcpyHostToDevice));
         GB_CHECK(cudaEventCreateWithFlags(&s->frontDone, cudaEventDisableTiming));
         GB_CHECK(cudaEventCreateWithFlags(&s->upDone, cudaEventDisableTiming));
+        for (auto& e : s->frontT) GB_CHECK(cudaEventCreate(&e));
         // the slot's front end as one graph: it always reads the slot's input buffer and
         // writes the slot's coefficient buffer
         cudaStream_t cap;
@@ -310,6 +322,8 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         if (s->graph) cudaGraphDestroy(s->graph);
         if (s->frontDone) cudaEventDestroy(s->frontDone);
         if (s->upDone) cudaEventDestroy(s->upDone);
+        for (auto e : s->frontT)
+            if (e) cudaEventDestroy(e);
         cudaGetLastError();
         std::lock_guard<std::mutex> lock(budgetM_);
         used_ -= c.slotBytes;
@@ -630,7 +644,14 @@ void EncodeEngine::codestreamWorker(int id) {
                     if (!rc) throw std::logic_error("no device rate control for this worker and class");
                     const DeviceTier1 f{reinterpret_cast<const GbCblkInfo*>(s->dInfoP), s->dLenP, s->dDataP, s->dHullP,
                                         s->dHullS};
+                    const auto rc0 = Clock::now();
                     const RateResult rr = rc->run(f, lim, cs_.tag, r->cs, st);
+                    if (timing_.load()) {
+                        const double ms = msBetween(rc0, Clock::now());
+                        std::lock_guard<std::mutex> lock(m_);
+                        times_.rcMs += ms;
+                        times_.rcFrames++;
+                    }
                     d2h += rr.d2hBytes;
                     launches = (uint64_t)rr.launches;
                     lam = minComp(rr);
@@ -708,6 +729,15 @@ EncodeEngine::Stats EncodeEngine::stats() const {
     return stats_;
 }
 
+void EncodeEngine::setStageTiming(bool on) { timing_.store(on); }
+
+EncodeEngine::StageTimes EncodeEngine::stageTimes(bool reset) {
+    std::lock_guard<std::mutex> lock(m_);
+    const StageTimes t = times_;
+    if (reset) times_ = StageTimes{};
+    return t;
+}
+
 bool EncodeEngine::admit() {
     bool progress = false;
     for (;;) {
@@ -742,7 +772,10 @@ bool EncodeEngine::admit() {
                                  copy_));
         GB_CHECK(cudaEventRecord(s->upDone, copy_));
         GB_CHECK(cudaStreamWaitEvent(front_, s->upDone, 0));
+        r->frontTimed = timing_.load() && s->frontT[0];
+        if (r->frontTimed) GB_CHECK(cudaEventRecord(s->frontT[0], front_));
         GB_CHECK(cudaGraphLaunch(s->exec, front_));
+        if (r->frontTimed) GB_CHECK(cudaEventRecord(s->frontT[1], front_));
         GB_CHECK(cudaEventRecord(s->frontDone, front_));
         std::lock_guard<std::mutex> lock(m_);
         if (!r->onDevice) stats_.h2dBytes += c.z.inBytes;
@@ -806,6 +839,8 @@ bool EncodeEngine::launchBatch(Batch& b) {
         base += r->slot->n;
     }
     GB_CHECK(cudaMemsetAsync(b.ctl, 0, 64, b.st));
+    b.timed = timing_.load() && b.t[0];
+    if (b.timed) GB_CHECK(cudaEventRecord(b.t[0], b.st));
     T1Launch L{b.dJobs, (uint32_t)total, b.info, b.end, b.len, b.dist, b.snaps, b.perm, b.ctl, dSlope_};
     bool any4k = false;  // a batch with a 4K frame is launched with the 4K tuning
     for (Request* r : sel) any4k = any4k || classes_[r->cls]->L.profile == 1;
@@ -815,7 +850,8 @@ bool EncodeEngine::launchBatch(Batch& b) {
     L.mqCtasPerSm = (uint16_t)tu.mqCtasPerSm;
     L.persistent = (uint16_t)tu.t1Persistent;
     L.work = b.work;
-    t1Encode(L, b.st);
+    t1Encode(L, b.st, b.timed ? &b.t[1] : nullptr);
+    if (b.timed) GB_CHECK(cudaEventRecord(b.t[3], b.st));
     // context modelling, ordering, MQ coding, truncation lengths: four launches or one
     uint64_t launches = tu.t1Persistent ? 1 : 4;
     bool onDevice, tier1;
@@ -849,6 +885,7 @@ bool EncodeEngine::launchBatch(Batch& b) {
         r->tier1 = tier1;
         r->devFrame = onDevice;
     }
+    if (b.timed) GB_CHECK(cudaEventRecord(b.t[4], b.st));
     GB_CHECK(cudaMemcpyAsync(b.hCtl, b.ctl, 64, cudaMemcpyDeviceToHost, b.st));
     GB_CHECK(cudaEventRecord(b.done, b.st));
     b.frames = std::move(sel);
@@ -867,7 +904,30 @@ bool EncodeEngine::collect(Batch& b) {
     GB_CHECK(e);
     const auto now = Clock::now();
     const uint32_t status = b.hCtl[1];
+    float ms[4] = {0, 0, 0, 0};
+    if (b.timed)
+        for (int k = 0; k < 4; ++k) GB_CHECK(cudaEventElapsedTime(&ms[k], b.t[k], b.t[k + 1]));
+    std::vector<float> front;
+    for (Request* r : b.frames)
+        if (r->frontTimed) {
+            float f = 0;
+            GB_CHECK(cudaEventElapsedTime(&f, r->slot->frontT[0], r->slot->frontT[1]));
+            front.push_back(f);
+            r->frontTimed = false;
+        }
     std::lock_guard<std::mutex> lock(m_);
+    if (b.timed) {
+        times_.cmMs += ms[0];
+        times_.orderMs += ms[1];
+        times_.mqMs += ms[2];
+        times_.packMs += ms[3];
+        times_.batches++;
+        times_.batchFrames += b.frames.size();
+    }
+    for (float f : front) {
+        times_.frontMs += f;
+        times_.frontFrames++;
+    }
     for (Request* r : b.frames) {
         r->latency = msBetween(r->t0, now);
         r->status = (status || r->slot->hTot[2]) ? kError : kOk;

@@ -110,6 +110,20 @@ public:
     };
     Stats stats() const;
 
+    // Per-stage times of the served path while on (CUDA events on the streams the work runs
+    // on; a little overhead, so off by default): each frame's front end (its CUDA graph:
+    // colour, wavelet, quantisation; the upload before it not included), and per Tier-1
+    // batch its context modelling, ordering, MQ coding with truncation lengths, and packing
+    // (elapsed on the batch stream: the two batches in flight and the front ends share the
+    // GPU meanwhile). Rate control and Tier-2 on the device: host wall time of each frame's
+    // round trips on its worker.
+    struct StageTimes {
+        double frontMs = 0, cmMs = 0, orderMs = 0, mqMs = 0, packMs = 0, rcMs = 0;
+        uint64_t frontFrames = 0, batches = 0, batchFrames = 0, rcFrames = 0;
+    };
+    void setStageTiming(bool on);
+    StageTimes stageTimes(bool reset);
+
 private:
     struct Class;
     struct Slot;
@@ -155,6 +169,8 @@ private:
     float* hZero_ = nullptr;  // a pinned 0 threshold for frames coded again
     std::string error_;
     Stats stats_;
+    std::atomic<bool> timing_{false};
+    StageTimes times_;  // under m_
     std::thread worker_;
     // codestream stage
     CodestreamConfig cs_;

@@ -22,6 +22,8 @@ def _bind():
                                  C.POINTER(C.c_int)]
     L.gb_engine_release.argtypes = [C.c_void_p, C.c_int64]
     L.gb_engine_stats.argtypes = [C.c_void_p, C.c_void_p]
+    L.gb_engine_stage_timing.argtypes = [C.c_void_p, C.c_int]
+    L.gb_engine_stage_times.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.gb_engine_set_codestream.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_char_p, C.c_char_p,
                                            C.c_int, C.c_int, C.c_int]
     L.gb_engine_set_slope_factor.argtypes = [C.c_void_p, C.c_double]
@@ -161,6 +163,19 @@ class Engine:
     def release(self, rid: int):
         check(lib().gb_engine_release(self.h, rid))
         self._keep.pop(rid, None)
+
+    def stage_timing(self, on: bool):
+        """Per-stage timing of the served path (CUDA events; a little overhead) on or off."""
+        check(lib().gb_engine_stage_timing(self.h, int(bool(on))))
+
+    def stage_times(self, reset: bool = False):
+        """Totals since the last reset: ms by stage (front, cm, order, mq, pack, rc) and the
+        counts they cover (front_frames, batches, batch_frames, rc_frames)."""
+        ms = np.zeros(6, np.float64)
+        n = np.zeros(4, np.uint64)
+        check(lib().gb_engine_stage_times(self.h, int(bool(reset)), ms.ctypes.data, n.ctypes.data))
+        return (dict(zip(["front", "cm", "order", "mq", "pack", "rc"], (float(x) for x in ms))),
+                dict(zip(["front_frames", "batches", "batch_frames", "rc_frames"], (int(x) for x in n))))
 
     def stats(self):
         out = np.zeros(5, np.uint64)
