@@ -240,29 +240,13 @@ def _pct(a, q):
 
 def served_latency(eng, cid, frames, rate, n, seed=7):
     """p50 / p99 latency (ms, submit to codestream) of n requests at Poisson rate `rate`,
-    and the rate achieved."""
-    import threading
-    arr = poisson_arrivals(n, rate, seed=seed)
-    lat = []
-
-    def collect():
-        for _ in range(n):
-            rid, _, ms, st = eng.wait(120000, copy=False)
-            if rid < 0 or st != 0:
-                raise RuntimeError(f"engine frame failed (id {rid}, status {st})")
-            lat.append(ms)
-            eng.release(rid)
-
-    th = threading.Thread(target=collect)
-    th.start()
-    t0 = time.perf_counter()
-    for i in range(n):
-        while time.perf_counter() - t0 < arr[i]:
-            pass
-        eng.submit(cid, frames[i % len(frames)])
-    th.join()
-    dt = time.perf_counter() - t0
-    return {"offered_fps": rate, "achieved_fps": n / dt, "requests": n, "p50_ms": _pct(lat, 50),
+    submitted and collected by the engine's own threads (gb_engine_open_loop), and the
+    rate achieved."""
+    lat, st, el = eng.open_loop([(cid, "encode", frames[i % len(frames)]) for i in range(n)],
+                                poisson_arrivals(n, rate, seed=seed))
+    if np.any(st != 0):
+        raise RuntimeError(f"{int(np.count_nonzero(st))} engine frames failed")
+    return {"offered_fps": rate, "achieved_fps": n / el, "requests": n, "p50_ms": _pct(lat, 50),
             "p99_ms": _pct(lat, 99)}
 
 
@@ -617,11 +601,17 @@ def run_decode_cfg(local, dev, workers, batch, policy, count=DECODE_FRAMES):
             eng = Engine(local, 0, max_batch=batch)
             dcls, _ = eng.add_decoder(lay, reduce=reduce)
             drain(eng, [eng.submit_decode(dcls, c) for c in streams])  # makes the decoder slots
+            eng.decode_times(reset=True)
             t0 = time.perf_counter()
             drain(eng, [eng.submit_decode(dcls, c) for _ in range(2) for c in streams])
             served = 2 * len(streams) / (time.perf_counter() - t0)
+            dt = eng.decode_times()
             eng.close()
-            row[f"reduce{reduce}"] = {"plain_fps": plain, "served_fps": served}
+            nd = max(1, dt["decodes"])
+            row[f"reduce{reduce}"] = {"plain_fps": plain, "served_fps": served,
+                                      "served_host_ms_per_decode": {k: dt[k] / nd for k in ("wait_ms", "parse_ms",
+                                                                                             "run_ms")},
+                                      "served_slots_made_later": dt["slots_made_later"]}
         out[name] = row
     return out
 
@@ -681,8 +671,10 @@ def run_six_profiles(local, dev, workers, count=16, repeat=4):
     from libgail_b200 import plugin as P
     from libgail_b200.engine import Engine
     from libgail_b200 import synth
+    import torch
     profs = [SIX_PROFILES[i % 6] for i in range(count)]
     frames = [synth.xyz12_to_rgb48(synth.xyz12_planes(w, h, seed=5000 + i)) for i, (w, h, _) in enumerate(profs)]
+    pinned = [torch.from_numpy(f.view(np.int16)).pin_memory() for f in frames]  # the served path's uploads
     lays = {p: P.LayoutHolder(*p) for p in SIX_PROFILES}
     saved = {k: AT.get_tuning(k) for k in (0, 1)}
     out = {"frames": count, "profiles": [f"{w}x{h}" for w, h, _ in SIX_PROFILES]}
@@ -693,9 +685,9 @@ def run_six_profiles(local, dev, workers, count=16, repeat=4):
         eng.set_policy(count, 100, 5.0)
         cls = {p: eng.add_encoder(lays[p], P.rgb48_format(p[0], p[1]), P.color_passthrough())[0] for p in SIX_PROFILES}
         eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
-        drain(eng, [eng.submit(cls[p], f) for p, f in zip(profs, frames)])
+        drain(eng, [eng.submit(cls[p], f) for p, f in zip(profs, pinned)])
         t0 = time.perf_counter()
-        drain(eng, [eng.submit(cls[p], f) for _ in range(repeat) for p, f in zip(profs, frames)])
+        drain(eng, [eng.submit(cls[p], f) for _ in range(repeat) for p, f in zip(profs, pinned)])
         out["served_persistent_fps"] = repeat * count / (time.perf_counter() - t0)
         st = eng.stats()
         out["frames_per_tier1_launch"] = st["batch_frames"] / max(1, st["batches"])
@@ -723,12 +715,12 @@ def run_six_profiles(local, dev, workers, count=16, repeat=4):
     return out
 
 
-def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_bytes, workers, policy, n=240,
-              loads=(100.0, 200.0, 300.0), seed=11):
+def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_bytes, workers, policy, n=480,
+              loads=(100.0, 200.0, 300.0, 400.0), seed=11):
     """Serving a mix as it arrives: Poisson requests, 70 % encode / 30 % decode, 60 % 4K
     (the benchmark's Y'CbCr frames and their codestreams) / 40 % 2K X'Y'Z', one engine with
     codestreams on; per offered load the achieved rate and p50/p99 latency by kind."""
-    import threading
+    import torch
 
     from libgail_b200 import codestream as CS
     from libgail_b200 import plugin as P
@@ -737,7 +729,8 @@ def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_
     W2, H2 = 1998, 1080
     lay2k = P.LayoutHolder(W2, H2, 0)
     fmt2k, col2k = P.rgb48_format(W2, H2), P.color_passthrough()
-    frames2k = [synth.xyz12_to_rgb48(synth.xyz12_planes(W2, H2, seed=seed + i)) for i in range(8)]
+    frames2k = [torch.from_numpy(synth.xyz12_to_rgb48(synth.xyz12_planes(W2, H2, seed=seed + i)).view(np.int16))
+                .pin_memory() for i in range(8)]
     eng = Engine(local, 64 * frame_bytes, max_batch=args.batch)
     eng.set_policy(policy["maxBatch"], policy["minBatchPct"], policy["maxWaitMs"])
     try:
@@ -766,44 +759,24 @@ def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_
         kinds = rng.random(n) < 0.7           # encode
         big = rng.random(n) < 0.6             # 4K
         picks = rng.integers(0, 1 << 30, n)
+        reqs = []
+        for i in range(n):
+            if kinds[i]:
+                reqs.append((e4, "encode", frames4k[picks[i] % len(frames4k)]) if big[i] else
+                            (e2, "encode", frames2k[picks[i] % len(frames2k)]))
+            else:
+                reqs.append((d4, "decode", streams4k[picks[i] % len(streams4k)]) if big[i] else
+                            (d2, "decode", streams2k[picks[i] % len(streams2k)]))
         out = []
         for load in loads:
-            arr = poisson_arrivals(n, load, seed=seed + int(load))
-            lat = {}
-            kind_of = {}
-            done = threading.Event()
-
-            def collect():
-                for _ in range(n):
-                    rid, _, ms, st = eng.wait(120000, copy=False)
-                    if rid < 0 or st != 0:
-                        raise RuntimeError(f"mixed request failed (id {rid}, status {st})")
-                    lat[rid] = ms
-                    eng.release(rid)
-                done.set()
-
-            th = threading.Thread(target=collect)
-            th.start()
-            t0 = time.perf_counter()
-            for i in range(n):
-                while time.perf_counter() - t0 < arr[i]:
-                    pass
-                if kinds[i]:
-                    rid = eng.submit(e4, frames4k[picks[i] % len(frames4k)]) if big[i] else \
-                        eng.submit(e2, frames2k[picks[i] % len(frames2k)])
-                    kind_of[rid] = "encode"
-                else:
-                    rid = eng.submit_decode(d4, streams4k[picks[i] % len(streams4k)]) if big[i] else \
-                        eng.submit_decode(d2, streams2k[picks[i] % len(streams2k)])
-                    kind_of[rid] = "decode"
-            th.join()
-            elapsed = time.perf_counter() - t0
-            if len(lat) != n:
-                raise RuntimeError("mixed serving lost requests")
+            lat, st, elapsed = eng.open_loop(reqs, poisson_arrivals(n, load, seed=seed + int(load)))
+            if np.any(st != 0):
+                raise RuntimeError("mixed requests failed")
             row = {"offered_fps": load, "achieved_fps": n / elapsed}
-            for k in ("encode", "decode"):
-                v = [lat[r] for r in lat if kind_of.get(r) == k]
-                row[k] = {"requests": len(v), "p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99))}
+            for k, sel in (("encode", kinds), ("decode", ~kinds)):
+                v = lat[sel]
+                row[k] = {"requests": int(v.size), "p50_ms": float(np.percentile(v, 50)),
+                          "p99_ms": float(np.percentile(v, 99))}
             out.append(row)
         return {"requests_per_load": n, "mix": "70 % encode / 30 % decode; 60 % 4K Y'CbCr PQ / 40 % 2K X'Y'Z'",
                 "loads": out}

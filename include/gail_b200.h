@@ -180,6 +180,21 @@ GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
  *   gb_engine_hull         a handed-out encode's PCRD hull points, computed on the GPU after
  *                          Tier-1 (valid until release; the layout of gb_tier1_hull, over the
  *                          frame's numPasses slots); its codestream's rate control takes them
+ *   gb_engine_open_loop    an open-loop load, driven natively: request i (kind 0: encode of
+ *                          the frame item[i] of class classId[i], on the device when
+ *                          onDevice[i]; kind 1: decode of the codestream item[i] of size[i]
+ *                          bytes) is submitted arrivalSec[i] seconds after the call starts
+ *                          (non-decreasing), whether or not earlier ones have finished; a
+ *                          second thread waits for each and releases it. Out: each request's
+ *                          latency (submit to finish, as gb_engine_wait reports it) and
+ *                          status, and the time from the start to the last finish. For
+ *                          latency under Poisson arrivals without the caller's own threads
+ *                          in the way
+ *   gb_engine_decode_times for the engine's decode requests since the last reset: ms3 = host
+ *                          time waiting for a free decoder slot, parsing, and in the slot
+ *                          (upload, device stages, picture back); counts2 = decodes, decoder
+ *                          slots made after their class was added (each allocates device and
+ *                          pinned host memory); reset 1 zeroes them
  *   gb_engine_stage_timing per-stage timing of the served path on (1) or off (0): CUDA events
  *                          around each frame's front-end graph and each Tier-1 batch's stages,
  *                          host wall time of each frame's device rate control
@@ -199,6 +214,10 @@ GB_API int gb_engine_wait(GbEngine* e, int timeoutMs, int64_t* id, GailCudaTier1
 GB_API int gb_engine_release(GbEngine* e, int64_t id);
 GB_API int gb_engine_stats(GbEngine* e, uint64_t* out5);
 GB_API int gb_engine_stage_timing(GbEngine* e, int on);
+GB_API int gb_engine_decode_times(GbEngine* e, int reset, double* ms3, uint64_t* counts2);
+GB_API int gb_engine_open_loop(GbEngine* e, uint32_t n, const int* classId, const int* kind, const void* const* item,
+                               const uint64_t* size, const int* onDevice, const double* arrivalSec, double* latencyMs,
+                               int* status, double* elapsedSec);
 GB_API int gb_engine_stage_times(GbEngine* e, int reset, double* ms6, uint64_t* counts4);
 /* Batch policy: at most maxBatch frames per Tier-1 launch; while another batch keeps the GPU
  * busy, a batch waits to gather minBatchPct % of maxBatch ready frames, but not past

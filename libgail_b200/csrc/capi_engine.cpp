@@ -1,5 +1,12 @@
 // C-ABI of the batched, served encode engine (engine.h).
+#include <atomic>
+#include <chrono>
 #include <memory>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
 
 #include "capi_util.h"
 #include "engine.h"
@@ -154,6 +161,85 @@ GB_API int gb_engine_stage_times(GbEngine* e, int reset, double* ms6, uint64_t* 
         const uint64_t n[4] = {t.frontFrames, t.batches, t.batchFrames, t.rcFrames};
         for (int i = 0; i < 6; ++i) ms6[i] = ms[i];
         for (int i = 0; i < 4; ++i) counts4[i] = n[i];
+    });
+}
+
+GB_API int gb_engine_open_loop(GbEngine* e, uint32_t n, const int* classId, const int* kind, const void* const* item,
+                               const uint64_t* size, const int* onDevice, const double* arrivalSec, double* latencyMs,
+                               int* status, double* elapsedSec) {
+    return gbGuard([&] {
+        if (!e || (n && (!classId || !kind || !item || !arrivalSec || !latencyMs || !status)) || !elapsedSec)
+            throw std::logic_error("null argument");
+        for (uint32_t i = 0; i < n; ++i) {
+            if (kind[i] != 0 && kind[i] != 1) throw std::logic_error("request kind is 0 (encode) or 1 (decode)");
+            if (kind[i] == 1 && !size) throw std::logic_error("decode requests need their sizes");
+            if (i && arrivalSec[i] < arrivalSec[i - 1]) throw std::logic_error("arrival times must not decrease");
+        }
+        using Clock = std::chrono::steady_clock;
+        EncodeEngine& eng = *e->e;
+        // the collector: every finished request's latency and status by id, released at once
+        struct Done {
+            double ms;
+            int st;
+        };
+        std::unordered_map<int64_t, Done> done;
+        done.reserve(n);
+        std::string failure;
+        std::atomic<bool> abort{false};
+        Clock::time_point last;
+        const auto t0 = Clock::now();
+        std::thread collector([&] {
+            try {
+                for (uint32_t k = 0; k < n && !abort.load(); ++k) {
+                    int64_t id = -1;
+                    GailCudaTier1 t1{};
+                    double ms = 0;
+                    int st = 0;
+                    while (!eng.wait(1000, &id, &t1, &ms, &st))
+                        if (abort.load()) return;
+                    done[id] = {ms, st};
+                    eng.release(id);
+                }
+                last = Clock::now();
+            } catch (const std::exception& ex) {
+                failure = ex.what();
+                abort = true;
+            }
+        });
+        std::vector<int64_t> ids(n, -1);
+        try {
+            for (uint32_t i = 0; i < n && !abort.load(); ++i) {
+                std::this_thread::sleep_until(t0 + std::chrono::duration_cast<Clock::duration>(
+                                                       std::chrono::duration<double>(arrivalSec[i])));
+                ids[i] = kind[i] == 0 ? eng.submit(classId[i], item[i], onDevice && onDevice[i], 0.0)
+                                      : eng.submitDecode(classId[i], static_cast<const uint8_t*>(item[i]), size[i]);
+            }
+        } catch (...) {
+            abort = true;
+            collector.join();
+            throw;
+        }
+        collector.join();
+        if (!failure.empty()) throw std::runtime_error(failure);
+        for (uint32_t i = 0; i < n; ++i) {
+            const auto it = done.find(ids[i]);
+            if (it == done.end()) throw std::runtime_error("a request did not come back");
+            latencyMs[i] = it->second.ms;
+            status[i] = it->second.st;
+        }
+        *elapsedSec = n ? std::chrono::duration<double>(last - t0).count() : 0.0;
+    });
+}
+
+GB_API int gb_engine_decode_times(GbEngine* e, int reset, double* ms3, uint64_t* counts2) {
+    return gbGuard([&] {
+        if (!e || !ms3 || !counts2) throw std::logic_error("null argument");
+        const EncodeEngine::DecodeTimes t = e->e->decodeTimes(reset != 0);
+        ms3[0] = t.waitMs;
+        ms3[1] = t.parseMs;
+        ms3[2] = t.runMs;
+        counts2[0] = t.decodes;
+        counts2[1] = t.slotsMadeLater;
     });
 }
 

@@ -461,10 +461,11 @@ int EncodeEngine::addDecodeClass(const GailCudaLayout& layout, const GailCudaDec
         cls = (int)decClasses_.size() - 1;
         workers = (int)csWorkers_.size();
     }
-    // two slots per host worker now (one decoding, one holding a picture not yet released),
-    // while the HBM budget has room: making one while serving (device memory, pinned host
-    // memory) stalls its worker and the device
-    for (int i = 0; i < 2 * workers; ++i) {
+    // three slots per host worker now (one decoding, up to two holding pictures not yet
+    // released), while the HBM budget has room: making one while serving (device memory,
+    // pinned host memory) stalls its worker and the device, so decodes wait for a released
+    // slot instead, and only a class left without any slot makes one later
+    for (int i = 0; i < 3 * workers; ++i) {
         DecSlot* ds = nullptr;
         try {
             ds = newDecSlot(cls);
@@ -553,10 +554,14 @@ void EncodeEngine::decodeJob(Request* r) {
     }
     Layout frame;
     std::vector<GbCblkCode> blocks;
+    const auto t0 = Clock::now();
+    auto t1 = t0, t2 = t0;
+    bool made = false;
     try {
         parseCodestream(r->input.data(), r->input.size(), frame, blocks);
         if (frame.width != c->L.width || frame.height != c->L.height || frame.levels != c->L.levels)
             throw std::runtime_error("codestream of another frame size than its decode class");
+        t1 = Clock::now();
         DecSlot* ds = nullptr;
         for (;;) {
             {
@@ -567,12 +572,23 @@ void EncodeEngine::decodeJob(Request* r) {
                     break;
                 }
             }
-            ds = newDecSlot(r->cls);
-            if (ds) break;
+            bool none;
+            {
+                std::lock_guard<std::mutex> lock(m_);
+                none = std::none_of(decSlots_.begin(), decSlots_.end(), [&](auto& d) { return d->cls == r->cls; });
+            }
+            if (none) {
+                ds = newDecSlot(r->cls);
+                if (ds) {
+                    made = true;
+                    break;
+                }
+            }
             std::unique_lock<std::mutex> lock(m_);  // no room: the next released slot
             cvDecSlot_.wait_for(lock, std::chrono::milliseconds(50), [&] { return !c->free.empty() || stop_.load(); });
             if (stop_) throw std::runtime_error("engine stopping");
         }
+        t2 = Clock::now();
         r->dslot = ds;
         ds->slot->enqueue(frame, r->input.data(), r->input.size(), blocks.data(), blocks.size(), false);
         r->pix = ds->slot->finish(nullptr);
@@ -580,6 +596,13 @@ void EncodeEngine::decodeJob(Request* r) {
     } catch (const std::exception&) {
         r->status = kError;
     }
+    const auto t3 = Clock::now();
+    std::lock_guard<std::mutex> lock(m_);
+    decTimes_.parseMs += msBetween(t0, t1);
+    decTimes_.waitMs += msBetween(t1, t2);
+    decTimes_.runMs += msBetween(t2, t3);
+    decTimes_.decodes++;
+    if (made) decTimes_.slotsMadeLater++;
 }
 
 bool EncodeEngine::codestream(int64_t id, const uint8_t** data, uint64_t* size, int* dciOk) {
@@ -730,6 +753,13 @@ EncodeEngine::Stats EncodeEngine::stats() const {
 }
 
 void EncodeEngine::setStageTiming(bool on) { timing_.store(on); }
+
+EncodeEngine::DecodeTimes EncodeEngine::decodeTimes(bool reset) {
+    std::lock_guard<std::mutex> lock(m_);
+    const DecodeTimes t = decTimes_;
+    if (reset) decTimes_ = DecodeTimes{};
+    return t;
+}
 
 EncodeEngine::StageTimes EncodeEngine::stageTimes(bool reset) {
     std::lock_guard<std::mutex> lock(m_);

@@ -93,7 +93,10 @@ public:
     // its frames in flight take decoder slots from the same HBM budget. A decode request
     // (the codestream is copied on submit) is parsed, decoded and handed out by the host
     // workers (those of setCodestream, or four started with the first decode class), each
-    // slot on its own stream, so decodes overlap each other and the encode batches.
+    // slot on its own stream, so decodes overlap each other and the encode batches. The
+    // class's slots (three per worker, as the budget allows) are made when it is added and
+    // none while serving: a decode waits for a slot whose picture was released, so a caller
+    // that keeps more pictures than that unreleased holds the workers up.
     int addDecodeClass(const GailCudaLayout& layout, const GailCudaDecodeSettings& s, uint64_t* frameBytes);
     int64_t submitDecode(int cls, const uint8_t* data, uint64_t size);
     // The picture of a finished decode (valid until release): height rows of width x 3
@@ -123,6 +126,14 @@ public:
     };
     void setStageTiming(bool on);
     StageTimes stageTimes(bool reset);
+    // Decode requests, always counted: host ms spent waiting for a free decoder slot,
+    // parsing, and in the slot (enqueue to finish: upload, device stages, picture back);
+    // decodes done; decoder slots made after their class was added (each one allocates).
+    struct DecodeTimes {
+        double waitMs = 0, parseMs = 0, runMs = 0;
+        uint64_t decodes = 0, slotsMadeLater = 0;
+    };
+    DecodeTimes decodeTimes(bool reset);
 
 private:
     struct Class;
@@ -171,6 +182,7 @@ private:
     Stats stats_;
     std::atomic<bool> timing_{false};
     StageTimes times_;  // under m_
+    DecodeTimes decTimes_;  // under m_
     std::thread worker_;
     // codestream stage
     CodestreamConfig cs_;

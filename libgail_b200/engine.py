@@ -23,6 +23,9 @@ def _bind():
     L.gb_engine_release.argtypes = [C.c_void_p, C.c_int64]
     L.gb_engine_stats.argtypes = [C.c_void_p, C.c_void_p]
     L.gb_engine_stage_timing.argtypes = [C.c_void_p, C.c_int]
+    L.gb_engine_decode_times.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.gb_engine_open_loop.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
     L.gb_engine_stage_times.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.gb_engine_set_codestream.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_char_p, C.c_char_p,
                                            C.c_int, C.c_int, C.c_int]
@@ -163,6 +166,48 @@ class Engine:
     def release(self, rid: int):
         check(lib().gb_engine_release(self.h, rid))
         self._keep.pop(rid, None)
+
+    def open_loop(self, requests, arrivals):
+        """An open-loop load driven by the library's own threads: requests[i] = (class id,
+        kind, item) with kind "encode" (item: a numpy array or a torch tensor, host or
+        device) or "decode" (item: codestream bytes), submitted arrivals[i] seconds after the
+        start. Returns (latency ms per request, status per request, seconds to the last
+        finish)."""
+        n = len(requests)
+        cls = np.array([r[0] for r in requests], np.int32)
+        kind = np.array([0 if r[1] == "encode" else 1 for r in requests], np.int32)
+        items = (C.c_void_p * max(1, n))()
+        sizes = np.zeros(max(1, n), np.uint64)
+        ondev = np.zeros(max(1, n), np.int32)
+        keep = []
+        for i, (_, k, it) in enumerate(requests):
+            if k == "encode":
+                on_device = hasattr(it, "is_cuda") and it.is_cuda
+                items[i] = it.data_ptr() if hasattr(it, "data_ptr") else it.ctypes.data
+                ondev[i] = int(on_device)
+            else:
+                b = C.create_string_buffer(bytes(it), len(it))
+                keep.append(b)
+                items[i] = C.cast(b, C.c_void_p).value
+                sizes[i] = len(it)
+            keep.append(it)
+        arr = np.ascontiguousarray(arrivals, np.float64)
+        lat = np.zeros(max(1, n), np.float64)
+        st = np.zeros(max(1, n), np.int32)
+        el = C.c_double()
+        check(lib().gb_engine_open_loop(self.h, n, cls.ctypes.data, kind.ctypes.data, items, sizes.ctypes.data,
+                                        ondev.ctypes.data, arr.ctypes.data, lat.ctypes.data, st.ctypes.data,
+                                        C.byref(el)))
+        return lat[:n], st[:n], el.value
+
+    def decode_times(self, reset: bool = False):
+        """For the decode requests since the last reset: host ms waiting for a decoder slot,
+        parsing and in the slot; decodes; decoder slots made after their class was added."""
+        ms = np.zeros(3, np.float64)
+        n = np.zeros(2, np.uint64)
+        check(lib().gb_engine_decode_times(self.h, int(bool(reset)), ms.ctypes.data, n.ctypes.data))
+        return {"wait_ms": float(ms[0]), "parse_ms": float(ms[1]), "run_ms": float(ms[2]), "decodes": int(n[0]),
+                "slots_made_later": int(n[1])}
 
     def stage_timing(self, on: bool):
         """Per-stage timing of the served path (CUDA events; a little overhead) on or off."""

@@ -19,8 +19,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import threading
-import time
 
 import numpy as np
 
@@ -106,47 +104,22 @@ def serve(requests: int, loads, budget_gb: float, workers: int, seed: int, log=p
             eng.release(rid)
 
         kinds, prof, picks = draw(requests, seed)
+        reqs = [(enc_cls[int(p)], "encode", frames[int(p)][int(k)]) if kd else
+                (dec_cls[int(p)], "decode", streams[int(p)][int(k)]) for kd, p, k in zip(kinds, prof, picks)]
         rows = []
         for load in loads:
-            arr = arrivals(requests, load, seed + int(load))
-            lat, meta = {}, {}
-            failed = []
-
-            def collect():
-                for _ in range(requests):
-                    rid, _, ms, st = eng.wait(120000, copy=False)
-                    if rid < 0 or st != 0:
-                        failed.append((rid, st))
-                        if rid < 0:
-                            return
-                    else:
-                        lat[rid] = ms
-                    eng.release(rid)
-
-            th = threading.Thread(target=collect)
-            th.start()
-            t0 = time.perf_counter()
-            for i in range(requests):
-                while True:  # until the request's arrival: sleep while far, yield when near
-                    ahead = arr[i] - (time.perf_counter() - t0)
-                    if ahead <= 0:
-                        break
-                    time.sleep(ahead - 1e-3 if ahead > 2e-3 else 0)
-                p, k = int(prof[i]), int(picks[i])
-                if kinds[i]:
-                    rid = eng.submit(enc_cls[p], frames[p][k])
-                else:
-                    rid = eng.submit_decode(dec_cls[p], streams[p][k])
-                meta[rid] = ("encode" if kinds[i] else "decode", p)
-            th.join()
-            elapsed = time.perf_counter() - t0
-            if failed:
-                raise RuntimeError(f"{len(failed)} requests failed at {load} requests/s, first {failed[0]}")
+            # submitted and collected by the library's own threads at the arrival times
+            # (open loop: a request arrives whether or not earlier ones have finished)
+            lat, st, elapsed = eng.open_loop(reqs, arrivals(requests, load, seed + int(load)))
+            bad = np.flatnonzero(st != 0)
+            if bad.size:
+                raise RuntimeError(f"{bad.size} requests failed at {load} requests/s, first {int(bad[0])}")
+            kind = np.where(kinds, "encode", "decode")
             row = {"offered_per_s": load, "achieved_per_s": requests / elapsed, "requests": requests}
-            for kind in ("encode", "decode"):
-                row[kind] = percentiles([lat[r] for r in lat if meta[r][0] == kind])
-            row["by_profile"] = {f"{W}x{H} {kind}": percentiles([lat[r] for r in lat if meta[r] == (kind, p)])
-                                 for p, (W, H, _, _) in enumerate(PROFILES) for kind in ("encode", "decode")}
+            for kd in ("encode", "decode"):
+                row[kd] = percentiles(list(lat[kind == kd]))
+            row["by_profile"] = {f"{W}x{H} {kd}": percentiles(list(lat[(kind == kd) & (prof == p)]))
+                                 for p, (W, H, _, _) in enumerate(PROFILES) for kd in ("encode", "decode")}
             log(json.dumps(row))
             rows.append(row)
         return {"mix": "70 % encode / 30 % decode; 50 % 4K flat, 30 % 2K flat, 20 % over the other four "
