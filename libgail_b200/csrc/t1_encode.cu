@@ -107,9 +107,10 @@ __device__ __forceinline__ uint32_t shDown(uint32_t v, int lane) {
 
 // The contexts as tables of a sample's neighbour bits. Zero coding, per orientation, by
 // bits 0-2: left column rows r-1..r+1, 3-5: right column rows r-1..r+1, 6: row above,
-// 7: row below. Sign coding, the whole decision byte (context << 1 | coded bit), by
-// bits 0-2: own signs rows r-1..r+1, 3: left significant, 4: its sign, 5: right
-// significant, 6: its sign, 7: row above significant, 8: row below significant.
+// 7: row below (all significance). Sign coding, the whole decision byte (context << 1 |
+// coded bit), by bits 1, 4, 6, 7 as in the zero-coding key (left, right, above, below
+// significant) and 0: sign of the row above, 2: the sample's own sign, 3: sign of the row
+// below, 5: sign of the left neighbour, 8: sign of the right neighbour.
 __device__ __forceinline__ void cmTables(uint8_t* s_zk, uint8_t* s_sk) {
     for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
         const int o = i >> 8, k = i & 255;
@@ -119,12 +120,20 @@ __device__ __forceinline__ void cmTables(uint8_t* s_zk, uint8_t* s_sk) {
         s_zk[i] = c_zc[45 * o + h + 3 * v + 9 * d];
     }
     for (int k = threadIdx.x; k < 512; k += blockDim.x) {
-        const int hc = clamp1(chiBits((k >> 3) & 1, (k >> 4) & 1) + chiBits((k >> 5) & 1, (k >> 6) & 1));
-        const int vc = clamp1(chiBits((k >> 7) & 1, k & 1) + chiBits((k >> 8) & 1, (k >> 2) & 1));
+        const int hc = clamp1(chiBits((k >> 1) & 1, (k >> 5) & 1) + chiBits((k >> 4) & 1, (k >> 8) & 1));
+        const int vc = clamp1(chiBits((k >> 6) & 1, k & 1) + chiBits((k >> 7) & 1, (k >> 3) & 1));
         const uint32_t t = c_sc[(hc + 1) * 3 + (vc + 1)];
-        s_sk[k] = (uint8_t)(((t & 31u) << 1) | (((uint32_t)k >> 1 & 1u) ^ (t >> 5)));
+        s_sk[k] = (uint8_t)(((t & 31u) << 1) | (((uint32_t)k >> 2 & 1u) ^ (t >> 5)));
     }
 }
+
+// Four rows' fields of a stripe side by side, one byte per row (row i of the stripe in
+// byte i), by one multiply: the four shifted copies of x land in disjoint bit ranges.
+// spread1: bit i of x (x < 16) to bit 0 of byte i; spread3: bits i..i+2 of x (x < 64) to
+// bits 0-2 of byte i.
+__device__ __forceinline__ uint32_t spread1(uint32_t x) { return (x * 0x00204081u) & 0x01010101u; }
+__device__ __forceinline__ uint32_t spread3(uint32_t x) { return (x * 0x00204081u) & 0x07070707u; }
+__device__ __forceinline__ uint32_t byteOf(uint32_t packed, int i) { return (packed >> (8 * i)) & 0xFFu; }
 
 // Context modelling of block `job` by one warp: its decisions to its symbol region, its
 // pass table and info words. mag: the warp's 32 x 32 magnitudes, buf: its plane staging,
@@ -194,27 +203,30 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
                         const int r0 = 4 * s;
                         const uint32_t S = sig, SL = shUp(S, lane), R = shDown(S, lane);
                         const uint32_t cand = (0xFu << r0) & valid & ~S;
-                        const uint32_t spreadLR = SL | (SL << 1) | (SL >> 1) | R | (R << 1) | (R >> 1);
-                        if (!__any_sync(kFull, cand & (spreadLR | (S << 1) | (S >> 1)))) continue;
+                        // what makes a row eligible apart from the left column: the right
+                        // column (rows r-1..r+1) and the own column's rows above and below,
+                        // as before this stripe
+                        const uint32_t fixed = R | (R << 1) | (R >> 1) | (S << 1) | (S >> 1);
+                        if (!__any_sync(kFull, cand & (SL | (SL << 1) | (SL >> 1) | fixed))) continue;
+                        // rows that turn significant once they are eligible
+                        const uint32_t grow = cand & Bp;
                         // from nn = 0 upwards; done when the left columns' new significance
                         // makes no further sample eligible (the right column, the row below
                         // and the in-column chain do not change between iterations)
                         uint32_t nn = 0, ee = 0, L = SL;
 #pragma unroll 1
                         for (int it = 0; it < 34; ++it) {
-                            const uint32_t side = L | (L << 1) | (L >> 1) | R | (R << 1) | (R >> 1) | (S >> 1);
-                            uint32_t n2 = 0, e2 = 0;
-#pragma unroll
-                            for (int k = 0; k < 4; ++k) {
-                                const uint32_t b = 1u << (r0 + k);
-                                if (!(cand & b)) continue;
-                                if ((side & b) | (((S | n2) << 1) & b)) {
-                                    e2 |= b;
-                                    n2 |= Bp & b;
-                                }
-                            }
-                            nn = n2;
-                            ee = e2;
+                            // eligible without the rows above turning significant in this
+                            // pass; those that turn significant (seed); then down the column,
+                            // a row below a new one is eligible and turns significant when
+                            // its bit is set: a chain of at most three more rows
+                            const uint32_t a = cand & (L | (L << 1) | (L >> 1) | fixed);
+                            const uint32_t seed = a & Bp;
+                            uint32_t n = seed | (grow & (seed << 1));
+                            n = seed | (grow & (n << 1));
+                            n = seed | (grow & (n << 1));
+                            nn = n;
+                            ee = a | (cand & (n << 1));
                             const uint32_t Ln = SL | shUp(nn, lane);
                             if (!__any_sync(kFull, cand & ~ee & (Ln | (Ln << 1) | (Ln >> 1)))) break;
                             L = Ln;
@@ -293,10 +305,15 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
                         uint32_t rows = E & Q;
                         if (!rows) continue;
                         if (type == 1) {
+                            // the stripe's four decision bytes: context 16 (refined before),
+                            // 15 (a significant neighbour) or 14, and the bit
+                            const uint32_t rf = spread1((refined >> r0) & 0xFu);
+                            const uint32_t dec = 0x1C1C1C1Cu + ((rf << 2) | ((spread1((nAny >> r0) & 0xFu) & ~rf) << 1) |
+                                                                spread1((Bp >> r0) & 0xFu));
 #pragma unroll 1
                             for (; rows; rows &= rows - 1) {
                                 const int r = __ffs(rows) - 1;
-                                buf[pos++] = (uint8_t)(((bit(refined, r) ? 16u : (bit(nAny, r) ? 15u : 14u)) << 1) | bit(Bp, r));
+                                buf[pos++] = (uint8_t)byteOf(dec, r - r0);
                                 dist += distRef((mag[r][lane] >> p) & 0x7Fu);
                             }
                             continue;
@@ -326,18 +343,21 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
                         const uint32_t wU = (uint32_t)(((unsigned long long)SN << 1) >> r0);
                         const uint32_t wS = q.S >> r0;
                         const uint32_t wG = (uint32_t)(((unsigned long long)sgn << 1) >> r0);
+                        // the four rows' zero-coding keys, byte i for row r0 + i
+                        const uint32_t zkeys = spread3(wL & 0x3Fu) | (spread3(wR & 0x3Fu) << 3) | (spread1(wU & 0xFu) << 6) |
+                                               (spread1((wS >> 1) & 0xFu) << 7);
+                        // and the sign bits of their sign-coding keys: own signs of rows r-1, r,
+                        // r+1 to bits 0, 2, 3, the left neighbour's to bit 5
+                        const uint32_t g3 = spread3(wG & 0x3Fu);
+                        const uint32_t skeys = (g3 & 0x01010101u) | ((g3 & 0x06060606u) << 1) |
+                                               (spread1((sgnL >> r0) & 0xFu) << 5);
 #pragma unroll 1
                         for (; rows; rows &= rows - 1) {
                             const int r = __ffs(rows) - 1, i = r - r0;
-                            const uint32_t up = (wU >> i) & 1u, down = (wS >> (i + 1)) & 1u;
-                            if (!((skip >> r) & 1u)) {
-                                const uint32_t key = ((wL >> i) & 7u) | (((wR >> i) & 7u) << 3) | (up << 6) | (down << 7);
-                                buf[pos++] = (uint8_t)((zk[key] << 1) | bit(Bp, r));
-                            }
+                            const uint32_t zkey = byteOf(zkeys, i);
+                            if (!((skip >> r) & 1u)) buf[pos++] = (uint8_t)((zk[zkey] << 1) | bit(Bp, r));
                             if (bit(NEW, r)) {
-                                const uint32_t key = ((wG >> i) & 7u) | (((wL >> (i + 1)) & 1u) << 3) | (((sgnL >> r) & 1u) << 4) |
-                                                     (((wR >> (i + 1)) & 1u) << 5) | (((sgnR >> r) & 1u) << 6) | (up << 7) |
-                                                     (down << 8);
+                                const uint32_t key = (zkey & 0xD2u) | (byteOf(skeys, i) & 0x2Du) | (((sgnR >> r) & 1u) << 8);
                                 buf[pos++] = s_sk[key];
                                 dist += distSig((mag[r][lane] >> p) & 0x7Fu);
                             }
