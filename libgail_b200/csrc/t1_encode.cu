@@ -80,6 +80,12 @@ __device__ __forceinline__ uint32_t nibbleCounts(uint32_t x) {
     return (x & 0x33333333u) + ((x >> 2) & 0x33333333u);
 }
 
+// Per stripe s of a row mask, at bit 4s: any of its four rows set; the row above it (4s - 1)
+// set; the row below it (4s + 4) set.
+__device__ __forceinline__ uint32_t nibbleAny(uint32_t m) { return (m | (m >> 1) | (m >> 2) | (m >> 3)) & 0x11111111u; }
+__device__ __forceinline__ uint32_t rowAbove(uint32_t m) { return (m << 1) & 0x11111111u; }
+__device__ __forceinline__ uint32_t rowBelow(uint32_t m) { return (m >> 4) & 0x11111111u; }
+
 // Warp-inclusive prefix sum.
 __device__ __forceinline__ uint32_t warpScan(uint32_t v, int lane) {
 #pragma unroll
@@ -149,12 +155,30 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
         const float slope = P.slope ? P.slope[J.slope] : 0.f;
         const uint8_t* zk = s_zk + 256 * orient;
 
-        // Load: lane x reads column x, one 128-byte row per step.
-        const uint32_t* src = J.coeffs;
+        // Load: the block's 4 KB into the warp's rows as 16-byte vectors, each lane's loads
+        // all in flight at once; then lane x reads column x. The words keep their sign bit
+        // (bit 31): no magnitude read below reaches it but the early-termination estimate,
+        // which masks it. Words outside w x h are zeroed here.
+        {
+            const uint4* src = reinterpret_cast<const uint4*>(J.coeffs);
+            uint4* dst = reinterpret_cast<uint4*>(&mag[0][0]);
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                uint4 v[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) v[k] = src[(4 * half + k) * 32 + lane];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) dst[(4 * half + k) * 32 + lane] = v[k];
+            }
+        }
+        __syncwarp();
+        if (w < 32 || h < 32)
+            for (int r = 0; r < 32; ++r)
+                if (lane >= w || r >= h) mag[r][lane] = 0u;
         uint32_t sgn = 0, colMax = 0;
+#pragma unroll 8
         for (int r = 0; r < 32; ++r) {
-            const uint32_t v = (lane < w && r < h) ? src[r * 32 + lane] : 0u;
-            mag[r][lane] = v & 0x7FFFFFFFu;
+            const uint32_t v = mag[r][lane];
             sgn |= (v >> 31) << r;
             colMax = max(colMax, v & 0x7FFFFFFFu);
         }
@@ -190,6 +214,9 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
             for (int r = 0; r < h; ++r) Bp |= ((mag[r][lane] >> (p + kFracBits)) & 1u) << r;
             const uint32_t sig0 = sig;
             uint32_t vis = 0, count = 0;
+            // the plane's decisions are staged at the alignment their region has in global
+            // memory, so that they go out as 16-byte vectors
+            uint8_t* const pb = buf + (symTotal & 15u);
             int32_t planeDist = 0;
             for (int type = (p == nbps - 1 ? 2 : 0); type < 3 && np < maxPasses; ++type) {
                 // (1) the pass's row masks: E = rows coded, NEW = rows that become significant
@@ -252,7 +279,7 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
                     const uint32_t NL = shUp(NEW, lane), NR = shDown(NEW, lane);
                     const uint32_t nAny = (Spass << 1) | (Spass >> 1) | SLp | (SLp << 1) | (SLp >> 1) | SRp | (SRp << 1) |
                                           (SRp >> 1);
-                    // cleanup run-length mode per stripe (bit s), first 1-bit of a run
+                    // cleanup run-length mode per stripe (bit 4s)
                     uint32_t runs = 0;
                     // (3) decisions per stripe, 10-bit fields, three stripes per word
                     uint32_t w0 = 0, w1 = 0, w2 = 0;
@@ -264,30 +291,28 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
                         w1 = ((c >> 12) & 0xFu) | (((c >> 16) & 0xFu) << 10) | (((c >> 20) & 0xFu) << 20);
                         w2 = ((c >> 24) & 0xFu) | (((c >> 28) & 0xFu) << 10);
                     } else {
-#pragma unroll 1
-                        for (int s = 0; s < nstripes; ++s) {
-                            const int r0 = 4 * s;
-                            const uint32_t Q = 0xFu << r0, P = (1u << r0) - 1u;
-                            uint32_t cnt = __popc(E & Q) + __popc(NEW & Q);
-                            if (r0 + 3 < h && (E & Q) == Q) {
-                                const uint32_t L = SLp | (NL & (P | Q)), R = SRp | (NR & P), Sb = Spass | (NEW & P);
-                                const uint32_t win = r0 == 0 ? 0x1Fu : (0x3Fu << (r0 - 1));
-                                if (!(L & win) && !(R & win) && !(Sb & win)) {
-                                    runs |= 1u << s;
-                                    const uint32_t nb = (NEW >> r0) & 0xFu;
-                                    if (nb == 0) {
-                                        cnt = 1;
-                                    } else {
-                                        const uint32_t after = Q & ~((2u << (r0 + __ffs(nb) - 1)) - 1u);
-                                        cnt = 4 + __popc(E & after) + __popc(NEW & after);
-                                    }
-                                }
-                            }
-                            const uint32_t f = cnt << (10 * (s % 3));
-                            if (s < 3) w0 |= f;
-                            else if (s < 6) w1 |= f;
-                            else w2 |= f;
-                        }
+                        // all stripes at once, one bit (4s) or one nibble per stripe s. Run-length
+                        // mode: all four rows in cleanup and no significant sample in the window
+                        // rows r0-1 .. r0+4 of the left column (new ones up to the stripe's end),
+                        // the right column and the own column (new ones above the stripe only).
+                        const uint32_t full = E & (E >> 1) & (E >> 2) & (E >> 3) & 0x11111111u;
+                        const uint32_t blocked = nibbleAny(SLp) | rowAbove(SLp) | rowBelow(SLp) | nibbleAny(NL) |
+                                                 rowAbove(NL) | nibbleAny(SRp) | rowAbove(SRp) | rowBelow(SRp) |
+                                                 rowAbove(NR) | nibbleAny(Spass) | rowAbove(Spass) | rowBelow(Spass) |
+                                                 rowAbove(NEW);
+                        runs = full & ~blocked;
+                        const uint32_t runRows = runs * 0xFu;
+                        // a run stripe: one decision when nothing in it turns significant, else
+                        // the run decision, two position decisions, and the first new sample's
+                        // sign, then the rows after it with their signs: 6 - first + new ones
+                        const uint32_t N = NEW & runRows;
+                        const uint32_t fill = N | ((N << 1) & 0xEEEEEEEEu) | ((N << 2) & 0xCCCCCCCCu) | ((N << 3) & 0x88888888u);
+                        const uint32_t newRun = nibbleAny(N);
+                        const uint32_t c = nibbleCounts(E & ~runRows) + nibbleCounts(NEW & ~runRows) + nibbleCounts(fill) +
+                                           nibbleCounts(N) + (newRun << 1) + (runs & ~newRun);
+                        w0 = (c & 0xFu) | (((c >> 4) & 0xFu) << 10) | (((c >> 8) & 0xFu) << 20);
+                        w1 = ((c >> 12) & 0xFu) | (((c >> 16) & 0xFu) << 10) | (((c >> 20) & 0xFu) << 20);
+                        w2 = ((c >> 24) & 0xFu) | (((c >> 28) & 0xFu) << 10);
                     }
                     const uint32_t i0 = warpScan(w0, lane), i1 = warpScan(w1, lane), i2 = warpScan(w2, lane);
                     const uint32_t t0 = __shfl_sync(kFull, i0, 31), t1 = __shfl_sync(kFull, i1, 31),
@@ -313,19 +338,19 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
 #pragma unroll 1
                             for (; rows; rows &= rows - 1) {
                                 const int r = __ffs(rows) - 1;
-                                buf[pos++] = (uint8_t)byteOf(dec, r - r0);
+                                pb[pos++] = (uint8_t)byteOf(dec, r - r0);
                                 dist += distRef((mag[r][lane] >> p) & 0x7Fu);
                             }
                             continue;
                         }
                         uint32_t skip = 0;  // the row whose zero-coding decision the run decisions replace
-                        if ((runs >> s) & 1u) {
+                        if ((runs >> r0) & 1u) {
                             const uint32_t nb = (NEW >> r0) & 0xFu;
-                            buf[pos++] = (uint8_t)((17u << 1) | (nb != 0));
+                            pb[pos++] = (uint8_t)((17u << 1) | (nb != 0));
                             if (nb == 0) continue;
                             const uint32_t first = __ffs(nb) - 1;
-                            buf[pos++] = (uint8_t)((18u << 1) | (first >> 1));
-                            buf[pos++] = (uint8_t)((18u << 1) | (first & 1u));
+                            pb[pos++] = (uint8_t)((18u << 1) | (first >> 1));
+                            pb[pos++] = (uint8_t)((18u << 1) | (first & 1u));
                             skip = 1u << (r0 + first);
                             rows &= ~(skip - 1u);
                         }
@@ -355,10 +380,10 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
                         for (; rows; rows &= rows - 1) {
                             const int r = __ffs(rows) - 1, i = r - r0;
                             const uint32_t zkey = byteOf(zkeys, i);
-                            if (!((skip >> r) & 1u)) buf[pos++] = (uint8_t)((zk[zkey] << 1) | bit(Bp, r));
+                            if (!((skip >> r) & 1u)) pb[pos++] = (uint8_t)((zk[zkey] << 1) | bit(Bp, r));
                             if (bit(NEW, r)) {
                                 const uint32_t key = (zkey & 0xD2u) | (byteOf(skeys, i) & 0x2Du) | (((sgnR >> r) & 1u) << 8);
-                                buf[pos++] = s_sk[key];
+                                pb[pos++] = s_sk[key];
                                 dist += distSig((mag[r][lane] >> p) & 0x7Fu);
                             }
                         }
@@ -378,7 +403,14 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
             count = min(count, (uint32_t)STAGE);
             __syncwarp();
             if (symTotal + count <= J.cap) {
-                for (uint32_t i = lane; i < count; i += 32) gsym[symTotal + i] = buf[i];
+                const uint32_t head = min(count, (16u - (symTotal & 15u)) & 15u);
+                if ((uint32_t)lane < head) gsym[symTotal + lane] = pb[lane];
+                const uint32_t nv = (count - head) >> 4;
+                const uint4* s4 = reinterpret_cast<const uint4*>(pb + head);
+                uint4* d4 = reinterpret_cast<uint4*>(gsym + symTotal + head);
+                for (uint32_t i = lane; i < nv; i += 32) d4[i] = s4[i];
+                const uint32_t done = head + 16u * nv;
+                if ((uint32_t)lane < count - done) gsym[symTotal + done + lane] = pb[done + lane];
             } else if (lane == 0) {
                 atomicOr(status, kErrSymbolSpace);
             }
@@ -387,7 +419,7 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
                 // early termination (the reference's stopAfterPlane, core/t1_ref.cpp:115-162),
                 // with every float operation in the CPU's order
                 for (uint32_t i = lane; i < count; i += 32) {
-                    const uint32_t s = buf[i];
+                    const uint32_t s = pb[i];
                     atomicAdd(&hist[s >> 1], (s & 1u) ? 0x10000u : 1u);
                 }
                 __syncwarp();
@@ -413,7 +445,7 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
                             const float step = exp2f((float)p);
                             for (int y = 0; y < h; ++y)
                                 for (int x = 0; x < w; ++x) {
-                                    const uint32_t m = mag[y][x];
+                                    const uint32_t m = mag[y][x] & 0x7FFFFFFFu;
                                     const float v = __fmul_rn((float)m, 1.f / 64.f);
                                     const uint32_t qq = m >> (p + kFracBits);
                                     const float rec = qq == 0 ? 0.f : __fmul_rn(__fadd_rn((float)qq, 0.5f), step);
@@ -445,7 +477,7 @@ __device__ __forceinline__ uint32_t cmJob(const T1Launch& P, uint32_t job, uint3
 }
 
 __global__ void __launch_bounds__(CM_THREADS, 7) t1CmKernel(T1Launch P) {
-    __shared__ uint32_t s_mag[CM_WARPS][32][32];
+    __shared__ __align__(16) uint32_t s_mag[CM_WARPS][32][32];  // 16-byte rows: filled by vector stores
     __shared__ __align__(16) uint8_t s_stage[CM_WARPS][STAGE];
     __shared__ uint8_t s_zk[4 * 256];
     __shared__ uint8_t s_sk[512];
