@@ -100,6 +100,8 @@ typedef struct GbTuning {
     uint32_t soloDecisions;
     int32_t cmCtasPerSm, mqCtasPerSm, decCtasPerSm;
     int32_t t1Persistent;
+    int32_t decHeavyPct;  /* Tier-1 decode: blocks whose codeword exceeds this % of the mean bytes per
+                             decoding warp run on SMs of their own, four per SM (0: none) */
 } GbTuning;
 GB_API int gb_set_tuning(int profile, const GbTuning* t);
 GB_API int gb_get_tuning(int profile, GbTuning* t);

@@ -20,14 +20,15 @@ import numpy as np
 
 from . import check, lib
 
-DEFAULTS = {"soloDecisions": 16384, "cmCtasPerSm": 16, "mqCtasPerSm": 16, "decCtasPerSm": 32, "t1Persistent": 0}
+DEFAULTS = {"soloDecisions": 16384, "cmCtasPerSm": 16, "mqCtasPerSm": 16, "decCtasPerSm": 32, "t1Persistent": 0,
+            "decHeavyPct": 250}
 POLICY_DEFAULT = {"maxBatch": 16, "minBatchPct": 25, "maxWaitMs": 2.0}
 PROFILES = {"2k": 0, "4k": 1}
 
 
 class GbTuning(C.Structure):
     _fields_ = [("soloDecisions", C.c_uint32), ("cmCtasPerSm", C.c_int32), ("mqCtasPerSm", C.c_int32),
-                ("decCtasPerSm", C.c_int32), ("t1Persistent", C.c_int32)]
+                ("decCtasPerSm", C.c_int32), ("t1Persistent", C.c_int32), ("decHeavyPct", C.c_int32)]
 
 
 def _bind():
@@ -189,6 +190,25 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
             log(f"[{name}] decoder grid cap (served decode ms per frame)")
             cfg, _, seen3 = coordinate_search(cfg, {"decCtasPerSm": [16, 24, 48, 64]}, _best_of(decode_ms, runs),
                                              log=log)
+            # the heavy-block threshold by one frame's Tier-1 decode on its own (the latency of
+            # decoder_decode: the longest codewords' serial chains set it)
+            blocks = [CS.parse(s)[1].view(P.CBLK_CODE_DTYPE) for s in streams]
+            dec = dev.decoder(lay)
+            pic = np.zeros((lay.height, lay.width, 3), np.uint16)
+
+            def decode_t1_ms(c):
+                set_tuning(prof, c)
+                t = []
+                for s, b in zip(streams, blocks):
+                    dec.decode(s, b, out=pic)
+                    t.append(dec.decode(s, b, out=pic)[1].t1)
+                return float(np.mean(t))
+
+            log(f"[{name}] decoder heavy-block threshold (Tier-1 decode ms of one frame)")
+            cfg, _, seen5 = coordinate_search(cfg, {"decHeavyPct": [0, 150, 400, 800]}, _best_of(decode_t1_ms, runs),
+                                             log=log)
+            seen3 = seen3 + seen5
+            dec.close()
             if name == "4k":
                 log("[4k] engine batch policy (served ms per frame)")
                 pol = dict(POLICY_DEFAULT)

@@ -52,6 +52,17 @@ __constant__ uint8_t c_zc[4 * 45];
 __constant__ uint8_t c_sc[9];
 __constant__ uint32_t c_mq[47];
 
+// Heavy blocks: the longest codewords, decoded on SMs of their own (at most four per SM, one
+// per scheduler) instead of beside 31 other decoding warps, where a block of a thousand
+// bytes or more takes the whole launch's time.
+constexpr uint32_t kMaxReserveSms = 32;
+constexpr uint32_t kMaxHeavy = 4 * kMaxReserveSms;
+// Control words: [0] queue head, [1] status, [2] wanted blocks, [3] heavy blocks, [4] the
+// wanted blocks' codeword bytes; from kCtlArrive a counter per reserved SM, from kCtlClaim a
+// claim flag per heavy block.
+constexpr uint32_t kCtlArrive = 16, kCtlClaim = kCtlArrive + kMaxReserveSms;
+constexpr uint32_t kCtlWords = kCtlClaim + kMaxHeavy;
+
 struct DecArgs {
     const uint8_t* bytes;
     uint64_t size;
@@ -62,7 +73,9 @@ struct DecArgs {
     uint32_t* planes;   // float planes seen as words while decoding
     uint32_t W;
     uint32_t* perm;
-    uint32_t* ctl;      // [0] queue head, [1] status, [2] wanted blocks
+    uint32_t* ctl;      // kCtlWords control words, zeroed before the launch
+    uint32_t slots;     // the decode launch's warps
+    uint32_t heavyPct;  // heavy: codeword bytes above heavyPct % of the mean per warp (0: none)
 };
 
 __device__ __forceinline__ uint32_t lenBucket(uint32_t len) {
@@ -73,16 +86,22 @@ __device__ __forceinline__ uint32_t lenBucket(uint32_t len) {
 
 __global__ void __launch_bounds__(1024) orderKernel(DecArgs a) {
     __shared__ uint32_t hist[ORDER_BUCKETS];
-    __shared__ uint32_t total;
+    __shared__ uint32_t total, bytes, heavy;
     for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
-    if (threadIdx.x == 0) total = 0;
+    if (threadIdx.x == 0) total = bytes = heavy = 0;
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < a.n; i += blockDim.x)
         if (a.blocks[i].wanted) {
-            atomicAdd(&hist[lenBucket(a.codes[i].len)], 1u);
+            const uint32_t len = a.codes[i].len;
+            atomicAdd(&hist[lenBucket(len)], 1u);
             atomicAdd(&total, 1u);
+            atomicAdd(&bytes, min(len, 1u << 20));
         }
     __syncthreads();
+    // heavy blocks: above heavyPct % of the mean codeword bytes per decoding warp
+    const uint64_t limit = (uint64_t)bytes * a.heavyPct / (100ull * max(a.slots, 1u));
+    for (uint32_t i = threadIdx.x; i < a.n; i += blockDim.x)
+        if (a.heavyPct && a.blocks[i].wanted && a.codes[i].len > limit) atomicAdd(&heavy, 1u);
     if (threadIdx.x == 0) {
         uint32_t run = 0;
         for (int b = 0; b < ORDER_BUCKETS; ++b) {
@@ -91,8 +110,10 @@ __global__ void __launch_bounds__(1024) orderKernel(DecArgs a) {
             run += c;
         }
         a.ctl[2] = total;
+        a.ctl[4] = bytes;
     }
     __syncthreads();
+    if (threadIdx.x == 0) a.ctl[3] = min(heavy, kMaxHeavy);  // the first ones of the order
     for (uint32_t i = threadIdx.x; i < a.n; i += blockDim.x)
         if (a.blocks[i].wanted) a.perm[atomicAdd(&hist[lenBucket(a.codes[i].len)], 1u)] = i;
 }
@@ -235,18 +256,15 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
     b.tab = s_tab;
     b.ctx = s_ctx;
     b.W = a.W;
-    const uint32_t count = a.ctl[2];
-    for (;;) {
-        const uint32_t q = atomicAdd(a.ctl, 1u);  // longest codewords first
-        if (q >= count) break;
-        const uint32_t j = a.perm[q];
+    const uint32_t count = a.ctl[2], heavy = a.ctl[3];
+    auto decodeBlock = [&](uint32_t j) {
         const DecBlock blk = a.blocks[j];
         const GbCblkCode code = a.codes[j];
         const int w = blk.w, h = blk.h;
         uint32_t* out = a.planes + blk.dst;  // zeroed before the launch: only significant samples are written
         const int nbps = code.nbps;
         const bool valid = code.passes > 0 && nbps >= 1 && nbps <= 30 && (uint64_t)code.offset + code.len <= a.size;
-        if (!valid) continue;
+        if (!valid) return;
         b.out = out;
         b.zk = s_zk + 512 * blk.orient;
         for (int i = 0; i < 34; ++i) s_sig[i] = s_sgn[i] = 0;
@@ -373,7 +391,27 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                 const float mag = (float)(v & 0x7FFFFFFFu) * half;
                 f[(size_t)y * a.W + x] = (v & 0x80000000u) ? -mag : mag;
             }
+    };
+
+    // the heavy blocks (the first of the order): on a reserved SM (%smid below the reserved
+    // count), the first four warps to arrive take one each and every other warp leaves, so
+    // that the SM runs their serial chains alone
+    uint32_t smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    const uint32_t reserved = (heavy + 3) / 4;
+    if (smid < reserved) {
+        const uint32_t k = atomicAdd(a.ctl + kCtlArrive + smid, 1u), hi = 4 * smid + k;
+        if (k < 4 && hi < heavy && atomicExch(a.ctl + kCtlClaim + hi, 1u) == 0) decodeBlock(a.perm[hi]);
+        return;
     }
+    for (;;) {
+        const uint32_t q = heavy + atomicAdd(a.ctl, 1u);  // longest codewords first
+        if (q >= count) break;
+        decodeBlock(a.perm[q]);
+    }
+    // heavy blocks no reserved SM's warp took (a grid that did not reach every reserved SM)
+    for (uint32_t hi = 0; hi < heavy; ++hi)
+        if (atomicExch(a.ctl + kCtlClaim + hi, 1u) == 0) decodeBlock(a.perm[hi]);
 }
 
 // ---------------------------------------------------------------------------- inverse DWT
@@ -552,7 +590,7 @@ DecoderSlot::DecoderSlot(int device, const Layout& L, const GailCudaDecodeSettin
         alloc(dCodes_, n * sizeof(GbCblkCode));
         alloc(dBlocks_, n * sizeof(DecBlock));
         alloc(dPerm_, n * 4);
-        alloc(dCtl_, 64);
+        alloc(dCtl_, kCtlWords * 4);
         alloc(dOut_, (uint64_t)outW_ * outH_ * 6);
         check(cudaHostAlloc((void**)&hOut_, std::max<uint64_t>(16, (uint64_t)outW_ * outH_ * 6), cudaHostAllocDefault),
               "pinned host memory");
@@ -657,14 +695,16 @@ void DecoderSlot::enqueue(const Layout& frame, const uint8_t* data, size_t size,
     GB_CHECK(cudaMemcpyAsync(dBytes_, hBytes_, size, cudaMemcpyHostToDevice, st));
     GB_CHECK(cudaMemcpyAsync(dCodes_, hCodes_, n * sizeof(GbCblkCode), cudaMemcpyHostToDevice, st));
     GB_CHECK(cudaMemcpyAsync(dHalf_, hHalf_, frame.bands.size() * 4, cudaMemcpyHostToDevice, st));
-    GB_CHECK(cudaMemsetAsync(dCtl_, 0, 64, st));
+    GB_CHECK(cudaMemsetAsync(dCtl_, 0, kCtlWords * 4, st));
     GB_CHECK(cudaMemsetAsync(dPlanes_, 0, npix * 12, st));  // coefficients of uncoded samples
-    DecArgs da{dBytes_, size, dCodes_, dBlocks_, (uint32_t)n, dHalf_, (uint32_t*)dPlanes_, (uint32_t)L_.width, dPerm_, dCtl_};
-    orderKernel<<<1, 1024, 0, st>>>(da);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_);
-    decodeKernel<<<std::min<uint32_t>((uint32_t)n, (uint32_t)(sms * tuningFor(L_.profile).decCtasPerSm)), DEC_THREADS, 0,
-                   st>>>(da);
+    const Tuning tu = tuningFor(L_.profile);
+    const uint32_t grid = std::min<uint32_t>((uint32_t)n, (uint32_t)(sms * tu.decCtasPerSm));
+    DecArgs da{dBytes_, size, dCodes_, dBlocks_, (uint32_t)n, dHalf_, (uint32_t*)dPlanes_, (uint32_t)L_.width, dPerm_, dCtl_,
+               grid, (uint32_t)tu.decHeavyPct};
+    orderKernel<<<1, 1024, 0, st>>>(da);
+    decodeKernel<<<grid, DEC_THREADS, 0, st>>>(da);
     GB_CHECK(cudaGetLastError());
     GB_CHECK(cudaEventRecord(ev_[1], st));
     // inverse wavelet, levels top down; the last one writes the picture (the planes are only

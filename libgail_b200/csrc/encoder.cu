@@ -37,7 +37,7 @@ uint64_t SlotSizes::deviceBytes() const {
     const uint64_t sizes[] = {inBytes,     65536 * 4,   4096 * 4,    2 * llFloats * 4 * 3, n * kCblkArea * 4,
                               n * 48,      arena,       arena,       n * 16,               n * kMaxPasses * 4 * 3,
                               n * kMaxPasses * 16,      n * 4,       t1WorkWords((uint32_t)n) * 4, 64, n * 20,
-                              n * 8,                    n * kMaxPasses * 8,       arena};
+                              n * 8,                    n * kMaxPasses * 8,       outCap};
     uint64_t t = 0;
     for (uint64_t b : sizes) t += page(b);
     return t;
@@ -56,6 +56,18 @@ uint64_t buildJobs(const Layout& L, const uint32_t* coeffs, uint8_t* sym, uint8_
         region += cap;
     }
     return region;
+}
+
+uint64_t buildJobOffsets(const Layout& L, const uint32_t* coeffs, uint32_t slope, std::vector<T1Job>& jobs) {
+    const size_t first = jobs.size();
+    const uint64_t arena = buildJobs(L, coeffs, nullptr, nullptr, slope, jobs);
+    uint64_t region = 0;
+    for (size_t i = first; i < jobs.size(); ++i) {
+        jobs[i].sym = reinterpret_cast<uint8_t*>(static_cast<uintptr_t>(region));
+        jobs[i].cw = reinterpret_cast<uint8_t*>(static_cast<uintptr_t>(region));
+        region += jobs[i].cap;
+    }
+    return arena;
 }
 
 std::vector<double> blockScales(const Layout& L) {
@@ -113,6 +125,7 @@ SlotSizes slotSizes(const Layout& L, const GbFrameFormat& in) {
     std::vector<T1Job> jobs;
     z.arena = buildJobs(L, nullptr, nullptr, nullptr, 0, jobs);
     z.llFloats = (uint64_t)L.levelW(1) * L.levelH(1);
+    z.outCap = std::min<uint64_t>(z.arena, z.npix * 6 + (64u << 10));
     return z;
 }
 
@@ -161,7 +174,7 @@ EncoderSlot::EncoderSlot(int device, const Layout& L, const GailCudaEncodeSettin
         alloc(dOffsets_, n * 8);
         alloc(dOutLen_, n * kMaxPasses * 4);
         alloc(dOutDist_, n * kMaxPasses * 4);
-        alloc(dOutData_, z_.arena);
+        alloc(dOutData_, z_.outCap);
         jobs_.clear();
         buildJobs(L_, dCoeffs_, dSym_, dCw_, 0, jobs_);
         auto pinned = [&](auto*& p, uint64_t bytes) {
@@ -263,7 +276,7 @@ void EncoderSlot::enqueueStages(const void* dFrame, bool taps, bool full) {
     GB_CHECK(cudaEventRecord(ev_[3], st));
     if (mark) GB_CHECK(cudaEventRecord(mark[4], st));
     CompactArgs ca{(uint32_t)n, dInfo_,    dLen_,      dDist_,   dJobs_,    dOutInfo_, dOutLen_,
-                   dOutDist_,   dOutData_, dCtl_ + 8, z_.arena, dPerm_,    dOffsets_, 0};
+                   dOutDist_,   dOutData_, dCtl_ + 8, z_.outCap, dPerm_,    dOffsets_, 0};
     compactTier1(ca, st);
     if (mark) GB_CHECK(cudaEventRecord(mark[5], st));
 }

@@ -19,7 +19,9 @@ namespace gb {
 
 // Device memory of one slot, in allocation order (also what encoder_bytes reports).
 struct SlotSizes {
-    uint64_t npix = 0, n = 0, inBytes = 0, arena = 0, llFloats = 0;
+    // outCap: the packed codewords' bound, 6 bytes per sample (beyond any 12-bit content;
+    // a frame past it fails with a status, not an overrun)
+    uint64_t npix = 0, n = 0, inBytes = 0, arena = 0, llFloats = 0, outCap = 0;
     uint64_t deviceBytes() const;
 };
 SlotSizes slotSizes(const Layout& L, const GbFrameFormat& in);
@@ -30,6 +32,9 @@ SlotSizes slotSizes(const Layout& L, const GbFrameFormat& in);
 // NULL buffers it only counts.
 uint64_t buildJobs(const Layout& L, const uint32_t* coeffs, uint8_t* sym, uint8_t* cw, uint32_t slope,
                    std::vector<T1Job>& jobs);
+// The same with each block's decision and codeword regions as offsets from the start of the
+// frame's arena (stored in the pointer fields), for arenas placed when the frame is coded.
+uint64_t buildJobOffsets(const Layout& L, const uint32_t* coeffs, uint32_t slope, std::vector<T1Job>& jobs);
 
 // Per block, the weight of its Tier-1 distortions in the PCRD hull: its band's
 // step^2 x weight, in double (as the host rate control forms it).

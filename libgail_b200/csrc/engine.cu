@@ -20,6 +20,23 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// A frame's Tier-1 jobs into a batch: the decision and codeword regions, stored as offsets,
+// become pointers into the frame's share of the batch's pools.
+__global__ void placeJobsKernel(const T1Job* src, T1Job* dst, uint32_t n, uint8_t* sym, uint8_t* cw) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T1Job j = src[i];
+    j.sym = sym + reinterpret_cast<uintptr_t>(j.sym);
+    j.cw = cw + reinterpret_cast<uintptr_t>(j.cw);
+    dst[i] = j;
+}
+
+void placeJobs(const T1Job* src, T1Job* dst, uint32_t n, uint8_t* sym, uint8_t* cw, cudaStream_t st) {
+    if (!n) return;
+    placeJobsKernel<<<(n + 255) / 256, 256, 0, st>>>(src, dst, n, sym, cw);
+    GB_CHECK(cudaGetLastError());
+}
+
 double msBetween(Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
 }
@@ -45,7 +62,8 @@ struct EncodeEngine::Slot {
     int cls = 0, index = 0;
     uint8_t* dIn = nullptr;
     uint32_t* dCoeffs = nullptr;
-    uint8_t *dSym = nullptr, *dCw = nullptr;
+    // its blocks' Tier-1 jobs; their decision and codeword regions are offsets into the
+    // frame's share of a batch's pools, made pointers when the frame joins a batch
     T1Job* dJobs = nullptr;
     uint32_t n = 0;
     // the packed Tier-1 frame, written by the device straight into mapped host memory
@@ -126,9 +144,13 @@ struct EncodeEngine::Batch {
     uint8_t* hullPasses = nullptr;
     double* hullSlope = nullptr;
     uint32_t cap = 0;
+    // the decision and codeword regions of every frame in the batch, each frame's at the
+    // offset its jobs were given (worst case of its blocks, as the arenas of a plain encoder)
+    uint8_t *symPool = nullptr, *cwPool = nullptr;
+    uint64_t poolCap = 0;
     std::vector<Request*> frames;
     bool busy = false;
-    std::vector<void*> dev;
+    std::vector<void*> dev, pools;
     // stage timing: start, after context modelling, after ordering, after MQ and
     // truncation lengths, after packing
     cudaEvent_t t[5] = {};
@@ -138,11 +160,9 @@ struct EncodeEngine::Batch {
 EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(device), maxBatch_(std::max(1, maxBatch)) {
     GB_CHECK(cudaSetDevice(dev_));
     ensureDevice();
-    if (hbmBudget == 0) {
-        size_t f = 0, t = 0;
-        GB_CHECK(cudaMemGetInfo(&f, &t));
-        hbmBudget = (uint64_t)(f * 0.9);
-    }
+    // 0: 90 % of what is free when the first slot is made (after the batches' pools, which
+    // the classes size)
+    budgetAuto_ = hbmBudget == 0;
     budget_ = hbmBudget;
     GB_CHECK(cudaStreamCreateWithFlags(&front_, cudaStreamNonBlocking));
     GB_CHECK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
@@ -188,6 +208,7 @@ EncodeEngine::~EncodeEngine() {
         for (void* p : c->dev) cudaFree(p);
     for (auto& b : batches_) {
         for (void* p : b->dev) cudaFree(p);
+        for (void* p : b->pools) cudaFree(p);
         if (b->hCtl) cudaFreeHost(b->hCtl);
         if (b->done) cudaEventDestroy(b->done);
         for (auto e : b->t)
@@ -235,21 +256,105 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
     std::memcpy(a.m, c->color.m, sizeof a.m);
     a.xyz = nullptr;
     const uint64_t n = c->z.n, npix = c->z.npix;
-    // packed output bound: codewords of 6 bytes per sample would be beyond any 12-bit content
-    c->dataCap = std::min<uint64_t>(c->z.arena, npix * 6 + (64u << 10));
-    c->slotBytes = c->z.inBytes + n * kCblkArea * 4 + 2 * c->z.arena + n * sizeof(T1Job) +
-                   n * 20 + n * kMaxPasses * (4 + 1 + 8) + c->dataCap;
+    c->dataCap = c->z.outCap;
+    c->slotBytes = c->z.inBytes + n * kCblkArea * 4 + n * sizeof(T1Job) + n * 20 + n * kMaxPasses * (4 + 1 + 8) +
+                   c->dataCap;
     if (frameBytes) *frameBytes = c->slotBytes;
-    std::lock_guard<std::mutex> lock(m_);
-    classes_.push_back(std::move(c));
-    if (csOn_ && cs_.onDevice) prepareRc();
-    return (int)classes_.size() - 1;
+    int id;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        classes_.push_back(std::move(c));
+        if (csOn_ && cs_.onDevice) prepareRc();
+        id = (int)classes_.size() - 1;
+    }
+    sizeBatches();
+    return id;
+}
+
+// Tier-1 batch tables and pools for maxBatch frames of the largest class (each pool at most
+// kPoolBytes, at least one frame: 8 frames of 4K), made while the batches are idle (at
+// set-up), so that serving does not allocate.
+constexpr uint64_t kPoolBytes = 8ull << 30;
+void EncodeEngine::sizeBatches() {
+    uint64_t blocks = 0, pool = 0;
+    int mb;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        for (auto& c : classes_) {
+            blocks = std::max<uint64_t>(blocks, c->z.n);
+            pool = std::max<uint64_t>(pool, poolShare(c->z.arena));
+        }
+        mb = maxBatch_;
+    }
+    if (!blocks) return;
+    std::lock_guard<std::mutex> lock(tablesM_);
+    for (auto& b : batches_) {
+        {
+            std::lock_guard<std::mutex> l2(m_);
+            if (b->busy) continue;  // sized by launchBatch when it next needs more
+        }
+        growBatch(*b, blocks * (uint64_t)mb, std::min<uint64_t>(pool * (uint64_t)mb, std::max<uint64_t>(pool, kPoolBytes)));
+    }
+}
+
+uint64_t EncodeEngine::poolShare(uint64_t arena) { return (arena + 255) & ~(uint64_t)255; }
+
+void EncodeEngine::growBatch(Batch& b, uint64_t blocks, uint64_t poolBytes) {
+    if (blocks > b.cap) {
+        for (void* p : b.dev) cudaFree(p);
+        b.dev.clear();
+        b.cap = 0;
+        const uint64_t cap = blocks;
+        auto alloc = [&](auto*& p, uint64_t bytes) {
+            void* q = nullptr;
+            check(cudaMalloc(&q, std::max<uint64_t>(bytes, 16)), "device memory for a Tier-1 batch");
+            b.dev.push_back(q);
+            p = static_cast<std::remove_reference_t<decltype(p)>>(q);
+        };
+        alloc(b.dJobs, cap * sizeof(T1Job));
+        alloc(b.info, cap * 16);
+        alloc(b.end, cap * kMaxPasses * 4);
+        alloc(b.len, cap * kMaxPasses * 4);
+        alloc(b.dist, cap * kMaxPasses * 4);
+        alloc(b.snaps, cap * kMaxPasses * 16);
+        alloc(b.perm, cap * 4);
+        alloc(b.work, t1WorkWords((uint32_t)cap) * 4);
+        alloc(b.offs, cap * 8);
+        alloc(b.hullPasses, cap * kMaxPasses);
+        alloc(b.hullSlope, cap * kMaxPasses * 8);
+        alloc(b.ctl, 64);
+        b.cap = (uint32_t)cap;
+    }
+    if (poolBytes > b.poolCap) {
+        for (void* p : b.pools) cudaFree(p);
+        b.pools.clear();
+        b.poolCap = 0;
+        b.symPool = b.cwPool = nullptr;
+        void* q = nullptr;
+        check(cudaMalloc(&q, poolBytes), "device memory for a Tier-1 batch's decision pool");
+        b.pools.push_back(q);
+        b.symPool = static_cast<uint8_t*>(q);
+        check(cudaMalloc(&q, poolBytes), "device memory for a Tier-1 batch's codeword pool");
+        b.pools.push_back(q);
+        b.cwPool = static_cast<uint8_t*>(q);
+        b.poolCap = poolBytes;
+    }
+}
+
+uint64_t EncodeEngine::budgetLocked() {
+    if (budgetAuto_) {
+        size_t f = 0, t = 0;
+        GB_CHECK(cudaMemGetInfo(&f, &t));
+        budget_ = used_ + (uint64_t)(f * 0.9);
+        budgetAuto_ = false;
+    }
+    return budget_;
 }
 
 EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
     {
         std::lock_guard<std::mutex> lock(budgetM_);
-        if (used_ + c.slotBytes > budget_) return nullptr;
+        if (used_ + c.slotBytes > budgetLocked()) return nullptr;
         used_ += c.slotBytes;  // reserved now, given back if the slot cannot be made
     }
     auto s = std::make_unique<Slot>();
@@ -273,8 +378,6 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
     try {
         alloc(s->dIn, c.z.inBytes);
         alloc(s->dCoeffs, (uint64_t)s->n * kCblkArea * 4);
-        alloc(s->dSym, c.z.arena);
-        alloc(s->dCw, c.z.arena);
         alloc(s->dJobs, (uint64_t)s->n * sizeof(T1Job));
         alloc(s->dInfoP, (uint64_t)s->n * 20);
         alloc(s->dLenP, (uint64_t)s->n * kMaxPasses * 4);
@@ -290,7 +393,7 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         mapped(s->hTot, 64);
         s->dataCap = c.dataCap;
         std::vector<T1Job> jobs;
-        buildJobs(c.L, s->dCoeffs, s->dSym, s->dCw, (uint32_t)s->index, jobs);
+        buildJobOffsets(c.L, s->dCoeffs, (uint32_t)s->index, jobs);
         GB_CHECK(cudaMemcpy(s->dJobs, jobs.data(), jobs.size() * sizeof(T1Job), cudaMemcpyHostToDevice));
         GB_CHECK(cudaEventCreateWithFlags(&s->frontDone, cudaEventDisableTiming));
         GB_CHECK(cudaEventCreateWithFlags(&s->upDone, cudaEventDisableTiming));
@@ -397,10 +500,13 @@ void EncodeEngine::release(int64_t id) {
 void EncodeEngine::setPolicy(int maxBatch, int minBatchPct, double maxWaitMs) {
     if (maxBatch < 1 || maxBatch > 1024 || minBatchPct < 0 || minBatchPct > 100 || !(maxWaitMs >= 0) || maxWaitMs > 1000)
         throw std::logic_error("batch policy out of range");
-    std::lock_guard<std::mutex> lock(m_);
-    maxBatch_ = maxBatch;
-    minBatchPct_ = minBatchPct;
-    maxWaitMs_ = maxWaitMs;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        maxBatch_ = maxBatch;
+        minBatchPct_ = minBatchPct;
+        maxWaitMs_ = maxWaitMs;
+    }
+    sizeBatches();
 }
 
 void EncodeEngine::setCodestream(const CodestreamConfig& c) {
@@ -488,7 +594,7 @@ EncodeEngine::DecSlot* EncodeEngine::newDecSlot(int cls) {
     }
     {
         std::lock_guard<std::mutex> lock(budgetM_);
-        if (used_ + c->slotBytes > budget_) return nullptr;
+        if (used_ + c->slotBytes > budgetLocked()) return nullptr;
         used_ += c->slotBytes;
     }
     auto d = std::make_unique<DecSlot>();
@@ -818,14 +924,20 @@ bool EncodeEngine::admit() {
 
 bool EncodeEngine::launchBatch(Batch& b) {
     std::vector<Request*> sel;
+    std::vector<uint64_t> shares;  // each frame's share of the batch's pools
     {
         std::lock_guard<std::mutex> lock(m_);
         if (front_q_.empty()) return false;
         const bool otherBusy = std::any_of(batches_.begin(), batches_.end(), [&](auto& x) { return x.get() != &b && x->busy; });
+        uint64_t pool = 0;
         for (Request* r : front_q_) {
             if ((int)sel.size() >= maxBatch_) break;
+            const uint64_t share = poolShare(classes_[r->cls]->z.arena);
+            if (!sel.empty() && pool + share > b.poolCap) break;  // the batch's pools are full
             if (cudaEventQuery(r->slot->frontDone) != cudaSuccess) break;  // in order: later ones are not done either
             sel.push_back(r);
+            shares.push_back(share);
+            pool += share;
         }
         // while the other batch keeps the GPU busy, let small batches grow a little
         if (sel.empty() || (otherBusy && (int)sel.size() < std::max(1, maxBatch_ * minBatchPct_ / 100) &&
@@ -833,40 +945,24 @@ bool EncodeEngine::launchBatch(Batch& b) {
             return false;
         front_q_.erase(front_q_.begin(), front_q_.begin() + (long)sel.size());
     }
-    uint64_t total = 0;
-    for (Request* r : sel) total += r->slot->n;
-    if (total > b.cap) {
-        // grow the batch's tables (kept for later batches)
-        for (void* p : b.dev) cudaFree(p);
-        b.dev.clear();
-        const uint64_t cap = std::max<uint64_t>(total, (uint64_t)b.cap * 2);
-        auto alloc = [&](auto*& p, uint64_t bytes) {
-            void* q = nullptr;
-            check(cudaMalloc(&q, std::max<uint64_t>(bytes, 16)), "device memory for a Tier-1 batch");
-            b.dev.push_back(q);
-            p = static_cast<std::remove_reference_t<decltype(p)>>(q);
-        };
-        alloc(b.dJobs, cap * sizeof(T1Job));
-        alloc(b.info, cap * 16);
-        alloc(b.end, cap * kMaxPasses * 4);
-        alloc(b.len, cap * kMaxPasses * 4);
-        alloc(b.dist, cap * kMaxPasses * 4);
-        alloc(b.snaps, cap * kMaxPasses * 16);
-        alloc(b.perm, cap * 4);
-        alloc(b.work, t1WorkWords((uint32_t)cap) * 4);
-        alloc(b.offs, cap * 8);
-        alloc(b.hullPasses, cap * kMaxPasses);
-        alloc(b.hullSlope, cap * kMaxPasses * 8);
-        alloc(b.ctl, 64);
-        b.cap = (uint32_t)cap;
+    std::lock_guard<std::mutex> tables(tablesM_);
+    uint64_t total = 0, pool = 0;
+    for (size_t i = 0; i < sel.size(); ++i) {
+        total += sel[i]->slot->n;
+        pool += shares[i];
     }
+    if (total > b.cap || pool > b.poolCap)  // a batch larger than set-up foresaw
+        growBatch(b, std::max<uint64_t>(total, (uint64_t)b.cap), std::max<uint64_t>(pool, b.poolCap));
     uint32_t base = 0;
-    for (Request* r : sel) {
+    uint64_t poolOff = 0;
+    for (size_t i = 0; i < sel.size(); ++i) {
+        Request* r = sel[i];
         GB_CHECK(cudaStreamWaitEvent(b.st, r->slot->frontDone, 0));
-        GB_CHECK(cudaMemcpyAsync(b.dJobs + base, r->slot->dJobs, (uint64_t)r->slot->n * sizeof(T1Job),
-                                 cudaMemcpyDeviceToDevice, b.st));
+        // the frame's jobs into the batch, their regions in its share of the pools
+        placeJobs(r->slot->dJobs, b.dJobs + base, r->slot->n, b.symPool + poolOff, b.cwPool + poolOff, b.st);
         r->jobBase = base;
         base += r->slot->n;
+        poolOff += shares[i];
     }
     GB_CHECK(cudaMemsetAsync(b.ctl, 0, 64, b.st));
     b.timed = timing_.load() && b.t[0];

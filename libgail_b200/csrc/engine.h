@@ -153,10 +153,16 @@ private:
     bool collect(Batch& b);
     Slot* newSlot(Class& c);
     DecSlot* newDecSlot(int cls);
+    void sizeBatches();
+    void growBatch(Batch& b, uint64_t blocks, uint64_t poolBytes);
+    static uint64_t poolShare(uint64_t arena);
+    uint64_t budgetLocked();  // under budgetM_
 
     int dev_;
     uint64_t budget_ = 0, used_ = 0;  // used_ under budgetM_
+    bool budgetAuto_ = false;        // budget_ set when the first slot is made
     std::mutex budgetM_;
+    std::mutex tablesM_;             // the batches' tables and pools while they are set up
     int maxBatch_;
     int minBatchPct_ = 25;
     double maxWaitMs_ = 2.0;
