@@ -66,8 +66,8 @@ DECODE_FRAMES = 48  # codestreams per profile of the decode configuration
 # DRAM bytes: ncu counters smsp__inst_executed.sum and dram__bytes_read.sum +
 # dram__bytes_write.sum of this build, divided by the frames in the launch. The achieved
 # issue rate in the roofline divides them by the launch time measured in the run.
-CM_WARP_INSTR_PER_FRAME = 912.5e6
-CM_DRAM_BYTES_PER_FRAME = 214.29e6
+CM_WARP_INSTR_PER_FRAME = 685.89e6
+CM_DRAM_BYTES_PER_FRAME = 220.35e6
 
 
 def parse():

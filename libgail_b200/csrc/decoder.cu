@@ -197,8 +197,7 @@ __device__ __forceinline__ uint32_t nbKey(uint32_t U, uint32_t M, uint32_t D, in
 struct BlockCtx {
     uint32_t* sig;  // significance rows -1..32 at index y + 1
     uint32_t* sgn;  // sign rows, the same indexing
-    uint32_t* out;  // the block's top-left word in the plane
-    uint32_t W;
+    uint32_t* words;  // the block's decoded words, 32 per row (shared memory)
     const uint8_t* zk;  // zero-coding context by neighbour key, this block's orientation
     const uint8_t* sk;  // sign context | xor bit << 5 by the sign key
     const uint32_t* tab;
@@ -217,13 +216,19 @@ struct BlockCtx {
         M |= 1u << x;
         sig[y + 1] = M;
         sgn[y + 1] = GM | (neg << x);
-        out[(size_t)y * W + x] = (neg << 31) | (3u << p);
+        words[y * 32 + x] = (neg << 31) | (3u << p);
     }
 };
 
 __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
     // per block: significance and sign of rows -1..32, coded-this-plane and refined rows 0..31
     __shared__ uint32_t s_sig[34], s_sgn[34], s_vis[32], s_ref[32];
+    // the block's decoded words (sign, twice the magnitude plus the mid-point of the planes
+    // not decoded), kept here and turned into floats in the plane when the block is done:
+    // each refinement updates its word, and a global read-modify-write per refinement put a
+    // memory round trip on the decoder's serial chain. Only significant samples' words are
+    // ever read, and each is written when its sample becomes significant.
+    __shared__ uint32_t s_word[32 * 32];
     __shared__ uint32_t s_ctx[19];
     __shared__ uint32_t s_tab[48];
     __shared__ uint8_t s_zc[4 * 45], s_sc[16];
@@ -255,7 +260,6 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
     b.sk = s_sk;
     b.tab = s_tab;
     b.ctx = s_ctx;
-    b.W = a.W;
     const uint32_t count = a.ctl[2], heavy = a.ctl[3];
     auto decodeBlock = [&](uint32_t j) {
         const DecBlock blk = a.blocks[j];
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
         const int nbps = code.nbps;
         const bool valid = code.passes > 0 && nbps >= 1 && nbps <= 30 && (uint64_t)code.offset + code.len <= a.size;
         if (!valid) return;
-        b.out = out;
+        b.words = s_word;
         b.zk = s_zk + 512 * blk.orient;
         for (int i = 0; i < 34; ++i) s_sig[i] = s_sgn[i] = 0;
         for (int i = 0; i < 32; ++i) s_vis[i] = s_ref[i] = 0;
@@ -327,7 +331,7 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                                     const uint32_t ref = s_ref[y];
                                     const int cx = bt(ref, x) ? 16 : (nbKey(U, M, D, x) ? 15 : 14);
                                     const uint32_t bit = b.mq.decode(s_ctx, cx, s_tab);
-                                    uint32_t& word = out[(size_t)y * a.W + x];
+                                    uint32_t& word = s_word[y * 32 + x];
                                     word = bit ? word + (1u << p) : word - (1u << p);
                                     s_ref[y] = ref | (1u << x);
                                 }
@@ -380,14 +384,14 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
             }
             for (int i = 0; i < 32; ++i) s_vis[i] = 0;
         }
-        // dequantise in place, the significant samples only (every other word is 0,
-        // which is 0.0f): word * step / 2, sign from bit 31
+        // dequantise into the plane, the significant samples only (every other sample
+        // is 0, which is 0.0f): word * step / 2, sign from bit 31
         const float half = a.half[blk.band];
         float* f = reinterpret_cast<float*>(out);
         for (int y = 0; y < h; ++y)
             for (uint32_t m = s_sig[y + 1] & wmask; m; m &= m - 1) {
                 const int x = __ffs(m) - 1;
-                const uint32_t v = out[(size_t)y * a.W + x];
+                const uint32_t v = s_word[y * 32 + x];
                 const float mag = (float)(v & 0x7FFFFFFFu) * half;
                 f[(size_t)y * a.W + x] = (v & 0x80000000u) ? -mag : mag;
             }

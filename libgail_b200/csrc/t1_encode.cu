@@ -535,6 +535,54 @@ __global__ void __launch_bounds__(1024) t1OrderKernel(T1Launch P, uint32_t maxSo
         P.perm[atomicAdd(&hist[orderBucket(P.info[4 * (size_t)i + 2])], 1u)] = i;
 }
 
+// Words of a launch's work area the wide ordering uses (those of the persistent launch's
+// solo count and bucket histogram: a launch is one or the other).
+constexpr uint32_t kWSoloWide = 2, kWHistWide = 16;
+
+// The same ordering over the whole GPU, for launches with a work area (the histogram and the
+// solo count in its words kWHist / kWSolo, zeroed before): per-CTA histograms summed into
+// the work area, one warp's exclusive scan of it, then a scatter through the bucket cursors.
+// Blocks within a bucket land in any order, as in the one-CTA form (the order only decides
+// which lane codes a block when, never its bytes).
+__global__ void __launch_bounds__(256) t1OrderCountKernel(T1Launch P) {
+    __shared__ uint32_t hist[ORDER_BUCKETS];
+    __shared__ uint32_t solo;
+    for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
+    if (threadIdx.x == 0) solo = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        const uint32_t d = P.info[4 * (size_t)i + 2];
+        atomicAdd(&hist[orderBucket(d)], 1u);
+        if (d >= P.soloDecisions) atomicAdd(&solo, 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < ORDER_BUCKETS; b += blockDim.x)
+        if (hist[b]) atomicAdd(P.work + kWHistWide + b, hist[b]);
+    if (threadIdx.x == 0 && solo) atomicAdd(P.work + kWSoloWide, solo);
+}
+
+__global__ void __launch_bounds__(32) t1OrderScanKernel(T1Launch P, uint32_t maxSolo) {
+    const int lane = threadIdx.x;
+    uint32_t* hist = P.work + kWHistWide;
+    uint32_t v[4], s = 0;
+    for (int k = 0; k < 4; ++k) {
+        v[k] = hist[4 * lane + k];
+        s += v[k];
+    }
+    const uint32_t incl = warpScan(s, lane);
+    uint32_t run = incl - s;
+    for (int k = 0; k < 4; ++k) {
+        hist[4 * lane + k] = run;
+        run += v[k];
+    }
+    if (lane == 0) P.ctl[3] = min(P.work[kWSoloWide], maxSolo);
+}
+
+__global__ void __launch_bounds__(256) t1OrderScatterKernel(T1Launch P) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x)
+        P.perm[atomicAdd(P.work + kWHistWide + orderBucket(P.info[4 * (size_t)i + 2]), 1u)] = i;
+}
+
 // ---------------------------------------------------------------------------- MQ coding
 // Context state word: Qe | MPS << 16 | state index << 17. nextStateEntry(k), k = state
 // index << 2 | MPS << 1 | LPS: the state word after a renormalising decision; the coder keeps
@@ -631,6 +679,7 @@ enum : uint32_t {
     kWList = 16 + ORDER_BUCKETS,
 };
 static_assert(kWList == kT1WorkHead, "work layout");
+static_assert(kWSoloWide == kWSolo && kWHistWide == kWHist, "the wide ordering's words");
 
 // Loads of what other warps of a persistent launch wrote during the launch, into lines an
 // SM may have read before (the info words, MQ states and codewords that truncation reads)
@@ -1108,7 +1157,16 @@ void t1Encode(const T1Launch& launch, cudaStream_t st, cudaEvent_t* marks) {
     // blocks end early take more from the queue
     const bool wide = divUp(L.n, MQ_THREADS) > (uint32_t)sms * 4u;
     const uint32_t mqBlocks = min(divUp(L.n, MQ_THREADS * (wide ? 2u : 1u)), (uint32_t)sms * L.mqCtasPerSm);
-    t1OrderKernel<<<1, 1024, 0, st>>>(L, mqBlocks * (MQ_THREADS / 32) / 2);
+    const uint32_t maxSolo = mqBlocks * (MQ_THREADS / 32) / 2;
+    if (L.work) {  // over the whole GPU: a batch of frames has 100,000 blocks and more
+        const uint32_t og = min(divUp(L.n, 256u), (uint32_t)sms * 2u);
+        GB_CHECK(cudaMemsetAsync(L.work, 0, kT1WorkHead * 4, st));
+        t1OrderCountKernel<<<og, 256, 0, st>>>(L);
+        t1OrderScanKernel<<<1, 32, 0, st>>>(L, maxSolo);
+        t1OrderScatterKernel<<<og, 256, 0, st>>>(L);
+    } else {
+        t1OrderKernel<<<1, 1024, 0, st>>>(L, maxSolo);
+    }
     if (marks) GB_CHECK(cudaEventRecord(marks[1], st));
     if (!wide) t1MqKernel<1><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
     else t1MqKernel<10><<<mqBlocks, MQ_THREADS, 0, st>>>(L);
