@@ -318,27 +318,40 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                             }
                         }
                     } else if (type == 1) {  // magnitude refinement
+                        // nothing changes significance in this pass, so every sample's context
+                        // is known before it: per row of the stripe, the samples to refine
+                        // (significant before this plane, not coded in it), those refined
+                        // before (context 16) and those with a significant neighbour (15,
+                        // else 14); per column their four rows as nibbles
+                        uint32_t e4[4] = {0, 0, 0, 0}, r4[4] = {0, 0, 0, 0}, n4[4] = {0, 0, 0, 0};
                         uint32_t cm = 0;
-                        for (int k = 0; k < n; ++k) cm |= s_sig[y0 + k + 1] & ~s_vis[y0 + k];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            if (k >= n) break;
+                            const uint32_t U = s_sig[y0 + k], M = s_sig[y0 + k + 1], D = s_sig[y0 + k + 2];
+                            e4[k] = M & ~s_vis[y0 + k];
+                            r4[k] = s_ref[y0 + k];
+                            n4[k] = U | (U << 1) | (U >> 1) | (M << 1) | (M >> 1) | D | (D << 1) | (D >> 1);
+                            cm |= e4[k];
+                        }
                         while (cm) {
                             const int x = __ffs(cm) - 1;
                             cm &= cm - 1;
-                            uint32_t U = s_sig[y0], M = s_sig[y0 + 1];
-                            for (int k = 0; k < n; ++k) {
-                                const int y = y0 + k;
-                                const uint32_t D = s_sig[y + 2];
-                                if (bt(M & ~s_vis[y], x)) {
-                                    const uint32_t ref = s_ref[y];
-                                    const int cx = bt(ref, x) ? 16 : (nbKey(U, M, D, x) ? 15 : 14);
-                                    const uint32_t bit = b.mq.decode(s_ctx, cx, s_tab);
-                                    uint32_t& word = s_word[y * 32 + x];
-                                    word = bit ? word + (1u << p) : word - (1u << p);
-                                    s_ref[y] = ref | (1u << x);
-                                }
-                                U = M;
-                                M = D;
+                            const uint32_t ec = bt(e4[0], x) | bt(e4[1], x) << 1 | bt(e4[2], x) << 2 | bt(e4[3], x) << 3;
+                            const uint32_t rc = bt(r4[0], x) | bt(r4[1], x) << 1 | bt(r4[2], x) << 2 | bt(r4[3], x) << 3;
+                            const uint32_t nc = bt(n4[0], x) | bt(n4[1], x) << 1 | bt(n4[2], x) << 2 | bt(n4[3], x) << 3;
+                            for (uint32_t m = ec; m; m &= m - 1) {
+                                const int k = __ffs(m) - 1;
+                                const int cx = bt(rc, k) ? 16 : (bt(nc, k) ? 15 : 14);
+                                const uint32_t bit = b.mq.decode(s_ctx, cx, s_tab);
+                                uint32_t& word = s_word[(y0 + k) * 32 + x];
+                                word = bit ? word + (1u << p) : word - (1u << p);
                             }
                         }
+                        // every sample refined here counts as refined from now on
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (k < n) s_ref[y0 + k] = r4[k] | e4[k];
                     } else {  // cleanup, with run-length coding of quiet columns
                         uint32_t cm = 0, any = s_sig[y0], vis = 0;
                         for (int k = 0; k < n; ++k) {
@@ -571,7 +584,8 @@ uint64_t decoderSlotBytes(const Layout& L, const GailCudaDecodeSettings& s) {
     return npix * 12 + 2 * ll * 12 + out + (uint64_t)L.numCblks() * (12 + 12 + 4) + (4ull << 20);
 }
 
-DecoderSlot::DecoderSlot(int device, const Layout& L, const GailCudaDecodeSettings& s) : dev_(device), L_(L), s_(s) {
+DecoderSlot::DecoderSlot(int device, const Layout& L, const GailCudaDecodeSettings& s, bool heavySms) : dev_(device), L_(L), s_(s) {
+    heavySms_ = heavySms;
     if (s.reduce < 0 || s.reduce > L.levels) throw std::runtime_error("more resolution levels left out than the stream has");
     outW_ = L.levelW(s.reduce);
     outH_ = L.levelH(s.reduce);
@@ -706,7 +720,7 @@ void DecoderSlot::enqueue(const Layout& frame, const uint8_t* data, size_t size,
     const Tuning tu = tuningFor(L_.profile);
     const uint32_t grid = std::min<uint32_t>((uint32_t)n, (uint32_t)(sms * tu.decCtasPerSm));
     DecArgs da{dBytes_, size, dCodes_, dBlocks_, (uint32_t)n, dHalf_, (uint32_t*)dPlanes_, (uint32_t)L_.width, dPerm_, dCtl_,
-               grid, (uint32_t)tu.decHeavyPct};
+               grid, heavySms_ ? (uint32_t)tu.decHeavyPct : 0u};
     orderKernel<<<1, 1024, 0, st>>>(da);
     decodeKernel<<<grid, DEC_THREADS, 0, st>>>(da);
     GB_CHECK(cudaGetLastError());

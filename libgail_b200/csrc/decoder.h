@@ -29,7 +29,10 @@ void decoderInit();
 
 class DecoderSlot {
 public:
-    DecoderSlot(int device, const Layout& L, const GailCudaDecodeSettings& s);
+    // heavySms: decode the heaviest code-blocks on SMs of their own (the tuning's decHeavyPct),
+    // for a decode that has the GPU to itself; slots of which several decode at once (the
+    // served engine's) leave it off, as their launches would all reserve the same SMs.
+    DecoderSlot(int device, const Layout& L, const GailCudaDecodeSettings& s, bool heavySms = true);
     ~DecoderSlot();
     DecoderSlot(const DecoderSlot&) = delete;
     DecoderSlot& operator=(const DecoderSlot&) = delete;
@@ -53,6 +56,7 @@ private:
     Layout L_;
     GailCudaDecodeSettings s_;
     int outW_ = 0, outH_ = 0;
+    bool heavySms_ = true;
     cudaStream_t st_ = nullptr;
     cudaEvent_t ev_[4] = {};
     std::vector<void*> allocs_;

@@ -600,7 +600,7 @@ EncodeEngine::DecSlot* EncodeEngine::newDecSlot(int cls) {
     auto d = std::make_unique<DecSlot>();
     d->cls = cls;
     try {
-        d->slot = std::make_unique<DecoderSlot>(dev_, c->L, c->s);
+        d->slot = std::make_unique<DecoderSlot>(dev_, c->L, c->s, false);  // several decode at once
     } catch (...) {
         std::lock_guard<std::mutex> lock(budgetM_);
         used_ -= c->slotBytes;
