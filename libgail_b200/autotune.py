@@ -21,7 +21,7 @@ import numpy as np
 from . import check, lib
 
 DEFAULTS = {"soloDecisions": 16384, "cmCtasPerSm": 16, "mqCtasPerSm": 16, "decCtasPerSm": 32, "t1Persistent": 0,
-            "decHeavyPct": 250}
+            "decHeavyPct": 150}
 POLICY_DEFAULT = {"maxBatch": 16, "minBatchPct": 25, "maxWaitMs": 2.0}
 PROFILES = {"2k": 0, "4k": 1}
 

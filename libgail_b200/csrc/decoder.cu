@@ -118,13 +118,34 @@ __global__ void __launch_bounds__(1024) orderKernel(DecArgs a) {
         if (a.blocks[i].wanted) a.perm[atomicAdd(&hist[lenBucket(a.codes[i].len)], 1u)] = i;
 }
 
-// MQ decoder (ISO/IEC 15444-1 C.3) over one codeword; bytes past its end read as 0xFF.
+// A block's first kCwCache codeword bytes are copied into shared memory before it is decoded.
+constexpr uint32_t kCwCache = 2048;
+
+// MQ decoder (ISO/IEC 15444-1 C.3) over one codeword; bytes past its end read as 0xFF. The
+// first `cached` bytes come from the shared-memory copy, so that a byte-in on the serial chain
+// does not wait for global memory.
 struct MqDecoder {
-    uint32_t A, C, bp, end;
+    uint32_t A, C, bp, end, cached;
     int CT;
     const uint8_t* in;
+    const uint8_t* cache;
 
-    __device__ __forceinline__ uint32_t at(uint32_t i) const { return i < end ? (uint32_t)in[i] : 0xFFu; }
+    __device__ __forceinline__ uint32_t at(uint32_t i) const {
+        return i < cached ? (uint32_t)cache[i] : (i < end ? (uint32_t)in[i] : 0xFFu);
+    }
+    // The decision in context state t when it is its context's MPS, 0, with no renormalisation:
+    // then only the interval changes (the context keeps its state), and it is made here; false
+    // (nothing changed) otherwise.
+    __device__ __forceinline__ bool fastZero(uint32_t t) {
+        const uint32_t qe = t & 0xFFFFu;
+        if ((t >> 16) & 1u) return false;
+        if ((C >> 16) < qe) return false;
+        const uint32_t a = A - qe;
+        if (!(a & 0x8000u)) return false;
+        A = a;
+        C -= qe << 16;
+        return true;
+    }
     __device__ __forceinline__ void bytein() {
         const uint32_t b = at(bp), b1 = at(bp + 1);
         if (b == 0xFFu) {
@@ -142,9 +163,11 @@ struct MqDecoder {
             CT = 8;
         }
     }
-    __device__ __forceinline__ void init(const uint8_t* data, uint32_t len) {
+    __device__ __forceinline__ void init(const uint8_t* data, uint32_t len, const uint8_t* copy, uint32_t copied) {
         in = data;
         end = len;
+        cache = copy;
+        cached = copied;
         bp = 0;
         C = at(0) << 16;
         bytein();
@@ -231,6 +254,7 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
     __shared__ uint32_t s_word[32 * 32];
     __shared__ uint32_t s_ctx[19];
     __shared__ uint32_t s_tab[48];
+    __shared__ uint8_t s_cw[kCwCache];  // the block's codeword, its first kCwCache bytes
     __shared__ uint8_t s_zc[4 * 45], s_sc[16];
     // zero coding by orientation and neighbour key (nbKey); sign coding by the sign key:
     // bits 0/1 left neighbour significant/negative, 2/3 right, 4/5 above, 6/7 below
@@ -253,7 +277,7 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
         s_sk[k] = s_sc[(hc + 1) * 3 + (vc + 1)];
     }
     __syncthreads();
-    if (threadIdx.x != 0) return;  // lane 0 decodes; the tables above were built by the whole warp
+    const uint32_t lane = threadIdx.x;
     BlockCtx b;
     b.sig = s_sig;
     b.sgn = s_sgn;
@@ -277,7 +301,7 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
         s_ctx[0] = s_tab[4];
         s_ctx[17] = s_tab[3];
         s_ctx[18] = s_tab[46];
-        b.mq.init(a.bytes + code.offset, code.len);
+        b.mq.init(a.bytes + code.offset, code.len, s_cw, min(code.len, kCwCache));
         const uint32_t wmask = w >= 32 ? 0xFFFFFFFFu : (1u << w) - 1u;
         int done = 0;
         const int passes = code.passes;
@@ -363,7 +387,19 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                         any |= s_sig[y0 + n + 1];
                         cm &= wmask;
                         while (cm) {
-                            const int x = __ffs(cm) - 1;
+                            int x = __ffs(cm) - 1;
+                            if (n == 4) {
+                                // quiet columns whose run-length decision is a 0 that is its
+                                // context's MPS and needs no renormalisation: nothing in them,
+                                // and only the interval changes
+                                const uint32_t t17 = s_ctx[17];
+                                while (!win3(any, x) && !bt(vis, x) && b.mq.fastZero(t17)) {
+                                    cm &= cm - 1;
+                                    if (!cm) break;
+                                    x = __ffs(cm) - 1;
+                                }
+                                if (!cm) break;
+                            }
                             cm &= cm - 1;
                             int r = 0;
                             // quiet column: nothing significant in rows y0-1..y0+4 around it and
@@ -410,25 +446,46 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
             }
     };
 
-    // the heavy blocks (the first of the order): on a reserved SM (%smid below the reserved
-    // count), the first four warps to arrive take one each and every other warp leaves, so
-    // that the SM runs their serial chains alone
+    // Every lane stays: lane 0 picks each block and decodes it, the others first copy its
+    // codeword into shared memory with it. The heavy blocks (the first of the order): on a
+    // reserved SM (%smid below the reserved count), the first four warps to arrive take one
+    // each and every other warp leaves, so that the SM runs their serial chains alone; the
+    // other warps take blocks from the queue, then any heavy block no reserved SM's warp took
+    // (a grid that did not reach every reserved SM).
     uint32_t smid;
     asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
     const uint32_t reserved = (heavy + 3) / 4;
-    if (smid < reserved) {
-        const uint32_t k = atomicAdd(a.ctl + kCtlArrive + smid, 1u), hi = 4 * smid + k;
-        if (k < 4 && hi < heavy && atomicExch(a.ctl + kCtlClaim + hi, 1u) == 0) decodeBlock(a.perm[hi]);
-        return;
-    }
+    int phase = smid < reserved ? 0 : 1;  // 0 reserved SM, 1 queue, 2 unclaimed heavy blocks, 3 done
+    uint32_t fb = 0;
     for (;;) {
-        const uint32_t q = heavy + atomicAdd(a.ctl, 1u);  // longest codewords first
-        if (q >= count) break;
-        decodeBlock(a.perm[q]);
+        uint32_t j = 0xFFFFFFFFu;
+        if (lane == 0) {
+            if (phase == 0) {
+                const uint32_t k = atomicAdd(a.ctl + kCtlArrive + smid, 1u), hi = 4 * smid + k;
+                if (k < 4 && hi < heavy && atomicExch(a.ctl + kCtlClaim + hi, 1u) == 0) j = a.perm[hi];
+                phase = 3;
+            } else if (phase == 1) {
+                const uint32_t q = heavy + atomicAdd(a.ctl, 1u);  // longest codewords first
+                if (q < count) j = a.perm[q];
+                else phase = 2;
+            }
+            if (phase == 2) {
+                while (fb < heavy && atomicExch(a.ctl + kCtlClaim + fb, 1u) != 0) ++fb;
+                if (fb < heavy) j = a.perm[fb++];
+                else phase = 3;
+            }
+        }
+        j = __shfl_sync(kFull, j, 0);
+        if (j == 0xFFFFFFFFu) break;
+        const GbCblkCode code = a.codes[j];
+        if ((uint64_t)code.offset + code.len <= a.size) {
+            const uint8_t* src = a.bytes + code.offset;
+            for (uint32_t i = lane; i < min(code.len, kCwCache); i += 32) s_cw[i] = src[i];
+        }
+        __syncwarp();
+        if (lane == 0) decodeBlock(j);
+        __syncwarp();
     }
-    // heavy blocks no reserved SM's warp took (a grid that did not reach every reserved SM)
-    for (uint32_t hi = 0; hi < heavy; ++hi)
-        if (atomicExch(a.ctl + kCtlClaim + hi, 1u) == 0) decodeBlock(a.perm[hi]);
 }
 
 // ---------------------------------------------------------------------------- inverse DWT

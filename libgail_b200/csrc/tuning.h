@@ -12,7 +12,7 @@ struct Tuning {
     int mqCtasPerSm = 16;            // MQ grid cap
     int decCtasPerSm = 32;           // Tier-1 decode grid cap
     int t1Persistent = 0;            // Tier-1 encode as one persistent launch (1) or four (0)
-    int decHeavyPct = 250;           // Tier-1 decode: blocks above this % of the mean codeword bytes per
+    int decHeavyPct = 150;           // Tier-1 decode: blocks above this % of the mean codeword bytes per
                                      // warp run on SMs of their own (0: none)
 };
 
