@@ -85,6 +85,12 @@ GB_API int gb_make_layout(int width, int height, int fourk, double baseStep, GbS
  * ColorConverter's lut()/params() (src/core/color.h:105-108). Any pointer may be NULL. */
 GB_API int gb_color_tables(const GailCudaColor* color, float* eotf65536, float* matrix9, float* thresholds4096);
 
+/* The colour route of a setting (0 direct, 1 tone map and / or gamut compression, 2 3D
+ * LUT), its constants in the positions of the reference's 48-float parameter block
+ * (src/kernels/color_params.h; ColorConverter::params(), src/core/color.h:106) and the LUT's
+ * nodes per axis (0 without one). A LUT given by path is read. route and lutN may be NULL. */
+GB_API int gb_color_route(const GailCudaColor* color, float* params48, int32_t* route, int32_t* lutN);
+
 /* Launch tuning per frame profile (0 = 2K, 1 = 4K), read by every launch of that profile
  * made after the call (plain encoders and decoders, engine batches). No counterpart in the
  * reference, whose launch shapes are fixed; libgail_b200/autotune.py measures candidates

@@ -33,6 +33,36 @@ GB_API int gb_color_tables(const GailCudaColor* color, float* eotf65536, float* 
     });
 }
 
+GB_API int gb_color_route(const GailCudaColor* color, float* params48, int32_t* route, int32_t* lutN) {
+    return gbGuard([&] {
+        if (!color || !params48) throw std::logic_error("null argument");
+        const ColorTables t = buildColorTables(*color);
+        const ToneParams& p = t.tone;
+        // the reference's parameter-block positions (kernels/color_params.h)
+        float* o = params48;
+        std::memset(o, 0, 48 * 4);
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) o[4 * r + c] = t.m[3 * r + c];
+        o[12] = (float)p.tone;
+        o[13] = p.srcRef;
+        o[14] = p.gain;
+        o[15] = p.knee;
+        o[16] = p.shoulderT;
+        o[17] = p.peak;
+        o[18] = (float)p.gamut;
+        o[19] = p.gamutThresh;
+        std::memcpy(o + 20, p.toTarget, 36);
+        std::memcpy(o + 29, p.fromTarget, 36);
+        o[38] = (float)t.lutN;
+        o[39] = p.pqSrcMax;
+        o[40] = p.pqMaxLum;
+        o[41] = p.pqKs;
+        o[42] = (float)p.norm;
+        if (route) *route = t.route;
+        if (lutN) *lutN = t.lutN;
+    });
+}
+
 GB_API int gb_set_tuning(int profile, const GbTuning* t) {
     return gbGuard([&] {
         if (!t) {

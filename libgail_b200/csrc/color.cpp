@@ -1,10 +1,15 @@
-// Colour tables (host side): EOTF, primaries matrix, 12-bit encoding thresholds.
+// Colour tables (host side): EOTF, primaries matrix, 12-bit encoding thresholds, the
+// managed route's tone-map and gamut constants, application 3D LUTs.
 #include "color.h"
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
+#include <string>
 
 namespace gb {
 
@@ -19,6 +24,14 @@ double pqEotf(double e) {
     e = std::clamp(e, 0.0, 1.0);
     const double p = std::pow(e, 1.0 / m2);
     return 10000.0 * std::pow(std::max(p - c1, 0.0) / (c2 - c3 * p), 1.0 / m1);
+}
+
+// Its inverse: cd/m^2 -> PQ signal in [0, 1].
+double pqInverseEotf(double nits) {
+    const double m1 = 2610.0 / 16384.0, m2 = 2523.0 / 4096.0 * 128.0, c1 = 3424.0 / 4096.0, c2 = 2413.0 / 4096.0 * 32.0,
+                 c3 = 2392.0 / 4096.0 * 32.0;
+    const double y = std::pow(std::clamp(nits / 10000.0, 0.0, 1.0), m1);
+    return std::pow((c1 + c2 * y) / (1.0 + c3 * y), m2);
 }
 
 // ITU-R BT.2100 HLG inverse OETF.
@@ -72,14 +85,69 @@ void rgbToXyz(int primaries, double M[9]) {
 
 int dciCode(float n) { return (int)std::floor(4095.0f * std::pow(n, 1.0f / 2.6f) + 0.5f); }
 
+namespace {
+
+// Parses up to `want` numbers from the start of s (spaces between, anything after the last
+// ignored); returns how many it read.
+int leadingFloats(const char* s, float* out, int want) {
+    int got = 0;
+    while (got < want) {
+        while (*s == ' ' || *s == '\t') ++s;
+        if (!(std::isdigit((unsigned char)*s) || *s == '-' || *s == '+' || *s == '.')) break;
+        char* end = nullptr;
+        const float v = std::strtof(s, &end);
+        if (end == s) break;
+        out[got++] = v;
+        s = end;
+    }
+    return got;
+}
+
+}  // namespace
+
+std::vector<float> readCube(const char* path, int32_t& n) {
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) throw std::runtime_error(std::string("cannot open LUT ") + path);
+    std::string text;
+    char buf[1 << 16];
+    for (size_t got; (got = std::fread(buf, 1, sizeof buf, f)) > 0;) text.append(buf, got);
+    std::fclose(f);
+    std::vector<float> nodes;
+    n = 0;
+    size_t at = 0;
+    while (at < text.size()) {
+        size_t eol = text.find('\n', at);
+        if (eol == std::string::npos) eol = text.size();
+        const std::string line = text.substr(at, eol - at);
+        at = eol + 1;
+        if (line.empty() || line[0] == '#') continue;
+        const size_t k0 = line.find_first_not_of(" \t\r");
+        if (k0 == std::string::npos) continue;
+        const size_t k1 = std::min(line.find_first_of(" \t\r", k0), line.size());
+        const std::string key = line.substr(k0, k1 - k0);
+        const char* rest = line.c_str() + k1;
+        if (key == "LUT_3D_SIZE") {
+            n = (int32_t)std::strtol(rest, nullptr, 10);
+        } else if (key == "LUT_1D_SIZE") {
+            throw std::runtime_error(std::string("1D .cube LUTs are not supported: ") + path);
+        } else if (key == "DOMAIN_MIN" || key == "DOMAIN_MAX") {
+            float d[3];
+            const float want = key == "DOMAIN_MIN" ? 0.f : 1.f;
+            if (leadingFloats(rest, d, 3) != 3 || d[0] != want || d[1] != want || d[2] != want)
+                throw std::runtime_error(std::string("LUT domain must be 0..1: ") + path);
+        } else if (key != "TITLE") {
+            float v[3];
+            if (leadingFloats(line.c_str(), v, 3) == 3) nodes.insert(nodes.end(), v, v + 3);
+        }
+    }
+    if (n < 2 || nodes.size() != (size_t)n * n * n * 3)
+        throw std::runtime_error(std::string("malformed 3D LUT (size / entry count) in ") + path);
+    return nodes;
+}
+
 ColorTables buildColorTables(const GailCudaColor& c) {
-    if (c.lut3dSize > 0 || (c.lut3d && c.lut3d[0]) || c.lut3dData)
-        throw std::logic_error("3D LUT colour conversion is not implemented on this backend");
     const bool hdr = c.transfer == 2 || c.transfer == 3;
     const bool passthrough = c.primaries == 4;
-    if (hdr && !passthrough && (c.toneMap == 1 || c.toneMap == 2))
-        throw std::logic_error("the shoulder and BT.2390 tone maps are not implemented on this backend");
-    if (!passthrough && c.gamut != 2) throw std::logic_error("gamut compression is not implemented on this backend");
     ColorTables t;
     t.eotf.resize(65536);
     for (int i = 0; i < 65536; ++i) {
@@ -99,6 +167,49 @@ ColorTables buildColorTables(const GailCudaColor& c) {
     double M[9];
     rgbToXyz(c.primaries, M);
     for (int i = 0; i < 9; ++i) t.m[i] = (float)M[i];
+    // the managed route's constants (ColorConverter's parameter block, core/color.cpp:344-388)
+    ToneParams& tp = t.tone;
+    tp.peak = (float)c.cinemaPeak;
+    if (hdr && !passthrough && c.toneMap == 1) {
+        const double gain = c.cinemaRefWhite / c.cinemaPeak;
+        const double vmax = gain * c.hdrPeak / c.hdrRefWhite;  // the source peak on the output scale
+        const double knee = vmax <= 1.0 ? 1.0 : std::clamp(c.knee, 0.05, 0.99);
+        tp.tone = 1;
+        tp.srcRef = (float)c.hdrRefWhite;
+        tp.gain = (float)gain;
+        tp.knee = (float)knee;
+        tp.shoulderT = (float)std::max(1e-3, (vmax - knee) / (1.0 - knee));
+    } else if (hdr && !passthrough && c.toneMap == 2 && c.hdrPeak > c.cinemaPeak) {
+        tp.tone = 2;
+        tp.pqSrcMax = (float)pqInverseEotf(c.hdrPeak);
+        tp.pqMaxLum = (float)(pqInverseEotf(c.cinemaPeak) / pqInverseEotf(c.hdrPeak));
+        tp.pqKs = std::max(0.f, 1.5f * tp.pqMaxLum - 0.5f);
+    }
+    tp.norm = c.toneNorm == 0 ? 2 : c.toneNorm == 1 ? 1 : 0;
+    if (!passthrough) {
+        double T[9], Ti[9];
+        rgbToXyz(c.gamut == 1 ? 3 : 2, T);  // DCI-P3 or P3-D65 projector primaries
+        invert3(T, Ti);
+        for (int i = 0; i < 9; ++i) {
+            tp.toTarget[i] = (float)(Ti[i] / c.cinemaPeak);
+            tp.fromTarget[i] = (float)(T[i] * c.cinemaPeak);
+        }
+        if (c.gamut != 2) {
+            tp.gamut = 1;
+            tp.gamutThresh = (float)std::clamp(c.gamutThreshold, 0.0, 0.99);
+        }
+    }
+    if (tp.tone != 0 || tp.gamut != 0) t.route = kRouteManaged;
+    // an application LUT replaces everything above: in memory, else from a .cube file
+    if (c.lut3dData && c.lut3dCount > 0) {
+        if (c.lut3dSize < 2 || c.lut3dCount != (uint64_t)c.lut3dSize * c.lut3dSize * c.lut3dSize * 3)
+            throw std::runtime_error("3D LUT data does not match its size");
+        t.lut3.assign(c.lut3dData, c.lut3dData + c.lut3dCount);
+        t.lutN = c.lut3dSize;
+    } else if (c.lut3d && c.lut3d[0]) {
+        t.lut3 = readCube(c.lut3d, t.lutN);
+    }
+    if (t.lutN > 1) t.route = kRouteLut;
     // thresholds by bisection on the float bit patterns of [0, 1] (the code is
     // non-decreasing in n; the tests check every threshold against its neighbours)
     t.thr.assign(4096, 0.f);

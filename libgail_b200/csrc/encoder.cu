@@ -155,6 +155,7 @@ EncoderSlot::EncoderSlot(int device, const Layout& L, const GailCudaEncodeSettin
         alloc(dIn_, z_.inBytes);
         alloc(dEotf_, 65536 * 4);
         alloc(dThr_, 4096 * 4);
+        alloc(dLut_, color_.lut3.size() * 4);
         alloc(dLL_[0], z_.llFloats * 4 * 3);
         alloc(dLL_[1], z_.llFloats * 4 * 3);
         alloc(dCoeffs_, n * kCblkArea * 4);
@@ -231,6 +232,8 @@ void EncoderSlot::release() {
 void EncoderSlot::uploadStatic() {
     GB_CHECK(cudaMemcpy(dEotf_, color_.eotf.data(), 65536 * 4, cudaMemcpyHostToDevice));
     GB_CHECK(cudaMemcpy(dThr_, color_.thr.data(), 4096 * 4, cudaMemcpyHostToDevice));
+    if (!color_.lut3.empty())
+        GB_CHECK(cudaMemcpy(dLut_, color_.lut3.data(), color_.lut3.size() * 4, cudaMemcpyHostToDevice));
     GB_CHECK(cudaMemcpy(dJobs_, jobs_.data(), jobs_.size() * sizeof(T1Job), cudaMemcpyHostToDevice));
 }
 
@@ -260,6 +263,10 @@ void EncoderSlot::enqueueStages(const void* dFrame, bool taps, bool full) {
     c.eotf = dEotf_;
     c.thr = dThr_;
     std::memcpy(c.m, m_, sizeof m_);
+    c.route = color_.route;
+    c.tone = color_.tone;
+    c.lut3 = dLut_;
+    c.lutN = color_.lutN;
     c.xyz = taps ? dXyz_ : nullptr;
     launchFrontEnd(L_, c, dLL_[0], dLL_[1], z_.llFloats, dCoeffs_, full ? dTap_ : nullptr, st);
     GB_CHECK(cudaEventRecord(ev_[2], st));

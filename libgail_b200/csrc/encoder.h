@@ -98,7 +98,7 @@ private:
 
     // device
     void* dIn_ = nullptr;
-    float *dEotf_ = nullptr, *dThr_ = nullptr, *dLL_[2] = {nullptr, nullptr}, *dSlope_ = nullptr, *dTap_ = nullptr;
+    float *dEotf_ = nullptr, *dThr_ = nullptr, *dLut_ = nullptr, *dLL_[2] = {nullptr, nullptr}, *dSlope_ = nullptr, *dTap_ = nullptr;
     uint32_t *dCoeffs_ = nullptr, *dInfo_ = nullptr, *dEnd_ = nullptr, *dLen_ = nullptr, *dPerm_ = nullptr,
              *dCtl_ = nullptr, *dOutInfo_ = nullptr, *dOutLen_ = nullptr, *dWork_ = nullptr;
     int32_t *dDist_ = nullptr, *dOutDist_ = nullptr;

@@ -51,6 +51,7 @@ struct EncodeEngine::Class {
     ColorArgs colorArgs{};
     float* dEotf = nullptr;
     float* dThr = nullptr;
+    float* dLut = nullptr;  // the application 3D LUT, if the colour route takes one
     float* dLL[2] = {nullptr, nullptr};
     double* dScale = nullptr;  // per block: the hull's distortion weight
     uint64_t slotBytes = 0, dataCap = 0;
@@ -241,6 +242,7 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
     };
     alloc(c->dEotf, 65536 * 4);
     alloc(c->dThr, 4096 * 4);
+    alloc(c->dLut, c->color.lut3.size() * 4);
     alloc(c->dLL[0], c->z.llFloats * 12);
     alloc(c->dLL[1], c->z.llFloats * 12);
     alloc(c->dScale, c->z.n * 8);
@@ -248,6 +250,8 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
     GB_CHECK(cudaMemcpy(c->dScale, scales.data(), scales.size() * 8, cudaMemcpyHostToDevice));
     GB_CHECK(cudaMemcpy(c->dEotf, c->color.eotf.data(), 65536 * 4, cudaMemcpyHostToDevice));
     GB_CHECK(cudaMemcpy(c->dThr, c->color.thr.data(), 4096 * 4, cudaMemcpyHostToDevice));
+    if (!c->color.lut3.empty())
+        GB_CHECK(cudaMemcpy(c->dLut, c->color.lut3.data(), c->color.lut3.size() * 4, cudaMemcpyHostToDevice));
     ColorArgs& a = c->colorArgs;
     a.kind = s.input.kind == GB_FRAME_PLANAR ? 1 : 0;
     a.pp = planarParams(s.input);
@@ -255,6 +259,10 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
     a.thr = c->dThr;
     std::memcpy(a.m, c->color.m, sizeof a.m);
     a.xyz = nullptr;
+    a.route = c->color.route;
+    a.tone = c->color.tone;
+    a.lut3 = c->dLut;
+    a.lutN = c->color.lutN;
     const uint64_t n = c->z.n, npix = c->z.npix;
     c->dataCap = c->z.outCap;
     c->slotBytes = c->z.inBytes + n * kCblkArea * 4 + n * sizeof(T1Job) + n * 20 + n * kMaxPasses * (4 + 1 + 8) +

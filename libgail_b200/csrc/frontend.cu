@@ -16,13 +16,20 @@
 // never written back as planes): R'G'B' from interleaved 16-bit or planar Y'CbCr,
 // EOTF lookup, 3x3 to XYZ, the 12-bit DCI encoding as the count of 4096 host-built
 // thresholds at or below the value (a fast power gives the first guess, the thresholds
-// decide), DC shift and forward ICT.
+// decide), DC shift and forward ICT. Two more routes are instantiations of their own, so
+// the common one keeps its registers: the managed route puts a tone map (shoulder or
+// BT.2390, on luminance, max(R,G,B) or each target channel) and a soft gamut compression
+// between the 3x3 and the encoding; the LUT route maps R'G'B' through an application 3D
+// LUT (trilinear) straight to codes.
 //
 // Float arithmetic is compiled without contraction and written in the reference's
 // operation order (Josephur/libgail core/dwt_cpu.cpp:24-93, core/color.cpp:142-189,
-// kernels/color_math.h:109-179, core/quant.h:20-25), so coefficients are bit-identical
-// to the CPU path's.
+// kernels/color_math.h:25-179, core/quant.h:20-25), so coefficients are bit-identical
+// to the CPU path's; the managed route's powers are taken in double precision and rounded
+// once to float, as the host's C library powf rounds them but for rare near-ties.
 #include <cuda_runtime.h>
+
+#include <stdexcept>
 
 #include "common.cuh"
 #include "frontend.cuh"
@@ -151,6 +158,161 @@ __device__ __forceinline__ int dciCode(const float* __restrict__ thr, float n) {
     return k;
 }
 
+// ---- the managed and LUT routes (kernels/color_math.h:25-179) ----
+// a power as the host's powf gives it: in double precision, rounded once to float
+__device__ __forceinline__ float powHost(float a, float b) { return (float)pow((double)a, (double)b); }
+
+// SMPTE ST 2084 constants (exact in float)
+constexpr float kPqM1 = 2610.0f / 16384.0f, kPqM2 = 2523.0f / 4096.0f * 128.0f, kPqC1 = 3424.0f / 4096.0f,
+                kPqC2 = 2413.0f / 4096.0f * 32.0f, kPqC3 = 2392.0f / 4096.0f * 32.0f;
+
+__device__ float pqToNits(float e) {
+    const float p = powHost(fminf(fmaxf(e, 0.0f), 1.0f), 1.0f / kPqM2);
+    return 10000.0f * powHost(fmaxf(p - kPqC1, 0.0f) / (kPqC2 - kPqC3 * p), 1.0f / kPqM1);
+}
+
+__device__ float nitsToPq(float nits) {
+    const float y = powHost(fminf(fmaxf(nits / 10000.0f, 0.0f), 1.0f), kPqM1);
+    return powHost((kPqC1 + kPqC2 * y) / (1.0f + kPqC3 * y), kPqM2);
+}
+
+// Target luminance (cd/m^2) for source luminance y.
+__device__ float toneCurve(const ToneParams& t, float y) {
+    if (y <= 0.0f) return 0.0f;
+    if (t.tone == 2) {
+        // BT.2390 EETF: identity below the knee ks (in PQ relative to the source peak), a
+        // Hermite segment from there to the target peak
+        const float e1 = nitsToPq(y) / t.pqSrcMax;
+        if (e1 < t.pqKs) return y;
+        const float s = (fminf(e1, 1.0f) - t.pqKs) / (1.0f - t.pqKs);
+        const float s2 = s * s, s3 = s2 * s;
+        const float e2 = (2.0f * s3 - 3.0f * s2 + 1.0f) * t.pqKs + (s3 - 2.0f * s2 + s) * (1.0f - t.pqKs) +
+                         (-2.0f * s3 + 3.0f * s2) * t.pqMaxLum;
+        return pqToNits(e2 * t.pqSrcMax);
+    }
+    // shoulder: linear up to the knee, then an extended-Reinhard segment that meets the
+    // target peak at the source peak
+    float v = t.gain * y / t.srcRef;
+    if (v > t.knee) {
+        const float u = (v - t.knee) / (1.0f - t.knee);
+        v = t.knee + (1.0f - t.knee) * fminf(u * (1.0f + u / (t.shoulderT * t.shoulderT)) / (1.0f + u), 1.0f);
+    }
+    return v * t.peak;
+}
+
+__device__ __forceinline__ void mul3(const float* A, float a, float b, float c, float o[3]) {
+    o[0] = A[0] * a + A[1] * b + A[2] * c;
+    o[1] = A[3] * a + A[4] * b + A[5] * c;
+    o[2] = A[6] * a + A[7] * b + A[8] * c;
+}
+
+// Moves XYZ toward the neutral of the same luminance until every target channel is in
+// [0, 1], compressing smoothly beyond gamutThresh of the way to the gamut edge.
+__device__ void compressGamut(const ToneParams& t, float xyz[3]) {
+    float c[3];
+    mul3(t.toTarget, xyz[0], xyz[1], xyz[2], c);
+    const float n = xyz[1] / t.peak;
+    if (n >= 1.0f) {
+        c[0] = c[1] = c[2] = 1.0f;
+    } else {
+        float amax = 1.0f, d[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            d[k] = c[k] - n;
+            if (d[k] > 0.0f) amax = fminf(amax, (1.0f - n) / d[k]);
+            if (d[k] < 0.0f) amax = fminf(amax, -n / d[k]);
+        }
+        const float dist = 1.0f / fmaxf(amax, 1e-6f), th = t.gamutThresh;
+        float alpha = 1.0f;
+        if (dist > th) {
+            const float x = (dist - th) / (1.0f - th);
+            const float y = x / (1.0f + x);
+            alpha = (th + (1.0f - th) * y) / dist;
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) c[k] = n + alpha * d[k];
+    }
+    mul3(t.fromTarget, c[0], c[1], c[2], xyz);
+}
+
+// XYZ (cd/m^2) of linear R, G, B with the tone map and the gamut compression applied.
+__device__ void managedXyz(const ColorArgs& c, float R, float G, float B, float xyz[3]) {
+    mul3(c.m, R, G, B, xyz);
+    const ToneParams& t = c.tone;
+    if (t.tone != 0 && xyz[1] > 0.0f) {
+        float tg[3];
+        mul3(t.toTarget, xyz[0], xyz[1], xyz[2], tg);
+        const float pk = t.peak;
+        if (t.norm == 2) {
+            // each target channel on its own; negative (out-of-gamut) channels scaled as the
+            // brightest one is
+            const float mx = fmaxf(tg[0], fmaxf(tg[1], tg[2])) * pk;
+            const float sneg = mx > 0.0f ? toneCurve(t, mx) / mx : 1.0f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) tg[k] = tg[k] > 0.0f ? toneCurve(t, tg[k] * pk) / pk : tg[k] * sneg;
+            mul3(t.fromTarget, tg[0], tg[1], tg[2], xyz);
+        } else {
+            const float m = t.norm == 1 ? fmaxf(xyz[1], fmaxf(tg[0], fmaxf(tg[1], tg[2])) * pk) : xyz[1];
+            const float s = toneCurve(t, m) / m;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) xyz[k] *= s;
+        }
+    }
+    if (t.gamut) compressGamut(t, xyz);
+}
+
+// X'Y'Z' codes of 16-bit R'G'B' through the application 3D LUT.
+__device__ void lutCodes(const ColorArgs& c, const uint32_t rgb[3], int code[3]) {
+    const int n = c.lutN;
+    const float top = (float)(n - 1);
+    int i0[3];
+    float w[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float f = fminf(fmaxf((float)rgb[k] / 65535.f, 0.0f), 1.0f) * top;
+        i0[k] = min((int)f, n - 2);
+        w[k] = f - (float)i0[k];
+    }
+    // the eight surrounding nodes, three floats each
+    const float* q[2][2][2];
+#pragma unroll
+    for (int db = 0; db < 2; ++db)
+#pragma unroll
+        for (int dg = 0; dg < 2; ++dg)
+#pragma unroll
+            for (int dr = 0; dr < 2; ++dr)
+                q[db][dg][dr] = c.lut3 + ((size_t)((i0[2] + db) * n + i0[1] + dg) * n + i0[0] + dr) * 3;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        float e[2][2];
+#pragma unroll
+        for (int db = 0; db < 2; ++db)
+#pragma unroll
+            for (int dg = 0; dg < 2; ++dg)
+                e[db][dg] = __ldg(q[db][dg][0] + ch) * (1.0f - w[0]) + __ldg(q[db][dg][1] + ch) * w[0];
+        const float v = (e[0][0] * (1.0f - w[1]) + e[0][1] * w[1]) * (1.0f - w[2]) +
+                        (e[1][0] * (1.0f - w[1]) + e[1][1] * w[1]) * w[2];
+        code[ch] = (int)floorf(fminf(fmaxf(v, 0.0f), 1.0f) * 4095.0f + 0.5f);
+    }
+}
+
+// The three 12-bit codes of a pixel by the route MODE (1 direct, 2 managed, 3 LUT).
+template <int MODE>
+__device__ __forceinline__ void pixelCodes(const ColorArgs& c, const uint32_t rgb[3], int code[3]) {
+    if (MODE == 3) {
+        lutCodes(c, rgb, code);
+        return;
+    }
+    // the EOTF table index floor(clamp(code / 65535) * 65535 + 0.5) is the code
+    // itself for every 16-bit code (checked exhaustively in float32)
+    const float R = __ldg(c.eotf + rgb[0]), G = __ldg(c.eotf + rgb[1]), B = __ldg(c.eotf + rgb[2]);
+    float xyz[3];
+    if (MODE == 2) managedXyz(c, R, G, B, xyz);
+    else mul3(c.m, R, G, B, xyz);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) code[k] = dciCode(c.thr, clamp01(xyz[k] / 52.37f));
+}
+
 // One 72-sample line of a tile, `step` floats between samples: the four lifting steps
 // (x[i] += c * (x[i-1] + x[i+1]) on odd 1..69, even 2..70, odd, even), then the scaling of
 // the 64 samples the tile outputs, written back in place. Sample k is final once delta
@@ -200,10 +362,13 @@ __device__ void writeOutputs(const LevelArgs& a, const float* t, int comp, int t
     }
 }
 
-template <bool COLOR>
-__global__ void __launch_bounds__(COLOR ? FE_THREADS_COLOR : FE_THREADS_PLAIN, COLOR ? 3 : 8)
+// MODE 0: a later level from the previous LL planes; 1..3: level 1 with the colour route
+// of pixelCodes.
+template <int MODE>
+__global__ void __launch_bounds__(MODE ? FE_THREADS_COLOR : FE_THREADS_PLAIN, MODE == 0 ? 8 : MODE == 1 ? 3 : 2)
     levelKernel(ColorArgs c, LevelArgs a) {
     extern __shared__ float smem[];
+    constexpr bool COLOR = MODE != 0;
     constexpr int THREADS = COLOR ? FE_THREADS_COLOR : FE_THREADS_PLAIN;
     constexpr int NC = COLOR ? 3 : 1;
     const int tid = threadIdx.x, tx = blockIdx.x, ty = blockIdx.y;
@@ -222,15 +387,9 @@ __global__ void __launch_bounds__(COLOR ? FE_THREADS_COLOR : FE_THREADS_PLAIN, C
             } else {
                 planarRgb(c.src, c.pp, gx, gy, rgb);
             }
-            // the EOTF table index floor(clamp(code / 65535) * 65535 + 0.5) is the code
-            // itself for every 16-bit code (checked exhaustively in float32)
-            const float R = __ldg(c.eotf + rgb[0]), G = __ldg(c.eotf + rgb[1]), B = __ldg(c.eotf + rgb[2]);
-            const float X = c.m[0] * R + c.m[1] * G + c.m[2] * B;
-            const float Yv = c.m[3] * R + c.m[4] * G + c.m[5] * B;
-            const float Z = c.m[6] * R + c.m[7] * G + c.m[8] * B;
-            const int cx = dciCode(c.thr, clamp01(X / 52.37f));
-            const int cy = dciCode(c.thr, clamp01(Yv / 52.37f));
-            const int cz = dciCode(c.thr, clamp01(Z / 52.37f));
+            int code[3];
+            pixelCodes<MODE>(c, rgb, code);
+            const int cx = code[0], cy = code[1], cz = code[2];
             if (c.xyz && lx >= HALO && lx < HALO + TS && ly >= HALO && ly < HALO + TS && x0 + lx < w && y0 + ly < h) {
                 uint16_t* o = c.xyz + ((size_t)(y0 + ly) * w + (x0 + lx)) * 3;
                 o[0] = (uint16_t)cx;
@@ -271,19 +430,28 @@ constexpr size_t kSmemPlain = (size_t)TW * TP * 4;
 }  // namespace
 
 void frontendInit() {
-    GB_CHECK(cudaFuncSetAttribute(levelKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemColor));
-    GB_CHECK(cudaFuncSetAttribute(levelKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemPlain));
+    GB_CHECK(cudaFuncSetAttribute(levelKernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemColor));
+    GB_CHECK(cudaFuncSetAttribute(levelKernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemColor));
+    GB_CHECK(cudaFuncSetAttribute(levelKernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemColor));
+    GB_CHECK(cudaFuncSetAttribute(levelKernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemPlain));
 }
 
 void launchLevel1(const ColorArgs& c, const LevelArgs& a, cudaStream_t st) {
     const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 1);
-    levelKernel<true><<<grid, FE_THREADS_COLOR, kSmemColor, st>>>(c, a);
+    if (c.route == kRouteLut) {
+        if (!c.lut3 || c.lutN < 2) throw std::logic_error("LUT route without a LUT");
+        levelKernel<3><<<grid, FE_THREADS_COLOR, kSmemColor, st>>>(c, a);
+    } else if (c.route == kRouteManaged) {
+        levelKernel<2><<<grid, FE_THREADS_COLOR, kSmemColor, st>>>(c, a);
+    } else {
+        levelKernel<1><<<grid, FE_THREADS_COLOR, kSmemColor, st>>>(c, a);
+    }
     GB_CHECK(cudaGetLastError());
 }
 
 void launchLevel(const LevelArgs& a, cudaStream_t st) {
     const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 3);
-    levelKernel<false><<<grid, FE_THREADS_PLAIN, kSmemPlain, st>>>(ColorArgs{}, a);
+    levelKernel<0><<<grid, FE_THREADS_PLAIN, kSmemPlain, st>>>(ColorArgs{}, a);
     GB_CHECK(cudaGetLastError());
 }
 

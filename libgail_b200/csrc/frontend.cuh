@@ -43,6 +43,10 @@ struct ColorArgs {
     const float* thr;        // 4096 thresholds
     float m[9];
     uint16_t* xyz;           // debug tap: interleaved 12-bit codes, or NULL
+    int32_t route;           // ColorRoute
+    ToneParams tone;         // route 1
+    const float* lut3;       // route 2: lutN^3 nodes of three floats, red fastest
+    int32_t lutN;
 };
 
 // Level 1 with the colour conversion folded into its tile loads.

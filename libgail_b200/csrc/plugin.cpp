@@ -152,6 +152,14 @@ uint64_t pEncoderBytes(GailCudaDevice*, const GailCudaLayout* layout, const Gail
         Layout L;
         layoutFromAbi(*layout, L);
         bytes = slotSizes(L, s->input).deviceBytes();
+        // an application 3D LUT lives on the device too
+        const GailCudaColor& c = s->color;
+        uint64_t lut = c.lut3dData ? c.lut3dCount : 0;
+        if (!lut && c.lut3d && c.lut3d[0]) {
+            int32_t n = 0;
+            lut = readCube(c.lut3d, n).size();
+        }
+        bytes += (lut * 4 + 255) / 256 * 256;
     });
     return bytes;
 }

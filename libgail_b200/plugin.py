@@ -12,7 +12,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import GailError, lib
+from . import GailError, check, lib
 
 
 class Subband(C.Structure):
@@ -143,6 +143,40 @@ def color(transfer="bt1886", primaries="bt709", sdr_white=48.0) -> Color:
     return Color(transfer=TRANSFER[transfer], primaries=PRIMARIES[primaries], toneMap=0, toneNorm=0, gamut=2,
                  lut3dSize=0, sdrWhite=sdr_white, hdrPeak=1000.0, cinemaPeak=48.0, hdrRefWhite=203.0,
                  cinemaRefWhite=16.0, knee=0.25, gamutThreshold=0.8, lut3d=b"", lut3dData=None, lut3dCount=0)
+
+
+TONE_MAP = {"signal": 0, "shoulder": 1, "bt2390": 2, "none": 3}
+TONE_NORM = {"channel": 0, "maxrgb": 1, "luminance": 2}
+GAMUT = {"p3d65": 0, "dcip3": 1, "none": 2}
+
+
+def color_managed(transfer="pq", primaries="bt2020", tone_map="signal", tone_norm="channel", gamut="none",
+                  sdr_white=48.0, hdr_peak=1000.0, cinema_peak=48.0, hdr_ref_white=203.0, cinema_ref_white=16.0,
+                  knee=0.25, gamut_threshold=0.8, lut=None, lut_size=0, lut_path="") -> Color:
+    """Every colour setting of ColorParams (core/color.h:84-100): tone map and its norm,
+    target gamut, or a 3D LUT (float32 lut_size^3 * 3, red fastest, or a .cube path) that
+    replaces them. The LUT array is kept alive by the returned structure."""
+    c = Color(transfer=TRANSFER[transfer], primaries=PRIMARIES[primaries], toneMap=TONE_MAP[tone_map],
+              toneNorm=TONE_NORM[tone_norm], gamut=GAMUT[gamut], lut3dSize=lut_size, sdrWhite=sdr_white,
+              hdrPeak=hdr_peak, cinemaPeak=cinema_peak, hdrRefWhite=hdr_ref_white, cinemaRefWhite=cinema_ref_white,
+              knee=knee, gamutThreshold=gamut_threshold, lut3d=lut_path.encode(), lut3dData=None, lut3dCount=0)
+    if lut is not None:
+        arr = np.ascontiguousarray(lut, dtype=np.float32)
+        c._lut = arr
+        c.lut3dData = arr.ctypes.data_as(C.POINTER(C.c_float))
+        c.lut3dCount = arr.size
+    return c
+
+
+def color_route(col: Color):
+    """(route, the reference-layout 48-float parameter block, LUT nodes per axis) the
+    library derives from a colour setting: route 0 direct, 1 tone map / gamut, 2 3D LUT."""
+    L = lib()
+    L.gb_color_route.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    params = np.zeros(48, np.float32)
+    route, n = C.c_int32(), C.c_int32()
+    check(L.gb_color_route(C.byref(col), params.ctypes.data, C.byref(route), C.byref(n)))
+    return route.value, params, n.value
 
 
 def rgb48_format(width, height) -> FrameFormat:

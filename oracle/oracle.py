@@ -36,6 +36,31 @@ class OrCblk(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("band", "x0", "y0", "w", "h")]
 
 
+class RefColor(C.Structure):
+    """Every colour setting of the reference (ColorParams, core/color.h:84-100)."""
+    _fields_ = [(n, C.c_int32) for n in ("transfer", "primaries", "toneMap", "toneNorm", "gamut", "lutSize")] + \
+        [(n, C.c_double) for n in ("sdrWhite", "hdrPeak", "cinemaPeak", "hdrRefWhite", "cinemaRefWhite", "knee",
+                                   "gamutThreshold")] + \
+        [("lutData", C.POINTER(C.c_float)), ("lutCount", C.c_uint64), ("lutPath", C.c_char_p)]
+
+
+def ref_color(transfer=0, primaries=0, tone_map=0, tone_norm=0, gamut=2, sdr_white=48.0, hdr_peak=1000.0,
+              cinema_peak=48.0, hdr_ref_white=203.0, cinema_ref_white=16.0, knee=0.25, gamut_threshold=0.8,
+              lut=None, lut_size=0, lut_path=b"") -> RefColor:
+    """A RefColor with the reference's defaults; `lut` (float32, lut_size^3 * 3) is kept
+    alive by the returned structure."""
+    c = RefColor(transfer=transfer, primaries=primaries, toneMap=tone_map, toneNorm=tone_norm, gamut=gamut,
+                 lutSize=lut_size, sdrWhite=sdr_white, hdrPeak=hdr_peak, cinemaPeak=cinema_peak,
+                 hdrRefWhite=hdr_ref_white, cinemaRefWhite=cinema_ref_white, knee=knee,
+                 gamutThreshold=gamut_threshold, lutData=None, lutCount=0, lutPath=lut_path)
+    if lut is not None:
+        arr = np.ascontiguousarray(lut, dtype=np.float32)
+        c._lut = arr
+        c.lutData = arr.ctypes.data_as(C.POINTER(C.c_float))
+        c.lutCount = arr.size
+    return c
+
+
 class Planar(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("width", "height", "active_w", "active_h", "ox", "oy", "sx", "sy", "rgb",
                                          "bits", "full_range", "chroma")] + [("kr", C.c_double), ("kb", C.c_double)]
@@ -215,6 +240,10 @@ class Reference(_Common):
         L.ref_plugin_layout_hash.restype = C.c_uint64
         L.ref_plugin_sizes.argtypes = [C.c_void_p]
         L.ref_usable_cpus.restype = C.c_int
+        L.ref_color_params.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_color_frame_full.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p]
+        L.ref_read_cube.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint64]
 
     def error(self) -> str:
         return self.lib.ref_last_error().decode()
@@ -287,6 +316,33 @@ class Reference(_Common):
         self.lib.ref_planar_to_rgb48(C.byref(fmt), _p(s), _p(out))
         return out
 
+    def color_params(self, color: RefColor):
+        """ColorConverter's parameter block (48 floats) and its 3D LUT size."""
+        params = np.zeros(48, np.float32)
+        n = C.c_int()
+        if self.lib.ref_color_params(C.byref(color), _p(params), C.byref(n)) != 0:
+            raise RuntimeError(self.error())
+        return params, n.value
+
+    def color_frame_full(self, rgb48: np.ndarray, color: RefColor):
+        """convertFrame under any colour setting: ICT planes and X'Y'Z' codes."""
+        rgb = np.ascontiguousarray(rgb48, dtype=np.uint16)
+        h, w = rgb.shape[:2]
+        planes = np.zeros((3, h, w), np.float32)
+        xyz = np.zeros((h, w, 3), np.uint16)
+        if self.lib.ref_color_frame_full(C.byref(color), _p(rgb), h * w, _p(planes[0]), _p(planes[1]),
+                                         _p(planes[2]), _p(xyz)) != 0:
+            raise RuntimeError(self.error())
+        return planes, xyz
+
+    def read_cube(self, path: str):
+        """readCubeLut: (n, n^3 * 3 floats); raises RuntimeError with the reference's message."""
+        n = C.c_int()
+        out = np.zeros(256 ** 3 * 3 // 64, np.float32)
+        if self.lib.ref_read_cube(path.encode(), C.byref(n), _p(out), out.size) != 0:
+            raise RuntimeError(self.error())
+        return n.value, out[: n.value ** 3 * 3].copy()
+
     def suite(self, which: int, ntrials: int):
         coeffs = np.zeros((ntrials, 1024), np.uint32)
         meta = np.zeros((ntrials, 4), np.int32)
@@ -332,6 +388,8 @@ def _ref_bind(L):
                                      C.c_int]
     L.ref_encoder_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.POINTER(RefEncOut)]
     L.ref_encoder_destroy.argtypes = [C.c_void_p]
+    L.ref_encoder_create_color.restype = C.c_void_p
+    L.ref_encoder_create_color.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int]
     L.ref_rate_and_build.restype = C.c_longlong
     L.ref_rate_and_build.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_uint64, C.c_void_p,
                                      C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_double, C.c_double,
@@ -360,12 +418,17 @@ class RefEncoder:
     """The reference CPU encoder (CpuSlot through createCpuDevice) on one frame format."""
 
     def __init__(self, ref: "Reference", width, height, fourk, transfer=5, primaries=4, sdr_white=48.0,
-                 planar: Planar = None, threads=0, base_step=1.0):
+                 planar: Planar = None, threads=0, base_step=1.0, color: RefColor = None):
         self.ref = ref
         _ref_bind(ref.lib)
-        self.h = ref.lib.ref_encoder_create(width, height, int(fourk), C.c_double(base_step), transfer, primaries,
-                                            C.c_double(sdr_white), C.byref(planar) if planar is not None else None,
-                                            threads)
+        pl = C.byref(planar) if planar is not None else None
+        if color is not None:  # every colour setting (tone map, gamut, 3D LUT)
+            self._color = color
+            self.h = ref.lib.ref_encoder_create_color(width, height, int(fourk), C.c_double(base_step),
+                                                      C.byref(color), pl, threads)
+        else:
+            self.h = ref.lib.ref_encoder_create(width, height, int(fourk), C.c_double(base_step), transfer,
+                                                primaries, C.c_double(sdr_white), pl, threads)
         if not self.h:
             raise RuntimeError(ref.error())
         self.width, self.height, self.fourk = width, height, fourk

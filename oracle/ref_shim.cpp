@@ -195,6 +195,76 @@ void ref_color_frame(int transfer, int primaries, double sdrWhite, const uint16_
     cc.convertFrame(rgb, npix, 1, planes, xyz12);
 }
 
+// Every colour setting (ColorParams, core/color.h:84-100; the enums' numbering): tone
+// map, norm, target gamut, a 3D LUT in memory or by .cube path.
+struct RefColor {
+    int32_t transfer, primaries, toneMap, toneNorm, gamut, lutSize;
+    double sdrWhite, hdrPeak, cinemaPeak, hdrRefWhite, cinemaRefWhite, knee, gamutThreshold;
+    const float* lutData;
+    uint64_t lutCount;
+    const char* lutPath;
+};
+
+static ColorParams colorOf(const RefColor& r) {
+    ColorParams c;
+    c.transfer = (Transfer)r.transfer;
+    c.primaries = (Primaries)r.primaries;
+    c.toneMap = (ToneMap)r.toneMap;
+    c.toneNorm = (ToneNorm)r.toneNorm;
+    c.gamut = (TargetGamut)r.gamut;
+    c.sdrWhite = r.sdrWhite;
+    c.hdrPeak = r.hdrPeak;
+    c.cinemaPeak = r.cinemaPeak;
+    c.hdrRefWhite = r.hdrRefWhite;
+    c.cinemaRefWhite = r.cinemaRefWhite;
+    c.knee = r.knee;
+    c.gamutThreshold = r.gamutThreshold;
+    if (r.lutData && r.lutCount) c.lut3dData.assign(r.lutData, r.lutData + r.lutCount);
+    c.lut3dSize = r.lutSize;
+    c.lut3d = r.lutPath ? r.lutPath : "";
+    return c;
+}
+
+// The converter's parameter block (CP_COUNT floats, kernels/color_params.h) and its LUT size.
+int ref_color_params(const RefColor* c, float* params48, int* lutN) {
+    try {
+        ColorConverter cc(colorOf(*c));
+        std::memcpy(params48, cc.params().data(), cc.params().size() * 4);
+        *lutN = cc.lut3dSize();
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+int ref_color_frame_full(const RefColor* c, const uint16_t* rgb, int npix, float* p0, float* p1, float* p2,
+                         uint16_t* xyz12) {
+    try {
+        ColorConverter cc(colorOf(*c));
+        float* planes[3] = {p0, p1, p2};
+        cc.convertFrame(rgb, npix, 1, planes, xyz12);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// readCubeLut (core/color.cpp:245-282): the LUT's size and up to cap floats of it.
+int ref_read_cube(const char* path, int* n, float* out, uint64_t cap) {
+    try {
+        int size = 0;
+        const std::vector<float> v = readCubeLut(path, size);
+        *n = size;
+        std::memcpy(out, v.data(), std::min<uint64_t>(cap, v.size()) * 4);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
 struct RefPlanar {
     int32_t width, height, activeW, activeH, ox, oy, sx, sy, rgb, bits, fullRange, chroma;
     double kr, kb;
@@ -232,8 +302,26 @@ struct EncView {
     FrameDebug dbg;
 };
 
+static void* encoderCreate(int width, int height, int fourk, double baseStep, const ColorParams& color,
+                           const RefPlanar* planar, int threads);
+
 void* ref_encoder_create(int width, int height, int fourk, double baseStep, int transfer, int primaries, double sdrWhite,
                          const RefPlanar* planar, int threads) {
+    return encoderCreate(width, height, fourk, baseStep, colorParams(transfer, primaries, sdrWhite), planar, threads);
+}
+
+void* ref_encoder_create_color(int width, int height, int fourk, double baseStep, const RefColor* color,
+                               const RefPlanar* planar, int threads) {
+    try {
+        return encoderCreate(width, height, fourk, baseStep, colorOf(*color), planar, threads);
+    } catch (const std::exception& ex) {
+        g_err = ex.what();
+        return nullptr;
+    }
+}
+
+static void* encoderCreate(int width, int height, int fourk, double baseStep, const ColorParams& color,
+                           const RefPlanar* planar, int threads) {
     try {
         auto e = std::make_unique<EncView>();
         e->L = layoutOf(width, height, fourk, baseStep);
@@ -242,7 +330,7 @@ void* ref_encoder_create(int width, int height, int fourk, double baseStep, int 
         s.width = width;
         s.height = height;
         s.baseStep = baseStep;
-        s.color = colorParams(transfer, primaries, sdrWhite);
+        s.color = color;
         if (planar) {
             s.input = formatOf(*planar);
         } else {

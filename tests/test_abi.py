@@ -116,8 +116,108 @@ def test_dci_code_is_monotone_on_a_dense_sweep():
     assert np.all(np.diff(codes) >= 0)
 
 
-def test_unsupported_color_routes_are_refused():
-    col = P.color("pq", "bt2020")
-    col.toneMap = 1
+# colour settings across the managed route's branches: tone map x norm x target gamut,
+# the shoulder's knee clamp and its no-shoulder case, BT.2390 with a source peak at or below
+# the cinema peak (no tone map), HLG, pass-through (tone settings ignored), LUTs
+ROUTE_CASES = [
+    dict(tone_map="shoulder", tone_norm="channel", gamut="p3d65", hdr_peak=4000.0),
+    dict(tone_map="shoulder", tone_norm="maxrgb", gamut="p3d65", hdr_peak=4000.0),
+    dict(tone_map="shoulder", tone_norm="luminance", gamut="p3d65", hdr_peak=4000.0),
+    dict(tone_map="bt2390", tone_norm="channel", gamut="p3d65", hdr_peak=4000.0),
+    dict(tone_map="bt2390", tone_norm="maxrgb", gamut="dcip3", hdr_peak=1000.0, cinema_peak=48.0),
+    dict(tone_map="bt2390", tone_norm="luminance", gamut="none", hdr_peak=40.0),
+    dict(tone_map="shoulder", knee=0.001, hdr_peak=600.0, gamut_threshold=1.5),
+    dict(tone_map="shoulder", knee=2.0, hdr_peak=100.0, cinema_ref_white=10.0, gamut="dcip3", gamut_threshold=-1.0),
+    dict(transfer="hlg", tone_map="shoulder", tone_norm="maxrgb", gamut="p3d65"),
+    dict(transfer="hlg", tone_map="none"),
+    dict(tone_map="signal", gamut="p3d65"),
+    dict(transfer="bt1886", primaries="bt709", gamut="dcip3", gamut_threshold=0.5),
+    dict(transfer="gamma26", primaries="xyz", tone_map="shoulder", gamut="p3d65"),
+    dict(transfer="srgb", primaries="bt709", lut_size=5, lut="sin"),
+]
+
+
+def _lut_of(case):
+    if case.get("lut") == "sin":
+        n = case["lut_size"]
+        return np.array([0.5 + 0.4 * np.sin(i * 0.7 + c) for i in range(n ** 3) for c in range(3)], np.float32)
+    return None
+
+
+def _route_case(case):
+    kw = dict(case)
+    lut = _lut_of(kw)
+    kw["lut"] = lut
+    mine = P.color_managed(**kw)
+    from oracle.oracle import ref_color
+    rkw = dict(transfer=P.TRANSFER[kw.pop("transfer", "pq")], primaries=P.PRIMARIES[kw.pop("primaries", "bt2020")],
+               tone_map=P.TONE_MAP[kw.pop("tone_map", "signal")], tone_norm=P.TONE_NORM[kw.pop("tone_norm", "channel")],
+               gamut=P.GAMUT[kw.pop("gamut", "none")])
+    rkw.update(lut=kw.pop("lut"), lut_size=kw.pop("lut_size", 0))
+    rkw.update(kw)
+    return mine, ref_color(**rkw)
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build not present")
+@pytest.mark.parametrize("case", ROUTE_CASES, ids=lambda c: "-".join(str(v) for k, v in c.items() if k != "lut"))
+def test_color_route_constants_match_reference(case):
+    """The managed route's constants, bit for bit in the positions of the reference's
+    parameter block (ColorConverter::params), and the route chosen."""
+    mine, theirs = _route_case(case)
+    route, params, n = P.color_route(mine)
+    ref_params, ref_n = Reference().color_params(theirs)
+    assert n == ref_n
+    assert np.array_equal(params.view(np.uint32), ref_params.view(np.uint32)), \
+        [(i, params[i], ref_params[i]) for i in range(48) if params.view(np.uint32)[i] != ref_params.view(np.uint32)[i]]
+    want = 2 if ref_n > 1 else 1 if (ref_params[12] != 0 or ref_params[18] != 0) else 0
+    assert route == want
+
+
+CUBE_GOOD = """# comment
+TITLE "test"
+LUT_3D_SIZE 2
+DOMAIN_MIN 0 0 0
+DOMAIN_MAX 1 1 1
+
+0 0 0
+1 0 0
+0 1 0
+1 1 0
+  0 0 1
+1 0 1 trailing words
+0 1 1
+1 1 1
+"""
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build not present")
+@pytest.mark.parametrize("name,text", [
+    ("good", CUBE_GOOD),
+    ("one_d", "LUT_1D_SIZE 4\n0 0 0\n"),
+    ("count", "LUT_3D_SIZE 2\n0 0 0\n1 1 1\n"),
+    ("domain", CUBE_GOOD.replace("DOMAIN_MAX 1 1 1", "DOMAIN_MAX 1 2 1")),
+    ("size1", "LUT_3D_SIZE 1\n0 0 0\n"),
+    ("crlf", CUBE_GOOD.replace("\n", "\r\n")),
+])
+def test_cube_reader_matches_reference(tmp_path, name, text):
+    """A .cube LUT given by path: read as the reference's readCubeLut reads it (the same
+    nodes, or an error where it gives one)."""
+    path = tmp_path / f"{name}.cube"
+    path.write_bytes(text.encode())
+    try:
+        rn, rdata = Reference().read_cube(str(path))
+    except RuntimeError:
+        rn = None
+    col = P.color_managed(transfer="srgb", primaries="bt709", lut_path=str(path))
+    if rn is None:
+        with pytest.raises(gb.GailError):
+            P.color_route(col)
+        return
+    route, params, n = P.color_route(col)
+    assert (route, n) == (2, rn)
+
+
+def test_lut_data_must_match_its_size():
+    lut = np.zeros(5 ** 3 * 3 - 1, np.float32)
     with pytest.raises(gb.GailError):
-        _tables(col)
+        P.color_route(P.color_managed(lut=lut, lut_size=5))
