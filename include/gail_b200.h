@@ -74,6 +74,14 @@ GB_API int gb_t1_encode_blocks_noalloc(const uint32_t* coeffs, const int32_t* ge
                                        const float* distScale, uint32_t* info4, uint32_t* passLen, int32_t* passDist,
                                        uint8_t* data, uint32_t dataStride);
 
+/* Failure detection of the persistent Tier-1 launch (GbTuning.t1Persistent), exercised
+ * without a fault: one warp waits on a device flag that nothing sets, as the launch's warps
+ * wait for a partner's announced work, with its limit lowered to limitMs (1..2000; the
+ * launch uses 2000) and returns. *status gets the device status bits it left (16: the wait
+ * gave up) and *elapsedMs (may be NULL) the launch's duration; the device stays usable.
+ * No counterpart in the reference (its kernels do not wait on one another). */
+GB_API int gb_t1_wait_selftest(uint32_t limitMs, uint32_t* status, float* elapsedMs);
+
 /* The DCI frame layout: subbands (with their quantisation steps) in the plugin ABI's
  * form, for callers that build GailCudaLayout themselves. Replaces makeLayout
  * (src/core/layout.h:87 with Profile::Cinema2K / Cinema4K). maxBands >= 3 * 19 + 3. */

@@ -82,4 +82,13 @@ GB_API int gb_t1_encode_blocks(const uint32_t* coeffs, const int32_t* geom4, uin
     });
 }
 
+GB_API int gb_t1_wait_selftest(uint32_t limitMs, uint32_t* status, float* elapsedMs) {
+    return gbGuard([&] {
+        if (!status) throw std::logic_error("null argument");
+        if (limitMs < 1 || limitMs > 2000) throw std::logic_error("limitMs must be 1..2000");
+        ensureDevice();
+        *status = t1WaitSelftest(limitMs, elapsedMs);
+    });
+}
+
 }  // extern "C"

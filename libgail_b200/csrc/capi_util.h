@@ -44,5 +44,8 @@ int gbGuard(F&& fn) noexcept {
 void ensureDevice();
 // Whether this library's kernels load on the current device (cudaSuccess when they do).
 cudaError_t kernelsLoadable();
+// One warp of the persistent Tier-1 launch's wait, on a flag nothing sets, given up after
+// limitMs: returns the status bits it left (kErrQueueWait) and the launch's duration.
+uint32_t t1WaitSelftest(uint32_t limitMs, float* elapsedMs);
 
 }  // namespace gb

@@ -964,11 +964,13 @@ __device__ __forceinline__ uint32_t ldRelaxed(const uint32_t* p) {
     return x;
 }
 
+constexpr uint64_t kQueueWaitNs = 2000000000ull;  // a persistent launch's longest wait
+
 // Waits until *p >= v (polling with relaxed loads, backing off from 0.25 to 8 us so that
 // thousands of waiting warps leave L2 to the working ones; the caller acquires once it
-// holds); gives up after 2 s with kErrQueueWait set, so that a launch whose other warps
-// stopped returns.
-__device__ bool waitFor(const uint32_t* p, uint32_t v, uint32_t* status) {
+// holds); gives up after limitNs (2 s in the launches) with kErrQueueWait set, so that a
+// launch whose other warps stopped returns.
+__device__ bool waitFor(const uint32_t* p, uint32_t v, uint32_t* status, uint64_t limitNs = kQueueWaitNs) {
     uint64_t t0, t1;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
     uint32_t nap = 256;
@@ -978,7 +980,7 @@ __device__ bool waitFor(const uint32_t* p, uint32_t v, uint32_t* status) {
         nap = min(nap * 2, 8192u);
         if ((it & 63u) == 63u) {
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-            if (t1 - t0 > 2000000000ull) break;
+            if (t1 - t0 > limitNs) break;
         }
     }
     atomicOr(status, kErrQueueWait);
@@ -989,8 +991,9 @@ __device__ bool waitFor(const uint32_t* p, uint32_t v, uint32_t* status) {
 // model orders later loads after the writes that preceded the release only for the thread
 // that performs the acquire, not for lanes that hear of the value from lane 0 by shuffle.
 // Returns *p as every lane read it, 0 when the wait gave up (warp-uniform).
-__device__ __forceinline__ uint32_t warpWaitFor(const uint32_t* p, uint32_t v, uint32_t* status, int lane) {
-    const bool ok = lane == 0 ? waitFor(p, v, status) : true;
+__device__ __forceinline__ uint32_t warpWaitFor(const uint32_t* p, uint32_t v, uint32_t* status, int lane,
+                                                uint64_t limitNs = kQueueWaitNs) {
+    const bool ok = lane == 0 ? waitFor(p, v, status, limitNs) : true;
     if (!__shfl_sync(kFull, ok, 0)) return 0u;
     return ldAcquire(p);
 }
@@ -1095,7 +1098,41 @@ __global__ void __launch_bounds__(CM_THREADS, 7) t1PersistentKernel(T1Launch P, 
     }
 }
 
+// One warp waits, as the persistent launch's warps wait, on a flag nothing sets: the
+// failure-detection path of that launch (a partner warp that never announces its work)
+// made to run out without a fault.
+__global__ void waitSelftestKernel(const uint32_t* flag, uint32_t* status, uint64_t limitNs) {
+    warpWaitFor(flag, 1u, status, (int)(threadIdx.x & 31), limitNs);
+}
+
 }  // namespace
+
+uint32_t t1WaitSelftest(uint32_t limitMs, float* elapsedMs) {
+    uint32_t* d = nullptr;  // [0] the flag, [1] the status word
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    uint32_t h[2] = {0, 0};
+    auto release = [&] {
+        for (auto& x : e)
+            if (x) cudaEventDestroy(x);
+        if (d) cudaFree(d);
+    };
+    try {
+        GB_CHECK(cudaMalloc(&d, 8));
+        GB_CHECK(cudaMemset(d, 0, 8));
+        for (auto& x : e) GB_CHECK(cudaEventCreate(&x));
+        GB_CHECK(cudaEventRecord(e[0], 0));
+        waitSelftestKernel<<<1, 32>>>(d, d + 1, (uint64_t)limitMs * 1000000ull);
+        GB_CHECK(cudaGetLastError());
+        GB_CHECK(cudaEventRecord(e[1], 0));
+        GB_CHECK(cudaMemcpy(h, d, 8, cudaMemcpyDeviceToHost));
+        if (elapsedMs) GB_CHECK(cudaEventElapsedTime(elapsedMs, e[0], e[1]));
+    } catch (...) {
+        release();
+        throw;
+    }
+    release();
+    return h[1];
+}
 
 cudaError_t kernelsLoadable() {
     cudaFuncAttributes attr;

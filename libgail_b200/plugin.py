@@ -118,8 +118,9 @@ class PluginTable(C.Structure):
     ]
 
 
-def table() -> PluginTable:
-    L = lib()
+def table(path: str | None = None) -> PluginTable:
+    """This library's plugin table, or that of another build of the plugin ABI at `path`."""
+    L = lib() if path is None else C.CDLL(path)
     L.gail_cuda_plugin_get.restype = C.POINTER(PluginTable)
     L.gail_cuda_plugin_get.argtypes = [C.c_uint32]
     p = L.gail_cuda_plugin_get(1)
@@ -224,8 +225,8 @@ def make_layout(width, height, fourk, base_step=1.0):
 
 
 class Plugin:
-    def __init__(self):
-        self.t = table()
+    def __init__(self, path: str | None = None):
+        self.t = table(path)
 
     def err(self):
         return self.t.last_error().decode(errors="replace")

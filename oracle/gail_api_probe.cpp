@@ -5,6 +5,7 @@
 // CudaHost (dlopen, gail_cuda_plugin_get, the ABI / size / layout checks) and runs its CUDA
 // backend on it. TEST INFRASTRUCTURE ONLY: the drop-in test loads this; the product never
 // does.
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -63,11 +64,35 @@ __attribute__((visibility("default"))) int probe_list_devices(int backend, char*
 // encoder through gail_encoder_send / gail_encoder_receive, in send order. Codestream i goes
 // to out + i * cap; sizes[i] and compliant[i] are set. Returns GAIL_OK or a status
 // (probe_last_error() then says why).
+static int encodeStream(int backend, int profile, int container, int format, int matrix, int preset, double fps,
+                        double maxMbps, int framesInFlight, const void* const* planes, int count, uint8_t* out,
+                        size_t cap, uint64_t* sizes, int* compliant, char* devices, size_t devCap, double* seconds);
+
 __attribute__((visibility("default"))) int probe_encode(int backend, int profile, int container, int format,
                                                         int matrix, int preset, double fps, double maxMbps,
                                                         int framesInFlight, const void* const* planes, int count,
                                                         uint8_t* out, size_t cap, uint64_t* sizes, int* compliant,
                                                         char* devices, size_t devCap) {
+    return encodeStream(backend, profile, container, format, matrix, preset, fps, maxMbps, framesInFlight, planes,
+                        count, out, cap, sizes, compliant, devices, devCap, nullptr);
+}
+
+// probe_encode with the seconds from the first gail_encoder_send to the last codestream
+// received (the encoder's set-up before it and its tear-down after it excluded), as a
+// throughput benchmark of the library times a stream.
+__attribute__((visibility("default"))) int probe_encode_timed(int backend, int profile, int container, int format,
+                                                              int matrix, int preset, double fps, double maxMbps,
+                                                              int framesInFlight, const void* const* planes, int count,
+                                                              uint8_t* out, size_t cap, uint64_t* sizes,
+                                                              int* compliant, char* devices, size_t devCap,
+                                                              double* seconds) {
+    return encodeStream(backend, profile, container, format, matrix, preset, fps, maxMbps, framesInFlight, planes,
+                        count, out, cap, sizes, compliant, devices, devCap, seconds);
+}
+
+static int encodeStream(int backend, int profile, int container, int format, int matrix, int preset, double fps,
+                        double maxMbps, int framesInFlight, const void* const* planes, int count, uint8_t* out,
+                        size_t cap, uint64_t* sizes, int* compliant, char* devices, size_t devCap, double* seconds) {
     const EncodeArgs a{backend, profile, container, format, matrix, preset, fps, maxMbps, framesInFlight};
     gail_config c;
     configure(a, c);
@@ -79,6 +104,7 @@ __attribute__((visibility("default"))) int probe_encode(int backend, int profile
     }
     copyOut(gail_encoder_devices(e), devices, devCap);
     int received = 0;
+    const auto t0 = std::chrono::steady_clock::now();
     auto take = [&](int wait) -> int {
         gail_packet pkt;
         std::memset(&pkt, 0, sizeof pkt);
@@ -114,6 +140,7 @@ __attribute__((visibility("default"))) int probe_encode(int backend, int profile
         if (r == GAIL_EOF) break;
         if (r != GAIL_OK) st = r;
     }
+    if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (st != GAIL_OK) g_err = gail_encoder_error(e) ? gail_encoder_error(e) : gail_last_error();
     else if (received != count) {
         g_err = "not every frame came back";

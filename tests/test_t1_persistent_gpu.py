@@ -3,7 +3,7 @@ context modelling, the largest-first order, MQ coding and truncation lengths fro
 queues in turn. Its Tier-1 frames must equal the four-launch path's byte for byte: single
 frames through the plain encoder (2K and 4K, every pass and with early termination), and
 16 frames of all six DCI profiles plus two Y'CbCr PQ frames batched into shared launches by
-the engine."""
+the engine. Its bounded waits give up with a status bit instead of hanging."""
 import numpy as np
 import pytest
 
@@ -102,3 +102,29 @@ def test_engine_batches_one_launch_equals_four(dev):
     finally:
         eng.close()
         _persistent(False)
+
+
+@pytest.mark.gpu
+def test_queue_wait_gives_up_and_the_device_stays_usable(dev):
+    """The launch's failure detection without a fault: a wait on a flag that nothing sets,
+    its limit lowered to 200 ms, returns with the queue-wait status bit after about that
+    long, and a frame encoded afterwards equals one encoded before."""
+    import ctypes as C
+
+    import libgail_b200 as gb
+    L = gb.lib()
+    L.gb_t1_wait_selftest.argtypes = [C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]
+    W, H = 1998, 1080
+    frame = synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=404))
+    enc = dev.encoder(P.LayoutHolder(W, H, 0), P.rgb48_format(W, H), P.color_passthrough())
+    try:
+        before = enc.encode(frame)[0]
+        status, ms = C.c_uint32(), C.c_float()
+        gb.check(L.gb_t1_wait_selftest(200, C.byref(status), C.byref(ms)))
+        assert status.value == 16, f"status {status.value}"
+        assert 190.0 <= ms.value <= 1200.0, f"the wait took {ms.value:.1f} ms"
+        assert _same(enc.encode(frame)[0], before)
+    finally:
+        enc.close()
+    with pytest.raises(gb.GailError):
+        gb.check(L.gb_t1_wait_selftest(0, C.byref(status), None))
