@@ -4,16 +4,20 @@
 // Tier-1 (decodeKernel): one code-block per warp at a time, decoded by its lane 0 (the
 // decode's control flow depends on every decoded bit, so lanes of one warp decoding
 // different blocks would only run one after another); up to 32 such warps per SM pull
-// blocks from a device queue ordered longest codeword first (orderKernel). A block's state is kept as row masks in
-// shared memory (significance and sign for rows -1..32, coded-this-plane and refined),
-// the scan visits only columns that have something to code (bit scans over candidate
-// masks) with the rows above, at and below the sample in registers (one shared load per
-// sample), zero-coding and sign contexts come from shared tables keyed by the neighbour
-// bits, and the decoded words (sign, twice the magnitude plus the mid-point of the
-// planes not decoded) are built in place in the wavelet plane and turned into floats
-// (word * step / 2) when the block is done. Untrusted input: bytes past the codeword read
-// as 0xFF, a block whose bytes lie outside the codestream decodes as zero, and nothing
-// outside the block's own samples is written.
+// blocks from a device queue ordered longest codeword first (orderKernel), the heaviest
+// on SMs of their own. A block's state is kept as row masks in shared memory
+// (significance and sign for rows -1..32, coded-this-plane and refined); the scan visits
+// only columns that have something to code (bit scans over candidate masks) with the rows
+// above, at and below the sample in registers (one shared load per sample), zero-coding
+// and sign contexts come from shared tables keyed by the neighbour bits, the refinement
+// pass keeps its three contexts in registers, and the decoded words (sign, twice the
+// magnitude plus the mid-point of the planes not decoded) are built in shared memory and
+// written to the wavelet plane as floats (word * step / 2) when the block is done. The
+// decoding lane is a serial chain of dependent instructions, so its length in
+// instructions is its time, and the code is kept compact: the instruction cache holds it
+// (the same loops unrolled to keep whole stripes in registers ran 1.6x slower). Untrusted
+// input: bytes past the codeword read as 0xFF, a block whose bytes lie outside the
+// codestream decodes as zero, and nothing outside the block's own samples is written.
 //
 // Inverse wavelet (invLevelKernel): per level, 64 x 64 output tiles with a 4-sample halo
 // in the interleaved domain, rows then columns (the reference's order), whole-sample
@@ -177,6 +181,12 @@ struct MqDecoder {
     }
     __device__ __forceinline__ void renorm() {
         int n = __clz(A) - 16;
+        if (n <= CT) {  // the usual case: the bits are already in C
+            A <<= n;
+            C <<= n;
+            CT -= n;
+            return;
+        }
         do {
             if (CT == 0) bytein();
             const int s = min(n, CT);
@@ -185,6 +195,25 @@ struct MqDecoder {
             CT -= s;
             n -= s;
         } while (n > 0);
+    }
+    // One decision in the context whose state word t a register holds (updated in place).
+    __device__ __forceinline__ uint32_t decodeIn(uint32_t& t, const uint32_t* tab) {
+        const uint32_t qe = t & 0xFFFFu, mps = (t >> 16) & 1u;
+        A -= qe;
+        bool lps;
+        if ((C >> 16) < qe) {
+            lps = A >= qe;
+            A = qe;
+        } else {
+            C -= qe << 16;
+            if (A & 0x8000u) return mps;
+            lps = A < qe;
+        }
+        const uint32_t nidx = lps ? (t >> 24) & 63u : (t >> 18) & 63u;
+        const uint32_t nm = mps ^ (lps ? (t >> 17) & 1u : 0u);
+        t = tab[nidx] | (nm << 16);
+        renorm();
+        return lps ? mps ^ 1u : mps;
     }
     // One decision in context cx (state word: table entry | mps << 16).
     __device__ __forceinline__ uint32_t decode(uint32_t* ctx, int cx, const uint32_t* tab) {
@@ -307,6 +336,13 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
         const int passes = code.passes;
         for (int p = nbps - 1; p >= 0 && done < passes; --p) {
             for (int type = (p == nbps - 1 ? 2 : 0); type < 3 && done < passes; ++type, ++done) {
+                // the refinement pass keeps its three contexts (14-16) in registers
+                uint32_t t14 = 0, t15 = 0, t16 = 0;
+                if (type == 1) {
+                    t14 = s_ctx[14];
+                    t15 = s_ctx[15];
+                    t16 = s_ctx[16];
+                }
                 // stripes of four rows from y0; rows y0-1..y0+4 lie in -1..32 (y0 <= 28) and
                 // rows at or past h are zero. Each column is scanned top to bottom with the
                 // rows above, at and below the sample in U, M, D.
@@ -366,8 +402,12 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                             const uint32_t nc = bt(n4[0], x) | bt(n4[1], x) << 1 | bt(n4[2], x) << 2 | bt(n4[3], x) << 3;
                             for (uint32_t m = ec; m; m &= m - 1) {
                                 const int k = __ffs(m) - 1;
-                                const int cx = bt(rc, k) ? 16 : (bt(nc, k) ? 15 : 14);
-                                const uint32_t bit = b.mq.decode(s_ctx, cx, s_tab);
+                                const bool c16 = bt(rc, k), c15 = bt(nc, k);
+                                uint32_t t = c16 ? t16 : (c15 ? t15 : t14);
+                                const uint32_t bit = b.mq.decodeIn(t, s_tab);
+                                if (c16) t16 = t;
+                                else if (c15) t15 = t;
+                                else t14 = t;
                                 uint32_t& word = s_word[(y0 + k) * 32 + x];
                                 word = bit ? word + (1u << p) : word - (1u << p);
                             }
@@ -429,6 +469,11 @@ __global__ void __launch_bounds__(DEC_THREADS) decodeKernel(DecArgs a) {
                             }
                         }
                     }
+                }
+                if (type == 1) {
+                    s_ctx[14] = t14;
+                    s_ctx[15] = t15;
+                    s_ctx[16] = t16;
                 }
             }
             for (int i = 0; i < 32; ++i) s_vis[i] = 0;

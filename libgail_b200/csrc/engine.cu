@@ -837,6 +837,7 @@ void EncodeEngine::codestreamWorker(int id) {
         }
         r->latency = msBetween(r->t0, Clock::now());
         done_.push_back(r);
+        --encActive_;
         stats_.frames++;
         cvDone_.notify_all();
     }
@@ -887,6 +888,7 @@ bool EncodeEngine::admit() {
     for (;;) {
         Request* r;
         Slot* s = nullptr;
+        bool grow = false;
         {
             std::lock_guard<std::mutex> lock(m_);
             if (pending_.empty()) break;
@@ -896,12 +898,19 @@ bool EncodeEngine::admit() {
                 s = c.free.back();
                 c.free.pop_back();
             }
+            // a new slot only while fewer frames than the pipeline's depth (four batches)
+            // are in progress: more would only wait on the device, and making a slot
+            // (device memory, a graph) stalls serving, so that under a burst every slot
+            // made beyond the depth made the backlog longer (finished frames whose results
+            // the caller still holds do not count)
+            grow = encActive_ < 4 * maxBatch_;
         }
-        if (!s) s = newSlot(*classes_[r->cls]);
+        if (!s && grow) s = newSlot(*classes_[r->cls]);
         if (!s) break;  // first in, first admitted: later requests wait too
         {
             std::lock_guard<std::mutex> lock(m_);
             pending_.pop_front();
+            ++encActive_;
         }
         Class& c = *classes_[r->cls];
         r->slot = s;
@@ -1069,6 +1078,7 @@ bool EncodeEngine::collect(Batch& b) {
             csq_.push_back(r);
         } else {
             done_.push_back(r);
+            --encActive_;
             stats_.frames++;
             const Slot* s = r->slot;
             stats_.d2hBytes += (uint64_t)s->n * 20 + (uint64_t)s->hTot[1] * 17 + s->hTot[0];

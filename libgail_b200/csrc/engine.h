@@ -179,6 +179,7 @@ private:
     mutable std::mutex m_;
     std::condition_variable cvDone_, cvWork_;
     std::deque<Request*> pending_;    // submitted, not admitted
+    int encActive_ = 0;               // encode requests admitted and not yet finished
     std::vector<Request*> front_q_;   // front end enqueued, not yet in a batch
     std::deque<Request*> done_;       // finished, not yet handed out
     std::atomic<bool> stop_{false};
