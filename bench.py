@@ -308,13 +308,15 @@ def run_ours(args):
 
     # ---- served: the batched engine, rate control and Tier-2 on the device -------------
     # a budget of 48 frame slots: deep enough to keep two Tier-1 batches and the front ends
-    # busy; every slot is made during the warm-up, none inside the timed region
+    # busy; all of them reserved up front (serving capacity set up before the first request),
+    # none made inside the timed region
     probe = Engine(local, 0, max_batch=args.batch)
     _, frame_bytes = probe.add_encoder(lay, fmt, col)
     probe.close()
     eng = Engine(local, 48 * frame_bytes + 1, max_batch=args.batch)
     eng.set_policy(policy["maxBatch"], policy["minBatchPct"], policy["maxWaitMs"])
     cid, frame_bytes = eng.add_encoder(lay, fmt, col)
+    eng.reserve(cid, 48)
     eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
     served_cs, kept_cs = [], []
 
@@ -409,6 +411,7 @@ def run_ours(args):
     eng = Engine(local, 48 * frame_bytes + 1, max_batch=args.batch)
     eng.set_policy(policy["maxBatch"], policy["minBatchPct"], policy["maxWaitMs"])
     cid_et, _ = eng.add_encoder(lay, fmt, col)
+    eng.reserve(cid_et, 48)
     eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
     eng.set_slope_factor(ET_FACTOR)
     et_res = []
@@ -684,9 +687,10 @@ def run_six_profiles(local, dev, workers, count=16, repeat=4):
         eng = Engine(local, 0, max_batch=count)
         eng.set_policy(count, 100, 5.0)
         cls = {p: eng.add_encoder(lays[p], P.rgb48_format(p[0], p[1]), P.color_passthrough())[0] for p in SIX_PROFILES}
+        for p in SIX_PROFILES:  # a slot for every frame of the burst, reserved up front
+            eng.reserve(cls[p], repeat * profs.count(p))
         eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
-        # the warm-up burst as large as the timed one: it makes every frame slot the timed
-        # run uses (a slot made while serving allocates and stalls the device)
+        # a warm-up burst as large as the timed one
         drain(eng, [eng.submit(cls[p], f) for _ in range(repeat) for p, f in zip(profs, pinned)])
         t0 = time.perf_counter()
         drain(eng, [eng.submit(cls[p], f) for _ in range(repeat) for p, f in zip(profs, pinned)])
@@ -738,6 +742,8 @@ def run_mixed(args, local, dev, lay4k, fmt4k, col4k, frames4k, streams4k, frame_
     try:
         e4, _ = eng.add_encoder(lay4k, fmt4k, col4k)
         e2, _ = eng.add_encoder(lay2k, fmt2k, col2k)
+        eng.reserve(e4, 32)
+        eng.reserve(e2, 24)
         d4, _ = eng.add_decoder(lay4k)
         d2, _ = eng.add_decoder(lay2k)
         eng.set_codestream(fps=FPS, label=CS.DEFAULT_LABEL, tag="b200", threads=workers)

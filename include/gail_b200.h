@@ -151,6 +151,11 @@ GB_API int gb_encoder_stage_times(GailCudaEncoder* e, double* ms5, int* count);
  *                          frames in flight (0: 90 % of the free memory)
  *   gb_engine_add_encoder  a frame class (layout, input format, colour); frameBytes: its
  *                          device footprint per frame in flight
+ *   gb_engine_reserve      make frame slots for a class now, until it has `slots` of them (or
+ *                          the budget is spent; *have: how many it has): capacity set up
+ *                          before serving. Otherwise a slot is made when a frame finds none
+ *                          free, by a thread of the engine's own, while fewer frames than
+ *                          eight batches are in progress (making one takes tens of ms)
  *   gb_engine_submit       queue one frame (host memory, pinned for speed, or device memory
  *                          with onDevice); the frame must stay valid until it is released
  *   gb_engine_wait         the next finished frame (id -1 after timeoutMs without one), its
@@ -224,6 +229,7 @@ GB_API int gb_engine_create(int device, uint64_t hbmBudget, int maxBatch, GbEngi
 GB_API void gb_engine_destroy(GbEngine* e);
 GB_API int gb_engine_add_encoder(GbEngine* e, const GailCudaLayout* layout, const GailCudaEncodeSettings* settings,
                                  int* classId, uint64_t* frameBytes);
+GB_API int gb_engine_reserve(GbEngine* e, int classId, int slots, int* have);
 GB_API int gb_engine_submit(GbEngine* e, int classId, const void* frame, int onDevice, double slope, int64_t* id);
 GB_API int gb_engine_wait(GbEngine* e, int timeoutMs, int64_t* id, GailCudaTier1* out, double* latencyMs,
                           int* frameStatus);

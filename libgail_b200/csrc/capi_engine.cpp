@@ -39,6 +39,14 @@ GB_API int gb_engine_add_encoder(GbEngine* e, const GailCudaLayout* layout, cons
     });
 }
 
+GB_API int gb_engine_reserve(GbEngine* e, int classId, int slots, int* have) {
+    return gbGuard([&] {
+        if (!e || slots < 0) throw std::logic_error("bad argument");
+        const int h = e->e->reserve(classId, slots);
+        if (have) *have = h;
+    });
+}
+
 GB_API int gb_engine_submit(GbEngine* e, int classId, const void* frame, int onDevice, double slope, int64_t* id) {
     return gbGuard([&] {
         if (!e || !id) throw std::logic_error("null argument");

@@ -180,6 +180,7 @@ EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(
         check(cudaHostAlloc((void**)&b->hCtl, 64, cudaHostAllocDefault), "pinned host memory");
     }
     worker_ = std::thread([this] { run(); });
+    maker_ = std::thread([this] { slotMaker(); });
 }
 
 EncodeEngine::~EncodeEngine() {
@@ -188,6 +189,8 @@ EncodeEngine::~EncodeEngine() {
         stop_ = true;
     }
     cvWork_.notify_all();
+    cvMake_.notify_all();
+    if (maker_.joinable()) maker_.join();
     if (worker_.joinable()) worker_.join();
     cvCs_.notify_all();
     for (auto& t : csWorkers_)
@@ -272,6 +275,7 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
     {
         std::lock_guard<std::mutex> lock(m_);
         classes_.push_back(std::move(c));
+        making_.push_back(0);
         if (csOn_ && cs_.onDevice) prepareRc();
         id = (int)classes_.size() - 1;
     }
@@ -359,16 +363,70 @@ uint64_t EncodeEngine::budgetLocked() {
     return budget_;
 }
 
-EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
+int EncodeEngine::reserve(int cls, int n) {
+    int have;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        if (cls < 0 || cls >= (int)classes_.size()) throw std::logic_error("unknown frame class");
+        have = 0;
+        for (auto& s : slots_) have += s->cls == cls;
+    }
+    while (have < n) {
+        Slot* s = newSlot(cls);
+        if (!s) break;
+        std::lock_guard<std::mutex> lock(m_);
+        classes_[cls]->free.push_back(s);
+        ++have;
+        cvWork_.notify_all();
+    }
+    return have;
+}
+
+// Makes the frame slots admit() asks for, one at a time, and hands each to its class.
+void EncodeEngine::slotMaker() {
+    try {
+        GB_CHECK(cudaSetDevice(dev_));
+        for (;;) {
+            int cls;
+            {
+                std::unique_lock<std::mutex> lock(m_);
+                cvMake_.wait(lock, [&] { return stop_.load() || !makeQ_.empty(); });
+                if (stop_) return;
+                cls = makeQ_.front();
+                makeQ_.pop_front();
+            }
+            Slot* s = newSlot(cls);
+            std::lock_guard<std::mutex> lock(m_);
+            --making_[cls];
+            if (s) classes_[cls]->free.push_back(s);
+            else slotsFull_ = true;
+            cvWork_.notify_all();
+        }
+    } catch (const std::exception& e) {
+        std::lock_guard<std::mutex> lock(m_);
+        if (error_.empty()) error_ = e.what();
+        cvDone_.notify_all();
+    }
+}
+
+EncodeEngine::Slot* EncodeEngine::newSlot(int cls) {
+    Class* cp;
+    int index;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        cp = classes_[cls].get();
+        index = (int)slots_.size();
+    }
+    Class& c = *cp;
+    if (index >= 1024) return nullptr;
     {
         std::lock_guard<std::mutex> lock(budgetM_);
         if (used_ + c.slotBytes > budgetLocked()) return nullptr;
         used_ += c.slotBytes;  // reserved now, given back if the slot cannot be made
     }
     auto s = std::make_unique<Slot>();
-    s->cls = (int)(std::find_if(classes_.begin(), classes_.end(), [&](auto& p) { return p.get() == &c; }) - classes_.begin());
-    s->index = (int)slots_.size();
-    if (s->index >= 1024) return nullptr;
+    s->cls = cls;
+    s->index = index;
     s->n = (uint32_t)c.z.n;
     auto alloc = [&](auto*& p, uint64_t bytes) {
         void* q = nullptr;
@@ -441,13 +499,13 @@ EncodeEngine::Slot* EncodeEngine::newSlot(Class& c) {
         return nullptr;  // out of memory now: the request waits for a slot to free up
     }
     Slot* raw = s.get();
-    slots_.push_back(std::move(s));
     uint64_t used;
     {
         std::lock_guard<std::mutex> lock(budgetM_);
         used = used_;
     }
     std::lock_guard<std::mutex> lock(m_);
+    slots_.push_back(std::move(s));
     stats_.slots = slots_.size();
     stats_.slotBytes = used;
     return raw;
@@ -888,7 +946,6 @@ bool EncodeEngine::admit() {
     for (;;) {
         Request* r;
         Slot* s = nullptr;
-        bool grow = false;
         {
             std::lock_guard<std::mutex> lock(m_);
             if (pending_.empty()) break;
@@ -897,15 +954,17 @@ bool EncodeEngine::admit() {
             if (!c.free.empty()) {
                 s = c.free.back();
                 c.free.pop_back();
+            } else if (!slotsFull_ && making_[r->cls] == 0 && encActive_ < std::max(32, 8 * maxBatch_)) {
+                // a new slot, made by the slot thread while this one keeps serving; only
+                // while fewer frames than the pipeline's depth are in progress (eight
+                // batches: two in Tier-1, the next ones' front ends, the frames whose
+                // codestreams the host workers are making): more would only wait, and
+                // finished frames whose results the caller still holds do not count
+                ++making_[r->cls];
+                makeQ_.push_back(r->cls);
+                cvMake_.notify_one();
             }
-            // a new slot only while fewer frames than the pipeline's depth (four batches)
-            // are in progress: more would only wait on the device, and making a slot
-            // (device memory, a graph) stalls serving, so that under a burst every slot
-            // made beyond the depth made the backlog longer (finished frames whose results
-            // the caller still holds do not count)
-            grow = encActive_ < 4 * maxBatch_;
         }
-        if (!s && grow) s = newSlot(*classes_[r->cls]);
         if (!s) break;  // first in, first admitted: later requests wait too
         {
             std::lock_guard<std::mutex> lock(m_);

@@ -52,6 +52,10 @@ public:
     // A frame class: one layout, input format and colour setting. Returns its id and the
     // device bytes one of its frames in flight takes.
     int addClass(const GailCudaLayout& layout, const GailCudaEncodeSettings& s, uint64_t* frameBytes);
+    // Makes frame slots for class cls now, on the calling thread, until it has n (or the
+    // budget is spent); returns how many it has. Slots asked for while serving are made by
+    // the slot thread instead, one at a time.
+    int reserve(int cls, int n);
     // Queues a frame of class cls: frame is host memory (pinned for a fast upload) or,
     // with onDevice, device memory; it must stay valid until the frame is released.
     int64_t submit(int cls, const void* frame, bool onDevice, double slope);
@@ -151,7 +155,8 @@ private:
     bool admit();
     bool launchBatch(Batch& b);
     bool collect(Batch& b);
-    Slot* newSlot(Class& c);
+    Slot* newSlot(int cls);
+    void slotMaker();
     DecSlot* newDecSlot(int cls);
     void sizeBatches();
     void growBatch(Batch& b, uint64_t blocks, uint64_t poolBytes);
@@ -180,6 +185,13 @@ private:
     std::condition_variable cvDone_, cvWork_;
     std::deque<Request*> pending_;    // submitted, not admitted
     int encActive_ = 0;               // encode requests admitted and not yet finished
+    // frame slots are made on a thread of their own: device memory, pinned host memory and a
+    // graph take tens of milliseconds, in which the serving thread would launch nothing
+    std::thread maker_;
+    std::condition_variable cvMake_;
+    std::deque<int> makeQ_;           // classes a slot is wanted for
+    std::vector<int> making_;         // per class: slots asked for, not yet made
+    bool slotsFull_ = false;          // a slot could not be made (budget or memory): ask no more
     std::vector<Request*> front_q_;   // front end enqueued, not yet in a batch
     std::deque<Request*> done_;       // finished, not yet handed out
     std::atomic<bool> stop_{false};

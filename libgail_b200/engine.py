@@ -17,6 +17,7 @@ def _bind():
     L.gb_engine_destroy.argtypes = [C.c_void_p]
     L.gb_engine_destroy.restype = None
     L.gb_engine_add_encoder.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]
+    L.gb_engine_reserve.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
     L.gb_engine_submit.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_int64)]
     L.gb_engine_wait.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(Tier1), C.POINTER(C.c_double),
                                  C.POINTER(C.c_int)]
@@ -67,6 +68,13 @@ class Engine:
         check(lib().gb_engine_add_encoder(self.h, C.byref(layout.abi), C.byref(s), C.byref(cid), C.byref(nbytes)))
         self._classes.append((layout, s))
         return cid.value, nbytes.value
+
+    def reserve(self, cls: int, slots: int) -> int:
+        """Makes frame slots for class cls now, until it has `slots` (or the HBM budget is
+        spent): serving capacity set up before the first request. Returns how many it has."""
+        have = C.c_int()
+        check(lib().gb_engine_reserve(self.h, cls, slots, C.byref(have)))
+        return have.value
 
     def submit(self, cls: int, frame, slope: float = 0.0) -> int:
         """frame: a numpy array (host) or a torch CUDA tensor (device)."""

@@ -27,7 +27,8 @@ PROFILES = [(3996, 2160, 1, 0.50), (1998, 1080, 0, 0.30), (2048, 858, 0, 0.05), 
             (4096, 1716, 1, 0.05), (4096, 2160, 1, 0.05)]
 ENCODE_SHARE = 0.7
 FRAMES_PER_PROFILE = 4
-WARM_BURST = 8  # requests of each class at once before the timed loads: the slots they use
+WARM_BURST = 8  # requests of each class at once before the timed loads
+RESERVE = 16    # frame slots reserved per encode class before serving
 
 
 def arrivals(n: int, rate: float, seed: int) -> np.ndarray:
@@ -75,6 +76,7 @@ def serve(requests: int, loads, budget_gb: float, workers: int, seed: int, log=p
             frames.append([torch.from_numpy(synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=seed * 1000 + 10 * i + k))
                                             .view(np.int16)).pin_memory() for k in range(FRAMES_PER_PROFILE)])
             enc_cls.append(eng.add_encoder(lay, P.rgb48_format(W, H), P.color_passthrough())[0])
+            eng.reserve(enc_cls[-1], RESERVE)  # serving capacity set up before the requests
             dec_cls.append(eng.add_decoder(lay)[0])
         eng.set_codestream(label=CS.DEFAULT_LABEL, tag="b200", threads=workers)
         # the codestreams to decode, made by this engine; this also makes every class's slots
@@ -91,8 +93,7 @@ def serve(requests: int, loads, budget_gb: float, workers: int, seed: int, log=p
             p, k = ids[rid]
             streams[p][k] = cs
             eng.release(rid)
-        # a burst of every class at once: the engine makes the frame and decoder slots the timed
-        # loads will use (making one while serving stalls the device)
+        # a burst of every class at once before the timed loads
         warm = [eng.submit(enc_cls[p], frames[p][k % FRAMES_PER_PROFILE]) for p in range(len(PROFILES))
                 for k in range(WARM_BURST)]
         warm += [eng.submit_decode(dec_cls[p], streams[p][k % FRAMES_PER_PROFILE]) for p in range(len(PROFILES))

@@ -307,3 +307,32 @@ def test_engine_early_termination(dev):
     finally:
         eng.close()
         enc.close()
+
+
+@pytest.mark.gpu
+def test_engine_reserve_makes_slots_up_front(dev):
+    """Slots reserved before serving are the ones frames use (no slot is made while the
+    burst runs), and a reservation stops at the HBM budget."""
+    W, H = 1998, 1080
+    lay = P.LayoutHolder(W, H, 0)
+    frame = synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=808))
+    eng = Engine(0, 0, max_batch=4)
+    try:
+        cid, frame_bytes = eng.add_encoder(lay, P.rgb48_format(W, H), P.color_passthrough())
+        assert eng.reserve(cid, 5) == 5
+        assert eng.stats()["slots"] == 5
+        assert eng.reserve(cid, 3) == 5  # it has five already
+        ids = [eng.submit(cid, frame) for _ in range(5)]
+        for _ in ids:
+            rid, _, _, st = eng.wait(60000, copy=False)
+            assert rid >= 0 and st == 0
+            eng.release(rid)
+        assert eng.stats()["slots"] == 5
+    finally:
+        eng.close()
+    eng = Engine(0, 2 * frame_bytes + 1, max_batch=4)
+    try:
+        cid, _ = eng.add_encoder(lay, P.rgb48_format(W, H), P.color_passthrough())
+        assert eng.reserve(cid, 5) == 2
+    finally:
+        eng.close()
