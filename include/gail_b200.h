@@ -116,6 +116,9 @@ typedef struct GbTuning {
     int32_t t1Persistent;
     int32_t decHeavyPct;  /* Tier-1 decode: blocks whose codeword exceeds this % of the mean bytes per
                              decoding warp run on SMs of their own, four per SM (0: none) */
+    int32_t dwtTile1, dwtTileN;  /* encoder front-end tile at level 1 and at levels 2..: 0 = 64 x 64,
+                                    1 = 128 x 64, 2 = 64 x 128 (same coefficients; read when an
+                                    encoder or engine frame slot is made) */
 } GbTuning;
 GB_API int gb_set_tuning(int profile, const GbTuning* t);
 GB_API int gb_get_tuning(int profile, GbTuning* t);

@@ -1,7 +1,8 @@
 """The project's autotuner: per frame profile (2K, 4K) on this GPU, the launch knobs whose
-best value depends on the workload and the device -- the MQ solo threshold, the grid caps of
-context modelling, MQ coding and Tier-1 decoding, Tier-1 as one persistent launch or four --
-and the engine's batch policy, chosen by
+best value depends on the workload and the device -- the front end's tile shape at level 1
+and at the later levels (64 x 64, 128 x 64, 64 x 128), the MQ solo threshold, the grid caps
+of context modelling, MQ coding and Tier-1 decoding, Tier-1 as one persistent launch or
+four, the decoder's heavy-block threshold -- and the engine's batch policy, chosen by
 timing candidates on seeded synthetic frames. Every candidate gives bit-identical output
 (the knobs change launch shapes and work order, never the arithmetic), so only speed is
 compared. The result is a JSON file keyed by the GPU's name; apply() loads it into the
@@ -21,14 +22,15 @@ import numpy as np
 from . import check, lib
 
 DEFAULTS = {"soloDecisions": 16384, "cmCtasPerSm": 16, "mqCtasPerSm": 16, "decCtasPerSm": 32, "t1Persistent": 0,
-            "decHeavyPct": 150}
+            "decHeavyPct": 150, "dwtTile1": 0, "dwtTileN": 0}
 POLICY_DEFAULT = {"maxBatch": 16, "minBatchPct": 25, "maxWaitMs": 2.0}
 PROFILES = {"2k": 0, "4k": 1}
 
 
 class GbTuning(C.Structure):
     _fields_ = [("soloDecisions", C.c_uint32), ("cmCtasPerSm", C.c_int32), ("mqCtasPerSm", C.c_int32),
-                ("decCtasPerSm", C.c_int32), ("t1Persistent", C.c_int32), ("decHeavyPct", C.c_int32)]
+                ("decCtasPerSm", C.c_int32), ("t1Persistent", C.c_int32), ("decHeavyPct", C.c_int32),
+                ("dwtTile1", C.c_int32), ("dwtTileN", C.c_int32)]
 
 
 def _bind():
@@ -135,7 +137,7 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
             torch.cuda.synchronize()
             enc = dev.encoder(lay, fmt, col)
 
-            def tier1_ms(cfg):  # context modelling + MQ, per frame, plain one-frame launches
+            def stage_ms(cfg, stages):  # the stages' device time per frame, plain one-frame launches
                 set_tuning(prof, cfg)
                 for f in dframes[:2]:
                     check(L.gb_encoder_enqueue_device(enc.h, C.c_void_p(f.data_ptr())))
@@ -147,7 +149,13 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
                     check(L.gb_encoder_enqueue_device(enc.h, C.c_void_p(f.data_ptr())))
                 check(L.gb_encoder_stage_times(enc.h, ms5.ctypes.data, C.byref(cnt)))
                 check(L.gb_encoder_stage_timing(enc.h, 0))
-                return float(ms5[1] + ms5[3]) / max(cnt.value, 1)
+                return float(sum(ms5[k] for k in stages)) / max(cnt.value, 1)
+
+            def tier1_ms(cfg):  # context modelling + MQ
+                return stage_ms(cfg, (1, 3))
+
+            def front_ms(cfg):  # colour + wavelet + quantisation
+                return stage_ms(cfg, (0,))
 
             eng = Engine(0, 0, max_batch=POLICY_DEFAULT["maxBatch"])
             cid, _ = eng.add_encoder(lay, fmt, col)
@@ -164,6 +172,9 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
                 return (time.perf_counter() - t0) * 1e3 / len(dframes)
 
             cfg = dict(DEFAULTS)
+            log(f"[{name}] front-end tile shapes (front-end ms per frame)")
+            tiles = {"dwtTile1": [1, 2], "dwtTileN": [1, 2]}
+            cfg, _, seen0 = coordinate_search(cfg, tiles, _best_of(front_ms, runs), log=log)
             log(f"[{name}] MQ solo threshold (Tier-1 ms per frame)")
             solo = {"soloDecisions": [4096, 8192, 32768, 1 << 30]}
             cfg, _, seen1 = coordinate_search(cfg, solo, _best_of(tier1_ms, runs), log=log)
@@ -224,7 +235,7 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
             eng.close()
             enc.close()
             out["profiles"][name] = cfg
-            out["measured"][name] = [[c, round(v, 4)] for c, v in seen1 + seen2 + seen3]
+            out["measured"][name] = [[c, round(v, 4)] for c, v in seen0 + seen1 + seen2 + seen3]
             set_tuning(prof, None)
     finally:
         dev.close()

@@ -77,6 +77,8 @@ GB_API int gb_set_tuning(int profile, const GbTuning* t) {
         v.decCtasPerSm = t->decCtasPerSm;
         v.t1Persistent = t->t1Persistent;
         v.decHeavyPct = t->decHeavyPct;
+        v.dwtTile1 = t->dwtTile1;
+        v.dwtTileN = t->dwtTileN;
         setTuning(profile, v);
     });
 }
@@ -86,7 +88,8 @@ GB_API int gb_get_tuning(int profile, GbTuning* t) {
         if (!t) throw std::logic_error("null argument");
         if (profile != 0 && profile != 1) throw std::logic_error("tuning profile must be 0 (2K) or 1 (4K)");
         const Tuning v = tuningFor(profile);
-        *t = {v.soloDecisions, v.cmCtasPerSm, v.mqCtasPerSm, v.decCtasPerSm, v.t1Persistent, v.decHeavyPct};
+        *t = {v.soloDecisions, v.cmCtasPerSm, v.mqCtasPerSm, v.decCtasPerSm, v.t1Persistent, v.decHeavyPct,
+              v.dwtTile1, v.dwtTileN};
     });
 }
 

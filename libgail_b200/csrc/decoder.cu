@@ -695,6 +695,7 @@ DecoderSlot::DecoderSlot(int device, const Layout& L, const GailCudaDecodeSettin
         GB_CHECK(cudaSetDevice(dev_));
         GB_CHECK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
         for (auto& e : ev_) GB_CHECK(cudaEventCreate(&e));
+        for (auto& e : bandEv_) GB_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         const uint64_t npix = (uint64_t)L.width * L.height, ll = (uint64_t)L.levelW(1) * L.levelH(1);
         const uint64_t n = (uint64_t)L.numCblks();
         auto alloc = [&](auto*& p, uint64_t bytes) {
@@ -756,6 +757,11 @@ void DecoderSlot::release() {
             cudaEventDestroy(e);
             e = nullptr;
         }
+    for (auto& e : bandEv_)
+        if (e) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
     if (st_) cudaStreamDestroy(st_);
     st_ = nullptr;
     cudaGetLastError();
@@ -763,15 +769,27 @@ void DecoderSlot::release() {
 
 void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, const GbCblkCode* blocks, size_t numBlocks,
                          void* dst, ptrdiff_t strideBytes, GailCudaDecodeTimings* tm) {
-    enqueue(frame, data, size, blocks, numBlocks, tm && tm->wantWavelet);
-    const uint16_t* pic = finish(tm);
-    // the picture from the pinned buffer into the caller's rows, in bands on the host pool
-    // and the calling thread (52 MB at 4K: one thread's copy took longer than the decode)
     const uint64_t rowBytes = (uint64_t)outW_ * 6;
-    constexpr int kBands = 8;
+    // page-locked caller rows (a serving layer's pinned buffers): the picture goes there
+    // from the device directly
+    cudaPointerAttributes at{};
+    const bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost &&
+                        strideBytes >= (ptrdiff_t)rowBytes;
+    cudaGetLastError();
+    if (pinned) {
+        enqueue(frame, data, size, blocks, numBlocks, tm && tm->wantWavelet, dst, strideBytes);
+        finish(tm);
+        return;
+    }
+    // pageable rows: the picture comes back in bands, and the host pool copies each band
+    // into the caller's rows as soon as it has arrived, while the next bands are in flight
+    // (52 MB at 4K: copied after the whole download it added its full time to the decode)
+    enqueue(frame, data, size, blocks, numBlocks, tm && tm->wantWavelet, nullptr, 0, kBands);
     parallelFor(kBands, [&](int k) {
+        GB_CHECK(cudaSetDevice(dev_));
+        GB_CHECK(cudaEventSynchronize(bandEv_[k]));
         const int y0 = (int)((int64_t)outH_ * k / kBands), y1 = (int)((int64_t)outH_ * (k + 1) / kBands);
-        const uint8_t* src = (const uint8_t*)pic + (uint64_t)y0 * rowBytes;
+        const uint8_t* src = (const uint8_t*)hOut_ + (uint64_t)y0 * rowBytes;
         uint8_t* out = (uint8_t*)dst + (ptrdiff_t)y0 * strideBytes;
         if (strideBytes == (ptrdiff_t)rowBytes) {
             std::memcpy(out, src, rowBytes * (uint64_t)(y1 - y0));
@@ -779,11 +797,12 @@ void DecoderSlot::decode(const Layout& frame, const uint8_t* data, size_t size, 
             for (int y = y0; y < y1; ++y, src += rowBytes, out += strideBytes) std::memcpy(out, src, rowBytes);
         }
     });
-    if (tm) tm->total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
+    finish(tm);
 }
 
 void DecoderSlot::enqueue(const Layout& frame, const uint8_t* data, size_t size, const GbCblkCode* blocks,
-                          size_t numBlocks, bool wantWavelet) {
+                          size_t numBlocks, bool wantWavelet, void* pinnedDst, ptrdiff_t dstStride, int bands) {
+    if (bands < 1 || bands > kBands) throw std::logic_error("picture bands out of range");
     t0_ = std::chrono::steady_clock::now();
     if (frame.width != L_.width || frame.height != L_.height || frame.levels != L_.levels ||
         frame.bands.size() != L_.bands.size() || (int)numBlocks != L_.numCblks())
@@ -861,8 +880,18 @@ void DecoderSlot::enqueue(const Layout& frame, const uint8_t* data, size_t size,
     }
     GB_CHECK(cudaGetLastError());
     GB_CHECK(cudaEventRecord(ev_[2], st));
-    const uint64_t outBytes = (uint64_t)outW_ * outH_ * 6;
-    GB_CHECK(cudaMemcpyAsync(hOut_, dOut_, outBytes, cudaMemcpyDeviceToHost, st));
+    const uint64_t rowBytes = (uint64_t)outW_ * 6;
+    if (pinnedDst) {
+        GB_CHECK(cudaMemcpy2DAsync(pinnedDst, (size_t)dstStride, dOut_, rowBytes, rowBytes, (size_t)outH_,
+                                   cudaMemcpyDeviceToHost, st));
+    } else {
+        for (int k = 0; k < bands; ++k) {
+            const uint64_t y0 = (uint64_t)outH_ * k / bands, y1 = (uint64_t)outH_ * (k + 1) / bands;
+            GB_CHECK(cudaMemcpyAsync((uint8_t*)hOut_ + y0 * rowBytes, (const uint8_t*)dOut_ + y0 * rowBytes,
+                                     (y1 - y0) * rowBytes, cudaMemcpyDeviceToHost, st));
+            if (bands > 1) GB_CHECK(cudaEventRecord(bandEv_[k], st));
+        }
+    }
     GB_CHECK(cudaMemcpyAsync(hCtl_, dCtl_, 64, cudaMemcpyDeviceToHost, st));
     GB_CHECK(cudaEventRecord(ev_[3], st));
 }

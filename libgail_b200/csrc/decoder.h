@@ -43,9 +43,12 @@ public:
     // The same in two halves: enqueue() copies the codestream and the blocks into the
     // slot's pinned buffers and starts every stage on the slot's stream; finish() waits,
     // checks the kernels' status and returns the picture in pinned host memory (outH rows
-    // of outW x 3 codes), valid until the next enqueue.
+    // of outW x 3 codes), valid until the next enqueue. With pinnedDst the picture goes from
+    // the device straight into those rows (page-locked host memory, dstStride bytes apart)
+    // instead; with bands > 1 it comes back in that many row bands, each recording
+    // bandDone(k) when it has arrived.
     void enqueue(const Layout& frame, const uint8_t* data, size_t size, const GbCblkCode* blocks, size_t numBlocks,
-                 bool wantWavelet);
+                 bool wantWavelet, void* pinnedDst = nullptr, ptrdiff_t dstStride = 0, int bands = 1);
     const uint16_t* finish(GailCudaDecodeTimings* tm);
     int outW() const { return outW_; }
     int outH() const { return outH_; }
@@ -59,6 +62,8 @@ private:
     bool heavySms_ = true;
     cudaStream_t st_ = nullptr;
     cudaEvent_t ev_[4] = {};
+    static constexpr int kBands = 8;
+    cudaEvent_t bandEv_[kBands] = {};  // a band of the picture has arrived in host memory
     std::vector<void*> allocs_;
     uint64_t capBytes_ = 0;
     float *dPlanes_ = nullptr, *dLL_[2] = {nullptr, nullptr}, *dHalf_ = nullptr;

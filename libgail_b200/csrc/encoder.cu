@@ -82,6 +82,7 @@ std::vector<double> blockScales(const Layout& L) {
 void launchFrontEnd(const Layout& L, const ColorArgs& c, float* ll0, float* ll1, uint64_t llFloats, uint32_t* coeffs,
                     float* tap, cudaStream_t st) {
     const int NL = L.levels;
+    const Tuning tu = tuningFor(L.profile);
     float* llBuf[2] = {ll0, ll1};
     for (int l = 1; l <= NL; ++l) {
         LevelArgs a{};
@@ -112,8 +113,8 @@ void launchFrontEnd(const Layout& L, const ColorArgs& c, float* ll0, float* ll1,
                 b.ncby = (b.h + 31) / 32;
             }
         }
-        if (l == 1) launchLevel1(c, a, st);
-        else launchLevel(a, st);
+        if (l == 1) launchLevel1(c, a, tu.dwtTile1, st);
+        else launchLevel(a, tu.dwtTileN, st);
     }
 }
 

@@ -1,16 +1,17 @@
 // Encoder front end: colour -> 9/7 DWT -> dead-zone quantisation, one kernel per level.
 //
-// Each CTA owns a 64 x 64 tile of the level's input, all three components, and loads it
-// with a 4-sample halo (72 x 72, whole-sample symmetric mirror at the image edges) into
-// shared memory. It lifts the columns, then the rows (the order of the reference, Annex
-// F.4.2): one thread per 72-sample line, in registers, the four lifting steps applied in
-// streaming order (alpha at j-1, beta at j-2, gamma at j-3, delta at j-4 as sample j
-// arrives), which gives every sample the same operands as step-by-step lifting. Then it
-// writes the four 32 x 32 subband pieces it produced. Because tiles are 64-aligned, each piece is
-// exactly one code-block of its band, so the high bands (and the LL band at the last
-// level) are quantised in registers and stored straight into the code-block-major
-// layout Tier-1 reads: 32 consecutive words per row, zero outside the band. The LL piece
-// of an intermediate level goes to a float plane for the next level.
+// Each CTA owns a tile of the level's input (64 x 64 by default; 128 x 64 or 64 x 128 by the
+// tuning knobs dwtTile1 / dwtTileN), all three components at level 1, one later, and loads
+// it with a 4-sample halo (whole-sample symmetric mirror at the image edges) into shared
+// memory. It lifts the columns, then the rows (the order of the reference, Annex F.4.2):
+// one thread per line, in registers, the four lifting steps applied in streaming order
+// (alpha at j-1, beta at j-2, gamma at j-3, delta at j-4 as sample j arrives), which gives
+// every sample the same operands as step-by-step lifting, so every tile shape gives the
+// same coefficients. Then it writes the subband pieces it produced. Because tiles are
+// 64-aligned, each piece is whole code-blocks of its band, so the high bands (and the LL
+// band at the last level) are quantised in registers and stored straight into the
+// code-block-major layout Tier-1 reads: 32 consecutive words per row, zero outside the
+// band. The LL piece of an intermediate level goes to a float plane for the next level.
 //
 // Level 1 also does the colour conversion in its tile loads (the frame is read once,
 // never written back as planes): R'G'B' from interleaved 16-bit or planar Y'CbCr,
@@ -38,10 +39,7 @@ namespace gb {
 
 namespace {
 
-constexpr int TS = 64, HALO = 4, TW = TS + 2 * HALO, TP = TW + 1;
-// level 1: the three components of a tile per CTA (the colour conversion yields all
-// three at once); later levels: one component per CTA
-constexpr int FE_THREADS_COLOR = 384, FE_THREADS_PLAIN = 128;
+constexpr int HALO = 4;
 // lifting coefficients alpha, beta, gamma, delta
 __device__ __forceinline__ constexpr float liftCoef(int s) {
     return s == 0 ? (float)-1.586134342059924
@@ -313,47 +311,61 @@ __device__ __forceinline__ void pixelCodes(const ColorArgs& c, const uint32_t rg
     for (int k = 0; k < 3; ++k) code[k] = dciCode(c.thr, clamp01(xyz[k] / 52.37f));
 }
 
-// One 72-sample line of a tile, `step` floats between samples: the four lifting steps
-// (x[i] += c * (x[i-1] + x[i+1]) on odd 1..69, even 2..70, odd, even), then the scaling of
-// the 64 samples the tile outputs, written back in place. Sample k is final once delta
-// has passed k + 1, so it is stored five samples behind the loads.
+// Tile shapes (the knob dwtTile1 / dwtTileN): 0 = 64 x 64, 1 = 128 x 64 (wide), 2 = 64 x 128
+// (tall) samples of the level's input, each with a 4-sample halo. A tile's band pieces
+// are whole code-blocks: CBX x CBY of them per band.
+template <int SHAPE>
+struct Tile {
+    static constexpr int X = SHAPE == 1 ? 128 : 64, Y = SHAPE == 2 ? 128 : 64;
+    static constexpr int WX = X + 2 * HALO, WY = Y + 2 * HALO, P = WX + 1;  // P: row pitch
+    static constexpr int CBX = X / 64, CBY = Y / 64;
+};
+
+// One line of N samples of a tile, `step` floats between samples: the four lifting steps
+// (x[i] += c * (x[i-1] + x[i+1]) on odd 1..N-3, even 2..N-2, odd, even), then the scaling
+// of the N - 8 samples the tile outputs, written back in place. Sample k is final once
+// delta has passed k + 1, so it is stored five samples behind the loads.
+template <int N>
 __device__ __forceinline__ void liftLine(float* t, int step) {
-    float x[TW];
+    float x[N];
 #pragma unroll
-    for (int j = 0; j < TW + 5; ++j) {
-        if (j < TW) x[j] = t[j * step];
+    for (int j = 0; j < N + 5; ++j) {
+        if (j < N) x[j] = t[j * step];
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             const int i = j - 1 - s;
             const bool odd = !(s & 1);
-            if (i >= (odd ? 1 : 2) && i <= (odd ? 69 : 70) && (i & 1) == (odd ? 1 : 0))
+            if (i >= (odd ? 1 : 2) && i <= (odd ? N - 3 : N - 2) && (i & 1) == (odd ? 1 : 0))
                 x[i] = x[i] + liftCoef(s) * (x[i - 1] + x[i + 1]);
         }
         const int k = j - 5;
-        if (k >= HALO && k < HALO + TS) t[k * step] = x[k] * ((k & 1) ? kHighScale : kLowScale);
+        if (k >= HALO && k < N - HALO) t[k * step] = x[k] * ((k & 1) ? kHighScale : kLowScale);
     }
 }
 
-// The tile's outputs for component comp: its code-block of each band (and LL floats).
-template <int THREADS>
+// The tile's outputs for component comp: its code-blocks of each band (and LL floats).
+template <int THREADS, int SHAPE>
 __device__ void writeOutputs(const LevelArgs& a, const float* t, int comp, int tx, int ty, int tid) {
-    const int x0 = tx * TS - HALO, y0 = ty * TS - HALO;
+    using T = Tile<SHAPE>;
+    const int x0 = tx * T::X - HALO, y0 = ty * T::Y - HALO;
     for (int o = 0; o < 4; ++o) {
         const BandOut& b = a.band[comp][o];
         const bool quant = o != 0 || a.last;
-        if (tx >= b.ncbx || ty >= b.ncby) continue;
-        uint32_t* blk = a.coeffs + ((size_t)b.cblkBase + (size_t)ty * b.ncbx + tx) * kCblkArea;
-        for (int idx = tid; idx < kCblkArea; idx += THREADS) {
-            const int i = idx & 31, j = idx >> 5;
-            const int bx = tx * 32 + i, by = ty * 32 + j;
+        for (int idx = tid; idx < T::CBX * T::CBY * kCblkArea; idx += THREADS) {
+            const int cb = idx >> 10, e = idx & (kCblkArea - 1);
+            const int cbx = tx * T::CBX + cb % T::CBX, cby = ty * T::CBY + cb / T::CBX;
+            if (cbx >= b.ncbx || cby >= b.ncby) continue;
+            const int i = e & 31, j = e >> 5;
+            const int bx = cbx * 32 + i, by = cby * 32 + j;
             const bool in = bx < b.w && by < b.h;
             float v = 0.f;
             if (in) {
                 const int gx = 2 * bx + (o & 1), gy = 2 * by + (o >> 1);
-                v = t[(gy - y0) * TP + (gx - x0)];
+                v = t[(gy - y0) * T::P + (gx - x0)];
             }
             if (quant) {
-                blk[idx] = in ? quantize(v, b.invDelta, b.maxMag) : 0u;
+                uint32_t* blk = a.coeffs + ((size_t)b.cblkBase + (size_t)cby * b.ncbx + cbx) * kCblkArea;
+                blk[e] = in ? quantize(v, b.invDelta, b.maxMag) : 0u;
                 if (in && a.tap) a.tap[comp * a.tapComp + (size_t)(b.py0 + by) * a.tapStride + b.px0 + bx] = v;
             } else if (in) {
                 a.ll[comp * a.llComp + (size_t)by * a.llStride + bx] = v;
@@ -362,21 +374,47 @@ __device__ void writeOutputs(const LevelArgs& a, const float* t, int comp, int t
     }
 }
 
+// Threads of a CTA: level 1 holds the three components of a tile, later levels one; enough
+// for a thread per column of every component and per output row.
+template <int MODE, int SHAPE>
+__host__ __device__ constexpr int feThreads() {
+    using T = Tile<SHAPE>;
+    constexpr int nc = MODE ? 3 : 1;
+    constexpr int need = (nc * T::WX > nc * T::Y ? nc * T::WX : nc * T::Y);
+    constexpr int base = MODE ? 384 : 128;
+    return ((need > base ? need : base) + 31) / 32 * 32;
+}
+template <int MODE, int SHAPE>
+__host__ __device__ constexpr size_t feSmem() {
+    using T = Tile<SHAPE>;
+    return (size_t)(MODE ? 3 : 1) * T::WY * T::P * 4;
+}
+// CTAs per SM the launch bounds ask for: as many as the shared memory allows (up to 8).
+template <int MODE, int SHAPE>
+__host__ __device__ constexpr int feMinCtas() {
+    constexpr size_t per = feSmem<MODE, SHAPE>() + 1024;
+    constexpr int fit = (int)((size_t)227 * 1024 / per);
+    constexpr int cap = MODE == 0 ? 8 : MODE == 1 ? 3 : 2;
+    return fit < 1 ? 1 : (fit < cap ? fit : cap);
+}
+
 // MODE 0: a later level from the previous LL planes; 1..3: level 1 with the colour route
-// of pixelCodes.
-template <int MODE>
-__global__ void __launch_bounds__(MODE ? FE_THREADS_COLOR : FE_THREADS_PLAIN, MODE == 0 ? 8 : MODE == 1 ? 3 : 2)
+// of pixelCodes. SHAPE: the tile shape.
+template <int MODE, int SHAPE>
+__global__ void __launch_bounds__(feThreads<MODE, SHAPE>(), feMinCtas<MODE, SHAPE>())
     levelKernel(ColorArgs c, LevelArgs a) {
     extern __shared__ float smem[];
+    using T = Tile<SHAPE>;
     constexpr bool COLOR = MODE != 0;
-    constexpr int THREADS = COLOR ? FE_THREADS_COLOR : FE_THREADS_PLAIN;
+    constexpr int THREADS = feThreads<MODE, SHAPE>();
     constexpr int NC = COLOR ? 3 : 1;
+    constexpr int PLANE = T::WY * T::P;
     const int tid = threadIdx.x, tx = blockIdx.x, ty = blockIdx.y;
-    const int x0 = tx * TS - HALO, y0 = ty * TS - HALO;
+    const int x0 = tx * T::X - HALO, y0 = ty * T::Y - HALO;
     const int w = a.w, h = a.h;
     if (COLOR) {
-        for (int idx = tid; idx < TW * TW; idx += THREADS) {
-            const int ly = idx / TW, lx = idx % TW;
+        for (int idx = tid; idx < T::WX * T::WY; idx += THREADS) {
+            const int ly = idx / T::WX, lx = idx % T::WX;
             const int gy = mirror(y0 + ly, h), gx = mirror(x0 + lx, w);
             uint32_t rgb[3];
             if (c.kind == 0) {
@@ -390,68 +428,90 @@ __global__ void __launch_bounds__(MODE ? FE_THREADS_COLOR : FE_THREADS_PLAIN, MO
             int code[3];
             pixelCodes<MODE>(c, rgb, code);
             const int cx = code[0], cy = code[1], cz = code[2];
-            if (c.xyz && lx >= HALO && lx < HALO + TS && ly >= HALO && ly < HALO + TS && x0 + lx < w && y0 + ly < h) {
+            if (c.xyz && lx >= HALO && lx < HALO + T::X && ly >= HALO && ly < HALO + T::Y && x0 + lx < w &&
+                y0 + ly < h) {
                 uint16_t* o = c.xyz + ((size_t)(y0 + ly) * w + (x0 + lx)) * 3;
                 o[0] = (uint16_t)cx;
                 o[1] = (uint16_t)cy;
                 o[2] = (uint16_t)cz;
             }
             const float fx = (float)(cx - 2048), fy = (float)(cy - 2048), fz = (float)(cz - 2048);
-            smem[0 * TW * TP + ly * TP + lx] = (float)0.299 * fx + (float)0.587 * fy + (float)0.114 * fz;
-            smem[1 * TW * TP + ly * TP + lx] = (float)(-0.16875) * fx + (float)(-0.33126) * fy + (float)0.5 * fz;
-            smem[2 * TW * TP + ly * TP + lx] = (float)0.5 * fx + (float)(-0.41869) * fy + (float)(-0.08131) * fz;
+            smem[0 * PLANE + ly * T::P + lx] = (float)0.299 * fx + (float)0.587 * fy + (float)0.114 * fz;
+            smem[1 * PLANE + ly * T::P + lx] = (float)(-0.16875) * fx + (float)(-0.33126) * fy + (float)0.5 * fz;
+            smem[2 * PLANE + ly * T::P + lx] = (float)0.5 * fx + (float)(-0.41869) * fy + (float)(-0.08131) * fz;
         }
     } else {
         const float* src = a.src + blockIdx.z * a.srcComp;
-        for (int idx = tid; idx < TW * TW; idx += THREADS) {
-            const int ly = idx / TW, lx = idx % TW;
-            smem[ly * TP + lx] = src[(size_t)mirror(y0 + ly, h) * a.srcStride + mirror(x0 + lx, w)];
+        for (int idx = tid; idx < T::WX * T::WY; idx += THREADS) {
+            const int ly = idx / T::WX, lx = idx % T::WX;
+            smem[ly * T::P + lx] = src[(size_t)mirror(y0 + ly, h) * a.srcStride + mirror(x0 + lx, w)];
         }
     }
     __syncthreads();
-    // columns: one thread per (component, column), all 72 columns
-    if (h >= 2 && tid < NC * TW) {
-        const int comp = tid / TW, col = tid - comp * TW;
-        liftLine(smem + comp * TW * TP + col, TP);
+    // columns: one thread per (component, column), every column of the tile and its halo
+    if (h >= 2 && tid < NC * T::WX) {
+        const int comp = tid / T::WX, col = tid - comp * T::WX;
+        liftLine<T::WY>(smem + comp * PLANE + col, T::P);
     }
     __syncthreads();
     // rows: one thread per (component, output row)
-    if (w >= 2 && tid < NC * TS) {
-        const int comp = tid / TS, r = HALO + (tid - comp * TS);
-        liftLine(smem + comp * TW * TP + r * TP, 1);
+    if (w >= 2 && tid < NC * T::Y) {
+        const int comp = tid / T::Y, r = HALO + (tid - comp * T::Y);
+        liftLine<T::WX>(smem + comp * PLANE + r * T::P, 1);
     }
     __syncthreads();
-    for (int k = 0; k < NC; ++k) writeOutputs<THREADS>(a, smem + k * TW * TP, COLOR ? k : (int)blockIdx.z, tx, ty, tid);
+    for (int k = 0; k < NC; ++k)
+        writeOutputs<THREADS, SHAPE>(a, smem + k * PLANE, COLOR ? k : (int)blockIdx.z, tx, ty, tid);
 }
 
-constexpr size_t kSmemColor = (size_t)3 * TW * TP * 4;
-constexpr size_t kSmemPlain = (size_t)TW * TP * 4;
+template <int MODE, int SHAPE>
+void optIn() {
+    GB_CHECK(cudaFuncSetAttribute(levelKernel<MODE, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)feSmem<MODE, SHAPE>()));
+}
+
+template <int MODE, int SHAPE>
+void launch(const ColorArgs& c, const LevelArgs& a, int comps, cudaStream_t st) {
+    using T = Tile<SHAPE>;
+    const dim3 grid(divUp(a.w, T::X), divUp(a.h, T::Y), comps);
+    levelKernel<MODE, SHAPE><<<grid, feThreads<MODE, SHAPE>(), feSmem<MODE, SHAPE>(), st>>>(c, a);
+}
 
 }  // namespace
 
 void frontendInit() {
-    GB_CHECK(cudaFuncSetAttribute(levelKernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemColor));
-    GB_CHECK(cudaFuncSetAttribute(levelKernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemColor));
-    GB_CHECK(cudaFuncSetAttribute(levelKernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemColor));
-    GB_CHECK(cudaFuncSetAttribute(levelKernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemPlain));
+    optIn<1, 0>();
+    optIn<1, 1>();
+    optIn<1, 2>();
+    optIn<2, 0>();
+    optIn<3, 0>();
+    optIn<0, 0>();
+    optIn<0, 1>();
+    optIn<0, 2>();
 }
 
-void launchLevel1(const ColorArgs& c, const LevelArgs& a, cudaStream_t st) {
-    const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 1);
+void launchLevel1(const ColorArgs& c, const LevelArgs& a, int shape, cudaStream_t st) {
+    if (shape < 0 || shape > 2) throw std::logic_error("tile shape must be 0, 1 or 2");
     if (c.route == kRouteLut) {
         if (!c.lut3 || c.lutN < 2) throw std::logic_error("LUT route without a LUT");
-        levelKernel<3><<<grid, FE_THREADS_COLOR, kSmemColor, st>>>(c, a);
+        launch<3, 0>(c, a, 1, st);  // the rarer routes keep the 64 x 64 tile
     } else if (c.route == kRouteManaged) {
-        levelKernel<2><<<grid, FE_THREADS_COLOR, kSmemColor, st>>>(c, a);
+        launch<2, 0>(c, a, 1, st);
+    } else if (shape == 1) {
+        launch<1, 1>(c, a, 1, st);
+    } else if (shape == 2) {
+        launch<1, 2>(c, a, 1, st);
     } else {
-        levelKernel<1><<<grid, FE_THREADS_COLOR, kSmemColor, st>>>(c, a);
+        launch<1, 0>(c, a, 1, st);
     }
     GB_CHECK(cudaGetLastError());
 }
 
-void launchLevel(const LevelArgs& a, cudaStream_t st) {
-    const dim3 grid(divUp(a.w, TS), divUp(a.h, TS), 3);
-    levelKernel<0><<<grid, FE_THREADS_PLAIN, kSmemPlain, st>>>(ColorArgs{}, a);
+void launchLevel(const LevelArgs& a, int shape, cudaStream_t st) {
+    if (shape < 0 || shape > 2) throw std::logic_error("tile shape must be 0, 1 or 2");
+    if (shape == 1) launch<0, 1>(ColorArgs{}, a, 3, st);
+    else if (shape == 2) launch<0, 2>(ColorArgs{}, a, 3, st);
+    else launch<0, 0>(ColorArgs{}, a, 3, st);
     GB_CHECK(cudaGetLastError());
 }
 

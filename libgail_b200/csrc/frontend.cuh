@@ -49,10 +49,11 @@ struct ColorArgs {
     int32_t lutN;
 };
 
-// Level 1 with the colour conversion folded into its tile loads.
-void launchLevel1(const ColorArgs& c, const LevelArgs& a, cudaStream_t st);
-// Levels 2.. from the previous level's LL planes.
-void launchLevel(const LevelArgs& a, cudaStream_t st);
+// Level 1 with the colour conversion folded into its tile loads; shape: the tile, 0 = 64 x
+// 64, 1 = 128 x 64, 2 = 64 x 128 (the tone-map and LUT routes always take 64 x 64).
+void launchLevel1(const ColorArgs& c, const LevelArgs& a, int shape, cudaStream_t st);
+// Levels 2.. from the previous level's LL planes, with tile shape `shape`.
+void launchLevel(const LevelArgs& a, int shape, cudaStream_t st);
 // Per-device set-up (shared-memory opt-in).
 void frontendInit();
 

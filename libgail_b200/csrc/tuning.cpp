@@ -26,6 +26,8 @@ void setTuning(int profile, const Tuning& t) {
         throw std::logic_error("grid caps must be 1..64 CTAs per SM");
     if (t.t1Persistent != 0 && t.t1Persistent != 1) throw std::logic_error("t1Persistent must be 0 or 1");
     if (t.decHeavyPct < 0 || t.decHeavyPct > 100000) throw std::logic_error("decHeavyPct must be 0..100000");
+    if (t.dwtTile1 < 0 || t.dwtTile1 > 2 || t.dwtTileN < 0 || t.dwtTileN > 2)
+        throw std::logic_error("tile shapes must be 0 (64 x 64), 1 (128 x 64) or 2 (64 x 128)");
     Tuning v = t;
     uint32_t p = 1;
     while (p * 2 <= v.soloDecisions && p < (1u << 30)) p *= 2;

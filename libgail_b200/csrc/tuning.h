@@ -14,6 +14,8 @@ struct Tuning {
     int t1Persistent = 0;            // Tier-1 encode as one persistent launch (1) or four (0)
     int decHeavyPct = 150;           // Tier-1 decode: blocks above this % of the mean codeword bytes per
                                      // warp run on SMs of their own (0: none)
+    int dwtTile1 = 0;                // front-end tile at level 1: 0 = 64 x 64, 1 = 128 x 64, 2 = 64 x 128
+    int dwtTileN = 0;                // the same for levels 2..
 };
 
 Tuning defaultTuning();

@@ -11,10 +11,10 @@ from libgail_b200 import autotune as AT
 def test_round_trip_and_rounding():
     try:
         AT.set_tuning(1, {"soloDecisions": 12000, "cmCtasPerSm": 8, "mqCtasPerSm": 24, "decCtasPerSm": 40,
-                          "t1Persistent": 1, "decHeavyPct": 250})
+                          "t1Persistent": 1, "decHeavyPct": 250, "dwtTile1": 1, "dwtTileN": 2})
         t = AT.get_tuning(1)
         assert t == {"soloDecisions": 8192, "cmCtasPerSm": 8, "mqCtasPerSm": 24, "decCtasPerSm": 40,
-                     "t1Persistent": 1, "decHeavyPct": 250}
+                     "t1Persistent": 1, "decHeavyPct": 250, "dwtTile1": 1, "dwtTileN": 2}
         assert AT.get_tuning(0) == AT.DEFAULTS  # profiles are independent
     finally:
         AT.set_tuning(1, None)
@@ -22,7 +22,7 @@ def test_round_trip_and_rounding():
 
 
 @pytest.mark.parametrize("bad", [{"soloDecisions": 100}, {"cmCtasPerSm": 0}, {"mqCtasPerSm": 65}, {"decCtasPerSm": -1},
-                                 {"t1Persistent": 2}, {"decHeavyPct": -1}])
+                                 {"t1Persistent": 2}, {"decHeavyPct": -1}, {"dwtTile1": 3}, {"dwtTileN": -1}])
 def test_invalid_values_refused(bad):
     with pytest.raises(GailError):
         AT.set_tuning(0, dict(AT.DEFAULTS, **bad))

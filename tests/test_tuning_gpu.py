@@ -34,3 +34,35 @@ def test_tuning_does_not_change_results():
     finally:
         AT.set_tuning(0, None)
         dev.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("W,H,fk,planar", [(1998, 1080, 0, False), (3996, 2160, 1, True), (2001, 1077, 0, False)])
+def test_tile_shapes_give_the_same_coefficients(W, H, fk, planar):
+    """Every front-end tile shape (64 x 64, 128 x 64, 64 x 128 at level 1 and at the later
+    levels) gives the same X'Y'Z' codes, wavelet planes, quantised words and Tier-1 frame."""
+    prof = 1 if fk else 0
+    dev = P.Plugin().device(0)
+    lay = P.LayoutHolder(W, H, fk)
+    if planar:
+        fmt, col = P.planar_format(W, H, bits=10, sx=1, sy=0), P.color("pq", "bt2020")
+        frame = synth.yuv422p10(W, H, seed=91)
+    else:
+        fmt, col = P.rgb48_format(W, H), P.color_passthrough()
+        frame = synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=91))
+    try:
+        enc = dev.encoder(lay, fmt, col)
+        ref, _, rtaps = enc.encode(frame, debug=True)
+        for t1, tn in ((1, 0), (2, 0), (0, 1), (0, 2), (1, 2), (2, 1)):
+            AT.set_tuning(prof, {"dwtTile1": t1, "dwtTileN": tn})
+            got, _, taps = enc.encode(frame, debug=True)
+            for k in ("xyz12", "coeffs"):
+                assert np.array_equal(taps[k], rtaps[k]), f"tiles {t1}/{tn}: {k} differ"
+            assert np.array_equal(taps["wavelet"].view(np.uint32), rtaps["wavelet"].view(np.uint32)), \
+                f"tiles {t1}/{tn}: wavelet planes differ"
+            assert np.array_equal(got.info, ref.info) and np.array_equal(got.data, ref.data)
+            assert np.array_equal(got.pass_len, ref.pass_len) and np.array_equal(got.pass_dist, ref.pass_dist)
+        enc.close()
+    finally:
+        AT.set_tuning(prof, None)
+        dev.close()
