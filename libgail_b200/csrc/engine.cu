@@ -52,7 +52,7 @@ struct EncodeEngine::Class {
     float* dEotf = nullptr;
     float* dThr = nullptr;
     float* dLut = nullptr;  // the application 3D LUT, if the colour route takes one
-    float* dLL[2] = {nullptr, nullptr};
+    float* dLL[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // per front stream
     double* dScale = nullptr;  // per block: the hull's distortion weight
     uint64_t slotBytes = 0, dataCap = 0;
     std::vector<Slot*> free;
@@ -165,7 +165,7 @@ EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(
     // the classes size)
     budgetAuto_ = hbmBudget == 0;
     budget_ = hbmBudget;
-    GB_CHECK(cudaStreamCreateWithFlags(&front_, cudaStreamNonBlocking));
+    for (auto& f : front_) GB_CHECK(cudaStreamCreateWithFlags(&f, cudaStreamNonBlocking));
     GB_CHECK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
     constexpr int kMaxSlots = 1024;
     check(cudaMalloc(&dSlope_, kMaxSlots * 4), "device memory for the engine");
@@ -222,7 +222,8 @@ EncodeEngine::~EncodeEngine() {
     if (dSlope_) cudaFree(dSlope_);
     if (hSlope_) cudaFreeHost(hSlope_);
     if (hZero_) cudaFreeHost(hZero_);
-    if (front_) cudaStreamDestroy(front_);
+    for (auto f : front_)
+        if (f) cudaStreamDestroy(f);
     if (copy_) cudaStreamDestroy(copy_);
     cudaGetLastError();
 }
@@ -246,8 +247,10 @@ int EncodeEngine::addClass(const GailCudaLayout& layout, const GailCudaEncodeSet
     alloc(c->dEotf, 65536 * 4);
     alloc(c->dThr, 4096 * 4);
     alloc(c->dLut, c->color.lut3.size() * 4);
-    alloc(c->dLL[0], c->z.llFloats * 12);
-    alloc(c->dLL[1], c->z.llFloats * 12);
+    for (auto& ll : c->dLL) {
+        alloc(ll[0], c->z.llFloats * 12);
+        alloc(ll[1], c->z.llFloats * 12);
+    }
     alloc(c->dScale, c->z.n * 8);
     const std::vector<double> scales = blockScales(c->L);
     GB_CHECK(cudaMemcpy(c->dScale, scales.data(), scales.size() * 8, cudaMemcpyHostToDevice));
@@ -471,7 +474,8 @@ EncodeEngine::Slot* EncodeEngine::newSlot(int cls) {
         ColorArgs a = c.colorArgs;
         a.src = s->dIn;
         GB_CHECK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-        launchFrontEnd(c.L, a, c.dLL[0], c.dLL[1], c.z.llFloats, s->dCoeffs, nullptr, cap);
+        const int fs = s->index % kFronts;  // the front stream this slot's frames take
+        launchFrontEnd(c.L, a, c.dLL[fs][0], c.dLL[fs][1], c.z.llFloats, s->dCoeffs, nullptr, cap);
         GB_CHECK(cudaStreamEndCapture(cap, &s->graph));
         GB_CHECK(cudaStreamDestroy(cap));
         size_t nodes = 0;
@@ -983,12 +987,13 @@ bool EncodeEngine::admit() {
         GB_CHECK(cudaMemcpyAsync(s->dIn, r->frame, c.z.inBytes, r->onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                  copy_));
         GB_CHECK(cudaEventRecord(s->upDone, copy_));
-        GB_CHECK(cudaStreamWaitEvent(front_, s->upDone, 0));
+        const cudaStream_t fst = front_[s->index % kFronts];
+        GB_CHECK(cudaStreamWaitEvent(fst, s->upDone, 0));
         r->frontTimed = timing_.load() && s->frontT[0];
-        if (r->frontTimed) GB_CHECK(cudaEventRecord(s->frontT[0], front_));
-        GB_CHECK(cudaGraphLaunch(s->exec, front_));
-        if (r->frontTimed) GB_CHECK(cudaEventRecord(s->frontT[1], front_));
-        GB_CHECK(cudaEventRecord(s->frontDone, front_));
+        if (r->frontTimed) GB_CHECK(cudaEventRecord(s->frontT[0], fst));
+        GB_CHECK(cudaGraphLaunch(s->exec, fst));
+        if (r->frontTimed) GB_CHECK(cudaEventRecord(s->frontT[1], fst));
+        GB_CHECK(cudaEventRecord(s->frontDone, fst));
         std::lock_guard<std::mutex> lock(m_);
         if (!r->onDevice) stats_.h2dBytes += c.z.inBytes;
         stats_.launches += (uint64_t)s->graphKernels;

@@ -171,7 +171,10 @@ private:
     int maxBatch_;
     int minBatchPct_ = 25;
     double maxWaitMs_ = 2.0;
-    cudaStream_t front_ = nullptr;
+    // front ends on two streams, a slot on the one its index picks, so that two frames'
+    // front ends can run at once (each stream has its own LL scratch planes per class)
+    static constexpr int kFronts = 2;
+    cudaStream_t front_[kFronts] = {};
     cudaStream_t copy_ = nullptr;  // frame uploads
     std::vector<std::unique_ptr<Class>> classes_;
     std::vector<std::unique_ptr<Slot>> slots_;
