@@ -95,6 +95,7 @@ def main():
             import time
             eng = Engine(0, 0, max_batch=args.batch)
             cid, _ = eng.add_encoder(lay, fmt, col)
+            eng.reserve(cid, len(dframes))  # a slot for every frame of the burst, made before it
             if args.codestreams:
                 from libgail_b200 import codestream as CS
                 eng.set_codestream(label=CS.DEFAULT_LABEL, tag="b200", threads=8)
