@@ -793,60 +793,32 @@ __device__ __forceinline__ void mqRun(const T1Launch& P, uint32_t* ctx, const ui
     };
 
     // A solo warp first codes its solo block (perm[0 .. solo)) on its lane 0 while the other
-    // lanes wait; then all its lanes take blocks from the shared queue, one at a time.
+    // lanes wait. Then the warp takes the next 32 blocks of the order at once, a lane each,
+    // and codes them until the last of them is done: the order is largest first in narrow
+    // size classes, so the 32 are about the same length, and the lanes start, run and end
+    // their blocks together instead of each claiming its next block at its own time (which
+    // left a third of the lanes of a warp idle at any moment).
     const uint32_t solo = ldx<false>(P.ctl + 3);
     uint32_t mine = warpId;
     if constexpr (PERS) {
         if (lane == 0) mine = atomicAdd(P.work + kWSoloHead, 1u);
         mine = __shfl_sync(kFull, mine, 0);
     }
-    bool soloPhase = mine < solo;
-    bool soloJob = false;
-    if (soloPhase && lane == 0) soloJob = begin(ldx<false>(P.perm + mine));
-
-    // A lane leaves only at the loop's top, after the solo phase's shuffle: a solo warp's
-    // lane 0 whose queue is empty when its solo block ends still tells the other lanes,
-    // which wait in that shuffle (otherwise they would pair it with the next shuffle lane 0
-    // makes, wherever that is).
-    bool finished = false;
-    for (;;) {
-        if (soloPhase) {  // warp-uniform; every lane of the warp is still in the loop
-            if (__shfl_sync(kFull, (int)soloJob, 0)) {
-                if (lane != 0) continue;
-            } else {
-                soloPhase = false;
-            }
+    // end of the block in hand: remaining pass ends, flush, the codeword's length (the
+    // truncation lengths are found afterwards, a warp per block)
+    auto endBlock = [&] {
+        while (k < np) {
+            P.snaps[(size_t)job * kMaxPasses + k] = make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
+            ++k;
         }
-        if (finished) break;
-        if (!have || pos >= nsym) {
-            if (have) {
-                // end of block: remaining pass ends, flush, truncation points
-                while (k < np) {
-                    P.snaps[(size_t)job * kMaxPasses + k] =
-                        make_uint4((uint32_t)e.bp, e.C, e.A | ((uint32_t)e.CT << 16), e.B);
-                    ++k;
-                }
-                const uint32_t len = e.flush();
-                if (e.overflow) atomicOr(status, kErrCodewordSpace);
-                // the truncation lengths are found afterwards, a warp per block
-                P.info[4 * (size_t)job + 3] = e.overflow ? 0u : len;
-                listed(job);
-                have = false;
-                soloJob = false;
-            }
-            // next block from the shared queue (after the solo blocks)
-            bool got = false;
-            for (;;) {
-                const uint32_t qi = solo + atomicAdd(P.ctl, 1u);
-                if (qi >= P.n) break;
-                if (begin(ldx<false>(P.perm + qi))) {
-                    got = true;
-                    break;
-                }
-            }
-            finished = !got;
-            continue;  // a block without decisions finishes at once
-        }
+        const uint32_t len = e.flush();
+        if (e.overflow) atomicOr(status, kErrCodewordSpace);
+        P.info[4 * (size_t)job + 3] = e.overflow ? 0u : len;
+        listed(job);
+        have = false;
+    };
+    // one aligned chunk of 16 decisions of the block in hand (fewer at its end)
+    auto chunk = [&] {
         // one aligned chunk of 16 decisions (fewer at the block's end): a word of four
         // decisions unrolled at a time, the next decision's context state read ahead, off
         // the serial chain of the coder
@@ -892,6 +864,29 @@ __device__ __forceinline__ void mqRun(const T1Launch& P, uint32_t* ctx, const ui
             w1 = w2;
             w2 = w3;
             w3 = w4;
+        }
+    };
+    if (mine < solo) {  // warp-uniform
+        if (lane == 0) have = begin(ldx<false>(P.perm + mine));
+        while (__shfl_sync(kFull, (int)have, 0)) {
+            if (lane == 0) {
+                if (pos >= nsym) endBlock();
+                else chunk();
+            }
+        }
+    }
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(P.ctl, 32u);
+        base = __shfl_sync(kFull, base, 0);
+        if (solo + base >= P.n) break;  // warp-uniform
+        const uint32_t qi = solo + base + lane;
+        have = qi < P.n && begin(ldx<false>(P.perm + qi));
+        while (__any_sync(kFull, have)) {
+            if (have) {
+                if (pos >= nsym) endBlock();
+                else chunk();
+            }
         }
     }
 }
