@@ -82,7 +82,8 @@ def parse():
                     help="most frames per Tier-1 launch (served path; default: the tuning file's, else 16)")
     ap.add_argument("--tuning", default=os.path.join(ROOT, "libgail_b200", "tuning_b200.json"),
                     help="autotuner file applied when it was made on this GPU ('' for the defaults)")
-    ap.add_argument("--slots", type=int, default=3, help="slot threads of the plain path")
+    ap.add_argument("--slots", type=int, default=4,
+                    help="slot threads (frames in flight) of the plain path, as libgail's gail-bench runs it (--slots 4)")
     return ap.parse_args()
 
 
