@@ -418,7 +418,7 @@ EncodeEngine::Slot* EncodeEngine::newSlot(int cls) {
     {
         std::lock_guard<std::mutex> lock(m_);
         cp = classes_[cls].get();
-        index = (int)slots_.size();
+        index = nextSlotIndex_++;  // the slot thread and reserve() may make slots at once
     }
     Class& c = *cp;
     if (index >= 1024) return nullptr;

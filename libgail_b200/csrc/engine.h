@@ -195,6 +195,7 @@ private:
     std::deque<int> makeQ_;           // classes a slot is wanted for
     std::vector<int> making_;         // per class: slots asked for, not yet made
     bool slotsFull_ = false;          // a slot could not be made (budget or memory): ask no more
+    int nextSlotIndex_ = 0;           // a slot's index into the per-slot arrays (under m_)
     std::vector<Request*> front_q_;   // front end enqueued, not yet in a batch
     std::deque<Request*> done_;       // finished, not yet handed out
     std::atomic<bool> stop_{false};
