@@ -159,6 +159,7 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
 
             eng = Engine(0, 0, max_batch=POLICY_DEFAULT["maxBatch"])
             cid, _ = eng.add_encoder(lay, fmt, col)
+            eng.reserve(cid, len(dframes))  # a slot per frame of a burst before the first one
 
             def served_ms(cfg):  # wall time per frame of a burst through the engine, Tier-1 only
                 set_tuning(prof, cfg)

@@ -43,6 +43,8 @@ double msBetween(Clock::time_point a, Clock::time_point b) {
 
 }  // namespace
 
+constexpr uint32_t kBatchSoloFloor = 16384;  // MQ solo threshold of batched launches, at least
+
 struct EncodeEngine::Class {
     Layout L;
     GailCudaEncodeSettings s;
@@ -1052,7 +1054,11 @@ bool EncodeEngine::launchBatch(Batch& b) {
     bool any4k = false;  // a batch with a 4K frame is launched with the 4K tuning
     for (Request* r : sel) any4k = any4k || classes_[r->cls]->L.profile == 1;
     const Tuning tu = tuningFor(any4k ? 1 : 0);
-    L.soloDecisions = tu.soloDecisions;
+    // the solo threshold is tuned on one-frame launches, where the longest blocks' chains set
+    // the time; a batch of frames has enough other blocks to hide them behind, and taking
+    // warps for solo blocks below 16,384 decisions cost it throughput (4K served codestreams:
+    // 560 per second at 16,384, 530 at 8,192, on B200)
+    L.soloDecisions = std::max<uint32_t>(tu.soloDecisions, kBatchSoloFloor);
     L.cmCtasPerSm = (uint16_t)tu.cmCtasPerSm;
     L.mqCtasPerSm = (uint16_t)tu.mqCtasPerSm;
     L.persistent = (uint16_t)tu.t1Persistent;
