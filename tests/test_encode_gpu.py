@@ -9,7 +9,7 @@ CPU encoder itself (oracle/_ref: the CpuSlot built from the reference sources):
   * Tier-1 of every code-block against the CpuSlot's Tier1Frame: nbps, pass count, every
     truncation length and distortion, the codeword bytes.
 
-All bit-identical (the north star allows 1 in 10^5 quantised words off by one; the count
+All bit-identical (the specification allows 1 in 10^5 quantised words off by one; the count
 found is 0 and the tests require 0)."""
 import numpy as np
 import pytest
