@@ -16,9 +16,9 @@ pass (bit-exact with the CPU reference). One step = encoding all 48 frames; the 
   e2e     the same with the frames in pinned host memory: uploads and codestreams inside.
   served_* / plain_*  codestreams/s and p50 / p99 latency of both paths at one Poisson load
           (80 % of the plain rate), and the served p99 at 90 % of its own end-to-end rate.
-          plain: the drop-in per-frame path as libgail drives the plugin (slot threads, each
-          encoder_encode from host memory, then the host codec's rate control, Tier-2 and
-          the DCI check).
+          plain: the drop-in per-frame path as libgail drives the plugin (four slot threads,
+          the frames in flight of the reference's own benchmark, each encoder_encode from
+          host memory, then the host codec's rate control, Tier-2 and the DCI check).
   stages  the served path's stage split, live (the same job once more with the engine's
           CUDA-event stage timing on): ms per frame, algorithmic bytes and HBM fraction.
   roofline  the dominant kernel of the served run, t1CmKernel: integer-issue bound, so its
@@ -28,7 +28,7 @@ pass (bit-exact with the CPU reference). One step = encoding all 48 frames; the 
   encode_decode_2k  the 2K configuration one frame at a time, encode and decode.
   six_profiles  16 frames over the six DCI profiles: Tier-1 as one persistent launch in
           the served engine against the plain per-frame path.
-  mixed   Poisson encode and decode requests of 4K and 2K at three loads.
+  mixed   Poisson encode and decode requests of 4K and 2K at four loads.
 
 --impl reference times the reference's own CPU path (the CpuSlot encoder, then its rate
 control, codestream writer and DCI checker, built from the reference sources into
