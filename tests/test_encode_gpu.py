@@ -111,11 +111,15 @@ def test_4k_yuv422_pq_frame_bit_exact(dev, ref):
 
 @pytest.mark.gpu
 def test_planar_variants_bit_exact(dev, ref):
-    """Letterboxed 4:2:0 8-bit BT.709 with centred chroma, full-range 4:4:4 12-bit, and
-    planar G'B'R' 10-bit."""
+    """Letterboxed 4:2:0 8-bit BT.709 with centred chroma, full-range 4:4:4 12-bit, planar
+    G'B'R' 10-bit and 16-bit, letterboxed 4:2:2 8-bit, and 4:2:0 12-bit with an odd active
+    picture and left-sited chroma (the reference's GAIL_PIX_* planar formats, gail.h:125-141)."""
     for (aw, ah, bits, sx, sy, chroma, full, rgbf, kr, kb) in [(180, 101, 8, 1, 1, 1, 0, 0, 0.2126, 0.0722),
                                                                (200, 120, 12, 0, 0, 2, 1, 0, 0.299, 0.114),
-                                                               (200, 120, 10, 0, 0, 0, 0, 1, 0.2627, 0.0593)]:
+                                                               (200, 120, 10, 0, 0, 0, 0, 1, 0.2627, 0.0593),
+                                                               (200, 120, 16, 0, 0, 0, 1, 1, 0.2627, 0.0593),
+                                                               (198, 108, 8, 1, 0, 0, 0, 0, 0.2126, 0.0722),
+                                                               (199, 119, 12, 1, 1, 0, 0, 0, 0.2627, 0.0593)]:
         W, H = 200, 120
         rng = np.random.default_rng(bits + rgbf)
         cw, ch = (aw + sx) >> sx, (ah + sy) >> sy
