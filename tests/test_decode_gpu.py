@@ -34,18 +34,25 @@ def _codestream(W, H, fourk, seed):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("W,H,fourk,reduce", [(1998, 1080, 0, 0), (1998, 1080, 0, 1), (3996, 2160, 1, 0),
-                                              (3996, 2160, 1, 1), (333, 200, 1, 0)])
-def test_decode_matches_cpu(dev, W, H, fourk, reduce):
+@pytest.mark.parametrize("W,H,fourk,reduce,high", [(1998, 1080, 0, 0, False), (1998, 1080, 0, 1, False),
+                                                   (1998, 1080, 0, 2, True), (3996, 2160, 1, 0, False),
+                                                   (3996, 2160, 1, 1, False), (3996, 2160, 1, 2, False),
+                                                   (333, 200, 1, 0, True)])
+def test_decode_matches_cpu(dev, W, H, fourk, reduce, high):
+    """Full, half and quarter size; `high`: the codes in the high 12 bits of each word (the
+    reference decoder's xyz12le output)."""
     ref, cs = _codestream(W, H, fourk, seed=7 + W)
     blocks, w, h, lv = ref_parse(ref, cs, reduce)
     lay = P.LayoutHolder(W, H, fourk)
-    dec = dev.decoder(lay, reduce=reduce, high_bits=False)
+    dec = dev.decoder(lay, reduce=reduce, high_bits=high)
     try:
         pic, tm, wl = dec.decode(cs, blocks.view(P.CBLK_CODE_DTYPE), wavelet=True)
     finally:
         dec.close()
-    want, wref, _ = ref_decode(ref, cs, W, H, reduce, wavelet=True)
+    want, wref, _ = ref_decode(ref, cs, W, H, reduce, high_bits=high, wavelet=True)
+    if high:  # the low four bits are zero on both sides; compare the codes
+        assert not np.any(pic & 15) and not np.any(want & 15)
+        pic, want = pic >> 4, want >> 4
     # coefficients of the decoded resolutions: bit-identical
     wl = wl.reshape(3, H, W)
     mask = np.zeros((H, W), bool)
