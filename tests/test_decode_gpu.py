@@ -37,7 +37,8 @@ def _codestream(W, H, fourk, seed):
 @pytest.mark.parametrize("W,H,fourk,reduce,high", [(1998, 1080, 0, 0, False), (1998, 1080, 0, 1, False),
                                                    (1998, 1080, 0, 2, True), (3996, 2160, 1, 0, False),
                                                    (3996, 2160, 1, 1, False), (3996, 2160, 1, 2, False),
-                                                   (333, 200, 1, 0, True)])
+                                                   (333, 200, 1, 0, True), (64, 64, 0, 0, False),
+                                                   (65, 67, 1, 1, False)])
 def test_decode_matches_cpu(dev, W, H, fourk, reduce, high):
     """Full, half and quarter size; `high`: the codes in the high 12 bits of each word (the
     reference decoder's xyz12le output)."""

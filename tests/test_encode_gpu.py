@@ -93,7 +93,8 @@ def test_2k_xyz_frame_bit_exact(dev, ref):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("w,h,fourk", [(333, 200, 1), (100, 77, 0), (2048, 858, 0), (4096, 1716, 1)])
+@pytest.mark.parametrize("w,h,fourk", [(333, 200, 1), (100, 77, 0), (2048, 858, 0), (4096, 1716, 1), (64, 64, 0),
+                                        (65, 67, 1)])
 def test_ragged_sizes_bit_exact(dev, ref, w, h, fourk):
     rgb = synth.xyz12_to_rgb48(synth.xyz12_planes(w, h, seed=5))
     _frame_parity(dev, ref, w, h, fourk, P.rgb48_format(w, h), P.color_passthrough(), rgb, 5, 4)
