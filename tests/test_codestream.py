@@ -51,17 +51,20 @@ def _ref_build(ref, W, H, fk, t1, passes, tag=b""):
 
 
 @pytest.mark.parametrize("prof", PROFILES)
-@pytest.mark.parametrize("mbps", [230.0, 90.0])
-def test_rate_and_build_matches_reference(ref, frames, prof, mbps):
+@pytest.mark.parametrize("mbps,fps", [(230.0, 24.0), (90.0, 24.0), (230.0, 48.0), (230.0, 25.0)])
+def test_rate_and_build_matches_reference(ref, frames, prof, mbps, fps):
+    """Rate control and codestream against the reference's allocateRate + buildCodestream, at
+    the DCI rate and a low one, and at 48 and 25 frames/s (the per-frame budget follows the
+    frame rate, dciLimits, rate_control.cpp:11-26)."""
     W, H, fk = prof
     t1 = frames[prof]
     lay = P.LayoutHolder(W, H, fk)
-    want, wpasses, wlam, _ = ref_codestream(ref, W, H, fk, t1, fps=24.0, mbps=mbps, tag=b"cuda13.0")
-    got, passes, lam = CS.rate_and_build(lay, t1, fps=24.0, max_mbps=mbps, label=LABEL, tag="cuda13.0")
+    want, wpasses, wlam, _ = ref_codestream(ref, W, H, fk, t1, fps=fps, mbps=mbps, tag=b"cuda13.0")
+    got, passes, lam = CS.rate_and_build(lay, t1, fps=fps, max_mbps=mbps, label=LABEL, tag="cuda13.0")
     assert np.array_equal(passes, wpasses)
     assert lam == wlam
     assert got == want
-    ok, msg = CS.check_dci(got)
+    ok, msg = CS.check_dci(got, fps)
     assert ok, msg
     assert msg == LABEL + " cuda13.0"
 

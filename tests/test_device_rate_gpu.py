@@ -48,6 +48,25 @@ def test_device_rate_and_build_equals_host(frames, prof, mbps, comp):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("prof", [(1998, 1080, 0), (3996, 2160, 1)])
+@pytest.mark.parametrize("fps", [48.0, 25.0])
+def test_device_rate_other_frame_rates(frames, prof, fps):
+    """At 48 and 25 frames/s (a smaller per-frame budget): the device path's codestream,
+    passes and lambda equal the host codec's and the reference's."""
+    ref, fr = frames
+    W, H, fk = prof
+    t1 = fr[prof]
+    lay = P.LayoutHolder(W, H, fk)
+    want = CS.rate_and_build(lay, t1, fps=fps, tag="cuda13.0")
+    got = CS.device_rate_and_build(lay, t1, fps=fps, tag="cuda13.0")
+    assert got[0] == want[0] and np.array_equal(got[1], want[1]) and got[2] == want[2]
+    rcs, _, rlam, _ = ref_codestream(ref, W, H, fk, t1, fps=fps, tag=b"cuda13.0")
+    assert got[0] == rcs and got[2] == rlam
+    ok, msg = CS.check_dci(got[0], fps)
+    assert ok, msg
+
+
+@pytest.mark.gpu
 def test_device_rate_control_flat_and_repeated(frames):
     """A nearly empty frame (flat picture: few passes) and the same frame twice in a row
     through the cached device rate control."""
