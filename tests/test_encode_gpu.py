@@ -101,6 +101,23 @@ def test_ragged_sizes_bit_exact(dev, ref, w, h, fourk):
 
 
 @pytest.mark.gpu
+def test_largest_container_and_extreme_pictures(dev, ref):
+    """The largest DCI container (4096 x 2160) with seeded content; then pictures at the
+    ends of the code range: black (every X'Y'Z' code 0: after the DC shift only the lowest
+    band codes anything), white (every code 4095) and a one-pixel checkerboard of both
+    (every high band at its largest magnitudes)."""
+    W, H = 4096, 2160
+    rgb = synth.xyz12_to_rgb48(synth.xyz12_planes(W, H, seed=17))
+    _frame_parity(dev, ref, W, H, 1, P.rgb48_format(W, H), P.color_passthrough(), rgb, 5, 4)
+    W, H = 1998, 1080
+    yy, xx = np.mgrid[0:H, 0:W]
+    for planes in (np.zeros((3, H, W), np.uint16), np.full((3, H, W), 4095, np.uint16),
+                   np.broadcast_to((((yy + xx) & 1) * 4095).astype(np.uint16), (3, H, W)).copy()):
+        _frame_parity(dev, ref, W, H, 0, P.rgb48_format(W, H), P.color_passthrough(), synth.xyz12_to_rgb48(planes),
+                      5, 4)
+
+
+@pytest.mark.gpu
 def test_4k_yuv422_pq_frame_bit_exact(dev, ref):
     W, H = 3996, 2160
     frame = synth.yuv422p10(W, H, seed=21)
