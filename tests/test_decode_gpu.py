@@ -88,3 +88,29 @@ def test_decode_damaged_input_stays_in_bounds(dev):
         dec.close()
     want, _, _ = ref_decode(ref, cs, W, H, 0)
     assert np.abs(pic2.astype(np.int32) - want.astype(np.int32)).max() <= 1
+
+
+@pytest.mark.gpu
+def test_decode_extreme_pictures(dev):
+    """Codestreams of black, white and one-pixel checkerboard pictures (the checkerboard
+    fills every high band at its largest magnitudes, truncated hard by the rate control):
+    coefficients bit-identical to the reference CPU decoder's, picture within one code."""
+    W, H, fk = 1998, 1080, 0
+    ref = Reference()
+    yy, xx = np.mgrid[0:H, 0:W]
+    lay = P.LayoutHolder(W, H, fk)
+    dec = dev.decoder(lay)
+    try:
+        for planes in (np.zeros((3, H, W), np.uint16), np.full((3, H, W), 4095, np.uint16),
+                       np.broadcast_to((((yy + xx) & 1) * 4095).astype(np.uint16), (3, H, W)).copy()):
+            enc = RefEncoder(ref, W, H, fk)
+            t1 = enc.encode(synth.xyz12_to_rgb48(planes))
+            enc.close()
+            cs, _, _, _ = ref_codestream(ref, W, H, fk, t1, mbps=250.0)
+            blocks, _, _, _ = ref_parse(ref, cs, 0)
+            pic, _, wl = dec.decode(cs, blocks.view(P.CBLK_CODE_DTYPE), wavelet=True)
+            want, wref, _ = ref_decode(ref, cs, W, H, 0, wavelet=True)
+            assert np.array_equal(wl.reshape(3, H, W).view(np.uint32), wref.view(np.uint32))
+            assert np.abs(pic.astype(np.int32) - want.astype(np.int32)).max() <= 1
+    finally:
+        dec.close()
