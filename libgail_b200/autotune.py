@@ -9,6 +9,7 @@ compared. The result is a JSON file keyed by the GPU's name; apply() loads it in
 library (gb_set_tuning) and returns the engine policy for Engine.set_policy().
 
   python -m libgail_b200.autotune --out libgail_b200/tuning_b200.json [--quick]
+  python -m libgail_b200.autotune --tiles     # the front-end tile-shape grid alone
 """
 from __future__ import annotations
 
@@ -106,6 +107,33 @@ def _workload(name: str, nframes: int):
     return P.LayoutHolder(W, H, 0), P.rgb48_format(W, H), P.color_passthrough(), frames
 
 
+def _stage_timer(L, enc, dframes, prof: int, n: int):
+    """stage_ms(cfg, stages): the plain encoder's device time per frame of the given stages
+    (0 front end, 1 context modelling, 2 ordering, 3 MQ, 4 packing; CUDA events) over n
+    device-resident frames, with the profile's knobs set to cfg first."""
+    def stage_ms(cfg, stages):
+        set_tuning(prof, cfg)
+        for f in dframes[:2]:
+            check(L.gb_encoder_enqueue_device(enc.h, C.c_void_p(f.data_ptr())))
+        check(L.gb_encoder_finish(enc.h))
+        ms5, cnt = np.zeros(5), C.c_int()
+        check(L.gb_encoder_stage_timing(enc.h, 1))
+        check(L.gb_encoder_stage_times(enc.h, ms5.ctypes.data, C.byref(cnt)))
+        for f in dframes[:n]:
+            check(L.gb_encoder_enqueue_device(enc.h, C.c_void_p(f.data_ptr())))
+        check(L.gb_encoder_stage_times(enc.h, ms5.ctypes.data, C.byref(cnt)))
+        check(L.gb_encoder_stage_timing(enc.h, 0))
+        return float(sum(ms5[k] for k in stages)) / max(cnt.value, 1)
+    return stage_ms
+
+
+def _bind_encoder_timing(L):
+    L.gb_encoder_enqueue_device.argtypes = [C.c_void_p, C.c_void_p]
+    L.gb_encoder_finish.argtypes = [C.c_void_p]
+    L.gb_encoder_stage_timing.argtypes = [C.c_void_p, C.c_int]
+    L.gb_encoder_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+
+
 def _best_of(measure, runs: int):
     """The fastest of `runs` measurements (noise on a shared host only ever adds time)."""
     return lambda cfg: min(measure(cfg) for _ in range(runs))
@@ -120,10 +148,7 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
     from .engine import Engine
 
     L = gb.lib()
-    L.gb_encoder_enqueue_device.argtypes = [C.c_void_p, C.c_void_p]
-    L.gb_encoder_finish.argtypes = [C.c_void_p]
-    L.gb_encoder_stage_timing.argtypes = [C.c_void_p, C.c_int]
-    L.gb_encoder_stage_times.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    _bind_encoder_timing(L)
     dev = P.Plugin().device(0)
     out = {"device": torch.cuda.get_device_name(0), "sms": torch.cuda.get_device_properties(0).multi_processor_count,
            "profiles": {}, "policy": {}, "measured": {}}
@@ -136,20 +161,7 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
             dframes = [torch.from_numpy(f.view(np.int16)).to("cuda:0") for f in frames]
             torch.cuda.synchronize()
             enc = dev.encoder(lay, fmt, col)
-
-            def stage_ms(cfg, stages):  # the stages' device time per frame, plain one-frame launches
-                set_tuning(prof, cfg)
-                for f in dframes[:2]:
-                    check(L.gb_encoder_enqueue_device(enc.h, C.c_void_p(f.data_ptr())))
-                check(L.gb_encoder_finish(enc.h))
-                ms5, cnt = np.zeros(5), C.c_int()
-                check(L.gb_encoder_stage_timing(enc.h, 1))
-                check(L.gb_encoder_stage_times(enc.h, ms5.ctypes.data, C.byref(cnt)))
-                for f in dframes[:n]:
-                    check(L.gb_encoder_enqueue_device(enc.h, C.c_void_p(f.data_ptr())))
-                check(L.gb_encoder_stage_times(enc.h, ms5.ctypes.data, C.byref(cnt)))
-                check(L.gb_encoder_stage_timing(enc.h, 0))
-                return float(sum(ms5[k] for k in stages)) / max(cnt.value, 1)
+            stage_ms = _stage_timer(L, enc, dframes, prof, n)  # plain one-frame launches
 
             def tier1_ms(cfg):  # context modelling + MQ
                 return stage_ms(cfg, (1, 3))
@@ -243,11 +255,54 @@ def tune(quick: bool = False, log=print, runs: int = 2) -> dict:
     return out
 
 
+def tile_sweep(runs: int = 3, nframes: int = 8, log=print) -> dict:
+    """The front end's device time per frame (colour, every 9/7 level and quantisation; ms,
+    best of `runs`) for every pair of tile shapes, level 1 x the later levels (0 = 64 x 64,
+    1 = 128 x 64, 2 = 64 x 128), on the 4K and 2K workloads: the whole grid the autotuner's
+    coordinate search walks part of."""
+    import torch
+
+    import libgail_b200 as gb
+    from . import plugin as P
+
+    L = gb.lib()
+    _bind_encoder_timing(L)
+    dev = P.Plugin().device(0)
+    out = {"device": torch.cuda.get_device_name(0)}
+    try:
+        for name in ("4k", "2k"):
+            prof = PROFILES[name]
+            lay, fmt, col, frames = _workload(name, nframes)
+            dframes = [torch.from_numpy(f.view(np.int16)).to("cuda:0") for f in frames]
+            torch.cuda.synchronize()
+            enc = dev.encoder(lay, fmt, col)
+            try:
+                stage_ms = _stage_timer(L, enc, dframes, prof, nframes)
+                table = {}
+                for t1 in range(3):
+                    for tn in range(3):
+                        cfg = dict(DEFAULTS, dwtTile1=t1, dwtTileN=tn)
+                        table[f"{t1},{tn}"] = round(min(stage_ms(cfg, (0,)) for _ in range(runs)), 4)
+                        log(f"[{name}] dwtTile1={t1} dwtTileN={tn}: {table[f'{t1},{tn}']:.4f} ms")
+            finally:
+                enc.close()
+                set_tuning(prof, None)
+            out[name] = table
+    finally:
+        dev.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default="tuning.json")
     ap.add_argument("--quick", action="store_true")
+    ap.add_argument("--tiles", action="store_true",
+                    help="only time every pair of front-end tile shapes and print the table")
     args = ap.parse_args()
+    if args.tiles:
+        print(json.dumps(tile_sweep()))
+        return
     res = tune(quick=args.quick)
     with open(args.out, "w") as f:
         json.dump(res, f, indent=1)
