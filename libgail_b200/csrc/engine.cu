@@ -44,6 +44,7 @@ double msBetween(Clock::time_point a, Clock::time_point b) {
 }  // namespace
 
 constexpr uint32_t kBatchSoloFloor = 16384;  // MQ solo threshold of batched launches, at least
+constexpr int kMaxSlots = 1024;               // frame slots an engine makes at most (per-slot arrays)
 
 struct EncodeEngine::Class {
     Layout L;
@@ -169,7 +170,6 @@ EncodeEngine::EncodeEngine(int device, uint64_t hbmBudget, int maxBatch) : dev_(
     budget_ = hbmBudget;
     for (auto& f : front_) GB_CHECK(cudaStreamCreateWithFlags(&f, cudaStreamNonBlocking));
     GB_CHECK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
-    constexpr int kMaxSlots = 1024;
     check(cudaMalloc(&dSlope_, kMaxSlots * 4), "device memory for the engine");
     check(cudaHostAlloc((void**)&hSlope_, kMaxSlots * 4, cudaHostAllocDefault), "pinned host memory");
     check(cudaHostAlloc((void**)&hZero_, 16, cudaHostAllocDefault), "pinned host memory");
@@ -416,18 +416,27 @@ void EncodeEngine::slotMaker() {
 
 EncodeEngine::Slot* EncodeEngine::newSlot(int cls) {
     Class* cp;
-    int index;
     {
         std::lock_guard<std::mutex> lock(m_);
         cp = classes_[cls].get();
-        index = nextSlotIndex_++;  // the slot thread and reserve() may make slots at once
     }
     Class& c = *cp;
-    if (index >= 1024) return nullptr;
     {
         std::lock_guard<std::mutex> lock(budgetM_);
         if (used_ + c.slotBytes > budgetLocked()) return nullptr;
         used_ += c.slotBytes;  // reserved now, given back if the slot cannot be made
+    }
+    // the slot's index into the per-slot arrays, taken only once the budget allows the slot
+    // (the slot thread and reserve() may make slots at once)
+    int index;
+    {
+        std::lock_guard<std::mutex> lock(m_);
+        index = nextSlotIndex_ < kMaxSlots ? nextSlotIndex_++ : -1;
+    }
+    if (index < 0) {
+        std::lock_guard<std::mutex> lock(budgetM_);
+        used_ -= c.slotBytes;
+        return nullptr;
     }
     auto s = std::make_unique<Slot>();
     s->cls = cls;
