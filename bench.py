@@ -305,7 +305,11 @@ def run_ours(args):
     col = P.color("pq", "bt2020")
     ncblk = lay.abi.numCblks
     budget, _ = CS.dci_limits(FPS)
-    workers = max(2, min(16, (os.cpu_count() or 8) - 2))
+    # host workers for the codestreams: the CPUs this process may use, shared by the ranks on
+    # this node, less two for the engine's own threads
+    usable = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 8)
+    per_node = int(os.environ.get("LOCAL_WORLD_SIZE", world))
+    workers = max(2, min(16, usable // max(1, per_node) - 2))
     sms = torch.cuda.get_device_properties(local).multi_processor_count
 
     # ---- served: the batched engine, rate control and Tier-2 on the device -------------
