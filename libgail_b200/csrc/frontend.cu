@@ -134,11 +134,10 @@ __device__ void planarRgb(const void* src, const PlanarParams& p, int x, int y, 
 }
 
 // 12-bit code: the number of thresholds at or below n (thr[0] = 0, thr ascending). A
-// fast power gives a guess within a code or two; the thresholds then decide exactly, with
-// a binary search when the guess is further off than a few steps.
-__device__ __forceinline__ int dciCode(const float* __restrict__ thr, float n) {
-    int k = (int)(4095.f * __powf(n, 1.f / 2.6f) + 0.5f);
-    k = min(max(k, 0), 4095);
+// fast power gives a guess within a code or two; four neighbouring thresholds, loaded at
+// once, decide among the guess and the codes either side of it, and a walk (then a binary
+// search) takes the rare guess further off.
+__device__ __noinline__ int dciCodeSearch(const float* __restrict__ thr, float n, int k) {
 #pragma unroll 1
     for (int it = 0; it < 8; ++it) {
         if (k < 4095 && __ldg(thr + k + 1) <= n) {
@@ -154,6 +153,13 @@ __device__ __forceinline__ int dciCode(const float* __restrict__ thr, float n) {
     for (int step = 2048; step > 0; step >>= 1)
         if (k + step <= 4095 && __ldg(thr + k + step) <= n) k += step;
     return k;
+}
+__device__ __forceinline__ int dciCode(const float* __restrict__ thr, float n) {
+    const int k = (int)(4095.f * __powf(n, 1.f / 2.6f) + 0.5f);
+    const int b = min(max(k, 1), 4093);
+    const float t0 = __ldg(thr + b - 1), t1 = __ldg(thr + b), t2 = __ldg(thr + b + 1), t3 = __ldg(thr + b + 2);
+    if (t0 <= n && t3 > n) return b - 1 + (t1 <= n ? 1 : 0) + (t2 <= n ? 1 : 0);
+    return dciCodeSearch(thr, n, b);
 }
 
 // ---- the managed and LUT routes (kernels/color_math.h:25-179) ----
