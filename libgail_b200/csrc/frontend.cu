@@ -92,24 +92,27 @@ __device__ void planarRgb(const void* src, const PlanarParams& p, int x, int y, 
     const int x0 = (int)cxp, x1 = min(x0 + 1, p.cw - 1);
     const float fx = cxp - x0;
     const size_t uOff = (size_t)p.aw * p.ah, vOff = uOff + (size_t)p.cw * p.ch;
+    // all four neighbours of both chroma planes and the luma sample are loaded at once (x1,
+    // y1 are in the plane); a weight of exactly zero multiplies a finite sample >= 0 to +0,
+    // and adding +0 changes nothing, so the result is the interpolation's whatever the weights
+    float s[9];
+    {
+        const size_t r0 = (size_t)y0 * p.cw, r1 = (size_t)y1 * p.cw;
+        const size_t at[9] = {uOff + r0 + x0, uOff + r0 + x1, uOff + r1 + x0, uOff + r1 + x1,
+                              vOff + r0 + x0, vOff + r0 + x1, vOff + r1 + x0, vOff + r1 + x1,
+                              (size_t)ay * p.aw + ax};
+#pragma unroll
+        for (int i = 0; i < 9; ++i) s[i] = sampleAt(src, p.bits, at[i]);
+    }
     float uv[2];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-        const size_t off = k ? vOff : uOff;
-        // a weight of exactly zero multiplies a finite sample >= 0 to +0, and adding +0
-        // changes nothing: those loads are skipped, the arithmetic kept
-        const float a = sampleAt(src, p.bits, off + (size_t)y0 * p.cw + x0);
-        const float b = fx != 0.f ? sampleAt(src, p.bits, off + (size_t)y0 * p.cw + x1) : 0.f;
-        const float top = a * (1 - fx) + b * fx;
-        float bot = 0.f;
-        if (fy != 0.f) {
-            const float c = sampleAt(src, p.bits, off + (size_t)y1 * p.cw + x0);
-            const float d = fx != 0.f ? sampleAt(src, p.bits, off + (size_t)y1 * p.cw + x1) : 0.f;
-            bot = c * (1 - fx) + d * fx;
-        }
+        const float* q = s + 4 * k;
+        const float top = q[0] * (1 - fx) + q[1] * fx;
+        const float bot = q[2] * (1 - fx) + q[3] * fx;
         uv[k] = top * (1 - fy) + bot * fy;
     }
-    float Y = sampleAt(src, p.bits, (size_t)ay * p.aw + ax), U = uv[0], V = uv[1];
+    float Y = s[8], U = uv[0], V = uv[1];
     float v[3];
     if (p.rgb) {  // planes G', B', R'
         v[0] = V / p.maxv;
