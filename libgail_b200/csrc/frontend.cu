@@ -356,28 +356,57 @@ __device__ __forceinline__ void liftLine(float* t, int step) {
 template <int THREADS, int SHAPE>
 __device__ void writeOutputs(const LevelArgs& a, const float* t, int comp, int tx, int ty, int tid) {
     using T = Tile<SHAPE>;
-    const int x0 = tx * T::X - HALO, y0 = ty * T::Y - HALO;
-    for (int o = 0; o < 4; ++o) {
-        const BandOut& b = a.band[comp][o];
-        const bool quant = o != 0 || a.last;
-        for (int idx = tid; idx < T::CBX * T::CBY * kCblkArea; idx += THREADS) {
-            const int cb = idx >> 10, e = idx & (kCblkArea - 1);
-            const int cbx = tx * T::CBX + cb % T::CBX, cby = ty * T::CBY + cb / T::CBX;
-            if (cbx >= b.ncbx || cby >= b.ncby) continue;
-            const int i = e & 31, j = e >> 5;
-            const int bx = cbx * 32 + i, by = cby * 32 + j;
-            const bool in = bx < b.w && by < b.h;
-            float v = 0.f;
-            if (in) {
-                const int gx = 2 * bx + (o & 1), gy = 2 * by + (o >> 1);
-                v = t[(gy - y0) * T::P + (gx - x0)];
+    if constexpr (T::CBX == 1 && T::CBY == 1) {  // the 64 x 64 tile
+        // one 32 x 32 code-block per band: a thread keeps one column of the block (lane =
+        // column, so the rows go out coalesced) and steps down its rows; the band's sample
+        // (column i, row j of the block) sits at tile column HALO + 2 i + (o & 1) and row
+        // HALO + 2 j + (o >> 1)
+        static_assert(THREADS % 32 == 0, "whole warps");
+        const int i = tid & 31;
+        for (int o = 0; o < 4; ++o) {
+            const BandOut& b = a.band[comp][o];
+            if (tx >= b.ncbx || ty >= b.ncby) continue;
+            const bool quant = o != 0 || a.last;
+            const int bx = tx * 32 + i;
+            const bool inx = bx < b.w;
+            const float* col = t + (HALO + (o >> 1)) * T::P + HALO + 2 * i + (o & 1);
+            uint32_t* blk = a.coeffs + ((size_t)b.cblkBase + (size_t)ty * b.ncbx + tx) * kCblkArea;
+            for (int j = tid >> 5; j < 32; j += THREADS / 32) {
+                const int by = ty * 32 + j;
+                const bool in = inx && by < b.h;
+                const float v = in ? col[2 * j * T::P] : 0.f;
+                if (quant) {
+                    blk[j * 32 + i] = in ? quantize(v, b.invDelta, b.maxMag) : 0u;
+                    if (in && a.tap) a.tap[comp * a.tapComp + (size_t)(b.py0 + by) * a.tapStride + b.px0 + bx] = v;
+                } else if (in) {
+                    a.ll[comp * a.llComp + (size_t)by * a.llStride + bx] = v;
+                }
             }
-            if (quant) {
-                uint32_t* blk = a.coeffs + ((size_t)b.cblkBase + (size_t)cby * b.ncbx + cbx) * kCblkArea;
-                blk[e] = in ? quantize(v, b.invDelta, b.maxMag) : 0u;
-                if (in && a.tap) a.tap[comp * a.tapComp + (size_t)(b.py0 + by) * a.tapStride + b.px0 + bx] = v;
-            } else if (in) {
-                a.ll[comp * a.llComp + (size_t)by * a.llStride + bx] = v;
+        }
+    } else {
+        const int x0 = tx * T::X - HALO, y0 = ty * T::Y - HALO;
+        for (int o = 0; o < 4; ++o) {
+            const BandOut& b = a.band[comp][o];
+            const bool quant = o != 0 || a.last;
+            for (int idx = tid; idx < T::CBX * T::CBY * kCblkArea; idx += THREADS) {
+                const int cb = idx >> 10, e = idx & (kCblkArea - 1);
+                const int cbx = tx * T::CBX + cb % T::CBX, cby = ty * T::CBY + cb / T::CBX;
+                if (cbx >= b.ncbx || cby >= b.ncby) continue;
+                const int i = e & 31, j = e >> 5;
+                const int bx = cbx * 32 + i, by = cby * 32 + j;
+                const bool in = bx < b.w && by < b.h;
+                float v = 0.f;
+                if (in) {
+                    const int gx = 2 * bx + (o & 1), gy = 2 * by + (o >> 1);
+                    v = t[(gy - y0) * T::P + (gx - x0)];
+                }
+                if (quant) {
+                    uint32_t* blk = a.coeffs + ((size_t)b.cblkBase + (size_t)cby * b.ncbx + cbx) * kCblkArea;
+                    blk[e] = in ? quantize(v, b.invDelta, b.maxMag) : 0u;
+                    if (in && a.tap) a.tap[comp * a.tapComp + (size_t)(b.py0 + by) * a.tapStride + b.px0 + bx] = v;
+                } else if (in) {
+                    a.ll[comp * a.llComp + (size_t)by * a.llStride + bx] = v;
+                }
             }
         }
     }
