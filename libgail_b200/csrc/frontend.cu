@@ -480,9 +480,12 @@ __global__ void __launch_bounds__(feThreads<MODE, SHAPE>(), feMinCtas<MODE, SHAP
         }
     } else {
         const float* src = a.src + blockIdx.z * a.srcComp;
+        // a thread's loads of the tile, several in flight at once (the later levels' grids
+        // are small: each CTA's load latency is most of its time)
+#pragma unroll 4
         for (int idx = tid; idx < T::WX * T::WY; idx += THREADS) {
             const int ly = idx / T::WX, lx = idx % T::WX;
-            smem[ly * T::P + lx] = src[(size_t)mirror(y0 + ly, h) * a.srcStride + mirror(x0 + lx, w)];
+            smem[ly * T::P + lx] = __ldg(src + (size_t)mirror(y0 + ly, h) * a.srcStride + mirror(x0 + lx, w));
         }
     }
     __syncthreads();
